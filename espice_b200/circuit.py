@@ -1,0 +1,277 @@
+"""Circuit description for the sweep-lane library: unknown numbering and the
+per-type instance tables the C ABI (``include/espice_lanes.h``) takes.
+
+This is the host half of the reference's frozen circuit
+(``src/device/Circuit.zig:77-167``): node 0 is ground and is row/column 0 of
+the matrix, held by a unit pin; every other unknown is an external node, a
+device-internal node (a diode's ``ai`` behind RS, a MOSFET's ``di``/``si``
+behind RD/RS) or a voltage source's branch current. External nodes are
+numbered in order of first use, then internal unknowns in batch order.
+
+Device tables mirror the Verilog-A parameter lists the reference compiles
+(``models/{resistor,capacitor,vsource,isource,diode,mos1}.va``). Values are
+the card values; bias-independent temperature maps run in the library.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+R, C, V, I, D, M = 0, 1, 2, 3, 4, 5
+NODES_PER = {R: 2, C: 2, V: 3, I: 2, D: 3, M: 6}
+
+# Diode parameter slots (models/diode.va:35-103).
+D_PARAMS = ["is", "n", "rs", "bv", "ibv", "cjo", "vj", "m", "fc", "tt", "area",
+            "gmin", "xti", "eg", "tnom", "temp"]
+D_DEFAULTS = dict(is_=1e-14, n=1.0, rs=0.0, bv=0.0, ibv=1e-3, cjo=0.0, vj=1.0, m=0.5,
+                  fc=0.5, tt=0.0, area=1.0, gmin=1e-12, xti=3.0, eg=1.11, tnom=27.0,
+                  temp=300.15)
+
+# MOS1 parameter slots (models/mos1.va:20-85); type +1 NMOS, -1 PMOS.
+M_PARAMS = ["type", "vto", "kp", "gamma", "phi", "lambda", "rd", "rs", "cbd", "cbs",
+            "is", "pb", "cgso", "cgdo", "cgbo", "cj", "mj", "cjsw", "mjsw", "tox",
+            "ld", "u0", "fc", "w", "l", "ad", "as", "pd", "ps", "delvto", "m", "gmin",
+            "tnom", "temp"]
+M_DEFAULTS = {"type": 1.0, "vto": 0.0, "kp": 2e-5, "gamma": 0.0, "phi": 0.6, "lambda": 0.0,
+              "rd": 0.0, "rs": 0.0, "cbd": 0.0, "cbs": 0.0, "is": 1e-14, "pb": 0.8,
+              "cgso": 0.0, "cgdo": 0.0, "cgbo": 0.0, "cj": 0.0, "mj": 0.5, "cjsw": 0.0,
+              "mjsw": 0.5, "tox": 0.0, "ld": 0.0, "u0": 600.0, "fc": 0.5, "w": 1e-4,
+              "l": 1e-4, "ad": 0.0, "as": 0.0, "pd": 0.0, "ps": 0.0, "delvto": 0.0,
+              "m": 1.0, "gmin": 1e-12, "tnom": 27.0, "temp": 300.15}
+
+V_PARAMS = ["dc", "wave", "v1", "v2", "td", "tr", "tf", "pw", "per", "phase"]
+PARAMS_PER = {R: 1, C: 1, V: len(V_PARAMS), I: 1, D: len(D_PARAMS), M: len(M_PARAMS)}
+PARAM_NAMES = {R: ["r"], C: ["c"], V: V_PARAMS, I: ["dc"], D: D_PARAMS, M: M_PARAMS}
+TYPE_ORDER = [R, C, V, I, D, M]
+TYPE_LETTER = {R: "R", C: "C", V: "V", I: "I", D: "D", M: "M"}
+
+
+@dataclass
+class _Dev:
+    name: str
+    type: int
+    ext: list          # external node names
+    params: list
+    internal: list = field(default_factory=list)  # "a"/"ai" markers resolved at freeze
+
+
+class Circuit:
+    """A netlist under construction; ``freeze`` numbers the unknowns."""
+
+    def __init__(self, temp_c: float = 27.0):
+        self.node_ids = {"0": 0, "gnd": 0}
+        self.devs: list[_Dev] = []
+        self.temp_k = temp_c + 273.15
+        self._frozen = None
+
+    def node(self, name) -> int:
+        name = str(name).lower()
+        if name not in self.node_ids:
+            self.node_ids[name] = len([k for k in self.node_ids if k != "gnd"])
+        return self.node_ids[name]
+
+    def _add(self, name, typ, ext, params):
+        for e in ext:
+            self.node(e)
+        self.devs.append(_Dev(name.lower(), typ, [str(e).lower() for e in ext], list(params)))
+        self._frozen = None
+
+    def R(self, name, p, n, r):
+        self._add(name, R, [p, n], [float(r)])
+
+    def C(self, name, p, n, c):
+        self._add(name, C, [p, n], [float(c)])
+
+    def V(self, name, p, n, dc=0.0, pulse=None):
+        prm = [float(dc), 0.0, 0, 0, 0, -1.0, -1.0, -1.0, -1.0, 0.0]
+        if pulse is not None:
+            prm[1] = 1.0
+            vals = list(pulse) + [None] * (8 - len(pulse))
+            defaults = [0.0, 0.0, 0.0, -1.0, -1.0, -1.0, -1.0, 0.0]
+            for k in range(8):
+                prm[2 + k] = float(vals[k]) if vals[k] is not None else defaults[k]
+        self._add(name, V, [p, n], prm)
+
+    def I(self, name, p, n, dc=0.0):
+        self._add(name, I, [p, n], [float(dc)])
+
+    def D(self, name, a, c, area=1.0, **model):
+        kw = dict(D_DEFAULTS)
+        kw["temp"] = self.temp_k
+        for k, v in model.items():
+            k = k.lower()
+            k = {"is": "is_", "js": "is_", "cj0": "cjo", "cj": "cjo", "mj": "m"}.get(k, k)
+            if k not in kw:
+                raise ValueError(f"diode parameter {k!r} is not supported")
+            kw[k] = float(v)
+        kw["area"] = float(area)
+        prm = [kw["is_"] if p == "is" else kw[p] for p in D_PARAMS]
+        self._add(name, D, [a, c], prm)
+
+    def M(self, name, d, g, s, b, **params):
+        kw = dict(M_DEFAULTS)
+        kw["temp"] = self.temp_k
+        given_tox = False
+        for k, v in params.items():
+            k = k.lower()
+            k = {"uo": "u0", "lambda_": "lambda"}.get(k, k)
+            if k not in kw:
+                raise ValueError(f"mos1 parameter {k!r} is not supported")
+            kw[k] = float(v)
+            given_tox |= k == "tox"
+        prm = [kw[p] for p in M_PARAMS]
+        self._add(name, M, [d, g, s, b], prm)
+
+    def set_temp(self, temp_c):
+        """Circuit temperature for every device without its own TEMP."""
+        self.temp_k = temp_c + 273.15
+        for d in self.devs:
+            if d.type == D:
+                d.params[D_PARAMS.index("temp")] = self.temp_k
+            elif d.type == M:
+                d.params[M_PARAMS.index("temp")] = self.temp_k
+        self._frozen = None
+
+    # ------------------------------------------------------------------
+    def freeze(self) -> "Frozen":
+        if self._frozen is not None:
+            return self._frozen
+        n_ext = len([k for k in self.node_ids if k != "gnd"])
+        nxt = n_ext
+        names = {v: k for k, v in self.node_ids.items() if k != "gnd"}
+        batches = {}
+        where = {}
+        current = []
+        for t in TYPE_ORDER:
+            devs = [d for d in self.devs if d.type == t]
+            if not devs:
+                continue
+            nodes = np.zeros((len(devs), NODES_PER[t]), dtype=np.uint32)
+            prm = np.zeros((len(devs), PARAMS_PER[t]), dtype=np.float64)
+            for i, d in enumerate(devs):
+                ext = [self.node_ids[e] for e in d.ext]
+                if t == V:
+                    ext.append(nxt)
+                    names[nxt] = f"i({d.name})"
+                    current.append(nxt)
+                    nxt += 1
+                elif t == D:
+                    if d.params[D_PARAMS.index("rs")] > 0:
+                        ext.append(nxt)
+                        names[nxt] = f"{d.name}#ai"
+                        nxt += 1
+                    else:
+                        ext.append(ext[0])
+                elif t == M:
+                    rd = d.params[M_PARAMS.index("rd")]
+                    rs = d.params[M_PARAMS.index("rs")]
+                    if rd > 0:
+                        ext.append(nxt)
+                        names[nxt] = f"{d.name}#di"
+                        nxt += 1
+                    else:
+                        ext.append(ext[0])
+                    if rs > 0:
+                        ext.append(nxt)
+                        names[nxt] = f"{d.name}#si"
+                        nxt += 1
+                    else:
+                        ext.append(ext[2])
+                nodes[i] = ext
+                prm[i] = d.params
+                where[d.name] = (len(batches), i)
+            batches[t] = (nodes, prm)
+        n = nxt
+        cur = np.zeros(n, dtype=np.uint8)
+        cur[current] = 1
+        self._frozen = Frozen(n, [(t, *batches[t]) for t in batches], cur, names, where,
+                              dict(self.node_ids))
+        return self._frozen
+
+
+class _Batch(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_uint32), ("count", ctypes.c_uint32),
+                ("nodes", ctypes.POINTER(ctypes.c_uint32)),
+                ("params", ctypes.POINTER(ctypes.c_double))]
+
+
+class _Circuit(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint32), ("n_batches", ctypes.c_uint32),
+                ("batches", ctypes.POINTER(_Batch)),
+                ("current_row", ctypes.POINTER(ctypes.c_uint8))]
+
+
+class Slot(ctypes.Structure):
+    """One swept parameter: batch, instance, parameter index."""
+    _fields_ = [("batch", ctypes.c_uint32), ("inst", ctypes.c_uint32),
+                ("param", ctypes.c_uint32)]
+
+
+class Frozen:
+    """A numbered circuit: ``n`` unknowns and one table per device type.
+
+    ``struct()`` returns the C view (``esl_circuit`` / ``orc_circuit``, one
+    layout) that stays valid while this object lives.
+    """
+
+    def __init__(self, n, batches, current_row, names, where, node_ids):
+        self.n = n
+        self.batches = [(t, np.ascontiguousarray(nd), np.ascontiguousarray(p))
+                        for t, nd, p in batches]
+        self.current_row = current_row
+        self.names = names
+        self.where = where
+        self.node_ids = node_ids
+        self._c = None
+
+    def struct(self):
+        if self._c is None:
+            arr = (_Batch * max(1, len(self.batches)))()
+            for i, (t, nd, p) in enumerate(self.batches):
+                arr[i].type = t
+                arr[i].count = nd.shape[0]
+                arr[i].nodes = nd.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+                arr[i].params = p.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            c = _Circuit(self.n, len(self.batches), arr,
+                         self.current_row.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+            self._c = (c, arr)
+        return self._c[0]
+
+    def slot(self, device, param) -> Slot:
+        """The sweep slot of ``device``'s ``param`` (card names)."""
+        b, i = self.where[device.lower()]
+        t = self.batches[b][0]
+        return Slot(b, i, PARAM_NAMES[t].index(param.lower()))
+
+    def slots_of(self, type_, param):
+        """Every instance of one device type, for per-device variation."""
+        out = []
+        for b, (t, nd, _) in enumerate(self.batches):
+            if t == type_:
+                k = PARAM_NAMES[t].index(param)
+                out += [Slot(b, i, k) for i in range(nd.shape[0])]
+        return out
+
+    def param(self, slot: Slot) -> float:
+        return float(self.batches[slot.batch][2][slot.inst, slot.param])
+
+    def unknown(self, name) -> int:
+        """Index of a node voltage v(name) or a branch current i(vname)."""
+        name = name.lower()
+        if name.startswith("v(") and name.endswith(")"):
+            return self.node_ids[name[2:-1]]
+        if name.startswith("i(") and name.endswith(")"):
+            for k, v in self.names.items():
+                if v == name:
+                    return k
+            raise KeyError(name)
+        return self.node_ids[name]
+
+    def slots_array(self, slots):
+        arr = (Slot * max(1, len(slots)))()
+        for i, s in enumerate(slots):
+            arr[i] = s
+        return arr

@@ -1,0 +1,167 @@
+/*
+ * TEST INFRASTRUCTURE, NOT PRODUCT CODE.
+ *
+ * CPU oracle for the sweep-lane Newton path: a plain C (FP64, no FMA
+ * contraction) restatement of the reference's CPU algorithm, used only by
+ * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg to check
+ * and time the CUDA library. Nothing in espice_b200/ links or imports it.
+ *
+ * Reference files restated (paths inside the ESPice project):
+ *   src/device/Circuit.zig:77-167            frozen CSC pattern, ground row 0
+ *   src/solver/order.zig                     BTF (Tarjan) + AMD + natural fallback
+ *   src/solver/sparse_lu.zig:260-1224        Gilbert-Peierls factor/refactor/solve
+ *   src/solver/direct.zig:32-55,228-383      bypass, refactor, replayHolds, re-pivot
+ *   src/solver/converger.zig:85-122,199-522,794-819   Newton gates
+ *   src/device/eval.zig:782-922              stamp, limiting correction
+ *   models/{resistor,capacitor,vsource,isource,diode,mos1}.va
+ *   src/analysis/dc/dc.zig:163-386           sequential .dc sweep
+ *   src/analysis/sweep/lanes.zig:34-92       independent sweep points
+ *   src/analysis/tran/{integrator,tran}.zig  trapezoidal transient + LTE
+ *
+ * Parity pinning: the reference cannot be built here (Zig 0.18-dev and its
+ * un-vendored VerA/Gompute dependencies are absent). The oracle is pinned
+ * against the reference's own ngspice-44.2 golden fixtures (DC rtol 1e-6,
+ * transient rtol 1e-3) committed under tests/golden/, and against the
+ * reference's bitwise self-consistency properties (lane == scalar).
+ */
+#ifndef ESPICE_ORACLE_H
+#define ESPICE_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Device types and their per-instance layouts (node count, param count). */
+enum {
+    ORC_R = 0,  /* nodes p n;          params r                          */
+    ORC_C = 1,  /* nodes p n;          params c                          */
+    ORC_V = 2,  /* nodes p n br;       params dc wave v1 v2 td tr tf pw per phase */
+    ORC_I = 3,  /* nodes p n;          params dc                         */
+    ORC_D = 4,  /* nodes a c ai;       params see ORC_D_* (ai == a: RS collapsed) */
+    ORC_M = 5,  /* nodes d g s b di si; params see ORC_M_*               */
+    ORC_NTYPES = 6
+};
+
+/* Diode parameter slots (models/diode.va). */
+enum {
+    ORC_D_IS = 0, ORC_D_N, ORC_D_RS, ORC_D_BV, ORC_D_IBV, ORC_D_CJO, ORC_D_VJ,
+    ORC_D_M, ORC_D_FC, ORC_D_TT, ORC_D_AREA, ORC_D_GMIN, ORC_D_XTI, ORC_D_EG,
+    ORC_D_TNOM, ORC_D_TEMP, ORC_D_NP
+};
+
+/* MOS1 parameter slots (models/mos1.va). TYPE = +1 NMOS, -1 PMOS. */
+enum {
+    ORC_M_TYPE = 0, ORC_M_VTO, ORC_M_KP, ORC_M_GAMMA, ORC_M_PHI, ORC_M_LAMBDA,
+    ORC_M_RD, ORC_M_RS, ORC_M_CBD, ORC_M_CBS, ORC_M_IS, ORC_M_PB, ORC_M_CGSO,
+    ORC_M_CGDO, ORC_M_CGBO, ORC_M_CJ, ORC_M_MJ, ORC_M_CJSW, ORC_M_MJSW,
+    ORC_M_TOX, ORC_M_LD, ORC_M_U0, ORC_M_FC, ORC_M_W, ORC_M_L, ORC_M_AD,
+    ORC_M_AS, ORC_M_PD, ORC_M_PS, ORC_M_DELVTO, ORC_M_M, ORC_M_GMIN,
+    ORC_M_TNOM, ORC_M_TEMP, ORC_M_NP
+};
+
+typedef struct {
+    uint32_t type;
+    uint32_t count;
+    const uint32_t *nodes;  /* count * nodes_per_type */
+    const double *params;   /* count * params_per_type */
+} orc_batch;
+
+typedef struct {
+    uint32_t n;             /* unknowns, ground row 0 included */
+    uint32_t n_batches;
+    const orc_batch *batches;
+    const uint8_t *current_row; /* n: 1 for a branch-current unknown */
+} orc_circuit;
+
+/* One swept parameter slot: batch, instance, param index. */
+typedef struct {
+    uint32_t batch, inst, param;
+} orc_slot;
+
+typedef struct {
+    double reltol, abstol, vntol, residual_tol, gmin;
+    uint32_t max_iter;      /* before the max(itl, 100) raise */
+} orc_newton_opts;
+
+int orc_nodes_per(uint32_t type);
+int orc_params_per(uint32_t type);
+
+/* Pattern (Circuit.freeze): CSC with every diagonal, rows ascending.
+ * col_ptr has n + 1 entries; row_idx capacity is given; returns nnz or -1. */
+int64_t orc_pattern(const orc_circuit *c, uint32_t *col_ptr, uint32_t *row_idx, size_t cap);
+
+/* Column order (order.zig `order`). 0 on success. */
+int orc_order(uint32_t n, const uint32_t *col_ptr, const uint32_t *row_idx, uint32_t *q);
+
+/* Full factor of one matrix (direct.Solver.factor from a fresh solver),
+ * exporting the pivot tape. Sizes out: counts[0] = nnz_L, counts[1] = nnz_U.
+ * Any output pointer may be NULL. Returns 0, or 1 for a singular matrix. */
+int orc_factor_tape(uint32_t n, const uint32_t *col_ptr, const uint32_t *row_idx,
+                    const double *vals, uint32_t *q, uint32_t *pinv,
+                    uint32_t *lp, uint32_t *li, double *lx,
+                    uint32_t *up, uint32_t *ui, double *ux, double *udiag,
+                    uint8_t *flags, uint32_t *counts, size_t cap);
+
+/* Refactor of `vals` on the tape a full factor of `lead` made, then
+ * dx = -A^-1 rhs; `bad` = the lane kernel's peel verdict (pivot test,
+ * growth, non-finite, wide multiplier). Bitwise the reference's
+ * lane_kernels.Bodies.refactor + solveNeg on the host. */
+int orc_lane_refactor_solve(uint32_t n, const uint32_t *col_ptr, const uint32_t *row_idx,
+                            const double *lead, uint32_t n_lanes, const double *vals,
+                            const double *rhs, double *dx, double *lx_out, double *ux_out,
+                            double *udiag_out, uint8_t *bad);
+
+/* Each lane a direct.Solver of its own: factor (bypass / refactor+replayHolds
+ * / full factor) then solveNeg, over `rounds` rounds of values per lane.
+ * vals [rounds][n_lanes][nnz], rhs [rounds][n_lanes][n] -> dx same shape,
+ * status [rounds][n_lanes] (0 ok, 1 singular). */
+int orc_solver_rounds(uint32_t n, const uint32_t *col_ptr, const uint32_t *row_idx,
+                      uint32_t rounds, uint32_t n_lanes, const double *vals,
+                      const double *rhs, double *dx, uint8_t *status);
+
+/* Independent DC sweep points (sweep/lanes.zig solveLanes): each lane
+ * installs its slot values, starts from `warm` (n values) or cold, and
+ * runs converger.run. x_out [n_lanes][n], iters, conv per lane. */
+int orc_dc_points(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
+                  const double *values, uint32_t n_lanes, const double *warm,
+                  const orc_newton_opts *opts, double *x_out, uint32_t *iters,
+                  uint8_t *conv);
+
+/* Sequential .dc sweep (dc.zig Sweep): point 0 cold, later points warm
+ * from the 2*last - prev predictor limited against the last point; a failed
+ * warm point takes the plain cold rung. x_out [n_pts][n]. */
+int orc_dc_sweep(const orc_circuit *c, orc_slot slot, const double *values,
+                 uint32_t n_pts, const orc_newton_opts *opts, double *x_out,
+                 uint32_t *iters, uint8_t *conv);
+
+/* Operating point (op.zig solve, plain rung, cold start). */
+int orc_op(const orc_circuit *c, const orc_newton_opts *opts, double *x_out,
+           uint32_t *iters);
+
+/* Transient (tran.zig Sim with HostOps; trapezoidal, order promotion,
+ * LTE step control, breakpoints): lanes independent, each with its slot
+ * values. Records the solution at every accepted step into a probe trace:
+ * probe_nodes[n_probes]; out_t / out_v capacity max_pts per lane;
+ * n_pts_out per lane; stats per lane: [accepted, rejected_newton,
+ * rejected_lte, newton_iters]. x_final [n_lanes][n]. */
+typedef struct {
+    double tstop, tstep, tmax;  /* .tran tstep tstop, max step */
+    double reltol, abstol, vntol, chgtol, trtol;
+    uint32_t itl4;
+    uint32_t method;            /* 1 trap (only) */
+    uint32_t max_steps;
+} orc_tran_opts;
+
+int orc_tran(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
+             const double *values, uint32_t n_lanes, const orc_tran_opts *topts,
+             const double *x0, const uint32_t *probe_nodes, uint32_t n_probes,
+             uint32_t max_pts, double *out_t, double *out_v, uint32_t *n_pts_out,
+             uint32_t *stats, double *x_final);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

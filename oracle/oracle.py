@@ -1,0 +1,170 @@
+"""TEST INFRASTRUCTURE: ctypes binding of the CPU oracle (liboracle.so).
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg load
+this module, as the checker of the CUDA library; the library never does.
+The oracle restates the reference's FP64 CPU path (see espice_oracle.h for
+the file map) and is pinned against the reference's ngspice-44.2 fixtures.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+_lib = None
+
+u32p = ctypes.POINTER(ctypes.c_uint32)
+f64p = ctypes.POINTER(ctypes.c_double)
+u8p = ctypes.POINTER(ctypes.c_uint8)
+
+
+class NewtonOpts(ctypes.Structure):
+    _fields_ = [("reltol", ctypes.c_double), ("abstol", ctypes.c_double),
+                ("vntol", ctypes.c_double), ("residual_tol", ctypes.c_double),
+                ("gmin", ctypes.c_double), ("max_iter", ctypes.c_uint32)]
+
+
+def newton_opts(reltol=1e-3, abstol=1e-12, vntol=1e-6, residual_tol=1e-9, gmin=0.0, max_iter=50):
+    return NewtonOpts(reltol, abstol, vntol, residual_tol, gmin, max_iter)
+
+
+def build():
+    """Compiles liboracle.so from oracle/*.c (make)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        _lib = ctypes.CDLL(LIB)
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def pattern(frozen):
+    cap = frozen.n + 64 + sum(nd.shape[0] * 80 for _, nd, _ in frozen.batches)
+    cp = np.zeros(frozen.n + 1, np.uint32)
+    ri = np.zeros(cap, np.uint32)
+    f = lib().orc_pattern
+    f.restype = ctypes.c_int64
+    nnz = f(ctypes.byref(frozen.struct()), _p(cp, u32p), _p(ri, u32p), ctypes.c_size_t(cap))
+    assert nnz >= 0
+    return cp, ri[:nnz].copy()
+
+
+def order(n, cp, ri):
+    q = np.zeros(n, np.uint32)
+    lib().orc_order(ctypes.c_uint32(n), _p(cp, u32p), _p(ri, u32p), _p(q, u32p))
+    return q
+
+
+def factor_tape(n, cp, ri, vals):
+    """Fresh direct.Solver full factor: q, pinv, lp, li, lx, up, ui, ux, udiag, flags."""
+    cap = 64 * (int(cp[n]) + n) + 64
+    out = dict(q=np.zeros(n, np.uint32), pinv=np.zeros(n, np.uint32),
+               lp=np.zeros(n + 1, np.uint32), li=np.zeros(cap, np.uint32),
+               lx=np.zeros(cap), up=np.zeros(n + 1, np.uint32), ui=np.zeros(cap, np.uint32),
+               ux=np.zeros(cap), udiag=np.zeros(n), flags=np.zeros(n, np.uint8))
+    counts = np.zeros(3, np.uint32)
+    vals = np.ascontiguousarray(vals, np.float64)
+    rc = lib().orc_factor_tape(
+        ctypes.c_uint32(n), _p(cp, u32p), _p(ri, u32p), _p(vals, f64p),
+        _p(out["q"], u32p), _p(out["pinv"], u32p), _p(out["lp"], u32p), _p(out["li"], u32p),
+        _p(out["lx"], f64p), _p(out["up"], u32p), _p(out["ui"], u32p), _p(out["ux"], f64p),
+        _p(out["udiag"], f64p), _p(out["flags"], u8p), _p(counts, u32p), ctypes.c_size_t(cap))
+    nl, nu = int(counts[0]), int(counts[1])
+    for k in ("li", "lx"):
+        out[k] = out[k][:nl].copy()
+    for k in ("ui", "ux"):
+        out[k] = out[k][:nu].copy()
+    out["n_void_slots"] = int(counts[2])
+    return rc, out
+
+
+def lane_refactor_solve(n, cp, ri, lead, vals, rhs):
+    """Bitwise host replay of the device refactor + solveNeg on lead's tape."""
+    rc, tape = factor_tape(n, cp, ri, lead)
+    assert rc == 0
+    lanes = vals.shape[0]
+    nl, nu = len(tape["li"]), len(tape["ui"])
+    dx = np.zeros((lanes, n))
+    lx = np.zeros((lanes, nl))
+    ux = np.zeros((lanes, nu))
+    ud = np.zeros((lanes, n))
+    bad = np.zeros(lanes, np.uint8)
+    vals = np.ascontiguousarray(vals, np.float64)
+    rhs = np.ascontiguousarray(rhs, np.float64)
+    lead = np.ascontiguousarray(lead, np.float64)
+    lib().orc_lane_refactor_solve(
+        ctypes.c_uint32(n), _p(cp, u32p), _p(ri, u32p), _p(lead, f64p), ctypes.c_uint32(lanes),
+        _p(vals, f64p), _p(rhs, f64p), _p(dx, f64p), _p(lx, f64p), _p(ux, f64p), _p(ud, f64p),
+        _p(bad, u8p))
+    return dict(dx=dx, lx=lx, ux=ux, udiag=ud, bad=bad, tape=tape)
+
+
+def solver_rounds(n, cp, ri, vals, rhs):
+    """vals [rounds][lanes][nnz], rhs [rounds][lanes][n]: per-lane direct.Solver."""
+    rounds, lanes = vals.shape[:2]
+    dx = np.zeros((rounds, lanes, n))
+    st = np.zeros((rounds, lanes), np.uint8)
+    vals = np.ascontiguousarray(vals, np.float64)
+    rhs = np.ascontiguousarray(rhs, np.float64)
+    lib().orc_solver_rounds(ctypes.c_uint32(n), _p(cp, u32p), _p(ri, u32p),
+                            ctypes.c_uint32(rounds), ctypes.c_uint32(lanes), _p(vals, f64p),
+                            _p(rhs, f64p), _p(dx, f64p), _p(st, u8p))
+    return dx, st
+
+
+def dc_points(frozen, slots, values, warm=None, opts=None):
+    """Independent sweep points (sweep/lanes.zig): x [lanes][n], iters, conv."""
+    opts = opts or newton_opts()
+    values = np.ascontiguousarray(values, np.float64).reshape(-1, max(1, len(slots)))
+    lanes = values.shape[0]
+    x = np.zeros((lanes, frozen.n))
+    it = np.zeros(lanes, np.uint32)
+    cv = np.zeros(lanes, np.uint8)
+    sa = frozen.slots_array(slots)
+    wp = None
+    if warm is not None:
+        warm = np.ascontiguousarray(warm, np.float64)
+        wp = _p(warm, f64p)
+    rc = lib().orc_dc_points(ctypes.byref(frozen.struct()), sa, ctypes.c_uint32(len(slots)),
+                             _p(values, f64p), ctypes.c_uint32(lanes), wp, ctypes.byref(opts),
+                             _p(x, f64p), _p(it, u32p), _p(cv, u8p))
+    assert rc == 0
+    return x, it, cv
+
+
+def dc_sweep(frozen, slot, values, opts=None):
+    """Sequential .dc sweep (dc.zig): x [points][n], iters, conv."""
+    opts = opts or newton_opts()
+    values = np.ascontiguousarray(values, np.float64)
+    pts = len(values)
+    x = np.zeros((pts, frozen.n))
+    it = np.zeros(pts, np.uint32)
+    cv = np.zeros(pts, np.uint8)
+    rc = lib().orc_dc_sweep(ctypes.byref(frozen.struct()), slot, _p(values, f64p),
+                            ctypes.c_uint32(pts), ctypes.byref(opts), _p(x, f64p),
+                            _p(it, u32p), _p(cv, u8p))
+    assert rc == 0
+    return x, it, cv
+
+
+def op(frozen, opts=None):
+    opts = opts or newton_opts(max_iter=100)
+    x = np.zeros(frozen.n)
+    it = ctypes.c_uint32(0)
+    rc = lib().orc_op(ctypes.byref(frozen.struct()), ctypes.byref(opts), _p(x, f64p),
+                      ctypes.byref(it))
+    return x, int(it.value), rc

@@ -1,0 +1,63 @@
+"""Regenerates tests/golden/*.json from the reference's own fixture corpus.
+
+Each golden file holds one reference deck (its .sp text) and the oracle
+values the reference checks it against (its .expected.json: ngspice-44.2 or
+analytic columns, with the per-column tolerances the reference scores at,
+tests/test_correctness.zig:397-398). Run in a container that has the
+reference checked out; the outputs are committed so tests never read it.
+
+    python tests/golden/make_golden.py /path/to/reference
+"""
+
+import json
+import os
+import sys
+
+FIXTURES = [
+    # DC sweeps: R, V, I, diode
+    "dc/bench_ensemble_sweep_lanes",
+    "dc/bench_dc_sweep_vin_sweep",
+    "dc/device_diode_iv_sweep",
+    "dc/device_diode_breakdown",
+    "dc/diode_forward",
+    "dc/diode_reverse",
+    "dc/diode_reverse_continuation",
+    "dc/bench_power_zener_reg",
+    "dc/device_diode_temp",
+    # operating points
+    "convergence/diode_stack_8",
+    "convergence/bench_diode_bridge",
+    "convergence/diode_knee",
+    "op/bench_medium_resistor_mesh",
+    "stress/scaling_resistor_grid_32x32",
+    # MOS1
+    "dc/device_mos1_transfer",
+    "dc/device_mos1_output",
+    "dc/bench_mosfet_cmos_inverter",
+    "tran/device_mos1_large_signal",
+]
+
+
+def main(ref):
+    here = os.path.dirname(os.path.abspath(__file__))
+    for f in FIXTURES:
+        base = os.path.join(ref, "tests", "fixtures", f)
+        with open(base + ".sp") as fh:
+            deck = fh.read()
+        with open(base + ".expected.json") as fh:
+            exp = json.load(fh)
+        out = {
+            "source": "tests/fixtures/" + f + ".sp",
+            "deck": deck,
+            "analysis": exp["analysis"],
+            "oracle": exp["oracle"]["kind"],
+            "plots": exp["expect"]["plots"],
+        }
+        name = f.replace("/", "__") + ".json"
+        with open(os.path.join(here, name), "w") as fh:
+            json.dump(out, fh, indent=1)
+        print("wrote", name)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,73 @@
+"""Test helper: runs a golden fixture deck through the oracle (or a library
+entry point with the same signature) and scores it as the reference does:
+|got - expected| <= atol + rtol * |expected| per column
+(tests/test_correctness.zig:625-627), on the selected rows."""
+
+import glob
+import json
+import os
+
+import numpy as np
+
+from netlist import Deck, sweep_values
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    with open(os.path.join(GOLDEN, name + ".json")) as fh:
+        return json.load(fh)
+
+
+def names(prefix=""):
+    out = []
+    for p in sorted(glob.glob(os.path.join(GOLDEN, "*.json"))):
+        n = os.path.basename(p)[:-5]
+        if n.startswith(prefix):
+            out.append(n)
+    return out
+
+
+def solve_deck(g, dc_sweep, op):
+    """Returns (frozen, rows [n_rows][n]) for the deck's analysis."""
+    deck = Deck(g["deck"])
+    ckt = deck.circuit()
+    an = deck.analysis
+    if an[0] == "op":
+        fr = ckt.freeze()
+        x, it, rc = op(fr, deck.newton_opts())
+        return fr, x[None, :], np.array([rc == 0])
+    assert an[0] == "dc"
+    inner = sweep_values(an[2], an[3], an[4])
+    outer = [None]
+    if len(an) > 5:
+        outer = sweep_values(an[6], an[7], an[8])
+    rows, conv = [], []
+    fr = None
+    for ov in outer:
+        if ov is not None:
+            if an[5] == "temp":
+                ckt.set_temp(ov)
+            else:
+                raise NotImplementedError("nested source sweep")
+        fr = ckt.freeze()
+        slot = fr.slot(an[1], "dc")
+        x, it, cv = dc_sweep(fr, slot, np.array(inner), deck.newton_opts())
+        rows.append(x)
+        conv.append(cv)
+    return fr, np.concatenate(rows), np.concatenate(conv)
+
+
+def score(g, fr, rows):
+    """List of (column, worst ratio err/allowed, n checked)."""
+    out = []
+    for plot in g["plots"]:
+        idx = plot.get("row_indices") or list(range(plot["row_count"]))
+        for col, spec in plot["columns"].items():
+            k = fr.unknown(col)
+            got = rows[idx, k]
+            exp = np.array(spec["values"], dtype=float)
+            allowed = spec["atol"] + spec["rtol"] * np.abs(exp)
+            err = np.abs(got - exp)
+            out.append((col, float(np.max(err / allowed)), len(exp)))
+    return out

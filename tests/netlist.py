@@ -1,0 +1,166 @@
+"""Test helper: reads the small SPICE decks of the golden fixtures (R, C, V,
+I, D, M cards, .model, .dc, .op, .tran, .options, .temp) into a
+``espice_b200.circuit.Circuit``. Parsing is not on the sweep-lane path; this
+covers only what the committed fixtures use.
+"""
+
+from __future__ import annotations
+
+import re
+
+from espice_b200.circuit import Circuit
+
+_SUFFIX = [("meg", 1e6), ("mil", 25.4e-6), ("t", 1e12), ("g", 1e9), ("k", 1e3),
+           ("m", 1e-3), ("u", 1e-6), ("n", 1e-9), ("p", 1e-12), ("f", 1e-15)]
+
+
+def num(tok: str) -> float:
+    t = tok.strip().lower()
+    m = re.match(r"^([-+]?(?:\d+\.?\d*|\.\d+)(?:e[-+]?\d+)?)([a-z]*)", t)
+    if not m:
+        raise ValueError(tok)
+    v = float(m.group(1))
+    rest = m.group(2)
+    for s, f in _SUFFIX:
+        if rest.startswith(s):
+            return v * f
+    return v
+
+
+def _kv(tokens):
+    out = {}
+    for t in tokens:
+        if "=" in t:
+            k, v = t.split("=", 1)
+            out[k.lower()] = num(v)
+    return out
+
+
+class Deck:
+    def __init__(self, text: str):
+        self.models = {}
+        self.cards = []
+        self.analysis = None
+        self.options = {}
+        self.temp = 27.0
+        lines = []
+        for raw in text.splitlines():
+            s = raw.strip()
+            if not s or s.startswith("*"):
+                continue
+            if s.startswith("+") and lines:
+                lines[-1] += " " + s[1:]
+            else:
+                lines.append(s)
+        for s in lines:
+            s = re.sub(r"\(\s*", "(", s)
+            low = s.lower()
+            if low.startswith(".model"):
+                m = re.match(r"\.model\s+(\S+)\s+(\S+?)\s*\((.*)\)", s, re.I)
+                if m:
+                    name, kind, body = m.group(1).lower(), m.group(2).lower(), m.group(3)
+                else:
+                    parts = s.split()
+                    name, kind, body = parts[1].lower(), parts[2].lower(), " ".join(parts[3:])
+                body = re.sub(r"\s*=\s*", "=", body)
+                self.models[name] = (kind, _kv(body.replace(",", " ").split()))
+            elif low.startswith(".dc"):
+                t = s.split()
+                self.analysis = ("dc", t[1].lower(), num(t[2]), num(t[3]), num(t[4]))
+                if len(t) >= 9:
+                    self.analysis += (t[5].lower(), num(t[6]), num(t[7]), num(t[8]))
+            elif low.startswith(".option"):
+                body = re.sub(r"\s*=\s*", "=", s)
+                self.options.update(_kv(body.split()[1:]))
+            elif low.split()[0] == ".op":
+                self.analysis = ("op",)
+            elif low.startswith(".tran"):
+                t = s.split()
+                self.analysis = ("tran", num(t[1]), num(t[2]))
+            elif low.startswith(".temp"):
+                self.temp = num(s.split()[1])
+            elif low.startswith(".end"):
+                break
+            elif low.startswith("."):
+                continue
+            else:
+                self.cards.append(s)
+        if "temp" in self.options:
+            self.temp = self.options["temp"]
+
+    def circuit(self) -> Circuit:
+        c = Circuit(temp_c=self.temp)
+        tnom = self.options.get("tnom", 27.0)
+        for s in self.cards:
+            t = re.sub(r"\s*=\s*", "=", s).split()
+            name = t[0].lower()
+            kind = name[0]
+            if kind == "r":
+                c.R(name, t[1], t[2], num(t[3]))
+            elif kind == "c":
+                c.C(name, t[1], t[2], num(t[3]))
+            elif kind in "vi":
+                rest = " ".join(t[3:])
+                dc = 0.0
+                pulse = None
+                m = re.search(r"pulse\s*\(([^)]*)\)", rest, re.I)
+                if m:
+                    pulse = [num(v) for v in m.group(1).replace(",", " ").split()]
+                    rest = rest[: m.start()] + rest[m.end():]
+                toks = rest.split()
+                if toks and toks[0].lower() == "dc":
+                    dc = num(toks[1])
+                elif toks:
+                    dc = num(toks[0])
+                if kind == "v":
+                    if pulse is not None and not m.group(0).lower().startswith("dc"):
+                        if not (toks and toks[0].lower() == "dc"):
+                            dc = pulse[0]
+                    c.V(name, t[1], t[2], dc=dc, pulse=pulse)
+                else:
+                    c.I(name, t[1], t[2], dc=dc)
+            elif kind == "d":
+                kindm, prm = self.models[t[3].lower()]
+                prm = dict(prm)
+                prm.setdefault("tnom", tnom)
+                area = 1.0
+                for tok in t[4:]:
+                    if "=" in tok:
+                        k, v = tok.split("=")
+                        if k.lower() == "area":
+                            area = num(v)
+                    else:
+                        area = num(tok)
+                prm.pop("level", None)
+                c.D(name, t[1], t[2], area=area, **prm)
+            elif kind == "m":
+                kindm, prm = self.models[t[5].lower()]
+                prm = dict(prm)
+                prm.pop("level", None)
+                prm.setdefault("tnom", tnom)
+                prm["type"] = 1.0 if kindm == "nmos" else -1.0
+                prm.update(_kv(t[6:]))
+                c.M(name, t[1], t[2], t[3], t[4], **prm)
+            else:
+                raise ValueError(f"card {s!r} is not supported")
+        return c
+
+    def newton_opts(self):
+        return dict(reltol=self.options.get("reltol", 1e-3),
+                    abstol=self.options.get("abstol", 1e-12),
+                    vntol=self.options.get("vntol", 1e-6))
+
+
+def sweep_values(start, stop, step):
+    """ngspice's accumulated sweep axis (v += step), as dc.zig steps it."""
+    import math
+    if step == 0 or (stop - start) * math.copysign(1.0, step) < 0:
+        n = 1
+    else:
+        n = int(math.floor((stop - start) / step + 1e-6)) + 1
+    out = []
+    v = start
+    for _ in range(n):
+        out.append(v)
+        v += step
+    return out

@@ -1,0 +1,27 @@
+"""The oracle against the reference's own golden fixtures (ngspice-44.2 and
+analytic oracles, scored at the reference's per-column tolerances)."""
+
+import pytest
+
+import golden_util as gu
+from oracle import oracle
+
+
+def _dc(fr, slot, values, opts):
+    return oracle.dc_sweep(fr, slot, values, oracle.newton_opts(**opts))
+
+
+def _op(fr, opts):
+    return oracle.op(fr, oracle.newton_opts(max_iter=100, **opts))
+
+
+DC_OP = [n for n in gu.names() if "mos" not in n and not n.startswith("tran")]
+
+
+@pytest.mark.parametrize("name", DC_OP)
+def test_oracle_matches_golden(name):
+    g = gu.load(name)
+    fr, rows, conv = gu.solve_deck(g, _dc, _op)
+    assert conv.all(), f"{name}: {int((~conv.astype(bool)).sum())} points did not converge"
+    for col, worst, count in gu.score(g, fr, rows):
+        assert worst <= 1.0, f"{name} {col}: error {worst:.3g}x the allowed tolerance"
