@@ -1,0 +1,64 @@
+"""Builds libespice_lanes.so in-tree with nvcc for sm_100a.
+
+The library is the product: CUDA kernels (csrc/kernels) and the C++ host
+runtime behind the C ABI (csrc/host, include/espice_lanes.h). Device code
+builds with --fmad=false and host code with -ffp-contract=off, so the
+refactor, solves and stamps round as the reference's strict-float Zig.
+"""
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB = os.path.join(HERE, "libespice_lanes.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+SOURCES = [
+    "csrc/host/sparse.cpp",
+    "csrc/host/schedule.cpp",
+    "csrc/host/records.cpp",
+    "csrc/host/api.cpp",
+    "csrc/kernels/newton.cu",
+]
+
+
+def sources():
+    return [os.path.join(HERE, s) for s in SOURCES]
+
+
+def headers():
+    out = [os.path.join(ROOT, "include", "espice_lanes.h")]
+    for d in ("csrc", "csrc/host", "csrc/kernels"):
+        p = os.path.join(HERE, d)
+        out += [os.path.join(p, f) for f in os.listdir(p) if f.endswith((".h", ".hpp", ".cuh"))]
+    return out
+
+
+def stale():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(f) > t for f in sources() + headers())
+
+
+def build(force=False, verbose=False):
+    if not force and not stale():
+        return LIB
+    cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3",
+           "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
+           "-Xptxas", "-v" if verbose else "-O3",
+           "-shared", "-o", LIB] + sources() + ["-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed building libespice_lanes.so")
+    if verbose:
+        sys.stderr.write(r.stderr)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force=True, verbose="-v" in sys.argv)
+    print(LIB)

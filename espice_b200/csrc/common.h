@@ -1,0 +1,64 @@
+// Structures shared by the host runtime and the CUDA kernels of the
+// sweep-lane library. Plain C++ (no CUDA types) so both compilers read it.
+#pragma once
+
+#include <cstdint>
+
+namespace esl {
+
+// Device types, numbered as the C ABI numbers them (include/espice_lanes.h).
+enum DevType : uint32_t { kR = 0, kC = 1, kV = 2, kI = 3, kD = 4, kM = 5, kNumTypes = 6 };
+
+constexpr int kMaxBatches = 8;
+
+// Fixed per-type staging layout: the cells one instance's eval writes, in
+// this order. The host's gather lists reference these positions.
+//   R: f0 f1 J00 J01 J10 J11
+//   C: q0 q1 C00 C01 C10 C11
+//   V: f0 f1 f2 J02 J12 J20 J21
+//   I: f0 f1
+//   D: f0 f1 f2 J00 J02 J11 J12 J20 J21 J22 | q1 q2 C11 C12 C21 C22
+constexpr int kStageR = 6, kStageC = 6, kStageV = 7, kStageI = 2, kStageD = 16;
+
+// Per-instance record fields (doubles, field-major per batch in a lane's
+// record block). Diode fields follow the bias-independent part of
+// models/diode.va.
+enum DiodeField {
+  kDVte, kDIs, kDVcrit, kDRs, kDGmin, kDBv, kDXbv, kDVtebrk, kDCjo, kDVj, kDMt, kDFc, kDTt,
+  kDHasRs, kDHasQ, kDiodeFields
+};
+constexpr int kRFields = 1, kCFields = 1, kVFields = 10, kIFields = 1;
+
+// Special gather sources beside staging positions.
+constexpr uint32_t kSrcOne = 0xfffffffeu;    // + 1.0 (the ground pin on g)
+constexpr uint32_t kSrcX0 = 0xfffffffdu;     // + x[0] (the ground pin on rhs)
+constexpr uint32_t kNoDiag = 0xffffffffu;
+
+// One op of a warp program over a lane's shared-memory values v (the tape
+// values, then the permuted right-hand side y). word0 = dst | (kind << 28);
+// word1 = a | (b << 16).
+enum OpKind : uint32_t {
+  kOpFlop = 0,       // v[dst] -= v[a] * v[b]
+  kOpDivGrowth = 1,  // v[dst] = v[dst] / v[a]; peel unless |v[a]| >= growth * |v[dst]|
+  kOpDivScaled = 2,  // v[dst] = v[dst] / v[a]; peel on a non-finite quotient
+  kOpSubNz = 3,      // v[dst] -= v[a] * v[b] when v[b] != 0 (the solves' zero skip)
+  kOpDivY = 4,       // v[dst] = v[dst] / v[a]
+  kOpNop = 7,
+};
+
+struct LaneOpts {
+  double reltol, abstol, vntol, residual_tol, gmin;
+  uint32_t max_iter;
+  uint32_t init_fix;
+};
+
+// Lane status words (device -> host).
+enum LaneStatus : uint32_t {
+  kRunning = 0,
+  kConverged = 1,
+  kMaxIter = 2,
+  kSingular = 3,
+  kNeedSolve = 4,   // paused at the linear solve: the host factors this lane
+};
+
+}  // namespace esl

@@ -1,0 +1,705 @@
+// C ABI of the sweep-lane library (include/espice_lanes.h): the host half
+// of the reference's GpuLanes (src/analysis/gpu_lanes.zig:349-1027) for DC
+// sweep lanes. It freezes the pattern, orders it, builds the stamp gather
+// tables, factors the lead lane's first Jacobian into the pivot tape,
+// compiles that tape into warp programs, and runs the fused Newton kernel;
+// lanes the frozen tape cannot stand in for pause and take a host factor
+// on their own direct solver (lane_solver.zig:76-131), then resume.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../../include/espice_lanes.h"
+#include "../kernels/launch.h"
+#include "records.hpp"
+#include "schedule.hpp"
+#include "sparse.hpp"
+
+using namespace esl;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  cudaError_t ensure(size_t b) {
+    if (b <= bytes && p) return cudaSuccess;
+    release();
+    bytes = b ? b : 8;
+    return cudaMalloc(&p, bytes);
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+struct HostBatch {
+  uint32_t type = 0, count = 0, nt = 0, np = 0;
+  uint32_t stage_base = 0, stride = 0, rec_off = 0, nfields = 0, lim_off = 0;
+  std::vector<uint32_t> nodes;
+  std::vector<double> params;
+};
+
+uint32_t stage_stride(uint32_t type) {
+  switch (type) {
+    case kR: return kStageR;
+    case kC: return kStageC;
+    case kV: return kStageV;
+    case kI: return kStageI;
+    case kD: return kStageD;
+    default: return 0;
+  }
+}
+
+// The cells one instance writes, in stamp order: its residual rows (local
+// row, staging position) and its Jacobian entries (local row, local column,
+// staging position), as src/device/eval.zig:864-895 orders them. Charge
+// entries are the transient planes' and are not gathered for DC.
+struct Entry {
+  uint8_t ru, cu, pos;
+};
+struct InstLayout {
+  std::vector<Entry> res, jac, q, qjac;
+};
+
+InstLayout layout_of(uint32_t type, const double* prm) {
+  InstLayout L;
+  switch (type) {
+    case kR:
+      L.res = {{0, 0, 0}, {1, 0, 1}};
+      L.jac = {{0, 0, 2}, {0, 1, 3}, {1, 0, 4}, {1, 1, 5}};
+      break;
+    case kC:
+      L.q = {{0, 0, 0}, {1, 0, 1}};
+      L.qjac = {{0, 0, 2}, {0, 1, 3}, {1, 0, 4}, {1, 1, 5}};
+      break;
+    case kV:
+      L.res = {{0, 0, 0}, {1, 0, 1}, {2, 0, 2}};
+      L.jac = {{0, 2, 3}, {1, 2, 4}, {2, 0, 5}, {2, 1, 6}};
+      break;
+    case kI:
+      L.res = {{0, 0, 0}, {1, 0, 1}};
+      break;
+    case kD: {
+      const bool rs = prm[2] > 0;
+      if (rs) L.res.push_back({0, 0, 0});
+      L.res.push_back({1, 0, 1});
+      L.res.push_back({2, 0, 2});
+      if (rs) {
+        L.jac.push_back({0, 0, 3});
+        L.jac.push_back({0, 2, 4});
+      }
+      L.jac.push_back({1, 1, 5});
+      L.jac.push_back({1, 2, 6});
+      if (rs) L.jac.push_back({2, 0, 7});
+      L.jac.push_back({2, 1, 8});
+      L.jac.push_back({2, 2, 9});
+      if (prm[5] > 0 || prm[9] > 0) {
+        L.q = {{1, 0, 10}, {2, 0, 11}};
+        L.qjac = {{1, 1, 12}, {1, 2, 13}, {2, 1, 14}, {2, 2, 15}};
+      }
+      break;
+    }
+    default:
+      break;
+  }
+  return L;
+}
+
+template <class T>
+cudaError_t upload(DevBuf& b, const std::vector<T>& v, cudaStream_t s) {
+  cudaError_t e = b.ensure(v.size() * sizeof(T));
+  if (e != cudaSuccess || v.empty()) return e;
+  return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+}  // namespace
+
+struct esl_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  uint32_t lanes_per_block = 4;
+
+  Csc pat;
+  std::vector<uint8_t> cur;
+  std::vector<uint32_t> order;
+  std::vector<HostBatch> bats;
+  uint32_t n_stage = 0, rec_size = 0, nlim = 0;
+  std::vector<uint32_t> rhs_ptr, rhs_src, a_ptr, a_src, slot_row;
+  std::vector<double> rec_nominal;
+
+  uint32_t n_lanes = 0;
+  std::vector<double> rec_lanes;
+
+  bool have_tape = false;
+  SparseLu lead;
+  Programs prog;
+
+  DevBuf d_nodes[kMaxBatches], d_rhs_ptr, d_rhs_src, d_a_ptr, d_a_src, d_slot_row, d_cur;
+  DevBuf d_amap, d_fill, d_a_ops, d_b_ops, d_l_scaled, d_pinv, d_q;
+  DevBuf d_rec, d_lim, d_lim_active, d_status, d_iters, d_flags, d_limit, d_a_vals, d_rhs, d_dx,
+      d_diag, d_paused, d_x;
+  TopoDev topo{};
+
+  std::unordered_map<uint32_t, DirectSolver> peel;
+
+  int32_t fail(int32_t code, const std::string& what) {
+    err = what;
+    return code;
+  }
+  int32_t cuda_fail(cudaError_t e, const char* where) {
+    err = std::string(where) + ": " + cudaGetErrorString(e);
+    return ESL_DEVICE_FAULT;
+  }
+};
+
+#define ESL_CUDA(call)                                   \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return ctx->cuda_fail(e_, #call); \
+  } while (0)
+
+namespace {
+
+// Pattern (Circuit.freeze): every diagonal, then every device entry off
+// ground; CSC with rows ascending.
+Csc build_pattern(const std::vector<HostBatch>& bats, uint32_t n) {
+  std::vector<uint64_t> keys;
+  for (uint32_t i = 0; i < n; ++i) keys.push_back((uint64_t(i) << 32) | i);
+  for (const auto& B : bats)
+    for (uint32_t id = 0; id < B.count; ++id) {
+      const uint32_t* nd = &B.nodes[size_t(id) * B.nt];
+      InstLayout L = layout_of(B.type, &B.params[size_t(id) * B.np]);
+      for (auto* list : {&L.jac, &L.qjac})
+        for (const Entry& e : *list) {
+          const uint32_t r = nd[e.ru], c = nd[e.cu];
+          if (r != 0 && c != 0) keys.push_back((uint64_t(c) << 32) | r);
+        }
+    }
+  std::sort(keys.begin(), keys.end());
+  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+  Csc pat;
+  pat.n = n;
+  pat.col_ptr.assign(n + 1, 0);
+  for (uint64_t k : keys) {
+    pat.row_idx.push_back(uint32_t(k & 0xffffffffu));
+    pat.col_ptr[(k >> 32) + 1]++;
+  }
+  for (uint32_t j = 0; j < n; ++j) pat.col_ptr[j + 1] += pat.col_ptr[j];
+  return pat;
+}
+
+// Copies a C-ABI circuit into host batches; false on a bad table.
+bool read_circuit(const esl_circuit* c, std::vector<HostBatch>& bats) {
+  uint32_t stage = 0, rec = 0, lim = 0;
+  for (uint32_t b = 0; b < c->n_batches; ++b) {
+    const esl_batch& src = c->batches[b];
+    if (src.type >= kNumTypes) return false;
+    HostBatch B;
+    B.type = src.type;
+    B.count = src.count;
+    B.nt = node_count(src.type);
+    B.np = param_count(src.type);
+    B.nodes.assign(src.nodes, src.nodes + size_t(src.count) * B.nt);
+    B.params.assign(src.params, src.params + size_t(src.count) * B.np);
+    for (uint32_t v : B.nodes)
+      if (v >= c->n) return false;
+    B.stride = stage_stride(src.type);
+    B.stage_base = stage;
+    stage += B.stride * B.count;
+    B.nfields = record_fields(src.type);
+    B.rec_off = rec;
+    rec += B.nfields * B.count;
+    B.lim_off = lim;
+    if (src.type == kD) lim += B.count;
+    bats.push_back(std::move(B));
+  }
+  return true;
+}
+
+// Gather lists: for each residual row and pattern slot, its staging cells
+// in stamp order, then the ground pin on row 0 and slot (0, 0).
+void build_gather(esl_ctx* ctx) {
+  const uint32_t n = ctx->pat.n, nnz = ctx->pat.nnz();
+  std::vector<std::vector<uint32_t>> rows(n), slots(nnz);
+  for (const auto& B : ctx->bats)
+    for (uint32_t id = 0; id < B.count; ++id) {
+      const uint32_t* nd = &B.nodes[size_t(id) * B.nt];
+      InstLayout L = layout_of(B.type, &B.params[size_t(id) * B.np]);
+      const uint32_t base = B.stage_base + id * B.stride;
+      for (const Entry& e : L.res)
+        if (nd[e.ru] != 0) rows[nd[e.ru]].push_back(base + e.pos);
+      for (const Entry& e : L.jac) {
+        const uint32_t s = ctx->pat.slot(nd[e.ru], nd[e.cu]);
+        if (s != nnz) slots[s].push_back(base + e.pos);
+      }
+    }
+  rows[0].push_back(kSrcX0);
+  slots[ctx->pat.col_ptr[0]].push_back(kSrcOne);
+  auto flatten = [](const std::vector<std::vector<uint32_t>>& v, std::vector<uint32_t>& ptr,
+                    std::vector<uint32_t>& src) {
+    ptr.assign(v.size() + 1, 0);
+    src.clear();
+    for (size_t i = 0; i < v.size(); ++i) {
+      src.insert(src.end(), v[i].begin(), v[i].end());
+      ptr[i + 1] = uint32_t(src.size());
+    }
+  };
+  flatten(rows, ctx->rhs_ptr, ctx->rhs_src);
+  flatten(slots, ctx->a_ptr, ctx->a_src);
+  ctx->slot_row.assign(nnz, kNoDiag);
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t s = i == 0 ? ctx->pat.col_ptr[0] : ctx->pat.slot(i, i);
+    ctx->slot_row[s] = i;
+  }
+}
+
+int32_t upload_topology(esl_ctx* ctx) {
+  cudaStream_t s = ctx->stream;
+  TopoDev& T = ctx->topo;
+  T.n = ctx->pat.n;
+  T.nnz = ctx->pat.nnz();
+  T.n_stage = ctx->n_stage;
+  T.nlim = ctx->nlim;
+  T.rec_size = ctx->rec_size;
+  T.n_batches = uint32_t(ctx->bats.size());
+  for (size_t b = 0; b < ctx->bats.size(); ++b) {
+    const HostBatch& B = ctx->bats[b];
+    ESL_CUDA(upload(ctx->d_nodes[b], B.nodes, s));
+    T.b[b] = BatchDev{B.type, B.count, B.nt, B.stage_base, B.stride, B.rec_off, B.lim_off,
+                      ctx->d_nodes[b].as<uint32_t>()};
+  }
+  ESL_CUDA(upload(ctx->d_rhs_ptr, ctx->rhs_ptr, s));
+  ESL_CUDA(upload(ctx->d_rhs_src, ctx->rhs_src, s));
+  ESL_CUDA(upload(ctx->d_a_ptr, ctx->a_ptr, s));
+  ESL_CUDA(upload(ctx->d_a_src, ctx->a_src, s));
+  ESL_CUDA(upload(ctx->d_slot_row, ctx->slot_row, s));
+  ESL_CUDA(upload(ctx->d_cur, ctx->cur, s));
+  T.rhs_ptr = ctx->d_rhs_ptr.as<uint32_t>();
+  T.rhs_src = ctx->d_rhs_src.as<uint32_t>();
+  T.a_ptr = ctx->d_a_ptr.as<uint32_t>();
+  T.a_src = ctx->d_a_src.as<uint32_t>();
+  T.slot_row = ctx->d_slot_row.as<uint32_t>();
+  T.cur_row = ctx->d_cur.as<uint8_t>();
+  return ESL_OK;
+}
+
+// The lead lane's pivot tape, compiled and uploaded.
+int32_t upload_tape(esl_ctx* ctx) {
+  cudaStream_t s = ctx->stream;
+  TopoDev& T = ctx->topo;
+  Programs& P = ctx->prog;
+  if (P.has_void) return ctx->fail(ESL_NOT_ELIGIBLE, "the lead factor fabricated a pivot for a void unknown");
+  if (P.ntv + P.n >= 65536) return ctx->fail(ESL_NOT_ELIGIBLE, "tape too large for one lane's shared memory");
+  ESL_CUDA(upload(ctx->d_amap, P.amap, s));
+  ESL_CUDA(upload(ctx->d_fill, P.fill, s));
+  ESL_CUDA(upload(ctx->d_a_ops, P.a_ops, s));
+  ESL_CUDA(upload(ctx->d_b_ops, P.b_ops, s));
+  ESL_CUDA(upload(ctx->d_l_scaled, P.l_scaled, s));
+  ESL_CUDA(upload(ctx->d_pinv, ctx->lead.pinv, s));
+  ESL_CUDA(upload(ctx->d_q, ctx->lead.q, s));
+  T.nu = P.nu;
+  T.nl = P.nl;
+  T.ntv = P.ntv;
+  T.amap = ctx->d_amap.as<uint32_t>();
+  T.fill = ctx->d_fill.as<uint32_t>();
+  T.n_fill = uint32_t(P.fill.size());
+  T.a_ops = ctx->d_a_ops.as<uint2>();
+  T.b_ops = ctx->d_b_ops.as<uint2>();
+  T.a_rows = P.a_rows;
+  T.b_rows = P.b_rows;
+  T.l_scaled = ctx->d_l_scaled.as<uint8_t>();
+  T.pinv = ctx->d_pinv.as<uint32_t>();
+  T.qcol = ctx->d_q.as<uint32_t>();
+  uint32_t d = 5 * T.n + T.ntv + T.n_stage + T.nlim;  // x xo rhs diag | tv y | staging | lim
+  T.smem_doubles = (d + 1) & ~1u;
+  if (size_t(T.smem_doubles) * 8 > 227 * 1024)
+    return ctx->fail(ESL_NOT_ELIGIBLE, "one lane's working set exceeds a CTA's shared memory");
+  ctx->have_tape = true;
+  return ESL_OK;
+}
+
+int32_t build_tape_from(esl_ctx* ctx, const double* lead_vals) {
+  ctx->lead.init(&ctx->pat, ctx->order);
+  ctx->lead.fill_cap = kRepivotFillCap;
+  ctx->lead.keep_min = kGrowthLimit;
+  if (!ctx->lead.factor(lead_vals, kPivotTol))
+    return ctx->fail(ESL_NOT_ELIGIBLE, "the lead lane's first Jacobian is singular");
+  ctx->prog = compile_tape(ctx->lead);
+  return upload_tape(ctx);
+}
+
+LaneDev lane_view(esl_ctx* ctx, uint32_t resume) {
+  LaneDev L{};
+  L.n_lanes = ctx->n_lanes;
+  L.resume = resume;
+  L.rec = ctx->d_rec.as<double>();
+  L.x = ctx->d_x.as<double>();
+  L.lim = ctx->d_lim.as<double>();
+  L.lim_active = ctx->d_lim_active.as<uint32_t>();
+  L.status = ctx->d_status.as<uint32_t>();
+  L.iters = ctx->d_iters.as<uint32_t>();
+  L.flags = ctx->d_flags.as<uint32_t>();
+  L.limit = ctx->d_limit.as<double>();
+  L.a_vals = ctx->d_a_vals.as<double>();
+  L.rhs = ctx->d_rhs.as<double>();
+  L.dx = ctx->d_dx.as<double>();
+  L.diag = ctx->d_diag.as<double>();
+  L.n_paused = ctx->d_paused.as<uint32_t>();
+  return L;
+}
+
+int32_t ensure_lane_buffers(esl_ctx* ctx) {
+  const size_t N = ctx->n_lanes, n = ctx->pat.n, nnz = ctx->pat.nnz();
+  ESL_CUDA(ctx->d_x.ensure(N * n * 8));
+  ESL_CUDA(ctx->d_lim.ensure(N * std::max<size_t>(ctx->nlim, 1) * 8));
+  ESL_CUDA(ctx->d_lim_active.ensure(N * 4));
+  ESL_CUDA(ctx->d_status.ensure(N * 4));
+  ESL_CUDA(ctx->d_iters.ensure(N * 4));
+  ESL_CUDA(ctx->d_flags.ensure(N * 4));
+  ESL_CUDA(ctx->d_limit.ensure(N * 8));
+  ESL_CUDA(ctx->d_a_vals.ensure(N * nnz * 8));
+  ESL_CUDA(ctx->d_rhs.ensure(N * n * 8));
+  ESL_CUDA(ctx->d_dx.ensure(N * n * 8));
+  ESL_CUDA(ctx->d_diag.ensure(N * n * 8));
+  ESL_CUDA(ctx->d_paused.ensure(4));
+  return ESL_OK;
+}
+
+// Host factor + solve of the paused lanes (lane_solver.zig peel), then
+// resume. A lane's first host factor is its own fresh factor when it paused
+// at its first iterate; later it continues the lead tape's replay history.
+int32_t serve_pauses(esl_ctx* ctx, esl_stats* st, bool* any) {
+  cudaStream_t s = ctx->stream;
+  uint32_t paused = 0;
+  ESL_CUDA(cudaMemcpyAsync(&paused, ctx->d_paused.p, 4, cudaMemcpyDeviceToHost, s));
+  ESL_CUDA(cudaStreamSynchronize(s));
+  *any = paused != 0;
+  if (!paused) return ESL_OK;
+  const uint32_t N = ctx->n_lanes, n = ctx->pat.n, nnz = ctx->pat.nnz();
+  std::vector<uint32_t> status(N), iters(N), flags(N);
+  ESL_CUDA(cudaMemcpyAsync(status.data(), ctx->d_status.p, N * 4, cudaMemcpyDeviceToHost, s));
+  ESL_CUDA(cudaMemcpyAsync(iters.data(), ctx->d_iters.p, N * 4, cudaMemcpyDeviceToHost, s));
+  ESL_CUDA(cudaMemcpyAsync(flags.data(), ctx->d_flags.p, N * 4, cudaMemcpyDeviceToHost, s));
+  ESL_CUDA(cudaStreamSynchronize(s));
+  std::vector<double> a(nnz), r(n), dx(n);
+  for (uint32_t l = 0; l < N; ++l) {
+    if (status[l] != kNeedSolve) continue;
+    ESL_CUDA(cudaMemcpy(a.data(), ctx->d_a_vals.as<double>() + size_t(l) * nnz, nnz * 8, cudaMemcpyDeviceToHost));
+    ESL_CUDA(cudaMemcpy(r.data(), ctx->d_rhs.as<double>() + size_t(l) * n, n * 8, cudaMemcpyDeviceToHost));
+    auto it = ctx->peel.find(l);
+    if (it == ctx->peel.end()) {
+      DirectSolver ds;
+      ds.init(&ctx->pat, ctx->order);
+      if (iters[l] != 0) ds.adopt(ctx->lead, nullptr);
+      it = ctx->peel.emplace(l, std::move(ds)).first;
+      it->second.lu.a = &ctx->pat;
+      if (st) st->peeled++;
+    }
+    DirectSolver& ds = it->second;
+    if (st) st->host_solves++;
+    if (!ds.factor(a.data())) {
+      status[l] = kSingular;
+      iters[l] = 0;
+      continue;
+    }
+    ds.solve_neg(r.data(), dx.data());
+    ESL_CUDA(cudaMemcpy(ctx->d_dx.as<double>() + size_t(l) * n, dx.data(), n * 8, cudaMemcpyHostToDevice));
+    if (ds.lu.same_tape(ctx->lead)) flags[l] &= ~2u;
+  }
+  ESL_CUDA(cudaMemcpyAsync(ctx->d_status.p, status.data(), N * 4, cudaMemcpyHostToDevice, s));
+  ESL_CUDA(cudaMemcpyAsync(ctx->d_iters.p, iters.data(), N * 4, cudaMemcpyHostToDevice, s));
+  ESL_CUDA(cudaMemcpyAsync(ctx->d_flags.p, flags.data(), N * 4, cudaMemcpyHostToDevice, s));
+  ESL_CUDA(cudaMemsetAsync(ctx->d_paused.p, 0, 4, s));
+  return ESL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t esl_create(const esl_circuit* circuit, const esl_options* opts, esl_ctx** out) {
+  if (!circuit || !out || circuit->n == 0 || circuit->n_batches > kMaxBatches) return ESL_INVALID_ARGUMENT;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return ESL_NO_DEVICE;
+  auto ctx = std::make_unique<esl_ctx>();
+  ctx->device = opts ? opts->device : 0;
+  if (opts && opts->lanes_per_block) ctx->lanes_per_block = std::min<uint32_t>(opts->lanes_per_block, 8);
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return ESL_NO_DEVICE;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return ESL_DEVICE_FAULT;
+  cudaEventCreate(&ctx->ev0);
+  cudaEventCreate(&ctx->ev1);
+  const uint32_t n = circuit->n;
+  ctx->cur.assign(circuit->current_row, circuit->current_row + n);
+  if (!read_circuit(circuit, ctx->bats)) return ESL_INVALID_ARGUMENT;
+  for (const auto& B : ctx->bats) {
+    if (B.type > kD) return ESL_NOT_ELIGIBLE;
+    ctx->n_stage += B.stride * B.count;
+    ctx->rec_size += B.nfields * B.count;
+    if (B.type == kD) ctx->nlim += B.count;
+  }
+  const uint32_t rec = ctx->rec_size;
+  ctx->pat = build_pattern(ctx->bats, n);
+  build_gather(ctx.get());
+  ctx->order = order_columns(ctx->pat);
+  ctx->rec_nominal.assign(rec, 0.0);
+  for (const auto& B : ctx->bats)
+    for (uint32_t id = 0; id < B.count; ++id)
+      derive_instance(B.type, &B.params[size_t(id) * B.np], &ctx->rec_nominal[B.rec_off + id], B.count);
+  if (int32_t rc = upload_topology(ctx.get())) {
+    *out = ctx.release();
+    return rc;
+  }
+  *out = ctx.release();
+  return ESL_OK;
+}
+
+int32_t esl_destroy(esl_ctx* ctx) {
+  if (!ctx) return ESL_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  cudaStream_t s = ctx->stream;
+  delete ctx;
+  if (s) cudaStreamDestroy(s);
+  return ESL_OK;
+}
+
+const char* esl_last_error(const esl_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int32_t esl_dims(const esl_ctx* ctx, uint32_t* n, uint32_t* nnz) {
+  if (!ctx) return ESL_INVALID_ARGUMENT;
+  if (n) *n = ctx->pat.n;
+  if (nnz) *nnz = ctx->pat.nnz();
+  return ESL_OK;
+}
+
+int32_t esl_set_lanes(esl_ctx* ctx, const esl_slot* slots, uint32_t n_slots, const double* values,
+                      uint32_t n_lanes) {
+  if (!ctx || n_lanes == 0 || (n_slots && (!slots || !values))) return ESL_INVALID_ARGUMENT;
+  for (uint32_t k = 0; k < n_slots; ++k) {
+    if (slots[k].batch >= ctx->bats.size()) return ESL_INVALID_ARGUMENT;
+    const HostBatch& B = ctx->bats[slots[k].batch];
+    if (slots[k].inst >= B.count || slots[k].param >= B.np) return ESL_INVALID_ARGUMENT;
+  }
+  cudaSetDevice(ctx->device);
+  ctx->n_lanes = n_lanes;
+  const size_t R = ctx->rec_size;
+  ctx->rec_lanes.resize(size_t(n_lanes) * R);
+  std::vector<double> prm;
+  for (uint32_t l = 0; l < n_lanes; ++l) {
+    double* rec = &ctx->rec_lanes[size_t(l) * R];
+    std::copy(ctx->rec_nominal.begin(), ctx->rec_nominal.end(), rec);
+    for (uint32_t k = 0; k < n_slots; ++k) {
+      // Instances touched by several slots are re-derived once per slot,
+      // the last time with every override in place.
+      const esl_slot& sl = slots[k];
+      const HostBatch& B = ctx->bats[sl.batch];
+      prm.assign(B.params.begin() + size_t(sl.inst) * B.np, B.params.begin() + size_t(sl.inst + 1) * B.np);
+      for (uint32_t j = 0; j < n_slots; ++j)
+        if (slots[j].batch == sl.batch && slots[j].inst == sl.inst) prm[slots[j].param] = values[size_t(l) * n_slots + j];
+      derive_instance(B.type, prm.data(), rec + B.rec_off + sl.inst, B.count);
+    }
+  }
+  ESL_CUDA(upload(ctx->d_rec, ctx->rec_lanes, ctx->stream));
+  ctx->topo.rec_size = ctx->rec_size;
+  ctx->peel.clear();
+  return ensure_lane_buffers(ctx);
+}
+
+int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d_x, int cold,
+                            uint32_t* d_iters, uint32_t* d_status, esl_stats* st) {
+  if (!ctx || !opts || !d_x || ctx->n_lanes == 0) return ESL_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const uint32_t N = ctx->n_lanes, n = ctx->pat.n;
+  if (st) std::memset(st, 0, sizeof(*st));
+  // Per-lane start state: cold lanes start at zero with the junction seeds
+  // (op.zig coldStart), warm lanes at x with limiting off.
+  std::vector<uint32_t> flags(N, opts->init_fix ? 1u : 0u), act(N, cold && ctx->nlim ? 1u : 0u);
+  std::vector<double> limit(N, 1e9), lim(size_t(N) * std::max<uint32_t>(ctx->nlim, 1), 0.0);
+  if (cold) {
+    for (uint32_t l = 0; l < N; ++l)
+      for (const auto& B : ctx->bats)
+        if (B.type == kD)
+          for (uint32_t i = 0; i < B.count; ++i)
+            lim[size_t(l) * ctx->nlim + B.lim_off + i] = ctx->rec_lanes[size_t(l) * ctx->rec_size + B.rec_off + kDVcrit * B.count + i];
+    ESL_CUDA(cudaMemsetAsync(d_x, 0, size_t(N) * n * 8, s));
+  }
+  ESL_CUDA(cudaMemcpyAsync(ctx->d_flags.p, flags.data(), N * 4, cudaMemcpyHostToDevice, s));
+  ESL_CUDA(cudaMemcpyAsync(ctx->d_lim_active.p, act.data(), N * 4, cudaMemcpyHostToDevice, s));
+  ESL_CUDA(cudaMemcpyAsync(ctx->d_limit.p, limit.data(), N * 8, cudaMemcpyHostToDevice, s));
+  ESL_CUDA(cudaMemcpyAsync(ctx->d_lim.p, lim.data(), lim.size() * 8, cudaMemcpyHostToDevice, s));
+  ESL_CUDA(cudaMemsetAsync(d_status, 0, N * 4, s));
+  ESL_CUDA(cudaMemsetAsync(d_iters, 0, N * 4, s));
+  ESL_CUDA(cudaMemsetAsync(ctx->d_paused.p, 0, 4, s));
+  ctx->peel.clear();
+
+  LaneDev L = lane_view(ctx, 0);
+  L.x = d_x;
+  L.iters = d_iters;
+  L.status = d_status;
+  if (!ctx->have_tape) {
+    // The lead lane's first Jacobian, factored on the host into the tape.
+    ESL_CUDA(launch_assemble(ctx->topo, L, 0, ctx->d_a_vals.as<double>(), s));
+    std::vector<double> a0(ctx->pat.nnz());
+    ESL_CUDA(cudaMemcpyAsync(a0.data(), ctx->d_a_vals.p, a0.size() * 8, cudaMemcpyDeviceToHost, s));
+    ESL_CUDA(cudaStreamSynchronize(s));
+    if (int32_t rc = build_tape_from(ctx, a0.data())) return rc;
+  }
+  LaneOpts o{opts->reltol, opts->abstol, opts->vntol, opts->residual_tol, opts->gmin, opts->max_iter, opts->init_fix};
+  ESL_CUDA(cudaEventRecord(ctx->ev0, s));
+  ESL_CUDA(launch_dc_newton(ctx->topo, L, o, ctx->lanes_per_block, s));
+  uint32_t launches = 1;
+  for (;;) {
+    bool any = false;
+    if (int32_t rc = serve_pauses(ctx, st, &any)) return rc;
+    if (!any) break;
+    LaneDev R = L;
+    R.resume = 1;
+    ESL_CUDA(launch_dc_newton(ctx->topo, R, o, ctx->lanes_per_block, s));
+    ++launches;
+  }
+  ESL_CUDA(cudaEventRecord(ctx->ev1, s));
+  ESL_CUDA(cudaEventSynchronize(ctx->ev1));
+  if (st) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    st->kernel_ms = ms;
+    st->launches = launches;
+    st->lanes = N;
+    std::vector<uint32_t> status(N);
+    ESL_CUDA(cudaMemcpy(status.data(), d_status, N * 4, cudaMemcpyDeviceToHost));
+    for (uint32_t v : status) st->converged += v == kConverged;
+  }
+  return ESL_OK;
+}
+
+int32_t esl_dc_solve(esl_ctx* ctx, const esl_newton_opts* opts, const double* x0, double* x_out,
+                     uint32_t* iters, uint32_t* status, esl_stats* st) {
+  if (!ctx || !opts || !x_out || ctx->n_lanes == 0) return ESL_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  const size_t N = ctx->n_lanes, n = ctx->pat.n;
+  if (x0) ESL_CUDA(cudaMemcpyAsync(ctx->d_x.p, x0, N * n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (int32_t rc = esl_dc_solve_device(ctx, opts, ctx->d_x.as<double>(), x0 == nullptr,
+                                       ctx->d_iters.as<uint32_t>(), ctx->d_status.as<uint32_t>(), st))
+    return rc;
+  ESL_CUDA(cudaMemcpyAsync(x_out, ctx->d_x.p, N * n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (iters) ESL_CUDA(cudaMemcpyAsync(iters, ctx->d_iters.p, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  if (status) ESL_CUDA(cudaMemcpyAsync(status, ctx->d_status.p, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  ESL_CUDA(cudaStreamSynchronize(ctx->stream));
+  return ESL_OK;
+}
+
+int32_t esl_pattern(const esl_circuit* circuit, uint32_t* col_ptr, uint32_t* row_idx, size_t cap,
+                    uint32_t* nnz) {
+  if (!circuit || !col_ptr || !nnz) return ESL_INVALID_ARGUMENT;
+  std::vector<HostBatch> bats;
+  if (!read_circuit(circuit, bats)) return ESL_INVALID_ARGUMENT;
+  Csc pat = build_pattern(bats, circuit->n);
+  *nnz = pat.nnz();
+  std::copy(pat.col_ptr.begin(), pat.col_ptr.end(), col_ptr);
+  if (row_idx && cap >= pat.nnz()) std::copy(pat.row_idx.begin(), pat.row_idx.end(), row_idx);
+  return cap >= pat.nnz() ? ESL_OK : ESL_INVALID_ARGUMENT;
+}
+
+int32_t esl_compile_tape(uint32_t n, const uint32_t* col_ptr, const uint32_t* row_idx, const double* lead,
+                         esl_tape_info* info, uint32_t* q, uint32_t* pinv, uint32_t* amap, uint32_t* fill,
+                         uint32_t* a_ops, uint32_t* b_ops, uint8_t* l_scaled) {
+  if (!col_ptr || !row_idx || !lead || !info || n == 0) return ESL_INVALID_ARGUMENT;
+  Csc pat;
+  pat.n = n;
+  pat.col_ptr.assign(col_ptr, col_ptr + n + 1);
+  pat.row_idx.assign(row_idx, row_idx + col_ptr[n]);
+  SparseLu lu;
+  lu.init(&pat, order_columns(pat));
+  lu.fill_cap = kRepivotFillCap;
+  lu.keep_min = kGrowthLimit;
+  if (!lu.factor(lead, kPivotTol)) return ESL_NOT_ELIGIBLE;
+  Programs P = compile_tape(lu);
+  info->nu = P.nu;
+  info->nl = P.nl;
+  info->ntv = P.ntv;
+  info->n_fill = uint32_t(P.fill.size());
+  info->a_rows = P.a_rows;
+  info->a_levels = P.a_levels;
+  info->a_nops = P.a_nops;
+  info->b_rows = P.b_rows;
+  info->b_levels = P.b_levels;
+  info->b_nops = P.b_nops;
+  info->flops = P.flops;
+  info->has_void = P.has_void;
+  if (q) std::copy(lu.q.begin(), lu.q.end(), q);
+  if (pinv) std::copy(lu.pinv.begin(), lu.pinv.end(), pinv);
+  if (amap) std::copy(P.amap.begin(), P.amap.end(), amap);
+  if (fill) std::copy(P.fill.begin(), P.fill.end(), fill);
+  auto words = [](const std::vector<Op>& ops, uint32_t* out) {
+    for (size_t i = 0; i < ops.size(); ++i) {
+      out[2 * i] = ops[i].w0;
+      out[2 * i + 1] = ops[i].w1;
+    }
+  };
+  if (a_ops) words(P.a_ops, a_ops);
+  if (b_ops) words(P.b_ops, b_ops);
+  if (l_scaled) std::copy(P.l_scaled.begin(), P.l_scaled.end(), l_scaled);
+  return ESL_OK;
+}
+
+int32_t esl_tape(const esl_ctx* ctx, uint32_t* q, uint32_t* pinv, uint32_t* counts) {
+  if (!ctx || !ctx->have_tape) return ESL_INVALID_ARGUMENT;
+  const uint32_t n = ctx->pat.n;
+  if (q) std::copy(ctx->lead.q.begin(), ctx->lead.q.end(), q);
+  if (pinv) std::copy(ctx->lead.pinv.begin(), ctx->lead.pinv.begin() + n, pinv);
+  if (counts) {
+    counts[0] = ctx->prog.nl;
+    counts[1] = ctx->prog.nu;
+    counts[2] = ctx->prog.a_levels;
+    counts[3] = ctx->prog.b_levels;
+  }
+  return ESL_OK;
+}
+
+int32_t esl_tape_size(const esl_ctx* ctx, uint32_t* nu, uint32_t* nl, uint32_t* ntv) {
+  if (!ctx || !ctx->have_tape) return ESL_INVALID_ARGUMENT;
+  if (nu) *nu = ctx->prog.nu;
+  if (nl) *nl = ctx->prog.nl;
+  if (ntv) *ntv = ctx->prog.ntv;
+  return ESL_OK;
+}
+
+int32_t esl_lu_replay_device(esl_ctx* ctx, const double* lead, uint32_t n_lanes, const double* d_a,
+                             const double* d_rhs, double* d_dx, uint8_t* d_bad, double* d_tv, float* ms) {
+  if (!ctx || !d_a || !d_rhs || !d_dx || !d_bad || n_lanes == 0) return ESL_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  if (!ctx->have_tape) {
+    if (!lead) return ESL_INVALID_ARGUMENT;
+    if (int32_t rc = build_tape_from(ctx, lead)) return rc;
+  }
+  ESL_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  ESL_CUDA(launch_lu_replay(ctx->topo, n_lanes, d_a, d_rhs, d_tv, d_dx, d_bad, ctx->lanes_per_block, ctx->stream));
+  ESL_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  ESL_CUDA(cudaEventSynchronize(ctx->ev1));
+  if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
+  return ESL_OK;
+}
+
+}  // extern "C"

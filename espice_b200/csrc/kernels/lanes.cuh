@@ -1,0 +1,74 @@
+// Device-side tables of one topology and of a lane batch, passed to the
+// kernels by value. A lane is one sweep point (or one Monte-Carlo sample):
+// one warp owns it, and its working values live in shared memory for the
+// whole Newton solve; the tables below are read-only and shared by every
+// lane of the topology (broadcast through L1/L2).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../common.h"
+
+namespace esl {
+
+struct BatchDev {
+  uint32_t type, count, nt;     // device type, instances, unknowns per instance
+  uint32_t stage_base, stride;  // staging cells: stage_base + inst * stride
+  uint32_t rec_off;             // record block offset (fields x count, field-major)
+  uint32_t lim_off;             // limited images: lim_off + inst
+  const uint32_t* nodes;        // count * nt unknown indices
+};
+
+struct TopoDev {
+  uint32_t n, nnz, nu, nl, ntv;   // unknowns, pattern, |U|, |L|, tape values (nu + n + nl + 1)
+  uint32_t n_stage, nlim, rec_size;
+  uint32_t n_batches;
+  BatchDev b[kMaxBatches];
+  // Residual gather: row i sums rhs_src[rhs_ptr[i] .. rhs_ptr[i + 1]).
+  const uint32_t* rhs_ptr;
+  const uint32_t* rhs_src;
+  // Matrix gather: pattern slot p sums a_src[a_ptr[p] ..) into tape value
+  // amap[p]; slot_row[p] = i when p is row i's diagonal.
+  const uint32_t* a_ptr;
+  const uint32_t* a_src;
+  const uint32_t* amap;
+  const uint32_t* slot_row;
+  // Tape values no pattern slot writes (fill-in): zeroed per iteration.
+  const uint32_t* fill;
+  uint32_t n_fill;
+  // Warp programs (rows of 32 ops): A = refactor + forward solve, B = back
+  // solve, over v = [tape values | y].
+  const uint2* a_ops;
+  const uint2* b_ops;
+  uint32_t a_rows, b_rows;
+  // L tape values whose column passed on the row-scaled test (no wide test).
+  const uint8_t* l_scaled;
+  // y[pinv[r]] = -rhs[r] before program A; dx[q[j]] = y[j] after program B.
+  const uint32_t* pinv;
+  const uint32_t* qcol;
+  const uint8_t* cur_row;
+  uint32_t smem_doubles;  // per lane
+};
+
+struct LaneDev {
+  uint32_t n_lanes;
+  uint32_t resume;        // 1: lanes paused at the solve take the host's dx
+  const double* rec;      // [lane][rec_size]
+  double* x;              // [lane][n]: start in, solution out
+  double* lim;            // [lane][nlim]
+  uint32_t* lim_active;   // [lane]
+  uint32_t* status;       // [lane] LaneStatus
+  uint32_t* iters;        // [lane]
+  uint32_t* flags;        // [lane] bit 0 INITFIX pending, bit 1 every solve on the host
+  double* limit;          // [lane] runaway bound of this solve
+  double* xo;             // [lane][n]  (pause state)
+  double* a_vals;         // [lane][nnz] (pause: matrix for the host factor)
+  double* rhs;            // [lane][n]   (pause: residual; resume: gate input)
+  double* dx;             // [lane][n]   (resume: the host's step)
+  double* diag;           // [lane][n]   (pause: assembled diagonal for the gate)
+  uint32_t* n_paused;     // device counter
+};
+
+}  // namespace esl

@@ -1,0 +1,518 @@
+// Fused sweep-lane Newton kernel for sm_100a: one warp per lane, the lane's
+// whole working set in shared memory, every phase of a Newton iteration in
+// one launch (eval + stamp -> assemble -> refactor on the lead lane's frozen
+// pivot tape -> forward/back solve -> update -> limiting -> gates), looping
+// on the device until the lane converges, runs out of iterations, or needs
+// the host (a pivot the frozen tape cannot stand in for).
+//
+// Reference path this replaces (src/analysis/gpu_lanes.zig:758-845 and the
+// 12 kernels of src/solver/lane_device.zig, bodies in
+// src/solver/lane_kernels.zig:49-301): there, each Newton tick is eight or
+// more launches of one thread per lane over lane-major HBM planes plus two
+// host syncs. Here one launch runs every tick of every lane.
+//
+// Bitwise contract: the refactor and solve ops use __dmul_rn / __dsub_rn
+// (no FMA contraction) in the reference's operation order per value, so a
+// lane's L, U and dx are bitwise the CPU replay (sparse_lu.zig refactor +
+// solve) on the same matrix. The whole file builds with --fmad=false so the
+// stamp and gates round as the reference's strict-float code does.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include "launch.h"
+#include "lanes.cuh"
+#include "models.cuh"
+
+namespace esl {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr double kGrowth = 1e-12;   // direct.zig refactor_growth_limit
+constexpr double kWide = 1e3;       // 1 / direct.zig pivot_tol
+constexpr double kXPlausible = 1e9; // converger.zig x_plausible
+
+__device__ __forceinline__ uint64_t dbits(double x) { return static_cast<uint64_t>(__double_as_longlong(x)); }
+__device__ __forceinline__ double from_bits(uint64_t u) { return __longlong_as_double(static_cast<long long>(u)); }
+
+__device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint64_t w = __shfl_xor_sync(kFull, v, o);
+    v = w > v ? w : v;
+  }
+  return v;
+}
+
+__device__ __forceinline__ double warp_fmax(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+
+// One lane's shared-memory view. The tape values and the permuted
+// right-hand side are one array v = [tv | y], the value space of the warp
+// programs.
+struct LaneMem {
+  double* x;     // n: current iterate
+  double* xo;    // n: previous iterate
+  double* rhs;   // n: residual F(x)
+  double* diag;  // n: assembled diagonal (gates, runaway bound)
+  double* tv;    // ntv: tape values (U, diagonal, L, discard)
+  double* y;     // n: permuted solve vector, right after tv
+  double* st;    // n_stage: device contributions
+  double* lim;   // nlim: limited junction images
+};
+
+__device__ __forceinline__ LaneMem carve(const TopoDev& T, double* base) {
+  LaneMem m;
+  m.x = base;
+  m.xo = m.x + T.n;
+  m.rhs = m.xo + T.n;
+  m.diag = m.rhs + T.n;
+  m.tv = m.diag + T.n;
+  m.y = m.tv + T.ntv;
+  m.st = m.y + T.n;
+  m.lim = m.st + T.n_stage;
+  return m;
+}
+
+// Device evaluation: every instance of every batch, strided over the warp,
+// each writing its own staging cells (no shared cell, no atomics).
+__device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, bool lim_active,
+                         const SimDev& sim, int tid) {
+  for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
+    const BatchDev& B = T.b[bi];
+    const int s = static_cast<int>(B.count);
+    for (uint32_t i = tid; i < B.count; i += 32) {
+      const uint32_t* nd = B.nodes + size_t(i) * B.nt;
+      double* st = m.st + B.stage_base + size_t(i) * B.stride;
+      const double* r = rec + B.rec_off + i;
+      switch (B.type) {
+        case kR: {
+          const double rv = r[0];
+          const double g = 1.0 / rv;
+          const double cur = (m.x[nd[0]] - m.x[nd[1]]) / rv;
+          st[0] = cur;
+          st[1] = -cur;
+          st[2] = g;
+          st[3] = -g;
+          st[4] = -g;
+          st[5] = g;
+          break;
+        }
+        case kC: {
+          const double c = r[0];
+          const double q = c * (m.x[nd[0]] - m.x[nd[1]]);
+          st[0] = q;
+          st[1] = -q;
+          st[2] = c;
+          st[3] = -c;
+          st[4] = -c;
+          st[5] = c;
+          break;
+        }
+        case kV: {
+          const double v = vsource_value(r, s, sim);
+          const double ib = m.x[nd[2]];
+          st[0] = ib;
+          st[1] = -ib;
+          st[2] = m.x[nd[0]] - m.x[nd[1]] - v;
+          st[3] = 1.0;
+          st[4] = -1.0;
+          st[5] = 1.0;
+          st[6] = -1.0;
+          break;
+        }
+        case kI: {
+          const double v = r[0] * sim.src_scale;
+          st[0] = v;
+          st[1] = -v;
+          break;
+        }
+        case kD:
+          diode_stamp(r, s, m.x[nd[0]], m.x[nd[1]], m.x[nd[2]], lim_active ? m.lim + B.lim_off + i : nullptr, st);
+          break;
+        default:
+          break;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ double gather_value(const LaneMem& m, uint32_t src) {
+  if (src == kSrcOne) return 1.0;
+  if (src == kSrcX0) return m.x[0];
+  return m.st[src];
+}
+
+// Assembly: each residual row and each pattern slot sums its contributions
+// in the reference's stamp order (batch, instance, local row, local column),
+// then the ground pin; the matrix lands in its tape value (amap).
+__device__ void assemble(const TopoDev& T, const LaneMem& m, int tid) {
+  for (uint32_t i = tid; i < T.n; i += 32) {
+    double s = 0.0;
+    for (uint32_t e = T.rhs_ptr[i]; e < T.rhs_ptr[i + 1]; ++e) s = __dadd_rn(s, gather_value(m, T.rhs_src[e]));
+    m.rhs[i] = s;
+  }
+  for (uint32_t j = tid; j < T.n_fill; j += 32) m.tv[T.fill[j]] = 0.0;
+  for (uint32_t p = tid; p < T.nnz; p += 32) {
+    double s = 0.0;
+    for (uint32_t e = T.a_ptr[p]; e < T.a_ptr[p + 1]; ++e) s = __dadd_rn(s, gather_value(m, T.a_src[e]));
+    m.tv[T.amap[p]] = s;
+    const uint32_t row = T.slot_row[p];
+    if (row != kNoDiag) m.diag[row] = s;
+  }
+}
+
+// The matrix in pattern order, for a lane the host factors.
+__device__ void gather_pattern(const TopoDev& T, const LaneMem& m, double* out, int tid) {
+  for (uint32_t p = tid; p < T.nnz; p += 32) {
+    double s = 0.0;
+    for (uint32_t e = T.a_ptr[p]; e < T.a_ptr[p + 1]; ++e) s = __dadd_rn(s, gather_value(m, T.a_src[e]));
+    out[p] = s;
+  }
+}
+
+// Runs one warp program: rows of 32 ops, thread t taking op t of each row,
+// the next row's op fetched while this one runs. Returns true when a
+// division failed its pivot test (thread-local; the caller reduces).
+__device__ __forceinline__ bool run_rows(const uint2* ops, uint32_t rows, double* v, int tid) {
+  bool bad = false;
+  if (rows == 0) return false;
+  uint2 op = ops[tid];
+  for (uint32_t r = 0; r < rows; ++r) {
+    const uint2 next = r + 1 < rows ? ops[(r + 1) * 32 + tid] : op;
+    const uint32_t kind = op.x >> 28, dst = op.x & 0x0fffffffu;
+    const uint32_t a = op.y & 0xffffu, b = op.y >> 16;
+    switch (kind) {
+      case kOpFlop:
+        v[dst] = __dsub_rn(v[dst], __dmul_rn(v[a], v[b]));
+        break;
+      case kOpDivGrowth: {
+        const double w = v[dst], d = v[a];
+        if (!(fabs(d) >= __dmul_rn(kGrowth, fabs(w)))) bad = true;
+        v[dst] = __ddiv_rn(w, d);
+        break;
+      }
+      case kOpDivScaled: {
+        const double l = __ddiv_rn(v[dst], v[a]);
+        if (!(fabs(l) < CUDART_INF)) bad = true;
+        v[dst] = l;
+        break;
+      }
+      case kOpSubNz: {
+        const double yb = v[b];
+        if (yb != 0.0) v[dst] = __dsub_rn(v[dst], __dmul_rn(v[a], yb));
+        break;
+      }
+      case kOpDivY:
+        v[dst] = __ddiv_rn(v[dst], v[a]);
+        break;
+      default:
+        break;
+    }
+    __syncwarp();
+    op = next;
+  }
+  return bad;
+}
+
+// Refactor on the frozen tape with the forward solve merged in (program A),
+// then the lane kernel's peel tests (lane_kernels.zig Bodies.refactor and
+// LaneSolver.wideMultipliers): U entries finite, pivots alive, L multipliers
+// within 1 / pivot_tol. y must hold P(-rhs). Warp-uniform verdict.
+__device__ bool refactor_forward(const TopoDev& T, double* v, int tid) {
+  bool bad = run_rows(T.a_ops, T.a_rows, v, tid);
+  const uint32_t l0 = T.nu + T.n;
+  for (uint32_t s = tid; s < T.nu; s += 32)
+    if (dbits(v[s] - v[s]) != 0) bad = true;
+  for (uint32_t k = tid; k < T.n; k += 32) {
+    const double d = v[T.nu + k];
+    if (d == 0.0 || !(fabs(d) < CUDART_INF)) bad = true;
+  }
+  for (uint32_t s = tid; s < T.nl; s += 32)
+    if (!T.l_scaled[s] && !(fabs(v[l0 + s]) <= kWide)) bad = true;
+  return __any_sync(kFull, bad);
+}
+
+__device__ __forceinline__ void load_y(const TopoDev& T, const double* rhs, double* y, int tid) {
+  for (uint32_t r = tid; r < T.n; r += 32) y[T.pinv[r]] = -rhs[r];
+}
+
+__device__ __forceinline__ double residual_gate(const LaneOpts& o, double diag, double xi) {
+  const double scale = fabs(diag);
+  const double s = scale == 0.0 ? 1.0 : scale;
+  return fmax(o.residual_tol, 10.0 * s * (o.reltol * fabs(xi) + o.vntol));
+}
+
+// pnjlim on every diode against its image (or x_old before the first pass);
+// true when any junction was limited (Circuit.applyLimits).
+__device__ bool apply_limits(const TopoDev& T, const double* rec, const LaneMem& m, bool lim_active, int tid) {
+  bool limited = false;
+  for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
+    const BatchDev& B = T.b[bi];
+    if (B.type != kD) continue;
+    const int s = static_cast<int>(B.count);
+    for (uint32_t i = tid; i < B.count; i += 32) {
+      const uint32_t* nd = B.nodes + size_t(i) * B.nt;
+      const double* r = rec + B.rec_off + i;
+      const double vnew = m.x[nd[2]] - m.x[nd[1]];
+      const double vold = lim_active ? m.lim[B.lim_off + i] : m.xo[nd[2]] - m.xo[nd[1]];
+      bool l = false;
+      m.lim[B.lim_off + i] = pnjlim_dev(vnew, vold, r[kDVte * s], r[kDVcrit * s], l);
+      limited |= l;
+    }
+  }
+  return __any_sync(kFull, limited);
+}
+
+}  // namespace
+
+// DC Newton over independent sweep points (sweep/lanes.zig solveBatch:
+// each lane bitwise its own converger.run), one warp per lane.
+__global__ void __launch_bounds__(256) dc_newton_kernel(TopoDev T, LaneDev L, LaneOpts o) {
+  extern __shared__ double smem[];
+  const int tid = threadIdx.x & 31;
+  const uint32_t lane = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (lane >= L.n_lanes) return;
+  const uint32_t status = L.status[lane];
+  const bool resuming = L.resume && status == kNeedSolve;
+  if (!(status == kRunning || resuming)) return;
+
+  const uint32_t n = T.n;
+  LaneMem m = carve(T, smem + size_t(threadIdx.x >> 5) * T.smem_doubles);
+  const double* rec = L.rec + size_t(lane) * T.rec_size;
+  for (uint32_t i = tid; i < n; i += 32) m.x[i] = L.x[size_t(lane) * n + i];
+  for (uint32_t i = tid; i < T.nlim; i += 32) m.lim[i] = L.lim[size_t(lane) * T.nlim + i];
+  bool lim_active = L.lim_active[lane] != 0;
+  uint32_t flags = L.flags[lane];
+  uint32_t iter = L.iters[lane];
+  double limit = L.limit[lane];
+  const uint32_t max_iter = o.max_iter < 100 ? 100 : o.max_iter;
+  SimDev sim;
+  sim.t = 0.0;
+  sim.src_scale = 1.0;
+  sim.kind = 0;
+  bool have_step = false;
+  if (resuming) {
+    for (uint32_t i = tid; i < n; i += 32) {
+      m.rhs[i] = L.rhs[size_t(lane) * n + i];
+      m.diag[i] = L.diag[size_t(lane) * n + i];
+      // the host's dx, permuted as the device solve leaves it
+    }
+    for (uint32_t j = tid; j < n; j += 32) m.y[j] = L.dx[size_t(lane) * n + T.qcol[j]];
+    have_step = true;
+  }
+  __syncwarp();
+
+  for (; iter < max_iter; ++iter) {
+    if (!have_step) {
+      eval_all(T, rec, m, lim_active, sim, tid);
+      __syncwarp();
+      assemble(T, m, tid);
+      __syncwarp();
+      if (o.gmin > 0) {
+        // loadExtras: diagonal gmin and its residual form
+        for (uint32_t p = tid; p < T.nnz; p += 32) {
+          const uint32_t row = T.slot_row[p];
+          if (row != kNoDiag) {
+            const double d = m.diag[row] + o.gmin;
+            m.diag[row] = d;
+            m.tv[T.amap[p]] = d;
+          }
+        }
+        for (uint32_t i = tid; i < n; i += 32) m.rhs[i] += o.gmin * m.x[i];
+        __syncwarp();
+      }
+      if (iter == 0) {
+        // plausibleLimit: 1e3 x the start's scale, at least x_plausible
+        double g = 1.0;
+        uint64_t xm = 0, fm = 0;
+        for (uint32_t i = tid; i < n; i += 32) {
+          g = fmax(g, fabs(m.diag[i]));
+          const uint64_t bx = dbits(fabs(m.x[i])), bf = dbits(fabs(m.rhs[i]));
+          xm = bx > xm ? bx : xm;
+          fm = bf > fm ? bf : fm;
+        }
+        g = warp_fmax(g);
+        xm = warp_max_u64(xm);
+        fm = warp_max_u64(fm);
+        const double scale = fmin(fmax(from_bits(xm), from_bits(fm) * g), 1e18);
+        limit = !(1e3 * scale > kXPlausible) ? kXPlausible : 1e3 * scale;
+      }
+      const bool host_mode = (flags & 2u) != 0;
+      bool bad = true;
+      if (!host_mode) {
+        load_y(T, m.rhs, m.y, tid);
+        __syncwarp();
+        bad = refactor_forward(T, m.tv, tid);
+      }
+      if (bad) {
+        // Pause: the host factors this lane with its own direct solver.
+        const size_t base = size_t(lane) * n;
+        gather_pattern(T, m, L.a_vals + size_t(lane) * T.nnz, tid);
+        for (uint32_t i = tid; i < n; i += 32) {
+          L.x[base + i] = m.x[i];
+          L.rhs[base + i] = m.rhs[i];
+          L.diag[base + i] = m.diag[i];
+        }
+        for (uint32_t i = tid; i < T.nlim; i += 32) L.lim[size_t(lane) * T.nlim + i] = m.lim[i];
+        if (tid == 0) {
+          L.lim_active[lane] = lim_active;
+          L.flags[lane] = flags | 2u;
+          L.iters[lane] = iter;
+          L.limit[lane] = limit;
+          L.status[lane] = kNeedSolve;
+          atomicAdd(L.n_paused, 1u);
+        }
+        return;
+      }
+      run_rows(T.b_ops, T.b_rows, m.tv, tid);
+    }
+    have_step = false;
+    __syncwarp();
+
+    // finalizeStep: x_old = x, x += dx, delta score (updateAndNorm)
+    uint64_t worst = 0;
+    for (uint32_t j = tid; j < n; j += 32) {
+      const uint32_t i = T.qcol[j];
+      const double d = m.y[j];
+      const double xold = m.x[i];
+      const double xn = xold + d;
+      m.xo[i] = xold;
+      m.x[i] = xn;
+      const double tol = o.reltol * fmax(fabs(xn), fabs(xold)) + (T.cur_row[i] ? o.abstol : o.vntol);
+      const bool finite = fabs(xn) < CUDART_INF && fabs(d) < CUDART_INF;
+      const double qv = fabs(d) / tol;
+      const double score = !finite ? CUDART_INF : (qv == qv ? qv : 0.0);
+      const uint64_t b = dbits(score);
+      worst = b > worst ? b : worst;
+    }
+    worst = warp_max_u64(worst);
+    __syncwarp();
+    const bool limited = apply_limits(T, rec, m, lim_active, tid);
+    if (T.nlim) lim_active = true;
+
+    bool ok = !limited && iter != 0 && !(from_bits(worst) >= 1.0);
+    if (ok) {
+      bool p = true;
+      for (uint32_t i = tid; i < n; i += 32) p &= fabs(m.x[i]) <= limit;
+      ok = __all_sync(kFull, p);
+    }
+    if (ok) {
+      bool p = true;
+      for (uint32_t i = tid; i < n; i += 32) p &= fabs(m.rhs[i]) <= residual_gate(o, m.diag[i], m.x[i]);
+      ok = __all_sync(kFull, p);
+    }
+    if (ok) {
+      if (flags & 1u) {
+        flags &= ~1u;  // INITFIX -> INITFLOAT: one more passing iterate
+      } else {
+        for (uint32_t i = tid; i < n; i += 32) L.x[size_t(lane) * n + i] = m.xo[i];
+        if (tid == 0) {
+          L.iters[lane] = iter + 1;
+          L.status[lane] = kConverged;
+          L.lim_active[lane] = 0;
+        }
+        return;
+      }
+    }
+    __syncwarp();
+  }
+  for (uint32_t i = tid; i < n; i += 32) L.x[size_t(lane) * n + i] = m.x[i];
+  if (tid == 0) {
+    L.iters[lane] = max_iter;
+    L.status[lane] = kMaxIter;
+    L.lim_active[lane] = 0;
+  }
+}
+
+// Standalone lane refactor + solve on the frozen tape (the reference's
+// arp_lane_refactor + arp_lane_solve): A [lane][nnz] and rhs [lane][n] in
+// HBM, L/U/diagonal tape values [lane][ntv], dx [lane][n] and the peel
+// verdict out. One warp per lane; the tape values stay in shared memory
+// between the scatter, the factor and the solves.
+__global__ void __launch_bounds__(256) lu_replay_kernel(TopoDev T, uint32_t n_lanes, const double* a,
+                                                         const double* rhs, double* tv_out, double* dx,
+                                                         uint8_t* bad_out) {
+  extern __shared__ double smem[];
+  const int tid = threadIdx.x & 31;
+  const uint32_t lane = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (lane >= n_lanes) return;
+  double* tv = smem + size_t(threadIdx.x >> 5) * (T.ntv + 2 * T.n + 2);
+  double* y = tv + T.ntv;
+  double* r = y + T.n;
+  for (uint32_t j = tid; j < T.n_fill; j += 32) tv[T.fill[j]] = 0.0;
+  const double* al = a + size_t(lane) * T.nnz;
+  for (uint32_t p = tid; p < T.nnz; p += 32) tv[T.amap[p]] = al[p];
+  for (uint32_t i = tid; i < T.n; i += 32) r[i] = rhs[size_t(lane) * T.n + i];
+  __syncwarp();
+  load_y(T, r, y, tid);
+  __syncwarp();
+  const bool bad = refactor_forward(T, tv, tid);
+  run_rows(T.b_ops, T.b_rows, tv, tid);
+  for (uint32_t j = tid; j < T.n; j += 32) dx[size_t(lane) * T.n + T.qcol[j]] = y[j];
+  if (tv_out)
+    for (uint32_t s = tid; s < T.ntv; s += 32) tv_out[size_t(lane) * T.ntv + s] = tv[s];
+  if (tid == 0) bad_out[lane] = bad;
+}
+
+}  // namespace esl
+
+namespace esl {
+
+// The matrix of one lane at its start point, in pattern order: the lead
+// lane's first Jacobian, which the host factors into the pivot tape
+// (gpu_lanes.zig:361-372 factors lane 0 on the host the same way).
+__global__ void assemble_kernel(TopoDev T, LaneDev L, uint32_t lane, double* out) {
+  extern __shared__ double smem[];
+  const int tid = threadIdx.x & 31;
+  if (threadIdx.x >= 32) return;
+  LaneMem m = carve(T, smem);
+  for (uint32_t i = tid; i < T.n; i += 32) m.x[i] = L.x[size_t(lane) * T.n + i];
+  for (uint32_t i = tid; i < T.nlim; i += 32) m.lim[i] = L.lim[size_t(lane) * T.nlim + i];
+  SimDev sim;
+  sim.t = 0.0;
+  sim.src_scale = 1.0;
+  sim.kind = 0;
+  __syncwarp();
+  eval_all(T, L.rec + size_t(lane) * T.rec_size, m, L.lim_active[lane] != 0, sim, tid);
+  __syncwarp();
+  gather_pattern(T, m, out, tid);
+}
+
+size_t lane_smem_bytes(const TopoDev& T) { return size_t(T.smem_doubles) * sizeof(double); }
+
+cudaError_t launch_dc_newton(const TopoDev& T, const LaneDev& L, const LaneOpts& o,
+                             uint32_t lanes_per_block, cudaStream_t s) {
+  const size_t smem = lanes_per_block * lane_smem_bytes(T);
+  cudaError_t e = cudaFuncSetAttribute(dc_newton_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  const uint32_t grid = (L.n_lanes + lanes_per_block - 1) / lanes_per_block;
+  dc_newton_kernel<<<grid, 32 * lanes_per_block, smem, s>>>(T, L, o);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_assemble(const TopoDev& T, const LaneDev& L, uint32_t lane, double* out, cudaStream_t s) {
+  // Before the tape exists (the lead lane's first Jacobian) a lane needs no
+  // tape values: x, xo, y, rhs, diag, staging and the limited images.
+  const size_t smem = size_t(5 * T.n + T.ntv + T.n_stage + T.nlim + 2) * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(assemble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  assemble_kernel<<<1, 32, smem, s>>>(T, L, lane, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lu_replay(const TopoDev& T, uint32_t n_lanes, const double* a, const double* rhs,
+                             double* tv, double* dx, uint8_t* bad, uint32_t lanes_per_block, cudaStream_t s) {
+  const size_t per = size_t(T.ntv + 2 * T.n + 2) * sizeof(double);
+  const size_t smem = lanes_per_block * per;
+  cudaError_t e = cudaFuncSetAttribute(lu_replay_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  const uint32_t grid = (n_lanes + lanes_per_block - 1) / lanes_per_block;
+  lu_replay_kernel<<<grid, 32 * lanes_per_block, smem, s>>>(T, n_lanes, a, rhs, tv, dx, bad);
+  return cudaGetLastError();
+}
+
+}  // namespace esl

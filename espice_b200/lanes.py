@@ -1,0 +1,247 @@
+"""Python binding of libespice_lanes.so (include/espice_lanes.h).
+
+The host-side mirror of the reference's lane entry points: ``DcLanes`` plays
+the role of ``sweep/lanes.solveBatch`` (src/analysis/sweep/lanes.zig:186-233)
+on the B200: every lane is one independent DC sweep point, solved by the
+fused CUDA Newton kernel, each lane bitwise its own scalar ``converger.run``.
+The library must be built (``espice_b200.build``); nothing here falls back to
+a CPU solve: a missing library or device raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .circuit import Frozen, Slot
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libespice_lanes.so")
+
+ESL_OK, ESL_INVALID_ARGUMENT, ESL_OUT_OF_MEMORY = 0, 1, 3
+ESL_NOT_ELIGIBLE, ESL_NO_DEVICE, ESL_DEVICE_FAULT, ESL_TIMEOUT = 4, 5, 6, 7
+LANE_CONVERGED, LANE_MAX_ITER, LANE_SINGULAR = 1, 2, 3
+
+# Every entry point include/espice_lanes.h declares.
+EXPORTS = ["esl_create", "esl_destroy", "esl_last_error", "esl_dims", "esl_set_lanes",
+           "esl_dc_solve", "esl_dc_solve_device", "esl_tape", "esl_lu_replay_device",
+           "esl_tape_size", "esl_pattern", "esl_compile_tape"]
+
+u32p = ctypes.POINTER(ctypes.c_uint32)
+f64p = ctypes.POINTER(ctypes.c_double)
+u8p = ctypes.POINTER(ctypes.c_uint8)
+
+
+class LaneError(RuntimeError):
+    def __init__(self, code, what):
+        super().__init__(f"espice_lanes error {code}: {what}")
+        self.code = code
+
+
+class NewtonOpts(ctypes.Structure):
+    _fields_ = [("reltol", ctypes.c_double), ("abstol", ctypes.c_double),
+                ("vntol", ctypes.c_double), ("residual_tol", ctypes.c_double),
+                ("gmin", ctypes.c_double), ("max_iter", ctypes.c_uint32),
+                ("init_fix", ctypes.c_uint32)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("lanes_per_block", ctypes.c_uint32)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("lanes", ctypes.c_uint32), ("converged", ctypes.c_uint32),
+                ("peeled", ctypes.c_uint32), ("host_solves", ctypes.c_uint32),
+                ("launches", ctypes.c_uint32), ("kernel_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TapeInfo(ctypes.Structure):
+    _fields_ = [("nu", ctypes.c_uint32), ("nl", ctypes.c_uint32), ("ntv", ctypes.c_uint32),
+                ("n_fill", ctypes.c_uint32), ("a_rows", ctypes.c_uint32),
+                ("a_levels", ctypes.c_uint32), ("a_nops", ctypes.c_uint32),
+                ("b_rows", ctypes.c_uint32), ("b_levels", ctypes.c_uint32),
+                ("b_nops", ctypes.c_uint32), ("flops", ctypes.c_uint64),
+                ("has_void", ctypes.c_uint32)]
+
+
+_lib = None
+
+
+def lib():
+    """Loads the in-tree library (building it first if the sources are newer)."""
+    global _lib
+    if _lib is None:
+        from . import build
+        if build.stale():
+            build.build()
+        if not os.path.exists(LIB_PATH):
+            raise LaneError(ESL_NO_DEVICE, "libespice_lanes.so is not built")
+        L = ctypes.CDLL(LIB_PATH)
+        L.esl_last_error.restype = ctypes.c_char_p
+        for name in EXPORTS:
+            if name != "esl_last_error":
+                getattr(L, name).restype = ctypes.c_int32
+        _lib = L
+    return _lib
+
+
+RECORD_FIELDS = {0: 1, 1: 1, 2: 10, 3: 1, 4: 15}
+
+
+def record_size(frozen: Frozen) -> int:
+    """Doubles of one lane's device records (csrc/host/records.cpp layout)."""
+    return sum(RECORD_FIELDS[t] * nd.shape[0] for t, nd, _ in frozen.batches)
+
+
+def newton_opts(reltol=1e-3, abstol=1e-12, vntol=1e-6, residual_tol=1e-9, gmin=0.0,
+                max_iter=50, init_fix=False):
+    return NewtonOpts(reltol, abstol, vntol, residual_tol, gmin, max_iter, int(init_fix))
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def pattern(frozen: Frozen):
+    """The library's frozen CSC pattern of a circuit (host only)."""
+    L = lib()
+    cp = np.zeros(frozen.n + 1, np.uint32)
+    nnz = ctypes.c_uint32(0)
+    L.esl_pattern(ctypes.byref(frozen.struct()), _p(cp, u32p), None, ctypes.c_size_t(0),
+                  ctypes.byref(nnz))
+    ri = np.zeros(nnz.value, np.uint32)
+    rc = L.esl_pattern(ctypes.byref(frozen.struct()), _p(cp, u32p), _p(ri, u32p),
+                       ctypes.c_size_t(nnz.value), ctypes.byref(nnz))
+    if rc:
+        raise LaneError(rc, "esl_pattern")
+    return cp, ri
+
+
+def compile_tape(n, col_ptr, row_idx, lead):
+    """Lead factor + compiled warp programs (host only): a dict of arrays."""
+    L = lib()
+    cp = np.ascontiguousarray(col_ptr, np.uint32)
+    ri = np.ascontiguousarray(row_idx, np.uint32)
+    lead = np.ascontiguousarray(lead, np.float64)
+    info = TapeInfo()
+    rc = L.esl_compile_tape(ctypes.c_uint32(n), _p(cp, u32p), _p(ri, u32p), _p(lead, f64p),
+                            ctypes.byref(info), *([None] * 7))
+    if rc:
+        raise LaneError(rc, "esl_compile_tape")
+    out = dict(q=np.zeros(n, np.uint32), pinv=np.zeros(n, np.uint32),
+               amap=np.zeros(int(cp[n]), np.uint32), fill=np.zeros(info.n_fill, np.uint32),
+               a_ops=np.zeros(2 * 32 * info.a_rows, np.uint32),
+               b_ops=np.zeros(2 * 32 * info.b_rows, np.uint32),
+               l_scaled=np.zeros(max(1, info.nl), np.uint8))
+    rc = L.esl_compile_tape(ctypes.c_uint32(n), _p(cp, u32p), _p(ri, u32p), _p(lead, f64p),
+                            ctypes.byref(info), _p(out["q"], u32p), _p(out["pinv"], u32p),
+                            _p(out["amap"], u32p), _p(out["fill"], u32p), _p(out["a_ops"], u32p),
+                            _p(out["b_ops"], u32p), _p(out["l_scaled"], u8p))
+    if rc:
+        raise LaneError(rc, "esl_compile_tape")
+    out["info"] = {k: getattr(info, k) for k, _ in info._fields_}
+    return out
+
+
+class DcLanes:
+    """DC sweep lanes on one B200: a frozen circuit, then lanes of swept
+    parameter values, each solved from its own start point."""
+
+    def __init__(self, frozen: Frozen, device: int = 0, lanes_per_block: int = 0):
+        self.frozen = frozen
+        self._L = lib()
+        self._ctx = ctypes.c_void_p()
+        opts = Options(device, lanes_per_block)
+        rc = self._L.esl_create(ctypes.byref(frozen.struct()), ctypes.byref(opts),
+                                ctypes.byref(self._ctx))
+        if rc:
+            self._ctx = None
+            raise LaneError(rc, "esl_create")
+        n = ctypes.c_uint32()
+        nnz = ctypes.c_uint32()
+        self._L.esl_dims(self._ctx, ctypes.byref(n), ctypes.byref(nnz))
+        self.n, self.nnz = n.value, nnz.value
+        self.n_lanes = 0
+
+    def _check(self, rc, what):
+        if rc:
+            msg = self._L.esl_last_error(self._ctx)
+            raise LaneError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if self._ctx:
+            self._L.esl_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_lanes(self, slots, values):
+        """values [lanes][len(slots)]: each lane's swept parameter values."""
+        values = np.ascontiguousarray(values, np.float64).reshape(-1, max(1, len(slots)))
+        arr = (Slot * max(1, len(slots)))(*slots)
+        self._check(self._L.esl_set_lanes(self._ctx, arr, ctypes.c_uint32(len(slots)),
+                                          _p(values, f64p), ctypes.c_uint32(values.shape[0])),
+                    "esl_set_lanes")
+        self.n_lanes = values.shape[0]
+
+    def solve(self, x0=None, opts=None):
+        """Host-buffer solve (copies in and out): x [lanes][n], iters, status, stats."""
+        opts = opts or newton_opts()
+        x = np.zeros((self.n_lanes, self.n))
+        it = np.zeros(self.n_lanes, np.uint32)
+        st = np.zeros(self.n_lanes, np.uint32)
+        stats = Stats()
+        xp = None
+        if x0 is not None:
+            x0 = np.ascontiguousarray(np.broadcast_to(x0, (self.n_lanes, self.n)), np.float64)
+            xp = _p(x0, f64p)
+        self._check(self._L.esl_dc_solve(self._ctx, ctypes.byref(opts), xp, _p(x, f64p),
+                                         _p(it, u32p), _p(st, u32p), ctypes.byref(stats)),
+                    "esl_dc_solve")
+        return x, it, st, stats.as_dict()
+
+    def solve_device(self, d_x, d_iters, d_status, cold=False, opts=None):
+        """Device-buffer solve: pointers (ints) to [lanes][n] f64 and [lanes] u32."""
+        opts = opts or newton_opts()
+        stats = Stats()
+        self._check(self._L.esl_dc_solve_device(self._ctx, ctypes.byref(opts),
+                                                ctypes.c_void_p(d_x), ctypes.c_int(int(cold)),
+                                                ctypes.c_void_p(d_iters), ctypes.c_void_p(d_status),
+                                                ctypes.byref(stats)),
+                    "esl_dc_solve_device")
+        return stats.as_dict()
+
+    def tape(self):
+        q = np.zeros(self.n, np.uint32)
+        pinv = np.zeros(self.n, np.uint32)
+        counts = np.zeros(4, np.uint32)
+        self._check(self._L.esl_tape(self._ctx, _p(q, u32p), _p(pinv, u32p), _p(counts, u32p)),
+                    "esl_tape")
+        return q, pinv, counts
+
+    def lu_replay(self, lead, d_a, d_rhs, d_dx, d_bad, n_lanes, d_tv=0):
+        """Standalone device refactor + solve; returns the kernel's ms."""
+        lead = np.ascontiguousarray(lead, np.float64)
+        ms = ctypes.c_float(0)
+        self._check(self._L.esl_lu_replay_device(self._ctx, _p(lead, f64p), ctypes.c_uint32(n_lanes),
+                                                 ctypes.c_void_p(d_a), ctypes.c_void_p(d_rhs),
+                                                 ctypes.c_void_p(d_dx), ctypes.c_void_p(d_bad),
+                                                 ctypes.c_void_p(d_tv) if d_tv else None,
+                                                 ctypes.byref(ms)),
+                    "esl_lu_replay_device")
+        return ms.value
+
+    def tape_size(self):
+        nu, nl, ntv = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(self._L.esl_tape_size(self._ctx, ctypes.byref(nu), ctypes.byref(nl),
+                                          ctypes.byref(ntv)), "esl_tape_size")
+        return nu.value, nl.value, ntv.value

@@ -1,0 +1,182 @@
+/*
+ * espice_lanes.h: C ABI of the B200 sweep-lane Newton library
+ * (libespice_lanes.so). Plain C types only; all device memory is owned by
+ * the context.
+ *
+ * The reference reaches this path through Gompute raw kernels driven by
+ * src/analysis/gpu_lanes.zig (GpuLanes.init / newton / deinit,
+ * gpu_lanes.zig:349-845) under tran.runGpuLanes (tran.zig:1654) and, on the
+ * CPU, sweep/lanes.solveBatch (sweep/lanes.zig:186-233). A Zig host would
+ * call these entry points where gpu_lanes.zig launches its kernels; the
+ * bindings a maintainer adds are in INTEGRATION.md.
+ *
+ * Threading: calls on one context must be serialized (the rule of
+ * include/espice.h:139-156 for a problem handle). Each context owns one CUDA
+ * stream on one device; contexts are independent.
+ */
+#ifndef ESPICE_LANES_H
+#define ESPICE_LANES_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (int32). The reference's outcomes they map to: */
+enum {
+    ESL_OK = 0,
+    ESL_INVALID_ARGUMENT = 1, /* espice.h ESPICE_INVALID_ARGUMENT */
+    ESL_OUT_OF_MEMORY = 3,    /* OutOfMemory */
+    ESL_NOT_ELIGIBLE = 4,     /* tran.zig:1612 gpuLaneRefusal: run on the CPU */
+    ESL_NO_DEVICE = 5,        /* no CUDA device / image: run on the CPU */
+    ESL_DEVICE_FAULT = 6,     /* a driver error mid-run: QueryCancelled (tran.zig:1824) */
+    ESL_TIMEOUT = 7           /* a bounded device wait ran out */
+};
+
+/* Device types and per-instance layouts (unknown indices; 0 is ground). */
+enum {
+    ESL_R = 0, /* nodes p n;          params r                               */
+    ESL_C = 1, /* nodes p n;          params c                               */
+    ESL_V = 2, /* nodes p n br;       params dc wave v1 v2 td tr tf pw per phase */
+    ESL_I = 3, /* nodes p n;          params dc                              */
+    ESL_D = 4, /* nodes a c ai;       params is n rs bv ibv cjo vj m fc tt area gmin xti eg tnom temp */
+    ESL_M = 5  /* nodes d g s b di si; params (MOS1, models/mos1.va)         */
+};
+
+/* Per-lane outcome (esl_lane_result.status). */
+enum {
+    ESL_LANE_CONVERGED = 1,
+    ESL_LANE_MAX_ITER = 2, /* Newton ran out of iterations (non-converged point) */
+    ESL_LANE_SINGULAR = 3  /* the lane's own factor failed (SingularMatrix) */
+};
+
+typedef struct {
+    uint32_t type;
+    uint32_t count;
+    const uint32_t *nodes;  /* count * nodes-per-type */
+    const double *params;   /* count * params-per-type */
+} esl_batch;
+
+/* A frozen circuit (src/device/Circuit.zig:77-167): n unknowns, ground is
+ * row/column 0 held by a unit pin, device batches in stamp order. */
+typedef struct {
+    uint32_t n;
+    uint32_t n_batches;
+    const esl_batch *batches;
+    const uint8_t *current_row; /* n: 1 for a branch-current unknown */
+} esl_circuit;
+
+/* One swept parameter of a lane: batch, instance, parameter index. */
+typedef struct {
+    uint32_t batch, inst, param;
+} esl_slot;
+
+/* converger.Options (converger.zig:99-122) for one solve. */
+typedef struct {
+    double reltol, abstol, vntol, residual_tol, gmin;
+    uint32_t max_iter;   /* raised to at least 100, as optionsFromTolerances does */
+    uint32_t init_fix;   /* MODEINITFIX: publish the second passing iterate */
+} esl_newton_opts;
+
+typedef struct {
+    int device;               /* CUDA ordinal */
+    uint32_t lanes_per_block; /* warps per CTA; 0 picks the tuned value */
+} esl_options;
+
+typedef struct esl_ctx esl_ctx;
+
+typedef struct {
+    uint32_t lanes;        /* lanes solved */
+    uint32_t converged;    /* lanes that converged */
+    uint32_t peeled;       /* lanes that paused for a host factor at least once */
+    uint32_t host_solves;  /* host factor+solve calls (lane_solver.zig peels) */
+    uint32_t launches;     /* kernel launches in the call */
+    double kernel_ms;      /* device time of the Newton launches */
+} esl_stats;
+
+/* Builds the pattern, column order and stamp tables of `circuit` on
+ * `opts->device` (NULL: device 0). Replaces GpuLanes.init's pattern and
+ * table work (gpu_lanes.zig:349-622). */
+int32_t esl_create(const esl_circuit *circuit, const esl_options *opts, esl_ctx **out);
+
+/* Frees every device buffer of the context (GpuLanes.deinit,
+ * gpu_lanes.zig:626-662). NULL is a no-op. */
+int32_t esl_destroy(esl_ctx *ctx);
+
+/* The last error's text on this context ("" when none). */
+const char *esl_last_error(const esl_ctx *ctx);
+
+/* Matrix dimension n and pattern size nnz of the context's circuit. */
+int32_t esl_dims(const esl_ctx *ctx, uint32_t *n, uint32_t *nnz);
+
+/* Installs n_lanes lanes: lane l sets slots[s] to values[l * n_slots + s]
+ * on the nominal circuit (the per-lane params of sweep/lanes.zig install,
+ * :96-100), derives each lane's device records and uploads them. */
+int32_t esl_set_lanes(esl_ctx *ctx, const esl_slot *slots, uint32_t n_slots,
+                      const double *values, uint32_t n_lanes);
+
+/* DC Newton for every lane, each bitwise its own converger.run on its own
+ * direct solver (sweep/lanes.zig solveBatch, :186-233). Host buffers:
+ * x0 [n_lanes][n] start points (NULL: cold, op.zig coldStart), x_out
+ * [n_lanes][n], iters and status [n_lanes] (ESL_LANE_*). The call copies
+ * the start points in and the results out. */
+int32_t esl_dc_solve(esl_ctx *ctx, const esl_newton_opts *opts, const double *x0,
+                     double *x_out, uint32_t *iters, uint32_t *status, esl_stats *stats);
+
+/* esl_dc_solve on device buffers: d_x [n_lanes][n] start points in place of
+ * x0 (overwritten with the solutions), d_iters/d_status device arrays.
+ * cold != 0 seeds the junctions and starts from zero. Returns once the
+ * lanes are done (host peels included). */
+int32_t esl_dc_solve_device(esl_ctx *ctx, const esl_newton_opts *opts, double *d_x, int cold,
+                            uint32_t *d_iters, uint32_t *d_status, esl_stats *stats);
+
+/* The lead lane's pivot tape after the last solve (buildTab,
+ * lane_kernels.zig:321-345): q[n], pinv[n]; counts[0] = |L|, counts[1] = |U|,
+ * counts[2] = refactor levels, counts[3] = solve levels. */
+int32_t esl_tape(const esl_ctx *ctx, uint32_t *q, uint32_t *pinv, uint32_t *counts);
+
+/* Standalone lane refactor + solve on the lead tape (arp_lane_refactor +
+ * arp_lane_solve, lane_device.zig:26-38): device buffers a [n_lanes][nnz]
+ * (pattern order), rhs [n_lanes][n] -> dx [n_lanes][n] = -A^-1 rhs and
+ * bad [n_lanes] (1: pivot failure, growth, non-finite entry or a multiplier
+ * past 1/pivot_tol: the lane must peel). tv [n_lanes][ntv] receives the
+ * tape values (U, diagonal, L) when not NULL; ntv via esl_tape_size.
+ * The tape is built from `lead` (host, nnz values) on the first call. */
+int32_t esl_lu_replay_device(esl_ctx *ctx, const double *lead, uint32_t n_lanes,
+                             const double *d_a, const double *d_rhs, double *d_dx,
+                             uint8_t *d_bad, double *d_tv, float *ms);
+
+int32_t esl_tape_size(const esl_ctx *ctx, uint32_t *nu, uint32_t *nl, uint32_t *ntv);
+
+/* Host-only symbolic stage (no device needed). */
+
+/* The frozen CSC pattern of `circuit` (Circuit.freeze, Circuit.zig:77-167):
+ * col_ptr [n + 1], row_idx [cap]; *nnz set even when cap is short. */
+int32_t esl_pattern(const esl_circuit *circuit, uint32_t *col_ptr, uint32_t *row_idx,
+                    size_t cap, uint32_t *nnz);
+
+typedef struct {
+    uint32_t nu, nl, ntv;        /* |U|, |L|, tape values (nu + n + nl + 1) */
+    uint32_t n_fill;             /* tape values no pattern slot writes */
+    uint32_t a_rows, a_levels, a_nops; /* program A (refactor + forward solve) */
+    uint32_t b_rows, b_levels, b_nops; /* program B (back solve) */
+    uint64_t flops;              /* refactor multiply-subtracts */
+    uint32_t has_void;           /* a fabricated pivot (not run on the device) */
+} esl_tape_info;
+
+/* Orders the pattern (order.zig), factors `lead` with threshold pivoting
+ * (sparse_lu.zig factor, pivot_tol 1e-3) and compiles the tape into the
+ * warp programs the kernels run (buildTab's role, lane_kernels.zig:321-345):
+ * rows of 32 ops, two u32 words per op, over v = [tape values | y]. Any
+ * output array may be NULL; sizes come from info. */
+int32_t esl_compile_tape(uint32_t n, const uint32_t *col_ptr, const uint32_t *row_idx,
+                         const double *lead, esl_tape_info *info, uint32_t *q, uint32_t *pinv,
+                         uint32_t *amap, uint32_t *fill, uint32_t *a_ops, uint32_t *b_ops,
+                         uint8_t *l_scaled);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
