@@ -39,10 +39,10 @@ constexpr uint32_t kNoDiag = 0xffffffffu;
 // word1 = a | (b << 16).
 enum OpKind : uint32_t {
   kOpFlop = 0,       // v[dst] -= v[a] * v[b]
-  kOpDivGrowth = 1,  // v[dst] = v[dst] / v[a]; peel unless |v[a]| >= growth * |v[dst]|
-  kOpDivScaled = 2,  // v[dst] = v[dst] / v[a]; peel on a non-finite quotient
+  kOpDivGrowth = 1,  // v[dst] = v[b] / v[a]; peel unless |v[a]| >= growth * |v[b]|
+  kOpDivScaled = 2,  // v[dst] = v[b] / v[a]; peel on a non-finite quotient
   kOpSubNz = 3,      // v[dst] -= v[a] * v[b] when v[b] != 0 (the solves' zero skip)
-  kOpDivY = 4,       // v[dst] = v[dst] / v[a]
+  kOpDivY = 4,       // v[dst] = v[b] / v[a]   (b = dst for a real op)
   kOpNop = 7,
 };
 

@@ -136,6 +136,7 @@ struct esl_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::string err;
   uint32_t lanes_per_block = 4;
+  uint32_t lanes_eff = 4;  // lanes per CTA that fit beside the staged programs
 
   Csc pat;
   std::vector<uint8_t> cur;
@@ -153,7 +154,7 @@ struct esl_ctx {
   Programs prog;
 
   DevBuf d_nodes[kMaxBatches], d_rhs_ptr, d_rhs_src, d_a_ptr, d_a_src, d_slot_row, d_cur;
-  DevBuf d_amap, d_fill, d_a_ops, d_b_ops, d_l_scaled, d_pinv, d_q;
+  DevBuf d_amap, d_fill, d_prog, d_l_scaled, d_pinv, d_q;
   DevBuf d_rec, d_lim, d_lim_active, d_status, d_iters, d_flags, d_limit, d_a_vals, d_rhs, d_dx,
       d_diag, d_paused, d_x;
   TopoDev topo{};
@@ -301,37 +302,146 @@ int32_t upload_topology(esl_ctx* ctx) {
   return ESL_OK;
 }
 
+// One lane's shared block, in doubles (newton.cu carves the same layout):
+// x | xo | rhs | diag | v = [tape values | y | 0.0 | 1.0 | sink] |
+// staging | limited images.
+struct LaneLayout {
+  uint32_t x, xo, rhs, diag, tv, y, zero, one, sink, st, lim, total;
+};
+
+LaneLayout lane_layout(uint32_t n, uint32_t ntv, uint32_t n_stage, uint32_t nlim) {
+  LaneLayout L;
+  L.x = 0;
+  L.xo = n;
+  L.rhs = 2 * n;
+  L.diag = 3 * n;
+  L.tv = 4 * n;
+  L.y = L.tv + ntv;
+  L.zero = L.y + n;
+  L.one = L.zero + 1;
+  L.sink = L.zero + 2;
+  L.st = L.zero + 3;
+  L.lim = L.st + n_stage;
+  L.total = (L.lim + nlim + 1) & ~1u;
+  return L;
+}
+
+struct GatherProgram {
+  std::vector<uint32_t> depth, off, src, dst;
+};
+
+// Assembly cells: every residual row, every pattern slot and every fill-in
+// tape value, each summing its staging cells in stamp order (+0.0 pads a
+// short list: a sum that starts at +0.0 is never -0.0, so adding +0.0 is
+// exact). Cells sorted by list length so a group of 32 pads little.
+GatherProgram build_gather_program(const esl_ctx* ctx, const Programs& P) {
+  const uint32_t n = ctx->pat.n, nnz = ctx->pat.nnz();
+  const LaneLayout L = lane_layout(n, P.ntv, ctx->n_stage, ctx->nlim);
+  struct Cell {
+    std::vector<uint32_t> src;
+    uint32_t d0, d1, d2;
+  };
+  std::vector<Cell> cells;
+  auto remap = [&](uint32_t s) { return s == kSrcOne ? L.one : s == kSrcX0 ? L.x : L.st + s; };
+  for (uint32_t i = 0; i < n; ++i) {
+    Cell c;
+    for (uint32_t e = ctx->rhs_ptr[i]; e < ctx->rhs_ptr[i + 1]; ++e) c.src.push_back(remap(ctx->rhs_src[e]));
+    c.d0 = L.rhs + i;
+    c.d1 = L.sink;
+    c.d2 = L.y + ctx->lead.pinv[i];
+    cells.push_back(std::move(c));
+  }
+  for (uint32_t p = 0; p < nnz; ++p) {
+    Cell c;
+    for (uint32_t e = ctx->a_ptr[p]; e < ctx->a_ptr[p + 1]; ++e) c.src.push_back(remap(ctx->a_src[e]));
+    c.d0 = L.tv + P.amap[p];
+    c.d1 = ctx->slot_row[p] != kNoDiag ? L.diag + ctx->slot_row[p] : L.sink;
+    c.d2 = L.sink;
+    cells.push_back(std::move(c));
+  }
+  for (uint32_t f : P.fill) cells.push_back(Cell{{}, L.tv + f, L.sink, L.sink});
+  std::stable_sort(cells.begin(), cells.end(), [](const Cell& a, const Cell& b) { return a.src.size() > b.src.size(); });
+  GatherProgram G;
+  for (size_t g0 = 0; g0 < cells.size(); g0 += 32) {
+    uint32_t depth = 0;
+    for (size_t t = 0; t < 32 && g0 + t < cells.size(); ++t) depth = std::max<uint32_t>(depth, cells[g0 + t].src.size());
+    G.depth.push_back(depth);
+    G.off.push_back(uint32_t(G.src.size()));
+    for (uint32_t k = 0; k < depth; ++k)
+      for (size_t t = 0; t < 32; ++t) {
+        const bool live = g0 + t < cells.size() && k < cells[g0 + t].src.size();
+        G.src.push_back(live ? cells[g0 + t].src[k] : L.zero);
+      }
+    for (size_t t = 0; t < 32; ++t) {
+      if (g0 + t < cells.size()) {
+        G.dst.push_back(cells[g0 + t].d0);
+        G.dst.push_back(cells[g0 + t].d1);
+        G.dst.push_back(cells[g0 + t].d2);
+      } else {
+        G.dst.push_back(L.sink);
+        G.dst.push_back(L.sink);
+        G.dst.push_back(L.sink);
+      }
+    }
+  }
+  return G;
+}
+
 // The lead lane's pivot tape, compiled and uploaded.
 int32_t upload_tape(esl_ctx* ctx) {
   cudaStream_t s = ctx->stream;
   TopoDev& T = ctx->topo;
   Programs& P = ctx->prog;
   if (P.has_void) return ctx->fail(ESL_NOT_ELIGIBLE, "the lead factor fabricated a pivot for a void unknown");
-  if (P.ntv + P.n >= 65536) return ctx->fail(ESL_NOT_ELIGIBLE, "tape too large for one lane's shared memory");
+  if (P.nv >= 65536) return ctx->fail(ESL_NOT_ELIGIBLE, "tape too large for one lane's shared memory");
   ESL_CUDA(upload(ctx->d_amap, P.amap, s));
   ESL_CUDA(upload(ctx->d_fill, P.fill, s));
-  ESL_CUDA(upload(ctx->d_a_ops, P.a_ops, s));
-  ESL_CUDA(upload(ctx->d_b_ops, P.b_ops, s));
   ESL_CUDA(upload(ctx->d_l_scaled, P.l_scaled, s));
   ESL_CUDA(upload(ctx->d_pinv, ctx->lead.pinv, s));
   ESL_CUDA(upload(ctx->d_q, ctx->lead.q, s));
   T.nu = P.nu;
   T.nl = P.nl;
   T.ntv = P.ntv;
+  T.nv = P.nv;
   T.amap = ctx->d_amap.as<uint32_t>();
   T.fill = ctx->d_fill.as<uint32_t>();
   T.n_fill = uint32_t(P.fill.size());
-  T.a_ops = ctx->d_a_ops.as<uint2>();
-  T.b_ops = ctx->d_b_ops.as<uint2>();
-  T.a_rows = P.a_rows;
-  T.b_rows = P.b_rows;
+  {
+    // One blob: A ops, B ops, gather depth/off/src/dst, each section
+    // 16-byte aligned.
+    GatherProgram G = build_gather_program(ctx, P);
+    std::vector<unsigned char> blob;
+    auto put = [&blob](const void* p, size_t bytes) {
+      const uint32_t at = uint32_t(blob.size());
+      blob.insert(blob.end(), static_cast<const unsigned char*>(p), static_cast<const unsigned char*>(p) + bytes);
+      blob.resize((blob.size() + 15) & ~size_t(15), 0);
+      return at;
+    };
+    T.o_a_ops = put(P.a_ops.data(), P.a_ops.size() * sizeof(Op));
+    T.o_b_ops = put(P.b_ops.data(), P.b_ops.size() * sizeof(Op));
+    T.o_g_depth = put(G.depth.data(), G.depth.size() * 4);
+    T.o_g_off = put(G.off.data(), G.off.size() * 4);
+    T.o_g_src = put(G.src.data(), G.src.size() * 4);
+    T.o_g_dst = put(G.dst.data(), G.dst.size() * 4);
+    ESL_CUDA(upload(ctx->d_prog, blob, s));
+    T.prog = ctx->d_prog.as<unsigned char>();
+    T.prog_bytes = uint32_t(blob.size());
+    T.a_rows = P.a_rows;
+    T.b_rows = P.b_rows;
+    T.n_groups = uint32_t(G.depth.size());
+  }
   T.l_scaled = ctx->d_l_scaled.as<uint8_t>();
   T.pinv = ctx->d_pinv.as<uint32_t>();
   T.qcol = ctx->d_q.as<uint32_t>();
-  uint32_t d = 5 * T.n + T.ntv + T.n_stage + T.nlim;  // x xo rhs diag | tv y | staging | lim
-  T.smem_doubles = (d + 1) & ~1u;
+  T.smem_doubles = lane_layout(T.n, T.ntv, T.n_stage, T.nlim).total;
   if (size_t(T.smem_doubles) * 8 > 227 * 1024)
     return ctx->fail(ESL_NOT_ELIGIBLE, "one lane's working set exceeds a CTA's shared memory");
+  // Every CTA stages the programs; as many lanes per CTA as fit beside them.
+  const size_t lane_bytes = size_t(T.smem_doubles) * 8;
+  const size_t room = size_t(227) * 1024;
+  if (T.prog_bytes + lane_bytes > room)
+    return ctx->fail(ESL_NOT_ELIGIBLE, "programs and one lane exceed a CTA's shared memory");
+  ctx->lanes_eff = std::max<uint32_t>(1, std::min<uint32_t>(ctx->lanes_per_block, uint32_t((room - T.prog_bytes) / lane_bytes)));
   ctx->have_tape = true;
   return ESL_OK;
 }
@@ -568,7 +678,7 @@ int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d
   }
   LaneOpts o{opts->reltol, opts->abstol, opts->vntol, opts->residual_tol, opts->gmin, opts->max_iter, opts->init_fix};
   ESL_CUDA(cudaEventRecord(ctx->ev0, s));
-  ESL_CUDA(launch_dc_newton(ctx->topo, L, o, ctx->lanes_per_block, s));
+  ESL_CUDA(launch_dc_newton(ctx->topo, L, o, ctx->lanes_eff, s));
   uint32_t launches = 1;
   for (;;) {
     bool any = false;
@@ -576,7 +686,7 @@ int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d
     if (!any) break;
     LaneDev R = L;
     R.resume = 1;
-    ESL_CUDA(launch_dc_newton(ctx->topo, R, o, ctx->lanes_per_block, s));
+    ESL_CUDA(launch_dc_newton(ctx->topo, R, o, ctx->lanes_eff, s));
     ++launches;
   }
   ESL_CUDA(cudaEventRecord(ctx->ev1, s));
@@ -695,7 +805,7 @@ int32_t esl_lu_replay_device(esl_ctx* ctx, const double* lead, uint32_t n_lanes,
     if (int32_t rc = build_tape_from(ctx, lead)) return rc;
   }
   ESL_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-  ESL_CUDA(launch_lu_replay(ctx->topo, n_lanes, d_a, d_rhs, d_tv, d_dx, d_bad, ctx->lanes_per_block, ctx->stream));
+  ESL_CUDA(launch_lu_replay(ctx->topo, n_lanes, d_a, d_rhs, d_tv, d_dx, d_bad, ctx->lanes_eff, ctx->stream));
   ESL_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
   ESL_CUDA(cudaEventSynchronize(ctx->ev1));
   if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);

@@ -23,10 +23,13 @@ Op encode(uint32_t kind, uint32_t dst, uint32_t a, uint32_t b) {
 // Levels: an op runs after the last write of each value it reads, after
 // the last write of its destination, and after every earlier read of its
 // destination by another op (no value is overwritten before it is read).
-// Each level is then packed into rows of kRow ops (one per thread), grouped
-// by kind within the level, padded with no-ops.
-void pack(const std::vector<SeqOp>& seq, uint32_t space, std::vector<Op>& rows, uint32_t& n_rows,
-          uint32_t& n_levels) {
+// Each level is then packed into rows of kRow ops (one per thread) of one
+// kind.
+// Padding ops keep the row's kind and write the sink slot (space - 1) from
+// the constants 1.0 (space - 2) and 0.0 (space - 3): a multiply-subtract of
+// 1.0 * 0.0, or 1.0 / 1.0 (divisions read their dividend at b).
+void pack(const std::vector<SeqOp>& seq, uint32_t space, std::vector<Op>& rows,
+          std::vector<uint32_t>& kinds, uint32_t& n_rows, uint32_t& n_levels) {
   std::vector<int32_t> lw(space, -1), lr(space, -1), level(seq.size());
   int32_t top = -1;
   for (size_t i = 0; i < seq.size(); ++i) {
@@ -44,19 +47,26 @@ void pack(const std::vector<SeqOp>& seq, uint32_t space, std::vector<Op>& rows, 
   std::vector<std::vector<uint32_t>> by(n_levels);
   for (size_t i = 0; i < seq.size(); ++i) by[level[i]].push_back(uint32_t(i));
   rows.clear();
+  kinds.clear();
   n_rows = 0;
   for (auto& ids : by) {
     std::stable_sort(ids.begin(), ids.end(), [&](uint32_t x, uint32_t y) { return seq[x].kind < seq[y].kind; });
-    for (size_t at = 0; at < ids.size(); at += kRow) {
+    for (size_t at = 0; at < ids.size();) {
+      const uint32_t kind = seq[ids[at]].kind;
+      size_t end = at;
+      while (end < ids.size() && end - at < kRow && seq[ids[end]].kind == kind) ++end;
       for (uint32_t t = 0; t < kRow; ++t) {
-        if (at + t < ids.size()) {
+        if (at + t < end) {
           const SeqOp& s = seq[ids[at + t]];
           rows.push_back(encode(s.kind, s.dst, s.a, s.b));
         } else {
-          rows.push_back(encode(kOpNop, 0, kNone, kNone));
+          const bool div = kind == kOpDivGrowth || kind == kOpDivScaled || kind == kOpDivY;
+          rows.push_back(encode(kind, space - 1, space - 2, div ? space - 2 : space - 3));
         }
       }
+      kinds.push_back(kind);
       ++n_rows;
+      at = end;
     }
   }
 }
@@ -99,11 +109,12 @@ Programs compile_tape(const SparseLu& lu) {
       P.amap[e] = (void_k && r > k) ? discard : pos[r];
     }
     const uint32_t div = lu.scaled[k] ? kOpDivScaled : kOpDivGrowth;
-    for (uint32_t q = lu.lp[k]; q < lu.lp[k + 1]; ++q) a.push_back({div, lx0 + q, P.nu + k, kNone});
+    for (uint32_t q = lu.lp[k]; q < lu.lp[k + 1]; ++q) a.push_back({div, lx0 + q, P.nu + k, lx0 + q});
     // Forward substitution of column k (sparse_lu.zig solve): y[li] -= l * y[k].
     for (uint32_t q = lu.lp[k]; q < lu.lp[k + 1]; ++q) a.push_back({kOpSubNz, y0 + lu.li[q], lx0 + q, y0 + k});
   }
-  pack(a, P.ntv + n, P.a_ops, P.a_rows, P.a_levels);
+  P.nv = P.ntv + n + 3;
+  pack(a, P.nv, P.a_ops, P.a_kind, P.a_rows, P.a_levels);
   P.a_nops = uint32_t(a.size());
 
   std::vector<uint8_t> written(P.ntv, 0);
@@ -118,10 +129,10 @@ Programs compile_tape(const SparseLu& lu) {
   // Back substitution through U: the diagonal division first in each column.
   std::vector<SeqOp> b;
   for (uint32_t k = n; k-- > 0;) {
-    b.push_back({kOpDivY, y0 + k, P.nu + k, kNone});
+    b.push_back({kOpDivY, y0 + k, P.nu + k, y0 + k});
     for (uint32_t p = lu.up[k]; p < lu.up[k + 1]; ++p) b.push_back({kOpSubNz, y0 + lu.ui[p], p, y0 + k});
   }
-  pack(b, P.ntv + n, P.b_ops, P.b_rows, P.b_levels);
+  pack(b, P.nv, P.b_ops, P.b_kind, P.b_rows, P.b_levels);
   P.b_nops = uint32_t(b.size());
   return P;
 }

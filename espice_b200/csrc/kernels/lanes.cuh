@@ -23,6 +23,7 @@ struct BatchDev {
 
 struct TopoDev {
   uint32_t n, nnz, nu, nl, ntv;   // unknowns, pattern, |U|, |L|, tape values (nu + n + nl + 1)
+  uint32_t nv;                    // program value space: ntv + n (y) + 3 (0.0, 1.0, sink)
   uint32_t n_stage, nlim, rec_size;
   uint32_t n_batches;
   BatchDev b[kMaxBatches];
@@ -38,11 +39,19 @@ struct TopoDev {
   // Tape values no pattern slot writes (fill-in): zeroed per iteration.
   const uint32_t* fill;
   uint32_t n_fill;
-  // Warp programs (rows of 32 ops): A = refactor + forward solve, B = back
-  // solve, over v = [tape values | y].
-  const uint2* a_ops;
-  const uint2* b_ops;
-  uint32_t a_rows, b_rows;
+  // The warp programs live in one 16-byte-aligned blob, staged into each
+  // CTA's shared memory: A = refactor + forward solve and B = back solve,
+  // rows of 32 ops of one kind over v = [tape values | y | 0.0 | 1.0 |
+  // sink] (the row's kind in every op word); and the assembly gather
+  // program: group g of 32 cells sums src[off[g] + k * 32 + t] for
+  // k < depth[g] (cell t, lane-block indices), then writes the sum to
+  // dst[3 * (32 g + t)] and [+1] and its negation to [+2] (residual rows,
+  // pattern slots into tape values, the diagonal copy and y = P(-rhs);
+  // fill-in tape values are empty cells). Offsets in bytes.
+  const unsigned char* prog;
+  uint32_t prog_bytes;
+  uint32_t o_a_ops, o_b_ops, o_g_depth, o_g_off, o_g_src, o_g_dst;
+  uint32_t a_rows, b_rows, n_groups;
   // L tape values whose column passed on the row-scaled test (no wide test).
   const uint8_t* l_scaled;
   // y[pinv[r]] = -rhs[r] before program A; dx[q[j]] = y[j] after program B.

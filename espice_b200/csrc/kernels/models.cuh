@@ -9,10 +9,21 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <math_constants.h>
 
 #include "../common.h"
 
 namespace esl {
+
+// a / b correctly rounded (IEEE round-to-nearest), bitwise __ddiv_rn. A zero
+// dividend over a finite nonzero divisor (frequent: zero fill-in, zero
+// steps, a node at zero volts) returns its signed zero directly, keeping the
+// division sequence on its fast path for the operands it is built for.
+__device__ __forceinline__ double div_rn(double a, double b) {
+  if (a == 0.0 && b != 0.0 && fabs(b) < CUDART_INF)
+    return __longlong_as_double((__double_as_longlong(a) ^ __double_as_longlong(b)) & (1ll << 63));
+  return __ddiv_rn(a, b);
+}
 
 struct SimDev {
   double t;          // time (transient)
@@ -51,25 +62,25 @@ __device__ __forceinline__ void diode_iv(const double* r, int s, double vd, doub
   const double vte = r[kDVte * s], is = r[kDIs * s];
   double id, gd;
   if (vd >= -3.0 * vte) {
-    const double u = vd / vte;
+    const double u = div_rn(vd, vte);
     const double ulim = fmin(u, 80.0);
     const double e = exp(ulim);
     id = is * ((e * (1.0 + (u - ulim))) - 1.0);
-    gd = is * e / vte;
+    gd = div_rn(is * e, vte);
   } else {
-    const double a = 3.0 * vte / (vd * 2.718281828459045);
+    const double a = div_rn(3.0 * vte, vd * 2.718281828459045);
     const double a3 = pow(a, 3.0);
     id = -is * (1.0 + a3);
-    gd = 3.0 * is * a3 / vd;
+    gd = div_rn(3.0 * is * a3, vd);
   }
   const double xbv = r[kDXbv * s];
   if (r[kDBv * s] > 0.0 && vd < -3.0 * vte && vd < -xbv) {
     const double vtb = r[kDVtebrk * s];
-    const double wb = -(xbv + vd) / vtb;
+    const double wb = div_rn(-(xbv + vd), vtb);
     const double wlim = fmin(wb, 80.0);
     const double e = exp(wlim);
     id = -is * e * (1.0 + (wb - wlim));
-    gd = is * e / vtb;
+    gd = div_rn(is * e, vtb);
   }
   const double gmin = r[kDGmin * s];
   i = id + gmin * vd;
@@ -85,8 +96,8 @@ __device__ __forceinline__ void diode_qc(const double* r, int s, double vd, doub
     const double vj = r[kDVj * s], mt = r[kDMt * s], fc = r[kDFc * s];
     const double vfc = fc * vj;
     if (vd < vfc) {
-      const double b = 1.0 - vd / vj;
-      qj = cjo * vj * (1.0 - pow(b, 1.0 - mt)) / (1.0 - mt);
+      const double b = 1.0 - div_rn(vd, vj);
+      qj = div_rn(cjo * vj * (1.0 - pow(b, 1.0 - mt)), 1.0 - mt);
       cj = cjo * pow(b, -mt);
     } else {
       const double f1 = vj * (1.0 - pow(1.0 - fc, 1.0 - mt)) / (1.0 - mt);
@@ -109,11 +120,11 @@ __device__ __forceinline__ void diode_qc(const double* r, int s, double vd, doub
 __device__ __forceinline__ double pnjlim_dev(double vnew, double vold, double vt, double vcrit, bool& lim) {
   if (vnew > vcrit && fabs(vnew - vold) > vt + vt) {
     if (vold > 0) {
-      const double arg = (vnew - vold) / vt;
+      const double arg = div_rn(vnew - vold, vt);
       if (arg > 0) vnew = vold + vt * (2 + log(arg - 2));
       else vnew = vold - vt * (2 + log(2 - arg));
     } else {
-      vnew = vt * log(vnew / vt);
+      vnew = vt * log(div_rn(vnew, vt));
     }
     lim = true;
   } else if (vnew < 0) {
@@ -147,7 +158,7 @@ __device__ __forceinline__ void diode_stamp(const double* r, int s, double xa, d
   const double rs_t = r[kDRs * s];
   const bool has_rs = r[kDHasRs * s] != 0.0;
   const double grs = 1.0 / rs_t;
-  const double irs = (xa - xai) / rs_t;
+  const double irs = div_rn(xa - xai, rs_t);
   st[0] = irs;
   st[1] = -ires;
   st[2] = has_rs ? ires - irs : ires;

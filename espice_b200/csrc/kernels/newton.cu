@@ -1,9 +1,10 @@
 // Fused sweep-lane Newton kernel for sm_100a: one warp per lane, the lane's
 // whole working set in shared memory, every phase of a Newton iteration in
 // one launch (eval + stamp -> assemble -> refactor on the lead lane's frozen
-// pivot tape -> forward/back solve -> update -> limiting -> gates), looping
-// on the device until the lane converges, runs out of iterations, or needs
-// the host (a pivot the frozen tape cannot stand in for).
+// pivot tape with the forward solve merged in -> back solve -> update ->
+// limiting -> gates), looping on the device until the lane converges, runs
+// out of iterations, or needs the host (a pivot the frozen tape cannot stand
+// in for).
 //
 // Reference path this replaces (src/analysis/gpu_lanes.zig:758-845 and the
 // 12 kernels of src/solver/lane_device.zig, bodies in
@@ -11,11 +12,18 @@
 // more launches of one thread per lane over lane-major HBM planes plus two
 // host syncs. Here one launch runs every tick of every lane.
 //
-// Bitwise contract: the refactor and solve ops use __dmul_rn / __dsub_rn
-// (no FMA contraction) in the reference's operation order per value, so a
-// lane's L, U and dx are bitwise the CPU replay (sparse_lu.zig refactor +
-// solve) on the same matrix. The whole file builds with --fmad=false so the
-// stamp and gates round as the reference's strict-float code does.
+// Shared memory of a CTA: the topology's program blob (warp programs and
+// the assembly gather program, staged once per CTA), then one block per
+// lane (warp): x | xo | rhs | diag | v | staging | limited images, where
+// v = [tape values | y | 0.0 | 1.0 | sink] is the value space of the warp
+// programs. The hot loops address shared memory explicitly (32-bit shared
+// addresses, ld.shared / st.shared).
+//
+// Bitwise contract: the refactor and solve ops use __dmul_rn / __dsub_rn /
+// __ddiv_rn in the reference's operation order per value, so a lane's L, U
+// and dx are bitwise the CPU replay (sparse_lu.zig refactor + solve) on the
+// same matrix. The file builds with --fmad=false so the stamp and gates
+// round as the reference's strict-float code does.
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
@@ -28,12 +36,34 @@ namespace esl {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr double kGrowth = 1e-12;   // direct.zig refactor_growth_limit
-constexpr double kWide = 1e3;       // 1 / direct.zig pivot_tol
-constexpr double kXPlausible = 1e9; // converger.zig x_plausible
+constexpr double kGrowth = 1e-12;    // direct.zig refactor_growth_limit
+constexpr double kWide = 1e3;        // 1 / direct.zig pivot_tol
+constexpr double kXPlausible = 1e9;  // converger.zig x_plausible
 
 __device__ __forceinline__ uint64_t dbits(double x) { return static_cast<uint64_t>(__double_as_longlong(x)); }
 __device__ __forceinline__ double from_bits(uint64_t u) { return __longlong_as_double(static_cast<long long>(u)); }
+
+__device__ __forceinline__ double lds(uint32_t a) {
+  double r;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(r) : "r"(a));
+  return r;
+}
+__device__ __forceinline__ void sts(uint32_t a, double x) {
+  asm volatile("st.shared.f64 [%0], %1;" ::"r"(a), "d"(x) : "memory");
+}
+__device__ __forceinline__ uint32_t lds_u32(uint32_t a) {
+  uint32_t r;
+  asm volatile("ld.shared.u32 %0, [%1];" : "=r"(r) : "r"(a));
+  return r;
+}
+__device__ __forceinline__ uint2 lds_u2(uint32_t a) {
+  uint2 r;
+  asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(r.x), "=r"(r.y) : "r"(a));
+  return r;
+}
+__device__ __forceinline__ uint32_t saddr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
 
 __device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
 #pragma unroll
@@ -50,31 +80,41 @@ __device__ __forceinline__ double warp_fmax(double v) {
   return v;
 }
 
-// One lane's shared-memory view. The tape values and the permuted
-// right-hand side are one array v = [tv | y], the value space of the warp
-// programs.
+// One lane's shared block (the host's lane_layout).
 struct LaneMem {
+  double* base;
   double* x;     // n: current iterate
   double* xo;    // n: previous iterate
   double* rhs;   // n: residual F(x)
   double* diag;  // n: assembled diagonal (gates, runaway bound)
-  double* tv;    // ntv: tape values (U, diagonal, L, discard)
-  double* y;     // n: permuted solve vector, right after tv
+  double* v;     // tape values (U, diagonal, L, discard) | y | 0.0 | 1.0 | sink
+  double* y;     // n: permuted solve vector, inside v
   double* st;    // n_stage: device contributions
   double* lim;   // nlim: limited junction images
 };
 
 __device__ __forceinline__ LaneMem carve(const TopoDev& T, double* base) {
   LaneMem m;
+  m.base = base;
   m.x = base;
   m.xo = m.x + T.n;
   m.rhs = m.xo + T.n;
   m.diag = m.rhs + T.n;
-  m.tv = m.diag + T.n;
-  m.y = m.tv + T.ntv;
-  m.st = m.y + T.n;
+  m.v = m.diag + T.n;
+  m.y = m.v + T.ntv;
+  m.st = m.v + T.nv;
   m.lim = m.st + T.n_stage;
   return m;
+}
+
+// Copies the program blob into the CTA's shared memory (every thread takes
+// part) and returns the lanes' area that follows it.
+__device__ __forceinline__ double* stage_programs(const TopoDev& T, unsigned char* smem) {
+  const uint4* src = reinterpret_cast<const uint4*>(T.prog);
+  uint4* dst = reinterpret_cast<uint4*>(smem);
+  for (uint32_t i = threadIdx.x; i < T.prog_bytes / 16; i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  return reinterpret_cast<double*>(smem + T.prog_bytes);
 }
 
 // Device evaluation: every instance of every batch, strided over the warp,
@@ -92,7 +132,7 @@ __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, 
         case kR: {
           const double rv = r[0];
           const double g = 1.0 / rv;
-          const double cur = (m.x[nd[0]] - m.x[nd[1]]) / rv;
+          const double cur = div_rn(m.x[nd[0]] - m.x[nd[1]], rv);
           st[0] = cur;
           st[1] = -cur;
           st[2] = g;
@@ -140,76 +180,78 @@ __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, 
   }
 }
 
-__device__ __forceinline__ double gather_value(const LaneMem& m, uint32_t src) {
-  if (src == kSrcOne) return 1.0;
-  if (src == kSrcX0) return m.x[0];
-  return m.st[src];
-}
-
-// Assembly: each residual row and each pattern slot sums its contributions
-// in the reference's stamp order (batch, instance, local row, local column),
-// then the ground pin; the matrix lands in its tape value (amap).
-__device__ void assemble(const TopoDev& T, const LaneMem& m, int tid) {
-  for (uint32_t i = tid; i < T.n; i += 32) {
+// Assembly: every residual row and pattern slot sums its staging cells in
+// the reference's stamp order (batch, instance, local row, local column),
+// the ground pin last; slots land in their tape values, the diagonal is
+// copied for the gates, y = P(-rhs) is loaded and fill-in zeroed, all in
+// one gather program (groups of 32 cells; a cell t of group g sums
+// src[off + k * 32 + t], lane-block indices, then writes three places).
+__device__ void assemble(const TopoDev& T, uint32_t prog, const LaneMem& m, int tid) {
+  const uint32_t lb = saddr(m.base);
+  const uint32_t depth = prog + T.o_g_depth, goff = prog + T.o_g_off;
+  const uint32_t gsrc = prog + T.o_g_src, gdst = prog + T.o_g_dst;
+  for (uint32_t g = 0; g < T.n_groups; ++g) {
+    const uint32_t d = lds_u32(depth + 4 * g);
+    const uint32_t src = gsrc + 4 * (lds_u32(goff + 4 * g) + tid);
     double s = 0.0;
-    for (uint32_t e = T.rhs_ptr[i]; e < T.rhs_ptr[i + 1]; ++e) s = __dadd_rn(s, gather_value(m, T.rhs_src[e]));
-    m.rhs[i] = s;
-  }
-  for (uint32_t j = tid; j < T.n_fill; j += 32) m.tv[T.fill[j]] = 0.0;
-  for (uint32_t p = tid; p < T.nnz; p += 32) {
-    double s = 0.0;
-    for (uint32_t e = T.a_ptr[p]; e < T.a_ptr[p + 1]; ++e) s = __dadd_rn(s, gather_value(m, T.a_src[e]));
-    m.tv[T.amap[p]] = s;
-    const uint32_t row = T.slot_row[p];
-    if (row != kNoDiag) m.diag[row] = s;
+    for (uint32_t k = 0; k < d; ++k) s = __dadd_rn(s, lds(lb + 8 * lds_u32(src + 128 * k)));
+    const uint32_t dst = gdst + 12 * (g * 32 + tid);
+    sts(lb + 8 * lds_u32(dst), s);
+    sts(lb + 8 * lds_u32(dst + 4), s);
+    sts(lb + 8 * lds_u32(dst + 8), -s);
   }
 }
 
-// The matrix in pattern order, for a lane the host factors.
+// The matrix in pattern order, for a lane the host factors (the CSR lists,
+// staging indices or the two pin sources).
 __device__ void gather_pattern(const TopoDev& T, const LaneMem& m, double* out, int tid) {
   for (uint32_t p = tid; p < T.nnz; p += 32) {
     double s = 0.0;
-    for (uint32_t e = T.a_ptr[p]; e < T.a_ptr[p + 1]; ++e) s = __dadd_rn(s, gather_value(m, T.a_src[e]));
+    for (uint32_t e = T.a_ptr[p]; e < T.a_ptr[p + 1]; ++e) {
+      const uint32_t src = T.a_src[e];
+      s = __dadd_rn(s, src == kSrcOne ? 1.0 : src == kSrcX0 ? m.x[0] : m.st[src]);
+    }
     out[p] = s;
   }
 }
 
-// Runs one warp program: rows of 32 ops, thread t taking op t of each row,
-// the next row's op fetched while this one runs. Returns true when a
-// division failed its pivot test (thread-local; the caller reduces).
-__device__ __forceinline__ bool run_rows(const uint2* ops, uint32_t rows, double* v, int tid) {
+// Runs one warp program over v (shared address vb): rows of 32 ops of one
+// kind (a warp-uniform switch), thread t taking op t, the next row's op
+// fetched while this one runs. Padding ops move 1.0 / 0.0 into the sink.
+// Returns true when a division failed its pivot test (thread-local).
+__device__ __forceinline__ bool run_rows(uint32_t ops, uint32_t rows, uint32_t vb, int tid) {
   bool bad = false;
   if (rows == 0) return false;
-  uint2 op = ops[tid];
+  uint2 op = lds_u2(ops + 8 * tid);
   for (uint32_t r = 0; r < rows; ++r) {
-    const uint2 next = r + 1 < rows ? ops[(r + 1) * 32 + tid] : op;
-    const uint32_t kind = op.x >> 28, dst = op.x & 0x0fffffffu;
-    const uint32_t a = op.y & 0xffffu, b = op.y >> 16;
+    const uint32_t rn = r + 1 < rows ? r + 1 : r;
+    const uint2 next = lds_u2(ops + 8 * (rn * 32 + tid));
+    const uint32_t kind = op.x >> 28;
+    const uint32_t pd = vb + 8 * (op.x & 0x0fffffffu);
+    const uint32_t pa = vb + 8 * (op.y & 0xffffu), pb = vb + 8 * (op.y >> 16);
     switch (kind) {
       case kOpFlop:
-        v[dst] = __dsub_rn(v[dst], __dmul_rn(v[a], v[b]));
+        sts(pd, __dsub_rn(lds(pd), __dmul_rn(lds(pa), lds(pb))));
         break;
-      case kOpDivGrowth: {
-        const double w = v[dst], d = v[a];
+      case kOpSubNz: {
+        const double yb = lds(pb);
+        if (yb != 0.0) sts(pd, __dsub_rn(lds(pd), __dmul_rn(lds(pa), yb)));
+        break;
+      }
+      case kOpDivGrowth: {  // dividend at b (the op's own value; 1.0 on padding)
+        const double w = lds(pb), d = lds(pa);
         if (!(fabs(d) >= __dmul_rn(kGrowth, fabs(w)))) bad = true;
-        v[dst] = __ddiv_rn(w, d);
+        sts(pd, div_rn(w, d));
         break;
       }
       case kOpDivScaled: {
-        const double l = __ddiv_rn(v[dst], v[a]);
+        const double l = div_rn(lds(pb), lds(pa));
         if (!(fabs(l) < CUDART_INF)) bad = true;
-        v[dst] = l;
+        sts(pd, l);
         break;
       }
-      case kOpSubNz: {
-        const double yb = v[b];
-        if (yb != 0.0) v[dst] = __dsub_rn(v[dst], __dmul_rn(v[a], yb));
-        break;
-      }
-      case kOpDivY:
-        v[dst] = __ddiv_rn(v[dst], v[a]);
-        break;
-      default:
+      default:  // kOpDivY
+        sts(pd, div_rn(lds(pb), lds(pa)));
         break;
     }
     __syncwarp();
@@ -222,8 +264,8 @@ __device__ __forceinline__ bool run_rows(const uint2* ops, uint32_t rows, double
 // then the lane kernel's peel tests (lane_kernels.zig Bodies.refactor and
 // LaneSolver.wideMultipliers): U entries finite, pivots alive, L multipliers
 // within 1 / pivot_tol. y must hold P(-rhs). Warp-uniform verdict.
-__device__ bool refactor_forward(const TopoDev& T, double* v, int tid) {
-  bool bad = run_rows(T.a_ops, T.a_rows, v, tid);
+__device__ bool refactor_forward(const TopoDev& T, uint32_t prog, double* v, int tid) {
+  bool bad = run_rows(prog + T.o_a_ops, T.a_rows, saddr(v), tid);
   const uint32_t l0 = T.nu + T.n;
   for (uint32_t s = tid; s < T.nu; s += 32)
     if (dbits(v[s] - v[s]) != 0) bad = true;
@@ -236,8 +278,20 @@ __device__ bool refactor_forward(const TopoDev& T, double* v, int tid) {
   return __any_sync(kFull, bad);
 }
 
+__device__ __forceinline__ void back_solve(const TopoDev& T, uint32_t prog, double* v, int tid) {
+  run_rows(prog + T.o_b_ops, T.b_rows, saddr(v), tid);
+}
+
 __device__ __forceinline__ void load_y(const TopoDev& T, const double* rhs, double* y, int tid) {
   for (uint32_t r = tid; r < T.n; r += 32) y[T.pinv[r]] = -rhs[r];
+}
+
+__device__ __forceinline__ void init_consts(const TopoDev& T, double* v, int tid) {
+  if (tid == 0) {
+    v[T.ntv + T.n] = 0.0;
+    v[T.ntv + T.n + 1] = 1.0;
+    v[T.ntv + T.n + 2] = 0.0;
+  }
 }
 
 __device__ __forceinline__ double residual_gate(const LaneOpts& o, double diag, double xi) {
@@ -269,22 +323,20 @@ __device__ bool apply_limits(const TopoDev& T, const double* rec, const LaneMem&
 
 }  // namespace
 
-// DC Newton over independent sweep points (sweep/lanes.zig solveBatch:
-// each lane bitwise its own converger.run), one warp per lane.
-__global__ void __launch_bounds__(256) dc_newton_kernel(TopoDev T, LaneDev L, LaneOpts o) {
-  extern __shared__ double smem[];
-  const int tid = threadIdx.x & 31;
-  const uint32_t lane = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (lane >= L.n_lanes) return;
+// One lane's DC Newton solve (converger.zig newtonLanes at W = 1 with the
+// lane's own direct solver), by the warp that owns it.
+__device__ void dc_solve_lane(const TopoDev& T, const LaneDev& L, const LaneOpts& o, uint32_t prog, double* block,
+                              uint32_t lane, int tid) {
   const uint32_t status = L.status[lane];
   const bool resuming = L.resume && status == kNeedSolve;
   if (!(status == kRunning || resuming)) return;
 
   const uint32_t n = T.n;
-  LaneMem m = carve(T, smem + size_t(threadIdx.x >> 5) * T.smem_doubles);
+  LaneMem m = carve(T, block);
   const double* rec = L.rec + size_t(lane) * T.rec_size;
   for (uint32_t i = tid; i < n; i += 32) m.x[i] = L.x[size_t(lane) * n + i];
   for (uint32_t i = tid; i < T.nlim; i += 32) m.lim[i] = L.lim[size_t(lane) * T.nlim + i];
+  init_consts(T, m.v, tid);
   bool lim_active = L.lim_active[lane] != 0;
   uint32_t flags = L.flags[lane];
   uint32_t iter = L.iters[lane];
@@ -299,8 +351,8 @@ __global__ void __launch_bounds__(256) dc_newton_kernel(TopoDev T, LaneDev L, La
     for (uint32_t i = tid; i < n; i += 32) {
       m.rhs[i] = L.rhs[size_t(lane) * n + i];
       m.diag[i] = L.diag[size_t(lane) * n + i];
-      // the host's dx, permuted as the device solve leaves it
     }
+    // the host's dx, permuted as the device solve leaves it
     for (uint32_t j = tid; j < n; j += 32) m.y[j] = L.dx[size_t(lane) * n + T.qcol[j]];
     have_step = true;
   }
@@ -310,7 +362,7 @@ __global__ void __launch_bounds__(256) dc_newton_kernel(TopoDev T, LaneDev L, La
     if (!have_step) {
       eval_all(T, rec, m, lim_active, sim, tid);
       __syncwarp();
-      assemble(T, m, tid);
+      assemble(T, prog, m, tid);
       __syncwarp();
       if (o.gmin > 0) {
         // loadExtras: diagonal gmin and its residual form
@@ -319,10 +371,12 @@ __global__ void __launch_bounds__(256) dc_newton_kernel(TopoDev T, LaneDev L, La
           if (row != kNoDiag) {
             const double d = m.diag[row] + o.gmin;
             m.diag[row] = d;
-            m.tv[T.amap[p]] = d;
+            m.v[T.amap[p]] = d;
           }
         }
         for (uint32_t i = tid; i < n; i += 32) m.rhs[i] += o.gmin * m.x[i];
+        __syncwarp();
+        load_y(T, m.rhs, m.y, tid);
         __syncwarp();
       }
       if (iter == 0) {
@@ -343,11 +397,7 @@ __global__ void __launch_bounds__(256) dc_newton_kernel(TopoDev T, LaneDev L, La
       }
       const bool host_mode = (flags & 2u) != 0;
       bool bad = true;
-      if (!host_mode) {
-        load_y(T, m.rhs, m.y, tid);
-        __syncwarp();
-        bad = refactor_forward(T, m.tv, tid);
-      }
+      if (!host_mode) bad = refactor_forward(T, prog, m.v, tid);
       if (bad) {
         // Pause: the host factors this lane with its own direct solver.
         const size_t base = size_t(lane) * n;
@@ -368,7 +418,7 @@ __global__ void __launch_bounds__(256) dc_newton_kernel(TopoDev T, LaneDev L, La
         }
         return;
       }
-      run_rows(T.b_ops, T.b_rows, m.tv, tid);
+      back_solve(T, prog, m.v, tid);
     }
     have_step = false;
     __syncwarp();
@@ -384,7 +434,7 @@ __global__ void __launch_bounds__(256) dc_newton_kernel(TopoDev T, LaneDev L, La
       m.x[i] = xn;
       const double tol = o.reltol * fmax(fabs(xn), fabs(xold)) + (T.cur_row[i] ? o.abstol : o.vntol);
       const bool finite = fabs(xn) < CUDART_INF && fabs(d) < CUDART_INF;
-      const double qv = fabs(d) / tol;
+      const double qv = div_rn(fabs(d), tol);
       const double score = !finite ? CUDART_INF : (qv == qv ? qv : 0.0);
       const uint64_t b = dbits(score);
       worst = b > worst ? b : worst;
@@ -428,45 +478,63 @@ __global__ void __launch_bounds__(256) dc_newton_kernel(TopoDev T, LaneDev L, La
   }
 }
 
+// DC Newton over independent sweep points (sweep/lanes.zig solveBatch:
+// each lane bitwise its own converger.run), one warp per lane; a persistent
+// grid, each CTA staging the programs once and taking lanes in turn.
+__global__ void __launch_bounds__(256) dc_newton_kernel(TopoDev T, LaneDev L, LaneOpts o) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* lanes_smem = stage_programs(T, smem_raw);
+  const uint32_t prog = saddr(smem_raw);
+  const int tid = threadIdx.x & 31;
+  const uint32_t warps = blockDim.x >> 5, w = threadIdx.x >> 5;
+  double* block = lanes_smem + size_t(w) * T.smem_doubles;
+  for (uint32_t lane = blockIdx.x * warps + w; lane < L.n_lanes; lane += gridDim.x * warps) {
+    dc_solve_lane(T, L, o, prog, block, lane, tid);
+    __syncwarp();
+  }
+}
+
 // Standalone lane refactor + solve on the frozen tape (the reference's
 // arp_lane_refactor + arp_lane_solve): A [lane][nnz] and rhs [lane][n] in
-// HBM, L/U/diagonal tape values [lane][ntv], dx [lane][n] and the peel
-// verdict out. One warp per lane; the tape values stay in shared memory
-// between the scatter, the factor and the solves.
+// HBM, the tape values (U, diagonal, L) [lane][ntv], dx [lane][n] and the
+// peel verdict out. One warp per lane; the tape values stay in shared
+// memory between the scatter, the factor and the solves.
 __global__ void __launch_bounds__(256) lu_replay_kernel(TopoDev T, uint32_t n_lanes, const double* a,
                                                          const double* rhs, double* tv_out, double* dx,
                                                          uint8_t* bad_out) {
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* lanes_smem = stage_programs(T, smem_raw);
+  const uint32_t prog = saddr(smem_raw);
   const int tid = threadIdx.x & 31;
-  const uint32_t lane = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (lane >= n_lanes) return;
-  double* tv = smem + size_t(threadIdx.x >> 5) * (T.ntv + 2 * T.n + 2);
-  double* y = tv + T.ntv;
-  double* r = y + T.n;
-  for (uint32_t j = tid; j < T.n_fill; j += 32) tv[T.fill[j]] = 0.0;
-  const double* al = a + size_t(lane) * T.nnz;
-  for (uint32_t p = tid; p < T.nnz; p += 32) tv[T.amap[p]] = al[p];
-  for (uint32_t i = tid; i < T.n; i += 32) r[i] = rhs[size_t(lane) * T.n + i];
-  __syncwarp();
-  load_y(T, r, y, tid);
-  __syncwarp();
-  const bool bad = refactor_forward(T, tv, tid);
-  run_rows(T.b_ops, T.b_rows, tv, tid);
-  for (uint32_t j = tid; j < T.n; j += 32) dx[size_t(lane) * T.n + T.qcol[j]] = y[j];
-  if (tv_out)
-    for (uint32_t s = tid; s < T.ntv; s += 32) tv_out[size_t(lane) * T.ntv + s] = tv[s];
-  if (tid == 0) bad_out[lane] = bad;
+  const uint32_t warps = blockDim.x >> 5, w = threadIdx.x >> 5;
+  double* v = lanes_smem + size_t(w) * (T.nv + T.n + 1);
+  double* y = v + T.ntv;
+  double* r = v + T.nv;
+  for (uint32_t lane = blockIdx.x * warps + w; lane < n_lanes; lane += gridDim.x * warps) {
+    init_consts(T, v, tid);
+    for (uint32_t j = tid; j < T.n_fill; j += 32) v[T.fill[j]] = 0.0;
+    const double* al = a + size_t(lane) * T.nnz;
+    for (uint32_t p = tid; p < T.nnz; p += 32) v[T.amap[p]] = al[p];
+    for (uint32_t i = tid; i < T.n; i += 32) r[i] = rhs[size_t(lane) * T.n + i];
+    __syncwarp();
+    load_y(T, r, y, tid);
+    __syncwarp();
+    const bool bad = refactor_forward(T, prog, v, tid);
+    back_solve(T, prog, v, tid);
+    for (uint32_t j = tid; j < T.n; j += 32) dx[size_t(lane) * T.n + T.qcol[j]] = y[j];
+    if (tv_out)
+      for (uint32_t s = tid; s < T.ntv; s += 32) tv_out[size_t(lane) * T.ntv + s] = v[s];
+    if (tid == 0) bad_out[lane] = bad;
+    __syncwarp();
+  }
 }
-
-}  // namespace esl
-
-namespace esl {
 
 // The matrix of one lane at its start point, in pattern order: the lead
 // lane's first Jacobian, which the host factors into the pivot tape
 // (gpu_lanes.zig:361-372 factors lane 0 on the host the same way).
 __global__ void assemble_kernel(TopoDev T, LaneDev L, uint32_t lane, double* out) {
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* smem = reinterpret_cast<double*>(smem_raw);
   const int tid = threadIdx.x & 31;
   if (threadIdx.x >= 32) return;
   LaneMem m = carve(T, smem);
@@ -484,34 +552,47 @@ __global__ void assemble_kernel(TopoDev T, LaneDev L, uint32_t lane, double* out
 
 size_t lane_smem_bytes(const TopoDev& T) { return size_t(T.smem_doubles) * sizeof(double); }
 
-cudaError_t launch_dc_newton(const TopoDev& T, const LaneDev& L, const LaneOpts& o,
-                             uint32_t lanes_per_block, cudaStream_t s) {
-  const size_t smem = lanes_per_block * lane_smem_bytes(T);
+// CTAs for a persistent launch: enough for every lane, at most as many as
+// the device holds at once (SMs x resident CTAs at this shared memory).
+template <class K>
+static uint32_t persistent_grid(K kernel, uint32_t n_lanes, uint32_t lanes_per_block, size_t smem) {
+  const uint32_t need = (n_lanes + lanes_per_block - 1) / lanes_per_block;
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, int(32 * lanes_per_block), smem);
+  const uint32_t cap = uint32_t(sms) * uint32_t(per_sm > 0 ? per_sm : 1);
+  return need < cap ? need : cap;
+}
+
+cudaError_t launch_dc_newton(const TopoDev& T, const LaneDev& L, const LaneOpts& o, uint32_t lanes_per_block,
+                             cudaStream_t s) {
+  const size_t smem = T.prog_bytes + lanes_per_block * lane_smem_bytes(T);
   cudaError_t e = cudaFuncSetAttribute(dc_newton_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
-  const uint32_t grid = (L.n_lanes + lanes_per_block - 1) / lanes_per_block;
-  dc_newton_kernel<<<grid, 32 * lanes_per_block, smem, s>>>(T, L, o);
+  dc_newton_kernel<<<persistent_grid(dc_newton_kernel, L.n_lanes, lanes_per_block, smem), 32 * lanes_per_block, smem,
+                     s>>>(T, L, o);
   return cudaGetLastError();
 }
 
 cudaError_t launch_assemble(const TopoDev& T, const LaneDev& L, uint32_t lane, double* out, cudaStream_t s) {
   // Before the tape exists (the lead lane's first Jacobian) a lane needs no
-  // tape values: x, xo, y, rhs, diag, staging and the limited images.
-  const size_t smem = size_t(5 * T.n + T.ntv + T.n_stage + T.nlim + 2) * sizeof(double);
+  // tape values: x, xo, rhs, diag, staging and the limited images (nv = 0).
+  const size_t smem = size_t(4 * T.n + T.nv + T.n_stage + T.nlim + 2) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(assemble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   assemble_kernel<<<1, 32, smem, s>>>(T, L, lane, out);
   return cudaGetLastError();
 }
 
-cudaError_t launch_lu_replay(const TopoDev& T, uint32_t n_lanes, const double* a, const double* rhs,
-                             double* tv, double* dx, uint8_t* bad, uint32_t lanes_per_block, cudaStream_t s) {
-  const size_t per = size_t(T.ntv + 2 * T.n + 2) * sizeof(double);
-  const size_t smem = lanes_per_block * per;
+cudaError_t launch_lu_replay(const TopoDev& T, uint32_t n_lanes, const double* a, const double* rhs, double* tv,
+                             double* dx, uint8_t* bad, uint32_t lanes_per_block, cudaStream_t s) {
+  const size_t per = size_t(T.nv + T.n + 1) * sizeof(double);
+  const size_t smem = T.prog_bytes + lanes_per_block * per;
   cudaError_t e = cudaFuncSetAttribute(lu_replay_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
-  const uint32_t grid = (n_lanes + lanes_per_block - 1) / lanes_per_block;
-  lu_replay_kernel<<<grid, 32 * lanes_per_block, smem, s>>>(T, n_lanes, a, rhs, tv, dx, bad);
+  lu_replay_kernel<<<persistent_grid(lu_replay_kernel, n_lanes, lanes_per_block, smem), 32 * lanes_per_block, smem,
+                     s>>>(T, n_lanes, a, rhs, tv, dx, bad);
   return cudaGetLastError();
 }
 

@@ -1,5 +1,6 @@
 """Test helper: runs the library's compiled warp programs (as
-esl_compile_tape returns them: rows of 32 ops over v = [tape values | y]) on
+esl_compile_tape returns them: rows of 32 ops of one kind over
+v = [tape values | y | 0.0 | 1.0 | sink], padding ops writing the sink) on
 the CPU, row by row, with numpy float64 (IEEE, no fused multiply-add).
 Every op of a row reads the values as they stood before the row (the
 parallel semantics), so a schedule that let two ops of one row touch the
@@ -25,12 +26,12 @@ def _run(words, v):
             if kind == FLOP:
                 v[dst] = snap[dst] - snap[a] * snap[b]
             elif kind == DIVG:
-                x, d = snap[dst], snap[a]
+                x, d = snap[b], snap[a]
                 if not (abs(d) >= 1e-12 * abs(x)):
                     bad = True
                 v[dst] = x / d
             elif kind == DIVS:
-                l = snap[dst] / snap[a]
+                l = snap[b] / snap[a]
                 if not np.isfinite(l):
                     bad = True
                 v[dst] = l
@@ -38,7 +39,7 @@ def _run(words, v):
                 if snap[b] != 0:
                     v[dst] = snap[dst] - snap[a] * snap[b]
             elif kind == DIVY:
-                v[dst] = snap[dst] / snap[a]
+                v[dst] = snap[b] / snap[a]
     return bad
 
 
@@ -46,7 +47,8 @@ def refactor_solve(tape, vals, rhs, n):
     """(tv, dx, bad) for one lane: program A, the peel tests, program B."""
     info = tape["info"]
     nu, nl, ntv = info["nu"], info["nl"], info["ntv"]
-    v = np.zeros(ntv + n)
+    v = np.zeros(ntv + n + 3)  # tape values | y | 0.0 | 1.0 | sink
+    v[ntv + n + 1] = 1.0
     v[tape["amap"]] = vals
     v[ntv + tape["pinv"]] = -rhs
     bad = _run(tape["a_ops"], v)
