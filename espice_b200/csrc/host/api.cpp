@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -700,6 +701,85 @@ int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d
     std::vector<uint32_t> status(N);
     ESL_CUDA(cudaMemcpy(status.data(), d_status, N * 4, cudaMemcpyDeviceToHost));
     for (uint32_t v : status) st->converged += v == kConverged;
+  }
+  return ESL_OK;
+}
+
+// Allocation-free variant of esl_dc_solve_device: the same fused kernel, with
+// the per-lane Newton state and hand-off buffers carved from the fixed device
+// array of newton.cu instead of the context's allocations, and the lane start
+// state written by a kernel instead of host vectors. Error text goes into the
+// context's message buffer, reserved on the first call.
+int32_t esl_dc_solve_device_static(esl_ctx* ctx, const esl_newton_opts* opts, double* d_x, int cold,
+                                   uint32_t* d_iters, uint32_t* d_status, uint32_t* n_paused) {
+  if (!ctx) return ESL_INVALID_ARGUMENT;
+  constexpr size_t kErrCap = 256;
+  if (ctx->err.capacity() < kErrCap) ctx->err.reserve(kErrCap);
+  char msg[kErrCap];
+  auto fail = [&](int32_t code, const char* text) {
+    ctx->err.assign(text, std::min(std::strlen(text), kErrCap - 1));
+    return code;
+  };
+  auto cuda = [&](cudaError_t e, const char* where) {
+    std::snprintf(msg, sizeof msg, "%s: %s", where, cudaGetErrorString(e));
+    return fail(ESL_DEVICE_FAULT, msg);
+  };
+  if (n_paused) *n_paused = 0;
+  if (!opts || !d_x || !d_iters || !d_status || ctx->n_lanes == 0)
+    return fail(ESL_INVALID_ARGUMENT, "null argument or no lanes set");
+  if (!ctx->have_tape)
+    return fail(ESL_NOT_ELIGIBLE, "no pivot tape yet: the first solve of a context must be esl_dc_solve_device");
+  if (cudaError_t e = cudaSetDevice(ctx->device)) return cuda(e, "cudaSetDevice");
+  void* base = nullptr;
+  if (cudaError_t e = static_scratch(&base)) return cuda(e, "cudaGetSymbolAddress(lane scratch)");
+
+  // Carve: the paused-lane counter, then each per-lane plane on 256 bytes.
+  const size_t N = ctx->n_lanes, n = ctx->pat.n, nnz = ctx->pat.nnz();
+  const size_t nlim = std::max<size_t>(ctx->nlim, 1);
+  size_t at = 256;
+  auto carve = [&](size_t bytes) {
+    const size_t off = at;
+    at += (bytes + 255) & ~size_t(255);
+    return static_cast<unsigned char*>(base) + off;
+  };
+  LaneDev L{};
+  L.n_lanes = ctx->n_lanes;
+  L.rec = ctx->d_rec.as<double>();
+  L.x = d_x;
+  L.iters = d_iters;
+  L.status = d_status;
+  L.n_paused = static_cast<uint32_t*>(base);
+  L.a_vals = reinterpret_cast<double*>(carve(N * nnz * 8));
+  L.rhs = reinterpret_cast<double*>(carve(N * n * 8));
+  L.dx = reinterpret_cast<double*>(carve(N * n * 8));
+  L.diag = reinterpret_cast<double*>(carve(N * n * 8));
+  L.lim = reinterpret_cast<double*>(carve(N * nlim * 8));
+  L.limit = reinterpret_cast<double*>(carve(N * 8));
+  L.flags = reinterpret_cast<uint32_t*>(carve(N * 4));
+  L.lim_active = reinterpret_cast<uint32_t*>(carve(N * 4));
+  if (at > kStaticScratchBytes) {
+    std::snprintf(msg, sizeof msg,
+                  "%zu lanes need %zu bytes of lane scratch, above the fixed %zu bytes: use fewer lanes per call",
+                  N, at, kStaticScratchBytes);
+    return fail(ESL_INVALID_ARGUMENT, msg);
+  }
+  const LaneOpts o{opts->reltol, opts->abstol, opts->vntol, opts->residual_tol, opts->gmin, opts->max_iter,
+                   opts->init_fix};
+  cudaStream_t s = ctx->stream;
+  if (cudaError_t e = launch_lane_init(ctx->topo, L, cold != 0, opts->init_fix != 0, s))
+    return cuda(e, "lane_init_kernel");
+  if (cudaError_t e = launch_dc_newton(ctx->topo, L, o, ctx->lanes_eff, s)) return cuda(e, "dc_newton_kernel");
+  uint32_t paused = 0;
+  if (cudaError_t e = cudaMemcpyAsync(&paused, L.n_paused, 4, cudaMemcpyDeviceToHost, s))
+    return cuda(e, "read paused-lane count");
+  if (cudaError_t e = cudaStreamSynchronize(s)) return cuda(e, "cudaStreamSynchronize");
+  if (n_paused) *n_paused = paused;
+  if (paused) {
+    std::snprintf(msg, sizeof msg,
+                  "%u lanes left the lead pivot tape (status ESL_LANE_NEED_SOLVE); their host factor "
+                  "needs memory: solve those points with esl_dc_solve_device",
+                  paused);
+    return fail(ESL_NOT_ELIGIBLE, msg);
   }
   return ESL_OK;
 }

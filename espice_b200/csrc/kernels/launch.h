@@ -18,4 +18,12 @@ cudaError_t launch_lu_replay(const TopoDev& T, uint32_t n_lanes, const double* a
                              double* tv, double* dx, uint8_t* bad, uint32_t lanes_per_block,
                              cudaStream_t s);
 
+// Fixed lane scratch of the allocation-free DC entry point: its size, the
+// device address of the array on the current device (looked up once per
+// device; the first call per device must precede any stream capture), and
+// the device-side lane start-state kernel.
+constexpr size_t kStaticScratchBytes = size_t(16) << 20;
+cudaError_t static_scratch(void** ptr);
+cudaError_t launch_lane_init(const TopoDev& T, const LaneDev& L, bool cold, bool init_fix, cudaStream_t s);
+
 }  // namespace esl

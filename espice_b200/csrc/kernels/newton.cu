@@ -27,6 +27,8 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
+#include <mutex>
+
 #include "launch.h"
 #include "lanes.cuh"
 #include "models.cuh"
@@ -593,6 +595,67 @@ cudaError_t launch_lu_replay(const TopoDev& T, uint32_t n_lanes, const double* a
   if (e != cudaSuccess) return e;
   lu_replay_kernel<<<persistent_grid(lu_replay_kernel, n_lanes, lanes_per_block, smem), 32 * lanes_per_block, smem,
                      s>>>(T, n_lanes, a, rhs, tv, dx, bad);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Fixed lane scratch for the allocation-free DC entry point
+// (esl_dc_solve_device_static). The per-lane Newton state and the paused-lane
+// hand-off buffers the fused kernel keeps in HBM live in one file-scope device
+// array instead of context-owned allocations. The array is created with the
+// module (zero-filled by the loader) and is reached through its symbol
+// address, looked up once per device.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_lane_scratch[kStaticScratchBytes];
+
+cudaError_t static_scratch(void** ptr) {
+  constexpr int kMaxDevices = 64;
+  static void* addr[kMaxDevices] = {};
+  static std::mutex mu;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_lane_scratch);
+    if (e != cudaSuccess) return e;
+    addr[dev] = p;
+  }
+  *ptr = addr[dev];
+  return cudaSuccess;
+}
+
+// Start state of every lane (the host-side set-up of esl_dc_solve_device done
+// on the device): iteration 0, running, limit 1e9, INITFIX from the options;
+// a cold lane starts at x = 0 with its junction images at the seeds the
+// records carry (diode vcrit) and limiting live, a warm lane at its x with
+// limiting off. The first thread also clears the paused-lane counter.
+__global__ void lane_init_kernel(TopoDev T, LaneDev L, uint32_t cold, uint32_t init_fix) {
+  const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
+  if (lane == 0) *L.n_paused = 0;
+  if (lane >= L.n_lanes) return;
+  L.status[lane] = kRunning;
+  L.iters[lane] = 0;
+  L.flags[lane] = init_fix ? 1u : 0u;
+  L.lim_active[lane] = cold && T.nlim ? 1u : 0u;
+  L.limit[lane] = 1e9;
+  double* lim = L.lim + size_t(lane) * T.nlim;
+  for (uint32_t i = 0; i < T.nlim; ++i) lim[i] = 0.0;
+  if (!cold) return;
+  for (uint32_t i = 0; i < T.n; ++i) L.x[size_t(lane) * T.n + i] = 0.0;
+  const double* rec = L.rec + size_t(lane) * T.rec_size;
+  for (uint32_t b = 0; b < T.n_batches; ++b) {
+    const BatchDev& B = T.b[b];
+    if (B.type != kD) continue;
+    for (uint32_t i = 0; i < B.count; ++i) lim[B.lim_off + i] = rec[B.rec_off + kDVcrit * B.count + i];
+  }
+}
+
+cudaError_t launch_lane_init(const TopoDev& T, const LaneDev& L, bool cold, bool init_fix, cudaStream_t s) {
+  const uint32_t threads = 128, blocks = (L.n_lanes + threads - 1) / threads;
+  lane_init_kernel<<<blocks > 0 ? blocks : 1, threads, 0, s>>>(T, L, cold ? 1u : 0u, init_fix ? 1u : 0u);
   return cudaGetLastError();
 }
 

@@ -22,11 +22,11 @@ LIB_PATH = os.path.join(HERE, "libespice_lanes.so")
 
 ESL_OK, ESL_INVALID_ARGUMENT, ESL_OUT_OF_MEMORY = 0, 1, 3
 ESL_NOT_ELIGIBLE, ESL_NO_DEVICE, ESL_DEVICE_FAULT, ESL_TIMEOUT = 4, 5, 6, 7
-LANE_CONVERGED, LANE_MAX_ITER, LANE_SINGULAR = 1, 2, 3
+LANE_CONVERGED, LANE_MAX_ITER, LANE_SINGULAR, LANE_NEED_SOLVE = 1, 2, 3, 4
 
 # Every entry point include/espice_lanes.h declares.
 EXPORTS = ["esl_create", "esl_destroy", "esl_last_error", "esl_dims", "esl_set_lanes",
-           "esl_dc_solve", "esl_dc_solve_device", "esl_tape", "esl_lu_replay_device",
+           "esl_dc_solve", "esl_dc_solve_device", "esl_dc_solve_device_static", "esl_tape", "esl_lu_replay_device",
            "esl_tape_size", "esl_pattern", "esl_compile_tape"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
@@ -219,6 +219,20 @@ class DcLanes:
                                                 ctypes.byref(stats)),
                     "esl_dc_solve_device")
         return stats.as_dict()
+
+    def solve_device_static(self, d_x, d_iters, d_status, cold=False, opts=None):
+        """solve_device through the allocation-free entry point (fixed lane
+        scratch in the library; the context's first solve must be
+        solve_device). Returns the number of lanes left paused (0 on success;
+        a nonzero count raises with ESL_NOT_ELIGIBLE)."""
+        opts = opts or newton_opts()
+        paused = ctypes.c_uint32(0)
+        self._check(self._L.esl_dc_solve_device_static(self._ctx, ctypes.byref(opts),
+                                                       ctypes.c_void_p(d_x), ctypes.c_int(int(cold)),
+                                                       ctypes.c_void_p(d_iters), ctypes.c_void_p(d_status),
+                                                       ctypes.byref(paused)),
+                    "esl_dc_solve_device_static")
+        return paused.value
 
     def tape(self):
         q = np.zeros(self.n, np.uint32)

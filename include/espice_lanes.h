@@ -49,7 +49,8 @@ enum {
 enum {
     ESL_LANE_CONVERGED = 1,
     ESL_LANE_MAX_ITER = 2, /* Newton ran out of iterations (non-converged point) */
-    ESL_LANE_SINGULAR = 3  /* the lane's own factor failed (SingularMatrix) */
+    ESL_LANE_SINGULAR = 3, /* the lane's own factor failed (SingularMatrix) */
+    ESL_LANE_NEED_SOLVE = 4 /* left the lead tape; only esl_dc_solve_device_static leaves it */
 };
 
 typedef struct {
@@ -131,6 +132,35 @@ int32_t esl_dc_solve(esl_ctx *ctx, const esl_newton_opts *opts, const double *x0
  * lanes are done (host peels included). */
 int32_t esl_dc_solve_device(esl_ctx *ctx, const esl_newton_opts *opts, double *d_x, int cold,
                             uint32_t *d_iters, uint32_t *d_status, esl_stats *stats);
+
+/* esl_dc_solve_device without allocating. No counterpart in the reference:
+ * its lane solver allocates its lane planes per call.
+ *
+ * For callers that cannot allocate device memory while they solve: a
+ * process whose device memory is held by a pool sized at start-up, and any
+ * caller that keeps work in flight on other streams, where cudaMalloc and
+ * cudaFree would synchronise the whole device. The call allocates no device
+ * memory: the per-lane Newton state and the paused-lane buffers live in one
+ * fixed 16 MiB device array in the library, and the lane start state is set
+ * by a kernel. Per lane it needs 8 * (nnz + 3 n + max(nlim, 1) + 1) + 8
+ * bytes (each plane rounded up to 256 bytes, plus 256 for a counter); more
+ * lanes than fit are refused with ESL_INVALID_ARGUMENT before any launch.
+ *
+ * Set-up: the first call on a device looks up the array's address, and the
+ * first call on a context reserves its error-message buffer; make that
+ * first call before any stream capture begins. The context needs its pivot
+ * tape (one esl_dc_solve_device call on it first) and its lanes (esl_set_lanes).
+ * Nothing has to start at zero: the call writes every lane's start state and
+ * clears the counter itself. Calls overlapping in time on one device (any
+ * contexts, streams or host threads) share the array and race: serialise them.
+ *
+ * Same arguments and results as esl_dc_solve_device, except that lanes that
+ * leave the lead pivot tape are not served on the host (that needs memory):
+ * they are left with status ESL_LANE_NEED_SOLVE, their count goes to
+ * *n_paused (may be NULL) and the call returns ESL_NOT_ELIGIBLE. */
+int32_t esl_dc_solve_device_static(esl_ctx *ctx, const esl_newton_opts *opts, double *d_x,
+                                   int cold, uint32_t *d_iters, uint32_t *d_status,
+                                   uint32_t *n_paused);
 
 /* The lead lane's pivot tape after the last solve (buildTab,
  * lane_kernels.zig:321-345): q[n], pinv[n]; counts[0] = |L|, counts[1] = |U|,
