@@ -18,7 +18,10 @@ constexpr int kMaxBatches = 8;
 //   V: f0 f1 f2 J02 J12 J20 J21
 //   I: f0 f1
 //   D: f0 f1 f2 J00 J02 J11 J12 J20 J21 J22 | q1 q2 C11 C12 C21 C22
-constexpr int kStageR = 6, kStageC = 6, kStageV = 7, kStageI = 2, kStageD = 16;
+//   M (local unknowns 0 d, 1 g, 2 s, 3 b, 4 di, 5 si):
+//      f0 f2 f3 f4 f5 | J00 J04 J22 J25 J33 J34 J35 J40 J41 J43 J44 J45 J51 J52 J53 J54 J55
+//      | q1 q3 q4 q5 | C11 C13 C14 C15 C31 C33 C34 C35 C41 C43 C44 C51 C53 C55
+constexpr int kStageR = 6, kStageC = 6, kStageV = 7, kStageI = 2, kStageD = 16, kStageM = 40;
 
 // Per-instance record fields (doubles, field-major per batch in a lane's
 // record block). Diode fields follow the bias-independent part of
@@ -28,6 +31,20 @@ enum DiodeField {
   kDHasRs, kDHasQ, kDiodeFields
 };
 constexpr int kRFields = 1, kCFields = 1, kVFields = 10, kIFields = 1;
+
+// MOS1 record fields: the bias-independent part of models/mos1.va
+// (temperature, geometry, junction sizing), in the type frame.
+enum MosField {
+  kMType, kMVt, kMVbit, kMGamma, kMPhit, kMBeta, kMLambda, kMIsats, kMIsatd, kMVcrits, kMVcritd,
+  kMGdrain, kMGsource, kMCzbd, kMCzbs, kMCzbdsw, kMCzbssw, kMPbt, kMMj, kMMjsw, kMFc, kMF2d, kMF3d,
+  kMF4d, kMF2s, kMF3s, kMF4s, kMCgs, kMCgd, kMCgb, kMGmin, kMHasQ, kMSeedVgs, kMosFields
+};
+constexpr int kMosParams = 34;
+constexpr int kMParamRd = 6, kMParamRs = 7, kMParamTox = 19;
+
+// Limited images per instance: a diode's junction voltage; a MOSFET's
+// vgs, vds, vbs in the type frame.
+constexpr uint32_t lim_count(uint32_t type) { return type == kD ? 1u : type == kM ? 3u : 0u; }
 
 // Special gather sources beside staging positions.
 constexpr uint32_t kSrcOne = 0xfffffffeu;    // + 1.0 (the ground pin on g)

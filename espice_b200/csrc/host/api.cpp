@@ -63,6 +63,7 @@ uint32_t stage_stride(uint32_t type) {
     case kV: return kStageV;
     case kI: return kStageI;
     case kD: return kStageD;
+    case kM: return kStageM;
     default: return 0;
   }
 }
@@ -113,6 +114,43 @@ InstLayout layout_of(uint32_t type, const double* prm) {
       if (prm[5] > 0 || prm[9] > 0) {
         L.q = {{1, 0, 10}, {2, 0, 11}};
         L.qjac = {{1, 1, 12}, {1, 2, 13}, {2, 1, 14}, {2, 2, 15}};
+      }
+      break;
+    }
+    case kM: {  // d g s b di si (models/mos1.va contributions)
+      const bool rd = prm[kMParamRd] > 0, rs = prm[kMParamRs] > 0;
+      if (rd) L.res.push_back({0, 0, 0});
+      if (rs) L.res.push_back({2, 0, 1});
+      L.res.push_back({3, 0, 2});
+      L.res.push_back({4, 0, 3});
+      L.res.push_back({5, 0, 4});
+      if (rd) {
+        L.jac.push_back({0, 0, 5});
+        L.jac.push_back({0, 4, 6});
+      }
+      if (rs) {
+        L.jac.push_back({2, 2, 7});
+        L.jac.push_back({2, 5, 8});
+      }
+      L.jac.push_back({3, 3, 9});
+      L.jac.push_back({3, 4, 10});
+      L.jac.push_back({3, 5, 11});
+      if (rd) L.jac.push_back({4, 0, 12});
+      L.jac.push_back({4, 1, 13});
+      L.jac.push_back({4, 3, 14});
+      L.jac.push_back({4, 4, 15});
+      L.jac.push_back({4, 5, 16});
+      L.jac.push_back({5, 1, 17});
+      if (rs) L.jac.push_back({5, 2, 18});
+      L.jac.push_back({5, 3, 19});
+      L.jac.push_back({5, 4, 20});
+      L.jac.push_back({5, 5, 21});
+      double rec[kMosFields];
+      derive_instance(kM, prm, rec, 1);
+      if (rec[kMHasQ] != 0.0) {
+        L.q = {{1, 0, 22}, {3, 0, 23}, {4, 0, 24}, {5, 0, 25}};
+        L.qjac = {{1, 1, 26}, {1, 3, 27}, {1, 4, 28}, {1, 5, 29}, {3, 1, 30}, {3, 3, 31}, {3, 4, 32},
+                  {3, 5, 33}, {4, 1, 34}, {4, 3, 35}, {4, 4, 36}, {5, 1, 37}, {5, 3, 38}, {5, 5, 39}};
       }
       break;
     }
@@ -230,7 +268,7 @@ bool read_circuit(const esl_circuit* c, std::vector<HostBatch>& bats) {
     B.rec_off = rec;
     rec += B.nfields * B.count;
     B.lim_off = lim;
-    if (src.type == kD) lim += B.count;
+    lim += lim_count(src.type) * B.count;
     bats.push_back(std::move(B));
   }
   return true;
@@ -562,10 +600,12 @@ int32_t esl_create(const esl_circuit* circuit, const esl_options* opts, esl_ctx*
   ctx->cur.assign(circuit->current_row, circuit->current_row + n);
   if (!read_circuit(circuit, ctx->bats)) return ESL_INVALID_ARGUMENT;
   for (const auto& B : ctx->bats) {
-    if (B.type > kD) return ESL_NOT_ELIGIBLE;
+    if (B.type == kM)
+      for (uint32_t id = 0; id < B.count; ++id)
+        if (B.params[size_t(id) * B.np + kMParamTox] > 0.0) return ESL_NOT_ELIGIBLE;
     ctx->n_stage += B.stride * B.count;
     ctx->rec_size += B.nfields * B.count;
-    if (B.type == kD) ctx->nlim += B.count;
+    ctx->nlim += lim_count(B.type) * B.count;
   }
   const uint32_t rec = ctx->rec_size;
   ctx->pat = build_pattern(ctx->bats, n);
@@ -650,10 +690,18 @@ int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d
   std::vector<double> limit(N, 1e9), lim(size_t(N) * std::max<uint32_t>(ctx->nlim, 1), 0.0);
   if (cold) {
     for (uint32_t l = 0; l < N; ++l)
-      for (const auto& B : ctx->bats)
+      for (const auto& B : ctx->bats) {
+        const double* rec = &ctx->rec_lanes[size_t(l) * ctx->rec_size + B.rec_off];
+        double* li = &lim[size_t(l) * ctx->nlim + B.lim_off];
         if (B.type == kD)
-          for (uint32_t i = 0; i < B.count; ++i)
-            lim[size_t(l) * ctx->nlim + B.lim_off + i] = ctx->rec_lanes[size_t(l) * ctx->rec_size + B.rec_off + kDVcrit * B.count + i];
+          for (uint32_t i = 0; i < B.count; ++i) li[i] = rec[kDVcrit * B.count + i];
+        if (B.type == kM)
+          for (uint32_t i = 0; i < B.count; ++i) {
+            li[3 * i] = rec[kMSeedVgs * B.count + i];
+            li[3 * i + 1] = 0.0;
+            li[3 * i + 2] = -1.0;
+          }
+      }
     ESL_CUDA(cudaMemsetAsync(d_x, 0, size_t(N) * n * 8, s));
   }
   ESL_CUDA(cudaMemcpyAsync(ctx->d_flags.p, flags.data(), N * 4, cudaMemcpyHostToDevice, s));

@@ -182,4 +182,251 @@ __device__ __forceinline__ void diode_stamp(const double* r, int s, double xa, d
   }
 }
 
+// ---------------------------------------------------------------------------
+// MOS1 (models/mos1.va), type frame: v = type * V. Derivatives hand-written
+// in the reference's forward-AD sense; gmbs as ngspice takes it,
+// gm * gamma / (2 sarg) on both branches of the body root (mos1.va:316-323).
+
+// DEVfetlim / DEVlimvds (ngspice devsup.c as the reference documents them,
+// dev/solvers/newton-raphson-convergence.md:58-69).
+__device__ __forceinline__ double fetlim_dev(double vnew, double vold, double vto) {
+  const double vtsthi = fabs(2 * (vold - vto)) + 2;
+  const double vtstlo = fabs(vold - vto) + 1;
+  const double vtox = vto + 3.5;
+  const double delv = vnew - vold;
+  if (vold >= vto) {
+    if (vold >= vtox) {
+      if (delv <= 0) {
+        if (vnew >= vtox) {
+          if (-delv > vtstlo) vnew = vold - vtstlo;
+        } else {
+          vnew = fmax(vnew, vto + 2);
+        }
+      } else if (delv >= vtsthi) {
+        vnew = vold + vtsthi;
+      }
+    } else if (delv <= 0) {
+      vnew = fmax(vnew, vto - 0.5);
+    } else {
+      vnew = fmin(vnew, vto + 4);
+    }
+  } else if (delv <= 0) {
+    if (-delv > vtsthi) vnew = vold - vtsthi;
+  } else {
+    const double vtemp = vto + 0.5;
+    if (vnew <= vtemp) {
+      if (delv > vtstlo) vnew = vold + vtstlo;
+    } else {
+      vnew = vtemp;
+    }
+  }
+  return vnew;
+}
+
+__device__ __forceinline__ double limvds_dev(double vnew, double vold) {
+  if (vold >= 3.5) {
+    if (vnew > vold) vnew = fmin(vnew, 3 * vold + 2);
+    else if (vnew < 3.5) vnew = fmax(vnew, 2.0);
+  } else if (vnew > vold) {
+    vnew = fmin(vnew, 4.0);
+  } else {
+    vnew = fmax(vnew, -0.5);
+  }
+  return vnew;
+}
+
+// jcur (mos1.va:118-129) and its slope.
+__device__ __forceinline__ void mos_jcur(double v, double isat, double vtx, double gm, double& i, double& g) {
+  if (v > -3.0 * vtx) {
+    const double u = fmin(div_rn(v, vtx), 80.0);
+    const double e = exp(u);
+    i = isat * (e * (1.0 + (div_rn(v, vtx) - u)) - 1.0) + gm * v;
+    g = div_rn(isat * e, vtx) + gm;
+  } else {
+    i = gm * v - isat;
+    g = gm;
+  }
+}
+
+// sbody (mos1.va:131-141); ds = -1 / (2 sarg) where sarg > 0.
+__device__ __forceinline__ double mos_sbody(double vbx, double phit, double& ds) {
+  double sv;
+  if (vbx <= 0.0) sv = sqrt(phit - vbx);
+  else sv = fmax(sqrt(phit) - div_rn(vbx, 2.0 * sqrt(phit)), 0.0);
+  ds = sv > 0.0 ? div_rn(-1.0, 2.0 * sv) : 0.0;
+  return sv;
+}
+
+// jchg (mos1.va:143-163) and its capacitance.
+__device__ __forceinline__ void mos_jchg(double v, double cz, double czsw, double pbx, double mjx, double mjswx,
+                                         double fcx, double f2, double f3, double f4, double& q, double& c) {
+  if (cz == 0.0 && czsw == 0.0) {
+    q = 0.0;
+    c = 0.0;
+  } else if (v < fcx * pbx) {
+    const double a = 1.0 - div_rn(v, pbx);
+    q = pbx * (div_rn(cz * (1.0 - pow(a, 1.0 - mjx)), 1.0 - mjx) + div_rn(czsw * (1.0 - pow(a, 1.0 - mjswx)), 1.0 - mjswx));
+    c = cz * pow(a, -mjx) + czsw * pow(a, -mjswx);
+  } else {
+    q = f4 + v * (f2 + 0.5 * f3 * v);
+    c = f2 + f3 * v;
+  }
+}
+
+// MOS1 stamp into its 40 staging cells (layout in common.h). `lim` is the
+// instance's three images (vgs, vds, vbs) when limiting is live; the
+// charges are written for a transient (`dyn`) when the instance has any.
+__device__ __forceinline__ void mos1_stamp(const double* r, int s, double xd, double xg, double xs, double xb,
+                                           double xdi, double xsi, const double* lim, bool dyn, double* st) {
+  const double type = r[kMType * s], vt = r[kMVt * s];
+  const double vgs_r = type * (xg - xsi), vds_r = type * (xdi - xsi), vbs_r = type * (xb - xsi);
+  const double vgs = lim ? lim[0] : vgs_r, vds = lim ? lim[1] : vds_r, vbs = lim ? lim[2] : vbs_r;
+  const double vbd = vbs - vds, vgd = vgs - vds;
+  double ibs, gbs, ibd, gbd;
+  mos_jcur(vbs, r[kMIsats * s], vt, r[kMGmin * s], ibs, gbs);
+  mos_jcur(vbd, r[kMIsatd * s], vt, r[kMGmin * s], ibd, gbd);
+  const double mode = vds >= 0.0 ? 1.0 : -1.0;
+  const double vbx = mode > 0 ? vbs : vbd;
+  const double vgsx = mode > 0 ? vgs : vgd;
+  const double vdsx = mode * vds;
+  double ds;
+  const double gamma = r[kMGamma * s];
+  const double sarg = mos_sbody(vbx, r[kMPhit * s], ds);
+  const double von = r[kMVbit * s] * type + gamma * sarg;
+  const double vgst = vgsx - von;
+  const double beta = r[kMBeta * s], lambda = r[kMLambda * s];
+  const double bp = beta * (1.0 + lambda * vdsx);
+  double id = 0.0, gm = 0.0, gds = 0.0;
+  if (vgst <= 0.0) {
+    id = 0.0;
+  } else if (vgst <= vdsx) {
+    id = 0.5 * bp * vgst * vgst;
+    gm = bp * vgst;
+    gds = 0.5 * beta * lambda * vgst * vgst;
+  } else {
+    id = bp * vdsx * (vgst - 0.5 * vdsx);
+    gm = bp * vdsx;
+    gds = beta * lambda * vdsx * (vgst - 0.5 * vdsx) + bp * (vgst - vdsx);
+  }
+  const double gmbs = gm * (-gamma * ds);
+  double ich, gmg, gdd, gbb;
+  if (mode > 0) {
+    ich = id;
+    gmg = gm;
+    gdd = gds;
+    gbb = gmbs;
+  } else {
+    ich = -id;
+    gmg = -gm;
+    gbb = -gmbs;
+    gdd = gm + gds + gmbs;
+  }
+  const double cgs_ = vgs_r - vgs, cds = vds_r - vds, cbs = vbs_r - vbs;
+  const double cbd = (vbs_r - vds_r) - vbd;
+  if (lim) {
+    if (cgs_ != 0.0 || cds != 0.0 || cbs != 0.0) ich = ich + (gmg * cgs_ + gdd * cds + gbb * cbs);
+    if (cbs != 0.0) ibs = ibs + gbs * cbs;
+    if (cbd != 0.0) ibd = ibd + gbd * cbd;
+  }
+  const double ids = type * ich, tbs = type * ibs, tbd = type * ibd;
+  const double gdr = r[kMGdrain * s], gsr = r[kMGsource * s];
+  const double idr = gdr * (xd - xdi), isr = gsr * (xs - xsi);
+  const double gsum = gmg + gdd + gbb;
+  st[0] = idr;
+  st[1] = isr;
+  st[2] = tbd + tbs;
+  st[3] = (ids - tbd) - idr;
+  st[4] = ((-ids) - tbs) - isr;
+  st[5] = gdr;
+  st[6] = -gdr;
+  st[7] = gsr;
+  st[8] = -gsr;
+  st[9] = gbd + gbs;
+  st[10] = -gbd;
+  st[11] = -gbs;
+  st[12] = -gdr;
+  st[13] = gmg;
+  st[14] = gbb - gbd;
+  st[15] = (gdd + gbd) + gdr;
+  st[16] = -gsum;
+  st[17] = -gmg;
+  st[18] = -gsr;
+  st[19] = (-gbb) - gbs;
+  st[20] = -gdd;
+  st[21] = (gsum + gbs) + gsr;
+  if (dyn && r[kMHasQ * s] != 0.0) {
+    double qbd, cbdc, qbs, cbsc;
+    const double pbt = r[kMPbt * s], mj = r[kMMj * s], mjsw = r[kMMjsw * s], fc = r[kMFc * s];
+    mos_jchg(vbd, r[kMCzbd * s], r[kMCzbdsw * s], pbt, mj, mjsw, fc, r[kMF2d * s], r[kMF3d * s], r[kMF4d * s], qbd, cbdc);
+    mos_jchg(vbs, r[kMCzbs * s], r[kMCzbssw * s], pbt, mj, mjsw, fc, r[kMF2s * s], r[kMF3s * s], r[kMF4s * s], qbs, cbsc);
+    if (lim) {
+      if (cbd != 0.0) qbd = qbd + cbdc * cbd;
+      if (cbs != 0.0) qbs = qbs + cbsc * cbs;
+    }
+    const double cgs = r[kMCgs * s], cgd = r[kMCgd * s], cgb = r[kMCgb * s];
+    const double qgs = cgs * (xg - xsi), qgd = cgd * (xg - xdi), qgb = cgb * (xg - xb);
+    const double tqbd = type * qbd, tqbs = type * qbs;
+    st[22] = (qgs + qgd) + qgb;
+    st[23] = (tqbd + tqbs) - qgb;
+    st[24] = (-tqbd) - qgd;
+    st[25] = (-tqbs) - qgs;
+    st[26] = (cgs + cgd) + cgb;
+    st[27] = -cgb;
+    st[28] = -cgd;
+    st[29] = -cgs;
+    st[30] = -cgb;
+    st[31] = (cbdc + cbsc) + cgb;
+    st[32] = -cbdc;
+    st[33] = -cbsc;
+    st[34] = -cgd;
+    st[35] = -cbdc;
+    st[36] = cbdc + cgd;
+    st[37] = -cgs;
+    st[38] = -cbsc;
+    st[39] = cbsc + cgs;
+  }
+}
+
+// The MOS1 limiting ladder (mos1load.c:361-384) against `old` (images, or
+// x_old's voltages before the first pass), writing the three images; true
+// when pnjlim limited. Images within 16 ulps of the raw value snap to it.
+__device__ __forceinline__ bool mos1_limit(const double* r, int s, double xg, double xb, double xdi, double xsi,
+                                           const double* old, double* img) {
+  const double type = r[kMType * s], vt = r[kMVt * s];
+  const double vgs_n = type * (xg - xsi), vds_n = type * (xdi - xsi), vbs_n = type * (xb - xsi);
+  const double vgd_n = type * (xg - xdi), vbd_n = type * (xb - xdi);
+  const double vgs_o = old[0], vds_o = old[1], vbs_o = old[2];
+  const double vgd_o = vgs_o - vds_o, vbd_o = vbs_o - vds_o;
+  const double vbx = vds_o >= 0.0 ? vbs_o : vbd_o;
+  double ds;
+  const double von = r[kMVbit * s] * type + r[kMGamma * s] * mos_sbody(vbx, r[kMPhit * s], ds);
+  double vgs, vds, vbs;
+  if (vds_o >= 0.0) {
+    vgs = fetlim_dev(vgs_n, vgs_o, von);
+    vds = vgs - vgd_n;
+    vds = limvds_dev(vds, vds_o);
+  } else {
+    const double vgd = fetlim_dev(vgd_n, vgd_o, von);
+    vds = vgs_n - vgd;
+    vds = -limvds_dev(-vds, -vds_o);
+    vgs = vgd + vds;
+  }
+  bool l = false;
+  if (vds >= 0.0) {
+    vbs = pnjlim_dev(vbs_n, vbs_o, vt, r[kMVcrits * s], l);
+  } else {
+    const double vbd = pnjlim_dev(vbd_n, vbd_o, vt, r[kMVcritd * s], l);
+    vbs = vbd + vds;
+  }
+  const double scale = fmax(fmax(fabs(xg), fabs(xb)), fmax(fabs(xdi), fabs(xsi)));
+  const double tol = 16.0 * 2.220446049250313e-16 * scale;
+  if (fabs(vgs - vgs_n) <= tol) vgs = vgs_n;
+  if (fabs(vds - vds_n) <= tol) vds = vds_n;
+  if (fabs(vbs - vbs_n) <= tol) vbs = vbs_n;
+  img[0] = vgs;
+  img[1] = vds;
+  img[2] = vbs;
+  return l;
+}
+
 }  // namespace esl

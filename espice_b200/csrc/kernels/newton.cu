@@ -175,6 +175,10 @@ __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, 
         case kD:
           diode_stamp(r, s, m.x[nd[0]], m.x[nd[1]], m.x[nd[2]], lim_active ? m.lim + B.lim_off + i : nullptr, st);
           break;
+        case kM:
+          mos1_stamp(r, s, m.x[nd[0]], m.x[nd[1]], m.x[nd[2]], m.x[nd[3]], m.x[nd[4]], m.x[nd[5]],
+                     lim_active ? m.lim + B.lim_off + 3 * i : nullptr, sim.kind != 0, st);
+          break;
         default:
           break;
       }
@@ -302,14 +306,34 @@ __device__ __forceinline__ double residual_gate(const LaneOpts& o, double diag, 
   return fmax(o.residual_tol, 10.0 * s * (o.reltol * fabs(xi) + o.vntol));
 }
 
-// pnjlim on every diode against its image (or x_old before the first pass);
-// true when any junction was limited (Circuit.applyLimits).
+// pnjlim on every diode, and the MOS1 ladder on every MOSFET, against their
+// images (or x_old before the first pass); true when any junction was
+// limited (Circuit.applyLimits).
 __device__ bool apply_limits(const TopoDev& T, const double* rec, const LaneMem& m, bool lim_active, int tid) {
   bool limited = false;
   for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
     const BatchDev& B = T.b[bi];
-    if (B.type != kD) continue;
     const int s = static_cast<int>(B.count);
+    if (B.type == kM) {
+      for (uint32_t i = tid; i < B.count; i += 32) {
+        const uint32_t* nd = B.nodes + size_t(i) * B.nt;
+        double* li = m.lim + B.lim_off + 3 * i;
+        double old[3];
+        if (lim_active) {
+          old[0] = li[0];
+          old[1] = li[1];
+          old[2] = li[2];
+        } else {
+          const double type = rec[B.rec_off + kMType * s + i];
+          old[0] = type * (m.xo[nd[1]] - m.xo[nd[5]]);
+          old[1] = type * (m.xo[nd[4]] - m.xo[nd[5]]);
+          old[2] = type * (m.xo[nd[3]] - m.xo[nd[5]]);
+        }
+        limited |= mos1_limit(rec + B.rec_off + i, s, m.x[nd[1]], m.x[nd[3]], m.x[nd[4]], m.x[nd[5]], old, li);
+      }
+      continue;
+    }
+    if (B.type != kD) continue;
     for (uint32_t i = tid; i < B.count; i += 32) {
       const uint32_t* nd = B.nodes + size_t(i) * B.nt;
       const double* r = rec + B.rec_off + i;
@@ -630,7 +654,7 @@ cudaError_t static_scratch(void** ptr) {
 // Start state of every lane (the host-side set-up of esl_dc_solve_device done
 // on the device): iteration 0, running, limit 1e9, INITFIX from the options;
 // a cold lane starts at x = 0 with its junction images at the seeds the
-// records carry (diode vcrit) and limiting live, a warm lane at its x with
+// records carry (diode vcrit; MOSFET vgs, vds = 0, vbs = -1) and limiting live, a warm lane at its x with
 // limiting off. The first thread also clears the paused-lane counter.
 __global__ void lane_init_kernel(TopoDev T, LaneDev L, uint32_t cold, uint32_t init_fix) {
   const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
@@ -648,8 +672,14 @@ __global__ void lane_init_kernel(TopoDev T, LaneDev L, uint32_t cold, uint32_t i
   const double* rec = L.rec + size_t(lane) * T.rec_size;
   for (uint32_t b = 0; b < T.n_batches; ++b) {
     const BatchDev& B = T.b[b];
-    if (B.type != kD) continue;
-    for (uint32_t i = 0; i < B.count; ++i) lim[B.lim_off + i] = rec[B.rec_off + kDVcrit * B.count + i];
+    if (B.type == kD)
+      for (uint32_t i = 0; i < B.count; ++i) lim[B.lim_off + i] = rec[B.rec_off + kDVcrit * B.count + i];
+    if (B.type == kM)
+      for (uint32_t i = 0; i < B.count; ++i) {
+        lim[B.lim_off + 3 * i] = rec[B.rec_off + kMSeedVgs * B.count + i];
+        lim[B.lim_off + 3 * i + 1] = 0.0;
+        lim[B.lim_off + 3 * i + 2] = -1.0;
+      }
   }
 }
 

@@ -34,7 +34,7 @@ int orc_params_per(uint32_t type) {
     return type < ORC_NTYPES ? t[type] : 0;
 }
 
-int dev_nstate(uint32_t type) { return type == ORC_M ? 3 : 0; }
+int dev_nstate(uint32_t type) { (void)type; return 0; }
 
 static void add_ent(layout_t *l, int ru, int cu) {
     l->jac[l->nj].ru = (uint8_t)ru;
@@ -82,6 +82,35 @@ void dev_layout(uint32_t type, const double *prm, layout_t *l) {
         if (prm[ORC_D_CJO] > 0 || prm[ORC_D_TT] > 0) {
             l->q_row[1] = l->q_row[2] = 1;
             add_qent(l, 1, 1); add_qent(l, 1, 2); add_qent(l, 2, 1); add_qent(l, 2, 2);
+        }
+        break;
+    }
+    case ORC_M: { /* d g s b di si */
+        double der[ORC_NDER];
+        mos1_derive(prm, der);
+        int rd = prm[ORC_M_RD] > 0, rs = prm[ORC_M_RS] > 0;
+        l->nlim = 3;
+        if (rd) {
+            l->res_row[0] = 1;
+            add_ent(l, 0, 0); add_ent(l, 0, 4);
+        }
+        if (rs) {
+            l->res_row[2] = 1;
+            add_ent(l, 2, 2); add_ent(l, 2, 5);
+        }
+        l->res_row[3] = l->res_row[4] = l->res_row[5] = 1;
+        add_ent(l, 3, 3); add_ent(l, 3, 4); add_ent(l, 3, 5);
+        if (rd) add_ent(l, 4, 0);
+        add_ent(l, 4, 1); add_ent(l, 4, 3); add_ent(l, 4, 4); add_ent(l, 4, 5);
+        add_ent(l, 5, 1);
+        if (rs) add_ent(l, 5, 2);
+        add_ent(l, 5, 3); add_ent(l, 5, 4); add_ent(l, 5, 5);
+        if (mos1_has_charge(der)) {
+            l->q_row[1] = l->q_row[3] = l->q_row[4] = l->q_row[5] = 1;
+            add_qent(l, 1, 1); add_qent(l, 1, 3); add_qent(l, 1, 4); add_qent(l, 1, 5);
+            add_qent(l, 3, 1); add_qent(l, 3, 3); add_qent(l, 3, 4); add_qent(l, 3, 5);
+            add_qent(l, 4, 1); add_qent(l, 4, 3); add_qent(l, 4, 4);
+            add_qent(l, 5, 1); add_qent(l, 5, 3); add_qent(l, 5, 5);
         }
         break;
     }

@@ -135,6 +135,8 @@ void mos1_eval(const uint32_t *nd, const double *prm, const double *der, const d
 int mos1_limit(const uint32_t *nd, const double *prm, const double *der, const double *x,
                const double *x_old, const double *lim_old, double *lim_new);
 int mos1_seed(const uint32_t *nd, const double *prm, const double *der, const double *x, double *lim);
+int mos1_has_charge(const double *der);
+int orc_mos1_supported(const double *prm);
 
 double pnjlim(double vnew, double vold, double vt, double vcrit, int *lim);
 double fetlim(double vnew, double vold, double vto);

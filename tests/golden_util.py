@@ -45,12 +45,13 @@ def solve_deck(g, dc_sweep, op):
     rows, conv = [], []
     fr = None
     for ov in outer:
-        if ov is not None:
-            if an[5] == "temp":
-                ckt.set_temp(ov)
-            else:
-                raise NotImplementedError("nested source sweep")
+        if ov is not None and an[5] == "temp":
+            ckt.set_temp(ov)
         fr = ckt.freeze()
+        if ov is not None and an[5] != "temp":
+            # nested source sweep: the outer source's bias, in place
+            ob = fr.slot(an[5], "dc")
+            fr.batches[ob.batch][2][ob.inst, ob.param] = ov
         slot = fr.slot(an[1], "dc")
         x, it, cv = dc_sweep(fr, slot, np.array(inner), deck.newton_opts())
         rows.append(x)

@@ -136,7 +136,7 @@ def test_replicas_bitwise_identical():
     assert (itg == itg[0]).all()
 
 
-DC_FIXTURES = [n for n in gu.names("dc__") if "mos" not in n and "temp" not in n]
+DC_FIXTURES = [n for n in gu.names("dc__") if "temp" not in n]
 
 # Points in deep breakdown solved cold and independently: the reference's
 # gates (converger.zig finalizeStep) judge a step assembled at the previous
@@ -157,13 +157,18 @@ def test_golden_fixtures_as_gpu_lanes(name):
     deck = Deck(g["deck"])
     fr = deck.circuit().freeze()
     an = deck.analysis
-    values = np.array(sweep_values(an[2], an[3], an[4])).reshape(-1, 1)
-    slot = fr.slot(an[1], "dc")
+    inner = np.array(sweep_values(an[2], an[3], an[4]))
+    slots = [fr.slot(an[1], "dc")]
+    values = inner.reshape(-1, 1)
+    if len(an) > 5:  # nested source sweep: one lane per (outer, inner) point
+        outer = np.array(sweep_values(an[6], an[7], an[8]))
+        slots.append(fr.slot(an[5], "dc"))
+        values = np.stack([np.tile(inner, len(outer)), np.repeat(outer, len(inner))], axis=1)
     opts = deck.newton_opts()
     ctx = lanes.DcLanes(fr)
-    ctx.set_lanes([slot], values)
+    ctx.set_lanes(slots, values)
     x, it, st, _ = ctx.solve(x0=None, opts=lanes.newton_opts(**opts))
-    xo, ito, cvo = oracle.dc_points(fr, [slot], values, warm=None, opts=oracle.newton_opts(**opts))
+    xo, ito, cvo = oracle.dc_points(fr, slots, values, warm=None, opts=oracle.newton_opts(**opts))
     assert np.array_equal(st == lanes.LANE_CONVERGED, cvo.astype(bool))
     same = it == ito
     assert same.mean() >= 0.95

@@ -15,7 +15,7 @@ def _op(fr, opts):
     return oracle.op(fr, oracle.newton_opts(max_iter=100, **opts))
 
 
-DC_OP = [n for n in gu.names() if "mos" not in n and not n.startswith("tran")]
+DC_OP = [n for n in gu.names() if not n.startswith("tran")]
 
 
 @pytest.mark.parametrize("name", DC_OP)

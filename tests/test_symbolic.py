@@ -45,7 +45,8 @@ def _lead_matrix(frozen):
 
 
 DECKS = ["dc__bench_ensemble_sweep_lanes", "convergence__diode_stack_8",
-         "stress__scaling_resistor_grid_32x32", "convergence__bench_diode_bridge"]
+         "stress__scaling_resistor_grid_32x32", "convergence__bench_diode_bridge",
+         "dc__bench_mosfet_cmos_inverter", "dc__device_mos1_output", "tran__device_mos1_large_signal"]
 
 
 @pytest.mark.parametrize("name", DECKS)
