@@ -141,25 +141,38 @@ int orc_dc_sweep(const orc_circuit *c, orc_slot slot, const double *values,
 int orc_op(const orc_circuit *c, const orc_newton_opts *opts, double *x_out,
            uint32_t *iters);
 
-/* Transient (tran.zig Sim with HostOps; trapezoidal, order promotion,
- * LTE step control, breakpoints): lanes independent, each with its slot
- * values. Records the solution at every accepted step into a probe trace:
- * probe_nodes[n_probes]; out_t / out_v capacity max_pts per lane;
- * n_pts_out per lane; stats per lane: [accepted, rejected_newton,
- * rejected_lte, newton_iters]. x_final [n_lanes][n]. */
+/* Transient (src/analysis/tran/tran.zig Sim.begin/end with HostOps,
+ * integrator.zig): each lane its own operating point (cold start, plain
+ * Newton), then BE-started trapezoidal steps with LTE control on the
+ * devices' charge states, order promotion, Newton rejection (dt / 8) and
+ * PULSE-corner breakpoints. Lanes are independent, each with its slot
+ * values. Records (t, x[probes]) at t = 0 and every accepted step:
+ * out_t [n_lanes][max_pts], out_v [n_lanes][max_pts][n_probes], rows
+ * written per lane in n_pts_out (recording stops at max_pts). stats
+ * [n_lanes][ORC_TS_N]; x_final [n_lanes][n] the last accepted solution. */
 typedef struct {
-    double tstop, tstep, tmax;  /* .tran tstep tstop, max step */
-    double reltol, abstol, vntol, chgtol, trtol;
-    uint32_t itl4;
-    uint32_t method;            /* 1 trap (only) */
+    double tstop, tstep, tmax;  /* .tran tstep tstop; tmax <= 0: min(tstep, tstop / 50) */
+    double reltol, abstol, vntol, chgtol, trtol, dt_min;
     uint32_t max_steps;
 } orc_tran_opts;
 
+enum {
+    ORC_TS_STATUS,      /* 0 reached tstop, 1 dt underflow, 2 OP failed, 3 max_steps */
+    ORC_TS_ACCEPTED,
+    ORC_TS_ATTEMPTS,
+    ORC_TS_NR_ITERS,
+    ORC_TS_REJ_NEWTON,
+    ORC_TS_REJ_LTE,
+    ORC_TS_BP_LANDINGS,
+    ORC_TS_OP_ITERS,
+    ORC_TS_N
+};
+
 int orc_tran(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
              const double *values, uint32_t n_lanes, const orc_tran_opts *topts,
-             const double *x0, const uint32_t *probe_nodes, uint32_t n_probes,
-             uint32_t max_pts, double *out_t, double *out_v, uint32_t *n_pts_out,
-             uint32_t *stats, double *x_final);
+             const uint32_t *probe_nodes, uint32_t n_probes, uint32_t max_pts,
+             double *out_t, double *out_v, uint32_t *n_pts_out, uint32_t *stats,
+             double *x_final);
 
 #ifdef __cplusplus
 }

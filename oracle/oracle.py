@@ -168,3 +168,43 @@ def op(frozen, opts=None):
     rc = lib().orc_op(ctypes.byref(frozen.struct()), ctypes.byref(opts), _p(x, f64p),
                       ctypes.byref(it))
     return x, int(it.value), rc
+
+
+class TranOpts(ctypes.Structure):
+    _fields_ = [("tstop", ctypes.c_double), ("tstep", ctypes.c_double), ("tmax", ctypes.c_double),
+                ("reltol", ctypes.c_double), ("abstol", ctypes.c_double), ("vntol", ctypes.c_double),
+                ("chgtol", ctypes.c_double), ("trtol", ctypes.c_double), ("dt_min", ctypes.c_double),
+                ("max_steps", ctypes.c_uint32)]
+
+
+def tran_opts(tstop, tstep, tmax=0.0, reltol=1e-3, abstol=1e-12, vntol=1e-6, chgtol=1e-14,
+              trtol=7.0, dt_min=1e-18, max_steps=1_000_000_000):
+    return TranOpts(tstop, tstep, tmax, reltol, abstol, vntol, chgtol, trtol, dt_min, max_steps)
+
+
+TS_FIELDS = ["status", "accepted", "attempts", "nr_iters", "rej_newton", "rej_lte", "bp_landings",
+             "op_iters"]
+
+
+def tran(frozen, slots, values, opts, probes=(), max_pts=0):
+    """Independent transient lanes (tran.zig Sim): returns (t [lanes][max_pts],
+    v [lanes][max_pts][n_probes], n_pts [lanes], stats [lanes][8] in
+    TS_FIELDS order, x_final [lanes][n])."""
+    values = np.ascontiguousarray(values, np.float64).reshape(-1, max(1, len(slots)))
+    lanes = values.shape[0]
+    probes = np.ascontiguousarray(probes, np.uint32)
+    npr = len(probes)
+    t = np.zeros((lanes, max(max_pts, 1)))
+    v = np.zeros((lanes, max(max_pts, 1), max(npr, 1)))
+    npts = np.zeros(lanes, np.uint32)
+    stats = np.zeros((lanes, len(TS_FIELDS)), np.uint32)
+    xf = np.zeros((lanes, frozen.n))
+    sa = frozen.slots_array(slots)
+    rec = max_pts > 0
+    rc = lib().orc_tran(ctypes.byref(frozen.struct()), sa, ctypes.c_uint32(len(slots)),
+                        _p(values, f64p), ctypes.c_uint32(lanes), ctypes.byref(opts),
+                        _p(probes, u32p) if npr else None, ctypes.c_uint32(npr),
+                        ctypes.c_uint32(max_pts), _p(t, f64p) if rec else None,
+                        _p(v, f64p) if rec else None, _p(npts, u32p), _p(stats, u32p), _p(xf, f64p))
+    assert rc == 0
+    return t, v, npts, stats, xf

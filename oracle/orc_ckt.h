@@ -28,6 +28,13 @@ typedef struct {
     double last_scaled;
     sim_t sim;
     dsv_t dsv;
+    /* transient companion hook (integrator.zig Hook): when `tran`, the
+     * residual gains ag0*(q - q1) (- ag1*ip for trap) and the matrix is
+     * G + ag0*C in av */
+    int tran, trap;
+    double ag0, ag1;
+    const double *q1, *ip;
+    double *av;
 } ckt_t;
 
 int ckt_init(ckt_t *k, const orc_circuit *c);
@@ -38,6 +45,7 @@ int ckt_apply_limits(ckt_t *k, const double *x, const double *x_old);
 void ckt_seed(ckt_t *k, double *x);
 void ckt_cold_start(ckt_t *k, double *x);
 int ckt_newton(ckt_t *k, double *x, const orc_newton_opts *opts, int init_fix, uint32_t *iters);
+uint32_t ckt_qtape(ckt_t *k, const double *x, double *out);
 int ckt_run(ckt_t *k, double *x, const orc_newton_opts *opts, int init_fix, uint32_t *iters);
 double update_and_norm(uint32_t n, double *x, const double *dx, double *x_old, const uint8_t *cur,
                        double reltol, double abstol, double vntol);

@@ -435,6 +435,24 @@ void dev_eval(uint32_t type, const uint32_t *nd, const double *prm, const double
     }
 }
 
+int dev_qtape(uint32_t type, const uint32_t *nd, const double *prm, const double *der,
+              const double *x, double *out) {
+    if (type == ORC_C) {
+        out[0] = prm[0] * (x[nd[0]] - x[nd[1]]);
+        return 1;
+    }
+    if (type == ORC_D && (prm[ORC_D_CJO] > 0 || prm[ORC_D_TT] > 0)) {
+        double i, g, qj, cj;
+        double vd = x[nd[2]] - x[nd[1]];
+        diode_iv(der, vd, &i, &g);
+        diode_qc(der, vd, i, g, &qj, &cj);
+        out[0] = qj;
+        return 1;
+    }
+    if (type == ORC_M) return mos1_qtape(nd, der, x, out);
+    return 0;
+}
+
 int dev_limit(uint32_t type, const uint32_t *nd, const double *prm, const double *der,
               const double *x, const double *x_old, const double *lim_old, double *lim_new) {
     if (type == ORC_D) {

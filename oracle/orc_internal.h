@@ -124,6 +124,11 @@ int dev_limit(uint32_t type, const uint32_t *nd, const double *prm, const double
 int dev_seed(uint32_t type, const uint32_t *nd, const double *prm, const double *der,
              const double *x, double *lim);
 int dev_nstate(uint32_t type);
+/* The instance's charge states that join the LTE (one per ddt() site the
+ * model keeps in the truncation-error test), at raw x; returns the count. */
+int dev_qtape(uint32_t type, const uint32_t *nd, const double *prm, const double *der,
+              const double *x, double *out);
+int mos1_qtape(const uint32_t *nd, const double *der, const double *x, double *out);
 /* Stage accepted-step state ($prev latches) from x; `static_` at an OP. */
 void dev_stage(uint32_t type, const uint32_t *nd, const double *prm, const double *der,
                const double *x, const double *lim, const sim_t *sim, double *staged);

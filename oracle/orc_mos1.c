@@ -316,6 +316,17 @@ int mos1_limit(const uint32_t *nd, const double *prm, const double *der, const d
     return l;
 }
 
+/* Meyer (overlap) gate charges, the sites mos1trun.c truncates: qgs, qgd,
+ * qgb, each kept when its capacitance is nonzero. */
+int mos1_qtape(const uint32_t *nd, const double *der, const double *x, double *out) {
+    int k = 0;
+    const double xg = x[nd[1]];
+    if (der[MD_CGS] != 0.0) out[k++] = der[MD_CGS] * (xg - x[nd[5]]);
+    if (der[MD_CGD] != 0.0) out[k++] = der[MD_CGD] * (xg - x[nd[4]]);
+    if (der[MD_CGB] != 0.0) out[k++] = der[MD_CGB] * (xg - x[nd[3]]);
+    return k;
+}
+
 /* MODEINITJCT (mos1load.c:397-407): vgs = type * tVto, vds = 0, vbs = -1. */
 int mos1_seed(const uint32_t *nd, const double *prm, const double *der, const double *x, double *lim) {
     (void)nd; (void)prm; (void)x;

@@ -81,6 +81,7 @@ int ckt_init(ckt_t *k, const orc_circuit *c) {
     k->q = (double *)calloc(n + 1, sizeof(double));
     k->dx = (double *)calloc(n + 1, sizeof(double));
     k->x_old = (double *)calloc(n + 1, sizeof(double));
+    k->av = (double *)calloc(k->nnz + 1, sizeof(double));
     k->sim.kind = 0;
     k->sim.src_scale = 1.0;
     k->sim.iteration = 1;
@@ -98,7 +99,7 @@ void ckt_free(ckt_t *k) {
     }
     free(k->bt);
     free(k->cp); free(k->ri); free(k->diag); free(k->lim); free(k->lim_new); free(k->st);
-    free(k->g); free(k->cv); free(k->rhs); free(k->q); free(k->dx); free(k->x_old);
+    free(k->g); free(k->cv); free(k->rhs); free(k->q); free(k->dx); free(k->x_old); free(k->av);
     dsv_free(&k->dsv);
     memset(k, 0, sizeof(*k));
 }
@@ -246,6 +247,16 @@ int ckt_newton(ckt_t *k, double *x, const orc_newton_opts *opts, int init_fix, u
         if (iter != 0) k->sim.iteration++;
         ckt_assemble(k, x);
         double *v = k->g;
+        if (k->tran) {
+            /* integrator.zig companionAt(accumulate) and Circuit.combineGC */
+            for (uint32_t j = 0; j < n; j++) {
+                double d = k->ag0 * (k->q[j] - k->q1[j]);
+                double base = k->rhs[j] + d;
+                k->rhs[j] = k->trap ? base - k->ag1 * k->ip[j] : base;
+            }
+            for (uint32_t s = 0; s < k->nnz; s++) k->av[s] = k->g[s] + k->ag0 * k->cv[s];
+            v = k->av;
+        }
         if (opts->gmin > 0) {
             for (uint32_t i = 0; i < n; i++) v[k->diag[i]] += opts->gmin;
             for (uint32_t i = 0; i < n; i++) k->rhs[i] += opts->gmin * x[i];
@@ -290,6 +301,24 @@ int ckt_newton(ckt_t *k, double *x, const orc_newton_opts *opts, int init_fix, u
     }
     *iters = max_iter;
     return 1;
+}
+
+/* The charge states of every instance at raw x, in batch/instance order. */
+uint32_t ckt_qtape(ckt_t *k, const double *x, double *out) {
+    uint32_t m = 0;
+    for (uint32_t b = 0; b < k->nb; b++) {
+        bat_t *bt = &k->bt[b];
+        for (uint32_t id = 0; id < bt->count; id++) {
+            const uint32_t *nd = bt->nodes + (size_t)id * bt->nt;
+            double tmp[4];
+            int c = dev_qtape(bt->type, nd, bt->prm + (size_t)id * bt->np, bt->der + (size_t)id * ORC_NDER, x, tmp);
+            for (int i = 0; i < c; i++) {
+                if (out) out[m] = tmp[i];
+                m++;
+            }
+        }
+    }
+    return m;
 }
 
 /* converger.run: newton, then clearLimits. */

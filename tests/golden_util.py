@@ -72,3 +72,33 @@ def score(g, fr, rows):
             err = np.abs(got - exp)
             out.append((col, float(np.max(err / allowed)), len(exp)))
     return out
+
+
+def solve_tran(g, max_pts=1_000_000):
+    """Runs a .tran fixture through the oracle: (frozen, t, v [pts][cols],
+    columns, stats dict)."""
+    from oracle import oracle
+    deck = Deck(g["deck"])
+    fr = deck.circuit().freeze()
+    _, tstep, tstop = deck.analysis[:3]
+    cols = list(g["plots"][0]["columns"])
+    probes = [fr.unknown(c) for c in cols]
+    o = oracle.tran_opts(tstop, tstep, **deck.newton_opts())
+    t, v, npts, stats, _ = oracle.tran(fr, [], np.zeros((1, 1)), o, probes, max_pts=max_pts)
+    n = int(npts[0])
+    return fr, t[0, :n], v[0, :n], cols, dict(zip(oracle.TS_FIELDS, stats[0].tolist()))
+
+
+def score_tran(g, t, v, cols):
+    """(column, worst err/allowed) with the waveform interpolated at the
+    fixture's sample times."""
+    plot = g["plots"][0]
+    at = np.array(plot["axis"]["values"])
+    out = []
+    for k, col in enumerate(cols):
+        spec = plot["columns"][col]
+        exp = np.array(spec["values"], dtype=float)
+        got = np.interp(at, t, v[:, k])
+        allowed = spec["atol"] + spec["rtol"] * np.abs(exp)
+        out.append((col, float(np.max(np.abs(got - exp) / allowed))))
+    return out

@@ -116,6 +116,16 @@ class Deck:
                     if pulse is not None and not m.group(0).lower().startswith("dc"):
                         if not (toks and toks[0].lower() == "dc"):
                             dc = pulse[0]
+                    if pulse is not None and self.analysis and self.analysis[0] == "tran":
+                        # PULSE defaults from the .tran card (ngspice TRANinit, the
+                        # reference's resolvePulseDefaults): TR = TF = TSTEP,
+                        # PW = PER = TSTOP
+                        tstep, tstop = self.analysis[1], self.analysis[2]
+                        full = list(pulse) + [None] * (7 - len(pulse))
+                        for k, dflt in ((3, tstep), (4, tstep), (5, tstop), (6, tstop)):
+                            if full[k] is None:
+                                full[k] = dflt
+                        pulse = [0.0 if v is None else v for v in full]
                     c.V(name, t[1], t[2], dc=dc, pulse=pulse)
                 else:
                     c.I(name, t[1], t[2], dc=dc)

@@ -25,3 +25,18 @@ def test_oracle_matches_golden(name):
     assert conv.all(), f"{name}: {int((~conv.astype(bool)).sum())} points did not converge"
     for col, worst, count in gu.score(g, fr, rows):
         assert worst <= 1.0, f"{name} {col}: error {worst:.3g}x the allowed tolerance"
+
+
+TRAN = gu.names("tran__")
+
+
+@pytest.mark.parametrize("name", TRAN)
+def test_oracle_transient_matches_golden(name):
+    """The transient restatement against the reference's ngspice-44.2
+    waveform: the oracle's accepted points, linearly interpolated at the
+    fixture's sample times, within each column's tolerance."""
+    g = gu.load(name)
+    fr, t, v, cols, st = gu.solve_tran(g)
+    assert st["status"] == 0, st
+    for col, worst in gu.score_tran(g, t, v, cols):
+        assert worst <= 1.0, f"{name} {col}: error {worst:.3g}x the allowed tolerance"
