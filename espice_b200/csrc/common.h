@@ -63,6 +63,24 @@ enum OpKind : uint32_t {
   kOpNop = 7,
 };
 
+// Per-lane transient statistics (the same fields, in the same order, as the
+// oracle's step counters), and the run's status word.
+enum TranStat : uint32_t {
+  kTsStatus, kTsAccepted, kTsAttempts, kTsNrIters, kTsRejNewton, kTsRejLte, kTsBpLandings, kTsOpIters,
+  kTsN
+};
+enum TranStatus : uint32_t {
+  kTranDone = 0,       // reached t_stop
+  kTranUnderflow = 1,  // dt fell below dt_min
+  kTranOpFailed = 2,   // the operating point did not converge
+  kTranMaxSteps = 3,
+  kTranLeftTape = 4,   // a factor left the lead pivot tape (needs a host factor)
+};
+
+// LTE charge states per instance: one per ddt() site kept in the
+// truncation-error test (capacitor; diode junction; MOS1 qgs, qgd, qgb).
+constexpr uint32_t qt_count(uint32_t type) { return type == kC ? 1u : type == kD ? 1u : type == kM ? 3u : 0u; }
+
 struct LaneOpts {
   double reltol, abstol, vntol, residual_tol, gmin;
   uint32_t max_iter;

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <string>
 #include <unordered_map>
@@ -52,6 +53,7 @@ struct DevBuf {
 struct HostBatch {
   uint32_t type = 0, count = 0, nt = 0, np = 0;
   uint32_t stage_base = 0, stride = 0, rec_off = 0, nfields = 0, lim_off = 0;
+  uint32_t qt_off = 0, qt_sites = 0;
   std::vector<uint32_t> nodes;
   std::vector<double> params;
 };
@@ -176,6 +178,7 @@ struct esl_ctx {
   std::string err;
   uint32_t lanes_per_block = 4;
   uint32_t lanes_eff = 4;  // lanes per CTA that fit beside the staged programs
+  uint32_t tran_lanes_eff = 0;  // the same for the transient kernel (0: does not fit)
 
   Csc pat;
   std::vector<uint8_t> cur;
@@ -183,6 +186,8 @@ struct esl_ctx {
   std::vector<HostBatch> bats;
   uint32_t n_stage = 0, rec_size = 0, nlim = 0;
   std::vector<uint32_t> rhs_ptr, rhs_src, a_ptr, a_src, slot_row;
+  std::vector<uint32_t> q_ptr, q_src, c_ptr, c_src;  // transient charge rows, capacitance slots
+  uint32_t n_qt = 0;
   std::vector<double> rec_nominal;
 
   uint32_t n_lanes = 0;
@@ -193,6 +198,7 @@ struct esl_ctx {
   Programs prog;
 
   DevBuf d_nodes[kMaxBatches], d_rhs_ptr, d_rhs_src, d_a_ptr, d_a_src, d_slot_row, d_cur;
+  DevBuf d_q_ptr, d_q_src, d_c_ptr, d_c_src, d_probes, d_tran_t, d_tran_v, d_tran_n, d_tran_stats;
   DevBuf d_amap, d_fill, d_prog, d_l_scaled, d_pinv, d_q;
   DevBuf d_rec, d_lim, d_lim_active, d_status, d_iters, d_flags, d_limit, d_a_vals, d_rhs, d_dx,
       d_diag, d_paused, d_x;
@@ -278,7 +284,7 @@ bool read_circuit(const esl_circuit* c, std::vector<HostBatch>& bats) {
 // in stamp order, then the ground pin on row 0 and slot (0, 0).
 void build_gather(esl_ctx* ctx) {
   const uint32_t n = ctx->pat.n, nnz = ctx->pat.nnz();
-  std::vector<std::vector<uint32_t>> rows(n), slots(nnz);
+  std::vector<std::vector<uint32_t>> rows(n), slots(nnz), qrows(n), cslots(nnz);
   for (const auto& B : ctx->bats)
     for (uint32_t id = 0; id < B.count; ++id) {
       const uint32_t* nd = &B.nodes[size_t(id) * B.nt];
@@ -289,6 +295,12 @@ void build_gather(esl_ctx* ctx) {
       for (const Entry& e : L.jac) {
         const uint32_t s = ctx->pat.slot(nd[e.ru], nd[e.cu]);
         if (s != nnz) slots[s].push_back(base + e.pos);
+      }
+      for (const Entry& e : L.q)
+        if (nd[e.ru] != 0) qrows[nd[e.ru]].push_back(base + e.pos);
+      for (const Entry& e : L.qjac) {
+        const uint32_t s = ctx->pat.slot(nd[e.ru], nd[e.cu]);
+        if (s != nnz) cslots[s].push_back(base + e.pos);
       }
     }
   rows[0].push_back(kSrcX0);
@@ -304,6 +316,8 @@ void build_gather(esl_ctx* ctx) {
   };
   flatten(rows, ctx->rhs_ptr, ctx->rhs_src);
   flatten(slots, ctx->a_ptr, ctx->a_src);
+  flatten(qrows, ctx->q_ptr, ctx->q_src);
+  flatten(cslots, ctx->c_ptr, ctx->c_src);
   ctx->slot_row.assign(nnz, kNoDiag);
   for (uint32_t i = 0; i < n; ++i) {
     const uint32_t s = i == 0 ? ctx->pat.col_ptr[0] : ctx->pat.slot(i, i);
@@ -324,8 +338,17 @@ int32_t upload_topology(esl_ctx* ctx) {
     const HostBatch& B = ctx->bats[b];
     ESL_CUDA(upload(ctx->d_nodes[b], B.nodes, s));
     T.b[b] = BatchDev{B.type, B.count, B.nt, B.stage_base, B.stride, B.rec_off, B.lim_off,
-                      ctx->d_nodes[b].as<uint32_t>()};
+                      ctx->d_nodes[b].as<uint32_t>(), B.qt_off, B.qt_sites};
   }
+  ESL_CUDA(upload(ctx->d_q_ptr, ctx->q_ptr, s));
+  ESL_CUDA(upload(ctx->d_q_src, ctx->q_src, s));
+  ESL_CUDA(upload(ctx->d_c_ptr, ctx->c_ptr, s));
+  ESL_CUDA(upload(ctx->d_c_src, ctx->c_src, s));
+  T.q_ptr = ctx->d_q_ptr.as<uint32_t>();
+  T.q_src = ctx->d_q_src.as<uint32_t>();
+  T.c_ptr = ctx->d_c_ptr.as<uint32_t>();
+  T.c_src = ctx->d_c_src.as<uint32_t>();
+  T.n_qt = ctx->n_qt;
   ESL_CUDA(upload(ctx->d_rhs_ptr, ctx->rhs_ptr, s));
   ESL_CUDA(upload(ctx->d_rhs_src, ctx->rhs_src, s));
   ESL_CUDA(upload(ctx->d_a_ptr, ctx->a_ptr, s));
@@ -481,6 +504,15 @@ int32_t upload_tape(esl_ctx* ctx) {
   if (T.prog_bytes + lane_bytes > room)
     return ctx->fail(ESL_NOT_ELIGIBLE, "programs and one lane exceed a CTA's shared memory");
   ctx->lanes_eff = std::max<uint32_t>(1, std::min<uint32_t>(ctx->lanes_per_block, uint32_t((room - T.prog_bytes) / lane_bytes)));
+  // Transient lanes add the accepted points, the charge rings and dynamic
+  // currents over the rows and the LTE states: cur | prev | q[4] | ip over
+  // n, then q[4] | ip over n_qt.
+  T.tran_doubles = (T.smem_doubles + 7 * T.n + 5 * T.n_qt + 1) & ~1u;
+  const size_t tran_bytes = size_t(T.tran_doubles) * 8;
+  ctx->tran_lanes_eff = T.prog_bytes + tran_bytes > room
+                            ? 0
+                            : std::max<uint32_t>(1, std::min<uint32_t>(ctx->lanes_per_block,
+                                                                       uint32_t((room - T.prog_bytes) / tran_bytes)));
   ctx->have_tape = true;
   return ESL_OK;
 }
@@ -606,6 +638,20 @@ int32_t esl_create(const esl_circuit* circuit, const esl_options* opts, esl_ctx*
     ctx->n_stage += B.stride * B.count;
     ctx->rec_size += B.nfields * B.count;
     ctx->nlim += lim_count(B.type) * B.count;
+  }
+  // LTE charge states: a batch keeps its sites when any instance has the
+  // charge (capacitors always; diodes with CJO or TT; MOSFETs with overlap
+  // capacitance).
+  for (auto& B : ctx->bats) {
+    bool any = B.type == kC;
+    for (uint32_t id = 0; id < B.count && !any; ++id) {
+      const double* p = &B.params[size_t(id) * B.np];
+      if (B.type == kD) any = p[5] > 0 || p[9] > 0;
+      if (B.type == kM) any = p[12] != 0 || p[13] != 0 || p[14] != 0;
+    }
+    B.qt_sites = any ? qt_count(B.type) : 0;
+    B.qt_off = ctx->n_qt;
+    ctx->n_qt += B.qt_sites * B.count;
   }
   const uint32_t rec = ctx->rec_size;
   ctx->pat = build_pattern(ctx->bats, n);
@@ -829,6 +875,120 @@ int32_t esl_dc_solve_device_static(esl_ctx* ctx, const esl_newton_opts* opts, do
                   paused);
     return fail(ESL_NOT_ELIGIBLE, msg);
   }
+  return ESL_OK;
+}
+
+namespace {
+
+// The lead tape from lane 0's cold-start Jacobian (x = 0, junction seeds),
+// as the first DC solve builds it.
+int32_t ensure_tape_cold(esl_ctx* ctx) {
+  if (ctx->have_tape) return ESL_OK;
+  cudaStream_t s = ctx->stream;
+  const uint32_t n = ctx->pat.n;
+  std::vector<double> lim(std::max<uint32_t>(ctx->nlim, 1), 0.0);
+  for (const auto& B : ctx->bats) {
+    const double* rec = &ctx->rec_lanes[B.rec_off];
+    if (B.type == kD)
+      for (uint32_t i = 0; i < B.count; ++i) lim[B.lim_off + i] = rec[kDVcrit * B.count + i];
+    if (B.type == kM)
+      for (uint32_t i = 0; i < B.count; ++i) {
+        lim[B.lim_off + 3 * i] = rec[kMSeedVgs * B.count + i];
+        lim[B.lim_off + 3 * i + 1] = 0.0;
+        lim[B.lim_off + 3 * i + 2] = -1.0;
+      }
+  }
+  const uint32_t act = ctx->nlim ? 1u : 0u;
+  ESL_CUDA(cudaMemsetAsync(ctx->d_x.p, 0, size_t(n) * 8, s));
+  ESL_CUDA(cudaMemcpyAsync(ctx->d_lim.p, lim.data(), lim.size() * 8, cudaMemcpyHostToDevice, s));
+  ESL_CUDA(cudaMemcpyAsync(ctx->d_lim_active.p, &act, 4, cudaMemcpyHostToDevice, s));
+  LaneDev L = lane_view(ctx, 0);
+  ESL_CUDA(launch_assemble(ctx->topo, L, 0, ctx->d_a_vals.as<double>(), s));
+  std::vector<double> a0(ctx->pat.nnz());
+  ESL_CUDA(cudaMemcpyAsync(a0.data(), ctx->d_a_vals.p, a0.size() * 8, cudaMemcpyDeviceToHost, s));
+  ESL_CUDA(cudaStreamSynchronize(s));
+  return build_tape_from(ctx, a0.data());
+}
+
+int32_t tran_view(esl_ctx* ctx, const esl_tran_opts* o, TranDev& P, LaneOpts& lo) {
+  if (!o || !(o->t_stop > 0) || !(o->t_step > 0)) return ctx->fail(ESL_INVALID_ARGUMENT, "t_stop and t_step must be positive");
+  P = TranDev{};
+  P.t_stop = o->t_stop;
+  P.t_step = o->t_step;
+  // src/frontend/analyses.zig:534: DELMAX, else min(TSTEP, span / 50)
+  P.dt_max = o->t_max > 0 ? o->t_max : std::min(o->t_step, o->t_stop / 50.0);
+  P.dt_min = o->dt_min > 0 ? o->dt_min : 1e-18;
+  P.reltol = o->reltol;
+  P.abstol = o->abstol;
+  P.vntol = o->vntol;
+  P.chgtol = o->chgtol;
+  P.trtol = o->trtol;
+  P.max_steps = o->max_steps ? o->max_steps : 1000000000u;
+  lo = LaneOpts{o->reltol, o->abstol, o->vntol, std::numeric_limits<double>::infinity(), 0.0, 100, 0};
+  return ESL_OK;
+}
+
+}  // namespace
+
+int32_t esl_tran_device(esl_ctx* ctx, const esl_tran_opts* opts, double* d_x, uint32_t* d_stats,
+                        const uint32_t* d_probes, uint32_t n_probes, uint32_t max_pts, double* d_t,
+                        double* d_v, uint32_t* d_n_pts, float* ms) {
+  if (!ctx || !d_x || !d_stats || ctx->n_lanes == 0) return ESL_INVALID_ARGUMENT;
+  if (max_pts && (!d_probes || !d_t || !d_v || !d_n_pts)) return ESL_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  TranDev P;
+  LaneOpts lo;
+  if (int32_t rc = tran_view(ctx, opts, P, lo)) return rc;
+  if (int32_t rc = ensure_tape_cold(ctx)) return rc;
+  if (ctx->tran_lanes_eff == 0) return ctx->fail(ESL_NOT_ELIGIBLE, "a transient lane exceeds a CTA's shared memory");
+  P.stats = d_stats;
+  P.n_probes = max_pts ? n_probes : 0;
+  P.max_pts = max_pts;
+  P.probes = d_probes;
+  P.out_t = max_pts ? d_t : nullptr;
+  P.out_v = d_v;
+  P.n_pts = max_pts ? d_n_pts : nullptr;
+  LaneDev L = lane_view(ctx, 0);
+  L.x = d_x;
+  cudaStream_t s = ctx->stream;
+  ESL_CUDA(cudaEventRecord(ctx->ev0, s));
+  ESL_CUDA(launch_tran(ctx->topo, L, P, lo, ctx->tran_lanes_eff, s));
+  ESL_CUDA(cudaEventRecord(ctx->ev1, s));
+  ESL_CUDA(cudaEventSynchronize(ctx->ev1));
+  if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
+  return ESL_OK;
+}
+
+int32_t esl_tran(esl_ctx* ctx, const esl_tran_opts* opts, const uint32_t* probes, uint32_t n_probes,
+                 uint32_t max_pts, double* t_out, double* v_out, uint32_t* n_pts, uint32_t* stats,
+                 double* x_out, float* ms) {
+  if (!ctx || !stats || !x_out || ctx->n_lanes == 0) return ESL_INVALID_ARGUMENT;
+  if (max_pts && (!probes || !t_out || !v_out || !n_pts || n_probes == 0)) return ESL_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const size_t N = ctx->n_lanes, n = ctx->pat.n;
+  for (uint32_t k = 0; k < n_probes && max_pts; ++k)
+    if (probes[k] >= n) return ctx->fail(ESL_INVALID_ARGUMENT, "probe index out of range");
+  ESL_CUDA(ctx->d_tran_stats.ensure(N * kTsN * 4));
+  if (max_pts) {
+    ESL_CUDA(ctx->d_probes.ensure(size_t(n_probes) * 4));
+    ESL_CUDA(ctx->d_tran_t.ensure(N * max_pts * 8));
+    ESL_CUDA(ctx->d_tran_v.ensure(N * max_pts * n_probes * 8));
+    ESL_CUDA(ctx->d_tran_n.ensure(N * 4));
+    ESL_CUDA(cudaMemcpyAsync(ctx->d_probes.p, probes, size_t(n_probes) * 4, cudaMemcpyHostToDevice, s));
+  }
+  if (int32_t rc = esl_tran_device(ctx, opts, ctx->d_x.as<double>(), ctx->d_tran_stats.as<uint32_t>(),
+                                   ctx->d_probes.as<uint32_t>(), n_probes, max_pts, ctx->d_tran_t.as<double>(),
+                                   ctx->d_tran_v.as<double>(), ctx->d_tran_n.as<uint32_t>(), ms))
+    return rc;
+  ESL_CUDA(cudaMemcpyAsync(x_out, ctx->d_x.p, N * n * 8, cudaMemcpyDeviceToHost, s));
+  ESL_CUDA(cudaMemcpyAsync(stats, ctx->d_tran_stats.p, N * kTsN * 4, cudaMemcpyDeviceToHost, s));
+  if (max_pts) {
+    ESL_CUDA(cudaMemcpyAsync(t_out, ctx->d_tran_t.p, N * max_pts * 8, cudaMemcpyDeviceToHost, s));
+    ESL_CUDA(cudaMemcpyAsync(v_out, ctx->d_tran_v.p, N * max_pts * n_probes * 8, cudaMemcpyDeviceToHost, s));
+    ESL_CUDA(cudaMemcpyAsync(n_pts, ctx->d_tran_n.p, N * 4, cudaMemcpyDeviceToHost, s));
+  }
+  ESL_CUDA(cudaStreamSynchronize(s));
   return ESL_OK;
 }
 

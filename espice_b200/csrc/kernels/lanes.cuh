@@ -17,8 +17,9 @@ struct BatchDev {
   uint32_t type, count, nt;     // device type, instances, unknowns per instance
   uint32_t stage_base, stride;  // staging cells: stage_base + inst * stride
   uint32_t rec_off;             // record block offset (fields x count, field-major)
-  uint32_t lim_off;             // limited images: lim_off + inst
+  uint32_t lim_off;             // limited images: lim_off + lim_count(type) * inst
   const uint32_t* nodes;        // count * nt unknown indices
+  uint32_t qt_off, qt_sites;    // LTE charge states: qt_off + inst * qt_sites + k
 };
 
 struct TopoDev {
@@ -59,6 +60,29 @@ struct TopoDev {
   const uint32_t* qcol;
   const uint8_t* cur_row;
   uint32_t smem_doubles;  // per lane
+  // Transient planes: row i's charge sums q_src[q_ptr[i] ..), slot p's
+  // capacitance sums c_src[c_ptr[p] ..) (staging cells, stamp order); the
+  // LTE charge states number n_qt.
+  const uint32_t* q_ptr;
+  const uint32_t* q_src;
+  const uint32_t* c_ptr;
+  const uint32_t* c_src;
+  uint32_t n_qt;
+  uint32_t tran_doubles;  // per lane, transient kernel
+};
+
+// One transient over every lane (tran.zig Sim): options, the probe trace
+// and the per-lane step statistics.
+struct TranDev {
+  double t_stop, t_step, dt_max, dt_min;
+  double reltol, abstol, vntol, chgtol, trtol;
+  uint32_t max_steps;
+  uint32_t n_probes, max_pts;
+  const uint32_t* probes;  // [n_probes] unknowns recorded
+  double* out_t;           // [lane][max_pts] accepted times (null: no trace)
+  double* out_v;           // [lane][max_pts][n_probes]
+  uint32_t* n_pts;         // [lane] rows recorded
+  uint32_t* stats;         // [lane][kTsN]
 };
 
 struct LaneDev {

@@ -689,4 +689,527 @@ cudaError_t launch_lane_init(const TopoDev& T, const LaneDev& L, bool cold, bool
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Transient lanes (src/analysis/tran/tran.zig Sim.begin / Sim.end with the
+// integrator.zig kernels): one warp runs one lane's whole transient, its
+// operating point included, without returning to the host between steps.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr double kLteBe = 0.5;            // integrator.lteCoeff, gearCoeff[0]
+constexpr double kLteTrap = 0.08333333333;  // trapCoeff[1]
+
+__device__ __forceinline__ double warp_fmin(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = v + __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+// One companion step's terms (integrator.zig Hook): rhs += ag0 * (q - q1)
+// (- ag1 * ip for trap), matrix G + ag0 * C.
+struct Companion {
+  double ag0, ag1;
+  bool trap;
+  const double* q1;  // n: accepted row charges
+  const double* ip;  // n: accepted dynamic currents
+};
+
+// Row charge sums and capacitance slot sums from the staging cells, in
+// stamp order; the companion folded into rhs, y and the tape values.
+__device__ void companion(const TopoDev& T, const LaneMem& m, const Companion& c, int tid) {
+  for (uint32_t i = tid; i < T.n; i += 32) {
+    double q = 0.0;
+    for (uint32_t e = T.q_ptr[i]; e < T.q_ptr[i + 1]; ++e) q = __dadd_rn(q, m.st[T.q_src[e]]);
+    const double d = c.ag0 * (q - c.q1[i]);
+    const double base = m.rhs[i] + d;
+    const double r = c.trap ? base - c.ag1 * c.ip[i] : base;
+    m.rhs[i] = r;
+    m.y[T.pinv[i]] = -r;
+  }
+  for (uint32_t p = tid; p < T.nnz; p += 32) {
+    double cs = 0.0;
+    for (uint32_t e = T.c_ptr[p]; e < T.c_ptr[p + 1]; ++e) cs = __dadd_rn(cs, m.st[T.c_src[e]]);
+    const uint32_t a = T.amap[p];
+    const double v = m.v[a] + c.ag0 * cs;
+    m.v[a] = v;
+    const uint32_t row = T.slot_row[p];
+    if (row != kNoDiag) m.diag[row] = v;
+  }
+}
+
+// Row charges of the last evaluation (the q plane, ground row 0 empty).
+__device__ __forceinline__ void row_charges(const TopoDev& T, const LaneMem& m, double* q, int tid) {
+  for (uint32_t i = tid; i < T.n; i += 32) {
+    double s = 0.0;
+    for (uint32_t e = T.q_ptr[i]; e < T.q_ptr[i + 1]; ++e) s = __dadd_rn(s, m.st[T.q_src[e]]);
+    q[i] = s;
+  }
+}
+
+// The LTE charge states at x (capacitor charges, diode junction charges,
+// MOS1 overlap gate charges).
+__device__ void state_charges(const TopoDev& T, const double* rec, const double* x, double* out, int tid) {
+  for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
+    const BatchDev& B = T.b[bi];
+    if (B.qt_sites == 0) continue;
+    const int s = static_cast<int>(B.count);
+    for (uint32_t i = tid; i < B.count; i += 32) {
+      const uint32_t* nd = B.nodes + size_t(i) * B.nt;
+      const double* r = rec + B.rec_off + i;
+      double* o = out + B.qt_off + i * B.qt_sites;
+      if (B.type == kC) {
+        o[0] = r[0] * (x[nd[0]] - x[nd[1]]);
+      } else if (B.type == kD) {
+        double q = 0.0, c;
+        if (r[kDHasQ * s] != 0.0) {
+          const double vd = x[nd[2]] - x[nd[1]];
+          double id, gd;
+          diode_iv(r, s, vd, id, gd);
+          diode_qc(r, s, vd, id, gd, q, c);
+        }
+        o[0] = q;
+      } else if (B.type == kM) {
+        const double xg = x[nd[1]];
+        o[0] = r[kMCgs * s] * (xg - x[nd[5]]);
+        o[1] = r[kMCgd * s] * (xg - x[nd[4]]);
+        o[2] = r[kMCgb * s] * (xg - x[nd[3]]);
+      }
+    }
+  }
+}
+
+// Newton on one lane (converger.newton at W = 1 on the frozen tape), for
+// the transient's operating point (no companion) and its steps. Returns 0
+// converged (x holds the published iterate), 1 out of iterations, 2 the
+// factor left the tape.
+__device__ int lane_newton(const TopoDev& T, uint32_t prog, const LaneMem& m, const double* rec, const LaneOpts& o,
+                           const SimDev& sim, const Companion* cp, bool& lim_active, bool init_fix,
+                           uint32_t& iters, int tid) {
+  const uint32_t n = T.n;
+  const uint32_t max_iter = o.max_iter < 100 ? 100 : o.max_iter;
+  double limit = kXPlausible;
+  for (uint32_t iter = 0; iter < max_iter; ++iter) {
+    eval_all(T, rec, m, lim_active, sim, tid);
+    __syncwarp();
+    assemble(T, prog, m, tid);
+    __syncwarp();
+    if (cp) {
+      companion(T, m, *cp, tid);
+      __syncwarp();
+    }
+    if (iter == 0) {
+      double g = 1.0;
+      uint64_t xm = 0, fm = 0;
+      for (uint32_t i = tid; i < n; i += 32) {
+        g = fmax(g, fabs(m.diag[i]));
+        const uint64_t bx = dbits(fabs(m.x[i])), bf = dbits(fabs(m.rhs[i]));
+        xm = bx > xm ? bx : xm;
+        fm = bf > fm ? bf : fm;
+      }
+      g = warp_fmax(g);
+      xm = warp_max_u64(xm);
+      fm = warp_max_u64(fm);
+      const double scale = fmin(fmax(from_bits(xm), from_bits(fm) * g), 1e18);
+      limit = !(1e3 * scale > kXPlausible) ? kXPlausible : 1e3 * scale;
+    }
+    if (refactor_forward(T, prog, m.v, tid)) {
+      iters = iter + 1;
+      return 2;
+    }
+    back_solve(T, prog, m.v, tid);
+    __syncwarp();
+    uint64_t worst = 0;
+    for (uint32_t j = tid; j < n; j += 32) {
+      const uint32_t i = T.qcol[j];
+      const double d = m.y[j];
+      const double xold = m.x[i];
+      const double xn = xold + d;
+      m.xo[i] = xold;
+      m.x[i] = xn;
+      const double tol = o.reltol * fmax(fabs(xn), fabs(xold)) + (T.cur_row[i] ? o.abstol : o.vntol);
+      const bool finite = fabs(xn) < CUDART_INF && fabs(d) < CUDART_INF;
+      const double qv = div_rn(fabs(d), tol);
+      const double score = !finite ? CUDART_INF : (qv == qv ? qv : 0.0);
+      const uint64_t b = dbits(score);
+      worst = b > worst ? b : worst;
+    }
+    worst = warp_max_u64(worst);
+    __syncwarp();
+    const bool limited = apply_limits(T, rec, m, lim_active, tid);
+    if (T.nlim) lim_active = true;
+    bool ok = !limited && iter != 0 && !(from_bits(worst) >= 1.0);
+    if (ok) {
+      bool p = true;
+      for (uint32_t i = tid; i < n; i += 32) p &= fabs(m.x[i]) <= limit;
+      ok = __all_sync(kFull, p);
+    }
+    if (ok) {
+      bool p = true;
+      for (uint32_t i = tid; i < n; i += 32) p &= fabs(m.rhs[i]) <= residual_gate(o, m.diag[i], m.x[i]);
+      ok = __all_sync(kFull, p);
+    }
+    if (ok) {
+      if (init_fix) {
+        init_fix = false;
+      } else {
+        for (uint32_t i = tid; i < n; i += 32) m.x[i] = m.xo[i];
+        __syncwarp();
+        iters = iter + 1;
+        return 0;
+      }
+    }
+    __syncwarp();
+  }
+  iters = max_iter;
+  return 1;
+}
+
+// CKTterr's bound over the LTE states (integrator.zig minDel at w = 1, then
+// the order-2 root): `method` 1 BE / 2 trap probed after a step integrated
+// with `cur`; q0..q3 the ring slots; NaN when a read entry is not finite.
+__device__ double step_bound(int method, int cur, uint32_t m, const double* q0, const double* q1, const double* q2,
+                             const double* q3, const double* ip, double ag0, double ag1, double dt, double dt1,
+                             double dt2, const TranDev& P, int tid) {
+  const double sum01 = dt + dt1, sum12 = dt1 + dt2, sum012 = dt + (dt1 + dt2);
+  const double coeff = method == 1 ? kLteBe : kLteTrap;
+  double vmin = CUDART_INF, poison = 0.0;
+  for (uint32_t j = tid; j < m; j += 32) {
+    const double qc = q0[j], qp = q1[j], qp2 = q2[j], ipj = ip[j];
+    const double i_new = cur == 2 ? ag0 * (qc - qp) - ag1 * ipj : ag0 * (qc - qp);
+    const double volttol = P.abstol + P.reltol * fmax(fabs(i_new), fabs(ipj));
+    const double chargetol = div_rn(P.reltol * fmax(fmax(fabs(qc), fabs(qp)), P.chgtol), dt);
+    const double tol = fmax(volttol, chargetol);
+    poison += (qc - qc) + (qp - qp) + (qp2 - qp2) + (ipj - ipj);
+    const double f12 = div_rn(qp - qp2, dt1);
+    double dd = div_rn(div_rn(qc - qp, dt) - f12, sum01);
+    if (method != 1) {
+      const double qp3 = q3[j];
+      poison += qp3 - qp3;
+      const double f123 = div_rn(f12 - div_rn(qp2 - qp3, dt2), sum12);
+      dd = div_rn(dd - f123, sum012);
+    }
+    const double del = div_rn(P.trtol * tol, fmax(P.abstol, coeff * fabs(dd)));
+    poison += del == del ? 0.0 : del;
+    vmin = fmin(vmin, del);
+  }
+  vmin = warp_fmin(vmin);
+  poison = warp_sum(poison);
+  if (poison != poison) return CUDART_NAN;
+  return method == 1 ? vmin : sqrt(vmin);
+}
+
+__device__ __forceinline__ bool almost_equal_ulps(double a, double b, long long ulps) {
+  if (a == b) return true;
+  if ((a < 0) != (b < 0)) return false;
+  const long long d = __double_as_longlong(a) - __double_as_longlong(b);
+  return (d < 0 ? -d : d) <= ulps;
+}
+
+// The first PULSE corner at or after `after` over every V source with a
+// PULSE wave (models/vsource.va:133-136: four periodic timers per source).
+__device__ bool next_bp(const TopoDev& T, const double* rec, double after, double& bp) {
+  double best = CUDART_INF;
+  for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
+    const BatchDev& B = T.b[bi];
+    if (B.type != kV) continue;
+    const int s = static_cast<int>(B.count);
+    for (uint32_t i = 0; i < B.count; ++i) {
+      const double* p = rec + B.rec_off + i;
+      if (p[1 * s] != 1.0) continue;
+      const double tr = p[5 * s] > 1.0e-12 ? p[5 * s] : 1.0e-12;
+      const double tf = p[6 * s] > 1.0e-12 ? p[6 * s] : 1.0e-12;
+      const double pwr = p[7 * s];
+      const double pw = (pwr > 0.0 ? pwr : 0.0) + (-pwr > 0.0 ? -pwr : 0.0) * 1.0e30;
+      double per = p[8 * s];
+      const double per_min = tr + pw + tf + 1.0e-12;
+      if (per < per_min) per = per_min;
+      const double td = p[4 * s];
+      const double st[4] = {td, td + tr, td + tr + pw, td + tr + pw + tf};
+      for (int k = 0; k < 4; ++k) {
+        double t = st[k];
+        if (t < after) {
+          const double kk = ceil(div_rn(after - st[k], per));
+          t = st[k] + kk * per;
+          if (t < after) t += per;
+        }
+        if (t < best) best = t;
+      }
+    }
+  }
+  if (best == CUDART_INF) return false;
+  bp = best;
+  return true;
+}
+
+}  // namespace
+
+__device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, const LaneOpts& o, uint32_t prog,
+                          double* block, uint32_t lane, int tid) {
+  const uint32_t n = T.n, nq = T.n_qt;
+  LaneMem m = carve(T, block);
+  double* cur = block + T.smem_doubles;
+  double* prev = cur + n;
+  double* qh = prev + n;   // 4 slots of n: the row-charge ring
+  double* ipr = qh + 4 * n;
+  double* qt = ipr + n;    // 4 slots of nq: the LTE-state ring
+  double* ipt = qt + 4 * nq;
+  const double* rec = L.rec + size_t(lane) * T.rec_size;
+  uint32_t stat[kTsN];
+  for (int k = 0; k < kTsN; ++k) stat[k] = 0;
+  init_consts(T, m.v, tid);
+
+  // operating point: cold start with the junction seeds, MODEINITFIX
+  SimDev sim;
+  sim.t = 0.0;
+  sim.src_scale = 1.0;
+  sim.kind = 0;
+  for (uint32_t i = tid; i < n; i += 32) m.x[i] = 0.0;
+  for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
+    const BatchDev& B = T.b[bi];
+    for (uint32_t i = tid; i < B.count; i += 32) {
+      if (B.type == kD) m.lim[B.lim_off + i] = rec[B.rec_off + kDVcrit * B.count + i];
+      if (B.type == kM) {
+        m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kMSeedVgs * B.count + i];
+        m.lim[B.lim_off + 3 * i + 1] = 0.0;
+        m.lim[B.lim_off + 3 * i + 2] = -1.0;
+      }
+    }
+  }
+  __syncwarp();
+  bool lim_active = T.nlim != 0;
+  LaneOpts op = o;
+  op.residual_tol = 1e-9;
+  op.gmin = 0.0;
+  op.max_iter = 100;
+  uint32_t it = 0;
+  int rc = lane_newton(T, prog, m, rec, op, sim, nullptr, lim_active, true, it, tid);
+  lim_active = false;
+  stat[kTsOpIters] = it;
+  uint32_t n_rec = 0;
+  auto record = [&](double t) {
+    if (P.out_t && n_rec < P.max_pts) {
+      if (tid == 0) P.out_t[size_t(lane) * P.max_pts + n_rec] = t;
+      for (uint32_t k = tid; k < P.n_probes; k += 32)
+        P.out_v[(size_t(lane) * P.max_pts + n_rec) * P.n_probes + k] = m.x[P.probes[k]];
+      ++n_rec;
+    }
+  };
+  if (rc != 0) {
+    stat[kTsStatus] = rc == 2 ? kTranLeftTape : kTranOpFailed;
+  } else {
+    for (uint32_t i = tid; i < n; i += 32) {
+      cur[i] = m.x[i];
+      prev[i] = m.x[i];
+    }
+    // charge histories, flat at q(x_op); no dynamic current yet
+    sim.kind = 1;
+    eval_all(T, rec, m, false, sim, tid);
+    __syncwarp();
+    row_charges(T, m, qh + n, tid);
+    state_charges(T, rec, m.x, qt + nq, tid);
+    __syncwarp();
+    for (uint32_t i = tid; i < n; i += 32) {
+      qh[2 * n + i] = qh[n + i];
+      qh[3 * n + i] = qh[n + i];
+      ipr[i] = 0.0;
+    }
+    for (uint32_t j = tid; j < nq; j += 32) {
+      qt[2 * nq + j] = qt[nq + j];
+      qt[3 * nq + j] = qt[nq + j];
+      ipt[j] = 0.0;
+    }
+    __syncwarp();
+    const bool has_charge = T.q_ptr[n] != 0 || T.c_ptr[T.nnz] != 0;
+    uint32_t hb = 0;  // ring slot r lives at (hb + r) & 3
+    auto slot = [&](double* base, uint32_t len, uint32_t r) { return base + size_t((hb + r) & 3u) * len; };
+
+    const double dt_max = P.dt_max;
+    const double delmin = 1e-11 * dt_max;
+    const double min_break = 10.0 * delmin;
+    double dt = fmin(div_rn(fmin(P.t_step, div_rn(P.t_stop, 100.0)), 10.0), dt_max);
+    double bp0;
+    if (next_bp(T, rec, min_break, bp0)) dt = fmin(dt, 0.1 * bp0);
+    dt = div_rn(dt, 10.0);
+    double dt_old[6];
+    for (int k = 0; k < 6; ++k) dt_old[k] = dt_max;
+    double t = 0.0;
+    int order = 1;
+    uint32_t steps = 0;
+    bool have_bp = false, bp_clamped = false;
+    double bp_next = 0.0, bp_save_dt = div_rn(P.t_stop, 50.0);
+    record(0.0);
+    LaneOpts nr = o;
+    nr.residual_tol = CUDART_INF;
+    nr.gmin = 0.0;
+    nr.max_iter = 100;
+    for (;;) {
+      if (!(t < P.t_stop && !almost_equal_ulps(t, P.t_stop, 100) && steps < P.max_steps)) break;
+      const double t_dev = t + dt;
+      sim.kind = 1;
+      sim.t = t_dev;
+      const bool trap = order == 2;
+      const double ag0 = trap ? div_rn(div_rn(1.0, dt), 1.0 - 0.5) : div_rn(1.0, dt);
+      const double ag1 = trap ? div_rn(0.5, 1.0 - 0.5) : 1.0;
+      // predictor, limited against the accepted point
+      const double xfact = div_rn(dt, dt_old[0]);
+      for (uint32_t i = tid; i < n; i += 32) {
+        m.x[i] = cur[i] + xfact * (cur[i] - prev[i]);
+        m.xo[i] = cur[i];
+      }
+      __syncwarp();
+      apply_limits(T, rec, m, false, tid);
+      lim_active = T.nlim != 0;
+      __syncwarp();
+      Companion c{ag0, ag1, trap, slot(qh, n, 1), ipr};
+      uint32_t iters = 0;
+      rc = lane_newton(T, prog, m, rec, nr, sim, &c, lim_active, false, iters, tid);
+      lim_active = false;
+      stat[kTsAttempts] += 1;
+      stat[kTsNrIters] += iters;
+      if (rc == 2) {
+        stat[kTsStatus] = kTranLeftTape;
+        break;
+      }
+      if (rc != 0) {
+        stat[kTsRejNewton] += 1;
+        order = 1;
+        dt = div_rn(dt, 8.0);
+        if (dt < P.dt_min) {
+          stat[kTsStatus] = kTranUnderflow;
+          break;
+        }
+        continue;
+      }
+      double dt_next = steps == 0 ? dt : fmin(dt * 2.0, dt_max);
+      if (has_charge) {
+        eval_all(T, rec, m, false, sim, tid);
+        __syncwarp();
+        row_charges(T, m, slot(qh, n, 0), tid);
+        state_charges(T, rec, m.x, slot(qt, nq, 0), tid);
+        __syncwarp();
+      }
+      const double dt1 = dt_old[0], dt2 = dt_old[1];
+      if (has_charge && steps > 0) {
+        const int mth = trap ? 2 : 1;
+        const double del = step_bound(mth, mth, nq, slot(qt, nq, 0), slot(qt, nq, 1), slot(qt, nq, 2),
+                                      slot(qt, nq, 3), ipt, ag0, ag1, dt, dt1, dt2, P, tid);
+        if (!(del >= 0.9 * dt)) {
+          stat[kTsRejLte] += 1;
+          if (del != del) {
+            order = 1;
+            dt = div_rn(dt, 8.0);
+          } else {
+            dt = del;
+          }
+          if (dt < P.dt_min) {
+            stat[kTsStatus] = kTranUnderflow;
+            break;
+          }
+          continue;
+        }
+        dt_next = fmin(fmin(fmax(del, P.dt_min), 2.0 * dt), dt_max);
+      }
+      if (has_charge) {
+        if (steps > 0 && order == 1) {
+          const double trial_del = step_bound(2, 1, nq, slot(qt, nq, 0), slot(qt, nq, 1), slot(qt, nq, 2),
+                                              slot(qt, nq, 3), ipt, ag0, ag1, dt, dt1, dt2, P, tid);
+          if (trial_del == trial_del) {
+            const double nd2 = fmin(2.0 * dt, trial_del);
+            if (nd2 > 1.05 * dt) order = 2;
+            dt_next = fmin(fmax(nd2, P.dt_min), dt_max);
+          }
+        }
+        // integrator.advanceCurrent over rows and states, then the rotation
+        const double* q0 = slot(qh, n, 0);
+        const double* q1 = slot(qh, n, 1);
+        for (uint32_t i = tid; i < n; i += 32) {
+          const double d = ag0 * (q0[i] - q1[i]);
+          ipr[i] = trap ? d - ag1 * ipr[i] : d;
+        }
+        const double* s0 = slot(qt, nq, 0);
+        const double* s1 = slot(qt, nq, 1);
+        for (uint32_t j = tid; j < nq; j += 32) {
+          const double d = ag0 * (s0[j] - s1[j]);
+          ipt[j] = trap ? d - ag1 * ipt[j] : d;
+        }
+        hb = (hb + 3u) & 3u;
+      }
+      for (int k = 5; k > 0; --k) dt_old[k] = dt_old[k - 1];
+      dt_old[0] = dt;
+      for (uint32_t i = tid; i < n; i += 32) {
+        prev[i] = cur[i];
+        cur[i] = m.x[i];
+      }
+      __syncwarp();
+      t = t + dt;
+      steps += 1;
+      stat[kTsAccepted] += 1;
+      const double t_new = t;
+      if (have_bp) {
+        const bool landed = bp_clamped ? fabs(t_new - bp_next) <= min_break
+                                       : (bp_next - t_new <= delmin || almost_equal_ulps(t_new, bp_next, 100));
+        if (landed) {
+          stat[kTsBpLandings] += 1;
+          order = 1;
+          double shrink = bp_save_dt, nb;
+          if (next_bp(T, rec, t_new + min_break, nb)) shrink = fmin(shrink, nb - t_new);
+          dt_next = fmin(dt_next, 0.1 * shrink);
+        }
+        have_bp = false;
+      }
+      record(t_new);
+      have_bp = next_bp(T, rec, t_new + min_break, bp_next);
+      bp_clamped = false;
+      if (have_bp) {
+        const double dt_to_bp = bp_next - t_new;
+        if (dt_to_bp < dt_next) {
+          bp_save_dt = dt_next;
+          dt_next = dt_to_bp;
+          bp_clamped = true;
+        }
+      }
+      dt = dt_next;
+      if (t_new + dt > P.t_stop) dt = P.t_stop - t_new;
+    }
+    if (stat[kTsStatus] == kTranDone && steps >= P.max_steps && !(t >= P.t_stop || almost_equal_ulps(t, P.t_stop, 100)))
+      stat[kTsStatus] = kTranMaxSteps;
+    for (uint32_t i = tid; i < n; i += 32) m.x[i] = cur[i];
+    __syncwarp();
+  }
+  for (uint32_t i = tid; i < n; i += 32) L.x[size_t(lane) * n + i] = m.x[i];
+  if (tid < kTsN) P.stats[size_t(lane) * kTsN + tid] = stat[tid];
+  if (tid == 0 && P.n_pts) P.n_pts[lane] = n_rec;
+}
+
+// Transient lanes: a persistent grid, each CTA staging the programs once,
+// each warp running one lane's transient to its end.
+__global__ void __launch_bounds__(256) tran_kernel(TopoDev T, LaneDev L, TranDev P, LaneOpts o) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* lanes_smem = stage_programs(T, smem_raw);
+  const uint32_t prog = saddr(smem_raw);
+  const int tid = threadIdx.x & 31;
+  const uint32_t warps = blockDim.x >> 5, w = threadIdx.x >> 5;
+  double* block = lanes_smem + size_t(w) * T.tran_doubles;
+  for (uint32_t lane = blockIdx.x * warps + w; lane < L.n_lanes; lane += gridDim.x * warps) {
+    tran_lane(T, L, P, o, prog, block, lane, tid);
+    __syncwarp();
+  }
+}
+
+cudaError_t launch_tran(const TopoDev& T, const LaneDev& L, const TranDev& P, const LaneOpts& o,
+                        uint32_t lanes_per_block, cudaStream_t s) {
+  const size_t smem = T.prog_bytes + lanes_per_block * size_t(T.tran_doubles) * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(tran_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  tran_kernel<<<persistent_grid(tran_kernel, L.n_lanes, lanes_per_block, smem), 32 * lanes_per_block, smem, s>>>(
+      T, L, P, o);
+  return cudaGetLastError();
+}
+
 }  // namespace esl

@@ -6,13 +6,21 @@ grid_diodes: an 8x8 resistor grid (R log-uniform in [100, 10k] ohm), 16
 diodes (IS = 1e-14 A, N = 1, RS = 10 ohm) from seeded grid nodes to ground
 and one voltage source at the corner node, swept 0..5 V in 256 points. About
 82 unknowns with the diodes' internal nodes and the source's branch row.
+
+ring_oscillator: a 31-stage CMOS ring of MOS1 inverters (NMOS KP = 120u,
+VTO = 0.45, LAMBDA = 0.05; PMOS KP = 40u, VTO = -0.45, LAMBDA = 0.05;
+W/L = 1u/0.18u), 10 fF load per stage, VDD = 1.8 V brought up by a 50 ps
+supply ramp from 0 V at t = 0 (the operating point is all-zero and the ring
+leaves its metastable point on the devices' mismatch, not on rounding). Each
+lane draws every device's VTO from N(nominal, 30 mV). 34 unknowns. The
+transient is trapezoidal to 20 ns with a 1 ps maximum step.
 """
 
 from __future__ import annotations
 
 import numpy as np
 
-from .circuit import Circuit
+from .circuit import M, Circuit
 
 
 def grid_diodes(seed: int = 1, rows: int = 8, cols: int = 8, n_diodes: int = 16,
@@ -35,3 +43,27 @@ def grid_diodes(seed: int = 1, rows: int = 8, cols: int = 8, n_diodes: int = 16,
     slot = fr.slot("vin", "dc")
     values = np.linspace(0.0, v_stop, points).reshape(-1, 1)
     return fr, [slot], values
+
+
+RING_T_STOP = 20e-9
+RING_T_STEP = 1e-12
+RING_T_MAX = 1e-12
+
+
+def ring_oscillator(seed: int = 1, stages: int = 31, lanes: int = 1024, sigma: float = 0.03,
+                    vdd: float = 1.8, c_load: float = 10e-15, ramp: float = 50e-12):
+    """Returns (frozen circuit, per-device vto slots, values [lanes][2 * stages])."""
+    rng = np.random.default_rng(seed)
+    c = Circuit()
+    c.V("vdd", "vdd", "0", dc=0.0, pulse=[0.0, vdd, 0.0, ramp, ramp, 1.0, 2.0])
+    for k in range(stages):
+        inp, out = f"s{(k - 1) % stages}", f"s{k}"
+        c.M(f"mn{k}", out, inp, "0", "0", type=1.0, vto=0.45, kp=120e-6, **{"lambda": 0.05}, w=1e-6, l=0.18e-6)
+        c.M(f"mp{k}", out, inp, "vdd", "vdd", type=-1.0, vto=-0.45, kp=40e-6, **{"lambda": 0.05}, w=1e-6,
+            l=0.18e-6)
+        c.C(f"cl{k}", out, "0", c_load)
+    fr = c.freeze()
+    slots = fr.slots_of(M, "vto")
+    nominal = np.array([fr.batches[s.batch][2][s.inst, s.param] for s in slots])
+    values = nominal + rng.normal(0.0, sigma, size=(lanes, len(slots)))
+    return fr, slots, values

@@ -27,7 +27,7 @@ LANE_CONVERGED, LANE_MAX_ITER, LANE_SINGULAR, LANE_NEED_SOLVE = 1, 2, 3, 4
 # Every entry point include/espice_lanes.h declares.
 EXPORTS = ["esl_create", "esl_destroy", "esl_last_error", "esl_dims", "esl_set_lanes",
            "esl_dc_solve", "esl_dc_solve_device", "esl_dc_solve_device_static", "esl_tape", "esl_lu_replay_device",
-           "esl_tape_size", "esl_pattern", "esl_compile_tape"]
+           "esl_tape_size", "esl_pattern", "esl_compile_tape", "esl_tran", "esl_tran_device"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 f64p = ctypes.POINTER(ctypes.c_double)
@@ -58,6 +58,22 @@ class Stats(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TranOpts(ctypes.Structure):
+    _fields_ = [("t_stop", ctypes.c_double), ("t_step", ctypes.c_double), ("t_max", ctypes.c_double),
+                ("reltol", ctypes.c_double), ("abstol", ctypes.c_double), ("vntol", ctypes.c_double),
+                ("chgtol", ctypes.c_double), ("trtol", ctypes.c_double), ("dt_min", ctypes.c_double),
+                ("max_steps", ctypes.c_uint32)]
+
+
+def tran_opts(t_stop, t_step, t_max=0.0, reltol=1e-3, abstol=1e-12, vntol=1e-6, chgtol=1e-14, trtol=7.0,
+              dt_min=1e-18, max_steps=0):
+    return TranOpts(t_stop, t_step, t_max, reltol, abstol, vntol, chgtol, trtol, dt_min, max_steps)
+
+
+TS_FIELDS = ["status", "accepted", "attempts", "nr_iters", "rej_newton", "rej_lte", "bp_landings", "op_iters"]
+TRAN_DONE, TRAN_UNDERFLOW, TRAN_OP_FAILED, TRAN_MAX_STEPS, TRAN_LEFT_TAPE = 0, 1, 2, 3, 4
 
 
 class TapeInfo(ctypes.Structure):
@@ -233,6 +249,37 @@ class DcLanes:
                                                        ctypes.byref(paused)),
                     "esl_dc_solve_device_static")
         return paused.value
+
+    def tran(self, opts, probes=(), max_pts=0):
+        """Transient lanes through esl_tran (host buffers): (t [lanes][max_pts],
+        v [lanes][max_pts][n_probes], n_pts [lanes], stats [lanes][8] in
+        TS_FIELDS order, x [lanes][n], kernel ms)."""
+        N = self.n_lanes
+        probes = np.ascontiguousarray(probes, np.uint32)
+        npr = len(probes)
+        t = np.zeros((N, max(max_pts, 1)))
+        v = np.zeros((N, max(max_pts, 1), max(npr, 1)))
+        npts = np.zeros(N, np.uint32)
+        stats = np.zeros((N, len(TS_FIELDS)), np.uint32)
+        x = np.zeros((N, self.n))
+        ms = ctypes.c_float(0)
+        rec = max_pts > 0
+        self._check(self._L.esl_tran(self._ctx, ctypes.byref(opts), _p(probes, u32p) if npr else None,
+                                     ctypes.c_uint32(npr), ctypes.c_uint32(max_pts),
+                                     _p(t, f64p) if rec else None, _p(v, f64p) if rec else None,
+                                     _p(npts, u32p) if rec else None, _p(stats, u32p), _p(x, f64p),
+                                     ctypes.byref(ms)), "esl_tran")
+        return t, v, npts, stats, x, ms.value
+
+    def tran_device(self, opts, d_x, d_stats):
+        """esl_tran_device without a trace: device pointers [lanes][n] f64 and
+        [lanes][8] u32; returns the kernel's ms."""
+        ms = ctypes.c_float(0)
+        self._check(self._L.esl_tran_device(self._ctx, ctypes.byref(opts), ctypes.c_void_p(d_x),
+                                            ctypes.c_void_p(d_stats), None, ctypes.c_uint32(0),
+                                            ctypes.c_uint32(0), None, None, None, ctypes.byref(ms)),
+                    "esl_tran_device")
+        return ms.value
 
     def tape(self):
         q = np.zeros(self.n, np.uint32)

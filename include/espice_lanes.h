@@ -162,6 +162,55 @@ int32_t esl_dc_solve_device_static(esl_ctx *ctx, const esl_newton_opts *opts, do
                                    int cold, uint32_t *d_iters, uint32_t *d_status,
                                    uint32_t *n_paused);
 
+/* Transient options (src/core/query.zig Tran with Tolerances). t_max <= 0
+ * takes min(t_step, t_stop / 50) (src/frontend/analyses.zig:534); dt_min <= 0
+ * takes 1e-18; max_steps 0 means unbounded. */
+typedef struct {
+    double t_stop, t_step, t_max;
+    double reltol, abstol, vntol, chgtol, trtol, dt_min;
+    uint32_t max_steps;
+} esl_tran_opts;
+
+/* Per-lane transient statistics, uint32 [n_lanes][ESL_TS_N]. */
+enum {
+    ESL_TS_STATUS = 0,      /* ESL_TRAN_* */
+    ESL_TS_ACCEPTED = 1,
+    ESL_TS_ATTEMPTS = 2,
+    ESL_TS_NR_ITERS = 3,
+    ESL_TS_REJ_NEWTON = 4,
+    ESL_TS_REJ_LTE = 5,
+    ESL_TS_BP_LANDINGS = 6,
+    ESL_TS_OP_ITERS = 7,
+    ESL_TS_N = 8
+};
+enum {
+    ESL_TRAN_DONE = 0,       /* reached t_stop */
+    ESL_TRAN_UNDERFLOW = 1,  /* TimestepTooSmall */
+    ESL_TRAN_OP_FAILED = 2,  /* the operating point did not converge */
+    ESL_TRAN_MAX_STEPS = 3,
+    ESL_TRAN_LEFT_TAPE = 4   /* a factor left the lead pivot tape: run the lane on the CPU */
+};
+
+/* Monte-Carlo transient lanes (tran.runGpuLanes, tran.zig:1654, driving
+ * gpu_lanes.zig predictRound/newton/apply per tick): each lane solves its
+ * operating point from a cold start, then steps trapezoidally (BE first
+ * step, order promotion, LTE control over the charge states, Newton
+ * rejection, PULSE breakpoints) to t_stop, all inside one launch. Host
+ * buffers: x_out [n_lanes][n] the last accepted solution, stats
+ * [n_lanes][ESL_TS_N]; with max_pts > 0, probes [n_probes] unknowns
+ * recorded at t = 0 and every accepted step into t_out [n_lanes][max_pts],
+ * v_out [n_lanes][max_pts][n_probes], rows per lane in n_pts. ms: the
+ * kernel's device time (may be NULL). */
+int32_t esl_tran(esl_ctx *ctx, const esl_tran_opts *opts, const uint32_t *probes,
+                 uint32_t n_probes, uint32_t max_pts, double *t_out, double *v_out,
+                 uint32_t *n_pts, uint32_t *stats, double *x_out, float *ms);
+
+/* esl_tran on device buffers (d_x, d_stats; the trace buffers may be NULL
+ * when max_pts is 0). */
+int32_t esl_tran_device(esl_ctx *ctx, const esl_tran_opts *opts, double *d_x, uint32_t *d_stats,
+                        const uint32_t *d_probes, uint32_t n_probes, uint32_t max_pts,
+                        double *d_t, double *d_v, uint32_t *d_n_pts, float *ms);
+
 /* The lead lane's pivot tape after the last solve (buildTab,
  * lane_kernels.zig:321-345): q[n], pinv[n]; counts[0] = |L|, counts[1] = |U|,
  * counts[2] = refactor levels, counts[3] = solve levels. */

@@ -1,0 +1,96 @@
+"""GPU transient lanes against the CPU oracle (B200).
+
+Each lane runs its operating point and its whole trapezoidal transient in one
+launch. Parity with the oracle's restatement of the reference's step control
+(src/analysis/tran/tran.zig Sim): the same step decisions (accepted steps,
+attempts, Newton and LTE rejections, breakpoint landings, Newton iterations),
+the accepted time grid and the recorded waveforms within 1e-9 relative or
+1e-12 absolute, and the reference's ngspice golden waveform at its own
+tolerances.
+"""
+
+import numpy as np
+import pytest
+
+import golden_util as gu
+from espice_b200 import decks, lanes
+from espice_b200.circuit import M
+from netlist import Deck
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+RTOL, ATOL = 1e-9, 1e-12
+DECISIONS = ["status", "accepted", "attempts", "rej_newton", "rej_lte", "bp_landings", "op_iters", "nr_iters"]
+
+
+def _close(a, b, rtol=RTOL, atol=ATOL):
+    return np.abs(a - b) <= atol + rtol * np.maximum(np.abs(a), np.abs(b))
+
+
+def _run_both(fr, slots, values, tstop, tstep, tmax=0.0, probes=(), max_pts=0):
+    go = lanes.tran_opts(tstop, tstep, tmax, max_steps=200_000)
+    oo = oracle.tran_opts(tstop, tstep, tmax, max_steps=200_000)
+    ctx = lanes.DcLanes(fr)
+    ctx.set_lanes(slots, values)
+    g = ctx.tran(go, probes, max_pts)
+    ctx.close()
+    o = oracle.tran(fr, slots, values, oo, probes, max_pts)
+    return g, o
+
+
+def _check_parity(g, o):
+    tg, vg, ng, sg, xg, _ = g
+    to, vo, no, so, xo = o
+    for k, name in enumerate(lanes.TS_FIELDS):
+        if name in DECISIONS:
+            assert np.array_equal(sg[:, k], so[:, k]), f"{name}: gpu {sg[:, k]} oracle {so[:, k]}"
+    assert np.array_equal(ng, no)
+    for lane in range(len(ng)):
+        n = int(ng[lane])
+        assert _close(tg[lane, :n], to[lane, :n], atol=0.0).all()
+        assert _close(vg[lane, :n], vo[lane, :n]).all()
+    assert _close(xg, xo).all()
+
+
+def test_mos1_inverter_transient_one_lane():
+    g = gu.load("tran__device_mos1_large_signal")
+    deck = Deck(g["deck"])
+    fr = deck.circuit().freeze()
+    cols = list(g["plots"][0]["columns"])
+    probes = [fr.unknown(c) for c in cols]
+    _, tstep, tstop = deck.analysis[:3]
+    res_g, res_o = _run_both(fr, [], np.zeros((1, 1)), tstop, tstep, probes=probes, max_pts=4000)
+    _check_parity(res_g, res_o)
+    tg, vg, ng, sg, _, _ = res_g
+    assert sg[0, 0] == lanes.TRAN_DONE
+    n = int(ng[0])
+    for col, worst in gu.score_tran(g, tg[0, :n], vg[0, :n], cols):
+        assert worst <= 1.0, f"{col}: {worst:.3g}x the fixture tolerance"
+
+
+def test_mos1_inverter_transient_lanes_vary_threshold():
+    """Eight lanes, each with its own NMOS and PMOS VTO."""
+    g = gu.load("tran__device_mos1_large_signal")
+    deck = Deck(g["deck"])
+    fr = deck.circuit().freeze()
+    slots = fr.slots_of(M, "vto")
+    nominal = np.array([fr.param(s) for s in slots])
+    rng = np.random.default_rng(7)
+    values = nominal + rng.normal(0.0, 0.05, size=(8, len(slots)))
+    probes = [fr.unknown("v(out)")]
+    _, tstep, tstop = deck.analysis[:3]
+    res_g, res_o = _run_both(fr, slots, values, tstop, tstep, probes=probes, max_pts=4000)
+    _check_parity(res_g, res_o)
+    assert (res_g[3][:, 0] == lanes.TRAN_DONE).all()
+
+
+def test_ring_oscillator_short_window():
+    """Sixteen ring-oscillator samples over the first 2 ns (about 2,000
+    steps each, the supply ramp and the escape from the metastable point)."""
+    fr, slots, values = decks.ring_oscillator(lanes=16)
+    probes = [fr.unknown("v(s0)"), fr.unknown("v(s15)")]
+    res_g, res_o = _run_both(fr, slots, values, 2e-9, decks.RING_T_STEP, decks.RING_T_MAX, probes=probes,
+                             max_pts=2500)
+    _check_parity(res_g, res_o)
+    assert (res_g[3][:, 0] == lanes.TRAN_DONE).all()
