@@ -2,18 +2,24 @@
 
     python bench.py --gpus N --steps K --warmup W [--impl reference]
 
-A step is one pass of the hot path over one batch of lanes: every lane (one
-sweep point) runs its whole Newton solve in the fused CUDA kernel. `value`
-is device-timed (CUDA events on the library's stream, inputs resident in
-HBM, L2 flushed between steps); `e2e` is the same metric through the public
-C ABI with host buffers (start points in, solutions and statuses out,
-copies inside the timed call). Under torchrun each rank solves its own batch
-(independent points: no collective on the data path, weak scaling); the
-times are the max over ranks.
+Workload (one GPU): Monte-Carlo transient lanes of a 31-stage MOS1 CMOS ring
+oscillator (1024 lanes, per-device VTO ~ N(nominal, 30 mV), trapezoidal to
+20 ns with a 1 ps maximum step). A point is one lane's whole transient (its
+operating point, then about 20,000 accepted steps); a step of the benchmark
+is one pass over all lanes, one launch of the fused transient kernel.
+`value` is device-timed (CUDA events on the library's stream, the lanes'
+records resident in HBM, L2 flushed between steps); `e2e` is the same metric
+through the public C ABI with host buffers (esl_set_lanes uploads each
+step's per-lane records, esl_tran returns solutions and step statistics),
+copies inside the timed region. The DC sweep of the grid-with-diodes deck is
+reported beside it (`dc_grid_diodes`). Under torchrun each rank runs its own
+lane batch (independent samples, no collective on the data path, weak
+scaling); times are the max over ranks.
 
 --impl reference times the reference's CPU algorithm on this host's cores
 (the C restatement under oracle/, since the Zig reference cannot be built
-here), one point per worker thread as the reference's sweep pool runs them.
+here): independent lanes, one per worker thread, as the reference's sweep
+pool runs them.
 """
 
 from __future__ import annotations
@@ -34,16 +40,27 @@ sys.path.insert(0, ROOT)
 
 METRIC = "converged sweep points/s on 1 B200, learned+mixed vs plain FP64 at 1e-9 rel"
 UNIT = "points/s"
+RING_LANES = 1024
 
 
-def workload(seed=1):
+def workload(seed=1, lanes_n=RING_LANES):
     from espice_b200 import decks
-    fr, slots, values = decks.grid_diodes(seed=seed, points=256)
-    cfg = {"workload": "grid_diodes: 8x8 R grid (100..10k log-uniform) + 16 diodes (IS=1e-14, N=1, RS=10), "
-                       "V source at the corner swept 0..5 V in 256 points, independent points from 0 V, plain FP64",
+    fr, slots, values = decks.ring_oscillator(seed=seed, lanes=lanes_n)
+    cfg = {"workload": "ring_oscillator: 31-stage CMOS ring, MOS1 (NMOS KP=120u VTO=0.45 LAMBDA=0.05; "
+                       "PMOS KP=40u VTO=-0.45 LAMBDA=0.05; W/L=1u/0.18u), 10 fF per stage, VDD=1.8 V "
+                       "(50 ps ramp), per-device VTO ~ N(nominal, 30 mV); trapezoidal to 20 ns, 1 ps "
+                       "max step; a point = one lane's whole transient, plain FP64",
            "lanes": int(values.shape[0]), "unknowns": int(fr.n), "seed": seed,
+           "t_stop": decks.RING_T_STOP, "t_max": decks.RING_T_MAX,
            "l2": "flushed between timed steps (256 MiB write)", "reltol": 1e-3, "vntol": 1e-6}
     return fr, slots, values, cfg
+
+
+def tran_opts_pair():
+    from espice_b200 import decks, lanes
+    from oracle import oracle
+    return (lanes.tran_opts(decks.RING_T_STOP, decks.RING_T_STEP, decks.RING_T_MAX),
+            oracle.tran_opts(decks.RING_T_STOP, decks.RING_T_STEP, decks.RING_T_MAX))
 
 
 class ClockSampler:
@@ -103,24 +120,25 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_sweep(fr, slots, values, threads):
-    """The oracle's per-point solves on `threads` host threads (ctypes calls
-    release the GIL), each worker taking the next chunk of points."""
+def cpu_tran(fr, slots, values, threads, seconds):
+    """The oracle's transient lanes on `threads` host threads (ctypes calls
+    release the GIL), one lane per task, until `seconds` have passed (the
+    lanes started by then finish). Returns (lanes done, wall seconds)."""
     from oracle import oracle
-    chunks = np.array_split(np.arange(values.shape[0]), max(1, threads * 4))
-    warm = np.zeros(fr.n)
-    conv = 0
+    _, oo = tran_opts_pair()
+    done = 0
+    t0 = time.perf_counter()
 
-    def run(idx):
-        if len(idx) == 0:
+    def run(i):
+        if time.perf_counter() - t0 > seconds:
             return 0
-        _, _, cv = oracle.dc_points(fr, slots, values[idx], warm=warm)
-        return int(cv.sum())
+        _, _, _, st, _ = oracle.tran(fr, slots, values[i:i + 1], oo)
+        return int(st[0, 0] == 0)
 
     with cf.ThreadPoolExecutor(max_workers=threads) as ex:
-        for c in ex.map(run, chunks):
-            conv += c
-    return conv
+        for c in ex.map(run, range(values.shape[0])):
+            done += c
+    return done, time.perf_counter() - t0
 
 
 def reference_arm(args, rank, world):
@@ -128,12 +146,15 @@ def reference_arm(args, rank, world):
         return
     fr, slots, values, cfg = workload()
     threads = os.cpu_count() or 1
+    per_step = max(threads, 2 * threads)  # a bounded sample of the batch
+    sample = values[:per_step]
     for _ in range(args.warmup):
-        cpu_sweep(fr, slots, values, threads)
+        cpu_tran(fr, slots, sample[:threads], threads, 1e9)
     t0 = time.perf_counter()
     pts = 0
     for _ in range(args.steps):
-        pts += cpu_sweep(fr, slots, values, threads)
+        d, _ = cpu_tran(fr, slots, sample, threads, 1e9)
+        pts += d
     dt = time.perf_counter() - t0
     v = pts / dt
     print(json.dumps({
@@ -142,29 +163,27 @@ def reference_arm(args, rank, world):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": cfg,
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} batches of {values.shape[0]} points"},
+                         "sample": f"{args.steps} steps of {per_step} of the {values.shape[0]} lanes"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
 
-def algorithmic_bytes(fr, lanes_n, iters_total):
-    """Bytes a lane-major, launch-per-phase design (the reference's) streams
-    per Newton iteration and lane, by SURVEY's per-unit figures: eval reads x
-    and writes the residual and matrix, the refactor reads A and writes
-    L, U and the diagonal, the solve reads them and rhs and writes dx."""
+def lane_major_bytes(fr, nr_iters_total):
+    """Bytes a lane-major, launch-per-phase design (the reference's GPU lanes)
+    streams per Newton iteration and lane (the per-unit figures of the scope
+    table): eval reads x and writes the residual and matrix, the refactor
+    reads A and writes L, U and the diagonal, the solve reads them and rhs
+    and writes dx."""
     from oracle import oracle
     cp, ri = oracle.pattern(fr)
     n, nnz = fr.n, len(ri)
-    rc, tape = oracle.factor_tape(n, cp, ri, np.ones(nnz) + np.eye(1, nnz, 0).ravel())
+    vals = np.ones(nnz)
+    for j in range(n):
+        vals[cp[j] + np.searchsorted(ri[cp[j]:cp[j + 1]], j)] += 8.0
+    rc, tape = oracle.factor_tape(n, cp, ri, vals)
     nlu = len(tape["li"]) + len(tape["ui"])
     per_iter = 8 * (n + nnz + n) + 8 * (nnz + nlu + n) + 8 * (nlu + n + n + n)
-    return per_iter * iters_total
-
-
-def fused_hbm_bytes(fr, rec_size, lanes_n):
-    """HBM bytes the fused kernel must move per solve: each lane's records and
-    start point in, its solution, iteration count and status out."""
-    return lanes_n * (8 * rec_size + 8 * fr.n * 2 + 8)
+    return per_iter * nr_iters_total
 
 
 def lu_replay_roofline(fr, ctx, hbm_peak, peak_src, lanes_n=32768, reps=5):
@@ -196,10 +215,50 @@ def lu_replay_roofline(fr, ctx, hbm_peak, peak_src, lanes_n=32768, reps=5):
     t = float(np.mean(ms[2:])) / 1e3
     per_lane = 8 * (nnz + n) + 8 * (ntv - 1 + n) + 1
     achieved = lanes_n * per_lane / t / 1e9
-    return {"kernel": "lu_replay_kernel", "lanes": lanes_n, "ms": t * 1e3,
+    return {"kernel": "lu_replay_kernel", "lanes": lanes_n, "unknowns": n, "ms": t * 1e3,
             "bytes_per_lane": per_lane, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
             "frac": achieved / hbm_peak, "peak_source": peak_src,
             "bad_lanes": int(bad.sum().item())}
+
+
+def dc_grid_diodes(args, local, flush):
+    """The DC sweep of the grid-with-diodes deck (256 independent points from
+    0 V, one fused DC launch per step), device-timed and end to end."""
+    import torch
+    from espice_b200 import decks, lanes
+    fr, slots, values = decks.grid_diodes(seed=1, points=256)
+    ctx = lanes.DcLanes(fr, device=local)
+    ctx.set_lanes(slots, values)
+    N, n = values.shape[0], fr.n
+    d_x = torch.zeros((N, n), dtype=torch.float64, device="cuda")
+    d_it = torch.zeros(N, dtype=torch.int32, device="cuda")
+    d_st = torch.zeros(N, dtype=torch.int32, device="cuda")
+    opts = lanes.newton_opts()
+    ms, conv = [], 0
+    for i in range(args.warmup + args.steps):
+        d_x.zero_()
+        flush.zero_()
+        torch.cuda.synchronize()
+        s = ctx.solve_device(d_x.data_ptr(), d_it.data_ptr(), d_st.data_ptr(), cold=False, opts=opts)
+        if i >= args.warmup:
+            ms.append(s["kernel_ms"])
+            conv += s["converged"]
+    x0_h = torch.zeros((N, n), dtype=torch.float64).pin_memory().numpy()
+    e2e_t, e2e_conv = [], 0
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        _, _, sth, _ = ctx.solve(x0=x0_h, opts=opts)
+        t2 = time.perf_counter()
+        if i >= args.warmup:
+            e2e_t.append(t2 - t1)
+            e2e_conv += int((sth == lanes.LANE_CONVERGED).sum())
+    ctx.close()
+    return {"workload": "grid_diodes: 8x8 R grid (100..10k log-uniform) + 16 diodes (IS=1e-14, N=1, "
+                        "RS=10), source swept 0..5 V in 256 independent points from 0 V",
+            "value": conv / (sum(ms) / 1e3), "unit": UNIT, "ms_per_step": float(np.mean(ms)),
+            "e2e": conv and e2e_conv / sum(e2e_t)}
 
 
 def our_arm(args, rank, world):
@@ -207,64 +266,60 @@ def our_arm(args, rank, world):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     from espice_b200 import lanes
-    fr, slots, values, cfg = workload(seed=1)
+    fr, slots, values, cfg = workload(seed=1 + rank)
+    go, _ = tran_opts_pair()
     ctx = lanes.DcLanes(fr, device=local)
     ctx.set_lanes(slots, values)
     N, n = values.shape[0], fr.n
-    d_x0 = torch.zeros((N, n), dtype=torch.float64, device="cuda")
-    d_x = torch.zeros_like(d_x0)
-    d_it = torch.zeros(N, dtype=torch.int32, device="cuda")
-    d_st = torch.zeros(N, dtype=torch.int32, device="cuda")
+    d_x = torch.zeros((N, n), dtype=torch.float64, device="cuda")
+    d_st = torch.zeros((N, len(lanes.TS_FIELDS)), dtype=torch.int32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    opts = lanes.newton_opts()
 
     def step():
-        d_x.copy_(d_x0)
         torch.cuda.synchronize()
-        return ctx.solve_device(d_x.data_ptr(), d_it.data_ptr(), d_st.data_ptr(), cold=False, opts=opts)
+        return ctx.tran_device(go, d_x.data_ptr(), d_st.data_ptr())
 
     for _ in range(args.warmup):
         step()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    ms, launches, conv, iters, peeled = [], 0, 0, 0, 0
+    ms, done, steps_acc, nr_iters = [], 0, 0, 0
     with ClockSampler(local) as clk:
         t0 = time.perf_counter()
         for _ in range(args.steps):
             flush.zero_()
-            s = step()
-            ms.append(s["kernel_ms"])
-            launches += s["launches"]
-            conv += s["converged"]
-            peeled += s["peeled"]
-            iters += int(d_it.sum().item())
+            ms.append(step())
+            st = d_st.cpu().numpy()
+            done += int((st[:, 0] == lanes.TRAN_DONE).sum())
+            steps_acc += int(st[:, 1].sum())
+            nr_iters += int(st[:, 3].sum())
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
     dev_s = sum(ms) / 1e3
 
-    # e2e through the public API with host buffers (pinned), copies included.
-    x0_h = torch.zeros((N, n), dtype=torch.float64).pin_memory().numpy()
-    e2e_t = []
+    # e2e through the public API with host buffers: each step uploads the
+    # lanes' parameters (esl_set_lanes) and reads back solutions and stats.
+    e2e_t, e2e_done = [], 0
     for i in range(args.warmup + args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        xh, ith, sth, _ = ctx.solve(x0=x0_h, opts=opts)
+        ctx.set_lanes(slots, values)
+        _, _, _, sth, xh, _ = ctx.tran(go)
         t2 = time.perf_counter()
         if i >= args.warmup:
             e2e_t.append(t2 - t1)
+            e2e_done += int((sth[:, 0] == lanes.TRAN_DONE).sum())
     e2e_s = sum(e2e_t)
-    e2e_conv = int((sth == lanes.LANE_CONVERGED).sum()) * args.steps
 
-    # max over ranks
     if world > 1:
         t = torch.tensor([dev_s, e2e_s], dtype=torch.float64, device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         dev_s, e2e_s = float(t[0]), float(t[1])
-        c = torch.tensor([conv, e2e_conv], dtype=torch.float64, device="cuda")
+        c = torch.tensor([done, e2e_done], dtype=torch.float64, device="cuda")
         torch.distributed.all_reduce(c)
-        conv, e2e_conv = int(c[0]), int(c[1])
+        done, e2e_done = int(c[0]), int(c[1])
     if rank != 0:
         ctx.close()
         return
@@ -277,41 +332,39 @@ def our_arm(args, rank, world):
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    per_launch_ms = sum(ms) / max(1, launches)
-    achieved = fused_hbm_bytes(fr, lanes.record_size(fr), N) / (sum(ms) / args.steps / 1e3) / 1e9
-    alg = algorithmic_bytes(fr, N, iters / args.steps)
+    step_s = dev_s / args.steps
+    rec_bytes = lanes.record_size(fr) * 8
+    hbm_bytes = N * (rec_bytes + 8 * n + 4 * len(lanes.TS_FIELDS))
+    achieved = hbm_bytes / step_s / 1e9
+    alg = lane_major_bytes(fr, nr_iters / args.steps)
     out = {
-        "metric": METRIC, "value": conv / dev_s, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps,
+        "metric": METRIC, "value": done / dev_s, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * step_s,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": cfg,
-        "e2e": {"value": e2e_conv / e2e_s, "unit": UNIT,
-                "h2d_bytes_per_step": int(N * n * 8),
-                "d2h_bytes_per_step": int(N * n * 8 + 2 * N * 4)},
-        "gpu_launches": launches,
+        "e2e": {"value": e2e_done / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": int(N * rec_bytes),
+                "d2h_bytes_per_step": int(N * n * 8 + N * 4 * len(lanes.TS_FIELDS))},
+        "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": None,
-                     "peak_source": peak_src,
-                     "note": "fused dc_newton_kernel: unavoidable HBM bytes (records, start point, "
-                             "solution) per launch / device time; the Newton working set stays in "
-                             "shared memory, so the kernel is latency-bound, not HBM-bound",
+                     "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
+                     "note": "fused tran_kernel: unavoidable HBM bytes (records in, solution and "
+                             "step statistics out) per launch / device time; every lane's Newton "
+                             "working set stays in shared memory for its whole transient, so the "
+                             "kernel is bound by dependent shared-memory latency, not by HBM",
                      "alg_bytes_lane_major_per_step": alg,
-                     "alg_equivalent_gbs": alg / (sum(ms) / args.steps / 1e3) / 1e9},
-        "newton_iters_per_point": iters / max(1, args.steps * N),
-        "peeled_lanes": peeled, "clocks": clk.summary(), "wall_s_timed": wall,
+                     "alg_equivalent_gbs": alg / step_s / 1e9},
+        "accepted_steps_per_point": steps_acc / max(1, args.steps * N),
+        "newton_iters_per_point": nr_iters / max(1, args.steps * N),
+        "clocks": clk.summary(), "wall_s_timed": wall,
     }
+    out["dc_grid_diodes"] = dc_grid_diodes(args, local, flush)
     out["lu_roofline"] = lu_replay_roofline(fr, ctx, hbm_peak, peak_src)
     if args.cpu_baseline:
         threads = os.cpu_count() or 1
-        t0 = time.perf_counter()
-        pts = 0
-        reps = 0
-        while time.perf_counter() - t0 < args.cpu_seconds:
-            pts += cpu_sweep(fr, slots, values, threads)
-            reps += 1
-        dt = time.perf_counter() - t0
-        out["cpu_baseline"] = {"value": pts / dt, "unit": UNIT, "cores": threads, "kind": "port",
-                               "sample": f"{reps} batches of {N} points ({dt:.1f} s)"}
+        d, dt = cpu_tran(fr, slots, values, threads, args.cpu_seconds)
+        out["cpu_baseline"] = {"value": d / dt, "unit": UNIT, "cores": threads, "kind": "port",
+                               "sample": f"{d} of the {N} lanes in {dt:.1f} s"}
     print(json.dumps(out), flush=True)
     ctx.close()
 
@@ -319,7 +372,7 @@ def our_arm(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
