@@ -106,7 +106,7 @@ def lib():
     return _lib
 
 
-RECORD_FIELDS = {0: 1, 1: 1, 2: 10, 3: 1, 4: 15}
+RECORD_FIELDS = {0: 1, 1: 1, 2: 10, 3: 1, 4: 15, 5: 33}
 
 
 def record_size(frozen: Frozen) -> int:
