@@ -22,6 +22,8 @@ constexpr int kMaxBatches = 8;
 //      f0 f2 f3 f4 f5 | J00 J04 J22 J25 J33 J34 J35 J40 J41 J43 J44 J45 J51 J52 J53 J54 J55
 //      | q1 q3 q4 q5 | C11 C13 C14 C15 C31 C33 C34 C35 C41 C43 C44 C51 C53 C55
 constexpr int kStageR = 6, kStageC = 6, kStageV = 7, kStageI = 2, kStageD = 16, kStageM = 40;
+// A MOS1 batch without any charge keeps only the residual and Jacobian cells.
+constexpr int kStageMNoQ = 22;
 
 // Per-instance record fields (doubles, field-major per batch in a lane's
 // record block). Diode fields follow the bias-independent part of

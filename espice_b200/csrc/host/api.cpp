@@ -176,9 +176,10 @@ struct esl_ctx {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::string err;
-  uint32_t lanes_per_block = 4;
+  uint32_t lanes_per_block = 0;  // 0: as many as the lane count spreads over the SMs
   uint32_t lanes_eff = 4;  // lanes per CTA that fit beside the staged programs
   uint32_t tran_lanes_eff = 0;  // the same for the transient kernel (0: does not fit)
+  int sms = 148;
 
   Csc pat;
   std::vector<uint8_t> cur;
@@ -268,6 +269,15 @@ bool read_circuit(const esl_circuit* c, std::vector<HostBatch>& bats) {
     for (uint32_t v : B.nodes)
       if (v >= c->n) return false;
     B.stride = stage_stride(src.type);
+    if (src.type == kM) {
+      bool any = false;
+      for (uint32_t id = 0; id < B.count && !any; ++id) {
+        double r[kMosFields];
+        derive_instance(kM, &B.params[size_t(id) * B.np], r, 1);
+        any = r[kMHasQ] != 0.0;
+      }
+      if (!any) B.stride = kStageMNoQ;
+    }
     B.stage_base = stage;
     stage += B.stride * B.count;
     B.nfields = record_fields(src.type);
@@ -503,7 +513,7 @@ int32_t upload_tape(esl_ctx* ctx) {
   const size_t room = size_t(227) * 1024;
   if (T.prog_bytes + lane_bytes > room)
     return ctx->fail(ESL_NOT_ELIGIBLE, "programs and one lane exceed a CTA's shared memory");
-  ctx->lanes_eff = std::max<uint32_t>(1, std::min<uint32_t>(ctx->lanes_per_block, uint32_t((room - T.prog_bytes) / lane_bytes)));
+  ctx->lanes_eff = std::max<uint32_t>(1, std::min<uint32_t>(8, uint32_t((room - T.prog_bytes) / lane_bytes)));
   // Transient lanes add the accepted points, the charge rings and dynamic
   // currents over the rows and the LTE states: cur | prev | q[4] | ip over
   // n, then q[4] | ip over n_qt.
@@ -511,8 +521,7 @@ int32_t upload_tape(esl_ctx* ctx) {
   const size_t tran_bytes = size_t(T.tran_doubles) * 8;
   ctx->tran_lanes_eff = T.prog_bytes + tran_bytes > room
                             ? 0
-                            : std::max<uint32_t>(1, std::min<uint32_t>(ctx->lanes_per_block,
-                                                                       uint32_t((room - T.prog_bytes) / tran_bytes)));
+                            : std::max<uint32_t>(1, std::min<uint32_t>(8, uint32_t((room - T.prog_bytes) / tran_bytes)));
   ctx->have_tape = true;
   return ESL_OK;
 }
@@ -525,6 +534,16 @@ int32_t build_tape_from(esl_ctx* ctx, const double* lead_vals) {
     return ctx->fail(ESL_NOT_ELIGIBLE, "the lead lane's first Jacobian is singular");
   ctx->prog = compile_tape(ctx->lead);
   return upload_tape(ctx);
+}
+
+// Lanes per CTA for a launch over n_lanes: the caller's choice when given,
+// else enough that the lanes spread over every SM once (each lane is a
+// latency-bound warp; fewer, fuller CTAs would leave SMs idle), at most what
+// shared memory fits.
+uint32_t lanes_per_cta(const esl_ctx* ctx, uint32_t n_lanes, uint32_t fit) {
+  uint32_t want = ctx->lanes_per_block;
+  if (want == 0) want = (n_lanes + uint32_t(ctx->sms) - 1) / uint32_t(ctx->sms);
+  return std::max<uint32_t>(1, std::min<uint32_t>(want, fit));
 }
 
 LaneDev lane_view(esl_ctx* ctx, uint32_t resume) {
@@ -624,6 +643,7 @@ int32_t esl_create(const esl_circuit* circuit, const esl_options* opts, esl_ctx*
   auto ctx = std::make_unique<esl_ctx>();
   ctx->device = opts ? opts->device : 0;
   if (opts && opts->lanes_per_block) ctx->lanes_per_block = std::min<uint32_t>(opts->lanes_per_block, 8);
+  cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->device);
   if (cudaSetDevice(ctx->device) != cudaSuccess) return ESL_NO_DEVICE;
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return ESL_DEVICE_FAULT;
   cudaEventCreate(&ctx->ev0);
@@ -773,7 +793,7 @@ int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d
   }
   LaneOpts o{opts->reltol, opts->abstol, opts->vntol, opts->residual_tol, opts->gmin, opts->max_iter, opts->init_fix};
   ESL_CUDA(cudaEventRecord(ctx->ev0, s));
-  ESL_CUDA(launch_dc_newton(ctx->topo, L, o, ctx->lanes_eff, s));
+  ESL_CUDA(launch_dc_newton(ctx->topo, L, o, lanes_per_cta(ctx, N, ctx->lanes_eff), s));
   uint32_t launches = 1;
   for (;;) {
     bool any = false;
@@ -781,7 +801,7 @@ int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d
     if (!any) break;
     LaneDev R = L;
     R.resume = 1;
-    ESL_CUDA(launch_dc_newton(ctx->topo, R, o, ctx->lanes_eff, s));
+    ESL_CUDA(launch_dc_newton(ctx->topo, R, o, lanes_per_cta(ctx, N, ctx->lanes_eff), s));
     ++launches;
   }
   ESL_CUDA(cudaEventRecord(ctx->ev1, s));
@@ -862,7 +882,7 @@ int32_t esl_dc_solve_device_static(esl_ctx* ctx, const esl_newton_opts* opts, do
   cudaStream_t s = ctx->stream;
   if (cudaError_t e = launch_lane_init(ctx->topo, L, cold != 0, opts->init_fix != 0, s))
     return cuda(e, "lane_init_kernel");
-  if (cudaError_t e = launch_dc_newton(ctx->topo, L, o, ctx->lanes_eff, s)) return cuda(e, "dc_newton_kernel");
+  if (cudaError_t e = launch_dc_newton(ctx->topo, L, o, lanes_per_cta(ctx, N, ctx->lanes_eff), s)) return cuda(e, "dc_newton_kernel");
   uint32_t paused = 0;
   if (cudaError_t e = cudaMemcpyAsync(&paused, L.n_paused, 4, cudaMemcpyDeviceToHost, s))
     return cuda(e, "read paused-lane count");
@@ -952,7 +972,7 @@ int32_t esl_tran_device(esl_ctx* ctx, const esl_tran_opts* opts, double* d_x, ui
   L.x = d_x;
   cudaStream_t s = ctx->stream;
   ESL_CUDA(cudaEventRecord(ctx->ev0, s));
-  ESL_CUDA(launch_tran(ctx->topo, L, P, lo, ctx->tran_lanes_eff, s));
+  ESL_CUDA(launch_tran(ctx->topo, L, P, lo, lanes_per_cta(ctx, ctx->n_lanes, ctx->tran_lanes_eff), s));
   ESL_CUDA(cudaEventRecord(ctx->ev1, s));
   ESL_CUDA(cudaEventSynchronize(ctx->ev1));
   if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
@@ -1093,7 +1113,7 @@ int32_t esl_lu_replay_device(esl_ctx* ctx, const double* lead, uint32_t n_lanes,
     if (int32_t rc = build_tape_from(ctx, lead)) return rc;
   }
   ESL_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-  ESL_CUDA(launch_lu_replay(ctx->topo, n_lanes, d_a, d_rhs, d_tv, d_dx, d_bad, ctx->lanes_eff, ctx->stream));
+  ESL_CUDA(launch_lu_replay(ctx->topo, n_lanes, d_a, d_rhs, d_tv, d_dx, d_bad, lanes_per_cta(ctx, n_lanes, ctx->lanes_eff), ctx->stream));
   ESL_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
   ESL_CUDA(cudaEventSynchronize(ctx->ev1));
   if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);

@@ -177,7 +177,7 @@ __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, 
           break;
         case kM:
           mos1_stamp(r, s, m.x[nd[0]], m.x[nd[1]], m.x[nd[2]], m.x[nd[3]], m.x[nd[4]], m.x[nd[5]],
-                     lim_active ? m.lim + B.lim_off + 3 * i : nullptr, sim.kind != 0, st);
+                     lim_active ? m.lim + B.lim_off + 3 * i : nullptr, sim.kind != 0 && B.stride >= kStageM, st);
           break;
         default:
           break;
