@@ -43,7 +43,7 @@ UNIT = "points/s"
 RING_LANES = 1024
 
 
-def workload(seed=1, lanes_n=RING_LANES):
+def workload(seed=1, lanes_n=RING_LANES, t_stop=None):
     from espice_b200 import decks
     fr, slots, values = decks.ring_oscillator(seed=seed, lanes=lanes_n)
     cfg = {"workload": "ring_oscillator: 31-stage CMOS ring, MOS1 (NMOS KP=120u VTO=0.45 LAMBDA=0.05; "
@@ -51,16 +51,17 @@ def workload(seed=1, lanes_n=RING_LANES):
                        "(50 ps ramp), per-device VTO ~ N(nominal, 30 mV); trapezoidal to 20 ns, 1 ps "
                        "max step; a point = one lane's whole transient, plain FP64",
            "lanes": int(values.shape[0]), "unknowns": int(fr.n), "seed": seed,
-           "t_stop": decks.RING_T_STOP, "t_max": decks.RING_T_MAX,
+           "t_stop": t_stop or decks.RING_T_STOP, "t_max": decks.RING_T_MAX,
            "l2": "flushed between timed steps (256 MiB write)", "reltol": 1e-3, "vntol": 1e-6}
     return fr, slots, values, cfg
 
 
-def tran_opts_pair():
+def tran_opts_pair(t_stop=None):
     from espice_b200 import decks, lanes
     from oracle import oracle
-    return (lanes.tran_opts(decks.RING_T_STOP, decks.RING_T_STEP, decks.RING_T_MAX),
-            oracle.tran_opts(decks.RING_T_STOP, decks.RING_T_STEP, decks.RING_T_MAX))
+    t_stop = t_stop or decks.RING_T_STOP
+    return (lanes.tran_opts(t_stop, decks.RING_T_STEP, decks.RING_T_MAX),
+            oracle.tran_opts(t_stop, decks.RING_T_STEP, decks.RING_T_MAX))
 
 
 class ClockSampler:
@@ -266,8 +267,8 @@ def our_arm(args, rank, world):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     from espice_b200 import lanes
-    fr, slots, values, cfg = workload(seed=1 + rank)
-    go, _ = tran_opts_pair()
+    fr, slots, values, cfg = workload(seed=1 + rank, lanes_n=args.lanes, t_stop=args.t_stop)
+    go, _ = tran_opts_pair(args.t_stop)
     ctx = lanes.DcLanes(fr, device=local)
     ctx.set_lanes(slots, values)
     N, n = values.shape[0], fr.n
@@ -377,6 +378,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    # a reduced case for profiler captures (the benchmark itself uses the defaults)
+    ap.add_argument("--lanes", type=int, default=RING_LANES)
+    ap.add_argument("--t-stop", type=float, default=None)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

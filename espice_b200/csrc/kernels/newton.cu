@@ -222,7 +222,7 @@ __device__ void gather_pattern(const TopoDev& T, const LaneMem& m, double* out, 
 }
 
 // Runs one warp program over v (shared address vb): rows of 32 ops of one
-// kind (a warp-uniform switch), thread t taking op t, the next row's op
+// kind (warp-uniform branches), thread t taking op t, the next row's op
 // fetched while this one runs. Padding ops move 1.0 / 0.0 into the sink.
 // Returns true when a division failed its pivot test (thread-local).
 __device__ __forceinline__ bool run_rows(uint32_t ops, uint32_t rows, uint32_t vb, int tid) {
@@ -235,30 +235,20 @@ __device__ __forceinline__ bool run_rows(uint32_t ops, uint32_t rows, uint32_t v
     const uint32_t kind = op.x >> 28;
     const uint32_t pd = vb + 8 * (op.x & 0x0fffffffu);
     const uint32_t pa = vb + 8 * (op.y & 0xffffu), pb = vb + 8 * (op.y >> 16);
-    switch (kind) {
-      case kOpFlop:
-        sts(pd, __dsub_rn(lds(pd), __dmul_rn(lds(pa), lds(pb))));
-        break;
-      case kOpSubNz: {
-        const double yb = lds(pb);
-        if (yb != 0.0) sts(pd, __dsub_rn(lds(pd), __dmul_rn(lds(pa), yb)));
-        break;
-      }
-      case kOpDivGrowth: {  // dividend at b (the op's own value; 1.0 on padding)
-        const double w = lds(pb), d = lds(pa);
-        if (!(fabs(d) >= __dmul_rn(kGrowth, fabs(w)))) bad = true;
-        sts(pd, div_rn(w, d));
-        break;
-      }
-      case kOpDivScaled: {
-        const double l = div_rn(lds(pb), lds(pa));
-        if (!(fabs(l) < CUDART_INF)) bad = true;
-        sts(pd, l);
-        break;
-      }
-      default:  // kOpDivY
-        sts(pd, div_rn(lds(pb), lds(pa)));
-        break;
+    // Two warp-uniform paths (a switch here compiles to an indirect jump
+    // that costs more than the op): the divisions with their checks
+    // predicated on the kind, and the multiply-subtracts (the solves skip a
+    // zero multiplier, the refactor never does).
+    const double a = lds(pa), b = lds(pb);
+    if (kind == kOpDivGrowth || kind == kOpDivScaled || kind == kOpDivY) {
+      // dividend at b (the op's own value; 1.0 on padding)
+      const double q = div_rn(b, a);
+      if (kind == kOpDivGrowth && !(fabs(a) >= __dmul_rn(kGrowth, fabs(b)))) bad = true;
+      if (kind == kOpDivScaled && !(fabs(q) < CUDART_INF)) bad = true;
+      sts(pd, q);
+    } else {
+      const double d = lds(pd);
+      if (kind == kOpFlop || b != 0.0) sts(pd, __dsub_rn(d, __dmul_rn(a, b)));
     }
     __syncwarp();
     op = next;
