@@ -21,6 +21,8 @@ SOURCES = [
     "csrc/host/records.cpp",
     "csrc/host/api.cpp",
     "csrc/kernels/newton.cu",
+    "csrc/kernels/mlp.cu",
+    "csrc/host/mlp_host.cu",
 ]
 
 

@@ -1,0 +1,323 @@
+// The learned warm start's network on the 5th-generation tensor cores:
+// a BF16 GEMM with FP32 accumulation in tensor memory (tcgen05.mma, operands
+// staged in shared memory in the canonical K-major layout, one elected
+// thread issuing, completion through an mbarrier, the accumulator read back
+// with tcgen05.ld), its fused epilogues (bias, tanh, BF16 copies), and the
+// small kernels of training (tanh backward, transposes, bias gradient, MSE
+// gradient, Adam).
+//
+// Descriptor layouts (bit positions of the instruction descriptor and the
+// shared-memory matrix descriptor) follow the sm100 UMMA definitions;
+// encode_idesc and encode_sdesc pack them by hand.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "mlp.h"
+
+namespace esl {
+
+namespace {
+
+constexpr int kTileM = 128;     // UMMA M (one CTA, cta_group::1)
+constexpr int kTileK = 64;      // K per staged chunk (4 MMAs of K = 16)
+constexpr int kThreads = 128;   // four warps: warp w owns TMEM lanes 32w..32w+31
+constexpr uint32_t kWaitLimit = 1u << 20;  // try_wait rounds before the error flag
+
+// Instruction descriptor, kind::f16: FP32 accumulator (bits 4-5 = 1), A and
+// B BF16 (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0),
+// N >> 3 at bits 17-22, M >> 4 at bits 24-28.
+__host__ __device__ constexpr uint32_t encode_idesc(uint32_t n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | (uint32_t(kTileM >> 4) << 24);
+}
+
+// Shared-memory matrix descriptor, no swizzle (K-major canonical layout
+// ((8, m), 2) : ((16 B, SBO), LBO)): start address >> 4 at bits 0-13,
+// leading byte offset >> 4 at 16-29, stride byte offset >> 4 at 32-45,
+// version 1 at bits 46-47, base offset 0, layout type 0 at bits 61-63.
+__device__ __forceinline__ uint64_t encode_sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return uint64_t((saddr >> 4) & 0x3fffu) | (uint64_t((lbo >> 4) & 0x3fffu) << 16) |
+         (uint64_t((sbo >> 4) & 0x3fffu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Canonical K-major placement of element (r, k) of a rows x kTileK chunk:
+// 8 x 8 core matrices of 128 contiguous bytes, row-group major, K groups of
+// one row group adjacent (LBO = 128 B, SBO = 1024 B).
+__device__ __forceinline__ uint32_t core_offset(uint32_t r, uint32_t k) {
+  return ((r >> 3) * (kTileK / 8) + (k >> 3)) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kWaitLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// C = A (M x K, row-major BF16) . B (N x K, row-major BF16)^T with FP32
+// accumulation; grid (ceil(M / 128), N / bn), block 128 threads. The
+// epilogue adds bias[n] when given, stores the FP32 result to c (ldc) when
+// given, and tanh (act = 1) or identity of it as BF16 to h (ldh) when given.
+// Rows >= M are read as zero and not stored. K is a multiple of 16 (zero
+// padded by the caller), bn a multiple of 16 in [16, 256].
+__global__ void __launch_bounds__(kThreads) gemm_bf16_tc(const __nv_bfloat16* __restrict__ a, int lda,
+                                                         const __nv_bfloat16* __restrict__ b, int ldb, int M, int K,
+                                                         int bn, const float* __restrict__ bias, float* c, int ldc,
+                                                         __nv_bfloat16* h, int ldh, int act, int* err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* sa = smem;                           // 128 x 64 BF16 = 16 KB
+  unsigned char* sb = smem + kTileM * kTileK * 2;     // bn x 64 BF16
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * bn;
+  uint32_t ncols = 32;
+  while (ncols < uint32_t(bn)) ncols <<= 1;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t idesc = encode_idesc(uint32_t(bn));
+  uint32_t parity = 0;
+  bool ok = true;
+
+  for (int k0 = 0; k0 < K; k0 += kTileK) {
+    const int kc = min(kTileK, K - k0);  // a multiple of 16
+    // stage the chunk: 8 BF16 (16 B) per thread per step, zero beyond M / K
+    for (int i = tid; i < kTileM * (kTileK / 8); i += kThreads) {
+      const int r = i / (kTileK / 8), kg = (i % (kTileK / 8)) * 8;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (m0 + r < M && kg < kc) v = *reinterpret_cast<const uint4*>(a + size_t(m0 + r) * lda + k0 + kg);
+      *reinterpret_cast<uint4*>(sa + core_offset(r, kg)) = v;
+    }
+    for (int i = tid; i < bn * (kTileK / 8); i += kThreads) {
+      const int r = i / (kTileK / 8), kg = (i % (kTileK / 8)) * 8;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (kg < kc) v = *reinterpret_cast<const uint4*>(b + size_t(n0 + r) * ldb + k0 + kg);
+      *reinterpret_cast<uint4*>(sb + core_offset(r, kg)) = v;
+    }
+    asm volatile("fence.proxy.async.shared::cta;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (tid == 0) {
+      for (int j = 0; j < kc / 16; ++j) {
+        const uint64_t da = encode_sdesc(smem_u32(sa) + j * 256, 128, 1024);
+        const uint64_t db = encode_sdesc(smem_u32(sb) + j * 256, 128, 1024);
+        const uint32_t acc = (k0 > 0 || j > 0) ? 1u : 0u;
+        const uint32_t z = 0;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+            "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(&bar)));
+    }
+    // the MMAs read the staged chunk: wait before it is overwritten
+    ok = mbar_wait(smem_u32(&bar), parity) && ok;
+    parity ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+  }
+  if (!ok && tid == 0) atomicExch(err, 1);
+
+  // epilogue: warp w reads accumulator rows 32w + lane, eight columns a time
+  const int m = m0 + warp * 32 + lane;
+  for (int c0 = 0; c0 < bn; c0 += 8) {
+    uint32_t r[8];
+    const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0);
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;");
+    if (m < M && ok) {
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const int n = n0 + c0 + t;
+        float v = __uint_as_float(r[t]);
+        if (bias) v += bias[n];
+        if (c) c[size_t(m) * ldc + n] = v;
+        if (h) h[size_t(m) * ldh + n] = __float2bfloat16_rn(act == 1 ? tanhf(v) : v);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+}
+
+// dZ = dH * (1 - H^2) for a tanh layer (H stored as BF16); FP32 out and a
+// BF16 copy for the next GEMMs.
+__global__ void tanh_backward(const float* dh, const __nv_bfloat16* hb, int ldh, const float* zpre, int rows, int cols,
+                              int ld, float* dz, __nv_bfloat16* dzb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows * cols) return;
+  const int r = i / cols, c = i % cols;
+  const float t = tanhf(zpre[size_t(r) * ld + c]);
+  const float g = dh[size_t(r) * ld + c] * (1.0f - t * t);
+  dz[size_t(r) * ld + c] = g;
+  dzb[size_t(r) * ld + c] = __float2bfloat16_rn(g);
+  (void)hb;
+  (void)ldh;
+}
+
+// out (cols x rows, BF16) = in (rows x cols)^T, through a 32 x 32 tile.
+template <class T>
+__global__ void transpose_to_bf16(const T* in, int rows, int cols, int ldi, __nv_bfloat16* out, int ldo) {
+  __shared__ float tile[32][33];
+  const int c = blockIdx.x * 32 + threadIdx.x, r0 = blockIdx.y * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int r = r0 + j;
+    tile[j][threadIdx.x] = (r < rows && c < cols) ? float(in[size_t(r) * ldi + c]) : 0.0f;
+  }
+  __syncthreads();
+  const int oc = r0 + threadIdx.x, orow0 = blockIdx.x * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int orow = orow0 + j;
+    if (orow < cols && oc < rows) out[size_t(orow) * ldo + oc] = __float2bfloat16_rn(tile[threadIdx.x][j]);
+  }
+}
+
+// db[c] = sum over rows of dz[r][c] (one thread per column; rows is a batch).
+__global__ void bias_grad(const float* dz, int rows, int cols, int ld, float* db) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  float s = 0.0f;
+  for (int r = 0; r < rows; ++r) s += dz[size_t(r) * ld + c];
+  db[c] = s;
+}
+
+// MSE gradient over the real output columns: d = 2 (y - t) / (rows * outs).
+__global__ void mse_grad(const float* y, const float* t, int rows, int outs, int ld, float* d, float* loss) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows * ld) return;
+  const int r = i / ld, c = i % ld;
+  float g = 0.0f;
+  if (c < outs) {
+    const float e = y[size_t(r) * ld + c] - t[size_t(r) * outs + c];
+    g = 2.0f * e / float(rows * outs);
+    atomicAdd(loss, e * e / float(rows * outs));
+  }
+  d[size_t(r) * ld + c] = g;
+}
+
+// Adam on FP32 master weights; refreshes the BF16 copy (and its transpose
+// when given, for the backward GEMMs).
+__global__ void adam_step(float* w, const float* g, float* m, float* v, int rows, int cols, float lr, float b1,
+                          float b2, float eps, float c1, float c2, __nv_bfloat16* wb, __nv_bfloat16* wt, int ldt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows * cols) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  w[i] = wi;
+  if (wb) wb[i] = __float2bfloat16_rn(wi);
+  if (wt) {
+    const int r = i / cols, c = i % cols;
+    wt[size_t(c) * ldt + r] = __float2bfloat16_rn(wi);
+  }
+}
+
+__global__ void to_bf16(const float* in, int n, __nv_bfloat16* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = __float2bfloat16_rn(in[i]);
+}
+
+}  // namespace
+
+cudaError_t launch_gemm_bf16(const __nv_bfloat16* a, int lda, const __nv_bfloat16* b, int ldb, int M, int N, int K,
+                             const float* bias, float* c, int ldc, __nv_bfloat16* h, int ldh, int act, int* err,
+                             cudaStream_t s) {
+  if (M <= 0 || N <= 0 || K <= 0 || K % 16 || N % 16 || lda % 8 || ldb % 8) return cudaErrorInvalidValue;
+  int bn = N <= 256 ? N : 128;
+  while (N % bn) bn -= 16;
+  // 100 KB of dynamic shared memory: at most two CTAs per SM, so their
+  // tensor-memory allocations (at most 256 columns each) fit in the SM's 512.
+  const size_t smem = 100 * 1024;
+  cudaError_t e = cudaFuncSetAttribute(gemm_bf16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  dim3 grid((M + kTileM - 1) / kTileM, N / bn);
+  gemm_bf16_tc<<<grid, kThreads, smem, s>>>(a, lda, b, ldb, M, K, bn, bias, c, ldc, h, ldh, act, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tanh_backward(const float* dh, const float* zpre, int rows, int cols, int ld, float* dz,
+                                 __nv_bfloat16* dzb, cudaStream_t s) {
+  const int n = rows * cols;
+  tanh_backward<<<(n + 255) / 256, 256, 0, s>>>(dh, nullptr, 0, zpre, rows, cols, ld, dz, dzb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transpose_f32(const float* in, int rows, int cols, int ldi, __nv_bfloat16* out, int ldo,
+                                 cudaStream_t s) {
+  dim3 grid((cols + 31) / 32, (rows + 31) / 32), block(32, 8);
+  transpose_to_bf16<float><<<grid, block, 0, s>>>(in, rows, cols, ldi, out, ldo);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transpose_bf16(const __nv_bfloat16* in, int rows, int cols, int ldi, __nv_bfloat16* out, int ldo,
+                                  cudaStream_t s) {
+  dim3 grid((cols + 31) / 32, (rows + 31) / 32), block(32, 8);
+  transpose_to_bf16<__nv_bfloat16><<<grid, block, 0, s>>>(in, rows, cols, ldi, out, ldo);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bias_grad(const float* dz, int rows, int cols, int ld, float* db, cudaStream_t s) {
+  bias_grad<<<(cols + 127) / 128, 128, 0, s>>>(dz, rows, cols, ld, db);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mse_grad(const float* y, const float* t, int rows, int outs, int ld, float* d, float* loss,
+                            cudaStream_t s) {
+  const int n = rows * ld;
+  mse_grad<<<(n + 255) / 256, 256, 0, s>>>(y, t, rows, outs, ld, d, loss);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adam(float* w, const float* g, float* m, float* v, int rows, int cols, float lr, int step,
+                        __nv_bfloat16* wb, __nv_bfloat16* wt, int ldt, cudaStream_t s) {
+  const float b1 = 0.9f, b2 = 0.999f;
+  float c1 = 1.0f, c2 = 1.0f;
+  for (int i = 0; i < step; ++i) {
+    c1 *= b1;
+    c2 *= b2;
+  }
+  const int n = rows * cols;
+  adam_step<<<(n + 255) / 256, 256, 0, s>>>(w, g, m, v, rows, cols, lr, b1, b2, 1e-8f, 1.0f - c1, 1.0f - c2, wb, wt,
+                                            ldt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_to_bf16(const float* in, int n, __nv_bfloat16* out, cudaStream_t s) {
+  to_bf16<<<(n + 255) / 256, 256, 0, s>>>(in, n, out);
+  return cudaGetLastError();
+}
+
+}  // namespace esl

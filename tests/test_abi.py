@@ -1,27 +1,29 @@
 """CPU checks of the C ABI: the library loads and exports every entry
-point include/espice_lanes.h declares (no compute without a GPU)."""
+point include/espice_lanes.h and include/espice_mlp.h declare (no compute
+without a GPU)."""
 
 import os
 import re
 
-from espice_b200 import lanes
+from espice_b200 import lanes, mlp
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared():
-    with open(os.path.join(ROOT, "include", "espice_lanes.h")) as fh:
+def declared(header):
+    with open(os.path.join(ROOT, "include", header)) as fh:
         text = fh.read()
-    return sorted(set(re.findall(r"\b(esl_[a-z_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(esl_[a-z0-9_]+)\s*\(", text)))
 
 
 def test_header_declarations_listed():
-    assert declared() == sorted(lanes.EXPORTS)
+    assert declared("espice_lanes.h") == sorted(lanes.EXPORTS)
+    assert declared("espice_mlp.h") == sorted(mlp.EXPORTS)
 
 
 def test_library_exports_every_declared_symbol():
     lib = lanes.lib()
-    missing = [s for s in declared() if not hasattr(lib, s)]
+    missing = [s for h in ("espice_lanes.h", "espice_mlp.h") for s in declared(h) if not hasattr(lib, s)]
     assert not missing, missing
 
 
@@ -35,3 +37,6 @@ def test_no_device_is_reported_not_faked():
     with pytest.raises(lanes.LaneError) as e:
         lanes.DcLanes(fr)
     assert e.value.code == lanes.ESL_NO_DEVICE
+    with pytest.raises(mlp.MlpError) as e:
+        mlp.Mlp(4, 32, 2, 4)
+    assert e.value.code == 5  # ESL_MLP_NO_DEVICE
