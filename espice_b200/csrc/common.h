@@ -87,6 +87,7 @@ struct LaneOpts {
   double reltol, abstol, vntol, residual_tol, gmin;
   uint32_t max_iter;
   uint32_t init_fix;
+  uint32_t iter_cap;  // 0 or a hard cap below max_iter
 };
 
 // Lane status words (device -> host).

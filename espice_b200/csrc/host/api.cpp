@@ -791,7 +791,8 @@ int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d
     ESL_CUDA(cudaStreamSynchronize(s));
     if (int32_t rc = build_tape_from(ctx, a0.data())) return rc;
   }
-  LaneOpts o{opts->reltol, opts->abstol, opts->vntol, opts->residual_tol, opts->gmin, opts->max_iter, opts->init_fix};
+  LaneOpts o{opts->reltol, opts->abstol, opts->vntol, opts->residual_tol, opts->gmin, opts->max_iter, opts->init_fix,
+             opts->iter_cap};
   ESL_CUDA(cudaEventRecord(ctx->ev0, s));
   ESL_CUDA(launch_dc_newton(ctx->topo, L, o, lanes_per_cta(ctx, N, ctx->lanes_eff), s));
   uint32_t launches = 1;
@@ -878,7 +879,7 @@ int32_t esl_dc_solve_device_static(esl_ctx* ctx, const esl_newton_opts* opts, do
     return fail(ESL_INVALID_ARGUMENT, msg);
   }
   const LaneOpts o{opts->reltol, opts->abstol, opts->vntol, opts->residual_tol, opts->gmin, opts->max_iter,
-                   opts->init_fix};
+                   opts->init_fix, opts->iter_cap};
   cudaStream_t s = ctx->stream;
   if (cudaError_t e = launch_lane_init(ctx->topo, L, cold != 0, opts->init_fix != 0, s))
     return cuda(e, "lane_init_kernel");
@@ -944,7 +945,7 @@ int32_t tran_view(esl_ctx* ctx, const esl_tran_opts* o, TranDev& P, LaneOpts& lo
   P.chgtol = o->chgtol;
   P.trtol = o->trtol;
   P.max_steps = o->max_steps ? o->max_steps : 1000000000u;
-  lo = LaneOpts{o->reltol, o->abstol, o->vntol, std::numeric_limits<double>::infinity(), 0.0, 100, 0};
+  lo = LaneOpts{o->reltol, o->abstol, o->vntol, std::numeric_limits<double>::infinity(), 0.0, 100, 0, 0};
   return ESL_OK;
 }
 

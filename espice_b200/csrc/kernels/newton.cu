@@ -357,7 +357,8 @@ __device__ void dc_solve_lane(const TopoDev& T, const LaneDev& L, const LaneOpts
   uint32_t flags = L.flags[lane];
   uint32_t iter = L.iters[lane];
   double limit = L.limit[lane];
-  const uint32_t max_iter = o.max_iter < 100 ? 100 : o.max_iter;
+  uint32_t max_iter = o.max_iter < 100 ? 100 : o.max_iter;
+  if (o.iter_cap && o.iter_cap < max_iter) max_iter = o.iter_cap;
   SimDev sim;
   sim.t = 0.0;
   sim.src_scale = 1.0;

@@ -45,6 +45,23 @@ def grid_diodes(seed: int = 1, rows: int = 8, cols: int = 8, n_diodes: int = 16,
     return fr, [slot], values
 
 
+def grid_diodes_16(seed: int = 1, points: int = 65536):
+    """The grid-with-diodes deck with 16 swept parameters per point (the
+    learned warm start's workload): the corner source uniform in [0, 5] V and
+    15 grid resistors each scaled by exp(U(-0.7, 0.7)) from seed. Returns
+    (frozen, 16 slots, values [points][16], nominal values [16])."""
+    fr, slots, _ = grid_diodes(seed=1)
+    rng = np.random.default_rng(seed + 1000)
+    rs = [s for s in fr.slots_of(0, "r")][:15]
+    slots = list(slots) + rs
+    nominal = np.array([fr.param(s) for s in slots])
+    nominal[0] = 2.5
+    values = np.empty((points, len(slots)))
+    values[:, 0] = rng.uniform(0.0, 5.0, points)
+    values[:, 1:] = nominal[1:] * np.exp(rng.uniform(-0.7, 0.7, size=(points, len(slots) - 1)))
+    return fr, slots, values, nominal
+
+
 RING_T_STOP = 20e-9
 RING_T_STEP = 1e-12
 RING_T_MAX = 1e-12

@@ -44,7 +44,7 @@ class NewtonOpts(ctypes.Structure):
     _fields_ = [("reltol", ctypes.c_double), ("abstol", ctypes.c_double),
                 ("vntol", ctypes.c_double), ("residual_tol", ctypes.c_double),
                 ("gmin", ctypes.c_double), ("max_iter", ctypes.c_uint32),
-                ("init_fix", ctypes.c_uint32)]
+                ("init_fix", ctypes.c_uint32), ("iter_cap", ctypes.c_uint32)]
 
 
 class Options(ctypes.Structure):
@@ -115,8 +115,8 @@ def record_size(frozen: Frozen) -> int:
 
 
 def newton_opts(reltol=1e-3, abstol=1e-12, vntol=1e-6, residual_tol=1e-9, gmin=0.0,
-                max_iter=50, init_fix=False):
-    return NewtonOpts(reltol, abstol, vntol, residual_tol, gmin, max_iter, int(init_fix))
+                max_iter=50, init_fix=False, iter_cap=0):
+    return NewtonOpts(reltol, abstol, vntol, residual_tol, gmin, max_iter, int(init_fix), int(iter_cap))
 
 
 def _p(a, t):

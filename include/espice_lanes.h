@@ -79,6 +79,8 @@ typedef struct {
     double reltol, abstol, vntol, residual_tol, gmin;
     uint32_t max_iter;   /* raised to at least 100, as optionsFromTolerances does */
     uint32_t init_fix;   /* MODEINITFIX: publish the second passing iterate */
+    uint32_t iter_cap;   /* 0, or a hard cap on Newton iterations below max_iter (a learned
+                            warm start's budget before its nominal fallback) */
 } esl_newton_opts;
 
 typedef struct {
