@@ -262,6 +262,76 @@ def dc_grid_diodes(args, local, flush):
             "e2e": conv and e2e_conv / sum(e2e_t)}
 
 
+def learned_dc(args, local, flush):
+    """The learned warm start against the plain FP64 lanes on the 16-parameter
+    grid-with-diodes deck: 65536 seeded points, the network trained on the
+    first 32768 (their plain-solver solutions, from the nominal warm start),
+    both paths timed on the other 32768: plain from the nominal start, learned
+    from the network's guesses (inference included) with an 8-iteration cap
+    and the nominal fallback."""
+    import torch
+    from espice_b200 import decks, lanes, learned
+    fr, slots, values, nominal = decks.grid_diodes_16(points=65536)
+    train, test = values[:32768], values[32768:]
+    ctx = lanes.DcLanes(fr, device=local)
+    fb = lanes.DcLanes(fr, device=local)
+    ctx.set_lanes(slots, nominal[None, :])
+    x_nom = ctx.solve(x0=None)[0][0]
+    ctx.set_lanes(slots, train)
+    x_tr, _, st_tr, _ = ctx.solve(x0=x_nom)
+    ok = st_tr == lanes.LANE_CONVERGED
+    ws = learned.LearnedWarmStart(len(slots), fr.n, hidden=256, layers=3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss = ws.fit(train[ok], x_tr[ok], epochs=60, batch=256, lr=2e-3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    ctx.set_lanes(slots, test)
+    N, n = test.shape[0], fr.n
+    d_x = torch.empty((N, n), dtype=torch.float64, device="cuda")
+    d_it = torch.zeros(N, dtype=torch.int32, device="cuda")
+    d_st = torch.zeros(N, dtype=torch.int32, device="cuda")
+    x_nom_d = torch.tensor(x_nom, device="cuda")
+    opts = lanes.newton_opts()
+    plain_t, learned_t, it_p, it_l, conv_p, conv_l, fallback = [], [], 0.0, 0.0, 0, 0, 0
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        d_x.copy_(x_nom_d.expand(N, n))
+        ctx.solve_device(d_x.data_ptr(), d_it.data_ptr(), d_st.data_ptr(), cold=False, opts=opts)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        if i >= args.warmup:
+            plain_t.append(t2 - t1)
+            it_p += float(d_it.double().mean())
+            conv_p += int((d_st == lanes.LANE_CONVERGED).sum())
+        flush.zero_()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        _, it, conv, nfb = learned.solve(ctx, fb, ws, slots, test, x_nom, k=8, opts=opts)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        if i >= args.warmup:
+            learned_t.append(t2 - t1)
+            it_l += float(it.mean())
+            conv_l += int(conv.sum())
+            fallback += nfb
+    ws.close()
+    fb.close()
+    ctx.close()
+    k = args.steps
+    return {"workload": "grid_diodes_16: the grid-with-diodes deck, 16 swept parameters (source 0..5 V, 15 "
+                        "resistors x exp(U(-0.7, 0.7))), 32768 held-out points; network 16->256->256->82 "
+                        "(tanh, BF16 tcgen05 GEMMs, FP32 accumulation) trained on 32768 plain-solver points",
+            "plain_points_per_s": conv_p / sum(plain_t), "learned_points_per_s": conv_l / sum(learned_t),
+            "speedup": (conv_l / sum(learned_t)) / (conv_p / sum(plain_t)),
+            "newton_iters_plain": it_p / k, "newton_iters_learned": it_l / k, "fallback_lanes": fallback / k,
+            "train_s": t_train, "train_loss_first_last": [float(loss[0]), float(loss[-1])],
+            "timing": "wall clock around each path with device synchronisation (inference, solve and "
+                      "fallback included)"}
+
+
 def our_arm(args, rank, world):
     import torch
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -360,6 +430,8 @@ def our_arm(args, rank, world):
         "clocks": clk.summary(), "wall_s_timed": wall,
     }
     out["dc_grid_diodes"] = dc_grid_diodes(args, local, flush)
+    if args.learned:
+        out["learned_warm_start"] = learned_dc(args, local, flush)
     out["lu_roofline"] = lu_replay_roofline(fr, ctx, hbm_peak, peak_src)
     if args.cpu_baseline:
         threads = os.cpu_count() or 1
@@ -380,6 +452,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     # a reduced case for profiler captures (the benchmark itself uses the defaults)
     ap.add_argument("--lanes", type=int, default=RING_LANES)
+    ap.add_argument("--no-learned", dest="learned", action="store_false")
     ap.add_argument("--t-stop", type=float, default=None)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -280,7 +280,7 @@ int32_t esl_mlp_set_scaling(esl_mlp* m, const float* in_mu, const float* in_sig,
 }
 
 int32_t esl_mlp_train(esl_mlp* m, const float* d_x, const float* d_y, uint32_t n, uint32_t epochs, uint32_t batch,
-                      float lr, uint64_t seed, float* loss_out) {
+                      float lr, float lr_end, uint64_t seed, float* loss_out) {
   if (!m || !d_x || !d_y || n == 0 || batch == 0 || batch % 16) return ESL_MLP_INVALID_ARGUMENT;
   cudaSetDevice(m->device);
   const int B = int(batch);
@@ -295,6 +295,10 @@ int32_t esl_mlp_train(esl_mlp* m, const float* d_x, const float* d_y, uint32_t n
   if (n_batches == 0) return m->fail(ESL_MLP_INVALID_ARGUMENT, "fewer samples than one batch");
   Layer& last = *m->layers.back();
   for (uint32_t ep = 0; ep < epochs; ++ep) {
+    // geometric decay from lr to lr_end over the epochs
+    const float lr_ep = (lr_end > 0 && epochs > 1)
+                            ? lr * std::pow(lr_end / lr, float(ep) / float(epochs - 1))
+                            : lr;
     std::shuffle(perm.begin(), perm.end(), rng);
     MLP_CUDA(cudaMemsetAsync(m->loss.p, 0, 4, s));
     for (uint32_t bi = 0; bi < n_batches; ++bi) {
@@ -311,10 +315,10 @@ int32_t esl_mlp_train(esl_mlp* m, const float* d_x, const float* d_y, uint32_t n
       if (int32_t rc = backward(m, B)) return rc;
       ++m->step;
       for (auto& ly : m->layers) {
-        MLP_CUDA(esl::launch_adam(ly->w.p, ly->gw.p, ly->mw.p, ly->vw.p, ly->n, ly->k, lr, m->step, ly->wb.p,
+        MLP_CUDA(esl::launch_adam(ly->w.p, ly->gw.p, ly->mw.p, ly->vw.p, ly->n, ly->k, lr_ep, m->step, ly->wb.p,
                                   ly->wt.p, ly->n, s));
-        MLP_CUDA(esl::launch_adam(ly->b.p, ly->gb.p, ly->mb.p, ly->vb.p, 1, ly->n, lr, m->step, nullptr, nullptr, 0,
-                                  s));
+        MLP_CUDA(esl::launch_adam(ly->b.p, ly->gb.p, ly->mb.p, ly->vb.p, 1, ly->n, lr_ep, m->step, nullptr, nullptr,
+                                  0, s));
       }
     }
     if (loss_out) {

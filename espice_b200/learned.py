@@ -25,7 +25,7 @@ class LearnedWarmStart:
     def close(self):
         self.net.close()
 
-    def fit(self, values, x, epochs=40, batch=256, lr=2e-3, seed=1):
+    def fit(self, values, x, epochs=40, batch=256, lr=2e-3, lr_end=2e-5, seed=1):
         """Trains on (values [N][n_params], x [N][n]); returns the loss per epoch."""
         import torch
         values = np.asarray(values, np.float64)
@@ -38,7 +38,8 @@ class LearnedWarmStart:
         dy = torch.tensor(x, dtype=torch.float32, device="cuda")
         torch.cuda.synchronize()
         n = (len(values) // batch) * batch
-        return self.net.train(dx.data_ptr(), dy.data_ptr(), n, epochs=epochs, batch=batch, lr=lr, seed=seed)
+        return self.net.train(dx.data_ptr(), dy.data_ptr(), n, epochs=epochs, batch=batch, lr=lr, lr_end=lr_end,
+                              seed=seed)
 
     def predict(self, d_values, n_points):
         """The guesses for device values [n_points][n_params] (float32), as a

@@ -80,11 +80,12 @@ class Mlp:
                 for a in (in_mu, in_sig, out_mu, out_sig)]
         self._check(self._L.esl_mlp_set_scaling(self._m, *[_fp(a) for a in keep]), "esl_mlp_set_scaling")
 
-    def train(self, d_x, d_y, n, epochs, batch=256, lr=1e-3, seed=1):
+    def train(self, d_x, d_y, n, epochs, batch=256, lr=1e-3, lr_end=0.0, seed=1):
         loss = np.zeros(max(epochs, 1), np.float32)
         self._check(self._L.esl_mlp_train(self._m, ctypes.c_void_p(d_x), ctypes.c_void_p(d_y), ctypes.c_uint32(n),
                                           ctypes.c_uint32(epochs), ctypes.c_uint32(batch), ctypes.c_float(lr),
-                                          ctypes.c_uint64(seed), loss.ctypes.data_as(f32p)), "esl_mlp_train")
+                                          ctypes.c_float(lr_end), ctypes.c_uint64(seed),
+                                          loss.ctypes.data_as(f32p)), "esl_mlp_train")
         return loss[:epochs]
 
     def predict(self, d_x, n, d_y):

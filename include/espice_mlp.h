@@ -44,9 +44,11 @@ int32_t esl_mlp_set_scaling(esl_mlp *m, const float *in_mu, const float *in_sig,
 
 /* Adam on the mean squared error of the standardised outputs: `epochs`
  * passes over d_x [n][n_in] -> d_y [n][n_out] in shuffled batches of
- * `batch` rows (a multiple of 16). loss_out [epochs] (host, may be NULL). */
+ * `batch` rows (a multiple of 16), the step size decaying geometrically from
+ * lr to lr_end (lr_end <= 0: constant). loss_out [epochs] (host, may be
+ * NULL). */
 int32_t esl_mlp_train(esl_mlp *m, const float *d_x, const float *d_y, uint32_t n, uint32_t epochs,
-                      uint32_t batch, float lr, uint64_t seed, float *loss_out);
+                      uint32_t batch, float lr, float lr_end, uint64_t seed, float *loss_out);
 
 /* d_y [n][n_out] = the network at d_x [n][n_in] (unstandardised). */
 int32_t esl_mlp_predict(esl_mlp *m, const float *d_x, uint32_t n, float *d_y);
