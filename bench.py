@@ -222,6 +222,42 @@ def lu_replay_roofline(fr, ctx, hbm_peak, peak_src, lanes_n=32768, reps=5):
             "bad_lanes": int(bad.sum().item())}
 
 
+def lu_lanes_roofline(fr, ctx, hbm_peak, peak_src, lanes_n=131072, reps=5):
+    """The lane-interleaved refactor + solve kernel (one thread per lane,
+    [entry][lane] planes: the reference's arp_lane_refactor + arp_lane_solve
+    layout) over a batch far larger than L2: A and rhs in, the L/U/diagonal
+    tape values and dx out."""
+    import torch
+    from oracle import oracle
+    cp, ri = oracle.pattern(fr)
+    n, nnz = fr.n, len(ri)
+    rng = np.random.default_rng(7)
+    lead = rng.uniform(0.5, 2.0, nnz)
+    for j in range(n):
+        lead[cp[j] + np.searchsorted(ri[cp[j]:cp[j + 1]], j)] += 8.0
+    a = torch.tensor(lead, dtype=torch.float64, device="cuda")[:, None].repeat(1, lanes_n)
+    a *= torch.empty_like(a).uniform_(0.9, 1.1)
+    rhs = torch.randn((n, lanes_n), dtype=torch.float64, device="cuda")
+    dx = torch.empty_like(rhs)
+    bad = torch.zeros(lanes_n, dtype=torch.uint8, device="cuda")
+    ctx.lu_lanes(lead, a.data_ptr(), rhs.data_ptr(), dx.data_ptr(), bad.data_ptr(), 32)
+    nu, nl, ntv = ctx.tape_size()
+    tv = torch.empty((ntv, lanes_n), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps + 2):
+        torch.cuda.synchronize()
+        ms.append(ctx.lu_lanes(lead, a.data_ptr(), rhs.data_ptr(), dx.data_ptr(), bad.data_ptr(), lanes_n,
+                               tv.data_ptr()))
+    t = float(np.mean(ms[2:])) / 1e3
+    per_lane = 8 * (nnz + n) + 8 * (ntv - 1 + n) + 1
+    achieved = lanes_n * per_lane / t / 1e9
+    return {"kernel": "lu_lanes_kernel", "lanes": lanes_n, "unknowns": n, "ms": t * 1e3,
+            "bytes_per_lane": per_lane, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+            "frac": achieved / hbm_peak, "peak_source": peak_src,
+            "bad_lanes": int(bad.sum().item())}
+
+
 def dc_grid_diodes(args, local, flush):
     """The DC sweep of the grid-with-diodes deck (256 independent points from
     0 V, one fused DC launch per step), device-timed and end to end."""
@@ -432,7 +468,8 @@ def our_arm(args, rank, world):
     out["dc_grid_diodes"] = dc_grid_diodes(args, local, flush)
     if args.learned:
         out["learned_warm_start"] = learned_dc(args, local, flush)
-    out["lu_roofline"] = lu_replay_roofline(fr, ctx, hbm_peak, peak_src)
+    out["lu_roofline"] = lu_lanes_roofline(fr, ctx, hbm_peak, peak_src)
+    out["lu_roofline_warp_per_lane"] = lu_replay_roofline(fr, ctx, hbm_peak, peak_src)
     if args.cpu_baseline:
         threads = os.cpu_count() or 1
         d, dt = cpu_tran(fr, slots, values, threads, args.cpu_seconds)

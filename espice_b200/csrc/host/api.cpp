@@ -200,7 +200,8 @@ struct esl_ctx {
 
   DevBuf d_nodes[kMaxBatches], d_rhs_ptr, d_rhs_src, d_a_ptr, d_a_src, d_slot_row, d_cur;
   DevBuf d_q_ptr, d_q_src, d_c_ptr, d_c_src, d_probes, d_tran_t, d_tran_v, d_tran_n, d_tran_stats;
-  DevBuf d_amap, d_fill, d_prog, d_l_scaled, d_pinv, d_q;
+  DevBuf d_amap, d_fill, d_prog, d_l_scaled, d_pinv, d_q, d_seq;
+  uint32_t n_seq_a = 0, n_seq = 0, seq_warps = 0;  // lane-interleaved op list
   DevBuf d_rec, d_lim, d_lim_active, d_status, d_iters, d_flags, d_limit, d_a_vals, d_rhs, d_dx,
       d_diag, d_paused, d_x;
   TopoDev topo{};
@@ -522,6 +523,24 @@ int32_t upload_tape(esl_ctx* ctx) {
   ctx->tran_lanes_eff = T.prog_bytes + tran_bytes > room
                             ? 0
                             : std::max<uint32_t>(1, std::min<uint32_t>(8, uint32_t((room - T.prog_bytes) / tran_bytes)));
+  // The sequential op list of the lane-interleaved kernel: the programs'
+  // real ops in row order (padding writes the sink, nv - 1).
+  {
+    std::vector<Op> seq;
+    for (const Op& o : P.a_ops)
+      if ((o.w0 & 0x0fffffffu) != P.nv - 1) seq.push_back(o);
+    ctx->n_seq_a = uint32_t(seq.size());
+    for (const Op& o : P.b_ops)
+      if ((o.w0 & 0x0fffffffu) != P.nv - 1) seq.push_back(o);
+    ctx->n_seq = uint32_t(seq.size());
+    ESL_CUDA(upload(ctx->d_seq, seq, s));
+    ctx->seq_warps = 0;
+    for (uint32_t w = 8; w >= 1; --w)
+      if (lu_lanes_smem(T, ctx->n_seq, w) <= room) {
+        ctx->seq_warps = w;
+        break;
+      }
+  }
   ctx->have_tape = true;
   return ESL_OK;
 }
@@ -1094,6 +1113,24 @@ int32_t esl_tape(const esl_ctx* ctx, uint32_t* q, uint32_t* pinv, uint32_t* coun
     counts[2] = ctx->prog.a_levels;
     counts[3] = ctx->prog.b_levels;
   }
+  return ESL_OK;
+}
+
+int32_t esl_lu_lanes_device(esl_ctx* ctx, const double* lead, uint32_t n_lanes, const double* d_a,
+                            const double* d_rhs, double* d_dx, uint8_t* d_bad, double* d_tv, float* ms) {
+  if (!ctx || !d_a || !d_rhs || !d_dx || !d_bad || n_lanes == 0) return ESL_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  if (!ctx->have_tape) {
+    if (!lead) return ESL_INVALID_ARGUMENT;
+    if (int32_t rc = build_tape_from(ctx, lead)) return rc;
+  }
+  if (ctx->seq_warps == 0) return ctx->fail(ESL_NOT_ELIGIBLE, "a warp's interleaved lane values exceed shared memory");
+  ESL_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  ESL_CUDA(launch_lu_lanes(ctx->topo, ctx->d_seq.as<uint2>(), ctx->n_seq_a, ctx->n_seq, n_lanes, d_a, d_rhs, d_tv,
+                           d_dx, d_bad, ctx->seq_warps, ctx->stream));
+  ESL_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  ESL_CUDA(cudaEventSynchronize(ctx->ev1));
+  if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
   return ESL_OK;
 }
 

@@ -21,6 +21,13 @@ cudaError_t launch_lu_replay(const TopoDev& T, uint32_t n_lanes, const double* a
 cudaError_t launch_tran(const TopoDev& T, const LaneDev& L, const TranDev& P, const LaneOpts& o,
                         uint32_t lanes_per_block, cudaStream_t s);
 
+// Lane-interleaved refactor + solve: seq = the programs' real ops in row
+// order (program A's first n_seq_a), planes [entry][lane].
+uint32_t lu_lanes_smem(const TopoDev& T, uint32_t n_seq, uint32_t warps);
+cudaError_t launch_lu_lanes(const TopoDev& T, const uint2* seq, uint32_t n_seq_a, uint32_t n_seq, uint32_t n_lanes,
+                            const double* a, const double* rhs, double* tv, double* dx, uint8_t* bad,
+                            uint32_t warps, cudaStream_t s);
+
 // Fixed lane scratch of the allocation-free DC entry point: its size, the
 // device address of the array on the current device (looked up once per
 // device; the first call per device must precede any stream capture), and

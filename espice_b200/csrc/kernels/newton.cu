@@ -614,6 +614,114 @@ cudaError_t launch_lu_replay(const TopoDev& T, uint32_t n_lanes, const double* a
 }
 
 // ---------------------------------------------------------------------------
+// Lane-interleaved refactor + solve: one thread per lane. The lane values of a
+// warp sit interleaved in shared memory (value i of the warp's lane t at
+// [i * 32 + t]: every access of the warp is 32 consecutive words), A, rhs and
+// dx are [entry][lane] planes in HBM (coalesced), and every thread walks the
+// same sequential op list (the programs' ops in row order, padding left
+// out), so control flow stays uniform. This is the reference's lane layout
+// (lane_kernels.zig Bodies.refactor / solveNeg over [nnz][N] planes) with the
+// working set staged on chip; the ops and their order per value are those of
+// the warp programs, so the results are bitwise theirs.
+// ---------------------------------------------------------------------------
+namespace {
+
+__global__ void __launch_bounds__(256) lu_lanes_kernel(TopoDev T, const uint2* seq, uint32_t n_seq_a, uint32_t n_seq,
+                                                       uint32_t n_lanes, const double* a, const double* rhs,
+                                                       double* tv_out, double* dx, uint8_t* bad_out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint2* ops = reinterpret_cast<uint2*>(smem_raw);
+  for (uint32_t i = threadIdx.x; i < n_seq; i += blockDim.x) ops[i] = seq[i];
+  unsigned char* lsc = smem_raw + ((size_t(n_seq) * 8 + 15) & ~size_t(15));
+  for (uint32_t i = threadIdx.x; i < T.nl; i += blockDim.x) lsc[i] = T.l_scaled[i];
+  __syncthreads();
+  const uint32_t vbase_off = (size_t(n_seq) * 8 + 15 + T.nl + 15) & ~15u;
+  const uint32_t t = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t nv = T.nv;
+  const uint32_t vb = saddr(smem_raw + vbase_off) + w * nv * 256 + t * 8;  // value i at vb + i * 256
+  const uint32_t ob = saddr(ops);
+  const uint32_t lanes_per_grid = gridDim.x * blockDim.x;
+  const uint32_t l0 = blockIdx.x * blockDim.x + threadIdx.x;
+  // every thread of a warp runs the loop the same number of times (lanes
+  // past the end compute on padding values and store nothing)
+  const uint32_t rounds = (n_lanes + lanes_per_grid - 1) / lanes_per_grid;
+  for (uint32_t rd = 0; rd < rounds; ++rd) {
+    const uint32_t lane = l0 + rd * lanes_per_grid;
+    const bool live = lane < n_lanes;
+    sts(vb + 256 * (nv - 3), 0.0);
+    sts(vb + 256 * (nv - 2), 1.0);
+    sts(vb + 256 * (nv - 1), 0.0);
+    for (uint32_t j = 0; j < T.n_fill; ++j) sts(vb + 256 * T.fill[j], 0.0);
+    for (uint32_t p = 0; p < T.nnz; ++p) sts(vb + 256 * T.amap[p], live ? a[size_t(p) * n_lanes + lane] : 1.0);
+    for (uint32_t r = 0; r < T.n; ++r)
+      sts(vb + 256 * (T.ntv + T.pinv[r]), live ? -rhs[size_t(r) * n_lanes + lane] : 0.0);
+    bool bad = false;
+    auto run = [&](uint32_t k0, uint32_t k1) {
+      for (uint32_t k = k0; k < k1; ++k) {
+        const uint2 op = lds_u2(ob + 8 * k);  // the same word in every thread: a broadcast
+        const uint32_t kind = op.x >> 28;
+        const uint32_t pd = vb + 256 * (op.x & 0x0fffffffu);
+        const uint32_t pa = vb + 256 * (op.y & 0xffffu), pb = vb + 256 * (op.y >> 16);
+        const double av = lds(pa), bv = lds(pb);
+        if (kind == kOpDivGrowth || kind == kOpDivScaled || kind == kOpDivY) {
+          const double q = div_rn(bv, av);
+          if (kind == kOpDivGrowth && !(fabs(av) >= __dmul_rn(kGrowth, fabs(bv)))) bad = true;
+          if (kind == kOpDivScaled && !(fabs(q) < CUDART_INF)) bad = true;
+          sts(pd, q);
+        } else {
+          const double d = lds(pd);
+          if (kind == kOpFlop || bv != 0.0) sts(pd, __dsub_rn(d, __dmul_rn(av, bv)));
+        }
+      }
+    };
+    run(0, n_seq_a);
+    // the refactor's peel tests (as refactor_forward)
+    const uint32_t l0v = T.nu + T.n;
+    for (uint32_t sv = 0; sv < T.nu; ++sv) {
+      const double u = lds(vb + 256 * sv);
+      if (dbits(u - u) != 0) bad = true;
+    }
+    for (uint32_t kk = 0; kk < T.n; ++kk) {
+      const double dg = lds(vb + 256 * (T.nu + kk));
+      if (dg == 0.0 || !(fabs(dg) < CUDART_INF)) bad = true;
+    }
+    for (uint32_t sv = 0; sv < T.nl; ++sv)
+      if (!lsc[sv] && !(fabs(lds(vb + 256 * (l0v + sv))) <= kWide)) bad = true;
+    run(n_seq_a, n_seq);
+    if (live) {
+      for (uint32_t j = 0; j < T.n; ++j) dx[size_t(T.qcol[j]) * n_lanes + lane] = lds(vb + 256 * (T.ntv + j));
+      if (tv_out)
+        for (uint32_t sv = 0; sv < T.ntv; ++sv) tv_out[size_t(sv) * n_lanes + lane] = lds(vb + 256 * sv);
+      bad_out[lane] = bad;
+    }
+  }
+}
+
+}  // namespace
+
+uint32_t lu_lanes_smem(const TopoDev& T, uint32_t n_seq, uint32_t warps) {
+  return uint32_t(((size_t(n_seq) * 8 + 15 + T.nl + 15) & ~size_t(15)) + size_t(warps) * T.nv * 256);
+}
+
+cudaError_t launch_lu_lanes(const TopoDev& T, const uint2* seq, uint32_t n_seq_a, uint32_t n_seq, uint32_t n_lanes,
+                            const double* a, const double* rhs, double* tv, double* dx, uint8_t* bad,
+                            uint32_t warps, cudaStream_t s) {
+  const size_t smem = lu_lanes_smem(T, n_seq, warps);
+  cudaError_t e = cudaFuncSetAttribute(lu_lanes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lu_lanes_kernel, int(32 * warps), smem);
+  const uint32_t per_cta = 32 * warps;
+  const uint32_t need = (n_lanes + per_cta - 1) / per_cta;
+  const uint32_t cap = uint32_t(sms) * uint32_t(per_sm > 0 ? per_sm : 1);
+  lu_lanes_kernel<<<need < cap ? need : cap, per_cta, smem, s>>>(T, seq, n_seq_a, n_seq, n_lanes, a, rhs, tv, dx,
+                                                                 bad);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Fixed lane scratch for the allocation-free DC entry point
 // (esl_dc_solve_device_static). The per-lane Newton state and the paused-lane
 // hand-off buffers the fused kernel keeps in HBM live in one file-scope device

@@ -229,6 +229,14 @@ int32_t esl_lu_replay_device(esl_ctx *ctx, const double *lead, uint32_t n_lanes,
                              const double *d_a, const double *d_rhs, double *d_dx,
                              uint8_t *d_bad, double *d_tv, float *ms);
 
+/* esl_lu_replay_device on lane-interleaved planes, one thread per lane (the
+ * reference's own layout: a [nnz][n_lanes], rhs and dx [n][n_lanes], tv
+ * [ntv][n_lanes], lane_kernels.zig:49-143). Same results, bitwise; for lane
+ * counts that fill the GPU many times over. ESL_NOT_ELIGIBLE when a warp's
+ * 32 lanes of tape values exceed shared memory. */
+int32_t esl_lu_lanes_device(esl_ctx *ctx, const double *lead, uint32_t n_lanes, const double *d_a,
+                            const double *d_rhs, double *d_dx, uint8_t *d_bad, double *d_tv, float *ms);
+
 int32_t esl_tape_size(const esl_ctx *ctx, uint32_t *nu, uint32_t *nl, uint32_t *ntv);
 
 /* Host-only symbolic stage (no device needed). */
