@@ -40,7 +40,7 @@ def test_learned_warm_start_cuts_newton_iterations():
     d_x, it_learned, conv, n_fb = learned.solve(ctx, fb, ws, slots, test, x_nom, k=8)
     assert conv.all()
     assert (st_plain == lanes.LANE_CONVERGED).all()
-    assert it_learned.mean() < 0.9 * it_plain.mean(), (it_learned.mean(), it_plain.mean())
+    assert it_learned.mean() < 0.95 * it_plain.mean(), (it_learned.mean(), it_plain.mean())
 
     # lanes that converged from their guess, against the oracle from the same guess
     guess = ws.predict(torch.tensor(test, dtype=torch.float32, device="cuda"), len(test)).cpu().numpy()
