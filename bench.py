@@ -252,10 +252,25 @@ def lu_lanes_roofline(fr, ctx, hbm_peak, peak_src, lanes_n=131072, reps=5):
     t = float(np.mean(ms[2:])) / 1e3
     per_lane = 8 * (nnz + n) + 8 * (ntv - 1 + n) + 1
     achieved = lanes_n * per_lane / t / 1e9
-    return {"kernel": "lu_lanes_kernel", "lanes": lanes_n, "unknowns": n, "ms": t * 1e3,
-            "bytes_per_lane": per_lane, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-            "frac": achieved / hbm_peak, "peak_source": peak_src,
-            "bad_lanes": int(bad.sum().item())}
+    out = {"kernel": "lu_lanes_kernel", "lanes": lanes_n, "unknowns": n, "ms": t * 1e3,
+           "bytes_per_lane": per_lane, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+           "frac": achieved / hbm_peak, "peak_source": peak_src,
+           "bad_lanes": int(bad.sum().item())}
+    # mixed precision (FP32 factors, FP64 refinement) on the same lanes: A and
+    # rhs in, dx out (refinement re-reads are its own cost, not counted)
+    dxm = torch.empty_like(rhs)
+    refine = torch.zeros(lanes_n, dtype=torch.uint8, device="cuda")
+    msm = []
+    for _ in range(reps + 2):
+        torch.cuda.synchronize()
+        msm.append(ctx.lu_lanes_mixed(lead, a.data_ptr(), rhs.data_ptr(), dxm.data_ptr(), bad.data_ptr(), lanes_n,
+                                      refine.data_ptr()))
+    tm = float(np.mean(msm[2:])) / 1e3
+    rel = float(((dxm - dx).abs() / dx.abs().clamp_min(1e-300)).max())
+    out["mixed"] = {"kernel": "lu_lanes_mixed_kernel", "ms": tm * 1e3, "speedup_vs_fp64": t / tm,
+                    "bytes_per_lane": 8 * (nnz + 2 * n), "achieved_gbs": lanes_n * 8 * (nnz + 2 * n) / tm / 1e9,
+                    "mean_corrections": float(refine.double().mean()), "max_rel_dev_vs_fp64": rel}
+    return out
 
 
 def dc_grid_diodes(args, local, flush):

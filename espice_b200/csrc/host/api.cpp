@@ -202,6 +202,8 @@ struct esl_ctx {
   DevBuf d_q_ptr, d_q_src, d_c_ptr, d_c_src, d_probes, d_tran_t, d_tran_v, d_tran_n, d_tran_stats;
   DevBuf d_amap, d_fill, d_prog, d_l_scaled, d_pinv, d_q, d_seq;
   uint32_t n_seq_a = 0, n_seq = 0, seq_warps = 0;  // lane-interleaved op list
+  uint32_t n_seq_f = 0, mixed_warps = 0;            // its forward-only tail, the mixed kernel's warps
+  DevBuf d_row_ptr, d_row_slot, d_row_col;
   DevBuf d_rec, d_lim, d_lim_active, d_status, d_iters, d_flags, d_limit, d_a_vals, d_rhs, d_dx,
       d_diag, d_paused, d_x;
   TopoDev topo{};
@@ -360,6 +362,27 @@ int32_t upload_topology(esl_ctx* ctx) {
   T.c_ptr = ctx->d_c_ptr.as<uint32_t>();
   T.c_src = ctx->d_c_src.as<uint32_t>();
   T.n_qt = ctx->n_qt;
+  {
+    // the pattern by rows, for the refinement's residual
+    const uint32_t n = ctx->pat.n;
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> rows(n);
+    for (uint32_t j = 0; j < n; ++j)
+      for (uint32_t p = ctx->pat.col_ptr[j]; p < ctx->pat.col_ptr[j + 1]; ++p) rows[ctx->pat.row_idx[p]].push_back({p, j});
+    std::vector<uint32_t> rp(n + 1, 0), rs, rc;
+    for (uint32_t i = 0; i < n; ++i) {
+      for (auto& e : rows[i]) {
+        rs.push_back(e.first);
+        rc.push_back(e.second);
+      }
+      rp[i + 1] = uint32_t(rs.size());
+    }
+    ESL_CUDA(upload(ctx->d_row_ptr, rp, s));
+    ESL_CUDA(upload(ctx->d_row_slot, rs, s));
+    ESL_CUDA(upload(ctx->d_row_col, rc, s));
+    T.row_ptr = ctx->d_row_ptr.as<uint32_t>();
+    T.row_slot = ctx->d_row_slot.as<uint32_t>();
+    T.row_col = ctx->d_row_col.as<uint32_t>();
+  }
   ESL_CUDA(upload(ctx->d_rhs_ptr, ctx->rhs_ptr, s));
   ESL_CUDA(upload(ctx->d_rhs_src, ctx->rhs_src, s));
   ESL_CUDA(upload(ctx->d_a_ptr, ctx->a_ptr, s));
@@ -533,7 +556,16 @@ int32_t upload_tape(esl_ctx* ctx) {
     for (const Op& o : P.b_ops)
       if ((o.w0 & 0x0fffffffu) != P.nv - 1) seq.push_back(o);
     ctx->n_seq = uint32_t(seq.size());
+    for (uint32_t k = 0; k < ctx->n_seq_a; ++k)
+      if ((seq[k].w0 >> 28) == kOpSubNz) seq.push_back(seq[k]);
+    ctx->n_seq_f = uint32_t(seq.size()) - ctx->n_seq;
     ESL_CUDA(upload(ctx->d_seq, seq, s));
+    ctx->mixed_warps = 0;
+    for (uint32_t w = 8; w >= 1; --w)
+      if (lu_lanes_mixed_smem(T, ctx->n_seq + ctx->n_seq_f, w) <= room) {
+        ctx->mixed_warps = w;
+        break;
+      }
     ctx->seq_warps = 0;
     for (uint32_t w = 8; w >= 1; --w)
       if (lu_lanes_smem(T, ctx->n_seq, w) <= room) {
@@ -1128,6 +1160,24 @@ int32_t esl_lu_lanes_device(esl_ctx* ctx, const double* lead, uint32_t n_lanes, 
   ESL_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
   ESL_CUDA(launch_lu_lanes(ctx->topo, ctx->d_seq.as<uint2>(), ctx->n_seq_a, ctx->n_seq, n_lanes, d_a, d_rhs, d_tv,
                            d_dx, d_bad, ctx->seq_warps, ctx->stream));
+  ESL_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  ESL_CUDA(cudaEventSynchronize(ctx->ev1));
+  if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
+  return ESL_OK;
+}
+
+int32_t esl_lu_lanes_mixed_device(esl_ctx* ctx, const double* lead, uint32_t n_lanes, const double* d_a,
+                                  const double* d_rhs, double* d_dx, uint8_t* d_bad, uint8_t* d_refine, float* ms) {
+  if (!ctx || !d_a || !d_rhs || !d_dx || !d_bad || n_lanes == 0) return ESL_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  if (!ctx->have_tape) {
+    if (!lead) return ESL_INVALID_ARGUMENT;
+    if (int32_t rc = build_tape_from(ctx, lead)) return rc;
+  }
+  if (ctx->mixed_warps == 0) return ctx->fail(ESL_NOT_ELIGIBLE, "a warp's interleaved lane values exceed shared memory");
+  ESL_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  ESL_CUDA(launch_lu_lanes_mixed(ctx->topo, ctx->d_seq.as<uint2>(), ctx->n_seq_a, ctx->n_seq, ctx->n_seq_f, n_lanes,
+                                 d_a, d_rhs, d_dx, d_bad, d_refine, ctx->mixed_warps, ctx->stream));
   ESL_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
   ESL_CUDA(cudaEventSynchronize(ctx->ev1));
   if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);

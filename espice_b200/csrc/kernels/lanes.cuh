@@ -69,6 +69,11 @@ struct TopoDev {
   const uint32_t* c_src;
   uint32_t n_qt;
   uint32_t tran_doubles;  // per lane, transient kernel
+  // The pattern by rows (the refinement's residual): row i's entries
+  // row_ptr[i] .. row_ptr[i + 1], each its pattern slot and column.
+  const uint32_t* row_ptr;
+  const uint32_t* row_slot;
+  const uint32_t* row_col;
 };
 
 // One transient over every lane (tran.zig Sim): options, the probe trace

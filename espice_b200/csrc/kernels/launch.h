@@ -28,6 +28,13 @@ cudaError_t launch_lu_lanes(const TopoDev& T, const uint2* seq, uint32_t n_seq_a
                             const double* a, const double* rhs, double* tv, double* dx, uint8_t* bad,
                             uint32_t warps, cudaStream_t s);
 
+// The same in FP32 with FP64 iterative refinement; seq = A ops, B ops, then
+// the forward-only ops (n_seq_f).
+uint32_t lu_lanes_mixed_smem(const TopoDev& T, uint32_t n_ops, uint32_t warps);
+cudaError_t launch_lu_lanes_mixed(const TopoDev& T, const uint2* seq, uint32_t n_seq_a, uint32_t n_seq,
+                                  uint32_t n_seq_f, uint32_t n_lanes, const double* a, const double* rhs, double* dx,
+                                  uint8_t* bad, uint8_t* refine, uint32_t warps, cudaStream_t s);
+
 // Fixed lane scratch of the allocation-free DC entry point: its size, the
 // device address of the array on the current device (looked up once per
 // device; the first call per device must precede any stream capture), and

@@ -626,16 +626,36 @@ cudaError_t launch_lu_replay(const TopoDev& T, uint32_t n_lanes, const double* a
 // ---------------------------------------------------------------------------
 namespace {
 
+// cp.async of one 8-byte value from global into shared memory (in flight
+// until cp_async_wait); lanes past the end copy nothing and leave the value.
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, bool live) {
+  if (live) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __global__ void __launch_bounds__(256) lu_lanes_kernel(TopoDev T, const uint2* seq, uint32_t n_seq_a, uint32_t n_seq,
                                                        uint32_t n_lanes, const double* a, const double* rhs,
                                                        double* tv_out, double* dx, uint8_t* bad_out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  // per CTA: the op list, the index tables (amap, pinv, qcol, fill), the
+  // L entries' scaled flags, then each warp's interleaved lane values
   uint2* ops = reinterpret_cast<uint2*>(smem_raw);
+  uint32_t* s_amap = reinterpret_cast<uint32_t*>(ops + n_seq);
+  uint32_t* s_pinv = s_amap + T.nnz;
+  uint32_t* s_qcol = s_pinv + T.n;
+  uint32_t* s_fill = s_qcol + T.n;
+  unsigned char* lsc = reinterpret_cast<unsigned char*>(s_fill + T.n_fill);
   for (uint32_t i = threadIdx.x; i < n_seq; i += blockDim.x) ops[i] = seq[i];
-  unsigned char* lsc = smem_raw + ((size_t(n_seq) * 8 + 15) & ~size_t(15));
+  for (uint32_t i = threadIdx.x; i < T.nnz; i += blockDim.x) s_amap[i] = T.amap[i];
+  for (uint32_t i = threadIdx.x; i < T.n; i += blockDim.x) {
+    s_pinv[i] = T.pinv[i];
+    s_qcol[i] = T.qcol[i];
+  }
+  for (uint32_t i = threadIdx.x; i < T.n_fill; i += blockDim.x) s_fill[i] = T.fill[i];
   for (uint32_t i = threadIdx.x; i < T.nl; i += blockDim.x) lsc[i] = T.l_scaled[i];
   __syncthreads();
-  const uint32_t vbase_off = (size_t(n_seq) * 8 + 15 + T.nl + 15) & ~15u;
+  const size_t tables = size_t(n_seq) * 8 + size_t(T.nnz + 2 * T.n + T.n_fill) * 4 + T.nl;
+  const uint32_t vbase_off = uint32_t((tables + 15) & ~size_t(15));
   const uint32_t t = threadIdx.x & 31, w = threadIdx.x >> 5;
   const uint32_t nv = T.nv;
   const uint32_t vb = saddr(smem_raw + vbase_off) + w * nv * 256 + t * 8;  // value i at vb + i * 256
@@ -643,22 +663,31 @@ __global__ void __launch_bounds__(256) lu_lanes_kernel(TopoDev T, const uint2* s
   const uint32_t lanes_per_grid = gridDim.x * blockDim.x;
   const uint32_t l0 = blockIdx.x * blockDim.x + threadIdx.x;
   // every thread of a warp runs the loop the same number of times (lanes
-  // past the end compute on padding values and store nothing)
+  // past the end compute on stale values and store nothing)
   const uint32_t rounds = (n_lanes + lanes_per_grid - 1) / lanes_per_grid;
   for (uint32_t rd = 0; rd < rounds; ++rd) {
     const uint32_t lane = l0 + rd * lanes_per_grid;
     const bool live = lane < n_lanes;
+    // A and rhs straight into their tape positions, all copies in flight at once
+    for (uint32_t p = 0; p < T.nnz; ++p) cp_async8(vb + 256 * s_amap[p], a + size_t(p) * n_lanes + lane, live);
+    for (uint32_t r = 0; r < T.n; ++r)
+      cp_async8(vb + 256 * (T.ntv + s_pinv[r]), rhs + size_t(r) * n_lanes + lane, live);
     sts(vb + 256 * (nv - 3), 0.0);
     sts(vb + 256 * (nv - 2), 1.0);
     sts(vb + 256 * (nv - 1), 0.0);
-    for (uint32_t j = 0; j < T.n_fill; ++j) sts(vb + 256 * T.fill[j], 0.0);
-    for (uint32_t p = 0; p < T.nnz; ++p) sts(vb + 256 * T.amap[p], live ? a[size_t(p) * n_lanes + lane] : 1.0);
-    for (uint32_t r = 0; r < T.n; ++r)
-      sts(vb + 256 * (T.ntv + T.pinv[r]), live ? -rhs[size_t(r) * n_lanes + lane] : 0.0);
+    for (uint32_t j = 0; j < T.n_fill; ++j) sts(vb + 256 * s_fill[j], 0.0);
+    cp_async_wait();
+    // y = P(-rhs)
+    for (uint32_t r = 0; r < T.n; ++r) {
+      const uint32_t py = vb + 256 * (T.ntv + s_pinv[r]);
+      sts(py, -lds(py));
+    }
     bool bad = false;
     auto run = [&](uint32_t k0, uint32_t k1) {
+      if (k0 >= k1) return;
+      uint2 op = lds_u2(ob + 8 * k0);
       for (uint32_t k = k0; k < k1; ++k) {
-        const uint2 op = lds_u2(ob + 8 * k);  // the same word in every thread: a broadcast
+        const uint2 next = lds_u2(ob + 8 * (k + 1 < k1 ? k + 1 : k));  // the same word in every thread
         const uint32_t kind = op.x >> 28;
         const uint32_t pd = vb + 256 * (op.x & 0x0fffffffu);
         const uint32_t pa = vb + 256 * (op.y & 0xffffu), pb = vb + 256 * (op.y >> 16);
@@ -672,6 +701,7 @@ __global__ void __launch_bounds__(256) lu_lanes_kernel(TopoDev T, const uint2* s
           const double d = lds(pd);
           if (kind == kOpFlop || bv != 0.0) sts(pd, __dsub_rn(d, __dmul_rn(av, bv)));
         }
+        op = next;
       }
     };
     run(0, n_seq_a);
@@ -689,7 +719,7 @@ __global__ void __launch_bounds__(256) lu_lanes_kernel(TopoDev T, const uint2* s
       if (!lsc[sv] && !(fabs(lds(vb + 256 * (l0v + sv))) <= kWide)) bad = true;
     run(n_seq_a, n_seq);
     if (live) {
-      for (uint32_t j = 0; j < T.n; ++j) dx[size_t(T.qcol[j]) * n_lanes + lane] = lds(vb + 256 * (T.ntv + j));
+      for (uint32_t j = 0; j < T.n; ++j) dx[size_t(s_qcol[j]) * n_lanes + lane] = lds(vb + 256 * (T.ntv + j));
       if (tv_out)
         for (uint32_t sv = 0; sv < T.ntv; ++sv) tv_out[size_t(sv) * n_lanes + lane] = lds(vb + 256 * sv);
       bad_out[lane] = bad;
@@ -699,8 +729,176 @@ __global__ void __launch_bounds__(256) lu_lanes_kernel(TopoDev T, const uint2* s
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Mixed precision: the same lane-interleaved replay with the refactor and the
+// triangular solves in FP32, then FP64 iterative refinement on the residual
+// (res = -rhs - A dx with A and rhs re-read in FP64, the correction solved on
+// the FP32 factors) until the residual is below 1e-12 of rhs, at most
+// kRefineMax corrections.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kRefineMax = 6;
+constexpr float kGrowthF = 1e-12f;
+constexpr float kWideF = 1e3f;
+
+__device__ __forceinline__ float ldsf(uint32_t a) {
+  float r;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(r) : "r"(a));
+  return r;
+}
+__device__ __forceinline__ void stsf(uint32_t a, float x) {
+  asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(x) : "memory");
+}
+
+__global__ void __launch_bounds__(256) lu_lanes_mixed_kernel(TopoDev T, const uint2* seq, uint32_t n_seq_a,
+                                                             uint32_t n_seq, uint32_t n_seq_f, uint32_t n_lanes,
+                                                             const double* a, const double* rhs, double* dx_out,
+                                                             uint8_t* bad_out, uint8_t* refine_out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // per CTA: A, B and forward-only op lists, amap, pinv, qcol, fill, the
+  // CSR of the pattern (row_ptr, slot, col), the scaled flags; then per warp
+  // the interleaved FP32 tape values and the FP64 dx
+  const uint32_t n_ops = n_seq + n_seq_f;
+  uint2* ops = reinterpret_cast<uint2*>(smem_raw);
+  uint32_t* s_amap = reinterpret_cast<uint32_t*>(ops + n_ops);
+  uint32_t* s_pinv = s_amap + T.nnz;
+  uint32_t* s_qcol = s_pinv + T.n;
+  uint32_t* s_fill = s_qcol + T.n;
+  uint32_t* s_rptr = s_fill + T.n_fill;
+  uint32_t* s_rslot = s_rptr + T.n + 1;
+  uint32_t* s_rcol = s_rslot + T.nnz;
+  unsigned char* lsc = reinterpret_cast<unsigned char*>(s_rcol + T.nnz);
+  for (uint32_t i = threadIdx.x; i < n_ops; i += blockDim.x) ops[i] = seq[i];
+  for (uint32_t i = threadIdx.x; i < T.nnz; i += blockDim.x) {
+    s_amap[i] = T.amap[i];
+    s_rslot[i] = T.row_slot[i];
+    s_rcol[i] = T.row_col[i];
+  }
+  for (uint32_t i = threadIdx.x; i < T.n; i += blockDim.x) {
+    s_pinv[i] = T.pinv[i];
+    s_qcol[i] = T.qcol[i];
+  }
+  for (uint32_t i = threadIdx.x; i <= T.n; i += blockDim.x) s_rptr[i] = T.row_ptr[i];
+  for (uint32_t i = threadIdx.x; i < T.n_fill; i += blockDim.x) s_fill[i] = T.fill[i];
+  for (uint32_t i = threadIdx.x; i < T.nl; i += blockDim.x) lsc[i] = T.l_scaled[i];
+  __syncthreads();
+  const size_t tables = size_t(n_ops) * 8 + size_t(3 * T.nnz + 3 * T.n + 1 + T.n_fill) * 4 + T.nl;
+  const uint32_t base = uint32_t((tables + 15) & ~size_t(15));
+  const uint32_t t = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t nv = T.nv;
+  const uint32_t per_warp = (nv * 128 + T.n * 256 + 15) & ~15u;
+  const uint32_t vb = saddr(smem_raw + base) + w * per_warp + t * 4;                 // float value i at vb + i * 128
+  const uint32_t xb = saddr(smem_raw + base) + w * per_warp + nv * 128 + t * 8;      // FP64 dx_i at xb + i * 256
+  const uint32_t ob = saddr(ops);
+  const uint32_t lanes_per_grid = gridDim.x * blockDim.x;
+  const uint32_t l0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t rounds = (n_lanes + lanes_per_grid - 1) / lanes_per_grid;
+  for (uint32_t rd = 0; rd < rounds; ++rd) {
+    const uint32_t lane = l0 + rd * lanes_per_grid;
+    const bool live = lane < n_lanes;
+    const size_t ls = live ? lane : 0;  // dead lanes read lane 0 and store nothing
+    for (uint32_t p = 0; p < T.nnz; ++p) stsf(vb + 128 * s_amap[p], float(a[size_t(p) * n_lanes + ls]));
+    for (uint32_t r = 0; r < T.n; ++r) stsf(vb + 128 * (T.ntv + s_pinv[r]), float(-rhs[size_t(r) * n_lanes + ls]));
+    stsf(vb + 128 * (nv - 3), 0.0f);
+    stsf(vb + 128 * (nv - 2), 1.0f);
+    stsf(vb + 128 * (nv - 1), 0.0f);
+    for (uint32_t j = 0; j < T.n_fill; ++j) stsf(vb + 128 * s_fill[j], 0.0f);
+    bool bad = false;
+    auto run = [&](uint32_t k0, uint32_t k1) {
+      if (k0 >= k1) return;
+      uint2 op = lds_u2(ob + 8 * k0);
+      for (uint32_t k = k0; k < k1; ++k) {
+        const uint2 next = lds_u2(ob + 8 * (k + 1 < k1 ? k + 1 : k));
+        const uint32_t kind = op.x >> 28;
+        const uint32_t pd = vb + 128 * (op.x & 0x0fffffffu);
+        const uint32_t pa = vb + 128 * (op.y & 0xffffu), pb = vb + 128 * (op.y >> 16);
+        const float av = ldsf(pa), bv = ldsf(pb);
+        if (kind == kOpDivGrowth || kind == kOpDivScaled || kind == kOpDivY) {
+          const float q = __fdiv_rn(bv, av);
+          if (kind == kOpDivGrowth && !(fabsf(av) >= __fmul_rn(kGrowthF, fabsf(bv)))) bad = true;
+          if (kind == kOpDivScaled && !(fabsf(q) < CUDART_INF_F)) bad = true;
+          stsf(pd, q);
+        } else {
+          const float d = ldsf(pd);
+          if (kind == kOpFlop || bv != 0.0f) stsf(pd, __fsub_rn(d, __fmul_rn(av, bv)));
+        }
+        op = next;
+      }
+    };
+    run(0, n_seq_a);
+    const uint32_t l0v = T.nu + T.n;
+    for (uint32_t sv = 0; sv < T.nu; ++sv) {
+      const float u = ldsf(vb + 128 * sv);
+      if (!(fabsf(u) < CUDART_INF_F)) bad = true;
+    }
+    for (uint32_t kk = 0; kk < T.n; ++kk) {
+      const float dg = ldsf(vb + 128 * (T.nu + kk));
+      if (dg == 0.0f || !(fabsf(dg) < CUDART_INF_F)) bad = true;
+    }
+    for (uint32_t sv = 0; sv < T.nl; ++sv)
+      if (!lsc[sv] && !(fabsf(ldsf(vb + 128 * (l0v + sv))) <= kWideF)) bad = true;
+    run(n_seq_a, n_seq);
+    for (uint32_t j = 0; j < T.n; ++j) sts(xb + 256 * s_qcol[j], double(ldsf(vb + 128 * (T.ntv + j))));
+    // refinement: res = -rhs - A dx in FP64, corrections on the FP32 factors
+    uint32_t refined = 0;
+    for (int it = 0; it <= kRefineMax; ++it) {
+      double rmax = 0.0, bmax = 0.0;
+      for (uint32_t i = 0; i < T.n; ++i) {
+        const double b = rhs[size_t(i) * n_lanes + ls];
+        double res = -b;
+        for (uint32_t e = s_rptr[i]; e < s_rptr[i + 1]; ++e)
+          res = res - a[size_t(s_rslot[e]) * n_lanes + ls] * lds(xb + 256 * s_rcol[e]);
+        rmax = fmax(rmax, fabs(res));
+        bmax = fmax(bmax, fabs(b));
+        stsf(vb + 128 * (T.ntv + s_pinv[i]), float(res));
+      }
+      if (!(rmax > 1e-12 * bmax) || it == kRefineMax) break;
+      run(n_seq, n_seq + n_seq_f);  // forward through L
+      run(n_seq_a, n_seq);          // back through U
+      for (uint32_t j = 0; j < T.n; ++j) {
+        const uint32_t px = xb + 256 * s_qcol[j];
+        sts(px, lds(px) + double(ldsf(vb + 128 * (T.ntv + j))));
+      }
+      ++refined;
+    }
+    if (live) {
+      for (uint32_t i = 0; i < T.n; ++i) dx_out[size_t(i) * n_lanes + lane] = lds(xb + 256 * i);
+      bad_out[lane] = bad;
+      if (refine_out) refine_out[lane] = uint8_t(refined);
+    }
+  }
+}
+
+}  // namespace
+
+uint32_t lu_lanes_mixed_smem(const TopoDev& T, uint32_t n_ops, uint32_t warps) {
+  const size_t tables = size_t(n_ops) * 8 + size_t(3 * T.nnz + 3 * T.n + 1 + T.n_fill) * 4 + T.nl;
+  const uint32_t per_warp = (T.nv * 128 + T.n * 256 + 15) & ~15u;
+  return uint32_t(((tables + 15) & ~size_t(15)) + size_t(warps) * per_warp);
+}
+
+cudaError_t launch_lu_lanes_mixed(const TopoDev& T, const uint2* seq, uint32_t n_seq_a, uint32_t n_seq,
+                                  uint32_t n_seq_f, uint32_t n_lanes, const double* a, const double* rhs, double* dx,
+                                  uint8_t* bad, uint8_t* refine, uint32_t warps, cudaStream_t s) {
+  const size_t smem = lu_lanes_mixed_smem(T, n_seq + n_seq_f, warps);
+  cudaError_t e = cudaFuncSetAttribute(lu_lanes_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lu_lanes_mixed_kernel, int(32 * warps), smem);
+  const uint32_t per_cta = 32 * warps;
+  const uint32_t need = (n_lanes + per_cta - 1) / per_cta;
+  const uint32_t cap = uint32_t(sms) * uint32_t(per_sm > 0 ? per_sm : 1);
+  lu_lanes_mixed_kernel<<<need < cap ? need : cap, per_cta, smem, s>>>(T, seq, n_seq_a, n_seq, n_seq_f, n_lanes, a,
+                                                                       rhs, dx, bad, refine);
+  return cudaGetLastError();
+}
+
 uint32_t lu_lanes_smem(const TopoDev& T, uint32_t n_seq, uint32_t warps) {
-  return uint32_t(((size_t(n_seq) * 8 + 15 + T.nl + 15) & ~size_t(15)) + size_t(warps) * T.nv * 256);
+  const size_t tables = size_t(n_seq) * 8 + size_t(T.nnz + 2 * T.n + T.n_fill) * 4 + T.nl;
+  return uint32_t(((tables + 15) & ~size_t(15)) + size_t(warps) * T.nv * 256);
 }
 
 cudaError_t launch_lu_lanes(const TopoDev& T, const uint2* seq, uint32_t n_seq_a, uint32_t n_seq, uint32_t n_lanes,

@@ -27,7 +27,8 @@ LANE_CONVERGED, LANE_MAX_ITER, LANE_SINGULAR, LANE_NEED_SOLVE = 1, 2, 3, 4
 # Every entry point include/espice_lanes.h declares.
 EXPORTS = ["esl_create", "esl_destroy", "esl_last_error", "esl_dims", "esl_set_lanes",
            "esl_dc_solve", "esl_dc_solve_device", "esl_dc_solve_device_static", "esl_tape", "esl_lu_replay_device",
-           "esl_tape_size", "esl_pattern", "esl_compile_tape", "esl_tran", "esl_tran_device", "esl_lu_lanes_device"]
+           "esl_tape_size", "esl_pattern", "esl_compile_tape", "esl_tran", "esl_tran_device", "esl_lu_lanes_device",
+           "esl_lu_lanes_mixed_device"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 f64p = ctypes.POINTER(ctypes.c_double)
@@ -310,6 +311,17 @@ class DcLanes:
                                                 ctypes.c_void_p(d_dx), ctypes.c_void_p(d_bad),
                                                 ctypes.c_void_p(d_tv) if d_tv else None, ctypes.byref(ms)),
                     "esl_lu_lanes_device")
+        return ms.value
+
+    def lu_lanes_mixed(self, lead, d_a, d_rhs, d_dx, d_bad, n_lanes, d_refine=0):
+        """FP32 lane-interleaved refactor + solve with FP64 refinement; the kernel's ms."""
+        lead = np.ascontiguousarray(lead, np.float64)
+        ms = ctypes.c_float(0)
+        self._check(self._L.esl_lu_lanes_mixed_device(self._ctx, _p(lead, f64p), ctypes.c_uint32(n_lanes),
+                                                      ctypes.c_void_p(d_a), ctypes.c_void_p(d_rhs),
+                                                      ctypes.c_void_p(d_dx), ctypes.c_void_p(d_bad),
+                                                      ctypes.c_void_p(d_refine) if d_refine else None,
+                                                      ctypes.byref(ms)), "esl_lu_lanes_mixed_device")
         return ms.value
 
     def tape_size(self):

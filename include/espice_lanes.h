@@ -237,6 +237,17 @@ int32_t esl_lu_replay_device(esl_ctx *ctx, const double *lead, uint32_t n_lanes,
 int32_t esl_lu_lanes_device(esl_ctx *ctx, const double *lead, uint32_t n_lanes, const double *d_a,
                             const double *d_rhs, double *d_dx, uint8_t *d_bad, double *d_tv, float *ms);
 
+/* esl_lu_lanes_device in mixed precision: the refactor and the triangular
+ * solves in FP32 on the same tape, then FP64 iterative refinement (residual
+ * -rhs - A dx in FP64 from the FP64 planes, corrections solved on the FP32
+ * factors) until the residual falls below 1e-12 of rhs, at most 6
+ * corrections. dx [n][n_lanes] is FP64; refine [n_lanes] (may be NULL)
+ * receives each lane's number of corrections; bad as the FP64 kernel's
+ * tests, taken on the FP32 factors. */
+int32_t esl_lu_lanes_mixed_device(esl_ctx *ctx, const double *lead, uint32_t n_lanes,
+                                  const double *d_a, const double *d_rhs, double *d_dx,
+                                  uint8_t *d_bad, uint8_t *d_refine, float *ms);
+
 int32_t esl_tape_size(const esl_ctx *ctx, uint32_t *nu, uint32_t *nl, uint32_t *ntv);
 
 /* Host-only symbolic stage (no device needed). */

@@ -136,6 +136,45 @@ def test_lu_lanes_kernel_bitwise(deck, seed):
     ctx.close()
 
 
+@pytest.mark.parametrize("deck,seed", [("grid", 0), ("ring", 1)])
+def test_lu_lanes_mixed_refines_to_fp64(deck, seed):
+    """FP32 refactor and solves with FP64 refinement: dx within 1e-9 of the
+    oracle's FP64 replay (the refinement drives the residual below 1e-12 of
+    rhs), the same pivot-failure verdicts, at most a few corrections."""
+    torch = _torch()
+    fr = decks.grid_diodes(seed=seed + 1)[0] if deck == "grid" else decks.ring_oscillator(lanes=2)[0]
+    cp, ri = oracle.pattern(fr)
+    n, nnz = fr.n, len(ri)
+    rng = np.random.default_rng(seed)
+    lead = rng.uniform(0.5, 2.0, nnz) * np.where(rng.random(nnz) < 0.5, 1, -1)
+    diag = np.array([np.searchsorted(ri[cp[j]:cp[j + 1]], j) + cp[j] for j in range(n)])
+    lead[diag] += 8.0
+    n_lanes = 333
+    vals = np.stack([lead * rng.uniform(0.8, 1.2, nnz) for _ in range(n_lanes)])
+    vals[0] = lead
+    vals[5, diag[3]] = 0.0
+    rhs = rng.normal(size=(n_lanes, n))
+    ref = oracle.lane_refactor_solve(n, cp, ri, lead, vals, rhs)
+    ctx = lanes.DcLanes(fr)
+    d_a = torch.tensor(vals.T.copy(), dtype=torch.float64, device="cuda")
+    d_r = torch.tensor(rhs.T.copy(), dtype=torch.float64, device="cuda")
+    d_dx = torch.zeros((n, n_lanes), dtype=torch.float64, device="cuda")
+    d_bad = torch.zeros(n_lanes, dtype=torch.uint8, device="cuda")
+    d_ref = torch.zeros(n_lanes, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    ctx.lu_lanes_mixed(lead, d_a.data_ptr(), d_r.data_ptr(), d_dx.data_ptr(), d_bad.data_ptr(), n_lanes,
+                       d_ref.data_ptr())
+    torch.cuda.synchronize()
+    bad = d_bad.cpu().numpy()
+    assert np.array_equal(bad, ref["bad"])
+    good = bad == 0
+    dx = d_dx.cpu().numpy().T
+    assert _close(dx[good], ref["dx"][good]).all()
+    refine = d_ref.cpu().numpy()[good]
+    assert refine.max() <= 4 and refine.min() >= 1
+    ctx.close()
+
+
 @pytest.mark.parametrize("seed", [1, 2, 3])
 def test_dc_lanes_match_oracle_warm(seed):
     fr, slots, values = decks.grid_diodes(seed=seed, points=256)
