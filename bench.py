@@ -435,13 +435,11 @@ def our_arm(args, rank, world):
             e2e_done += int((sth[:, 0] == lanes.TRAN_DONE).sum())
     e2e_s = sum(e2e_t)
 
-    if world > 1:
-        t = torch.tensor([dev_s, e2e_s], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        dev_s, e2e_s = float(t[0]), float(t[1])
-        c = torch.tensor([done, e2e_done], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(c)
-        done, e2e_done = int(c[0]), int(c[1])
+    # weak scaling: every rank ran its own batch; the job's time is the
+    # slowest rank's, its count the sum
+    from espice_b200 import shard
+    dev_s, done = shard.reduce_run(dev_s, done)
+    e2e_s, e2e_done = shard.reduce_run(e2e_s, e2e_done)
     if rank != 0:
         ctx.close()
         return
