@@ -204,6 +204,7 @@ struct esl_ctx {
   uint32_t n_seq_a = 0, n_seq = 0, seq_warps = 0;  // lane-interleaved op list
   uint32_t n_seq_f = 0, mixed_warps = 0;            // its forward-only tail, the mixed kernel's warps
   DevBuf d_row_ptr, d_row_slot, d_row_col;
+  DevBuf d_group_topo, d_group_lanes, d_group_cta_ctx, d_group_cta_first, d_group_lpb;  // a group launch's tables
   DevBuf d_rec, d_lim, d_lim_active, d_status, d_iters, d_flags, d_limit, d_a_vals, d_rhs, d_dx,
       d_diag, d_paused, d_x;
   TopoDev topo{};
@@ -794,10 +795,13 @@ int32_t esl_set_lanes(esl_ctx* ctx, const esl_slot* slots, uint32_t n_slots, con
   return ensure_lane_buffers(ctx);
 }
 
-int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d_x, int cold,
-                            uint32_t* d_iters, uint32_t* d_status, esl_stats* st) {
-  if (!ctx || !opts || !d_x || ctx->n_lanes == 0) return ESL_INVALID_ARGUMENT;
-  cudaSetDevice(ctx->device);
+namespace {
+
+// Every lane's start state (cold: zero with the junction seeds, op.zig
+// coldStart; warm: x with limiting off) and, on a context's first solve,
+// the lead tape from lane 0's first Jacobian. Leaves the lane view in L.
+int32_t prepare_dc(esl_ctx* ctx, const esl_newton_opts* opts, double* d_x, int cold, uint32_t* d_iters,
+                   uint32_t* d_status, esl_stats* st, LaneDev& L) {
   cudaStream_t s = ctx->stream;
   const uint32_t N = ctx->n_lanes, n = ctx->pat.n;
   if (st) std::memset(st, 0, sizeof(*st));
@@ -830,7 +834,7 @@ int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d
   ESL_CUDA(cudaMemsetAsync(ctx->d_paused.p, 0, 4, s));
   ctx->peel.clear();
 
-  LaneDev L = lane_view(ctx, 0);
+  L = lane_view(ctx, 0);
   L.x = d_x;
   L.iters = d_iters;
   L.status = d_status;
@@ -842,6 +846,19 @@ int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d
     ESL_CUDA(cudaStreamSynchronize(s));
     if (int32_t rc = build_tape_from(ctx, a0.data())) return rc;
   }
+  return ESL_OK;
+}
+
+}  // namespace
+
+int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d_x, int cold,
+                            uint32_t* d_iters, uint32_t* d_status, esl_stats* st) {
+  if (!ctx || !opts || !d_x || ctx->n_lanes == 0) return ESL_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const uint32_t N = ctx->n_lanes;
+  LaneDev L;
+  if (int32_t rc = prepare_dc(ctx, opts, d_x, cold, d_iters, d_status, st, L)) return rc;
   LaneOpts o{opts->reltol, opts->abstol, opts->vntol, opts->residual_tol, opts->gmin, opts->max_iter, opts->init_fix,
              opts->iter_cap};
   ESL_CUDA(cudaEventRecord(ctx->ev0, s));
@@ -1061,6 +1078,110 @@ int32_t esl_tran(esl_ctx* ctx, const esl_tran_opts* opts, const uint32_t* probes
     ESL_CUDA(cudaMemcpyAsync(n_pts, ctx->d_tran_n.p, N * 4, cudaMemcpyDeviceToHost, s));
   }
   ESL_CUDA(cudaStreamSynchronize(s));
+  return ESL_OK;
+}
+
+int32_t esl_group_dc_solve_device(esl_ctx* const* ctxs, uint32_t n_ctx, const esl_newton_opts* opts,
+                                  double* const* d_x, const int* cold, uint32_t* const* d_iters,
+                                  uint32_t* const* d_status, esl_stats* stats) {
+  if (!ctxs || n_ctx == 0 || !opts || !d_x || !d_iters || !d_status) return ESL_INVALID_ARGUMENT;
+  esl_ctx* c0 = ctxs[0];
+  for (uint32_t c = 0; c < n_ctx; ++c) {
+    if (!ctxs[c] || ctxs[c]->n_lanes == 0 || !d_x[c] || !d_iters[c] || !d_status[c]) return ESL_INVALID_ARGUMENT;
+    if (ctxs[c]->device != c0->device) return c0->fail(ESL_INVALID_ARGUMENT, "a group's contexts share one device");
+  }
+  cudaSetDevice(c0->device);
+  esl_ctx* ctx = c0;  // ESL_CUDA reports on the first context
+  std::vector<LaneDev> lanes(n_ctx);
+  std::vector<TopoDev> topos(n_ctx);
+  std::vector<uint32_t> cta_ctx, cta_first, lpb(n_ctx);
+  size_t smem = 0;
+  uint32_t max_lpb = 1;
+  for (uint32_t c = 0; c < n_ctx; ++c) {
+    esl_ctx* x = ctxs[c];
+    if (int32_t rc = prepare_dc(x, opts, d_x[c], cold ? cold[c] : 0, d_iters[c], d_status[c],
+                                stats ? &stats[c] : nullptr, lanes[c]))
+      return rc;
+    ESL_CUDA(cudaStreamSynchronize(x->stream));
+    topos[c] = x->topo;
+    lpb[c] = lanes_per_cta(x, x->n_lanes, x->lanes_eff);
+    max_lpb = std::max(max_lpb, lpb[c]);
+    smem = std::max(smem, size_t(x->topo.prog_bytes) + size_t(lpb[c]) * x->topo.smem_doubles * 8);
+    for (uint32_t f = 0; f < x->n_lanes; f += lpb[c]) {
+      cta_ctx.push_back(c);
+      cta_first.push_back(f);
+    }
+  }
+  if (smem > size_t(227) * 1024) return c0->fail(ESL_NOT_ELIGIBLE, "a group CTA exceeds shared memory");
+  cudaStream_t s = c0->stream;
+  ESL_CUDA(upload(c0->d_group_topo, topos, s));
+  ESL_CUDA(upload(c0->d_group_lanes, lanes, s));
+  ESL_CUDA(upload(c0->d_group_cta_ctx, cta_ctx, s));
+  ESL_CUDA(upload(c0->d_group_cta_first, cta_first, s));
+  ESL_CUDA(upload(c0->d_group_lpb, lpb, s));
+  const LaneOpts o{opts->reltol, opts->abstol, opts->vntol, opts->residual_tol, opts->gmin, opts->max_iter,
+                   opts->init_fix, opts->iter_cap};
+  ESL_CUDA(cudaEventRecord(c0->ev0, s));
+  ESL_CUDA(launch_dc_newton_group(c0->d_group_topo.as<TopoDev>(), c0->d_group_lanes.as<LaneDev>(),
+                                  c0->d_group_cta_ctx.as<uint32_t>(), c0->d_group_cta_first.as<uint32_t>(),
+                                  c0->d_group_lpb.as<uint32_t>(), uint32_t(cta_ctx.size()), max_lpb, smem, o, s));
+  ESL_CUDA(cudaEventRecord(c0->ev1, s));
+  ESL_CUDA(cudaEventSynchronize(c0->ev1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c0->ev0, c0->ev1);
+  // lanes that left their tape: each context's host peels, then its own resume launches
+  for (uint32_t c = 0; c < n_ctx; ++c) {
+    esl_ctx* x = ctxs[c];
+    ctx = x;
+    uint32_t launches = 1;
+    for (;;) {
+      bool any = false;
+      if (int32_t rc = serve_pauses(x, stats ? &stats[c] : nullptr, &any)) return rc;
+      if (!any) break;
+      LaneDev R = lanes[c];
+      R.resume = 1;
+      ESL_CUDA(launch_dc_newton(x->topo, R, o, lanes_per_cta(x, x->n_lanes, x->lanes_eff), x->stream));
+      ++launches;
+    }
+    ESL_CUDA(cudaStreamSynchronize(x->stream));
+    if (stats) {
+      stats[c].kernel_ms = ms;
+      stats[c].launches = launches;
+      stats[c].lanes = x->n_lanes;
+      std::vector<uint32_t> status(x->n_lanes);
+      ESL_CUDA(cudaMemcpy(status.data(), d_status[c], x->n_lanes * 4, cudaMemcpyDeviceToHost));
+      for (uint32_t v : status) stats[c].converged += v == kConverged;
+    }
+  }
+  return ESL_OK;
+}
+
+int32_t esl_autotune(esl_ctx* ctx, const esl_newton_opts* opts, const double* x0, uint32_t* lanes_per_block) {
+  if (!ctx || !opts || ctx->n_lanes == 0) return ESL_INVALID_ARGUMENT;
+  const size_t N = ctx->n_lanes, n = ctx->pat.n;
+  std::vector<double> x(N * n);
+  std::vector<uint32_t> it(N), st(N);
+  esl_stats stats;
+  // the first solve builds the tape (and fixes the lanes that fit per CTA)
+  ctx->lanes_per_block = 0;
+  if (int32_t rc = esl_dc_solve(ctx, opts, x0, x.data(), it.data(), st.data(), &stats)) return rc;
+  uint32_t best = 0;
+  float best_ms = 0;
+  for (uint32_t cand : {1u, 2u, 4u, 8u}) {
+    if (cand > ctx->lanes_eff) break;
+    ctx->lanes_per_block = cand;
+    float t = 0;
+    for (int rep = 0; rep < 2; ++rep) {
+      if (int32_t rc = esl_dc_solve(ctx, opts, x0, x.data(), it.data(), st.data(), &stats)) return rc;
+      t = rep == 0 ? float(stats.kernel_ms) : std::min(t, float(stats.kernel_ms));
+    }
+    if (best == 0 || t < best_ms) {
+      best = cand;
+      best_ms = t;
+    }
+  }
+  ctx->lanes_per_block = best;
+  if (lanes_per_block) *lanes_per_block = best;
   return ESL_OK;
 }
 

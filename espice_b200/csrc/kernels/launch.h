@@ -35,6 +35,11 @@ cudaError_t launch_lu_lanes_mixed(const TopoDev& T, const uint2* seq, uint32_t n
                                   uint32_t n_seq_f, uint32_t n_lanes, const double* a, const double* rhs, double* dx,
                                   uint8_t* bad, uint8_t* refine, uint32_t warps, cudaStream_t s);
 
+// Uneven batching: one launch over the lanes of several topologies.
+cudaError_t launch_dc_newton_group(const TopoDev* d_topos, const LaneDev* d_lanes, const uint32_t* d_cta_ctx,
+                                   const uint32_t* d_cta_first, const uint32_t* d_ctx_lpb, uint32_t n_ctas,
+                                   uint32_t max_lpb, size_t smem, const LaneOpts& o, cudaStream_t s);
+
 // Fixed lane scratch of the allocation-free DC entry point: its size, the
 // device address of the array on the current device (looked up once per
 // device; the first call per device must precede any stream capture), and

@@ -1484,6 +1484,41 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
   if (tid == 0 && P.n_pts) P.n_pts[lane] = n_rec;
 }
 
+// Uneven batching: lanes of several topologies (circuits of different sizes)
+// in one launch. CTA b serves topology cta_ctx[b], lanes cta_first[b] ..
+// + ctx_lpb[that topology] (one warp each); it copies its topology's tables
+// into shared memory and stages that topology's programs, then runs the same
+// per-lane solve as dc_newton_kernel.
+__global__ void __launch_bounds__(256) dc_newton_group_kernel(const TopoDev* Ts, const LaneDev* Ls,
+                                                              const uint32_t* cta_ctx, const uint32_t* cta_first,
+                                                              const uint32_t* ctx_lpb, LaneOpts o) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ TopoDev T;
+  __shared__ LaneDev L;
+  const uint32_t c = cta_ctx[blockIdx.x];
+  if (threadIdx.x == 0) {
+    T = Ts[c];
+    L = Ls[c];
+  }
+  __syncthreads();
+  double* lanes_smem = stage_programs(T, smem_raw);
+  const uint32_t prog = saddr(smem_raw);
+  const int tid = threadIdx.x & 31;
+  const uint32_t w = threadIdx.x >> 5;
+  const uint32_t lane = cta_first[blockIdx.x] + w;
+  if (w < ctx_lpb[c] && lane < L.n_lanes)
+    dc_solve_lane(T, L, o, prog, lanes_smem + size_t(w) * T.smem_doubles, lane, tid);
+}
+
+cudaError_t launch_dc_newton_group(const TopoDev* d_topos, const LaneDev* d_lanes, const uint32_t* d_cta_ctx,
+                                   const uint32_t* d_cta_first, const uint32_t* d_ctx_lpb, uint32_t n_ctas,
+                                   uint32_t max_lpb, size_t smem, const LaneOpts& o, cudaStream_t s) {
+  cudaError_t e = cudaFuncSetAttribute(dc_newton_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  dc_newton_group_kernel<<<n_ctas, 32 * max_lpb, smem, s>>>(d_topos, d_lanes, d_cta_ctx, d_cta_first, d_ctx_lpb, o);
+  return cudaGetLastError();
+}
+
 // Transient lanes: a persistent grid, each CTA staging the programs once,
 // each warp running one lane's transient to its end.
 __global__ void __launch_bounds__(256) tran_kernel(TopoDev T, LaneDev L, TranDev P, LaneOpts o) {

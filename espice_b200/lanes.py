@@ -28,7 +28,7 @@ LANE_CONVERGED, LANE_MAX_ITER, LANE_SINGULAR, LANE_NEED_SOLVE = 1, 2, 3, 4
 EXPORTS = ["esl_create", "esl_destroy", "esl_last_error", "esl_dims", "esl_set_lanes",
            "esl_dc_solve", "esl_dc_solve_device", "esl_dc_solve_device_static", "esl_tape", "esl_lu_replay_device",
            "esl_tape_size", "esl_pattern", "esl_compile_tape", "esl_tran", "esl_tran_device", "esl_lu_lanes_device",
-           "esl_lu_lanes_mixed_device"]
+           "esl_lu_lanes_mixed_device", "esl_group_dc_solve_device", "esl_autotune"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 f64p = ctypes.POINTER(ctypes.c_double)
@@ -282,6 +282,17 @@ class DcLanes:
                     "esl_tran_device")
         return ms.value
 
+    def autotune(self, x0=None, opts=None):
+        """Times lanes per CTA 1/2/4/8 on the current lanes and keeps the fastest."""
+        opts = opts or newton_opts()
+        best = ctypes.c_uint32(0)
+        xp = None
+        if x0 is not None:
+            x0 = np.ascontiguousarray(np.broadcast_to(x0, (self.n_lanes, self.n)), np.float64)
+            xp = _p(x0, f64p)
+        self._check(self._L.esl_autotune(self._ctx, ctypes.byref(opts), xp, ctypes.byref(best)), "esl_autotune")
+        return best.value
+
     def tape(self):
         q = np.zeros(self.n, np.uint32)
         pinv = np.zeros(self.n, np.uint32)
@@ -329,3 +340,19 @@ class DcLanes:
         self._check(self._L.esl_tape_size(self._ctx, ctypes.byref(nu), ctypes.byref(nl),
                                           ctypes.byref(ntv)), "esl_tape_size")
         return nu.value, nl.value, ntv.value
+
+
+def group_solve_device(ctxs, d_xs, d_iters, d_status, cold=None, opts=None):
+    """One launch over the lanes of several DcLanes contexts (uneven batching);
+    device pointers per context. Returns each context's stats."""
+    opts = opts or newton_opts()
+    k = len(ctxs)
+    arr = (ctypes.c_void_p * k)(*[c._ctx for c in ctxs])
+    px = (ctypes.c_void_p * k)(*d_xs)
+    pi = (ctypes.c_void_p * k)(*d_iters)
+    ps = (ctypes.c_void_p * k)(*d_status)
+    cl = (ctypes.c_int * k)(*[int(bool(v)) for v in (cold or [False] * k)])
+    stats = (Stats * k)()
+    rc = ctxs[0]._L.esl_group_dc_solve_device(arr, ctypes.c_uint32(k), ctypes.byref(opts), px, cl, pi, ps, stats)
+    ctxs[0]._check(rc, "esl_group_dc_solve_device")
+    return [s.as_dict() for s in stats]

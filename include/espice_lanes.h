@@ -213,6 +213,22 @@ int32_t esl_tran_device(esl_ctx *ctx, const esl_tran_opts *opts, double *d_x, ui
                         const uint32_t *d_probes, uint32_t n_probes, uint32_t max_pts,
                         double *d_t, double *d_v, uint32_t *d_n_pts, float *ms);
 
+/* Uneven batching: the DC solves of n_ctx contexts (circuits of any sizes,
+ * one device) in one launch, each context's lanes with its own topology and
+ * tape; per context its device buffers as esl_dc_solve_device takes them,
+ * cold[c] (NULL: all warm) and stats[c] (may be NULL). Lanes that leave
+ * their tape are served per context afterwards. No reference counterpart:
+ * the reference's lanes run one topology per round (gpu_lanes.zig:349). */
+int32_t esl_group_dc_solve_device(esl_ctx *const *ctxs, uint32_t n_ctx, const esl_newton_opts *opts,
+                                  double *const *d_x, const int *cold, uint32_t *const *d_iters,
+                                  uint32_t *const *d_status, esl_stats *stats);
+
+/* Picks the context's lanes per CTA (1, 2, 4 or 8, as shared memory allows)
+ * by timing its DC solve from x0 (NULL: cold) on its current lanes; keeps
+ * the fastest for later launches and returns it in *lanes_per_block. */
+int32_t esl_autotune(esl_ctx *ctx, const esl_newton_opts *opts, const double *x0,
+                     uint32_t *lanes_per_block);
+
 /* The lead lane's pivot tape after the last solve (buildTab,
  * lane_kernels.zig:321-345): q[n], pinv[n]; counts[0] = |L|, counts[1] = |U|,
  * counts[2] = refactor levels, counts[3] = solve levels. */
