@@ -122,9 +122,12 @@ __device__ __forceinline__ double* stage_programs(const TopoDev& T, unsigned cha
 // Device evaluation: every instance of every batch, strided over the warp,
 // each writing its own staging cells (no shared cell, no atomics).
 __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, bool lim_active,
-                         const SimDev& sim, int tid) {
+                         const SimDev& sim, int tid, bool charges_only = false) {
   for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
     const BatchDev& B = T.b[bi];
+    // the charge re-read (the reference's evalQ) needs only the batches
+    // that carry charge: capacitors, diodes, MOSFETs with charge cells
+    if (charges_only && !(B.type == kC || B.type == kD || (B.type == kM && B.stride >= kStageM))) continue;
     const int s = static_cast<int>(B.count);
     for (uint32_t i = tid; i < B.count; i += 32) {
       const uint32_t* nd = B.nodes + size_t(i) * B.nt;
@@ -1306,7 +1309,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
     }
     // charge histories, flat at q(x_op); no dynamic current yet
     sim.kind = 1;
-    eval_all(T, rec, m, false, sim, tid);
+    eval_all(T, rec, m, false, sim, tid, true);
     __syncwarp();
     row_charges(T, m, qh + n, tid);
     state_charges(T, rec, m.x, qt + nq, tid);
@@ -1385,7 +1388,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
       }
       double dt_next = steps == 0 ? dt : fmin(dt * 2.0, dt_max);
       if (has_charge) {
-        eval_all(T, rec, m, false, sim, tid);
+        eval_all(T, rec, m, false, sim, tid, true);
         __syncwarp();
         row_charges(T, m, slot(qh, n, 0), tid);
         state_charges(T, rec, m.x, slot(qt, nq, 0), tid);
