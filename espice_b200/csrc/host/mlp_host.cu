@@ -335,7 +335,7 @@ int32_t esl_mlp_predict(esl_mlp* m, const float* d_x, uint32_t n, float* d_y) {
   if (!m || !d_x || !d_y || n == 0) return ESL_MLP_INVALID_ARGUMENT;
   cudaSetDevice(m->device);
   cudaStream_t s = m->stream;
-  const uint32_t chunk = 8192;
+  const uint32_t chunk = 32768;
   if (int32_t rc = ensure_batch(m, int(chunk))) return rc;
   MLP_CUDA(cudaMemsetAsync(m->gerr.p, 0, 4, s));
   const int kin = m->layers[0]->k;

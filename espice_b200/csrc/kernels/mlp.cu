@@ -12,6 +12,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "mlp.h"
@@ -67,19 +68,28 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   return false;
 }
 
+// 16-byte asynchronous copy global -> shared; src_bytes 0 fills zeros.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+
 // C = A (M x K, row-major BF16) . B (N x K, row-major BF16)^T with FP32
 // accumulation; grid (ceil(M / 128), N / bn), block 128 threads. The
 // epilogue adds bias[n] when given, stores the FP32 result to c (ldc) when
 // given, and tanh (act = 1) or identity of it as BF16 to h (ldh) when given.
 // Rows >= M are read as zero and not stored. K is a multiple of 16 (zero
 // padded by the caller), bn a multiple of 16 in [16, 256].
+//
+// Two staging buffers: while the MMAs of K chunk k run, the cp.async copies
+// of chunk k + 1 fill the other buffer, whose previous reader (the MMAs of
+// chunk k - 1) is known complete through the mbarrier.
 __global__ void __launch_bounds__(kThreads) gemm_bf16_tc(const __nv_bfloat16* __restrict__ a, int lda,
                                                          const __nv_bfloat16* __restrict__ b, int ldb, int M, int K,
                                                          int bn, const float* __restrict__ bias, float* c, int ldc,
                                                          __nv_bfloat16* h, int ldh, int act, int* err) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  unsigned char* sa = smem;                           // 128 x 64 BF16 = 16 KB
-  unsigned char* sb = smem + kTileM * kTileK * 2;     // bn x 64 BF16
+  const uint32_t a_bytes = kTileM * kTileK * 2, b_bytes = uint32_t(bn) * kTileK * 2;
+  unsigned char* buf[2] = {smem, smem + a_bytes + b_bytes};
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -101,32 +111,43 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tc(const __nv_bfloat16* __
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = tmem_slot;
   const uint32_t idesc = encode_idesc(uint32_t(bn));
-  uint32_t parity = 0;
-  bool ok = true;
+  const int n_chunks = (K + kTileK - 1) / kTileK;
 
-  for (int k0 = 0; k0 < K; k0 += kTileK) {
-    const int kc = min(kTileK, K - k0);  // a multiple of 16
-    // stage the chunk: 8 BF16 (16 B) per thread per step, zero beyond M / K
+  // stage chunk q into buffer q & 1: 16 B per copy, zero beyond M and K
+  auto stage = [&](int q) {
+    const int k0 = q * kTileK, kc = min(kTileK, K - k0);
+    unsigned char* sa = buf[q & 1];
+    unsigned char* sb = sa + a_bytes;
     for (int i = tid; i < kTileM * (kTileK / 8); i += kThreads) {
       const int r = i / (kTileK / 8), kg = (i % (kTileK / 8)) * 8;
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (m0 + r < M && kg < kc) v = *reinterpret_cast<const uint4*>(a + size_t(m0 + r) * lda + k0 + kg);
-      *reinterpret_cast<uint4*>(sa + core_offset(r, kg)) = v;
+      const bool in = m0 + r < M && kg < kc;
+      const __nv_bfloat16* src = a + size_t(in ? m0 + r : 0) * lda + (in ? k0 + kg : 0);
+      cp_async16(smem_u32(sa + core_offset(r, kg)), src, in ? 16u : 0u);
     }
     for (int i = tid; i < bn * (kTileK / 8); i += kThreads) {
       const int r = i / (kTileK / 8), kg = (i % (kTileK / 8)) * 8;
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (kg < kc) v = *reinterpret_cast<const uint4*>(b + size_t(n0 + r) * ldb + k0 + kg);
-      *reinterpret_cast<uint4*>(sb + core_offset(r, kg)) = v;
+      const bool in = kg < kc;
+      const __nv_bfloat16* src = b + size_t(n0 + r) * ldb + (in ? k0 + kg : 0);
+      cp_async16(smem_u32(sb + core_offset(r, kg)), src, in ? 16u : 0u);
     }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+
+  uint32_t parity = 0;
+  bool ok = true;
+  stage(0);
+  for (int q = 0; q < n_chunks; ++q) {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");  // chunk q has landed
     asm volatile("fence.proxy.async.shared::cta;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
+    const int kc = min(kTileK, K - q * kTileK);
     if (tid == 0) {
+      const uint32_t sa = smem_u32(buf[q & 1]), sb = sa + a_bytes;
       for (int j = 0; j < kc / 16; ++j) {
-        const uint64_t da = encode_sdesc(smem_u32(sa) + j * 256, 128, 1024);
-        const uint64_t db = encode_sdesc(smem_u32(sb) + j * 256, 128, 1024);
-        const uint32_t acc = (k0 > 0 || j > 0) ? 1u : 0u;
+        const uint64_t da = encode_sdesc(sa + j * 256, 128, 1024);
+        const uint64_t db = encode_sdesc(sb + j * 256, 128, 1024);
+        const uint32_t acc = (q > 0 || j > 0) ? 1u : 0u;
         const uint32_t z = 0;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -137,7 +158,8 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tc(const __nv_bfloat16* __
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
           smem_u32(&bar)));
     }
-    // the MMAs read the staged chunk: wait before it is overwritten
+    // the other buffer's last reader (chunk q - 1) completed at the previous wait
+    if (q + 1 < n_chunks) stage(q + 1);
     ok = mbar_wait(smem_u32(&bar), parity) && ok;
     parity ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;");
@@ -258,9 +280,10 @@ cudaError_t launch_gemm_bf16(const __nv_bfloat16* a, int lda, const __nv_bfloat1
   if (M <= 0 || N <= 0 || K <= 0 || K % 16 || N % 16 || lda % 8 || ldb % 8) return cudaErrorInvalidValue;
   int bn = N <= 256 ? N : 128;
   while (N % bn) bn -= 16;
-  // 100 KB of dynamic shared memory: at most two CTAs per SM, so their
-  // tensor-memory allocations (at most 256 columns each) fit in the SM's 512.
-  const size_t smem = 100 * 1024;
+  // Two staging buffers of A (16 KB) and B (bn x 64 BF16, at most 32 KB);
+  // at least 100 KB per CTA, so at most two CTAs share an SM and their
+  // tensor-memory allocations (at most 256 columns each) fit in its 512.
+  const size_t smem = std::max<size_t>(100 * 1024, 2 * (size_t(kTileM) * kTileK * 2 + size_t(bn) * kTileK * 2));
   cudaError_t e = cudaFuncSetAttribute(gemm_bf16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   dim3 grid((M + kTileM - 1) / kTileM, N / bn);
