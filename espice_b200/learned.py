@@ -50,16 +50,18 @@ class LearnedWarmStart:
         return out.double()
 
 
-def solve(ctx, fallback, ws, slots, values, x_nominal, k=8, opts=None):
+def solve(ctx, fallback, ws, slots, values, x_nominal, k=8, opts=None, d_values=None):
     """Solves every lane of `ctx` (lanes already set to `values`) from the
     learned guess with at most `k` Newton iterations, then the lanes that did
     not converge again from `x_nominal` on `fallback` (a DcLanes of the same
-    circuit). Returns (x [N][n] device tensor, iterations [N] (both passes),
-    converged mask [N] host, number of fallback lanes)."""
+    circuit). `d_values`: the values already on the device as float32 (as the
+    lanes' records are), else they are uploaded. Returns (x [N][n] device
+    tensor, iterations [N] (both passes), converged mask [N] host, number of
+    fallback lanes)."""
     import torch
     opts = opts or lanes.newton_opts()
     N = values.shape[0]
-    d_vals = torch.tensor(values, dtype=torch.float32, device="cuda")
+    d_vals = d_values if d_values is not None else torch.tensor(values, dtype=torch.float32, device="cuda")
     d_x = ws.predict(d_vals, N)
     d_it = torch.zeros(N, dtype=torch.int32, device="cuda")
     d_st = torch.zeros(N, dtype=torch.int32, device="cuda")
