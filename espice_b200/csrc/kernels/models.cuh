@@ -28,7 +28,7 @@ __device__ __forceinline__ double div_rn(double a, double b) {
 struct SimDev {
   double t;          // time (transient)
   double src_scale;  // source-stepping factor
-  int kind;          // 0 static (.op / .dc), 1 transient
+  int kind;          // 0 static (.op / .dc), 1 transient, 2 transient op
 };
 
 // PULSE (vsource.va:211-222); p = the 10 V-source fields.
@@ -50,7 +50,8 @@ __device__ __forceinline__ double pulse_value(const double* p, int stride, doubl
   return v1;
 }
 
-// V source value: static analyses bias at `dc`; the transient at its wave.
+// V source value: static analyses (kind 0) bias at `dc`; the transient and
+// its own operating point (kinds 1, 2) at the wave.
 __device__ __forceinline__ double vsource_value(const double* p, int stride, const SimDev& sim) {
   double out = p[0];
   if (sim.kind != 0 && p[stride] == 1.0) out = pulse_value(p, stride, sim.t);

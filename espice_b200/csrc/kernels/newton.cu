@@ -180,7 +180,7 @@ __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, 
           break;
         case kM:
           mos1_stamp(r, s, m.x[nd[0]], m.x[nd[1]], m.x[nd[2]], m.x[nd[3]], m.x[nd[4]], m.x[nd[5]],
-                     lim_active ? m.lim + B.lim_off + 3 * i : nullptr, sim.kind != 0 && B.stride >= kStageM, st);
+                     lim_active ? m.lim + B.lim_off + 3 * i : nullptr, sim.kind == 1 && B.stride >= kStageM, st);
           break;
         default:
           break;
@@ -1264,11 +1264,12 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
   for (int k = 0; k < kTsN; ++k) stat[k] = 0;
   init_consts(T, m.v, tid);
 
-  // operating point: cold start with the junction seeds, MODEINITFIX
+  // operating point: cold start with the junction seeds, MODEINITFIX; the
+  // source waves at t = 0 (kind 2: vsource.va:214-219)
   SimDev sim;
   sim.t = 0.0;
   sim.src_scale = 1.0;
-  sim.kind = 0;
+  sim.kind = 2;
   for (uint32_t i = tid; i < n; i += 32) m.x[i] = 0.0;
   for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
     const BatchDev& B = T.b[bi];

@@ -238,7 +238,7 @@ void mos1_eval(const uint32_t *nd, const double *prm, const double *der, const d
     o->J[4][0] = -gdr; o->J[4][1] = gmg; o->J[4][3] = gbb - gbd; o->J[4][4] = (gdd + gbd) + gdr; o->J[4][5] = -gsum;
     o->J[5][1] = -gmg; o->J[5][2] = -gsr; o->J[5][3] = (-gbb) - gbs; o->J[5][4] = -gdd; o->J[5][5] = (gsum + gbs) + gsr;
 
-    if (sim->kind != 0 && der[MD_HASQ] != 0.0) {
+    if (sim->kind == 1 && der[MD_HASQ] != 0.0) {
         double qbd, cbdc, qbs, cbsc;
         jchg(vbd, der[MD_CZBD], der[MD_CZBDSW], der[MD_PBT], der[MD_MJ], der[MD_MJSW], der[MD_FC],
              der[MD_F2D], der[MD_F3D], der[MD_F4D], &qbd, &cbdc);

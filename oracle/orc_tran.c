@@ -156,9 +156,12 @@ static void tran_lane(ckt_t *k, const orc_tran_opts *o, rec_t *rec, uint32_t *st
     double *trial = (double *)calloc(n, sizeof(double));
     memset(st, 0, sizeof(uint32_t) * ORC_TS_N);
 
-    /* operating point: sources at their static value, cold start */
+    /* operating point, cold start: the transient's own operating point
+       evaluates the source waves at t = 0 (vsource.va:214-219, the ic phase
+       where analysis("tran") is true), so a PULSE source with an explicit DC
+       value biases at its first level, not at DC */
     orc_newton_opts op = {o->reltol, o->abstol, o->vntol, 1e-9, 0.0, 100};
-    k->sim.kind = 0;
+    k->sim.kind = 2;
     k->sim.t = 0.0;
     k->tran = 0;
     ckt_cold_start(k, cur);

@@ -35,6 +35,18 @@ FIXTURES = [
     "dc/device_mos1_output",
     "dc/bench_mosfet_cmos_inverter",
     "tran/device_mos1_large_signal",
+    "dc/device_mos1_body_effect",
+    "dc/device_mos1_pmos",
+    "dc/device_mos1_subthreshold",
+    "dc/bench_sweep_cmos_inv_sizing",
+    # transients: RC networks and MOS1 under PULSE sources
+    "tran/bench_tran_rc_pulse",
+    "tran/bench_medium_rc_ladder_50",
+    "tran/bench_digital_rc_filter_chain",
+    "tran/bench_digital_buffer_rc",
+    "tran/bench_mosfet_nmos_cs",
+    "tran/rc_pulse_history_trap",
+    "tran/finite_rise_positive",
 ]
 
 

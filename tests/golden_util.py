@@ -80,10 +80,12 @@ def solve_tran(g, max_pts=1_000_000):
     from oracle import oracle
     deck = Deck(g["deck"])
     fr = deck.circuit().freeze()
-    _, tstep, tstop = deck.analysis[:3]
+    _, tstep, tstop, tstart, tmax = deck.analysis
+    assert tstart == 0.0, "a TSTART after 0 is not supported"
+    assert deck.options.get("method", "trap") == "trap", "the trapezoidal integrator only"
     cols = list(g["plots"][0]["columns"])
     probes = [fr.unknown(c) for c in cols]
-    o = oracle.tran_opts(tstop, tstep, **deck.newton_opts())
+    o = oracle.tran_opts(tstop, tstep, tmax, **deck.newton_opts())
     t, v, npts, stats, _ = oracle.tran(fr, [], np.zeros((1, 1)), o, probes, max_pts=max_pts)
     n = int(npts[0])
     return fr, t[0, :n], v[0, :n], cols, dict(zip(oracle.TS_FIELDS, stats[0].tolist()))

@@ -32,7 +32,10 @@ def _kv(tokens):
     for t in tokens:
         if "=" in t:
             k, v = t.split("=", 1)
-            out[k.lower()] = num(v)
+            try:
+                out[k.lower()] = num(v)
+            except ValueError:
+                out[k.lower()] = v.lower()
     return out
 
 
@@ -75,8 +78,10 @@ class Deck:
             elif low.split()[0] == ".op":
                 self.analysis = ("op",)
             elif low.startswith(".tran"):
-                t = s.split()
-                self.analysis = ("tran", num(t[1]), num(t[2]))
+                t = [v for v in s.split() if v.lower() != "uic"]
+                tstart = num(t[3]) if len(t) > 3 else 0.0
+                tmax = num(t[4]) if len(t) > 4 else 0.0
+                self.analysis = ("tran", num(t[1]), num(t[2]), tstart, tmax)
             elif low.startswith(".temp"):
                 self.temp = num(s.split()[1])
             elif low.startswith(".end"):

@@ -94,3 +94,35 @@ def test_ring_oscillator_short_window():
                              max_pts=2500)
     _check_parity(res_g, res_o)
     assert (res_g[3][:, 0] == lanes.TRAN_DONE).all()
+
+
+TRAN_FIXTURES = gu.names("tran__")
+
+
+@pytest.mark.parametrize("name", TRAN_FIXTURES)
+def test_golden_transients_as_gpu_lanes(name):
+    """Every reference transient fixture as GPU lanes at the deck's own
+    options and .tran card (TMAX included): the oracle's step decisions and
+    waveforms, and the reference's ngspice waveform at its tolerances."""
+    g = gu.load(name)
+    deck = Deck(g["deck"])
+    fr = deck.circuit().freeze()
+    cols = list(g["plots"][0]["columns"])
+    probes = [fr.unknown(c) for c in cols]
+    _, tstep, tstop, tstart, tmax = deck.analysis
+    assert tstart == 0.0
+    opts = deck.newton_opts()
+    go = lanes.tran_opts(tstop, tstep, tmax, max_steps=200_000, **opts)
+    oo = oracle.tran_opts(tstop, tstep, tmax, max_steps=200_000, **opts)
+    values = np.zeros((2, 1))
+    ctx = lanes.DcLanes(fr)
+    ctx.set_lanes([], values)
+    res_g = ctx.tran(go, probes, 20_000)
+    ctx.close()
+    res_o = oracle.tran(fr, [], values, oo, probes, 20_000)
+    _check_parity(res_g, res_o)
+    tg, vg, ng, sg, _, _ = res_g
+    assert (sg[:, 0] == lanes.TRAN_DONE).all()
+    n = int(ng[0])
+    for col, worst in gu.score_tran(g, tg[0, :n], vg[0, :n], cols):
+        assert worst <= 1.0, f"{name} {col}: {worst:.3g}x the fixture tolerance"
