@@ -20,54 +20,99 @@ Op encode(uint32_t kind, uint32_t dst, uint32_t a, uint32_t b) {
   return o;
 }
 
-// Levels: an op runs after the last write of each value it reads, after
-// the last write of its destination, and after every earlier read of its
-// destination by another op (no value is overwritten before it is read).
-// Each level is then packed into rows of kRow ops (one per thread) of one
-// kind.
-// Padding ops keep the row's kind and write the sink slot (space - 1) from
-// the constants 1.0 (space - 2) and 0.0 (space - 3): a multiply-subtract of
-// 1.0 * 0.0, or 1.0 / 1.0 (divisions read their dividend at b).
-void pack(const std::vector<SeqOp>& seq, uint32_t space, std::vector<Op>& rows,
-          std::vector<uint32_t>& kinds, uint32_t& n_rows, uint32_t& n_levels) {
-  std::vector<int32_t> lw(space, -1), lr(space, -1), level(seq.size());
-  int32_t top = -1;
-  for (size_t i = 0; i < seq.size(); ++i) {
+bool is_div(uint32_t kind) { return kind == kOpDivGrowth || kind == kOpDivScaled || kind == kOpDivY; }
+
+// Dependences: an op follows the last write of each value it reads, the
+// last write of its destination (a value's updates keep their sequential
+// order, so every sum rounds as in the column replay), and every read of its
+// destination since that write (no value is overwritten before it is read).
+// The ops are then list-scheduled into rows of kRow ops (one per thread),
+// each row one class, the divisions or the multiply-subtracts (the kernel's
+// two warp-uniform paths; the checks inside a path are per op): row by row,
+// the class of the ready op with the longest path to the end of the program,
+// then up to kRow ready ops of that class, longest paths first. An op's
+// successors become ready only for a later row. `n_levels` is the longest
+// dependence chain, the least number of rows any packing can have.
+// Padding ops write the sink slot (space - 1) from the constants 1.0
+// (space - 2) and 0.0 (space - 3): 1.0 / 1.0 in a division row, a
+// zero-skipped 1.0 * 0.0 in a multiply-subtract row.
+void pack(const std::vector<SeqOp>& seq, uint32_t space, std::vector<Op>& rows, uint32_t& n_rows,
+          uint32_t& n_levels) {
+  const size_t n = seq.size();
+  std::vector<int32_t> last_write(space, -1);
+  std::vector<std::vector<uint32_t>> readers(space);
+  std::vector<uint32_t> succ_ptr(n + 1, 0), n_pred(n, 0);
+  std::vector<std::pair<uint32_t, uint32_t>> edges;  // (pred, succ)
+  std::vector<uint32_t> preds;
+  for (size_t i = 0; i < n; ++i) {
     const SeqOp& s = seq[i];
-    int32_t l = std::max(lw[s.dst], lr[s.dst]) + 1;
-    if (s.a != kNone) l = std::max(l, lw[s.a] + 1);
-    if (s.b != kNone) l = std::max(l, lw[s.b] + 1);
-    level[i] = l;
-    lw[s.dst] = l;
-    if (s.a != kNone) lr[s.a] = std::max(lr[s.a], l);
-    if (s.b != kNone) lr[s.b] = std::max(lr[s.b], l);
-    top = std::max(top, l);
+    preds.clear();
+    for (uint32_t src : {s.a, s.b})
+      if (src != kNone && last_write[src] >= 0) preds.push_back(uint32_t(last_write[src]));
+    if (last_write[s.dst] >= 0) preds.push_back(uint32_t(last_write[s.dst]));
+    for (uint32_t r : readers[s.dst])
+      if (r != i) preds.push_back(r);
+    std::sort(preds.begin(), preds.end());
+    preds.erase(std::unique(preds.begin(), preds.end()), preds.end());
+    for (uint32_t p : preds) edges.push_back({p, uint32_t(i)});
+    n_pred[i] = uint32_t(preds.size());
+    last_write[s.dst] = int32_t(i);
+    readers[s.dst].clear();
+    for (uint32_t src : {s.a, s.b})
+      if (src != kNone) readers[src].push_back(uint32_t(i));
   }
-  n_levels = uint32_t(top + 1);
-  std::vector<std::vector<uint32_t>> by(n_levels);
-  for (size_t i = 0; i < seq.size(); ++i) by[level[i]].push_back(uint32_t(i));
+  for (const auto& e : edges) ++succ_ptr[e.first + 1];
+  for (size_t i = 0; i < n; ++i) succ_ptr[i + 1] += succ_ptr[i];
+  std::vector<uint32_t> succ(edges.size()), fill(succ_ptr.begin(), succ_ptr.end() - 1);
+  for (const auto& e : edges) succ[fill[e.first]++] = e.second;
+  // height: ops on the longest path from this op to the end, inclusive
+  std::vector<uint32_t> height(n, 1);
+  uint32_t top = 0;
+  for (size_t i = n; i-- > 0;) {
+    for (uint32_t e = succ_ptr[i]; e < succ_ptr[i + 1]; ++e) height[i] = std::max(height[i], height[succ[e]] + 1);
+    top = std::max(top, height[i]);
+  }
+  n_levels = top;
+  // ready queues per class, longest path first, then sequence order
+  auto later = [&](uint32_t x, uint32_t y) { return height[x] != height[y] ? height[x] < height[y] : x > y; };
+  std::vector<uint32_t> ready[2];
+  for (size_t i = 0; i < n; ++i)
+    if (n_pred[i] == 0) ready[is_div(seq[i].kind)].push_back(uint32_t(i));
+  for (auto& q : ready) std::make_heap(q.begin(), q.end(), later);
   rows.clear();
-  kinds.clear();
   n_rows = 0;
-  for (auto& ids : by) {
-    std::stable_sort(ids.begin(), ids.end(), [&](uint32_t x, uint32_t y) { return seq[x].kind < seq[y].kind; });
-    for (size_t at = 0; at < ids.size();) {
-      const uint32_t kind = seq[ids[at]].kind;
-      size_t end = at;
-      while (end < ids.size() && end - at < kRow && seq[ids[end]].kind == kind) ++end;
-      for (uint32_t t = 0; t < kRow; ++t) {
-        if (at + t < end) {
-          const SeqOp& s = seq[ids[at + t]];
-          rows.push_back(encode(s.kind, s.dst, s.a, s.b));
-        } else {
-          const bool div = kind == kOpDivGrowth || kind == kOpDivScaled || kind == kOpDivY;
-          rows.push_back(encode(kind, space - 1, space - 2, div ? space - 2 : space - 3));
+  std::vector<uint32_t> row;
+  while (!ready[0].empty() || !ready[1].empty()) {
+    int c;
+    if (ready[0].empty()) c = 1;
+    else if (ready[1].empty()) c = 0;
+    else c = later(ready[0].front(), ready[1].front()) ? 1 : 0;
+    auto& q = ready[c];
+    row.clear();
+    while (!q.empty() && row.size() < kRow) {
+      std::pop_heap(q.begin(), q.end(), later);
+      row.push_back(q.back());
+      q.pop_back();
+    }
+    for (uint32_t t = 0; t < kRow; ++t) {
+      if (t < row.size()) {
+        const SeqOp& s = seq[row[t]];
+        rows.push_back(encode(s.kind, s.dst, s.a, s.b));
+      } else {
+        rows.push_back(c ? encode(kOpDivY, space - 1, space - 2, space - 2)
+                         : encode(kOpSubNz, space - 1, space - 2, space - 3));
+      }
+    }
+    ++n_rows;
+    for (uint32_t i : row)
+      for (uint32_t e = succ_ptr[i]; e < succ_ptr[i + 1]; ++e) {
+        const uint32_t j = succ[e];
+        if (--n_pred[j] == 0) {
+          auto& qj = ready[is_div(seq[j].kind)];
+          qj.push_back(j);
+          std::push_heap(qj.begin(), qj.end(), later);
         }
       }
-      kinds.push_back(kind);
-      ++n_rows;
-      at = end;
-    }
   }
 }
 
@@ -114,7 +159,7 @@ Programs compile_tape(const SparseLu& lu) {
     for (uint32_t q = lu.lp[k]; q < lu.lp[k + 1]; ++q) a.push_back({kOpSubNz, y0 + lu.li[q], lx0 + q, y0 + k});
   }
   P.nv = P.ntv + n + 3;
-  pack(a, P.nv, P.a_ops, P.a_kind, P.a_rows, P.a_levels);
+  pack(a, P.nv, P.a_ops, P.a_rows, P.a_levels);
   P.a_nops = uint32_t(a.size());
 
   std::vector<uint8_t> written(P.ntv, 0);
@@ -132,7 +177,7 @@ Programs compile_tape(const SparseLu& lu) {
     b.push_back({kOpDivY, y0 + k, P.nu + k, y0 + k});
     for (uint32_t p = lu.up[k]; p < lu.up[k + 1]; ++p) b.push_back({kOpSubNz, y0 + lu.ui[p], p, y0 + k});
   }
-  pack(b, P.nv, P.b_ops, P.b_kind, P.b_rows, P.b_levels);
+  pack(b, P.nv, P.b_ops, P.b_rows, P.b_levels);
   P.b_nops = uint32_t(b.size());
   return P;
 }

@@ -7,9 +7,10 @@
 // Program A is the refactor with the forward substitution through unit L
 // merged in (a column's forward updates run as soon as its L entries and
 // y entry are final, overlapping later columns' refactor); program B is the
-// back substitution through U. Each is level-scheduled and packed in rows of
-// 32 ops of one kind, one op per thread of the lane's warp, padded with
-// no-ops, so every branch on the kind is uniform across the warp.
+// back substitution through U. Each is list-scheduled into rows of 32 ops,
+// one op per thread of the lane's warp, padded with no-ops; a row holds
+// divisions only or multiply-subtracts only, so the kernel's branch between
+// the two is uniform across the warp.
 #pragma once
 
 #include <cstdint>
@@ -30,9 +31,7 @@ struct Programs {
   std::vector<uint32_t> fill;      // tape values no pattern slot writes
   std::vector<Op> a_ops;           // rows x 32: refactor + forward solve
   std::vector<Op> b_ops;           // rows x 32: back solve
-  std::vector<uint32_t> a_kind;    // per row: the one OpKind every op of the row has
-  std::vector<uint32_t> b_kind;
-  uint32_t a_rows = 0, b_rows = 0, a_levels = 0, b_levels = 0;
+  uint32_t a_rows = 0, b_rows = 0, a_levels = 0, b_levels = 0;  // levels: longest chain
   uint32_t a_nops = 0, b_nops = 0; // real ops (no padding)
   std::vector<uint8_t> l_scaled;   // per L entry: its column took the row-scaled pivot
   uint64_t flops = 0;              // refactor multiply-subtracts (the census F)
