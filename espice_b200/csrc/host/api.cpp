@@ -484,6 +484,62 @@ GatherProgram build_gather_program(const esl_ctx* ctx, const Programs& P) {
   return G;
 }
 
+// The transient companion's cells (integrator.zig Hook): every row with
+// charge cells (its charge sum; dst pair: the row, its y value) and then
+// every pattern slot with capacitance cells (its capacitance sum; dst pair:
+// the tape value, the diagonal copy or the sink), each part sorted by list
+// length. Rows and slots without such cells are left out: their companion
+// terms are exactly zero and their values, sums from +0.0, are never -0.0,
+// so adding the zero terms would change no bit.
+GatherProgram build_companion_program(const esl_ctx* ctx, const Programs& P, uint32_t& n_row_groups) {
+  const uint32_t n = ctx->pat.n, nnz = ctx->pat.nnz();
+  const LaneLayout L = lane_layout(n, P.ntv, ctx->n_stage, ctx->nlim);
+  struct Cell {
+    std::vector<uint32_t> src;
+    uint32_t d0, d1;
+  };
+  auto by_len = [](const Cell& a, const Cell& b) { return a.src.size() > b.src.size(); };
+  std::vector<Cell> rows, slots;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (ctx->q_ptr[i + 1] == ctx->q_ptr[i]) continue;
+    Cell c{{}, i, L.y + ctx->lead.pinv[i]};
+    for (uint32_t e = ctx->q_ptr[i]; e < ctx->q_ptr[i + 1]; ++e) c.src.push_back(L.st + ctx->q_src[e]);
+    rows.push_back(std::move(c));
+  }
+  for (uint32_t p = 0; p < nnz; ++p) {
+    if (ctx->c_ptr[p + 1] == ctx->c_ptr[p]) continue;
+    Cell c{{}, L.tv + P.amap[p], ctx->slot_row[p] != kNoDiag ? L.diag + ctx->slot_row[p] : L.sink};
+    for (uint32_t e = ctx->c_ptr[p]; e < ctx->c_ptr[p + 1]; ++e) c.src.push_back(L.st + ctx->c_src[e]);
+    slots.push_back(std::move(c));
+  }
+  std::stable_sort(rows.begin(), rows.end(), by_len);
+  std::stable_sort(slots.begin(), slots.end(), by_len);
+  GatherProgram K;
+  auto pack = [&](const std::vector<Cell>& cells, uint32_t pad0) {
+    for (size_t g0 = 0; g0 < cells.size(); g0 += 32) {
+      uint32_t depth = 0;
+      for (size_t t = 0; t < 32 && g0 + t < cells.size(); ++t)
+        depth = std::max<uint32_t>(depth, cells[g0 + t].src.size());
+      K.depth.push_back(depth);
+      K.off.push_back(uint32_t(K.src.size()));
+      for (uint32_t k = 0; k < depth; ++k)
+        for (size_t t = 0; t < 32; ++t) {
+          const bool live = g0 + t < cells.size() && k < cells[g0 + t].src.size();
+          K.src.push_back(live ? cells[g0 + t].src[k] : L.zero);
+        }
+      for (size_t t = 0; t < 32; ++t) {
+        const bool live = g0 + t < cells.size();
+        K.dst.push_back(live ? cells[g0 + t].d0 : pad0);  // kNone: the kernel's kNoDiag
+        K.dst.push_back(live ? cells[g0 + t].d1 : L.sink);
+      }
+    }
+  };
+  pack(rows, kNone);
+  n_row_groups = uint32_t(K.depth.size());
+  pack(slots, L.sink);
+  return K;
+}
+
 // The lead lane's pivot tape, compiled and uploaded.
 int32_t upload_tape(esl_ctx* ctx) {
   cudaStream_t s = ctx->stream;
@@ -520,6 +576,14 @@ int32_t upload_tape(esl_ctx* ctx) {
     T.o_g_off = put(G.off.data(), G.off.size() * 4);
     T.o_g_src = put(G.src.data(), G.src.size() * 4);
     T.o_g_dst = put(G.dst.data(), G.dst.size() * 4);
+    uint32_t n_kr = 0;
+    GatherProgram K = build_companion_program(ctx, P, n_kr);
+    T.o_k_depth = put(K.depth.data(), K.depth.size() * 4);
+    T.o_k_off = put(K.off.data(), K.off.size() * 4);
+    T.o_k_src = put(K.src.data(), K.src.size() * 4);
+    T.o_k_dst = put(K.dst.data(), K.dst.size() * 4);
+    T.n_kr_groups = n_kr;
+    T.n_ks_groups = uint32_t(K.depth.size()) - n_kr;
     ESL_CUDA(upload(ctx->d_prog, blob, s));
     T.prog = ctx->d_prog.as<unsigned char>();
     T.prog_bytes = uint32_t(blob.size());

@@ -175,12 +175,12 @@ __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, 
           st[1] = -v;
           break;
         }
-        case kD:
-          diode_stamp(r, s, m.x[nd[0]], m.x[nd[1]], m.x[nd[2]], lim_active ? m.lim + B.lim_off + i : nullptr, st);
-          break;
         case kM:
           mos1_stamp(r, s, m.x[nd[0]], m.x[nd[1]], m.x[nd[2]], m.x[nd[3]], m.x[nd[4]], m.x[nd[5]],
                      lim_active ? m.lim + B.lim_off + 3 * i : nullptr, sim.kind == 1 && B.stride >= kStageM, st);
+          break;
+        case kD:
+          diode_stamp(r, s, m.x[nd[0]], m.x[nd[1]], m.x[nd[2]], lim_active ? m.lim + B.lim_off + i : nullptr, st);
           break;
         default:
           break;
@@ -195,15 +195,33 @@ __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, 
 // copied for the gates, y = P(-rhs) is loaded and fill-in zeroed, all in
 // one gather program (groups of 32 cells; a cell t of group g sums
 // src[off + k * 32 + t], lane-block indices, then writes three places).
+// One gather cell's sum: +0.0 plus the d values at lane-block indices
+// src[k * 32] (shared addresses), added in list order. Four indices, then
+// their four values, are loaded before the four additions, so one pair of
+// shared-memory round trips serves four terms.
+__device__ __forceinline__ double gather_sum(uint32_t src, uint32_t d, uint32_t lb) {
+  double s = 0.0;
+  uint32_t k = 0;
+  for (; k + 4 <= d; k += 4) {
+    const uint32_t i0 = lds_u32(src + 128 * k), i1 = lds_u32(src + 128 * (k + 1));
+    const uint32_t i2 = lds_u32(src + 128 * (k + 2)), i3 = lds_u32(src + 128 * (k + 3));
+    const double v0 = lds(lb + 8 * i0), v1 = lds(lb + 8 * i1), v2 = lds(lb + 8 * i2), v3 = lds(lb + 8 * i3);
+    s = __dadd_rn(s, v0);
+    s = __dadd_rn(s, v1);
+    s = __dadd_rn(s, v2);
+    s = __dadd_rn(s, v3);
+  }
+  for (; k < d; ++k) s = __dadd_rn(s, lds(lb + 8 * lds_u32(src + 128 * k)));
+  return s;
+}
+
 __device__ void assemble(const TopoDev& T, uint32_t prog, const LaneMem& m, int tid) {
   const uint32_t lb = saddr(m.base);
   const uint32_t depth = prog + T.o_g_depth, goff = prog + T.o_g_off;
   const uint32_t gsrc = prog + T.o_g_src, gdst = prog + T.o_g_dst;
   for (uint32_t g = 0; g < T.n_groups; ++g) {
     const uint32_t d = lds_u32(depth + 4 * g);
-    const uint32_t src = gsrc + 4 * (lds_u32(goff + 4 * g) + tid);
-    double s = 0.0;
-    for (uint32_t k = 0; k < d; ++k) s = __dadd_rn(s, lds(lb + 8 * lds_u32(src + 128 * k)));
+    const double s = gather_sum(gsrc + 4 * (lds_u32(goff + 4 * g) + tid), d, lb);
     const uint32_t dst = gdst + 12 * (g * 32 + tid);
     sts(lb + 8 * lds_u32(dst), s);
     sts(lb + 8 * lds_u32(dst + 4), s);
@@ -1021,25 +1039,30 @@ struct Companion {
 };
 
 // Row charge sums and capacitance slot sums from the staging cells, in
-// stamp order; the companion folded into rhs, y and the tape values.
-__device__ void companion(const TopoDev& T, const LaneMem& m, const Companion& c, int tid) {
-  for (uint32_t i = tid; i < T.n; i += 32) {
-    double q = 0.0;
-    for (uint32_t e = T.q_ptr[i]; e < T.q_ptr[i + 1]; ++e) q = __dadd_rn(q, m.st[T.q_src[e]]);
-    const double d = c.ag0 * (q - c.q1[i]);
-    const double base = m.rhs[i] + d;
-    const double r = c.trap ? base - c.ag1 * c.ip[i] : base;
-    m.rhs[i] = r;
-    m.y[T.pinv[i]] = -r;
-  }
-  for (uint32_t p = tid; p < T.nnz; p += 32) {
-    double cs = 0.0;
-    for (uint32_t e = T.c_ptr[p]; e < T.c_ptr[p + 1]; ++e) cs = __dadd_rn(cs, m.st[T.c_src[e]]);
-    const uint32_t a = T.amap[p];
-    const double v = m.v[a] + c.ag0 * cs;
-    m.v[a] = v;
-    const uint32_t row = T.slot_row[p];
-    if (row != kNoDiag) m.diag[row] = v;
+// stamp order (the companion gather program in shared memory); the
+// companion folded into rhs, y and the tape values. Rows and slots without
+// charge or capacitance cells have exactly zero terms and are not visited.
+__device__ void companion(const TopoDev& T, uint32_t prog, const LaneMem& m, const Companion& c, int tid) {
+  const uint32_t lb = saddr(m.base);
+  const uint32_t depth = prog + T.o_k_depth, koff = prog + T.o_k_off;
+  const uint32_t ksrc = prog + T.o_k_src, kdst = prog + T.o_k_dst;
+  const uint32_t ng = T.n_kr_groups + T.n_ks_groups;
+  for (uint32_t g = 0; g < ng; ++g) {
+    const double s = gather_sum(ksrc + 4 * (lds_u32(koff + 4 * g) + tid), lds_u32(depth + 4 * g), lb);
+    const uint2 d = lds_u2(kdst + 8 * (g * 32 + tid));
+    if (g < T.n_kr_groups) {
+      if (d.x != kNoDiag) {
+        const double dq = c.ag0 * (s - c.q1[d.x]);
+        const double base = m.rhs[d.x] + dq;
+        const double r = c.trap ? base - c.ag1 * c.ip[d.x] : base;
+        m.rhs[d.x] = r;
+        sts(lb + 8 * d.y, -r);
+      }
+    } else {
+      const double v = lds(lb + 8 * d.x) + c.ag0 * s;
+      sts(lb + 8 * d.x, v);
+      sts(lb + 8 * d.y, v);
+    }
   }
 }
 
@@ -1100,7 +1123,7 @@ __device__ int lane_newton(const TopoDev& T, uint32_t prog, const LaneMem& m, co
     assemble(T, prog, m, tid);
     __syncwarp();
     if (cp) {
-      companion(T, m, *cp, tid);
+      companion(T, prog, m, *cp, tid);
       __syncwarp();
     }
     if (iter == 0) {
