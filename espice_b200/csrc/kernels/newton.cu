@@ -196,20 +196,46 @@ __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, 
 // one gather program (groups of 32 cells; a cell t of group g sums
 // src[off + k * 32 + t], lane-block indices, then writes three places).
 // One gather cell's sum: +0.0 plus the d values at lane-block indices
-// src[k * 32] (shared addresses), added in list order. Four indices, then
-// their four values, are loaded before the four additions, so one pair of
-// shared-memory round trips serves four terms.
+// src[k * 32] (shared addresses), added in list order (d is the same for
+// the whole warp). Software-pipelined in blocks of four: while a block's
+// four additions run, the next block's values and the indices of the block
+// after it are in flight, so a long list (a supply node's row sums one cell
+// per device on it) costs about its chain of additions, not a
+// shared-memory round trip per term.
 __device__ __forceinline__ double gather_sum(uint32_t src, uint32_t d, uint32_t lb) {
   double s = 0.0;
+  const uint32_t nb = d >> 2;
   uint32_t k = 0;
-  for (; k + 4 <= d; k += 4) {
-    const uint32_t i0 = lds_u32(src + 128 * k), i1 = lds_u32(src + 128 * (k + 1));
-    const uint32_t i2 = lds_u32(src + 128 * (k + 2)), i3 = lds_u32(src + 128 * (k + 3));
-    const double v0 = lds(lb + 8 * i0), v1 = lds(lb + 8 * i1), v2 = lds(lb + 8 * i2), v3 = lds(lb + 8 * i3);
+  if (nb >= 2) {
+    uint32_t i0 = lds_u32(src), i1 = lds_u32(src + 128), i2 = lds_u32(src + 256), i3 = lds_u32(src + 384);
+    double v0 = lds(lb + 8 * i0), v1 = lds(lb + 8 * i1), v2 = lds(lb + 8 * i2), v3 = lds(lb + 8 * i3);
+    i0 = lds_u32(src + 512);
+    i1 = lds_u32(src + 640);
+    i2 = lds_u32(src + 768);
+    i3 = lds_u32(src + 896);
+    for (uint32_t b = 1; b < nb; ++b) {
+      const double w0 = lds(lb + 8 * i0), w1 = lds(lb + 8 * i1), w2 = lds(lb + 8 * i2), w3 = lds(lb + 8 * i3);
+      if (b + 1 < nb) {
+        const uint32_t at = src + 512 * (b + 1);
+        i0 = lds_u32(at);
+        i1 = lds_u32(at + 128);
+        i2 = lds_u32(at + 256);
+        i3 = lds_u32(at + 384);
+      }
+      s = __dadd_rn(s, v0);
+      s = __dadd_rn(s, v1);
+      s = __dadd_rn(s, v2);
+      s = __dadd_rn(s, v3);
+      v0 = w0;
+      v1 = w1;
+      v2 = w2;
+      v3 = w3;
+    }
     s = __dadd_rn(s, v0);
     s = __dadd_rn(s, v1);
     s = __dadd_rn(s, v2);
     s = __dadd_rn(s, v3);
+    k = nb << 2;
   }
   for (; k < d; ++k) s = __dadd_rn(s, lds(lb + 8 * lds_u32(src + 128 * k)));
   return s;
