@@ -52,6 +52,8 @@ constexpr uint32_t lim_count(uint32_t type) { return type == kD ? 1u : type == k
 constexpr uint32_t kSrcOne = 0xfffffffeu;    // + 1.0 (the ground pin on g)
 constexpr uint32_t kSrcX0 = 0xfffffffdu;     // + x[0] (the ground pin on rhs)
 constexpr uint32_t kNoDiag = 0xffffffffu;
+constexpr uint32_t kGatherEnd = 0x80000000u;  // a segmented gather's cell ends at this segment
+constexpr int kGatherBlock = 8;                // terms per pipelined block of the segmented gather
 
 // One op of a warp program over a lane's shared-memory values v (the tape
 // values, then the permuted right-hand side y). word0 = dst | (kind << 28);

@@ -428,20 +428,18 @@ struct GatherProgram {
 };
 
 // Assembly cells: every residual row, every pattern slot and every fill-in
-// tape value, each summing its staging cells in stamp order (+0.0 pads a
-// short list: a sum that starts at +0.0 is never -0.0, so adding +0.0 is
-// exact). Cells sorted by list length so a group of 32 pads little.
-GatherProgram build_gather_program(const esl_ctx* ctx, const Programs& P) {
+// tape value, each summing its staging cells in stamp order.
+struct AsmCell {
+  std::vector<uint32_t> src;
+  uint32_t d0, d1, d2;
+};
+
+std::vector<AsmCell> assembly_cells(const esl_ctx* ctx, const Programs& P, const LaneLayout& L) {
   const uint32_t n = ctx->pat.n, nnz = ctx->pat.nnz();
-  const LaneLayout L = lane_layout(n, P.ntv, ctx->n_stage, ctx->nlim);
-  struct Cell {
-    std::vector<uint32_t> src;
-    uint32_t d0, d1, d2;
-  };
-  std::vector<Cell> cells;
+  std::vector<AsmCell> cells;
   auto remap = [&](uint32_t s) { return s == kSrcOne ? L.one : s == kSrcX0 ? L.x : L.st + s; };
   for (uint32_t i = 0; i < n; ++i) {
-    Cell c;
+    AsmCell c;
     for (uint32_t e = ctx->rhs_ptr[i]; e < ctx->rhs_ptr[i + 1]; ++e) c.src.push_back(remap(ctx->rhs_src[e]));
     c.d0 = L.rhs + i;
     c.d1 = L.sink;
@@ -449,37 +447,80 @@ GatherProgram build_gather_program(const esl_ctx* ctx, const Programs& P) {
     cells.push_back(std::move(c));
   }
   for (uint32_t p = 0; p < nnz; ++p) {
-    Cell c;
+    AsmCell c;
     for (uint32_t e = ctx->a_ptr[p]; e < ctx->a_ptr[p + 1]; ++e) c.src.push_back(remap(ctx->a_src[e]));
     c.d0 = L.tv + P.amap[p];
     c.d1 = ctx->slot_row[p] != kNoDiag ? L.diag + ctx->slot_row[p] : L.sink;
     c.d2 = L.sink;
     cells.push_back(std::move(c));
   }
-  for (uint32_t f : P.fill) cells.push_back(Cell{{}, L.tv + f, L.sink, L.sink});
-  std::stable_sort(cells.begin(), cells.end(), [](const Cell& a, const Cell& b) { return a.src.size() > b.src.size(); });
-  GatherProgram G;
-  for (size_t g0 = 0; g0 < cells.size(); g0 += 32) {
-    uint32_t depth = 0;
-    for (size_t t = 0; t < 32 && g0 + t < cells.size(); ++t) depth = std::max<uint32_t>(depth, cells[g0 + t].src.size());
-    G.depth.push_back(depth);
-    G.off.push_back(uint32_t(G.src.size()));
-    for (uint32_t k = 0; k < depth; ++k)
-      for (size_t t = 0; t < 32; ++t) {
-        const bool live = g0 + t < cells.size() && k < cells[g0 + t].src.size();
-        G.src.push_back(live ? cells[g0 + t].src[k] : L.zero);
-      }
-    for (size_t t = 0; t < 32; ++t) {
-      if (g0 + t < cells.size()) {
-        G.dst.push_back(cells[g0 + t].d0);
-        G.dst.push_back(cells[g0 + t].d1);
-        G.dst.push_back(cells[g0 + t].d2);
-      } else {
-        G.dst.push_back(L.sink);
-        G.dst.push_back(L.sink);
-        G.dst.push_back(L.sink);
-      }
+  for (uint32_t f : P.fill) cells.push_back(AsmCell{{}, L.tv + f, L.sink, L.sink});
+  return cells;
+}
+
+// The assembly as one segmented gather: the warp walks nseg segments of
+// seg_len terms (a multiple of kGatherBlock), thread t summing term k of its column at
+// src[k * 32 + t]; at each segment's end every thread whose cell ends there
+// stores its sum (twice, and the negation) to that segment's destination
+// triple for it (dst[(3 s + i) * 32 + t], kGatherEnd on the first word) and
+// starts over from +0.0. A cell spans ceil(len / seg_len) consecutive
+// segments of one column, its terms at the end of that span and +0.0 before
+// them (a sum that starts at +0.0 is never -0.0, so a +0.0 term changes no
+// bit). Cells go to the least loaded column, longest first, and seg_len is
+// the multiple of kGatherBlock that minimises the segments walked times (seg_len +
+// the boundary's cost): one long sum (a supply node's row, a term per device
+// on the node) then runs beside all the short ones instead of after them.
+struct GatherSegments {
+  std::vector<uint32_t> src, dst;
+  uint32_t nseg = 0, seg_len = kGatherBlock;
+};
+
+GatherSegments build_gather_segments(const esl_ctx* ctx, const Programs& P) {
+  const LaneLayout L = lane_layout(ctx->pat.n, P.ntv, ctx->n_stage, ctx->nlim);
+  std::vector<AsmCell> cells = assembly_cells(ctx, P, L);
+  std::stable_sort(cells.begin(), cells.end(),
+                   [](const AsmCell& a, const AsmCell& b) { return a.src.size() > b.src.size(); });
+  const size_t longest = cells.empty() ? 0 : cells.front().src.size();
+  constexpr size_t kBoundaryCost = 8;  // terms' worth of time per segment boundary
+  auto place = [&](uint32_t seg_len, uint32_t* column) {
+    std::vector<uint32_t> load(32, 0);
+    for (size_t c = 0; c < cells.size(); ++c) {
+      const uint32_t segs = std::max<uint32_t>(1, uint32_t((cells[c].src.size() + seg_len - 1) / seg_len));
+      const uint32_t t = uint32_t(std::min_element(load.begin(), load.end()) - load.begin());
+      if (column) column[c] = t;
+      load[t] += segs;
     }
+    return *std::max_element(load.begin(), load.end());
+  };
+  const uint32_t gb = kGatherBlock;
+  uint32_t best_len = gb, best_nseg = place(gb, nullptr);
+  for (uint32_t len = 2 * gb; len <= std::max<size_t>(gb, (longest + gb - 1) / gb * gb); len += gb) {
+    const uint32_t nseg = place(len, nullptr);
+    if (size_t(nseg) * (len + kBoundaryCost) < size_t(best_nseg) * (best_len + kBoundaryCost)) {
+      best_len = len;
+      best_nseg = nseg;
+    }
+  }
+  std::vector<uint32_t> column(cells.size());
+  place(best_len, column.data());
+  GatherSegments G;
+  G.seg_len = best_len;
+  G.nseg = best_nseg;
+  G.src.assign(size_t(G.nseg) * G.seg_len * 32, L.zero);
+  // one sink triple past the last segment: the kernel loads a triple ahead
+  G.dst.assign(size_t(G.nseg + 1) * 3 * 32, L.sink);
+  std::vector<uint32_t> at(32, 0);  // next free segment per column
+  for (size_t c = 0; c < cells.size(); ++c) {
+    const uint32_t t = column[c];
+    const size_t len = cells[c].src.size();
+    const uint32_t segs = std::max<uint32_t>(1, uint32_t((len + G.seg_len - 1) / G.seg_len));
+    const size_t end = size_t(at[t] + segs) * G.seg_len;  // one past the cell's last term
+    for (size_t k = 0; k < len; ++k) G.src[(end - len + k) * 32 + t] = cells[c].src[k];
+    const size_t s = at[t] + segs - 1;
+    G.dst[(3 * s + 0) * 32 + t] = cells[c].d0 | kGatherEnd;
+    G.dst[(3 * s + 1) * 32 + t] = cells[c].d1;
+    G.dst[(3 * s + 2) * 32 + t] = cells[c].d2;
+    at[t] += segs;
   }
   return G;
 }
@@ -562,7 +603,7 @@ int32_t upload_tape(esl_ctx* ctx) {
   {
     // One blob: A ops, B ops, gather depth/off/src/dst, each section
     // 16-byte aligned.
-    GatherProgram G = build_gather_program(ctx, P);
+    GatherSegments G = build_gather_segments(ctx, P);
     std::vector<unsigned char> blob;
     auto put = [&blob](const void* p, size_t bytes) {
       const uint32_t at = uint32_t(blob.size());
@@ -572,8 +613,6 @@ int32_t upload_tape(esl_ctx* ctx) {
     };
     T.o_a_ops = put(P.a_ops.data(), P.a_ops.size() * sizeof(Op));
     T.o_b_ops = put(P.b_ops.data(), P.b_ops.size() * sizeof(Op));
-    T.o_g_depth = put(G.depth.data(), G.depth.size() * 4);
-    T.o_g_off = put(G.off.data(), G.off.size() * 4);
     T.o_g_src = put(G.src.data(), G.src.size() * 4);
     T.o_g_dst = put(G.dst.data(), G.dst.size() * 4);
     uint32_t n_kr = 0;
@@ -589,7 +628,8 @@ int32_t upload_tape(esl_ctx* ctx) {
     T.prog_bytes = uint32_t(blob.size());
     T.a_rows = P.a_rows;
     T.b_rows = P.b_rows;
-    T.n_groups = uint32_t(G.depth.size());
+    T.g_nseg = G.nseg;
+    T.g_seg_blocks = G.seg_len / kGatherBlock;
   }
   T.l_scaled = ctx->d_l_scaled.as<uint8_t>();
   T.pinv = ctx->d_pinv.as<uint32_t>();

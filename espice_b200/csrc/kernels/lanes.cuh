@@ -44,20 +44,23 @@ struct TopoDev {
   // CTA's shared memory: A = refactor + forward solve and B = back solve,
   // rows of 32 ops over v = [tape values | y | 0.0 | 1.0 | sink], each row
   // divisions only or multiply-subtracts only (every op word carries its
-  // kind); the assembly gather program: group g of 32 cells sums
-  // src[off[g] + k * 32 + t] for k < depth[g] (cell t, lane-block
-  // indices), then writes the sum to dst[3 * (32 g + t)] and [+1] and its
-  // negation to [+2] (residual rows, pattern slots into tape values, the
-  // diagonal copy and y = P(-rhs); fill-in tape values are empty cells);
-  // and the transient companion's gather program, the same form over the
-  // rows with charge cells (groups 0 .. n_kr_groups - 1; dst pair: the row,
-  // or kNone on padding, and its y value) and then the pattern slots with
-  // capacitance cells (dst pair: the tape value, the diagonal copy or the
-  // sink). Offsets in bytes.
+  // kind); the assembly as one segmented gather: g_nseg segments of
+  // kGatherBlock g_seg_blocks terms, thread t summing term k of its column at
+  // src[k * 32 + t] (lane-block indices) and, at a segment's end where its
+  // destination triple (dst[(3 s + i) * 32 + t]) carries kGatherEnd,
+  // writing the sum to the first two places and its negation to the third
+  // and starting over (residual rows, pattern slots into tape values, the
+  // diagonal copy and y = P(-rhs); fill-in tape values sum +0.0); and the
+  // transient companion's gather program in groups of 32 cells, cell t of
+  // group g summing src[off[g] + k * 32 + t] for k < depth[g]: the rows with
+  // charge cells (groups 0 .. n_kr_groups - 1; dst pair: the row, or kNone
+  // on padding, and its y value), then the pattern slots with capacitance
+  // cells (dst pair: the tape value, the diagonal copy or the sink).
+  // Offsets in bytes.
   const unsigned char* prog;
   uint32_t prog_bytes;
-  uint32_t o_a_ops, o_b_ops, o_g_depth, o_g_off, o_g_src, o_g_dst;
-  uint32_t a_rows, b_rows, n_groups;
+  uint32_t o_a_ops, o_b_ops, o_g_src, o_g_dst;
+  uint32_t a_rows, b_rows, g_nseg, g_seg_blocks;
   uint32_t o_k_depth, o_k_off, o_k_src, o_k_dst;
   uint32_t n_kr_groups, n_ks_groups;
   // L tape values whose column passed on the row-scaled test (no wide test).

@@ -241,17 +241,59 @@ __device__ __forceinline__ double gather_sum(uint32_t src, uint32_t d, uint32_t 
   return s;
 }
 
+// Assembly: the segmented gather. Every thread sums its column's terms,
+// software-pipelined in blocks of eight: while a block's additions run, the
+// next block's values and the indices of the block after it are in flight.
+// At each segment's end a thread whose cell ends there stores it and starts
+// over; the next segment's destinations are loaded a segment ahead.
 __device__ void assemble(const TopoDev& T, uint32_t prog, const LaneMem& m, int tid) {
   const uint32_t lb = saddr(m.base);
-  const uint32_t depth = prog + T.o_g_depth, goff = prog + T.o_g_off;
-  const uint32_t gsrc = prog + T.o_g_src, gdst = prog + T.o_g_dst;
-  for (uint32_t g = 0; g < T.n_groups; ++g) {
-    const uint32_t d = lds_u32(depth + 4 * g);
-    const double s = gather_sum(gsrc + 4 * (lds_u32(goff + 4 * g) + tid), d, lb);
-    const uint32_t dst = gdst + 12 * (g * 32 + tid);
-    sts(lb + 8 * lds_u32(dst), s);
-    sts(lb + 8 * lds_u32(dst + 4), s);
-    sts(lb + 8 * lds_u32(dst + 8), -s);
+  const uint32_t sb = T.g_seg_blocks, nblk = T.g_nseg * sb;
+  if (nblk == 0) return;
+  const uint32_t src = prog + T.o_g_src + 4 * tid;
+  uint32_t dp = prog + T.o_g_dst + 4 * tid;
+  uint32_t d0 = lds_u32(dp), d1 = lds_u32(dp + 128), d2 = lds_u32(dp + 256);
+  dp += 384;
+  uint32_t i[kGatherBlock];
+  double v[kGatherBlock];
+#pragma unroll
+  for (int j = 0; j < kGatherBlock; ++j) i[j] = lds_u32(src + 128 * j);
+#pragma unroll
+  for (int j = 0; j < kGatherBlock; ++j) v[j] = lds(lb + 8 * i[j]);
+  {
+    const uint32_t at = src + 128 * kGatherBlock * (nblk > 1 ? 1u : 0u);
+#pragma unroll
+    for (int j = 0; j < kGatherBlock; ++j) i[j] = lds_u32(at + 128 * j);
+  }
+  double s = 0.0;
+  uint32_t left = sb;
+  for (uint32_t b = 0; b < nblk; ++b) {
+    double w[kGatherBlock];
+#pragma unroll
+    for (int j = 0; j < kGatherBlock; ++j) w[j] = lds(lb + 8 * i[j]);
+    if (b + 2 < nblk) {
+      const uint32_t at = src + 128 * kGatherBlock * (b + 2);
+#pragma unroll
+      for (int j = 0; j < kGatherBlock; ++j) i[j] = lds_u32(at + 128 * j);
+    }
+#pragma unroll
+    for (int j = 0; j < kGatherBlock; ++j) s = __dadd_rn(s, v[j]);
+#pragma unroll
+    for (int j = 0; j < kGatherBlock; ++j) v[j] = w[j];
+    if (--left == 0) {
+      left = sb;
+      const uint32_t e0 = lds_u32(dp), e1 = lds_u32(dp + 128), e2 = lds_u32(dp + 256);
+      dp += 384;
+      if (d0 & kGatherEnd) {
+        sts(lb + 8 * (d0 & ~kGatherEnd), s);
+        sts(lb + 8 * d1, s);
+        sts(lb + 8 * d2, -s);
+        s = 0.0;
+      }
+      d0 = e0;
+      d1 = e1;
+      d2 = e2;
+    }
   }
 }
 
