@@ -348,11 +348,13 @@ int32_t upload_topology(esl_ctx* ctx) {
   T.nlim = ctx->nlim;
   T.rec_size = ctx->rec_size;
   T.n_batches = uint32_t(ctx->bats.size());
+  T.n_src = 0;
   for (size_t b = 0; b < ctx->bats.size(); ++b) {
     const HostBatch& B = ctx->bats[b];
     ESL_CUDA(upload(ctx->d_nodes[b], B.nodes, s));
     T.b[b] = BatchDev{B.type, B.count, B.nt, B.stage_base, B.stride, B.rec_off, B.lim_off,
-                      ctx->d_nodes[b].as<uint32_t>(), B.qt_off, B.qt_sites};
+                      ctx->d_nodes[b].as<uint32_t>(), B.qt_off, B.qt_sites, T.n_src};
+    if (B.type == kV) T.n_src += B.count;
   }
   ESL_CUDA(upload(ctx->d_q_ptr, ctx->q_ptr, s));
   ESL_CUDA(upload(ctx->d_q_src, ctx->q_src, s));
@@ -645,8 +647,9 @@ int32_t upload_tape(esl_ctx* ctx) {
   ctx->lanes_eff = std::max<uint32_t>(1, std::min<uint32_t>(8, uint32_t((room - T.prog_bytes) / lane_bytes)));
   // Transient lanes add the accepted points, the charge rings and dynamic
   // currents over the rows and the LTE states: cur | prev | q[4] | ip over
-  // n, then q[4] | ip over n_qt.
-  T.tran_doubles = (T.smem_doubles + 7 * T.n + 5 * T.n_qt + 1) & ~1u;
+  // n, then q[4] | ip over n_qt, then the V sources' values at the current
+  // time point.
+  T.tran_doubles = (T.smem_doubles + 7 * T.n + 5 * T.n_qt + T.n_src + 1) & ~1u;
   const size_t tran_bytes = size_t(T.tran_doubles) * 8;
   ctx->tran_lanes_eff = T.prog_bytes + tran_bytes > room
                             ? 0

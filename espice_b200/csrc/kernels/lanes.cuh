@@ -20,6 +20,7 @@ struct BatchDev {
   uint32_t lim_off;             // limited images: lim_off + lim_count(type) * inst
   const uint32_t* nodes;        // count * nt unknown indices
   uint32_t qt_off, qt_sites;    // LTE charge states: qt_off + inst * qt_sites + k
+  uint32_t src_off;             // V sources: the lane's cached value at src_off + inst
 };
 
 struct TopoDev {
@@ -78,6 +79,7 @@ struct TopoDev {
   const uint32_t* c_ptr;
   const uint32_t* c_src;
   uint32_t n_qt;
+  uint32_t n_src;         // V source instances (the transient's cached source values)
   uint32_t tran_doubles;  // per lane, transient kernel
   // The pattern by rows (the refinement's residual): row i's entries
   // row_ptr[i] .. row_ptr[i + 1], each its pattern slot and column.

@@ -122,7 +122,7 @@ __device__ __forceinline__ double* stage_programs(const TopoDev& T, unsigned cha
 // Device evaluation: every instance of every batch, strided over the warp,
 // each writing its own staging cells (no shared cell, no atomics).
 __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, bool lim_active,
-                         const SimDev& sim, int tid, bool charges_only = false) {
+                         const SimDev& sim, int tid, bool charges_only = false, const double* vcache = nullptr) {
   for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
     const BatchDev& B = T.b[bi];
     // the charge re-read (the reference's evalQ) needs only the batches
@@ -158,7 +158,7 @@ __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, 
           break;
         }
         case kV: {
-          const double v = vsource_value(r, s, sim);
+          const double v = vcache ? vcache[B.src_off + i] : vsource_value(r, s, sim);
           const double ib = m.x[nd[2]];
           st[0] = ib;
           st[1] = -ib;
@@ -1176,17 +1176,25 @@ __device__ void state_charges(const TopoDev& T, const double* rec, const double*
 }
 
 // Newton on one lane (converger.newton at W = 1 on the frozen tape), for
-// the transient's operating point (no companion) and its steps. Returns 0
-// converged (x holds the published iterate), 1 out of iterations, 2 the
-// factor left the tape.
+// the transient's operating point (no companion) and its steps. `vcache`
+// (T.n_src values) takes the V sources' values, which depend on the time
+// point alone, once for all the iterations. Returns 0 converged (x holds
+// the published iterate), 1 out of iterations, 2 the factor left the tape.
 __device__ int lane_newton(const TopoDev& T, uint32_t prog, const LaneMem& m, const double* rec, const LaneOpts& o,
                            const SimDev& sim, const Companion* cp, bool& lim_active, bool init_fix,
-                           uint32_t& iters, int tid) {
+                           uint32_t& iters, double* vcache, int tid) {
   const uint32_t n = T.n;
   const uint32_t max_iter = o.max_iter < 100 ? 100 : o.max_iter;
+  for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
+    const BatchDev& B = T.b[bi];
+    if (B.type != kV) continue;
+    for (uint32_t i = tid; i < B.count; i += 32)
+      vcache[B.src_off + i] = vsource_value(rec + B.rec_off + i, static_cast<int>(B.count), sim);
+  }
+  __syncwarp();
   double limit = kXPlausible;
   for (uint32_t iter = 0; iter < max_iter; ++iter) {
-    eval_all(T, rec, m, lim_active, sim, tid);
+    eval_all(T, rec, m, lim_active, sim, tid, false, vcache);
     __syncwarp();
     assemble(T, prog, m, tid);
     __syncwarp();
@@ -1350,6 +1358,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
   double* ipr = qh + 4 * n;
   double* qt = ipr + n;    // 4 slots of nq: the LTE-state ring
   double* ipt = qt + 4 * nq;
+  double* vsrc = ipt + nq;  // T.n_src: the V sources at the current time point
   const double* rec = L.rec + size_t(lane) * T.rec_size;
   uint32_t stat[kTsN];
   for (int k = 0; k < kTsN; ++k) stat[k] = 0;
@@ -1380,7 +1389,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
   op.gmin = 0.0;
   op.max_iter = 100;
   uint32_t it = 0;
-  int rc = lane_newton(T, prog, m, rec, op, sim, nullptr, lim_active, true, it, tid);
+  int rc = lane_newton(T, prog, m, rec, op, sim, nullptr, lim_active, true, it, vsrc, tid);
   lim_active = false;
   stat[kTsOpIters] = it;
   uint32_t n_rec = 0;
@@ -1460,7 +1469,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
       __syncwarp();
       Companion c{ag0, ag1, trap, slot(qh, n, 1), ipr};
       uint32_t iters = 0;
-      rc = lane_newton(T, prog, m, rec, nr, sim, &c, lim_active, false, iters, tid);
+      rc = lane_newton(T, prog, m, rec, nr, sim, &c, lim_active, false, iters, vsrc, tid);
       lim_active = false;
       stat[kTsAttempts] += 1;
       stat[kTsNrIters] += iters;
