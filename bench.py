@@ -169,6 +169,14 @@ def reference_arm(args, rank, world):
     }), flush=True)
 
 
+# DRAM bytes per lane of one tran_kernel launch, from an ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum, --set full) of 148 ring
+# lanes to 0.1 ns: 1,478,144 B read, 0 B written. The kernel reads each
+# lane's records once and keeps its working set in shared memory, so the
+# traffic grows with lanes, not with simulated time.
+TRAN_DRAM_BYTES_PER_LANE = 1478144 / 148
+
+
 def lane_major_bytes(fr, nr_iters_total):
     """Bytes a lane-major, launch-per-phase design (the reference's GPU lanes)
     streams per Newton iteration and lane (the per-unit figures of the scope
@@ -468,7 +476,10 @@ def our_arm(args, rank, world):
                 "d2h_bytes_per_step": int(N * n * 8 + N * 4 * len(lanes.TS_FIELDS))},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
+                     "frac": achieved / hbm_peak, "traffic": TRAN_DRAM_BYTES_PER_LANE * N,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                       "tran_kernel launch on 148 ring lanes, scaled by lanes",
+                     "peak_source": peak_src,
                      "note": "fused tran_kernel: unavoidable HBM bytes (records in, solution and "
                              "step statistics out) per launch / device time; every lane's Newton "
                              "working set stays in shared memory for its whole transient, so the "
