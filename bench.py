@@ -321,6 +321,37 @@ def dc_grid_diodes(args, local, flush):
             "e2e": conv and e2e_conv / sum(e2e_t)}
 
 
+def dc_sweep_lanes(args, local, flush):
+    """Sequential .dc sweeps, one per lane: 1024 Monte-Carlo samples of the
+    grid-with-diodes deck (four grid resistors scaled by exp(U(-0.5, 0.5)) per
+    sample), each sweeping its source 0..5 V in 256 points as dc.zig does
+    (predictor, limiting against the last point, warm Newton, cold rung on
+    failure), all in one launch."""
+    from espice_b200 import decks, lanes
+    from espice_b200.circuit import R, V
+    fr, _, _ = decks.grid_diodes(seed=1, points=4)
+    rs = fr.slots_of(R, "r")[:4]
+    nominal = np.array([fr.param(s) for s in rs])
+    rng = np.random.default_rng(11)
+    lane_vals = nominal * np.exp(rng.uniform(-0.5, 0.5, size=(1024, len(rs))))
+    src = fr.slots_of(V, "dc")[0]
+    pts = np.linspace(0.0, 5.0, 256)
+    ctx = lanes.DcLanes(fr, device=local)
+    ctx.set_lanes(rs, lane_vals)
+    ms, conv, left = [], 0, 0
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        x, it, cv, st, t = ctx.sweep(src, pts)
+        if i >= args.warmup:
+            ms.append(t)
+            conv += int(cv.sum())
+            left += int((st != lanes.SWEEP_DONE).sum())
+    ctx.close()
+    return {"workload": "grid_diodes sweep lanes: 1024 samples x 256 sequential points (0..5 V)",
+            "value": conv / (sum(ms) / 1e3), "unit": UNIT, "ms_per_step": float(np.mean(ms)),
+            "lanes_left_tape": left, "newton_iters_per_point": float(it.mean())}
+
+
 def learned_dc(args, local, flush):
     """The learned warm start against the plain FP64 lanes on the 16-parameter
     grid-with-diodes deck: 65536 seeded points, the network trained on the
@@ -491,6 +522,7 @@ def our_arm(args, rank, world):
         "clocks": clk.summary(), "wall_s_timed": wall,
     }
     out["dc_grid_diodes"] = dc_grid_diodes(args, local, flush)
+    out["dc_sweep_lanes"] = dc_sweep_lanes(args, local, flush)
     if args.learned:
         out["learned_warm_start"] = learned_dc(args, local, flush)
     out["lu_roofline"] = lu_lanes_roofline(fr, ctx, hbm_peak, peak_src)

@@ -73,6 +73,10 @@ enum TranStat : uint32_t {
   kTsStatus, kTsAccepted, kTsAttempts, kTsNrIters, kTsRejNewton, kTsRejLte, kTsBpLandings, kTsOpIters,
   kTsN
 };
+enum SweepStatus : uint32_t {
+  kSweepDone = 0,      // every point ran (each point's convergence is its own flag)
+  kSweepLeftTape = 4,  // a factor left the lead pivot tape: the rest of the sweep is the CPU's
+};
 enum TranStatus : uint32_t {
   kTranDone = 0,       // reached t_stop
   kTranUnderflow = 1,  // dt fell below dt_min

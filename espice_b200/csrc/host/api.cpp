@@ -200,7 +200,7 @@ struct esl_ctx {
 
   DevBuf d_nodes[kMaxBatches], d_rhs_ptr, d_rhs_src, d_a_ptr, d_a_src, d_slot_row, d_cur;
   DevBuf d_q_ptr, d_q_src, d_c_ptr, d_c_src, d_probes, d_tran_t, d_tran_v, d_tran_n, d_tran_stats;
-  DevBuf d_amap, d_fill, d_prog, d_l_scaled, d_pinv, d_q, d_seq;
+  DevBuf d_amap, d_fill, d_prog, d_l_scaled, d_pinv, d_q, d_seq, d_sweep_values;
   uint32_t n_seq_a = 0, n_seq = 0, seq_warps = 0;  // lane-interleaved op list
   uint32_t n_seq_f = 0, mixed_warps = 0;            // its forward-only tail, the mixed kernel's warps
   DevBuf d_row_ptr, d_row_slot, d_row_col;
@@ -354,7 +354,7 @@ int32_t upload_topology(esl_ctx* ctx) {
     ESL_CUDA(upload(ctx->d_nodes[b], B.nodes, s));
     T.b[b] = BatchDev{B.type, B.count, B.nt, B.stage_base, B.stride, B.rec_off, B.lim_off,
                       ctx->d_nodes[b].as<uint32_t>(), B.qt_off, B.qt_sites, T.n_src};
-    if (B.type == kV) T.n_src += B.count;
+    if (B.type == kV || B.type == kI) T.n_src += B.count;
   }
   ESL_CUDA(upload(ctx->d_q_ptr, ctx->q_ptr, s));
   ESL_CUDA(upload(ctx->d_q_src, ctx->q_src, s));
@@ -1149,6 +1149,55 @@ int32_t esl_tran_device(esl_ctx* ctx, const esl_tran_opts* opts, double* d_x, ui
   cudaStream_t s = ctx->stream;
   ESL_CUDA(cudaEventRecord(ctx->ev0, s));
   ESL_CUDA(launch_tran(ctx->topo, L, P, lo, lanes_per_cta(ctx, ctx->n_lanes, ctx->tran_lanes_eff), s));
+  ESL_CUDA(cudaEventRecord(ctx->ev1, s));
+  ESL_CUDA(cudaEventSynchronize(ctx->ev1));
+  if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
+  return ESL_OK;
+}
+
+int32_t esl_dc_sweep_device(esl_ctx* ctx, const esl_slot* slot, const double* values, uint32_t n_pts,
+                            const esl_newton_opts* opts, double* d_x, uint32_t* d_iters, uint8_t* d_conv,
+                            uint32_t* d_status, float* ms) {
+  if (!ctx || !slot || !values || !opts || !d_x || !d_iters || !d_conv || !d_status || n_pts == 0 ||
+      ctx->n_lanes == 0)
+    return ESL_INVALID_ARGUMENT;
+  if (slot->batch >= ctx->bats.size()) return ctx->fail(ESL_INVALID_ARGUMENT, "swept slot: no such batch");
+  const HostBatch& SB = ctx->bats[slot->batch];
+  if (slot->inst >= SB.count) return ctx->fail(ESL_INVALID_ARGUMENT, "swept slot: no such instance");
+  if ((SB.type != kV && SB.type != kI) || slot->param != 0)
+    return ctx->fail(ESL_NOT_ELIGIBLE, "a sweep lane sweeps a V or I source's DC value (parameter 0)");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  if (!ctx->have_tape) {
+    // The lead tape from lane 0's cold Jacobian at the sweep's first point
+    // (the first Jacobian the sweep solves), its source set there for the
+    // assembly and restored after.
+    double* src = ctx->d_rec.as<double>() + SB.rec_off + slot->inst;
+    const double first = values[0], keep = ctx->rec_lanes[SB.rec_off + slot->inst];
+    ESL_CUDA(cudaMemcpyAsync(src, &first, 8, cudaMemcpyHostToDevice, s));
+    const int32_t rc = ensure_tape_cold(ctx);
+    ESL_CUDA(cudaMemcpyAsync(src, &keep, 8, cudaMemcpyHostToDevice, s));
+    ESL_CUDA(cudaStreamSynchronize(s));
+    if (rc) return rc;
+  }
+  const TopoDev& T = ctx->topo;
+  const size_t lane_bytes = size_t(sweep_doubles(T)) * 8, room = size_t(227) * 1024;
+  if (T.prog_bytes + lane_bytes > room) return ctx->fail(ESL_NOT_ELIGIBLE, "a sweep lane exceeds a CTA's shared memory");
+  const uint32_t fit = std::max<uint32_t>(1, std::min<uint32_t>(8, uint32_t((room - T.prog_bytes) / lane_bytes)));
+  ESL_CUDA(ctx->d_sweep_values.ensure(size_t(n_pts) * 8));
+  ESL_CUDA(cudaMemcpyAsync(ctx->d_sweep_values.p, values, size_t(n_pts) * 8, cudaMemcpyHostToDevice, s));
+  SweepDev P{};
+  P.values = ctx->d_sweep_values.as<double>();
+  P.n_pts = n_pts;
+  P.src = T.b[slot->batch].src_off + slot->inst;
+  P.x_out = d_x;
+  P.iters = d_iters;
+  P.conv = d_conv;
+  P.status = d_status;
+  const LaneOpts o{opts->reltol, opts->abstol, opts->vntol, opts->residual_tol, opts->gmin, opts->max_iter, 0, 0};
+  LaneDev L = lane_view(ctx, 0);
+  ESL_CUDA(cudaEventRecord(ctx->ev0, s));
+  ESL_CUDA(launch_sweep(T, L, P, o, lanes_per_cta(ctx, ctx->n_lanes, fit), s));
   ESL_CUDA(cudaEventRecord(ctx->ev1, s));
   ESL_CUDA(cudaEventSynchronize(ctx->ev1));
   if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);

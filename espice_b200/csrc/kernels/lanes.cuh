@@ -20,7 +20,7 @@ struct BatchDev {
   uint32_t lim_off;             // limited images: lim_off + lim_count(type) * inst
   const uint32_t* nodes;        // count * nt unknown indices
   uint32_t qt_off, qt_sites;    // LTE charge states: qt_off + inst * qt_sites + k
-  uint32_t src_off;             // V sources: the lane's cached value at src_off + inst
+  uint32_t src_off;             // V and I sources: the lane's cached value at src_off + inst
 };
 
 struct TopoDev {
@@ -79,7 +79,7 @@ struct TopoDev {
   const uint32_t* c_ptr;
   const uint32_t* c_src;
   uint32_t n_qt;
-  uint32_t n_src;         // V source instances (the transient's cached source values)
+  uint32_t n_src;         // V and I source instances (the cached source values)
   uint32_t tran_doubles;  // per lane, transient kernel
   // The pattern by rows (the refinement's residual): row i's entries
   // row_ptr[i] .. row_ptr[i + 1], each its pattern slot and column.
@@ -101,6 +101,26 @@ struct TranDev {
   uint32_t* n_pts;         // [lane] rows recorded
   uint32_t* stats;         // [lane][kTsN]
 };
+
+// Sequential .dc sweeps, one per lane (dc.zig Sweep): the swept source
+// (its index among the V and I sources' cached values) takes values[pt] at
+// point pt; per lane and point the solution, the Newton iterations and
+// whether it converged; per lane a status (kSweepDone, kSweepLeftTape).
+struct SweepDev {
+  const double* values;  // [n_pts]
+  uint32_t n_pts;
+  uint32_t src;
+  double* x_out;     // [lane][n_pts][n]
+  uint32_t* iters;   // [lane][n_pts]
+  uint8_t* conv;     // [lane][n_pts]
+  uint32_t* status;  // [lane]
+};
+
+// Shared-memory doubles per lane of sweep_kernel: the lane working set,
+// then the sweep's solution and previous point, then the cached sources.
+__host__ __device__ inline uint32_t sweep_doubles(const TopoDev& T) {
+  return (T.smem_doubles + 2 * T.n + T.n_src + 1) & ~1u;
+}
 
 struct LaneDev {
   uint32_t n_lanes;

@@ -18,6 +18,8 @@ cudaError_t launch_lu_replay(const TopoDev& T, uint32_t n_lanes, const double* a
                              double* tv, double* dx, uint8_t* bad, uint32_t lanes_per_block,
                              cudaStream_t s);
 
+cudaError_t launch_sweep(const TopoDev& T, const LaneDev& L, const SweepDev& P, const LaneOpts& o,
+                         uint32_t lanes_per_block, cudaStream_t s);
 cudaError_t launch_tran(const TopoDev& T, const LaneDev& L, const TranDev& P, const LaneOpts& o,
                         uint32_t lanes_per_block, cudaStream_t s);
 

@@ -170,7 +170,7 @@ __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, 
           break;
         }
         case kI: {
-          const double v = r[0] * sim.src_scale;
+          const double v = vcache ? vcache[B.src_off + i] : r[0] * sim.src_scale;
           st[0] = v;
           st[1] = -v;
           break;
@@ -1175,23 +1175,29 @@ __device__ void state_charges(const TopoDev& T, const double* rec, const double*
   }
 }
 
-// Newton on one lane (converger.newton at W = 1 on the frozen tape), for
-// the transient's operating point (no companion) and its steps. `vcache`
-// (T.n_src values) takes the V sources' values, which depend on the time
-// point alone, once for all the iterations. Returns 0 converged (x holds
-// the published iterate), 1 out of iterations, 2 the factor left the tape.
-__device__ int lane_newton(const TopoDev& T, uint32_t prog, const LaneMem& m, const double* rec, const LaneOpts& o,
-                           const SimDev& sim, const Companion* cp, bool& lim_active, bool init_fix,
-                           uint32_t& iters, double* vcache, int tid) {
-  const uint32_t n = T.n;
-  const uint32_t max_iter = o.max_iter < 100 ? 100 : o.max_iter;
+// The V and I sources' values at `sim` (they depend on the time point and
+// the source scale alone), once for all the Newton iterations there.
+__device__ void fill_sources(const TopoDev& T, const double* rec, const SimDev& sim, double* vcache, int tid) {
   for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
     const BatchDev& B = T.b[bi];
-    if (B.type != kV) continue;
+    if (B.type != kV && B.type != kI) continue;
     for (uint32_t i = tid; i < B.count; i += 32)
-      vcache[B.src_off + i] = vsource_value(rec + B.rec_off + i, static_cast<int>(B.count), sim);
+      vcache[B.src_off + i] = B.type == kV ? vsource_value(rec + B.rec_off + i, static_cast<int>(B.count), sim)
+                                           : rec[B.rec_off + i] * sim.src_scale;
   }
   __syncwarp();
+}
+
+// Newton on one lane (converger.newton at W = 1 on the frozen tape), for
+// the transient's operating point (no companion) and its steps, and for the
+// points of a sequential sweep. `vcache` holds the sources' values
+// (fill_sources). Returns 0 converged (x holds the published iterate), 1
+// out of iterations, 2 the factor left the tape.
+__device__ int lane_newton(const TopoDev& T, uint32_t prog, const LaneMem& m, const double* rec, const LaneOpts& o,
+                           const SimDev& sim, const Companion* cp, bool& lim_active, bool init_fix,
+                           uint32_t& iters, const double* vcache, int tid) {
+  const uint32_t n = T.n;
+  const uint32_t max_iter = o.max_iter < 100 ? 100 : o.max_iter;
   double limit = kXPlausible;
   for (uint32_t iter = 0; iter < max_iter; ++iter) {
     eval_all(T, rec, m, lim_active, sim, tid, false, vcache);
@@ -1200,6 +1206,21 @@ __device__ int lane_newton(const TopoDev& T, uint32_t prog, const LaneMem& m, co
     __syncwarp();
     if (cp) {
       companion(T, prog, m, *cp, tid);
+      __syncwarp();
+    }
+    if (o.gmin > 0) {
+      // loadExtras (converger.zig:321-330): diagonal gmin and its residual form
+      for (uint32_t p = tid; p < T.nnz; p += 32) {
+        const uint32_t row = T.slot_row[p];
+        if (row != kNoDiag) {
+          const double d = m.diag[row] + o.gmin;
+          m.diag[row] = d;
+          m.v[T.amap[p]] = d;
+        }
+      }
+      for (uint32_t i = tid; i < n; i += 32) m.rhs[i] += o.gmin * m.x[i];
+      __syncwarp();
+      load_y(T, m.rhs, m.y, tid);
       __syncwarp();
     }
     if (iter == 0) {
@@ -1358,7 +1379,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
   double* ipr = qh + 4 * n;
   double* qt = ipr + n;    // 4 slots of nq: the LTE-state ring
   double* ipt = qt + 4 * nq;
-  double* vsrc = ipt + nq;  // T.n_src: the V sources at the current time point
+  double* vsrc = ipt + nq;  // T.n_src: the V and I sources at the current time point
   const double* rec = L.rec + size_t(lane) * T.rec_size;
   uint32_t stat[kTsN];
   for (int k = 0; k < kTsN; ++k) stat[k] = 0;
@@ -1389,6 +1410,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
   op.gmin = 0.0;
   op.max_iter = 100;
   uint32_t it = 0;
+  fill_sources(T, rec, sim, vsrc, tid);
   int rc = lane_newton(T, prog, m, rec, op, sim, nullptr, lim_active, true, it, vsrc, tid);
   lim_active = false;
   stat[kTsOpIters] = it;
@@ -1469,6 +1491,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
       __syncwarp();
       Companion c{ag0, ag1, trap, slot(qh, n, 1), ipr};
       uint32_t iters = 0;
+      fill_sources(T, rec, sim, vsrc, tid);
       rc = lane_newton(T, prog, m, rec, nr, sim, &c, lim_active, false, iters, vsrc, tid);
       lim_active = false;
       stat[kTsAttempts] += 1;
@@ -1588,6 +1611,113 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
   if (tid == 0 && P.n_pts) P.n_pts[lane] = n_rec;
 }
 
+// One lane's sequential .dc sweep over the points of one swept source
+// (dc.zig Sweep, :163-386): per point the MODEINITPRED predictor
+// 2 last - prev (:330-337), limited against the last point (prepareWarm,
+// :342-347), and a warm Newton; when that fails, or before any point has
+// converged, a cold start (op.zig coldStart: zero x and the junction seeds)
+// and Newton with MODEINITFIX at the operating point's 100 iterations, the
+// ladder's plain rung (endPoint, dc.zig:361-365). Point 0, once converged,
+// is also `prev` (dc.zig:376-379, after dctrcurv.c). A factor that leaves
+// the lead tape ends the lane's sweep (kSweepLeftTape); its later points
+// read not converged.
+__device__ void sweep_lane(const TopoDev& T, const LaneDev& L, const SweepDev& P, const LaneOpts& o, uint32_t prog,
+                           double* block, uint32_t lane, int tid) {
+  const uint32_t n = T.n;
+  LaneMem m = carve(T, block);
+  double* sol = block + T.smem_doubles;
+  double* prev = sol + n;
+  double* vsrc = prev + n;  // T.n_src
+  const double* rec = L.rec + size_t(lane) * T.rec_size;
+  init_consts(T, m.v, tid);
+  SimDev sim;
+  sim.t = 0.0;
+  sim.src_scale = 1.0;
+  sim.kind = 0;
+  fill_sources(T, rec, sim, vsrc, tid);
+  for (uint32_t i = tid; i < n; i += 32) {
+    sol[i] = 0.0;
+    prev[i] = 0.0;
+  }
+  LaneOpts cold_o = o;
+  cold_o.max_iter = 100;
+  uint32_t status = kSweepDone;
+  bool cold = true;
+  for (uint32_t pt = 0; pt < P.n_pts; ++pt) {
+    const size_t row = size_t(lane) * P.n_pts + pt;
+    if (status != kSweepDone) {
+      for (uint32_t i = tid; i < n; i += 32) P.x_out[row * n + i] = 0.0;
+      if (tid == 0) {
+        P.iters[row] = 0;
+        P.conv[row] = 0;
+      }
+      continue;
+    }
+    if (tid == 0) vsrc[P.src] = P.values[pt];
+    for (uint32_t i = tid; i < n; i += 32) {
+      const double last = sol[i];
+      sol[i] = 2.0 * last - prev[i];
+      prev[i] = last;
+    }
+    __syncwarp();
+    uint32_t it_total = 0;
+    int rc = 1;
+    bool lim_active = false;
+    if (!cold) {
+      for (uint32_t i = tid; i < n; i += 32) {
+        m.x[i] = sol[i];
+        m.xo[i] = prev[i];
+      }
+      __syncwarp();
+      apply_limits(T, rec, m, false, tid);
+      lim_active = T.nlim != 0;
+      __syncwarp();
+      uint32_t it = 0;
+      rc = lane_newton(T, prog, m, rec, o, sim, nullptr, lim_active, false, it, vsrc, tid);
+      it_total += it;
+      for (uint32_t i = tid; i < n; i += 32) sol[i] = m.x[i];
+      __syncwarp();
+    }
+    if (rc == 1) {
+      for (uint32_t i = tid; i < n; i += 32) m.x[i] = 0.0;
+      for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
+        const BatchDev& B = T.b[bi];
+        for (uint32_t i = tid; i < B.count; i += 32) {
+          if (B.type == kD) m.lim[B.lim_off + i] = rec[B.rec_off + kDVcrit * B.count + i];
+          if (B.type == kM) {
+            m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kMSeedVgs * B.count + i];
+            m.lim[B.lim_off + 3 * i + 1] = 0.0;
+            m.lim[B.lim_off + 3 * i + 2] = -1.0;
+          }
+        }
+      }
+      __syncwarp();
+      lim_active = T.nlim != 0;
+      uint32_t it = 0;
+      rc = lane_newton(T, prog, m, rec, cold_o, sim, nullptr, lim_active, true, it, vsrc, tid);
+      it_total += it;
+      for (uint32_t i = tid; i < n; i += 32) sol[i] = m.x[i];
+      __syncwarp();
+    }
+    if (rc == 2) status = kSweepLeftTape;
+    const bool converged = rc == 0;
+    for (uint32_t i = tid; i < n; i += 32) P.x_out[row * n + i] = sol[i];
+    if (tid == 0) {
+      P.iters[row] = it_total;
+      P.conv[row] = converged ? 1 : 0;
+    }
+    if (converged) {
+      if (pt == 0)
+        for (uint32_t i = tid; i < n; i += 32) prev[i] = sol[i];
+      cold = false;
+    } else {
+      cold = true;
+    }
+    __syncwarp();
+  }
+  if (tid == 0) P.status[lane] = status;
+}
+
 // Uneven batching: lanes of several topologies (circuits of different sizes)
 // in one launch. CTA b serves topology cta_ctx[b], lanes cta_first[b] ..
 // + ctx_lpb[that topology] (one warp each); it copies its topology's tables
@@ -1636,6 +1766,29 @@ __global__ void __launch_bounds__(256) tran_kernel(TopoDev T, LaneDev L, TranDev
     tran_lane(T, L, P, o, prog, block, lane, tid);
     __syncwarp();
   }
+}
+
+__global__ void __launch_bounds__(256) sweep_kernel(TopoDev T, LaneDev L, SweepDev P, LaneOpts o) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* lanes_smem = stage_programs(T, smem_raw);
+  const uint32_t prog = saddr(smem_raw);
+  const int tid = threadIdx.x & 31;
+  const uint32_t warps = blockDim.x >> 5, w = threadIdx.x >> 5;
+  double* block = lanes_smem + size_t(w) * sweep_doubles(T);
+  for (uint32_t lane = blockIdx.x * warps + w; lane < L.n_lanes; lane += gridDim.x * warps) {
+    sweep_lane(T, L, P, o, prog, block, lane, tid);
+    __syncwarp();
+  }
+}
+
+cudaError_t launch_sweep(const TopoDev& T, const LaneDev& L, const SweepDev& P, const LaneOpts& o,
+                         uint32_t lanes_per_block, cudaStream_t s) {
+  const size_t smem = T.prog_bytes + lanes_per_block * size_t(sweep_doubles(T)) * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  sweep_kernel<<<persistent_grid(sweep_kernel, L.n_lanes, lanes_per_block, smem), 32 * lanes_per_block, smem, s>>>(
+      T, L, P, o);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_tran(const TopoDev& T, const LaneDev& L, const TranDev& P, const LaneOpts& o,

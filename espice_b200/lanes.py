@@ -28,7 +28,7 @@ LANE_CONVERGED, LANE_MAX_ITER, LANE_SINGULAR, LANE_NEED_SOLVE = 1, 2, 3, 4
 EXPORTS = ["esl_create", "esl_destroy", "esl_last_error", "esl_dims", "esl_set_lanes",
            "esl_dc_solve", "esl_dc_solve_device", "esl_dc_solve_device_static", "esl_tape", "esl_lu_replay_device",
            "esl_tape_size", "esl_pattern", "esl_compile_tape", "esl_tran", "esl_tran_device", "esl_lu_lanes_device",
-           "esl_lu_lanes_mixed_device", "esl_group_dc_solve_device", "esl_autotune"]
+           "esl_lu_lanes_mixed_device", "esl_group_dc_solve_device", "esl_autotune", "esl_dc_sweep_device"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 f64p = ctypes.POINTER(ctypes.c_double)
@@ -75,6 +75,7 @@ def tran_opts(t_stop, t_step, t_max=0.0, reltol=1e-3, abstol=1e-12, vntol=1e-6, 
 
 TS_FIELDS = ["status", "accepted", "attempts", "nr_iters", "rej_newton", "rej_lte", "bp_landings", "op_iters"]
 TRAN_DONE, TRAN_UNDERFLOW, TRAN_OP_FAILED, TRAN_MAX_STEPS, TRAN_LEFT_TAPE = 0, 1, 2, 3, 4
+SWEEP_DONE, SWEEP_LEFT_TAPE = 0, 4
 
 
 class TapeInfo(ctypes.Structure):
@@ -281,6 +282,29 @@ class DcLanes:
                                             ctypes.c_uint32(0), None, None, None, ctypes.byref(ms)),
                     "esl_tran_device")
         return ms.value
+
+    def sweep(self, slot, values, opts=None):
+        """Sequential .dc sweeps, one per lane (esl_dc_sweep_device): every
+        lane sweeps the DC value of the V or I source at `slot` through
+        `values`. Returns (x [lanes][points][n], iters [lanes][points],
+        converged [lanes][points] bool, status [lanes], kernel ms)."""
+        import torch
+        opts = opts or newton_opts()
+        values = np.ascontiguousarray(values, np.float64).reshape(-1)
+        N, P = self.n_lanes, len(values)
+        d_x = torch.empty((N, P, self.n), dtype=torch.float64, device="cuda")
+        d_it = torch.empty((N, P), dtype=torch.int32, device="cuda")
+        d_cv = torch.empty((N, P), dtype=torch.uint8, device="cuda")
+        d_st = torch.empty(N, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        ms = ctypes.c_float(0)
+        self._check(self._L.esl_dc_sweep_device(self._ctx, ctypes.byref(slot), _p(values, f64p), ctypes.c_uint32(P),
+                                                ctypes.byref(opts), ctypes.c_void_p(d_x.data_ptr()),
+                                                ctypes.c_void_p(d_it.data_ptr()), ctypes.c_void_p(d_cv.data_ptr()),
+                                                ctypes.c_void_p(d_st.data_ptr()), ctypes.byref(ms)),
+                    "esl_dc_sweep_device")
+        return (d_x.cpu().numpy(), d_it.cpu().numpy().astype(np.uint32), d_cv.cpu().numpy().astype(bool),
+                d_st.cpu().numpy().astype(np.uint32), ms.value)
 
     def autotune(self, x0=None, opts=None):
         """Times lanes per CTA 1/2/4/8 on the current lanes and keeps the fastest."""

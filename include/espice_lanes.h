@@ -213,6 +213,24 @@ int32_t esl_tran_device(esl_ctx *ctx, const esl_tran_opts *opts, double *d_x, ui
                         const uint32_t *d_probes, uint32_t n_probes, uint32_t max_pts,
                         double *d_t, double *d_v, uint32_t *d_n_pts, float *ms);
 
+/* Sequential .dc sweeps, one per lane (dc.zig Sweep :163-386; the
+ * reference's `.dc` path, which the oracle's orc_dc_sweep restates): every
+ * lane (its own parameters from esl_set_lanes) sweeps the DC value of one V
+ * or I source (`slot`, parameter 0) through values[0 .. n_pts). Per point: the
+ * MODEINITPRED predictor 2 last - prev, limited against the last point, a
+ * warm Newton; on its failure, or before a point has converged, a cold start
+ * with MODEINITFIX at 100 iterations (op.zig's plain rung). Device buffers:
+ * d_x [n_lanes][n_pts][n], d_iters [n_lanes][n_pts] (both solves of a
+ * point), d_conv [n_lanes][n_pts], d_status [n_lanes] (ESL_SWEEP_*). A lane
+ * whose factor leaves the lead pivot tape stops there with
+ * ESL_SWEEP_LEFT_TAPE (its later points read 0 and not converged; its
+ * sweep is the CPU's). ESL_NOT_ELIGIBLE for a slot that is not a source's
+ * DC value. ms: the kernel's device time (may be NULL). */
+enum { ESL_SWEEP_DONE = 0, ESL_SWEEP_LEFT_TAPE = 4 };
+int32_t esl_dc_sweep_device(esl_ctx *ctx, const esl_slot *slot, const double *values, uint32_t n_pts,
+                            const esl_newton_opts *opts, double *d_x, uint32_t *d_iters, uint8_t *d_conv,
+                            uint32_t *d_status, float *ms);
+
 /* Uneven batching: the DC solves of n_ctx contexts (circuits of any sizes,
  * one device) in one launch, each context's lanes with its own topology and
  * tape; per context its device buffers as esl_dc_solve_device takes them,

@@ -137,6 +137,14 @@ int orc_dc_sweep(const orc_circuit *c, orc_slot slot, const double *values,
                  uint32_t n_pts, const orc_newton_opts *opts, double *x_out,
                  uint32_t *iters, uint8_t *conv);
 
+/* One sequential sweep per lane, each lane first setting slots[] to its row
+ * of lane_values [n_lanes][n_slots]; x_out [n_lanes][n_pts][n], iters and
+ * conv [n_lanes][n_pts]. */
+int orc_dc_sweep_lanes(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
+                       const double *lane_values, uint32_t n_lanes, orc_slot sweep,
+                       const double *values, uint32_t n_pts, const orc_newton_opts *opts,
+                       double *x_out, uint32_t *iters, uint8_t *conv);
+
 /* Operating point (op.zig solve, plain rung, cold start). */
 int orc_op(const orc_circuit *c, const orc_newton_opts *opts, double *x_out,
            uint32_t *iters);

@@ -161,6 +161,25 @@ def dc_sweep(frozen, slot, values, opts=None):
     return x, it, cv
 
 
+def dc_sweep_lanes(frozen, slots, lane_values, sweep_slot, values, opts=None):
+    """One sequential sweep per lane (esl_dc_sweep_device's semantics):
+    x [lanes][points][n], iters [lanes][points], conv [lanes][points]."""
+    opts = opts or newton_opts()
+    values = np.ascontiguousarray(values, np.float64)
+    lane_values = np.ascontiguousarray(lane_values, np.float64).reshape(-1, max(1, len(slots)))
+    lanes, pts = lane_values.shape[0], len(values)
+    sa = frozen.slots_array(slots)
+    x = np.zeros((lanes, pts, frozen.n))
+    it = np.zeros((lanes, pts), np.uint32)
+    cv = np.zeros((lanes, pts), np.uint8)
+    rc = lib().orc_dc_sweep_lanes(ctypes.byref(frozen.struct()), sa, ctypes.c_uint32(len(slots)),
+                                  _p(lane_values, f64p), ctypes.c_uint32(lanes), sweep_slot,
+                                  _p(values, f64p), ctypes.c_uint32(pts), ctypes.byref(opts),
+                                  _p(x, f64p), _p(it, u32p), _p(cv, u8p))
+    assert rc == 0
+    return x, it, cv
+
+
 def op(frozen, opts=None):
     opts = opts or newton_opts(max_iter=100)
     x = np.zeros(frozen.n)

@@ -363,12 +363,11 @@ int orc_op(const orc_circuit *c, const orc_newton_opts *opts, double *x_out, uin
     return rc;
 }
 
-int orc_dc_sweep(const orc_circuit *c, orc_slot slot, const double *values,
-                 uint32_t n_pts, const orc_newton_opts *opts, double *x_out,
-                 uint32_t *iters, uint8_t *conv) {
-    ckt_t k;
-    if (ckt_init(&k, c)) return -1;
-    uint32_t n = c->n;
+/* One sequential sweep on an initialized circuit (dc.zig Sweep :163-386). */
+static void sweep_run(ckt_t *kp, orc_slot slot, const double *values, uint32_t n_pts,
+                      const orc_newton_opts *opts, double *x_out, uint32_t *iters, uint8_t *conv) {
+    ckt_t k = *kp;
+    uint32_t n = k.n;
     double *sol = (double *)calloc(n, sizeof(double));
     double *prev = (double *)calloc(n, sizeof(double));
     int cold = 1;
@@ -411,7 +410,33 @@ int orc_dc_sweep(const orc_circuit *c, orc_slot slot, const double *values,
     }
     free(sol);
     free(prev);
+    *kp = k;
+}
+
+int orc_dc_sweep(const orc_circuit *c, orc_slot slot, const double *values,
+                 uint32_t n_pts, const orc_newton_opts *opts, double *x_out,
+                 uint32_t *iters, uint8_t *conv) {
+    ckt_t k;
+    if (ckt_init(&k, c)) return -1;
+    sweep_run(&k, slot, values, n_pts, opts, x_out, iters, conv);
     ckt_free(&k);
+    return 0;
+}
+
+/* One sequential sweep per lane, each lane first setting its own slots
+ * (esl_dc_sweep_device's semantics). x_out [lanes][n_pts][n]. */
+int orc_dc_sweep_lanes(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
+                       const double *lane_values, uint32_t n_lanes, orc_slot sweep,
+                       const double *values, uint32_t n_pts, const orc_newton_opts *opts,
+                       double *x_out, uint32_t *iters, uint8_t *conv) {
+    for (uint32_t l = 0; l < n_lanes; l++) {
+        ckt_t k;
+        if (ckt_init(&k, c)) return -1;
+        for (uint32_t s = 0; s < n_slots; s++) ckt_set(&k, slots[s], lane_values[(size_t)l * n_slots + s]);
+        const size_t at = (size_t)l * n_pts;
+        sweep_run(&k, sweep, values, n_pts, opts, x_out + at * c->n, iters + at, conv + at);
+        ckt_free(&k);
+    }
     return 0;
 }
 
