@@ -647,9 +647,10 @@ int32_t upload_tape(esl_ctx* ctx) {
   ctx->lanes_eff = std::max<uint32_t>(1, std::min<uint32_t>(8, uint32_t((room - T.prog_bytes) / lane_bytes)));
   // Transient lanes add the accepted points, the charge rings and dynamic
   // currents over the rows and the LTE states: cur | prev | q[4] | ip over
-  // n, then q[4] | ip over n_qt, then the V sources' values at the current
-  // time point.
-  T.tran_doubles = (T.smem_doubles + 7 * T.n + 5 * T.n_qt + T.n_src + 1) & ~1u;
+  // n, then q[4] | ip over n_qt, then the V and I sources' values at the
+  // current time point and the PULSE corner timers (4 start/period pairs
+  // per source).
+  T.tran_doubles = (T.smem_doubles + 7 * T.n + 5 * T.n_qt + 9 * T.n_src + 1) & ~1u;
   const size_t tran_bytes = size_t(T.tran_doubles) * 8;
   ctx->tran_lanes_eff = T.prog_bytes + tran_bytes > room
                             ? 0

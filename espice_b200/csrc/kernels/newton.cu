@@ -1137,12 +1137,17 @@ __device__ void companion(const TopoDev& T, uint32_t prog, const LaneMem& m, con
   }
 }
 
-// Row charges of the last evaluation (the q plane, ground row 0 empty).
-__device__ __forceinline__ void row_charges(const TopoDev& T, const LaneMem& m, double* q, int tid) {
-  for (uint32_t i = tid; i < T.n; i += 32) {
-    double s = 0.0;
-    for (uint32_t e = T.q_ptr[i]; e < T.q_ptr[i + 1]; ++e) s = __dadd_rn(s, m.st[T.q_src[e]]);
-    q[i] = s;
+// Row charges of the last evaluation (the q plane) for the rows with charge
+// cells, from the companion program's row part; the other rows' charges are
+// zero in every slot of the ring from the start and stay so.
+__device__ __forceinline__ void row_charges(const TopoDev& T, uint32_t prog, const LaneMem& m, double* q, int tid) {
+  const uint32_t lb = saddr(m.base);
+  const uint32_t depth = prog + T.o_k_depth, koff = prog + T.o_k_off;
+  const uint32_t ksrc = prog + T.o_k_src, kdst = prog + T.o_k_dst;
+  for (uint32_t g = 0; g < T.n_kr_groups; ++g) {
+    const double s = gather_sum(ksrc + 4 * (lds_u32(koff + 4 * g) + tid), lds_u32(depth + 4 * g), lb);
+    const uint32_t row = lds_u32(kdst + 8 * (g * 32 + tid));
+    if (row != kNoDiag) q[row] = s;
   }
 }
 
@@ -1336,15 +1341,25 @@ __device__ __forceinline__ bool almost_equal_ulps(double a, double b, long long 
 
 // The first PULSE corner at or after `after` over every V source with a
 // PULSE wave (models/vsource.va:133-136: four periodic timers per source).
-__device__ bool next_bp(const TopoDev& T, const double* rec, double after, double& bp) {
-  double best = CUDART_INF;
+// The PULSE corner timers (vsource.va:133-136, the 4 periodic timers of
+// each V source with a PULSE wave) into `tm`: timer k at tm[2 k] (start)
+// and tm[2 k + 1] (period); 4 per V source, start +inf where the source has
+// no PULSE wave. Each lane computes its table once.
+__device__ void pulse_timers(const TopoDev& T, const double* rec, double* tm, int tid) {
   for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
     const BatchDev& B = T.b[bi];
     if (B.type != kV) continue;
     const int s = static_cast<int>(B.count);
-    for (uint32_t i = 0; i < B.count; ++i) {
+    for (uint32_t i = tid; i < B.count; i += 32) {
       const double* p = rec + B.rec_off + i;
-      if (p[1 * s] != 1.0) continue;
+      double* t = tm + 8 * (B.src_off + i);
+      if (p[1 * s] != 1.0) {
+        for (int k = 0; k < 4; ++k) {
+          t[2 * k] = CUDART_INF;
+          t[2 * k + 1] = 1.0;
+        }
+        continue;
+      }
       const double tr = p[5 * s] > 1.0e-12 ? p[5 * s] : 1.0e-12;
       const double tf = p[6 * s] > 1.0e-12 ? p[6 * s] : 1.0e-12;
       const double pwr = p[7 * s];
@@ -1355,16 +1370,31 @@ __device__ bool next_bp(const TopoDev& T, const double* rec, double after, doubl
       const double td = p[4 * s];
       const double st[4] = {td, td + tr, td + tr + pw, td + tr + pw + tf};
       for (int k = 0; k < 4; ++k) {
-        double t = st[k];
-        if (t < after) {
-          const double kk = ceil(div_rn(after - st[k], per));
-          t = st[k] + kk * per;
-          if (t < after) t += per;
-        }
-        if (t < best) best = t;
+        t[2 * k] = st[k];
+        t[2 * k + 1] = per;
       }
     }
   }
+  __syncwarp();
+}
+
+// The first timer event at or after `after` (tran.zig nextBp), the timers
+// spread over the warp and the earliest taken by a warp minimum.
+__device__ bool next_bp(const TopoDev& T, const double* tm, double after, double& bp) {
+  const int tid = threadIdx.x & 31;
+  double best = CUDART_INF;
+  for (uint32_t k = tid; k < 4 * T.n_src; k += 32) {
+    const double start = tm[2 * k], per = tm[2 * k + 1];
+    if (!(start < CUDART_INF)) continue;
+    double t = start;
+    if (t < after) {
+      const double kk = ceil(div_rn(after - start, per));
+      t = start + kk * per;
+      if (t < after) t += per;
+    }
+    if (t < best) best = t;
+  }
+  best = warp_fmin(best);
   if (best == CUDART_INF) return false;
   bp = best;
   return true;
@@ -1383,6 +1413,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
   double* qt = ipr + n;    // 4 slots of nq: the LTE-state ring
   double* ipt = qt + 4 * nq;
   double* vsrc = ipt + nq;  // T.n_src: the V and I sources at the current time point
+  double* tmr = vsrc + T.n_src;  // 8 T.n_src: the PULSE corner timers
   const double* rec = L.rec + size_t(lane) * T.rec_size;
   uint32_t stat[kTsN];
   for (int k = 0; k < kTsN; ++k) stat[k] = 0;
@@ -1437,7 +1468,9 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
     sim.kind = 1;
     eval_all(T, rec, m, false, sim, tid, true);
     __syncwarp();
-    row_charges(T, m, qh + n, tid);
+    for (uint32_t i = tid; i < 4 * n; i += 32) qh[i] = 0.0;
+    __syncwarp();
+    row_charges(T, prog, m, qh + n, tid);
     state_charges(T, rec, m.x, qt + nq, tid);
     __syncwarp();
     for (uint32_t i = tid; i < n; i += 32) {
@@ -1455,12 +1488,13 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
     uint32_t hb = 0;  // ring slot r lives at (hb + r) & 3
     auto slot = [&](double* base, uint32_t len, uint32_t r) { return base + size_t((hb + r) & 3u) * len; };
 
+    pulse_timers(T, rec, tmr, tid);
     const double dt_max = P.dt_max;
     const double delmin = 1e-11 * dt_max;
     const double min_break = 10.0 * delmin;
     double dt = fmin(div_rn(fmin(P.t_step, div_rn(P.t_stop, 100.0)), 10.0), dt_max);
     double bp0;
-    if (next_bp(T, rec, min_break, bp0)) dt = fmin(dt, 0.1 * bp0);
+    if (next_bp(T, tmr, min_break, bp0)) dt = fmin(dt, 0.1 * bp0);
     dt = div_rn(dt, 10.0);
     double dt_old[6];
     for (int k = 0; k < 6; ++k) dt_old[k] = dt_max;
@@ -1517,7 +1551,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
       if (has_charge) {
         eval_all(T, rec, m, false, sim, tid, true);
         __syncwarp();
-        row_charges(T, m, slot(qh, n, 0), tid);
+        row_charges(T, prog, m, slot(qh, n, 0), tid);
         state_charges(T, rec, m.x, slot(qt, nq, 0), tid);
         __syncwarp();
       }
@@ -1585,13 +1619,13 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
           stat[kTsBpLandings] += 1;
           order = 1;
           double shrink = bp_save_dt, nb;
-          if (next_bp(T, rec, t_new + min_break, nb)) shrink = fmin(shrink, nb - t_new);
+          if (next_bp(T, tmr, t_new + min_break, nb)) shrink = fmin(shrink, nb - t_new);
           dt_next = fmin(dt_next, 0.1 * shrink);
         }
         have_bp = false;
       }
       record(t_new);
-      have_bp = next_bp(T, rec, t_new + min_break, bp_next);
+      have_bp = next_bp(T, tmr, t_new + min_break, bp_next);
       bp_clamped = false;
       if (have_bp) {
         const double dt_to_bp = bp_next - t_new;
