@@ -77,12 +77,19 @@ enum SweepStatus : uint32_t {
   kSweepDone = 0,      // every point ran (each point's convergence is its own flag)
   kSweepLeftTape = 4,  // a factor left the lead pivot tape: the rest of the sweep is the CPU's
 };
+// Streamed measure cards and clause counts (esl_measure).
+enum MeasKind : uint32_t { kMeasWhen = 0, kMeasTrigTarg = 1, kMeasFindAt = 2 };
+constexpr int32_t kMeasUnset = -1;
+constexpr int32_t kMeasLast = -2;
+constexpr uint32_t kMaxMeas = 32;  // one warp thread per card
+
 enum TranStatus : uint32_t {
   kTranDone = 0,       // reached t_stop
   kTranUnderflow = 1,  // dt fell below dt_min
   kTranOpFailed = 2,   // the operating point did not converge
   kTranMaxSteps = 3,
   kTranLeftTape = 4,   // a factor left the lead pivot tape (needs a host factor)
+  kTranResolved = 5,   // every measure card resolved and the run stopped early
 };
 
 // LTE charge states per instance: one per ddt() site kept in the

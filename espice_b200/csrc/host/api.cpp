@@ -200,7 +200,7 @@ struct esl_ctx {
 
   DevBuf d_nodes[kMaxBatches], d_rhs_ptr, d_rhs_src, d_a_ptr, d_a_src, d_slot_row, d_cur;
   DevBuf d_q_ptr, d_q_src, d_c_ptr, d_c_src, d_probes, d_tran_t, d_tran_v, d_tran_n, d_tran_stats;
-  DevBuf d_amap, d_fill, d_prog, d_l_scaled, d_pinv, d_q, d_seq, d_sweep_values;
+  DevBuf d_amap, d_fill, d_prog, d_l_scaled, d_pinv, d_q, d_seq, d_sweep_values, d_meas;
   uint32_t n_seq_a = 0, n_seq = 0, seq_warps = 0;  // lane-interleaved op list
   uint32_t n_seq_f = 0, mixed_warps = 0;            // its forward-only tail, the mixed kernel's warps
   DevBuf d_row_ptr, d_row_slot, d_row_col;
@@ -1199,6 +1199,47 @@ int32_t esl_dc_sweep_device(esl_ctx* ctx, const esl_slot* slot, const double* va
   LaneDev L = lane_view(ctx, 0);
   ESL_CUDA(cudaEventRecord(ctx->ev0, s));
   ESL_CUDA(launch_sweep(T, L, P, o, lanes_per_cta(ctx, ctx->n_lanes, fit), s));
+  ESL_CUDA(cudaEventRecord(ctx->ev1, s));
+  ESL_CUDA(cudaEventSynchronize(ctx->ev1));
+  if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
+  return ESL_OK;
+}
+
+static_assert(sizeof(esl_meas_clause) == sizeof(MeasClauseDev) && sizeof(esl_measure) == sizeof(MeasDev),
+              "esl_measure and the device card share one layout");
+
+int32_t esl_tran_meas_device(esl_ctx* ctx, const esl_tran_opts* opts, const esl_measure* meas, uint32_t n_meas,
+                             int early_stop, double* d_x, uint32_t* d_stats, double* d_values, float* ms) {
+  if (!ctx || !meas || !d_x || !d_stats || !d_values || n_meas == 0 || ctx->n_lanes == 0)
+    return ESL_INVALID_ARGUMENT;
+  if (n_meas > kMaxMeas) return ctx->fail(ESL_INVALID_ARGUMENT, "at most 32 measure cards");
+  for (uint32_t c = 0; c < n_meas; ++c) {
+    const esl_measure& m = meas[c];
+    if (m.kind > ESL_MEAS_FIND_AT) return ctx->fail(ESL_INVALID_ARGUMENT, "unknown measure kind");
+    if (m.a.unknown >= ctx->pat.n || (m.kind == ESL_MEAS_TRIG_TARG && m.b.unknown >= ctx->pat.n))
+      return ctx->fail(ESL_INVALID_ARGUMENT, "measure probe out of range");
+  }
+  cudaSetDevice(ctx->device);
+  TranDev P;
+  LaneOpts lo;
+  if (int32_t rc = tran_view(ctx, opts, P, lo)) return rc;
+  if (int32_t rc = ensure_tape_cold(ctx)) return rc;
+  const TopoDev& T = ctx->topo;
+  const size_t lane_bytes = (size_t(T.tran_doubles) + size_t(kMeasDoubles) * n_meas) * 8, room = size_t(227) * 1024;
+  if (T.prog_bytes + lane_bytes > room) return ctx->fail(ESL_NOT_ELIGIBLE, "a transient lane exceeds a CTA's shared memory");
+  const uint32_t fit = std::max<uint32_t>(1, std::min<uint32_t>(8, uint32_t((room - T.prog_bytes) / lane_bytes)));
+  cudaStream_t s = ctx->stream;
+  ESL_CUDA(ctx->d_meas.ensure(size_t(n_meas) * sizeof(esl_measure)));
+  ESL_CUDA(cudaMemcpyAsync(ctx->d_meas.p, meas, size_t(n_meas) * sizeof(esl_measure), cudaMemcpyHostToDevice, s));
+  P.stats = d_stats;
+  P.meas = ctx->d_meas.as<MeasDev>();
+  P.n_meas = n_meas;
+  P.early_stop = early_stop ? 1u : 0u;
+  P.meas_out = d_values;
+  LaneDev L = lane_view(ctx, 0);
+  L.x = d_x;
+  ESL_CUDA(cudaEventRecord(ctx->ev0, s));
+  ESL_CUDA(launch_tran(T, L, P, lo, lanes_per_cta(ctx, ctx->n_lanes, fit), s));
   ESL_CUDA(cudaEventRecord(ctx->ev1, s));
   ESL_CUDA(cudaEventSynchronize(ctx->ev1));
   if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);

@@ -90,6 +90,29 @@ struct TopoDev {
 
 // One transient over every lane (tran.zig Sim): options, the probe trace
 // and the per-lane step statistics.
+// A streamed transient measure card (esl_measure's layout): WHEN, TRIG/TARG
+// or FIND AT over clauses of one probed unknown each.
+struct MeasClauseDev {
+  uint32_t unknown;
+  int32_t rise, fall, cross;  // -1 unset, -2 LAST, else the event count
+  double val, td, from, to, at;
+};
+struct MeasDev {
+  uint32_t kind, pad;
+  MeasClauseDev a, b;
+};
+// One clause's scan state (measure.zig Cross / At), in the lane's shared
+// memory: kMeasDoubles per card (two clauses).
+struct CrossDev {
+  double td, prev, prev_x, last, hit;
+  int32_t want_rise, want_fall, want_cross;
+  int32_t rise, fall, cross;
+  uint32_t first;
+  int32_t above, pending, found, over;
+  int32_t pad;
+};
+constexpr uint32_t kMeasDoubles = 2 * sizeof(CrossDev) / sizeof(double);
+
 struct TranDev {
   double t_stop, t_step, dt_max, dt_min;
   double reltol, abstol, vntol, chgtol, trtol;
@@ -100,6 +123,9 @@ struct TranDev {
   double* out_v;           // [lane][max_pts][n_probes]
   uint32_t* n_pts;         // [lane] rows recorded
   uint32_t* stats;         // [lane][kTsN]
+  const MeasDev* meas;     // [n_meas] cards fed every recorded row (null: none)
+  uint32_t n_meas, early_stop;
+  double* meas_out;        // [lane][n_meas] card values (NaN: unresolved)
 };
 
 // Sequential .dc sweeps, one per lane (dc.zig Sweep): the swept source

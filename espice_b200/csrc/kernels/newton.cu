@@ -1400,6 +1400,122 @@ __device__ bool next_bp(const TopoDev& T, const double* tm, double after, double
   return true;
 }
 
+// Streamed measures (src/output/measure.zig, after ngspice com_measure2.c):
+// Cross counts RISE/FALL/CROSS events from a clause's second sample and
+// interpolates the level crossing on the last segment (:1269-1365); At
+// takes the first segment holding AT (:1379-1398). Thread c runs card c.
+__device__ void meas_start(const MeasDev& mc, CrossDev* x) {
+  for (int k = 0; k < 2; ++k) {
+    const MeasClauseDev& c = k ? mc.b : mc.a;
+    CrossDev& s = x[k];
+    s.td = c.td;
+    s.prev = s.prev_x = 0.0;
+    s.last = s.hit = CUDART_NAN;
+    s.want_rise = c.rise;
+    s.want_fall = c.fall;
+    s.want_cross = c.cross;
+    s.rise = s.fall = s.cross = 0;
+    s.first = 0;
+    s.above = s.pending = s.found = s.over = 0;
+  }
+}
+
+// Cross.feed for one event; true once the scan is over (its event found,
+// or past TO).
+__device__ bool cross_feed(CrossDev& s, const MeasClauseDev& c, double xv, double v) {
+  if (s.over) return true;
+  if (xv < s.td) return false;
+  if (xv < c.from) return false;
+  if (c.to != 0.0 && xv > c.to) {
+    s.over = 1;
+    return true;
+  }
+  const double level = c.val, prev_level = c.val;
+  if (s.first == 1) {
+    s.cross = 0;
+    s.above = !(v < level);
+    if (!s.above && s.prev >= prev_level) {
+      s.fall = 1;
+      s.cross = 1;
+    } else if (s.above && s.prev < prev_level) {
+      s.rise = 1;
+      s.cross = 1;
+    }
+  }
+  if (s.first > 1) {
+    if (!s.above && v >= level) {
+      s.above = 1;
+      s.cross += 1;
+      s.rise += 1;
+      if (c.fall != kMeasLast) s.pending = 1;
+    } else if (s.above && v <= level) {
+      s.above = 0;
+      s.cross += 1;
+      s.fall += 1;
+      if (c.rise != kMeasLast) s.pending = 1;
+    }
+    const double hit = s.prev_x + div_rn((prev_level - s.prev) * (xv - s.prev_x), ((v - s.prev) - level) + prev_level);
+    if (s.cross == s.want_cross || s.rise == s.want_rise || s.fall == s.want_fall) {
+      s.hit = hit;
+      s.found = 1;
+      s.over = 1;
+      return true;
+    }
+    if (s.pending) {
+      if (c.cross == kMeasUnset && c.rise == kMeasUnset && c.fall == kMeasUnset) {
+        s.hit = hit;
+        s.found = 1;
+        s.over = 1;
+        return true;
+      }
+      if (c.cross == kMeasLast || c.rise == kMeasLast || c.fall == kMeasLast) s.last = hit;
+      s.pending = 0;
+    }
+  }
+  s.first += 1;
+  s.prev = v;
+  s.prev_x = xv;
+  return false;
+}
+
+__device__ bool at_feed(CrossDev& s, const MeasClauseDev& c, double xv, double v) {
+  if (s.over) return true;
+  if (s.first > 0 && s.prev_x <= c.at && xv >= c.at) {
+    s.hit = s.prev + div_rn((c.at - s.prev_x) * (v - s.prev), xv - s.prev_x);
+    s.found = 1;
+    s.over = 1;
+    return true;
+  }
+  s.first += 1;
+  s.prev_x = xv;
+  s.prev = v;
+  return false;
+}
+
+// Feeds the row (t, x) to card c; true once the card has resolved.
+__device__ bool meas_feed(const MeasDev& mc, CrossDev* x, double t, const double* xs) {
+  if (mc.kind == kMeasFindAt) return at_feed(x[0], mc.a, t, xs[mc.a.unknown]);
+  if (mc.kind == kMeasWhen) return cross_feed(x[0], mc.a, t, xs[mc.a.unknown]);
+  const bool da = cross_feed(x[0], mc.a, t, xs[mc.a.unknown]);
+  const bool db = cross_feed(x[1], mc.b, t, xs[mc.b.unknown]);
+  return da && db;
+}
+
+// A card's value at the end: WHEN the event time (else a LAST count's last
+// event, else NaN), TRIG/TARG targ - trig, FIND the interpolated value.
+__device__ double meas_value(const MeasDev& mc, const CrossDev* x) {
+  double v;
+  if (mc.kind == kMeasFindAt) {
+    v = x[0].found ? x[0].hit : CUDART_NAN;
+  } else if (mc.kind == kMeasWhen) {
+    v = x[0].found ? x[0].hit : x[0].last;
+  } else {
+    const double trig = x[0].found ? x[0].hit : x[0].last, targ = x[1].found ? x[1].hit : x[1].last;
+    v = isfinite(trig) && isfinite(targ) ? targ - trig : CUDART_NAN;
+  }
+  return isfinite(v) ? v : CUDART_NAN;
+}
+
 }  // namespace
 
 __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, const LaneOpts& o, uint32_t prog,
@@ -1414,6 +1530,10 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
   double* ipt = qt + 4 * nq;
   double* vsrc = ipt + nq;  // T.n_src: the V and I sources at the current time point
   double* tmr = vsrc + T.n_src;  // 8 T.n_src: the PULSE corner timers
+  // past the lane's tran_doubles: kMeasDoubles per measure card
+  CrossDev* mstate = reinterpret_cast<CrossDev*>(block + T.tran_doubles) + 2 * tid;
+  const bool card = P.meas && uint32_t(tid) < P.n_meas;
+  if (card) meas_start(P.meas[tid], mstate);
   const double* rec = L.rec + size_t(lane) * T.rec_size;
   uint32_t stat[kTsN];
   for (int k = 0; k < kTsN; ++k) stat[k] = 0;
@@ -1449,13 +1569,21 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
   lim_active = false;
   stat[kTsOpIters] = it;
   uint32_t n_rec = 0;
+  // Records the row (t, m.x) and feeds it to the measure cards; true while
+  // a card is still open.
   auto record = [&](double t) {
+    bool open = false;
+    if (P.meas) {
+      const bool done = card ? meas_feed(P.meas[tid], mstate, t, m.x) : true;
+      open = __any_sync(kFull, !done);
+    }
     if (P.out_t && n_rec < P.max_pts) {
       if (tid == 0) P.out_t[size_t(lane) * P.max_pts + n_rec] = t;
       for (uint32_t k = tid; k < P.n_probes; k += 32)
         P.out_v[(size_t(lane) * P.max_pts + n_rec) * P.n_probes + k] = m.x[P.probes[k]];
       ++n_rec;
     }
+    return open;
   };
   if (rc != 0) {
     stat[kTsStatus] = rc == 2 ? kTranLeftTape : kTranOpFailed;
@@ -1624,7 +1752,12 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
         }
         have_bp = false;
       }
-      record(t_new);
+      const bool open = record(t_new);
+      if (P.meas && P.early_stop && !open) {
+        // tran.zig:1060-1063: every card resolved, the run ends here
+        stat[kTsStatus] = kTranResolved;
+        break;
+      }
       have_bp = next_bp(T, tmr, t_new + min_break, bp_next);
       bp_clamped = false;
       if (have_bp) {
@@ -1644,6 +1777,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
     __syncwarp();
   }
   for (uint32_t i = tid; i < n; i += 32) L.x[size_t(lane) * n + i] = m.x[i];
+  if (card) P.meas_out[size_t(lane) * P.n_meas + tid] = meas_value(P.meas[tid], mstate);
   if (tid < kTsN) P.stats[size_t(lane) * kTsN + tid] = stat[tid];
   if (tid == 0 && P.n_pts) P.n_pts[lane] = n_rec;
 }
@@ -1798,7 +1932,7 @@ __global__ void __launch_bounds__(256) tran_kernel(TopoDev T, LaneDev L, TranDev
   const uint32_t prog = saddr(smem_raw);
   const int tid = threadIdx.x & 31;
   const uint32_t warps = blockDim.x >> 5, w = threadIdx.x >> 5;
-  double* block = lanes_smem + size_t(w) * T.tran_doubles;
+  double* block = lanes_smem + size_t(w) * (T.tran_doubles + kMeasDoubles * P.n_meas);
   for (uint32_t lane = blockIdx.x * warps + w; lane < L.n_lanes; lane += gridDim.x * warps) {
     tran_lane(T, L, P, o, prog, block, lane, tid);
     __syncwarp();
@@ -1830,7 +1964,8 @@ cudaError_t launch_sweep(const TopoDev& T, const LaneDev& L, const SweepDev& P, 
 
 cudaError_t launch_tran(const TopoDev& T, const LaneDev& L, const TranDev& P, const LaneOpts& o,
                         uint32_t lanes_per_block, cudaStream_t s) {
-  const size_t smem = T.prog_bytes + lanes_per_block * size_t(T.tran_doubles) * sizeof(double);
+  const size_t smem =
+      T.prog_bytes + lanes_per_block * size_t(T.tran_doubles + kMeasDoubles * P.n_meas) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(tran_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   tran_kernel<<<persistent_grid(tran_kernel, L.n_lanes, lanes_per_block, smem), 32 * lanes_per_block, smem, s>>>(

@@ -28,7 +28,8 @@ LANE_CONVERGED, LANE_MAX_ITER, LANE_SINGULAR, LANE_NEED_SOLVE = 1, 2, 3, 4
 EXPORTS = ["esl_create", "esl_destroy", "esl_last_error", "esl_dims", "esl_set_lanes",
            "esl_dc_solve", "esl_dc_solve_device", "esl_dc_solve_device_static", "esl_tape", "esl_lu_replay_device",
            "esl_tape_size", "esl_pattern", "esl_compile_tape", "esl_tran", "esl_tran_device", "esl_lu_lanes_device",
-           "esl_lu_lanes_mixed_device", "esl_group_dc_solve_device", "esl_autotune", "esl_dc_sweep_device"]
+           "esl_lu_lanes_mixed_device", "esl_group_dc_solve_device", "esl_autotune", "esl_dc_sweep_device",
+           "esl_tran_meas_device"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 f64p = ctypes.POINTER(ctypes.c_double)
@@ -76,6 +77,41 @@ def tran_opts(t_stop, t_step, t_max=0.0, reltol=1e-3, abstol=1e-12, vntol=1e-6, 
 TS_FIELDS = ["status", "accepted", "attempts", "nr_iters", "rej_newton", "rej_lte", "bp_landings", "op_iters"]
 TRAN_DONE, TRAN_UNDERFLOW, TRAN_OP_FAILED, TRAN_MAX_STEPS, TRAN_LEFT_TAPE = 0, 1, 2, 3, 4
 SWEEP_DONE, SWEEP_LEFT_TAPE = 0, 4
+TRAN_RESOLVED = 5
+
+
+class MeasClause(ctypes.Structure):
+    """esl_meas_clause: the probed unknown, RISE/FALL/CROSS counts (MEAS_UNSET,
+    MEAS_LAST or k >= 1), VAL, TD, FROM, TO (0: none), AT."""
+    _fields_ = [("unknown", ctypes.c_uint32), ("rise", ctypes.c_int32), ("fall", ctypes.c_int32),
+                ("cross", ctypes.c_int32), ("val", ctypes.c_double), ("td", ctypes.c_double),
+                ("from_", ctypes.c_double), ("to", ctypes.c_double), ("at", ctypes.c_double)]
+
+
+class Measure(ctypes.Structure):
+    """esl_measure: MEAS_WHEN (a), MEAS_TRIG_TARG (a = TRIG, b = TARG) or MEAS_FIND_AT (a)."""
+    _fields_ = [("kind", ctypes.c_uint32), ("pad", ctypes.c_uint32), ("a", MeasClause), ("b", MeasClause)]
+
+
+MEAS_WHEN, MEAS_TRIG_TARG, MEAS_FIND_AT = 0, 1, 2
+MEAS_UNSET, MEAS_LAST = -1, -2
+
+
+def meas_clause(unknown, val=1e99, rise=MEAS_UNSET, fall=MEAS_UNSET, cross=MEAS_UNSET, td=0.0, from_=0.0,
+                to=0.0, at=1e99):
+    return MeasClause(unknown, rise, fall, cross, val, td, from_, to, at)
+
+
+def when(unknown, val, rise=MEAS_UNSET, fall=MEAS_UNSET, cross=MEAS_UNSET, td=0.0):
+    return Measure(MEAS_WHEN, 0, meas_clause(unknown, val, rise, fall, cross, td), meas_clause(0))
+
+
+def trig_targ(trig, targ):
+    return Measure(MEAS_TRIG_TARG, 0, trig, targ)
+
+
+def find_at(unknown, at):
+    return Measure(MEAS_FIND_AT, 0, meas_clause(unknown, at=at), meas_clause(0))
 
 
 class TapeInfo(ctypes.Structure):
@@ -305,6 +341,25 @@ class DcLanes:
                     "esl_dc_sweep_device")
         return (d_x.cpu().numpy(), d_it.cpu().numpy().astype(np.uint32), d_cv.cpu().numpy().astype(bool),
                 d_st.cpu().numpy().astype(np.uint32), ms.value)
+
+    def tran_meas(self, opts, measures, early_stop=False):
+        """esl_tran_meas_device: the transient with streamed measure cards.
+        Returns (values [lanes][n_meas] (NaN: unresolved), stats [lanes][8],
+        x [lanes][n], kernel ms)."""
+        import torch
+        N, M = self.n_lanes, len(measures)
+        cards = (Measure * M)(*measures)
+        d_x = torch.empty((N, self.n), dtype=torch.float64, device="cuda")
+        d_st = torch.empty((N, len(TS_FIELDS)), dtype=torch.int32, device="cuda")
+        d_v = torch.empty((N, M), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        ms = ctypes.c_float(0)
+        self._check(self._L.esl_tran_meas_device(self._ctx, ctypes.byref(opts), cards, ctypes.c_uint32(M),
+                                                 ctypes.c_int(1 if early_stop else 0),
+                                                 ctypes.c_void_p(d_x.data_ptr()), ctypes.c_void_p(d_st.data_ptr()),
+                                                 ctypes.c_void_p(d_v.data_ptr()), ctypes.byref(ms)),
+                    "esl_tran_meas_device")
+        return (d_v.cpu().numpy(), d_st.cpu().numpy().astype(np.uint32), d_x.cpu().numpy(), ms.value)
 
     def autotune(self, x0=None, opts=None):
         """Times lanes per CTA 1/2/4/8 on the current lanes and keeps the fastest."""

@@ -213,6 +213,34 @@ int32_t esl_tran_device(esl_ctx *ctx, const esl_tran_opts *opts, double *d_x, ui
                         const uint32_t *d_probes, uint32_t n_probes, uint32_t max_pts,
                         double *d_t, double *d_v, uint32_t *d_n_pts, float *ms);
 
+/* Streamed transient measures (.meas tran, src/output/measure.zig, a port
+ * of ngspice com_measure2.c): every recorded row (t = 0 and each accepted
+ * step) feeds each card. WHEN: the time of a clause's event; TRIG/TARG:
+ * targ - trig (each clause with its own TD); FIND .. AT=: the value at a
+ * time. A clause: the probed unknown, the level VAL, RISE/FALL/CROSS counts
+ * (ESL_MEAS_UNSET, ESL_MEAS_LAST or k >= 1), TD, FROM, TO (0: none), AT. An
+ * event is counted from the clause's second sample and its time is the
+ * level crossing interpolated on the last segment, as ngspice does. */
+enum { ESL_MEAS_WHEN = 0, ESL_MEAS_TRIG_TARG = 1, ESL_MEAS_FIND_AT = 2 };
+enum { ESL_MEAS_UNSET = -1, ESL_MEAS_LAST = -2 };
+typedef struct {
+    uint32_t unknown;
+    int32_t rise, fall, cross;
+    double val, td, from, to, at;
+} esl_meas_clause;
+typedef struct {
+    uint32_t kind, pad;
+    esl_meas_clause a, b;  /* b: TRIG/TARG's target */
+} esl_measure;
+enum { ESL_TRAN_RESOLVED = 5 };
+
+/* esl_tran_device (no trace) with up to 32 measure cards: d_values
+ * [n_lanes][n_meas] the cards' values (NaN: unresolved). With early_stop a
+ * lane ends its transient once every card has resolved (tran.zig:1057-1064,
+ * `early_stop`), with status ESL_TRAN_RESOLVED. */
+int32_t esl_tran_meas_device(esl_ctx *ctx, const esl_tran_opts *opts, const esl_measure *meas, uint32_t n_meas,
+                             int early_stop, double *d_x, uint32_t *d_stats, double *d_values, float *ms);
+
 /* Sequential .dc sweeps, one per lane (dc.zig Sweep :163-386; the
  * reference's `.dc` path, which the oracle's orc_dc_sweep restates): every
  * lane (its own parameters from esl_set_lanes) sweeps the DC value of one V

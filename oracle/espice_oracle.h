@@ -176,6 +176,33 @@ enum {
     ORC_TS_N
 };
 
+/* Streamed transient measures (src/output/measure.zig): WHEN (the time of
+ * a clause's event), TRIG/TARG (targ - trig, each clause its own TD) and
+ * FIND .. AT= (the value at a time). A clause: the probed unknown, the level
+ * VAL, RISE/FALL/CROSS counts (ORC_MEAS_UNSET, ORC_MEAS_LAST or k >= 1),
+ * TD, FROM, TO (0: none) and AT. */
+enum { ORC_MEAS_WHEN = 0, ORC_MEAS_TRIG_TARG = 1, ORC_MEAS_FIND_AT = 2 };
+enum { ORC_MEAS_UNSET = -1, ORC_MEAS_LAST = -2 };
+typedef struct {
+    uint32_t unknown;
+    int32_t rise, fall, cross;
+    double val, td, from, to, at;
+} orc_meas_clause;
+typedef struct {
+    uint32_t kind, pad;
+    orc_meas_clause a, b;
+} orc_measure;
+
+/* orc_tran with measures: meas [n_meas] cards fed every recorded row (t = 0
+ * and every accepted step); values [n_lanes][n_meas] (NaN: unresolved);
+ * with early_stop a lane ends its transient once every card has resolved
+ * (status ORC_TRAN_RESOLVED). */
+enum { ORC_TRAN_RESOLVED = 5 };
+int orc_tran_meas(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
+                  const double *values, uint32_t n_lanes, const orc_tran_opts *topts,
+                  const orc_measure *meas, uint32_t n_meas, int early_stop, double *meas_out,
+                  uint32_t *stats, double *x_final);
+
 int orc_tran(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
              const double *values, uint32_t n_lanes, const orc_tran_opts *topts,
              const uint32_t *probe_nodes, uint32_t n_probes, uint32_t max_pts,

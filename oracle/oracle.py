@@ -180,6 +180,44 @@ def dc_sweep_lanes(frozen, slots, lane_values, sweep_slot, values, opts=None):
     return x, it, cv
 
 
+class MeasClause(ctypes.Structure):
+    _fields_ = [("unknown", ctypes.c_uint32), ("rise", ctypes.c_int32), ("fall", ctypes.c_int32),
+                ("cross", ctypes.c_int32), ("val", ctypes.c_double), ("td", ctypes.c_double),
+                ("from_", ctypes.c_double), ("to", ctypes.c_double), ("at", ctypes.c_double)]
+
+
+class Measure(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_uint32), ("pad", ctypes.c_uint32), ("a", MeasClause), ("b", MeasClause)]
+
+
+MEAS_WHEN, MEAS_TRIG_TARG, MEAS_FIND_AT = 0, 1, 2
+MEAS_UNSET, MEAS_LAST = -1, -2
+TRAN_RESOLVED = 5
+
+
+def meas_clause(unknown, val=1e99, rise=MEAS_UNSET, fall=MEAS_UNSET, cross=MEAS_UNSET, td=0.0, from_=0.0,
+                to=0.0, at=1e99):
+    return MeasClause(unknown, rise, fall, cross, val, td, from_, to, at)
+
+
+def tran_meas(frozen, slots, values, opts, measures, early_stop=False):
+    """The transient with streamed measures: (values [lanes][n_meas] (NaN:
+    unresolved), stats [lanes][8], x_final [lanes][n])."""
+    values = np.ascontiguousarray(values, np.float64).reshape(-1, max(1, len(slots)))
+    lanes = values.shape[0]
+    ms = (Measure * max(1, len(measures)))(*measures)
+    out = np.zeros((lanes, max(1, len(measures))))
+    stats = np.zeros((lanes, len(TS_FIELDS)), np.uint32)
+    x = np.zeros((lanes, frozen.n))
+    sa = frozen.slots_array(slots)
+    rc = lib().orc_tran_meas(ctypes.byref(frozen.struct()), sa, ctypes.c_uint32(len(slots)),
+                             _p(values, f64p), ctypes.c_uint32(lanes), ctypes.byref(opts), ms,
+                             ctypes.c_uint32(len(measures)), ctypes.c_int(1 if early_stop else 0),
+                             _p(out, f64p), _p(stats, u32p), _p(x, f64p))
+    assert rc == 0
+    return out[:, :len(measures)], stats, x
+
+
 def op(frozen, opts=None):
     opts = opts or newton_opts(max_iter=100)
     x = np.zeros(frozen.n)

@@ -14,11 +14,13 @@
  *   models/vsource.va:133-136            PULSE corners as periodic timers
  * Left out (no device on this path uses them): uic, VPI callbacks, state
  * flips and reject_at, bound_step, stateful-charge rebase, delay-line
- * echoes, gear orders above 2, tangents and .meas streaming. The operating
- * point is the plain Newton rung from a cold start.
+ * echoes, gear orders above 2 and tangents. Measures (orc_meas.c) are fed
+ * every recorded row, with the early stop of tran.zig:1057-1064. The
+ * operating point is the plain Newton rung from a cold start.
  */
 #include "orc_internal.h"
 #include "orc_ckt.h"
+#include "orc_meas.h"
 
 #include <math.h>
 #include <stdlib.h>
@@ -139,13 +141,21 @@ typedef struct {
     uint32_t n_probes, max_pts, n_pts;
     const uint32_t *probes;
     double *out_t, *out_v;
+    const orc_measure *meas;
+    uint32_t n_meas;
+    int early_stop;
+    orc_meas_state *ms;
 } rec_t;
 
-static void record(rec_t *r, double t, const double *x) {
-    if (!r->out_t || r->n_pts >= r->max_pts) return;
+/* Records the row (t, x) and feeds it to the measures; returns the cards
+ * still open. */
+static int record(rec_t *r, double t, const double *x) {
+    int open = r->n_meas ? meas_feed(r->ms, r->meas, r->n_meas, t, x) : 1;
+    if (!r->out_t || r->n_pts >= r->max_pts) return open;
     r->out_t[r->n_pts] = t;
     for (uint32_t p = 0; p < r->n_probes; p++) r->out_v[(size_t)r->n_pts * r->n_probes + p] = x[r->probes[p]];
     r->n_pts++;
+    return open;
 }
 
 /* One lane: operating point, then the step loop. */
@@ -313,7 +323,11 @@ static void tran_lane(ckt_t *k, const orc_tran_opts *o, rec_t *rec, uint32_t *st
             }
             have_bp = 0;
         }
-        record(rec, t_new, cur);
+        const int open = record(rec, t_new, cur);
+        if (rec->early_stop && rec->n_meas && open == 0) {
+            st[ORC_TS_STATUS] = ORC_TRAN_RESOLVED;
+            break;
+        }
         have_bp = next_bp(tm, nt, t_new + min_break, &bp_next);
         bp_clamped = 0;
         if (have_bp) {
@@ -348,11 +362,31 @@ int orc_tran(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
         for (uint32_t s = 0; s < n_slots; s++) ckt_set(&k, slots[s], values[(size_t)l * n_slots + s]);
         rec_t r = {n_probes, max_pts, 0, probe_nodes,
                    out_t ? out_t + (size_t)l * max_pts : NULL,
-                   out_v ? out_v + (size_t)l * max_pts * n_probes : NULL};
+                   out_v ? out_v + (size_t)l * max_pts * n_probes : NULL, NULL, 0, 0, NULL};
         k.lim_active = 0;
         tran_lane(&k, topts, &r, stats + (size_t)l * ORC_TS_N, x_final + (size_t)l * k.n);
         if (n_pts_out) n_pts_out[l] = r.n_pts;
     }
+    ckt_free(&k);
+    return 0;
+}
+
+int orc_tran_meas(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
+                  const double *values, uint32_t n_lanes, const orc_tran_opts *topts,
+                  const orc_measure *meas, uint32_t n_meas, int early_stop, double *meas_out,
+                  uint32_t *stats, double *x_final) {
+    ckt_t k;
+    if (ckt_init(&k, c) != 0) return -1;
+    orc_meas_state *ms = (orc_meas_state *)calloc(n_meas ? n_meas : 1, sizeof(orc_meas_state));
+    for (uint32_t l = 0; l < n_lanes; l++) {
+        for (uint32_t s = 0; s < n_slots; s++) ckt_set(&k, slots[s], values[(size_t)l * n_slots + s]);
+        meas_init(ms, meas, n_meas);
+        rec_t r = {0, 0, 0, NULL, NULL, NULL, meas, n_meas, early_stop, ms};
+        k.lim_active = 0;
+        tran_lane(&k, topts, &r, stats + (size_t)l * ORC_TS_N, x_final + (size_t)l * k.n);
+        meas_results(ms, meas, n_meas, meas_out + (size_t)l * n_meas);
+    }
+    free(ms);
     ckt_free(&k);
     return 0;
 }
