@@ -47,6 +47,9 @@ FIXTURES = [
     "tran/bench_mosfet_nmos_cs",
     "tran/rc_pulse_history_trap",
     "tran/finite_rise_positive",
+    # transient measures (FIND .. AT=) against ngspice's printed values
+    "tran/zero_abstol_vntol",
+    "tran/zero_vntol_chgtol",
 ]
 
 
@@ -63,7 +66,8 @@ def main(ref):
             "deck": deck,
             "analysis": exp["analysis"],
             "oracle": exp["oracle"]["kind"],
-            "plots": exp["expect"]["plots"],
+            "plots": exp["expect"].get("plots", []),
+            "checks": [c for c in exp["expect"].get("checks", []) if c.get("kind") == "measure"],
         }
         name = f.replace("/", "__") + ".json"
         with open(os.path.join(here, name), "w") as fh:

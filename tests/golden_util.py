@@ -104,3 +104,50 @@ def score_tran(g, t, v, cols):
         allowed = spec["atol"] + spec["rtol"] * np.abs(exp)
         out.append((col, float(np.max(np.abs(got - exp) / allowed))))
     return out
+
+
+def measure_cards(deck, fr, mod):
+    """The deck's .meas cards as `mod`'s Measure structs (mod: the library's
+    lanes module or the oracle)."""
+    kinds = {"when": mod.MEAS_WHEN, "trig_targ": mod.MEAS_TRIG_TARG, "find_at": mod.MEAS_FIND_AT}
+    out = []
+    for m in deck.measures:
+        cl = [mod.meas_clause(fr.unknown(c["vec"]), val=c["val"], rise=c["rise"], fall=c["fall"],
+                              cross=c["cross"], td=c["td"], from_=c["from"], to=c["to"], at=c["at"])
+              for c in m["clauses"]]
+        while len(cl) < 2:
+            cl.append(mod.meas_clause(0))
+        out.append(mod.Measure(kinds[m["kind"]], 0, cl[0], cl[1]))
+    return out
+
+
+def tran_options(deck):
+    """The .tran card's options for tran_opts: (tstop, tstep, tmax, kwargs)."""
+    _, tstep, tstop, tstart, tmax = deck.analysis
+    assert tstart == 0.0, "a TSTART after 0 is not supported"
+    kw = dict(deck.newton_opts())
+    for k in ("chgtol", "trtol"):
+        if k in deck.options:
+            kw[k] = deck.options[k]
+    return tstop, tstep, tmax, kw
+
+
+def solve_meas(g):
+    """The fixture's .meas cards through the oracle's transient: {name: value}."""
+    from oracle import oracle
+    deck = Deck(g["deck"])
+    fr = deck.circuit().freeze()
+    tstop, tstep, tmax, kw = tran_options(deck)
+    o = oracle.tran_opts(tstop, tstep, tmax, max_steps=2_000_000, **kw)
+    v, st, _ = oracle.tran_meas(fr, [], np.zeros((1, 1)), o, measure_cards(deck, fr, oracle))
+    return {m["name"]: float(v[0, k]) for k, m in enumerate(deck.measures)}, st[0]
+
+
+def score_meas(g, values):
+    """(name, err / allowed) for every measure check of the fixture."""
+    out = []
+    for c in g.get("checks", []):
+        got = values[c["name"].lower()]
+        allowed = c["atol"] + c["rtol"] * abs(c["value"])
+        out.append((c["name"], abs(got - c["value"]) / allowed))
+    return out

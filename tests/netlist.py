@@ -39,12 +39,50 @@ def _kv(tokens):
     return out
 
 
+def _meas(card):
+    """A `.meas tran` card of the streamed forms: FIND v AT=t, WHEN v=val
+    [RISE|FALL|CROSS=k|LAST] [TD=t], TRIG v VAL=.. .. TARG v VAL=.. .. as
+    {"name", "kind", clauses [{"vec", "val", "rise", "fall", "cross", "td",
+    "from", "to", "at"}]}."""
+    t = re.sub(r"\s*=\s*", "=", card).split()
+    assert t[1].lower() == "tran", card
+    name, words = t[2].lower(), [w.lower() for w in t[3:]]
+
+    def clause():
+        return {"vec": "", "val": 1e99, "rise": -1, "fall": -1, "cross": -1, "td": 0.0, "from": 0.0,
+                "to": 0.0, "at": 1e99}
+
+    out = {"name": name, "kind": None, "clauses": []}
+    cur = None
+    for w in words:
+        if w in ("find", "trig", "targ"):
+            out["kind"] = out["kind"] or {"find": "find_at", "trig": "trig_targ"}.get(w)
+            cur = clause()
+            out["clauses"].append(cur)
+        elif w == "when":
+            out["kind"] = "when"
+            cur = clause()
+            out["clauses"].append(cur)
+        elif "=" in w:
+            k, v = w.split("=", 1)
+            if k in ("rise", "fall", "cross"):
+                cur[k] = -2 if v == "last" else int(num(v))
+            elif k in ("val", "td", "from", "to", "at"):
+                cur[k] = num(v)
+            elif not cur["vec"]:  # WHEN v(x)=level
+                cur["vec"], cur["val"] = k, num(v)
+        elif not cur["vec"]:
+            cur["vec"] = w
+    return out
+
+
 class Deck:
     def __init__(self, text: str):
         self.models = {}
         self.cards = []
         self.analysis = None
         self.options = {}
+        self.measures = []
         self.temp = 27.0
         lines = []
         for raw in text.splitlines():
@@ -82,6 +120,8 @@ class Deck:
                 tstart = num(t[3]) if len(t) > 3 else 0.0
                 tmax = num(t[4]) if len(t) > 4 else 0.0
                 self.analysis = ("tran", num(t[1]), num(t[2]), tstart, tmax)
+            elif low.startswith(".meas"):
+                self.measures.append(_meas(s))
             elif low.startswith(".temp"):
                 self.temp = num(s.split()[1])
             elif low.startswith(".end"):

@@ -8,7 +8,9 @@ arithmetic differing from the CPU's in the last bits)."""
 import numpy as np
 import pytest
 
+import golden_util as gu
 from espice_b200 import decks, lanes
+from netlist import Deck
 from oracle import oracle
 
 pytestmark = pytest.mark.gpu
@@ -78,3 +80,29 @@ def test_early_stop_ends_lanes():
     resolved = sg[:, 0] == lanes.TRAN_RESOLVED
     assert resolved.any()
     assert (np.isfinite(vg[resolved, 0])).all()
+
+
+MEAS_FIXTURES = [n for n in gu.names("tran__") if gu.load(n).get("checks")]
+
+
+@pytest.mark.parametrize("name", MEAS_FIXTURES)
+def test_golden_measures_as_gpu_lanes(name):
+    """A transient fixture's .meas cards on the device: the oracle's values
+    and ngspice's printed ones at the fixture's tolerance."""
+    g = gu.load(name)
+    deck = Deck(g["deck"])
+    fr = deck.circuit().freeze()
+    tstop, tstep, tmax, kw = gu.tran_options(deck)
+    ctx = lanes.DcLanes(fr)
+    ctx.set_lanes([], np.zeros((2, 1)))
+    vg, sg, _, _ = ctx.tran_meas(lanes.tran_opts(tstop, tstep, tmax, max_steps=2_000_000, **kw),
+                                 gu.measure_cards(deck, fr, lanes))
+    ctx.close()
+    values_o, so = gu.solve_meas(g)
+    vo = np.array([values_o[m["name"]] for m in deck.measures])
+    assert (sg[:, 0] == lanes.TRAN_DONE).all()
+    assert np.array_equal(sg[0], so)
+    assert _same(vg[0], vo).all() and _same(vg[1], vo).all()
+    values = {m["name"]: float(vg[0, k]) for k, m in enumerate(deck.measures)}
+    for nm, worst in gu.score_meas(g, values):
+        assert worst <= 1.0, f"{name} {nm}: {worst:.3g}x the fixture tolerance"

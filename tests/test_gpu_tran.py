@@ -96,7 +96,7 @@ def test_ring_oscillator_short_window():
     assert (res_g[3][:, 0] == lanes.TRAN_DONE).all()
 
 
-TRAN_FIXTURES = gu.names("tran__")
+TRAN_FIXTURES = [n for n in gu.names("tran__") if gu.load(n)["plots"]]
 
 
 @pytest.mark.parametrize("name", TRAN_FIXTURES)

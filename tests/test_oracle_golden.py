@@ -27,7 +27,8 @@ def test_oracle_matches_golden(name):
         assert worst <= 1.0, f"{name} {col}: error {worst:.3g}x the allowed tolerance"
 
 
-TRAN = gu.names("tran__")
+TRAN = [n for n in gu.names("tran__") if gu.load(n)["plots"]]
+MEAS = [n for n in gu.names("tran__") if gu.load(n).get("checks")]
 
 
 @pytest.mark.parametrize("name", TRAN)
@@ -40,3 +41,14 @@ def test_oracle_transient_matches_golden(name):
     assert st["status"] == 0, st
     for col, worst in gu.score_tran(g, t, v, cols):
         assert worst <= 1.0, f"{name} {col}: error {worst:.3g}x the allowed tolerance"
+
+
+@pytest.mark.parametrize("name", MEAS)
+def test_oracle_measures_match_golden(name):
+    """The streamed .meas cards of a transient fixture against the values
+    ngspice printed, at the fixture's tolerance."""
+    g = gu.load(name)
+    values, st = gu.solve_meas(g)
+    assert st[0] == 0, st
+    for nm, worst in gu.score_meas(g, values):
+        assert worst <= 1.0, f"{name} {nm}: error {worst:.3g}x the allowed tolerance"
