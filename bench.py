@@ -352,6 +352,35 @@ def dc_sweep_lanes(args, local, flush):
             "lanes_left_tape": left, "newton_iters_per_point": float(it.mean())}
 
 
+def ring_period_early_stop(args, local, flush):
+    """The ring oscillator's period as a streamed measure (TRIG v(s0) VAL=0.9
+    RISE=2, TARG v(s0) VAL=0.9 RISE=3) on the headline's 1024 lanes and
+    20 ns window, each lane ending its transient once the card resolves
+    (tran.zig's early stop). Lanes/s counts lanes that resolved."""
+    from espice_b200 import decks, lanes
+    fr, slots, values = decks.ring_oscillator(lanes=1024)
+    s0 = fr.unknown("v(s0)")
+    card = [lanes.trig_targ(lanes.meas_clause(s0, val=0.9, rise=2), lanes.meas_clause(s0, val=0.9, rise=3))]
+    t_stop = args.t_stop or decks.RING_T_STOP
+    o = lanes.tran_opts(t_stop, decks.RING_T_STEP, decks.RING_T_MAX, max_steps=10_000_000)
+    ctx = lanes.DcLanes(fr, device=local)
+    ctx.set_lanes(slots, values)
+    ms, resolved, steps = [], 0, 0
+    for i in range(min(args.warmup, 1) + max(1, args.steps // 5)):
+        flush.zero_()
+        v, st, _, t = ctx.tran_meas(o, card, early_stop=True)
+        if i >= min(args.warmup, 1):
+            ms.append(t)
+            resolved += int((st[:, 0] == lanes.TRAN_RESOLVED).sum())
+            steps += int(st[:, 1].sum())
+    ctx.close()
+    n = len(ms)
+    return {"workload": "ring_oscillator period measure with early stop: 1024 lanes, t_stop %g s" % t_stop,
+            "value": resolved / (sum(ms) / 1e3), "unit": "measured lanes/s", "ms_per_step": float(np.mean(ms)),
+            "resolved_fraction": resolved / (n * 1024), "accepted_steps_per_lane": steps / (n * 1024),
+            "period_s_median": float(np.nanmedian(v[:, 0]))}
+
+
 def learned_dc(args, local, flush):
     """The learned warm start against the plain FP64 lanes on the 16-parameter
     grid-with-diodes deck: 65536 seeded points, the network trained on the
@@ -523,6 +552,7 @@ def our_arm(args, rank, world):
     }
     out["dc_grid_diodes"] = dc_grid_diodes(args, local, flush)
     out["dc_sweep_lanes"] = dc_sweep_lanes(args, local, flush)
+    out["ring_period_early_stop"] = ring_period_early_stop(args, local, flush)
     if args.learned:
         out["learned_warm_start"] = learned_dc(args, local, flush)
     out["lu_roofline"] = lu_lanes_roofline(fr, ctx, hbm_peak, peak_src)
