@@ -200,7 +200,7 @@ struct esl_ctx {
 
   DevBuf d_nodes[kMaxBatches], d_rhs_ptr, d_rhs_src, d_a_ptr, d_a_src, d_slot_row, d_cur;
   DevBuf d_q_ptr, d_q_src, d_c_ptr, d_c_src, d_probes, d_tran_t, d_tran_v, d_tran_n, d_tran_stats;
-  DevBuf d_amap, d_fill, d_prog, d_l_scaled, d_pinv, d_q, d_seq, d_sweep_values, d_meas;
+  DevBuf d_amap, d_fill, d_prog, d_l_scaled, d_pinv, d_q, d_seq, d_sweep_values, d_meas, d_next_lane;
   uint32_t n_seq_a = 0, n_seq = 0, seq_warps = 0;  // lane-interleaved op list
   uint32_t n_seq_f = 0, mixed_warps = 0;            // its forward-only tail, the mixed kernel's warps
   DevBuf d_row_ptr, d_row_slot, d_row_col;
@@ -1148,6 +1148,8 @@ int32_t esl_tran_device(esl_ctx* ctx, const esl_tran_opts* opts, double* d_x, ui
   LaneDev L = lane_view(ctx, 0);
   L.x = d_x;
   cudaStream_t s = ctx->stream;
+  ESL_CUDA(ctx->d_next_lane.ensure(sizeof(uint32_t)));
+  P.next_lane = ctx->d_next_lane.as<uint32_t>();
   ESL_CUDA(cudaEventRecord(ctx->ev0, s));
   ESL_CUDA(launch_tran(ctx->topo, L, P, lo, lanes_per_cta(ctx, ctx->n_lanes, ctx->tran_lanes_eff), s));
   ESL_CUDA(cudaEventRecord(ctx->ev1, s));
@@ -1197,6 +1199,8 @@ int32_t esl_dc_sweep_device(esl_ctx* ctx, const esl_slot* slot, const double* va
   P.status = d_status;
   const LaneOpts o{opts->reltol, opts->abstol, opts->vntol, opts->residual_tol, opts->gmin, opts->max_iter, 0, 0};
   LaneDev L = lane_view(ctx, 0);
+  ESL_CUDA(ctx->d_next_lane.ensure(sizeof(uint32_t)));
+  P.next_lane = ctx->d_next_lane.as<uint32_t>();
   ESL_CUDA(cudaEventRecord(ctx->ev0, s));
   ESL_CUDA(launch_sweep(T, L, P, o, lanes_per_cta(ctx, ctx->n_lanes, fit), s));
   ESL_CUDA(cudaEventRecord(ctx->ev1, s));
@@ -1238,6 +1242,8 @@ int32_t esl_tran_meas_device(esl_ctx* ctx, const esl_tran_opts* opts, const esl_
   P.meas_out = d_values;
   LaneDev L = lane_view(ctx, 0);
   L.x = d_x;
+  ESL_CUDA(ctx->d_next_lane.ensure(sizeof(uint32_t)));
+  P.next_lane = ctx->d_next_lane.as<uint32_t>();
   ESL_CUDA(cudaEventRecord(ctx->ev0, s));
   ESL_CUDA(launch_tran(T, L, P, lo, lanes_per_cta(ctx, ctx->n_lanes, fit), s));
   ESL_CUDA(cudaEventRecord(ctx->ev1, s));

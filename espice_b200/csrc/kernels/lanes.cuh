@@ -126,6 +126,7 @@ struct TranDev {
   const MeasDev* meas;     // [n_meas] cards fed every recorded row (null: none)
   uint32_t n_meas, early_stop;
   double* meas_out;        // [lane][n_meas] card values (NaN: unresolved)
+  uint32_t* next_lane;     // the lane-refill counter, zero at launch
 };
 
 // Sequential .dc sweeps, one per lane (dc.zig Sweep): the swept source
@@ -140,6 +141,7 @@ struct SweepDev {
   uint32_t* iters;   // [lane][n_pts]
   uint8_t* conv;     // [lane][n_pts]
   uint32_t* status;  // [lane]
+  uint32_t* next_lane;  // the lane-refill counter, zero at launch
 };
 
 // Shared-memory doubles per lane of sweep_kernel: the lane working set,

@@ -1933,7 +1933,14 @@ __global__ void __launch_bounds__(256) tran_kernel(TopoDev T, LaneDev L, TranDev
   const int tid = threadIdx.x & 31;
   const uint32_t warps = blockDim.x >> 5, w = threadIdx.x >> 5;
   double* block = lanes_smem + size_t(w) * (T.tran_doubles + kMeasDoubles * P.n_meas);
-  for (uint32_t lane = blockIdx.x * warps + w; lane < L.n_lanes; lane += gridDim.x * warps) {
+  // Lane refill: a warp that finishes takes the next lane from a counter,
+  // so lanes of unequal length (early stops, rejections) balance over the
+  // GPU instead of following a fixed stride.
+  for (;;) {
+    uint32_t lane = 0;
+    if (tid == 0) lane = atomicAdd(P.next_lane, 1u);
+    lane = __shfl_sync(kFull, lane, 0);
+    if (lane >= L.n_lanes) break;
     tran_lane(T, L, P, o, prog, block, lane, tid);
     __syncwarp();
   }
@@ -1946,7 +1953,11 @@ __global__ void __launch_bounds__(256) sweep_kernel(TopoDev T, LaneDev L, SweepD
   const int tid = threadIdx.x & 31;
   const uint32_t warps = blockDim.x >> 5, w = threadIdx.x >> 5;
   double* block = lanes_smem + size_t(w) * sweep_doubles(T);
-  for (uint32_t lane = blockIdx.x * warps + w; lane < L.n_lanes; lane += gridDim.x * warps) {
+  for (;;) {  // lane refill, as tran_kernel
+    uint32_t lane = 0;
+    if (tid == 0) lane = atomicAdd(P.next_lane, 1u);
+    lane = __shfl_sync(kFull, lane, 0);
+    if (lane >= L.n_lanes) break;
     sweep_lane(T, L, P, o, prog, block, lane, tid);
     __syncwarp();
   }
@@ -1956,6 +1967,8 @@ cudaError_t launch_sweep(const TopoDev& T, const LaneDev& L, const SweepDev& P, 
                          uint32_t lanes_per_block, cudaStream_t s) {
   const size_t smem = T.prog_bytes + lanes_per_block * size_t(sweep_doubles(T)) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(P.next_lane, 0, sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
   sweep_kernel<<<persistent_grid(sweep_kernel, L.n_lanes, lanes_per_block, smem), 32 * lanes_per_block, smem, s>>>(
       T, L, P, o);
@@ -1967,6 +1980,8 @@ cudaError_t launch_tran(const TopoDev& T, const LaneDev& L, const TranDev& P, co
   const size_t smem =
       T.prog_bytes + lanes_per_block * size_t(T.tran_doubles + kMeasDoubles * P.n_meas) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(tran_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(P.next_lane, 0, sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
   tran_kernel<<<persistent_grid(tran_kernel, L.n_lanes, lanes_per_block, smem), 32 * lanes_per_block, smem, s>>>(
       T, L, P, o);
