@@ -78,7 +78,9 @@ enum SweepStatus : uint32_t {
   kSweepLeftTape = 4,  // a factor left the lead pivot tape: the rest of the sweep is the CPU's
 };
 // Streamed measure cards and clause counts (esl_measure).
-enum MeasKind : uint32_t { kMeasWhen = 0, kMeasTrigTarg = 1, kMeasFindAt = 2 };
+enum MeasKind : uint32_t {
+  kMeasWhen = 0, kMeasTrigTarg = 1, kMeasFindAt = 2, kMeasMin = 3, kMeasMax = 4, kMeasAvg = 5, kMeasPp = 6
+};
 constexpr int32_t kMeasUnset = -1;
 constexpr int32_t kMeasLast = -2;
 constexpr uint32_t kMaxMeas = 32;  // one warp thread per card

@@ -1219,7 +1219,7 @@ int32_t esl_tran_meas_device(esl_ctx* ctx, const esl_tran_opts* opts, const esl_
   if (n_meas > kMaxMeas) return ctx->fail(ESL_INVALID_ARGUMENT, "at most 32 measure cards");
   for (uint32_t c = 0; c < n_meas; ++c) {
     const esl_measure& m = meas[c];
-    if (m.kind > ESL_MEAS_FIND_AT) return ctx->fail(ESL_INVALID_ARGUMENT, "unknown measure kind");
+    if (m.kind > ESL_MEAS_PP) return ctx->fail(ESL_INVALID_ARGUMENT, "unknown measure kind");
     if (m.a.unknown >= ctx->pat.n || (m.kind == ESL_MEAS_TRIG_TARG && m.b.unknown >= ctx->pat.n))
       return ctx->fail(ESL_INVALID_ARGUMENT, "measure probe out of range");
   }

@@ -1417,7 +1417,42 @@ __device__ void meas_start(const MeasDev& mc, CrossDev* x) {
     s.rise = s.fall = s.cross = 0;
     s.first = 0;
     s.above = s.pending = s.found = s.over = 0;
+    if (mc.kind >= kMeasMin) {
+      s.hit = 0.0;  // Extremum's m
+      s.td = 0.0;   // its span
+    }
   }
+}
+
+// Extremum.feed (measure.zig:1401-1449, not DC): op 0 MIN, 1 MAX (the last
+// sample reaching the extreme), 2 AVG (trapezoids over the samples' span;
+// hit the sum, td the span); inside FROM..TO, no interpolated ends; true
+// once past TO.
+__device__ bool ext_feed(CrossDev& s, const MeasClauseDev& c, int op, double xv, double v) {
+  if (s.over) return true;
+  if (xv < c.from) return false;
+  if (c.to != 0.0 && xv > c.to) {
+    s.over = 1;
+    return true;
+  }
+  if (!s.first) {
+    s.first = 1;
+    s.hit = op == 2 ? 0.0 : v;
+    s.prev = v;
+    s.prev_x = xv;
+    return false;
+  }
+  if (op == 0) {
+    if (v <= s.hit) s.hit = v;
+  } else if (op == 1) {
+    if (v >= s.hit) s.hit = v;
+  } else {
+    s.hit = s.hit + 0.5 * (v + s.prev) * (xv - s.prev_x);
+    s.td = s.td + (xv - s.prev_x);
+    s.prev = v;
+    s.prev_x = xv;
+  }
+  return false;
 }
 
 // Cross.feed for one event; true once the scan is over (its event found,
@@ -1495,6 +1530,13 @@ __device__ bool at_feed(CrossDev& s, const MeasClauseDev& c, double xv, double v
 // Feeds the row (t, x) to card c; true once the card has resolved.
 __device__ bool meas_feed(const MeasDev& mc, CrossDev* x, double t, const double* xs) {
   if (mc.kind == kMeasFindAt) return at_feed(x[0], mc.a, t, xs[mc.a.unknown]);
+  if (mc.kind == kMeasMin || mc.kind == kMeasMax || mc.kind == kMeasAvg)
+    return ext_feed(x[0], mc.a, int(mc.kind - kMeasMin), t, xs[mc.a.unknown]);
+  if (mc.kind == kMeasPp) {
+    const bool d0 = ext_feed(x[0], mc.a, 0, t, xs[mc.a.unknown]);
+    const bool d1 = ext_feed(x[1], mc.a, 1, t, xs[mc.a.unknown]);
+    return d0 && d1;
+  }
   if (mc.kind == kMeasWhen) return cross_feed(x[0], mc.a, t, xs[mc.a.unknown]);
   const bool da = cross_feed(x[0], mc.a, t, xs[mc.a.unknown]);
   const bool db = cross_feed(x[1], mc.b, t, xs[mc.b.unknown]);
@@ -1502,11 +1544,18 @@ __device__ bool meas_feed(const MeasDev& mc, CrossDev* x, double t, const double
 }
 
 // A card's value at the end: WHEN the event time (else a LAST count's last
-// event, else NaN), TRIG/TARG targ - trig, FIND the interpolated value.
+// event, else NaN), TRIG/TARG targ - trig, FIND the interpolated value,
+// MIN/MAX the extreme, AVG the trapezoidal mean, PP max - min.
 __device__ double meas_value(const MeasDev& mc, const CrossDev* x) {
   double v;
   if (mc.kind == kMeasFindAt) {
     v = x[0].found ? x[0].hit : CUDART_NAN;
+  } else if (mc.kind == kMeasMin || mc.kind == kMeasMax) {
+    v = x[0].hit;  // 0 when no sample fell in the window
+  } else if (mc.kind == kMeasAvg) {
+    v = div_rn(x[0].hit, x[0].first ? x[0].td : 1.0);
+  } else if (mc.kind == kMeasPp) {
+    v = x[1].hit - x[0].hit;
   } else if (mc.kind == kMeasWhen) {
     v = x[0].found ? x[0].hit : x[0].last;
   } else {

@@ -93,7 +93,7 @@ class Measure(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_uint32), ("pad", ctypes.c_uint32), ("a", MeasClause), ("b", MeasClause)]
 
 
-MEAS_WHEN, MEAS_TRIG_TARG, MEAS_FIND_AT = 0, 1, 2
+MEAS_WHEN, MEAS_TRIG_TARG, MEAS_FIND_AT, MEAS_MIN, MEAS_MAX, MEAS_AVG, MEAS_PP = 0, 1, 2, 3, 4, 5, 6
 MEAS_UNSET, MEAS_LAST = -1, -2
 
 
@@ -112,6 +112,11 @@ def trig_targ(trig, targ):
 
 def find_at(unknown, at):
     return Measure(MEAS_FIND_AT, 0, meas_clause(unknown, at=at), meas_clause(0))
+
+
+def window(kind, unknown, from_=0.0, to=0.0):
+    """MIN, MAX, AVG or PP (MEAS_*) of `unknown` over FROM..TO (TO 0: to the end)."""
+    return Measure(kind, 0, meas_clause(unknown, from_=from_, to=to), meas_clause(0))
 
 
 class TapeInfo(ctypes.Structure):

@@ -217,11 +217,15 @@ int32_t esl_tran_device(esl_ctx *ctx, const esl_tran_opts *opts, double *d_x, ui
  * of ngspice com_measure2.c): every recorded row (t = 0 and each accepted
  * step) feeds each card. WHEN: the time of a clause's event; TRIG/TARG:
  * targ - trig (each clause with its own TD); FIND .. AT=: the value at a
- * time. A clause: the probed unknown, the level VAL, RISE/FALL/CROSS counts
+ * time; MIN, MAX, AVG (trapezoidal mean) and PP of clause a's unknown over
+ * its FROM..TO window (the samples inside it, ends not interpolated; MIN
+ * and MAX read 0 when no sample falls inside, as the reference's do). A
+ * clause: the probed unknown, the level VAL, RISE/FALL/CROSS counts
  * (ESL_MEAS_UNSET, ESL_MEAS_LAST or k >= 1), TD, FROM, TO (0: none), AT. An
  * event is counted from the clause's second sample and its time is the
  * level crossing interpolated on the last segment, as ngspice does. */
-enum { ESL_MEAS_WHEN = 0, ESL_MEAS_TRIG_TARG = 1, ESL_MEAS_FIND_AT = 2 };
+enum { ESL_MEAS_WHEN = 0, ESL_MEAS_TRIG_TARG = 1, ESL_MEAS_FIND_AT = 2,
+       ESL_MEAS_MIN = 3, ESL_MEAS_MAX = 4, ESL_MEAS_AVG = 5, ESL_MEAS_PP = 6 };
 enum { ESL_MEAS_UNSET = -1, ESL_MEAS_LAST = -2 };
 typedef struct {
     uint32_t unknown;

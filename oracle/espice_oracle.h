@@ -178,10 +178,12 @@ enum {
 
 /* Streamed transient measures (src/output/measure.zig): WHEN (the time of
  * a clause's event), TRIG/TARG (targ - trig, each clause its own TD) and
- * FIND .. AT= (the value at a time). A clause: the probed unknown, the level
+ * FIND .. AT= (the value at a time), and MIN, MAX, AVG (trapezoidal mean)
+ * and PP over the FROM..TO window of clause a. A clause: the probed unknown, the level
  * VAL, RISE/FALL/CROSS counts (ORC_MEAS_UNSET, ORC_MEAS_LAST or k >= 1),
  * TD, FROM, TO (0: none) and AT. */
-enum { ORC_MEAS_WHEN = 0, ORC_MEAS_TRIG_TARG = 1, ORC_MEAS_FIND_AT = 2 };
+enum { ORC_MEAS_WHEN = 0, ORC_MEAS_TRIG_TARG = 1, ORC_MEAS_FIND_AT = 2,
+       ORC_MEAS_MIN = 3, ORC_MEAS_MAX = 4, ORC_MEAS_AVG = 5, ORC_MEAS_PP = 6 };
 enum { ORC_MEAS_UNSET = -1, ORC_MEAS_LAST = -2 };
 typedef struct {
     uint32_t unknown;

@@ -190,7 +190,7 @@ class Measure(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_uint32), ("pad", ctypes.c_uint32), ("a", MeasClause), ("b", MeasClause)]
 
 
-MEAS_WHEN, MEAS_TRIG_TARG, MEAS_FIND_AT = 0, 1, 2
+MEAS_WHEN, MEAS_TRIG_TARG, MEAS_FIND_AT, MEAS_MIN, MEAS_MAX, MEAS_AVG, MEAS_PP = 0, 1, 2, 3, 4, 5, 6
 MEAS_UNSET, MEAS_LAST = -1, -2
 TRAN_RESOLVED = 5
 

@@ -7,11 +7,16 @@
  *                          second sample, the level crossing interpolated
  *                          on the last segment, LAST counts, TD, FROM/TO
  *   measure.zig:1379-1398  At: FIND .. AT=, the first segment holding AT
- *   measure.zig:575-605    TRIG/TARG (targ - trig), WHEN, FIND AT
+ *   measure.zig:1401-1449  Extremum: MIN/MAX (the last sample reaching
+ *                          the extreme), AVG (trapezoids over the samples'
+ *                          span), inside FROM..TO, without interpolated ends
+ *   measure.zig:575-650    TRIG/TARG (targ - trig), WHEN, FIND AT, MIN,
+ *                          MAX, AVG, PP (max - min)
  *   tran.zig:1057-1064     feeding accepted rows and the early stop once
  *                          every card has resolved
- * Only WHEN, TRIG/TARG (each clause its own TD) and FIND AT are restated,
- * with VAL levels (no vector levels), as the device streams them.
+ * Only WHEN, TRIG/TARG (each clause its own TD), FIND AT, MIN, MAX, AVG and
+ * PP are restated, with VAL levels (no vector levels), as the device
+ * streams them.
  */
 #include "orc_meas.h"
 
@@ -30,6 +35,10 @@ void meas_init(orc_meas_state *s, const orc_measure *m, uint32_t n_meas) {
             x->want_cross = cl->cross;
             x->last = NAN;
             x->hit = NAN;
+            if (m[c].kind >= ORC_MEAS_MIN) {
+                x->hit = 0.0;  /* Extremum's m */
+                x->td = 0.0;   /* its span */
+            }
         }
     }
 }
@@ -107,6 +116,35 @@ static int at_feed(orc_cross *s, const orc_meas_clause *c, double xv, double v) 
     return 0;
 }
 
+/* measure.zig Extremum.feed (not DC): op 0 min, 1 max, 2 avg; hit holds
+ * m, prev/prev_x the last sample, td the span; 1 once past TO. */
+static int ext_feed(orc_cross *s, const orc_meas_clause *c, int op, double xv, double v) {
+    if (s->over) return 1;
+    if (xv < c->from) return 0;
+    if (c->to != 0 && xv > c->to) {
+        s->over = 1;
+        return 1;
+    }
+    if (!s->first) {
+        s->first = 1;
+        s->hit = op == 2 ? 0.0 : v;
+        s->prev = v;
+        s->prev_x = xv;
+        return 0;
+    }
+    if (op == 0) {
+        if (v <= s->hit) s->hit = v;
+    } else if (op == 1) {
+        if (v >= s->hit) s->hit = v;
+    } else {
+        s->hit += 0.5 * (v + s->prev) * (xv - s->prev_x);
+        s->td += xv - s->prev_x;
+        s->prev = v;
+        s->prev_x = xv;
+    }
+    return 0;
+}
+
 int meas_feed(orc_meas_state *s, const orc_measure *m, uint32_t n_meas, double t, const double *x) {
     int open = 0;
     for (uint32_t c = 0; c < n_meas; c++) {
@@ -114,6 +152,12 @@ int meas_feed(orc_meas_state *s, const orc_measure *m, uint32_t n_meas, double t
         int done;
         if (mc->kind == ORC_MEAS_FIND_AT) {
             done = at_feed(&s[c].x[0], &mc->a, t, x[mc->a.unknown]);
+        } else if (mc->kind == ORC_MEAS_MIN || mc->kind == ORC_MEAS_MAX || mc->kind == ORC_MEAS_AVG) {
+            done = ext_feed(&s[c].x[0], &mc->a, (int)(mc->kind - ORC_MEAS_MIN), t, x[mc->a.unknown]);
+        } else if (mc->kind == ORC_MEAS_PP) {
+            const int d0 = ext_feed(&s[c].x[0], &mc->a, 0, t, x[mc->a.unknown]);
+            const int d1 = ext_feed(&s[c].x[1], &mc->a, 1, t, x[mc->a.unknown]);
+            done = d0 && d1;
         } else if (mc->kind == ORC_MEAS_WHEN) {
             done = cross_feed(&s[c].x[0], &mc->a, t, x[mc->a.unknown]);
         } else {
@@ -139,6 +183,12 @@ void meas_results(const orc_meas_state *s, const orc_measure *m, uint32_t n_meas
         double v;
         if (mc->kind == ORC_MEAS_FIND_AT) {
             v = s[c].x[0].found ? s[c].x[0].hit : NAN;
+        } else if (mc->kind == ORC_MEAS_MIN || mc->kind == ORC_MEAS_MAX) {
+            v = s[c].x[0].hit;  /* 0 when no sample fell in the window */
+        } else if (mc->kind == ORC_MEAS_AVG) {
+            v = s[c].x[0].hit / (s[c].x[0].first ? s[c].x[0].td : 1.0);
+        } else if (mc->kind == ORC_MEAS_PP) {
+            v = s[c].x[1].hit - s[c].x[0].hit;
         } else if (mc->kind == ORC_MEAS_WHEN) {
             v = cross_result(&s[c].x[0]);
         } else {

@@ -36,13 +36,18 @@ def _cards(fr, mod):
         mod.Measure(mod.MEAS_FIND_AT, 0, mod.meas_clause(s5, at=0.37e-9), mod.meas_clause(0)),
         mod.Measure(mod.MEAS_WHEN, 0, mod.meas_clause(s0, val=0.9, rise=1, from_=0.5e-9, to=1.5e-9),
                     mod.meas_clause(0)),
+        mod.Measure(mod.MEAS_MAX, 0, mod.meas_clause(s0, from_=1e-9, to=2e-9), mod.meas_clause(0)),
+        mod.Measure(mod.MEAS_MIN, 0, mod.meas_clause(s5, from_=0.5e-9, to=2.5e-9), mod.meas_clause(0)),
+        mod.Measure(mod.MEAS_AVG, 0, mod.meas_clause(s0, from_=1e-9), mod.meas_clause(0)),
+        mod.Measure(mod.MEAS_PP, 0, mod.meas_clause(s5, from_=1e-9), mod.meas_clause(0)),
     ]
 
 
 @pytest.mark.parametrize("early", [False, True])
 def test_ring_measures_match_oracle(early):
     """24 ring-oscillator samples over 3 ns: a period, a stage delay, a
-    delayed fall, a LAST crossing, a FIND and a windowed rise."""
+    delayed fall, a LAST crossing, a FIND, a windowed rise, and MAX, MIN,
+    AVG and PP over windows."""
     fr, slots, values = decks.ring_oscillator(lanes=24)
     go = lanes.tran_opts(3e-9, decks.RING_T_STEP, decks.RING_T_MAX, max_steps=200_000)
     oo = oracle.tran_opts(3e-9, decks.RING_T_STEP, decks.RING_T_MAX, max_steps=200_000)
