@@ -9,7 +9,7 @@ behind RD/RS) or a voltage source's branch current. External nodes are
 numbered in order of first use, then internal unknowns in batch order.
 
 Device tables mirror the Verilog-A parameter lists the reference compiles
-(``models/{resistor,capacitor,vsource,isource,diode,mos1}.va``). Values are
+(``models/{resistor,capacitor,vsource,isource,diode,mos1,bsim3}.va``). Values are
 the card values; bias-independent temperature maps run in the library.
 """
 
@@ -20,8 +20,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-R, C, V, I, D, M = 0, 1, 2, 3, 4, 5
-NODES_PER = {R: 2, C: 2, V: 3, I: 2, D: 3, M: 6}
+R, C, V, I, D, M, B3 = 0, 1, 2, 3, 4, 5, 6
+NODES_PER = {R: 2, C: 2, V: 3, I: 2, D: 3, M: 6, B3: 6}
 
 # Diode parameter slots (models/diode.va:35-103).
 D_PARAMS = ["is", "n", "rs", "bv", "ibv", "cjo", "vj", "m", "fc", "tt", "area",
@@ -42,11 +42,52 @@ M_DEFAULTS = {"type": 1.0, "vto": 0.0, "kp": 2e-5, "gamma": 0.0, "phi": 0.6, "la
               "l": 1e-4, "ad": 0.0, "as": 0.0, "pd": 0.0, "ps": 0.0, "delvto": 0.0,
               "m": 1.0, "gmin": 1e-12, "tnom": 27.0, "temp": 300.15}
 
+# BSIM3v3 DC-core parameter slots (models/bsim3.va:26-138: the model card,
+# then the instance, then gmin and the device temperature in K). NaN marks a
+# parameter left off the card whose default the model derives
+# ($param_given): TOXM, NCH, GAMMA1, GAMMA2, VBX, K1, K2, VTH0, VFB, DSUB,
+# UC, UC1, U0.
+B3_PARAMS = ["type", "mobmod", "tnom", "tox", "toxm", "xj", "nch", "nsub", "ngate", "gamma1",
+             "gamma2", "xt", "vbx", "vbm", "k1", "k2", "k3", "k3b", "w0", "nlx", "vth0", "vfb",
+             "dvt0", "dvt1", "dvt2", "dvt0w", "dvt1w", "dvt2w", "drout", "dsub", "nfactor",
+             "cdsc", "cdscb", "cdscd", "cit", "vsat", "at", "a0", "ags", "a1", "a2", "keta",
+             "ua", "ua1", "ub", "ub1", "uc", "uc1", "u0", "ute", "voff", "delta", "rdsw",
+             "prwg", "prwb", "prt", "wr", "eta0", "etab", "pclm", "pdiblc1", "pdiblc2",
+             "pdiblcb", "pscbe1", "pscbe2", "pvag", "dwg", "dwb", "b0", "b1", "alpha0",
+             "alpha1", "beta0", "kt1", "kt1l", "kt2", "lint", "ll", "lln", "lw", "lwn", "lwl",
+             "wint", "wl", "wln", "ww", "wwn", "wwl", "xl", "xw", "js", "jsw", "nj", "xti",
+             "ijth", "rsh", "l", "w", "ad", "as", "pd", "ps", "nrd", "nrs", "m", "delvto",
+             "mulu0", "gmin", "temp"]
+_NAN = float("nan")
+B3_DEFAULTS = {
+    "type": 1.0, "mobmod": 1.0, "tnom": 27.0, "tox": 150.0e-10, "toxm": _NAN, "xj": 0.15e-6,
+    "nch": _NAN, "nsub": 6.0e16, "ngate": 0.0, "gamma1": _NAN, "gamma2": _NAN, "xt": 1.55e-7,
+    "vbx": _NAN, "vbm": -3.0, "k1": _NAN, "k2": _NAN, "k3": 80.0, "k3b": 0.0, "w0": 2.5e-6,
+    "nlx": 1.74e-7, "vth0": _NAN, "vfb": _NAN, "dvt0": 2.2, "dvt1": 0.53, "dvt2": -0.032,
+    "dvt0w": 0.0, "dvt1w": 5.3e6, "dvt2w": -0.032, "drout": 0.56, "dsub": _NAN,
+    "nfactor": 1.0, "cdsc": 2.4e-4, "cdscb": 0.0, "cdscd": 0.0, "cit": 0.0, "vsat": 8.0e4,
+    "at": 3.3e4, "a0": 1.0, "ags": 0.0, "a1": 0.0, "a2": 1.0, "keta": -0.047, "ua": 2.25e-9,
+    "ua1": 4.31e-9, "ub": 5.87e-19, "ub1": -7.61e-18, "uc": _NAN, "uc1": _NAN, "u0": _NAN,
+    "ute": -1.5, "voff": -0.08, "delta": 0.01, "rdsw": 0.0, "prwg": 0.0, "prwb": 0.0,
+    "prt": 0.0, "wr": 1.0, "eta0": 0.08, "etab": -0.07, "pclm": 1.3, "pdiblc1": 0.39,
+    "pdiblc2": 0.0086, "pdiblcb": 0.0, "pscbe1": 4.24e8, "pscbe2": 1.0e-5, "pvag": 0.0,
+    "dwg": 0.0, "dwb": 0.0, "b0": 0.0, "b1": 0.0, "alpha0": 0.0, "alpha1": 0.0, "beta0": 30.0,
+    "kt1": -0.11, "kt1l": 0.0, "kt2": 0.022, "lint": 0.0, "ll": 0.0, "lln": 1.0, "lw": 0.0,
+    "lwn": 1.0, "lwl": 0.0, "wint": 0.0, "wl": 0.0, "wln": 1.0, "ww": 0.0, "wwn": 1.0,
+    "wwl": 0.0, "xl": 0.0, "xw": 0.0, "js": 1.0e-4, "jsw": 0.0, "nj": 1.0, "xti": 3.0,
+    "ijth": 0.1, "rsh": 0.0, "l": 5.0e-6, "w": 5.0e-6, "ad": 0.0, "as": 0.0, "pd": 0.0,
+    "ps": 0.0, "nrd": 1.0, "nrs": 1.0, "m": 1.0, "delvto": 0.0, "mulu0": 1.0, "gmin": 1e-12,
+    "temp": 300.15}
+# ngspice card spellings that name the same parameter
+B3_ALIASES = {"npeak": "nch", "uo": "u0"}
+
 V_PARAMS = ["dc", "wave", "v1", "v2", "td", "tr", "tf", "pw", "per", "phase"]
-PARAMS_PER = {R: 1, C: 1, V: len(V_PARAMS), I: 1, D: len(D_PARAMS), M: len(M_PARAMS)}
-PARAM_NAMES = {R: ["r"], C: ["c"], V: V_PARAMS, I: ["dc"], D: D_PARAMS, M: M_PARAMS}
-TYPE_ORDER = [R, C, V, I, D, M]
-TYPE_LETTER = {R: "R", C: "C", V: "V", I: "I", D: "D", M: "M"}
+PARAMS_PER = {R: 1, C: 1, V: len(V_PARAMS), I: 1, D: len(D_PARAMS), M: len(M_PARAMS),
+              B3: len(B3_PARAMS)}
+PARAM_NAMES = {R: ["r"], C: ["c"], V: V_PARAMS, I: ["dc"], D: D_PARAMS, M: M_PARAMS,
+               B3: B3_PARAMS}
+TYPE_ORDER = [R, C, V, I, D, M, B3]
+TYPE_LETTER = {R: "R", C: "C", V: "V", I: "I", D: "D", M: "M", B3: "M"}
 
 
 @dataclass
@@ -125,6 +166,17 @@ class Circuit:
         prm = [kw[p] for p in M_PARAMS]
         self._add(name, M, [d, g, s, b], prm)
 
+    def B3(self, name, d, g, s, b, **params):
+        """A BSIM3v3 MOSFET (LEVEL 8/49 card, DC core)."""
+        kw = dict(B3_DEFAULTS)
+        kw["temp"] = self.temp_k
+        for k, v in params.items():
+            k = B3_ALIASES.get(k.lower(), k.lower())
+            if k not in kw:
+                raise ValueError(f"bsim3 parameter {k!r} is not supported")
+            kw[k] = float(v)
+        self._add(name, B3, [d, g, s, b], [kw[p] for p in B3_PARAMS])
+
     def set_temp(self, temp_c):
         """Circuit temperature for every device without its own TEMP."""
         self.temp_k = temp_c + 273.15
@@ -133,6 +185,8 @@ class Circuit:
                 d.params[D_PARAMS.index("temp")] = self.temp_k
             elif d.type == M:
                 d.params[M_PARAMS.index("temp")] = self.temp_k
+            elif d.type == B3:
+                d.params[B3_PARAMS.index("temp")] = self.temp_k
         self._frozen = None
 
     # ------------------------------------------------------------------
@@ -180,6 +234,16 @@ class Circuit:
                         nxt += 1
                     else:
                         ext.append(ext[2])
+                elif t == B3:
+                    # RSH times the squares NRD / NRS, else the node collapses
+                    rsh = d.params[B3_PARAMS.index("rsh")]
+                    for k, (sq, ref) in enumerate((("nrd", 0), ("nrs", 2))):
+                        if rsh > 0 and d.params[B3_PARAMS.index(sq)] > 0:
+                            ext.append(nxt)
+                            names[nxt] = f"{d.name}#{'di' if k == 0 else 'si'}"
+                            nxt += 1
+                        else:
+                            ext.append(ext[ref])
                 nodes[i] = ext
                 prm[i] = d.params
                 where[d.name] = (len(batches), i)

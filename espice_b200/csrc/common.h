@@ -7,7 +7,7 @@
 namespace esl {
 
 // Device types, numbered as the C ABI numbers them (include/espice_lanes.h).
-enum DevType : uint32_t { kR = 0, kC = 1, kV = 2, kI = 3, kD = 4, kM = 5, kNumTypes = 6 };
+enum DevType : uint32_t { kR = 0, kC = 1, kV = 2, kI = 3, kD = 4, kM = 5, kB3 = 6, kNumTypes = 7 };
 
 constexpr int kMaxBatches = 8;
 
@@ -21,7 +21,9 @@ constexpr int kMaxBatches = 8;
 //   M (local unknowns 0 d, 1 g, 2 s, 3 b, 4 di, 5 si):
 //      f0 f2 f3 f4 f5 | J00 J04 J22 J25 J33 J34 J35 J40 J41 J43 J44 J45 J51 J52 J53 J54 J55
 //      | q1 q3 q4 q5 | C11 C13 C14 C15 C31 C33 C34 C35 C41 C43 C44 C51 C53 C55
-constexpr int kStageR = 6, kStageC = 6, kStageV = 7, kStageI = 2, kStageD = 16, kStageM = 40;
+//   B3 (BSIM3 DC core, the MOS1 node set; the substrate current adds J31):
+//      f0 f2 f3 f4 f5 | J00 J04 J22 J25 J31 J33 J34 J35 J40 J41 J43 J44 J45 J51 J52 J53 J54 J55
+constexpr int kStageR = 6, kStageC = 6, kStageV = 7, kStageI = 2, kStageD = 16, kStageM = 40, kStageB3 = 23;
 // A MOS1 batch without any charge keeps only the residual and Jacobian cells.
 constexpr int kStageMNoQ = 22;
 
@@ -44,9 +46,28 @@ enum MosField {
 constexpr int kMosParams = 34;
 constexpr int kMParamRd = 6, kMParamRs = 7, kMParamTox = 19;
 
+// BSIM3v3 record fields: the bias-independent part of models/bsim3.va
+// (b3temp.c: temperature, geometry, parameter defaulting, junction sizing)
+// and the card values the bias-dependent chain reads, in the type frame.
+enum B3Field {
+  kB3Type, kB3Mobmod, kB3Vt, kB3Tratio1, kB3Vth0i, kB3Isats, kB3Isatd, kB3Nvtmj, kB3Vjsm, kB3Isevjsm,
+  kB3Vjdm, kB3Isevjdm, kB3Ijth, kB3Gmin, kB3Vbsc, kB3Phi, kB3Sqrtphi, kB3Phis3, kB3Xdep0, kB3Factor1,
+  kB3Dvt2, kB3Dvt2w, kB3Dvt1, kB3Dvt1w, kB3Dvt0, kB3Dvt0w, kB3Leff, kB3Weff, kB3Vbi, kB3Nlx, kB3K1x,
+  kB3K1ox, kB3K2ox, kB3Kt1, kB3Kt1l, kB3Kt2, kB3Tox, kB3W0, kB3K3, kB3K3b, kB3Eta0, kB3Etab,
+  kB3Theta0vb0, kB3Nfactor, kB3Cdsc, kB3Cdscb, kB3Cdscd, kB3Cit, kB3Cox, kB3Vfbi, kB3Ngate, kB3Voff,
+  kB3Cdep0, kB3Dwg, kB3Dwb, kB3Rds0, kB3Prwg, kB3Prwb, kB3Xj, kB3A0, kB3B0, kB3B1, kB3Ags, kB3Keta,
+  kB3Ua, kB3Ub, kB3Uc, kB3U0temp, kB3Vsattemp, kB3A1, kB3A2, kB3Delta, kB3Pclm, kB3Litl,
+  kB3Thetarout, kB3Pdiblcb, kB3Pvag, kB3Pscbe1, kB3Pscbe2, kB3Alpha0, kB3Alpha1, kB3Beta0, kB3M,
+  kB3Gdrain, kB3Gsource, kB3Vt0, kB3Vcrit, kB3SeedVgs, kB3Fields
+};
+// Card slots (models/bsim3.va:26-138, then gmin and the temperature in K);
+// NaN marks a parameter whose default the model derives ($param_given).
+constexpr int kB3Params = 109;
+constexpr int kB3ParamRsh = 95, kB3ParamNrd = 102, kB3ParamNrs = 103;
+
 // Limited images per instance: a diode's junction voltage; a MOSFET's
 // vgs, vds, vbs in the type frame.
-constexpr uint32_t lim_count(uint32_t type) { return type == kD ? 1u : type == kM ? 3u : 0u; }
+constexpr uint32_t lim_count(uint32_t type) { return type == kD ? 1u : (type == kM || type == kB3) ? 3u : 0u; }
 
 // Special gather sources beside staging positions.
 constexpr uint32_t kSrcOne = 0xfffffffeu;    // + 1.0 (the ground pin on g)

@@ -66,6 +66,7 @@ uint32_t stage_stride(uint32_t type) {
     case kI: return kStageI;
     case kD: return kStageD;
     case kM: return kStageM;
+    case kB3: return kStageB3;
     default: return 0;
   }
 }
@@ -154,6 +155,38 @@ InstLayout layout_of(uint32_t type, const double* prm) {
         L.qjac = {{1, 1, 26}, {1, 3, 27}, {1, 4, 28}, {1, 5, 29}, {3, 1, 30}, {3, 3, 31}, {3, 4, 32},
                   {3, 5, 33}, {4, 1, 34}, {4, 3, 35}, {4, 4, 36}, {5, 1, 37}, {5, 3, 38}, {5, 5, 39}};
       }
+      break;
+    }
+    case kB3: {  // d g s b di si (models/bsim3.va:613-624); the DC core has no charges
+      const double rsh = prm[kB3ParamRsh];
+      const bool rd = rsh > 0 && prm[kB3ParamNrd] > 0, rs = rsh > 0 && prm[kB3ParamNrs] > 0;
+      if (rd) L.res.push_back({0, 0, 0});
+      if (rs) L.res.push_back({2, 0, 1});
+      L.res.push_back({3, 0, 2});
+      L.res.push_back({4, 0, 3});
+      L.res.push_back({5, 0, 4});
+      if (rd) {
+        L.jac.push_back({0, 0, 5});
+        L.jac.push_back({0, 4, 6});
+      }
+      if (rs) {
+        L.jac.push_back({2, 2, 7});
+        L.jac.push_back({2, 5, 8});
+      }
+      L.jac.push_back({3, 1, 9});
+      L.jac.push_back({3, 3, 10});
+      L.jac.push_back({3, 4, 11});
+      L.jac.push_back({3, 5, 12});
+      if (rd) L.jac.push_back({4, 0, 13});
+      L.jac.push_back({4, 1, 14});
+      L.jac.push_back({4, 3, 15});
+      L.jac.push_back({4, 4, 16});
+      L.jac.push_back({4, 5, 17});
+      L.jac.push_back({5, 1, 18});
+      if (rs) L.jac.push_back({5, 2, 19});
+      L.jac.push_back({5, 3, 20});
+      L.jac.push_back({5, 4, 21});
+      L.jac.push_back({5, 5, 22});
       break;
     }
     default:
@@ -930,6 +963,12 @@ int32_t prepare_dc(esl_ctx* ctx, const esl_newton_opts* opts, double* d_x, int c
             li[3 * i + 1] = 0.0;
             li[3 * i + 2] = -1.0;
           }
+        if (B.type == kB3)
+          for (uint32_t i = 0; i < B.count; ++i) {
+            li[3 * i] = rec[kB3SeedVgs * B.count + i];
+            li[3 * i + 1] = 0.1;
+            li[3 * i + 2] = 0.0;
+          }
       }
     ESL_CUDA(cudaMemsetAsync(d_x, 0, size_t(N) * n * 8, s));
   }
@@ -1093,6 +1132,12 @@ int32_t ensure_tape_cold(esl_ctx* ctx) {
         lim[B.lim_off + 3 * i] = rec[kMSeedVgs * B.count + i];
         lim[B.lim_off + 3 * i + 1] = 0.0;
         lim[B.lim_off + 3 * i + 2] = -1.0;
+      }
+    if (B.type == kB3)
+      for (uint32_t i = 0; i < B.count; ++i) {
+        lim[B.lim_off + 3 * i] = rec[kB3SeedVgs * B.count + i];
+        lim[B.lim_off + 3 * i + 1] = 0.1;
+        lim[B.lim_off + 3 * i + 2] = 0.0;
       }
   }
   const uint32_t act = ctx->nlim ? 1u : 0u;
@@ -1328,7 +1373,8 @@ int32_t esl_group_dc_solve_device(esl_ctx* const* ctxs, uint32_t n_ctx, const es
   ESL_CUDA(cudaEventRecord(c0->ev0, s));
   ESL_CUDA(launch_dc_newton_group(c0->d_group_topo.as<TopoDev>(), c0->d_group_lanes.as<LaneDev>(),
                                   c0->d_group_cta_ctx.as<uint32_t>(), c0->d_group_cta_first.as<uint32_t>(),
-                                  c0->d_group_lpb.as<uint32_t>(), uint32_t(cta_ctx.size()), max_lpb, smem, o, s));
+                                  c0->d_group_lpb.as<uint32_t>(), uint32_t(cta_ctx.size()), max_lpb, smem, o,
+                                  std::any_of(topos.begin(), topos.end(), topo_has_b3), s));
   ESL_CUDA(cudaEventRecord(c0->ev1, s));
   ESL_CUDA(cudaEventSynchronize(c0->ev1));
   float ms = 0;

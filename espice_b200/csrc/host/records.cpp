@@ -23,17 +23,18 @@ uint32_t record_fields(uint32_t type) {
     case kI: return kIFields;
     case kD: return kDiodeFields;
     case kM: return kMosFields;
+    case kB3: return kB3Fields;
     default: return 0;
   }
 }
 
 uint32_t param_count(uint32_t type) {
-  static const uint32_t n[kNumTypes] = {1, 1, 10, 1, kDiodeParams, kMosParams};
+  static const uint32_t n[kNumTypes] = {1, 1, 10, 1, kDiodeParams, kMosParams, kB3Params};
   return type < kNumTypes ? n[type] : 0;
 }
 
 uint32_t node_count(uint32_t type) {
-  static const uint32_t n[kNumTypes] = {2, 2, 3, 2, 3, 6};
+  static const uint32_t n[kNumTypes] = {2, 2, 3, 2, 3, 6, 6};
   return type < kNumTypes ? n[type] : 0;
 }
 
@@ -188,6 +189,233 @@ static void mos1_record(const double* p, double* rec, uint32_t stride) {
   put(kMSeedVgs, type * vbit + gammax * std::sqrt(phit));
 }
 
+// BSIM3v3 card slots, in the order of include/espice_lanes.h (ESL_B3).
+enum B3Slot {
+  sType, sMobmod, sTnom, sTox, sToxm, sXj, sNch, sNsub, sNgate, sGamma1, sGamma2, sXt, sVbx, sVbm, sK1,
+  sK2, sK3, sK3b, sW0, sNlx, sVth0, sVfb, sDvt0, sDvt1, sDvt2, sDvt0w, sDvt1w, sDvt2w, sDrout, sDsub,
+  sNfactor, sCdsc, sCdscb, sCdscd, sCit, sVsat, sAt, sA0, sAgs, sA1, sA2, sKeta, sUa, sUa1, sUb, sUb1,
+  sUc, sUc1, sU0, sUte, sVoff, sDelta, sRdsw, sPrwg, sPrwb, sPrt, sWr, sEta0, sEtab, sPclm, sPdiblc1,
+  sPdiblc2, sPdiblcb, sPscbe1, sPscbe2, sPvag, sDwg, sDwb, sB0, sB1, sAlpha0, sAlpha1, sBeta0, sKt1,
+  sKt1l, sKt2, sLint, sLl, sLln, sLw, sLwn, sLwl, sWint, sWl, sWln, sWw, sWwn, sWwl, sXl, sXw, sJs,
+  sJsw, sNj, sXti, sIjth, sRsh, sL, sW, sAd, sAs, sPd, sPs, sNrd, sNrs, sMult, sDelvto, sMulu0, sGmin,
+  sTemp, sB3Slots
+};
+static_assert(sB3Slots == kB3Params && sRsh == kB3ParamRsh && sNrd == kB3ParamNrd && sNrs == kB3ParamNrs,
+              "BSIM3 card slots");
+
+// models/bsim3.va:186-346 (b3temp.c): temperature scaling, geometry,
+// parameter defaulting ($param_given = a non-NaN slot), the doping-derived
+// quantities, the k1/k2 ladder, vfb/vth0, junction sizing and the series
+// resistance; then the fields the bias-dependent chain reads.
+static void bsim3_record(const double* p, double* rec, uint32_t stride) {
+  auto given = [&](int k) { return !std::isnan(p[k]); };
+  const double type = p[sType], tox = p[sTox];
+  const double tnomk = p[sTnom] + 273.15, tk = p[sTemp];
+  const double tratio = tk / tnomk;
+  const double vtnom = 8.617087e-5 * tnomk;
+  const double vt = 8.617087e-5 * tk;
+  const double eg0 = 1.16 - 7.02e-4 * tnomk * tnomk / (tnomk + 1108.0);
+  const double eg = 1.16 - 7.02e-4 * tk * tk / (tk + 1108.0);
+  const double ni = 1.45e10 * (tnomk / 300.15) * std::sqrt(tnomk / 300.15) * std::exp(21.5565981 - eg0 / (2.0 * vtnom));
+  const double cox = 3.453133e-11 / tox;
+  const double factor1 = std::sqrt(1.03594e-10 / 3.453133e-11 * tox);
+  // pnjlim's constants at the device-support frame's 300.15 K
+  const double vt0 = kBoltz * 300.15 / kCharge;
+  const double vcrit = vt0 * std::log(vt0 / (1.4142135623730951 * 1.0e-14));
+  double jst = p[sJs], jswt = p[sJsw];
+  if (tk != tnomk) {
+    const double jtmp = std::exp((eg0 / vtnom - eg / vt + p[sXti] * std::log(tratio)) / p[sNj]);
+    jst = p[sJs] * jtmp;
+    jswt = p[sJsw] * jtmp;
+  }
+  if (jst < 0.0) jst = 0.0;
+  if (jswt < 0.0) jswt = 0.0;
+
+  const double l = p[sL], w = p[sW];
+  const double pl = std::pow(l, p[sLln]), pw = std::pow(w, p[sLwn]);
+  const double dl = p[sLint] + p[sLl] / pl + p[sLw] / pw + p[sLwl] / (pl * pw);
+  const double ql = std::pow(l, p[sWln]), qw = std::pow(w, p[sWwn]);
+  const double dw = p[sWint] + p[sWl] / ql + p[sWw] / qw + p[sWwl] / (ql * qw);
+  double leff = l + p[sXl] - 2.0 * dl;
+  double weff = w + p[sXw] - 2.0 * dw;
+  if (leff < 1.0e-9) leff = 1.0e-9;
+  if (weff < 1.0e-9) weff = 1.0e-9;
+
+  const int mobmod = static_cast<int>(p[sMobmod]);
+  const double uax = p[sUa] + p[sUa1] * (tratio - 1.0);
+  const double ubx = p[sUb] + p[sUb1] * (tratio - 1.0);
+  double ucx = given(sUc) ? p[sUc] : (mobmod == 3 ? -0.0465 : -0.0465e-9);
+  const double uc1x = given(sUc1) ? p[sUc1] : (mobmod == 3 ? -0.056 : -0.056e-9);
+  ucx = ucx + uc1x * (tratio - 1.0);
+  double u0x = given(sU0) ? p[sU0] : (type > 0.0 ? 0.067 : 0.025);
+  if (u0x > 1.0) u0x = u0x / 1.0e4;  // a cm^2/Vs card value
+  const double u0temp = u0x * std::pow(tratio, p[sUte]) * p[sMulu0];
+  const double vsattemp = p[sVsat] - p[sAt] * (tratio - 1.0);
+  const double rds0 = (p[sRdsw] + p[sPrt] * (tratio - 1.0)) / std::pow(weff * 1.0e6, p[sWr]);
+
+  double npeak;
+  if (given(sNch)) {
+    npeak = p[sNch];
+    if (npeak > 1.0e20) npeak = npeak * 1.0e-6;  // an m^-3 card value
+  } else if (given(sGamma1)) {
+    const double g = p[sGamma1] * cox;
+    npeak = 3.021e22 * g * g;
+  } else {
+    npeak = 1.7e17;
+  }
+  double ngate = p[sNgate];
+  if (ngate > 1.000001e24) ngate = ngate * 1.0e-6;
+  const double phi = 2.0 * vtnom * std::log(npeak / ni);
+  const double sqrtphi = std::sqrt(phi);
+  const double xdep0 = std::sqrt(2.0 * 1.03594e-10 / (1.60219e-19 * npeak * 1.0e6)) * sqrtphi;
+  const double vbi = vtnom * std::log(1.0e20 * npeak / (ni * ni));
+  const double cdep0 = std::sqrt(1.60219e-19 * 1.03594e-10 * npeak * 1.0e6 / 2.0 / phi);
+
+  double vbm = p[sVbm], k1, k2;
+  if (given(sK1) || given(sK2)) {
+    k1 = given(sK1) ? p[sK1] : 0.53;
+    k2 = given(sK2) ? p[sK2] : -0.0186;
+  } else {
+    double vbx = given(sVbx) ? p[sVbx] : phi - 7.7348e-4 * npeak * p[sXt] * p[sXt];
+    if (vbx > 0.0) vbx = -vbx;
+    if (vbm > 0.0) vbm = -vbm;
+    const double g1 = given(sGamma1) ? p[sGamma1] : 5.753e-12 * std::sqrt(npeak) / cox;
+    const double g2 = given(sGamma2) ? p[sGamma2] : 5.753e-12 * std::sqrt(p[sNsub]) / cox;
+    const double a = g1 - g2;
+    const double b = std::sqrt(phi - vbx) - sqrtphi;
+    const double c = std::sqrt(phi * (phi - vbm)) - phi;
+    k2 = a * b / (2.0 * c + vbm);
+    k1 = g2 - 2.0 * k2 * std::sqrt(phi - vbm);
+  }
+  double vbsc = -30.0;
+  if (k2 < 0.0) {
+    const double h = 0.5 * k1 / k2;
+    vbsc = 0.9 * (phi - h * h);
+    if (vbsc > -3.0) vbsc = -3.0;
+    else if (vbsc < -30.0) vbsc = -30.0;
+  }
+  if (vbsc > vbm) vbsc = vbm;
+
+  double vfb;
+  if (given(sVfb)) vfb = p[sVfb];
+  else if (given(sVth0)) vfb = type * p[sVth0] - phi - k1 * sqrtphi;
+  else vfb = -1.0;
+  const double vth0 = given(sVth0) ? p[sVth0] : type * (vfb + phi + k1 * sqrtphi);
+  const double vth0i = vth0 + p[sDelvto];
+  const double vfbi = vfb + type * p[sDelvto];
+  const double toxm = given(sToxm) ? p[sToxm] : tox;
+  const double dsub = given(sDsub) ? p[sDsub] : p[sDrout];
+  const double lt0 = factor1 * std::sqrt(xdep0);
+  const double e1 = std::exp(-0.5 * dsub * leff / lt0);
+  const double e2 = std::exp(-0.5 * p[sDrout] * leff / lt0);
+
+  const double nvtmj = vt * p[sNj];
+  const double isats = (p[sAs] <= 0.0 && p[sPs] <= 0.0) ? 1.0e-14 : p[sAs] * jst + p[sPs] * jswt;
+  const double isatd = (p[sAd] <= 0.0 && p[sPd] <= 0.0) ? 1.0e-14 : p[sAd] * jst + p[sPd] * jswt;
+  const double ijth = p[sIjth];
+  double vjsm = 0.0, isevjsm = 0.0, vjdm = 0.0, isevjdm = 0.0;
+  if (isats > 0.0 && ijth > 0.0) {
+    vjsm = nvtmj * std::log(ijth / isats + 1.0);
+    isevjsm = isats * std::exp(vjsm / nvtmj);
+  }
+  if (isatd > 0.0 && ijth > 0.0) {
+    vjdm = nvtmj * std::log(ijth / isatd + 1.0);
+    isevjdm = isatd * std::exp(vjdm / nvtmj);
+  }
+  const double m = p[sMult], rsh = p[sRsh];
+
+  auto put = [&](int f, double v) { rec[f * stride] = v; };
+  put(kB3Type, type);
+  put(kB3Mobmod, static_cast<double>(mobmod));
+  put(kB3Vt, vt);
+  put(kB3Tratio1, tk / tnomk - 1.0);
+  put(kB3Vth0i, vth0i);
+  put(kB3Isats, isats);
+  put(kB3Isatd, isatd);
+  put(kB3Nvtmj, nvtmj);
+  put(kB3Vjsm, vjsm);
+  put(kB3Isevjsm, isevjsm);
+  put(kB3Vjdm, vjdm);
+  put(kB3Isevjdm, isevjdm);
+  put(kB3Ijth, ijth);
+  put(kB3Gmin, p[sGmin]);
+  put(kB3Vbsc, vbsc);
+  put(kB3Phi, phi);
+  put(kB3Sqrtphi, sqrtphi);
+  put(kB3Phis3, sqrtphi * phi);
+  put(kB3Xdep0, xdep0);
+  put(kB3Factor1, factor1);
+  put(kB3Dvt2, p[sDvt2]);
+  put(kB3Dvt2w, p[sDvt2w]);
+  put(kB3Dvt1, p[sDvt1]);
+  put(kB3Dvt1w, p[sDvt1w]);
+  put(kB3Dvt0, p[sDvt0]);
+  put(kB3Dvt0w, p[sDvt0w]);
+  put(kB3Leff, leff);
+  put(kB3Weff, weff);
+  put(kB3Vbi, vbi);
+  put(kB3Nlx, p[sNlx]);
+  put(kB3K1x, k1);
+  put(kB3K1ox, k1 * tox / toxm);
+  put(kB3K2ox, k2 * tox / toxm);
+  put(kB3Kt1, p[sKt1]);
+  put(kB3Kt1l, p[sKt1l]);
+  put(kB3Kt2, p[sKt2]);
+  put(kB3Tox, tox);
+  put(kB3W0, p[sW0]);
+  put(kB3K3, p[sK3]);
+  put(kB3K3b, p[sK3b]);
+  put(kB3Eta0, p[sEta0]);
+  put(kB3Etab, p[sEtab]);
+  put(kB3Theta0vb0, e1 + 2.0 * e1 * e1);
+  put(kB3Nfactor, p[sNfactor]);
+  put(kB3Cdsc, p[sCdsc]);
+  put(kB3Cdscb, p[sCdscb]);
+  put(kB3Cdscd, p[sCdscd]);
+  put(kB3Cit, p[sCit]);
+  put(kB3Cox, cox);
+  put(kB3Vfbi, vfbi);
+  put(kB3Ngate, ngate);
+  put(kB3Voff, p[sVoff]);
+  put(kB3Cdep0, cdep0);
+  put(kB3Dwg, p[sDwg]);
+  put(kB3Dwb, p[sDwb]);
+  put(kB3Rds0, rds0);
+  put(kB3Prwg, p[sPrwg]);
+  put(kB3Prwb, p[sPrwb]);
+  put(kB3Xj, p[sXj]);
+  put(kB3A0, p[sA0]);
+  put(kB3B0, p[sB0]);
+  put(kB3B1, p[sB1]);
+  put(kB3Ags, p[sAgs]);
+  put(kB3Keta, p[sKeta]);
+  put(kB3Ua, uax);
+  put(kB3Ub, ubx);
+  put(kB3Uc, ucx);
+  put(kB3U0temp, u0temp);
+  put(kB3Vsattemp, vsattemp);
+  put(kB3A1, p[sA1]);
+  put(kB3A2, p[sA2]);
+  put(kB3Delta, p[sDelta]);
+  put(kB3Pclm, p[sPclm]);
+  put(kB3Litl, std::sqrt(3.0 * p[sXj] * tox));
+  put(kB3Thetarout, p[sPdiblc1] * (e2 + 2.0 * e2 * e2) + p[sPdiblc2]);
+  put(kB3Pdiblcb, p[sPdiblcb]);
+  put(kB3Pvag, p[sPvag]);
+  put(kB3Pscbe1, p[sPscbe1]);
+  put(kB3Pscbe2, p[sPscbe2]);
+  put(kB3Alpha0, p[sAlpha0]);
+  put(kB3Alpha1, p[sAlpha1]);
+  put(kB3Beta0, p[sBeta0]);
+  put(kB3M, m);
+  put(kB3Gdrain, (rsh > 0.0 && p[sNrd] > 0.0) ? m / (rsh * p[sNrd]) : 0.0);
+  put(kB3Gsource, (rsh > 0.0 && p[sNrs] > 0.0) ? m / (rsh * p[sNrs]) : 0.0);
+  put(kB3Vt0, vt0);
+  put(kB3Vcrit, vcrit);
+  // MODEINITJCT (b3ld.c:202-214): vgs = type*vth0 + 0.1, vds = 0.1, vbs = 0
+  put(kB3SeedVgs, type * vth0i + 0.1);
+}
+
 void derive_instance(uint32_t type, const double* params, double* rec, uint32_t stride) {
   switch (type) {
     case kR:
@@ -203,6 +431,9 @@ void derive_instance(uint32_t type, const double* params, double* rec, uint32_t 
       break;
     case kM:
       mos1_record(params, rec, stride);
+      break;
+    case kB3:
+      bsim3_record(params, rec, stride);
       break;
     default:
       break;

@@ -40,7 +40,10 @@ cudaError_t launch_lu_lanes_mixed(const TopoDev& T, const uint2* seq, uint32_t n
 // Uneven batching: one launch over the lanes of several topologies.
 cudaError_t launch_dc_newton_group(const TopoDev* d_topos, const LaneDev* d_lanes, const uint32_t* d_cta_ctx,
                                    const uint32_t* d_cta_first, const uint32_t* d_ctx_lpb, uint32_t n_ctas,
-                                   uint32_t max_lpb, size_t smem, const LaneOpts& o, cudaStream_t s);
+                                   uint32_t max_lpb, size_t smem, const LaneOpts& o, bool has_b3, cudaStream_t s);
+// True when a topology has a BSIM3 batch (its lanes run the kernels'
+// BSIM3 instantiation).
+bool topo_has_b3(const TopoDev& T);
 
 // Fixed lane scratch of the allocation-free DC entry point: its size, the
 // device address of the array on the current device (looked up once per

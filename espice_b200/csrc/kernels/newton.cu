@@ -32,6 +32,7 @@
 #include "launch.h"
 #include "lanes.cuh"
 #include "models.cuh"
+#include "bsim3.cuh"
 
 namespace esl {
 
@@ -121,6 +122,7 @@ __device__ __forceinline__ double* stage_programs(const TopoDev& T, unsigned cha
 
 // Device evaluation: every instance of every batch, strided over the warp,
 // each writing its own staging cells (no shared cell, no atomics).
+template <bool kHasB3>
 __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, bool lim_active,
                          const SimDev& sim, int tid, bool charges_only = false, const double* vcache = nullptr) {
   for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
@@ -181,6 +183,11 @@ __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, 
           break;
         case kD:
           diode_stamp(r, s, m.x[nd[0]], m.x[nd[1]], m.x[nd[2]], lim_active ? m.lim + B.lim_off + i : nullptr, st);
+          break;
+        case kB3:
+          if constexpr (kHasB3)
+            bsim3_stamp(r, s, m.x[nd[0]], m.x[nd[1]], m.x[nd[2]], m.x[nd[3]], m.x[nd[4]], m.x[nd[5]],
+                        lim_active ? m.lim + B.lim_off + 3 * i : nullptr, st);
           break;
         default:
           break;
@@ -391,12 +398,13 @@ __device__ __forceinline__ double residual_gate(const LaneOpts& o, double diag, 
 // pnjlim on every diode, and the MOS1 ladder on every MOSFET, against their
 // images (or x_old before the first pass); true when any junction was
 // limited (Circuit.applyLimits).
+template <bool kHasB3>
 __device__ bool apply_limits(const TopoDev& T, const double* rec, const LaneMem& m, bool lim_active, int tid) {
   bool limited = false;
   for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
     const BatchDev& B = T.b[bi];
     const int s = static_cast<int>(B.count);
-    if (B.type == kM) {
+    if (B.type == kM || B.type == kB3) {
       for (uint32_t i = tid; i < B.count; i += 32) {
         const uint32_t* nd = B.nodes + size_t(i) * B.nt;
         double* li = m.lim + B.lim_off + 3 * i;
@@ -406,12 +414,15 @@ __device__ bool apply_limits(const TopoDev& T, const double* rec, const LaneMem&
           old[1] = li[1];
           old[2] = li[2];
         } else {
-          const double type = rec[B.rec_off + kMType * s + i];
+          const double type = rec[B.rec_off + (B.type == kM ? kMType : kB3Type) * s + i];
           old[0] = type * (m.xo[nd[1]] - m.xo[nd[5]]);
           old[1] = type * (m.xo[nd[4]] - m.xo[nd[5]]);
           old[2] = type * (m.xo[nd[3]] - m.xo[nd[5]]);
         }
-        limited |= mos1_limit(rec + B.rec_off + i, s, m.x[nd[1]], m.x[nd[3]], m.x[nd[4]], m.x[nd[5]], old, li);
+        if (B.type == kM)
+          limited |= mos1_limit(rec + B.rec_off + i, s, m.x[nd[1]], m.x[nd[3]], m.x[nd[4]], m.x[nd[5]], old, li);
+        else if constexpr (kHasB3)
+          limited |= bsim3_limit(rec + B.rec_off + i, s, m.x[nd[1]], m.x[nd[3]], m.x[nd[4]], m.x[nd[5]], old, li);
       }
       continue;
     }
@@ -433,6 +444,7 @@ __device__ bool apply_limits(const TopoDev& T, const double* rec, const LaneMem&
 
 // One lane's DC Newton solve (converger.zig newtonLanes at W = 1 with the
 // lane's own direct solver), by the warp that owns it.
+template <bool kHasB3>
 __device__ void dc_solve_lane(const TopoDev& T, const LaneDev& L, const LaneOpts& o, uint32_t prog, double* block,
                               uint32_t lane, int tid) {
   const uint32_t status = L.status[lane];
@@ -469,7 +481,7 @@ __device__ void dc_solve_lane(const TopoDev& T, const LaneDev& L, const LaneOpts
 
   for (; iter < max_iter; ++iter) {
     if (!have_step) {
-      eval_all(T, rec, m, lim_active, sim, tid);
+      eval_all<kHasB3>(T, rec, m, lim_active, sim, tid);
       __syncwarp();
       assemble(T, prog, m, tid);
       __syncwarp();
@@ -550,7 +562,7 @@ __device__ void dc_solve_lane(const TopoDev& T, const LaneDev& L, const LaneOpts
     }
     worst = warp_max_u64(worst);
     __syncwarp();
-    const bool limited = apply_limits(T, rec, m, lim_active, tid);
+    const bool limited = apply_limits<kHasB3>(T, rec, m, lim_active, tid);
     if (T.nlim) lim_active = true;
 
     bool ok = !limited && iter != 0 && !(from_bits(worst) >= 1.0);
@@ -590,6 +602,7 @@ __device__ void dc_solve_lane(const TopoDev& T, const LaneDev& L, const LaneOpts
 // DC Newton over independent sweep points (sweep/lanes.zig solveBatch:
 // each lane bitwise its own converger.run), one warp per lane; a persistent
 // grid, each CTA staging the programs once and taking lanes in turn.
+template <bool kHasB3>
 __global__ void __launch_bounds__(256) dc_newton_kernel(TopoDev T, LaneDev L, LaneOpts o) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* lanes_smem = stage_programs(T, smem_raw);
@@ -598,7 +611,7 @@ __global__ void __launch_bounds__(256) dc_newton_kernel(TopoDev T, LaneDev L, La
   const uint32_t warps = blockDim.x >> 5, w = threadIdx.x >> 5;
   double* block = lanes_smem + size_t(w) * T.smem_doubles;
   for (uint32_t lane = blockIdx.x * warps + w; lane < L.n_lanes; lane += gridDim.x * warps) {
-    dc_solve_lane(T, L, o, prog, block, lane, tid);
+    dc_solve_lane<kHasB3>(T, L, o, prog, block, lane, tid);
     __syncwarp();
   }
 }
@@ -641,6 +654,7 @@ __global__ void __launch_bounds__(256) lu_replay_kernel(TopoDev T, uint32_t n_la
 // The matrix of one lane at its start point, in pattern order: the lead
 // lane's first Jacobian, which the host factors into the pivot tape
 // (gpu_lanes.zig:361-372 factors lane 0 on the host the same way).
+template <bool kHasB3>
 __global__ void assemble_kernel(TopoDev T, LaneDev L, uint32_t lane, double* out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* smem = reinterpret_cast<double*>(smem_raw);
@@ -654,7 +668,7 @@ __global__ void assemble_kernel(TopoDev T, LaneDev L, uint32_t lane, double* out
   sim.src_scale = 1.0;
   sim.kind = 0;
   __syncwarp();
-  eval_all(T, L.rec + size_t(lane) * T.rec_size, m, L.lim_active[lane] != 0, sim, tid);
+  eval_all<kHasB3>(T, L.rec + size_t(lane) * T.rec_size, m, L.lim_active[lane] != 0, sim, tid);
   __syncwarp();
   gather_pattern(T, m, out, tid);
 }
@@ -674,23 +688,41 @@ static uint32_t persistent_grid(K kernel, uint32_t n_lanes, uint32_t lanes_per_b
   return need < cap ? need : cap;
 }
 
+// Every lane kernel comes in two instantiations: without BSIM3 (the
+// register budget of the MOS1, diode and passive models) and with it (the
+// BSIM3 dual-number chain raises the per-thread register need). The launch
+// takes the second only for a topology that has a BSIM3 batch.
+bool topo_has_b3(const TopoDev& T) {
+  for (uint32_t b = 0; b < T.n_batches; ++b)
+    if (T.b[b].type == kB3) return true;
+  return false;
+}
+
+template <bool kHasB3>
+static cudaError_t launch_dc_newton_t(const TopoDev& T, const LaneDev& L, const LaneOpts& o, uint32_t lanes_per_block,
+                                      cudaStream_t s) {
+  const size_t smem = T.prog_bytes + lanes_per_block * lane_smem_bytes(T);
+  auto* k = dc_newton_kernel<kHasB3>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  k<<<persistent_grid(k, L.n_lanes, lanes_per_block, smem), 32 * lanes_per_block, smem, s>>>(T, L, o);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_dc_newton(const TopoDev& T, const LaneDev& L, const LaneOpts& o, uint32_t lanes_per_block,
                              cudaStream_t s) {
-  const size_t smem = T.prog_bytes + lanes_per_block * lane_smem_bytes(T);
-  cudaError_t e = cudaFuncSetAttribute(dc_newton_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  if (e != cudaSuccess) return e;
-  dc_newton_kernel<<<persistent_grid(dc_newton_kernel, L.n_lanes, lanes_per_block, smem), 32 * lanes_per_block, smem,
-                     s>>>(T, L, o);
-  return cudaGetLastError();
+  return topo_has_b3(T) ? launch_dc_newton_t<true>(T, L, o, lanes_per_block, s)
+                        : launch_dc_newton_t<false>(T, L, o, lanes_per_block, s);
 }
 
 cudaError_t launch_assemble(const TopoDev& T, const LaneDev& L, uint32_t lane, double* out, cudaStream_t s) {
   // Before the tape exists (the lead lane's first Jacobian) a lane needs no
   // tape values: x, xo, rhs, diag, staging and the limited images (nv = 0).
   const size_t smem = size_t(4 * T.n + T.nv + T.n_stage + T.nlim + 2) * sizeof(double);
-  cudaError_t e = cudaFuncSetAttribute(assemble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  auto* k = topo_has_b3(T) ? assemble_kernel<true> : assemble_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
-  assemble_kernel<<<1, 32, smem, s>>>(T, L, lane, out);
+  k<<<1, 32, smem, s>>>(T, L, lane, out);
   return cudaGetLastError();
 }
 
@@ -1069,6 +1101,12 @@ __global__ void lane_init_kernel(TopoDev T, LaneDev L, uint32_t cold, uint32_t i
         lim[B.lim_off + 3 * i + 1] = 0.0;
         lim[B.lim_off + 3 * i + 2] = -1.0;
       }
+    if (B.type == kB3)
+      for (uint32_t i = 0; i < B.count; ++i) {
+        lim[B.lim_off + 3 * i] = rec[B.rec_off + kB3SeedVgs * B.count + i];
+        lim[B.lim_off + 3 * i + 1] = 0.1;
+        lim[B.lim_off + 3 * i + 2] = 0.0;
+      }
   }
 }
 
@@ -1153,7 +1191,7 @@ __device__ __forceinline__ void row_charges(const TopoDev& T, uint32_t prog, con
 
 // The LTE charge states at x (capacitor charges, diode junction charges,
 // MOS1 overlap gate charges).
-__device__ void state_charges(const TopoDev& T, const double* rec, const double* x, double* out, int tid) {
+__device__ __forceinline__ void state_charges(const TopoDev& T, const double* rec, const double* x, double* out, int tid) {
   for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
     const BatchDev& B = T.b[bi];
     if (B.qt_sites == 0) continue;
@@ -1201,6 +1239,7 @@ __device__ void fill_sources(const TopoDev& T, const double* rec, const SimDev& 
 // points of a sequential sweep. `vcache` holds the sources' values
 // (fill_sources). Returns 0 converged (x holds the published iterate), 1
 // out of iterations, 2 the factor left the tape.
+template <bool kHasB3>
 __device__ int lane_newton(const TopoDev& T, uint32_t prog, const LaneMem& m, const double* rec, const LaneOpts& o,
                            const SimDev& sim, const Companion* cp, bool& lim_active, bool init_fix,
                            uint32_t& iters, const double* vcache, int tid) {
@@ -1208,7 +1247,7 @@ __device__ int lane_newton(const TopoDev& T, uint32_t prog, const LaneMem& m, co
   const uint32_t max_iter = o.max_iter < 100 ? 100 : o.max_iter;
   double limit = kXPlausible;
   for (uint32_t iter = 0; iter < max_iter; ++iter) {
-    eval_all(T, rec, m, lim_active, sim, tid, false, vcache);
+    eval_all<kHasB3>(T, rec, m, lim_active, sim, tid, false, vcache);
     __syncwarp();
     assemble(T, prog, m, tid);
     __syncwarp();
@@ -1269,7 +1308,7 @@ __device__ int lane_newton(const TopoDev& T, uint32_t prog, const LaneMem& m, co
     }
     worst = warp_max_u64(worst);
     __syncwarp();
-    const bool limited = apply_limits(T, rec, m, lim_active, tid);
+    const bool limited = apply_limits<kHasB3>(T, rec, m, lim_active, tid);
     if (T.nlim) lim_active = true;
     bool ok = !limited && iter != 0 && !(from_bits(worst) >= 1.0);
     if (ok) {
@@ -1301,7 +1340,7 @@ __device__ int lane_newton(const TopoDev& T, uint32_t prog, const LaneMem& m, co
 // CKTterr's bound over the LTE states (integrator.zig minDel at w = 1, then
 // the order-2 root): `method` 1 BE / 2 trap probed after a step integrated
 // with `cur`; q0..q3 the ring slots; NaN when a read entry is not finite.
-__device__ double step_bound(int method, int cur, uint32_t m, const double* q0, const double* q1, const double* q2,
+__device__ __forceinline__ double step_bound(int method, int cur, uint32_t m, const double* q0, const double* q1, const double* q2,
                              const double* q3, const double* ip, double ag0, double ag1, double dt, double dt1,
                              double dt2, const TranDev& P, int tid) {
   const double sum01 = dt + dt1, sum12 = dt1 + dt2, sum012 = dt + (dt1 + dt2);
@@ -1567,6 +1606,7 @@ __device__ double meas_value(const MeasDev& mc, const CrossDev* x) {
 
 }  // namespace
 
+template <bool kHasB3>
 __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, const LaneOpts& o, uint32_t prog,
                           double* block, uint32_t lane, int tid) {
   const uint32_t n = T.n, nq = T.n_qt;
@@ -1604,6 +1644,11 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
         m.lim[B.lim_off + 3 * i + 1] = 0.0;
         m.lim[B.lim_off + 3 * i + 2] = -1.0;
       }
+      if (B.type == kB3) {
+        m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kB3SeedVgs * B.count + i];
+        m.lim[B.lim_off + 3 * i + 1] = 0.1;
+        m.lim[B.lim_off + 3 * i + 2] = 0.0;
+      }
     }
   }
   __syncwarp();
@@ -1614,7 +1659,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
   op.max_iter = 100;
   uint32_t it = 0;
   fill_sources(T, rec, sim, vsrc, tid);
-  int rc = lane_newton(T, prog, m, rec, op, sim, nullptr, lim_active, true, it, vsrc, tid);
+  int rc = lane_newton<kHasB3>(T, prog, m, rec, op, sim, nullptr, lim_active, true, it, vsrc, tid);
   lim_active = false;
   stat[kTsOpIters] = it;
   uint32_t n_rec = 0;
@@ -1643,7 +1688,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
     }
     // charge histories, flat at q(x_op); no dynamic current yet
     sim.kind = 1;
-    eval_all(T, rec, m, false, sim, tid, true);
+    eval_all<kHasB3>(T, rec, m, false, sim, tid, true);
     __syncwarp();
     for (uint32_t i = tid; i < 4 * n; i += 32) qh[i] = 0.0;
     __syncwarp();
@@ -1700,13 +1745,13 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
         m.xo[i] = cur[i];
       }
       __syncwarp();
-      apply_limits(T, rec, m, false, tid);
+      apply_limits<kHasB3>(T, rec, m, false, tid);
       lim_active = T.nlim != 0;
       __syncwarp();
       Companion c{ag0, ag1, trap, slot(qh, n, 1), ipr};
       uint32_t iters = 0;
       fill_sources(T, rec, sim, vsrc, tid);
-      rc = lane_newton(T, prog, m, rec, nr, sim, &c, lim_active, false, iters, vsrc, tid);
+      rc = lane_newton<kHasB3>(T, prog, m, rec, nr, sim, &c, lim_active, false, iters, vsrc, tid);
       lim_active = false;
       stat[kTsAttempts] += 1;
       stat[kTsNrIters] += iters;
@@ -1726,7 +1771,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
       }
       double dt_next = steps == 0 ? dt : fmin(dt * 2.0, dt_max);
       if (has_charge) {
-        eval_all(T, rec, m, false, sim, tid, true);
+        eval_all<kHasB3>(T, rec, m, false, sim, tid, true);
         __syncwarp();
         row_charges(T, prog, m, slot(qh, n, 0), tid);
         state_charges(T, rec, m.x, slot(qt, nq, 0), tid);
@@ -1841,6 +1886,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
 // is also `prev` (dc.zig:376-379, after dctrcurv.c). A factor that leaves
 // the lead tape ends the lane's sweep (kSweepLeftTape); its later points
 // read not converged.
+template <bool kHasB3>
 __device__ void sweep_lane(const TopoDev& T, const LaneDev& L, const SweepDev& P, const LaneOpts& o, uint32_t prog,
                            double* block, uint32_t lane, int tid) {
   const uint32_t n = T.n;
@@ -1889,11 +1935,11 @@ __device__ void sweep_lane(const TopoDev& T, const LaneDev& L, const SweepDev& P
         m.xo[i] = prev[i];
       }
       __syncwarp();
-      apply_limits(T, rec, m, false, tid);
+      apply_limits<kHasB3>(T, rec, m, false, tid);
       lim_active = T.nlim != 0;
       __syncwarp();
       uint32_t it = 0;
-      rc = lane_newton(T, prog, m, rec, o, sim, nullptr, lim_active, false, it, vsrc, tid);
+      rc = lane_newton<kHasB3>(T, prog, m, rec, o, sim, nullptr, lim_active, false, it, vsrc, tid);
       it_total += it;
       for (uint32_t i = tid; i < n; i += 32) sol[i] = m.x[i];
       __syncwarp();
@@ -1909,12 +1955,17 @@ __device__ void sweep_lane(const TopoDev& T, const LaneDev& L, const SweepDev& P
             m.lim[B.lim_off + 3 * i + 1] = 0.0;
             m.lim[B.lim_off + 3 * i + 2] = -1.0;
           }
+          if (B.type == kB3) {
+            m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kB3SeedVgs * B.count + i];
+            m.lim[B.lim_off + 3 * i + 1] = 0.1;
+            m.lim[B.lim_off + 3 * i + 2] = 0.0;
+          }
         }
       }
       __syncwarp();
       lim_active = T.nlim != 0;
       uint32_t it = 0;
-      rc = lane_newton(T, prog, m, rec, cold_o, sim, nullptr, lim_active, true, it, vsrc, tid);
+      rc = lane_newton<kHasB3>(T, prog, m, rec, cold_o, sim, nullptr, lim_active, true, it, vsrc, tid);
       it_total += it;
       for (uint32_t i = tid; i < n; i += 32) sol[i] = m.x[i];
       __syncwarp();
@@ -1943,6 +1994,7 @@ __device__ void sweep_lane(const TopoDev& T, const LaneDev& L, const SweepDev& P
 // + ctx_lpb[that topology] (one warp each); it copies its topology's tables
 // into shared memory and stages that topology's programs, then runs the same
 // per-lane solve as dc_newton_kernel.
+template <bool kHasB3>
 __global__ void __launch_bounds__(256) dc_newton_group_kernel(const TopoDev* Ts, const LaneDev* Ls,
                                                               const uint32_t* cta_ctx, const uint32_t* cta_first,
                                                               const uint32_t* ctx_lpb, LaneOpts o) {
@@ -1961,20 +2013,22 @@ __global__ void __launch_bounds__(256) dc_newton_group_kernel(const TopoDev* Ts,
   const uint32_t w = threadIdx.x >> 5;
   const uint32_t lane = cta_first[blockIdx.x] + w;
   if (w < ctx_lpb[c] && lane < L.n_lanes)
-    dc_solve_lane(T, L, o, prog, lanes_smem + size_t(w) * T.smem_doubles, lane, tid);
+    dc_solve_lane<kHasB3>(T, L, o, prog, lanes_smem + size_t(w) * T.smem_doubles, lane, tid);
 }
 
 cudaError_t launch_dc_newton_group(const TopoDev* d_topos, const LaneDev* d_lanes, const uint32_t* d_cta_ctx,
                                    const uint32_t* d_cta_first, const uint32_t* d_ctx_lpb, uint32_t n_ctas,
-                                   uint32_t max_lpb, size_t smem, const LaneOpts& o, cudaStream_t s) {
-  cudaError_t e = cudaFuncSetAttribute(dc_newton_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+                                   uint32_t max_lpb, size_t smem, const LaneOpts& o, bool has_b3, cudaStream_t s) {
+  auto* k = has_b3 ? dc_newton_group_kernel<true> : dc_newton_group_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
-  dc_newton_group_kernel<<<n_ctas, 32 * max_lpb, smem, s>>>(d_topos, d_lanes, d_cta_ctx, d_cta_first, d_ctx_lpb, o);
+  k<<<n_ctas, 32 * max_lpb, smem, s>>>(d_topos, d_lanes, d_cta_ctx, d_cta_first, d_ctx_lpb, o);
   return cudaGetLastError();
 }
 
 // Transient lanes: a persistent grid, each CTA staging the programs once,
 // each warp running one lane's transient to its end.
+template <bool kHasB3>
 __global__ void __launch_bounds__(256) tran_kernel(TopoDev T, LaneDev L, TranDev P, LaneOpts o) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* lanes_smem = stage_programs(T, smem_raw);
@@ -1990,11 +2044,12 @@ __global__ void __launch_bounds__(256) tran_kernel(TopoDev T, LaneDev L, TranDev
     if (tid == 0) lane = atomicAdd(P.next_lane, 1u);
     lane = __shfl_sync(kFull, lane, 0);
     if (lane >= L.n_lanes) break;
-    tran_lane(T, L, P, o, prog, block, lane, tid);
+    tran_lane<kHasB3>(T, L, P, o, prog, block, lane, tid);
     __syncwarp();
   }
 }
 
+template <bool kHasB3>
 __global__ void __launch_bounds__(256) sweep_kernel(TopoDev T, LaneDev L, SweepDev P, LaneOpts o) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* lanes_smem = stage_programs(T, smem_raw);
@@ -2007,7 +2062,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(TopoDev T, LaneDev L, SweepD
     if (tid == 0) lane = atomicAdd(P.next_lane, 1u);
     lane = __shfl_sync(kFull, lane, 0);
     if (lane >= L.n_lanes) break;
-    sweep_lane(T, L, P, o, prog, block, lane, tid);
+    sweep_lane<kHasB3>(T, L, P, o, prog, block, lane, tid);
     __syncwarp();
   }
 }
@@ -2015,12 +2070,12 @@ __global__ void __launch_bounds__(256) sweep_kernel(TopoDev T, LaneDev L, SweepD
 cudaError_t launch_sweep(const TopoDev& T, const LaneDev& L, const SweepDev& P, const LaneOpts& o,
                          uint32_t lanes_per_block, cudaStream_t s) {
   const size_t smem = T.prog_bytes + lanes_per_block * size_t(sweep_doubles(T)) * sizeof(double);
-  cudaError_t e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  auto* k = topo_has_b3(T) ? sweep_kernel<true> : sweep_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(P.next_lane, 0, sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
-  sweep_kernel<<<persistent_grid(sweep_kernel, L.n_lanes, lanes_per_block, smem), 32 * lanes_per_block, smem, s>>>(
-      T, L, P, o);
+  k<<<persistent_grid(k, L.n_lanes, lanes_per_block, smem), 32 * lanes_per_block, smem, s>>>(T, L, P, o);
   return cudaGetLastError();
 }
 
@@ -2028,12 +2083,12 @@ cudaError_t launch_tran(const TopoDev& T, const LaneDev& L, const TranDev& P, co
                         uint32_t lanes_per_block, cudaStream_t s) {
   const size_t smem =
       T.prog_bytes + lanes_per_block * size_t(T.tran_doubles + kMeasDoubles * P.n_meas) * sizeof(double);
-  cudaError_t e = cudaFuncSetAttribute(tran_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  auto* k = topo_has_b3(T) ? tran_kernel<true> : tran_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(P.next_lane, 0, sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
-  tran_kernel<<<persistent_grid(tran_kernel, L.n_lanes, lanes_per_block, smem), 32 * lanes_per_block, smem, s>>>(
-      T, L, P, o);
+  k<<<persistent_grid(k, L.n_lanes, lanes_per_block, smem), 32 * lanes_per_block, smem, s>>>(T, L, P, o);
   return cudaGetLastError();
 }
 

@@ -14,13 +14,22 @@ supply ramp from 0 V at t = 0 (the operating point is all-zero and the ring
 leaves its metastable point on the devices' mismatch, not on rounding). Each
 lane draws every device's VTO from N(nominal, 30 mV). 34 unknowns. The
 transient is trapezoidal to 20 ns with a 1 ps maximum step.
+
+bsim3_inverters: a chain of CMOS inverters of BSIM3v3 (LEVEL 49) devices,
+L = 0.18 um, VDD = 1.8 V, each output loaded by 50 kohm to ground. The NMOS
+cards cycle through three variants so every branch of the DC core runs:
+the ngspice-fixture card (given VTH0, K1, K2), a card with the k1/k2 ladder
+and the vfb/vth0 defaults derived, RSH series resistance (internal drain and
+source nodes), impact ionisation (ALPHA0) and poly depletion (NGATE) under
+MOBMOD 2, and a MOBMOD 3 card. Each lane draws the input voltage from
+U(0, VDD) and every device's DELVTO from N(0, 20 mV).
 """
 
 from __future__ import annotations
 
 import numpy as np
 
-from .circuit import M, Circuit
+from .circuit import B3, M, Circuit
 
 
 def grid_diodes(seed: int = 1, rows: int = 8, cols: int = 8, n_diodes: int = 16,
@@ -83,4 +92,42 @@ def ring_oscillator(seed: int = 1, stages: int = 31, lanes: int = 1024, sigma: f
     slots = fr.slots_of(M, "vto")
     nominal = np.array([fr.batches[s.batch][2][s.inst, s.param] for s in slots])
     values = nominal + rng.normal(0.0, sigma, size=(lanes, len(slots)))
+    return fr, slots, values
+
+
+# BSIM3v3 cards (LEVEL 49): the NMOS of the reference's ngspice fixtures and
+# two variants, and the fixtures' PMOS.
+B3_NMOS = [
+    dict(type=1.0, tox=4.1e-9, vth0=0.35, k1=0.53, k2=-0.06, k3=80.0, vsat=1.5e5, ua=-1.4e-9, ub=2.3e-18,
+         uc=-4.6e-11, rdsw=200.0, u0=280.0, pclm=1.3, pdiblc1=0.39, pdiblc2=0.0086),
+    dict(type=1.0, mobmod=2.0, tox=4.1e-9, nch=2.3e17, vsat=1.4e5, u0=300.0, rdsw=150.0, rsh=20.0, nrd=1.0,
+         nrs=1.0, alpha0=1e-6, beta0=25.0, ngate=5e19),
+    dict(type=1.0, mobmod=3.0, tox=4.1e-9, vth0=0.4, k1=0.5, k2=-0.05, u0=260.0, ua=1.0e-9, ub=1.0e-18,
+         vsat=1.2e5, rdsw=250.0),
+]
+B3_PMOS = dict(type=-1.0, tox=4.1e-9, vth0=-0.4, k1=0.55, k2=-0.05, k3=80.0, vsat=1.2e5, ua=-1.4e-9,
+               ub=2.3e-18, uc=-4.6e-11, rdsw=400.0, u0=100.0, pclm=1.3, pdiblc1=0.39, pdiblc2=0.0086)
+
+
+def bsim3_inverters(seed: int = 1, stages: int = 6, lanes: int = 256, sigma: float = 0.02,
+                    vdd: float = 1.8, r_load: float = 50e3):
+    """Returns (frozen circuit, [input dc slot] + per-device delvto slots,
+    values [lanes][1 + 2 * stages])."""
+    rng = np.random.default_rng(seed)
+    c = Circuit()
+    c.V("vdd", "vdd", "0", dc=vdd)
+    c.V("vin", "s_in", "0", dc=0.0)
+    prev = "s_in"
+    for k in range(stages):
+        out = f"s{k}"
+        c.B3(f"mn{k}", out, prev, "0", "0", w=2e-6, l=0.18e-6, **B3_NMOS[k % len(B3_NMOS)])
+        c.B3(f"mp{k}", out, prev, "vdd", "vdd", w=4e-6, l=0.18e-6, **B3_PMOS)
+        c.R(f"rl{k}", out, "0", r_load)
+        prev = out
+    fr = c.freeze()
+    from .circuit import V
+    slots = [fr.slots_of(V, "dc")[1]] + fr.slots_of(B3, "delvto")
+    values = np.empty((lanes, len(slots)))
+    values[:, 0] = rng.uniform(0.0, vdd, lanes)
+    values[:, 1:] = rng.normal(0.0, sigma, size=(lanes, len(slots) - 1))
     return fr, slots, values

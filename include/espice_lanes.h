@@ -42,8 +42,23 @@ enum {
     ESL_V = 2, /* nodes p n br;       params dc wave v1 v2 td tr tf pw per phase */
     ESL_I = 3, /* nodes p n;          params dc                              */
     ESL_D = 4, /* nodes a c ai;       params is n rs bv ibv cjo vj m fc tt area gmin xti eg tnom temp */
-    ESL_M = 5  /* nodes d g s b di si; params (MOS1, models/mos1.va)         */
+    ESL_M = 5, /* nodes d g s b di si; params (MOS1, models/mos1.va)         */
+    ESL_B3 = 6 /* nodes d g s b di si; params (BSIM3v3 DC core, models/bsim3.va) */
 };
+
+/* ESL_B3 parameter slots: the model card of models/bsim3.va:26-138 in its
+ * order (type mobmod tnom tox toxm xj nch nsub ngate gamma1 gamma2 xt vbx
+ * vbm k1 k2 k3 k3b w0 nlx vth0 vfb dvt0 dvt1 dvt2 dvt0w dvt1w dvt2w drout
+ * dsub nfactor cdsc cdscb cdscd cit vsat at a0 ags a1 a2 keta ua ua1 ub ub1
+ * uc uc1 u0 ute voff delta rdsw prwg prwb prt wr eta0 etab pclm pdiblc1
+ * pdiblc2 pdiblcb pscbe1 pscbe2 pvag dwg dwb b0 b1 alpha0 alpha1 beta0 kt1
+ * kt1l kt2 lint ll lln lw lwn lwl wint wl wln ww wwn wwl xl xw js jsw nj xti
+ * ijth rsh), then the instance (l w ad as pd ps nrd nrs m delvto mulu0),
+ * then gmin and the device temperature in K: ESL_B3_PARAMS doubles. type is
+ * +1 NMOS, -1 PMOS. A NaN slot is a parameter left off the card: toxm, nch,
+ * gamma1, gamma2, vbx, k1, k2, vth0, vfb, dsub, uc, uc1 and u0 then take the
+ * defaults the model derives ($param_given). The DC core has no charges. */
+#define ESL_B3_PARAMS 109
 
 /* Per-lane outcome (esl_lane_result.status). */
 enum {

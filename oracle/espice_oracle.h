@@ -42,7 +42,8 @@ enum {
     ORC_I = 3,  /* nodes p n;          params dc                         */
     ORC_D = 4,  /* nodes a c ai;       params see ORC_D_* (ai == a: RS collapsed) */
     ORC_M = 5,  /* nodes d g s b di si; params see ORC_M_*               */
-    ORC_NTYPES = 6
+    ORC_B3 = 6, /* nodes d g s b di si; params see ORC_B3_* (BSIM3v3 DC) */
+    ORC_NTYPES = 7
 };
 
 /* Diode parameter slots (models/diode.va). */
@@ -60,6 +61,31 @@ enum {
     ORC_M_TOX, ORC_M_LD, ORC_M_U0, ORC_M_FC, ORC_M_W, ORC_M_L, ORC_M_AD,
     ORC_M_AS, ORC_M_PD, ORC_M_PS, ORC_M_DELVTO, ORC_M_M, ORC_M_GMIN,
     ORC_M_TNOM, ORC_M_TEMP, ORC_M_NP
+};
+
+/* BSIM3v3 DC-core parameter slots (models/bsim3.va:26-138, model card then
+ * instance). A NaN value means "not given": the slots whose defaults depend
+ * on $param_given (TOXM, NCH, GAMMA1, GAMMA2, VBX, K1, K2, VTH0, VFB, DSUB,
+ * UC, UC1, U0) take their derived defaults then. */
+enum {
+    ORC_B3_TYPE = 0, ORC_B3_MOBMOD, ORC_B3_TNOM, ORC_B3_TOX, ORC_B3_TOXM, ORC_B3_XJ,
+    ORC_B3_NCH, ORC_B3_NSUB, ORC_B3_NGATE, ORC_B3_GAMMA1, ORC_B3_GAMMA2, ORC_B3_XT,
+    ORC_B3_VBX, ORC_B3_VBM, ORC_B3_K1, ORC_B3_K2, ORC_B3_K3, ORC_B3_K3B, ORC_B3_W0,
+    ORC_B3_NLX, ORC_B3_VTH0, ORC_B3_VFB, ORC_B3_DVT0, ORC_B3_DVT1, ORC_B3_DVT2,
+    ORC_B3_DVT0W, ORC_B3_DVT1W, ORC_B3_DVT2W, ORC_B3_DROUT, ORC_B3_DSUB, ORC_B3_NFACTOR,
+    ORC_B3_CDSC, ORC_B3_CDSCB, ORC_B3_CDSCD, ORC_B3_CIT, ORC_B3_VSAT, ORC_B3_AT,
+    ORC_B3_A0, ORC_B3_AGS, ORC_B3_A1, ORC_B3_A2, ORC_B3_KETA, ORC_B3_UA, ORC_B3_UA1,
+    ORC_B3_UB, ORC_B3_UB1, ORC_B3_UC, ORC_B3_UC1, ORC_B3_U0, ORC_B3_UTE, ORC_B3_VOFF,
+    ORC_B3_DELTA, ORC_B3_RDSW, ORC_B3_PRWG, ORC_B3_PRWB, ORC_B3_PRT, ORC_B3_WR,
+    ORC_B3_ETA0, ORC_B3_ETAB, ORC_B3_PCLM, ORC_B3_PDIBLC1, ORC_B3_PDIBLC2,
+    ORC_B3_PDIBLCB, ORC_B3_PSCBE1, ORC_B3_PSCBE2, ORC_B3_PVAG, ORC_B3_DWG, ORC_B3_DWB,
+    ORC_B3_B0, ORC_B3_B1, ORC_B3_ALPHA0, ORC_B3_ALPHA1, ORC_B3_BETA0, ORC_B3_KT1,
+    ORC_B3_KT1L, ORC_B3_KT2, ORC_B3_LINT, ORC_B3_LL, ORC_B3_LLN, ORC_B3_LW, ORC_B3_LWN,
+    ORC_B3_LWL, ORC_B3_WINT, ORC_B3_WL, ORC_B3_WLN, ORC_B3_WW, ORC_B3_WWN, ORC_B3_WWL,
+    ORC_B3_XL, ORC_B3_XW, ORC_B3_JS, ORC_B3_JSW, ORC_B3_NJ, ORC_B3_XTI, ORC_B3_IJTH,
+    ORC_B3_RSH, ORC_B3_L, ORC_B3_W, ORC_B3_AD, ORC_B3_AS, ORC_B3_PD, ORC_B3_PS,
+    ORC_B3_NRD, ORC_B3_NRS, ORC_B3_M, ORC_B3_DELVTO, ORC_B3_MULU0, ORC_B3_GMIN,
+    ORC_B3_TEMP, ORC_B3_NP
 };
 
 typedef struct {
@@ -88,6 +114,11 @@ typedef struct {
 
 int orc_nodes_per(uint32_t type);
 int orc_params_per(uint32_t type);
+/* One instance's static stamp at local voltages xloc[nodes_per(type)] (node
+ * k of the instance is xloc[k]), no limiting: residuals f[6] and Jacobian
+ * J[6][6] over its local nodes, row-major. A test hook for the models'
+ * derivatives. Returns 0, or 1 for an unknown type. */
+int orc_dev_stamp(uint32_t type, const double *prm, const double *xloc, double *f, double *J);
 
 /* Pattern (Circuit.freeze): CSC with every diagonal, rows ascending.
  * col_ptr has n + 1 entries; row_idx capacity is given; returns nnz or -1. */

@@ -25,12 +25,12 @@
 #define QE 1.6021766208e-19
 
 int orc_nodes_per(uint32_t type) {
-    static const int t[ORC_NTYPES] = {2, 2, 3, 2, 3, 6};
+    static const int t[ORC_NTYPES] = {2, 2, 3, 2, 3, 6, 6};
     return type < ORC_NTYPES ? t[type] : 0;
 }
 
 int orc_params_per(uint32_t type) {
-    static const int t[ORC_NTYPES] = {1, 1, 10, 1, ORC_D_NP, ORC_M_NP};
+    static const int t[ORC_NTYPES] = {1, 1, 10, 1, ORC_D_NP, ORC_M_NP, ORC_B3_NP};
     return type < ORC_NTYPES ? t[type] : 0;
 }
 
@@ -112,6 +112,27 @@ void dev_layout(uint32_t type, const double *prm, layout_t *l) {
             add_qent(l, 4, 1); add_qent(l, 4, 3); add_qent(l, 4, 4);
             add_qent(l, 5, 1); add_qent(l, 5, 3); add_qent(l, 5, 5);
         }
+        break;
+    }
+    case ORC_B3: { /* d g s b di si (models/bsim3.va:613-624); no charges */
+        const double rsh = prm[ORC_B3_RSH];
+        int rd = rsh > 0 && prm[ORC_B3_NRD] > 0, rs = rsh > 0 && prm[ORC_B3_NRS] > 0;
+        l->nlim = 3;
+        if (rd) {
+            l->res_row[0] = 1;
+            add_ent(l, 0, 0); add_ent(l, 0, 4);
+        }
+        if (rs) {
+            l->res_row[2] = 1;
+            add_ent(l, 2, 2); add_ent(l, 2, 5);
+        }
+        l->res_row[3] = l->res_row[4] = l->res_row[5] = 1;
+        add_ent(l, 3, 1); add_ent(l, 3, 3); add_ent(l, 3, 4); add_ent(l, 3, 5);
+        if (rd) add_ent(l, 4, 0);
+        add_ent(l, 4, 1); add_ent(l, 4, 3); add_ent(l, 4, 4); add_ent(l, 4, 5);
+        add_ent(l, 5, 1);
+        if (rs) add_ent(l, 5, 2);
+        add_ent(l, 5, 3); add_ent(l, 5, 4); add_ent(l, 5, 5);
         break;
     }
     default:
@@ -326,6 +347,7 @@ void dev_derive(uint32_t type, const double *prm, double *der) {
     memset(der, 0, sizeof(double) * ORC_NDER);
     if (type == ORC_D) diode_derive(prm, der);
     if (type == ORC_M) mos1_derive(prm, der);
+    if (type == ORC_B3) bsim3_derive(prm, der);
 }
 
 /* PULSE waveform (vsource.va:211-222). */
@@ -430,6 +452,9 @@ void dev_eval(uint32_t type, const uint32_t *nd, const double *prm, const double
     case ORC_M:
         mos1_eval(nd, prm, der, x, lim, st, sim, o);
         break;
+    case ORC_B3:
+        bsim3_eval(nd, der, x, lim, o);
+        break;
     default:
         break;
     }
@@ -463,6 +488,7 @@ int dev_limit(uint32_t type, const uint32_t *nd, const double *prm, const double
         return l;
     }
     if (type == ORC_M) return mos1_limit(nd, prm, der, x, x_old, lim_old, lim_new);
+    if (type == ORC_B3) return bsim3_limit(nd, der, x, x_old, lim_old, lim_new);
     return 0;
 }
 
@@ -478,5 +504,25 @@ int dev_seed(uint32_t type, const uint32_t *nd, const double *prm, const double 
         return 1;
     }
     if (type == ORC_M) return mos1_seed(nd, prm, der, x, lim);
+    if (type == ORC_B3) return bsim3_seed(der, lim);
+    return 0;
+}
+
+int orc_dev_stamp(uint32_t type, const double *prm, const double *xloc, double *f, double *J) {
+    if (type >= ORC_NTYPES) return 1;
+    uint32_t nd[ORC_MAX_U];
+    for (uint32_t k = 0; k < ORC_MAX_U; k++) nd[k] = k;
+    double der[ORC_NDER];
+    dev_derive(type, prm, der);
+    sim_t sim;
+    memset(&sim, 0, sizeof(sim));
+    sim.src_scale = 1.0;
+    sim.iteration = 1;
+    devout_t o;
+    dev_eval(type, nd, prm, der, xloc, NULL, NULL, &sim, &o);
+    for (int r = 0; r < ORC_MAX_U; r++) {
+        f[r] = o.f[r];
+        for (int c = 0; c < ORC_MAX_U; c++) J[r * ORC_MAX_U + c] = o.J[r][c];
+    }
     return 0;
 }

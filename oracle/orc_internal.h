@@ -100,7 +100,7 @@ typedef struct {
     int nlim; /* limited images per instance */
 } layout_t;
 
-#define ORC_NDER 48 /* derived (bias-independent) values per instance */
+#define ORC_NDER 96 /* derived (bias-independent) values per instance */
 
 typedef struct {
     double f[ORC_MAX_U];
@@ -137,6 +137,11 @@ double source_value(const double *p, const sim_t *sim);
 void mos1_derive(const double *prm, double *der);
 void mos1_eval(const uint32_t *nd, const double *prm, const double *der, const double *x,
                const double *lim, const double *st, const sim_t *sim, devout_t *o);
+void bsim3_derive(const double *prm, double *der);
+void bsim3_eval(const uint32_t *nd, const double *der, const double *x, const double *lim, devout_t *o);
+int bsim3_limit(const uint32_t *nd, const double *der, const double *x, const double *x_old,
+                const double *lim_old, double *lim_new);
+int bsim3_seed(const double *der, double *lim);
 int mos1_limit(const uint32_t *nd, const double *prm, const double *der, const double *x,
                const double *x_old, const double *lim_old, double *lim_new);
 int mos1_seed(const uint32_t *nd, const double *prm, const double *der, const double *x, double *lim);

@@ -39,6 +39,13 @@ FIXTURES = [
     "dc/device_mos1_pmos",
     "dc/device_mos1_subthreshold",
     "dc/bench_sweep_cmos_inv_sizing",
+    # BSIM3v3 DC core (LEVEL 49)
+    "dc/device_bsim3_transfer",
+    "dc/device_bsim3_output",
+    "dc/device_bsim3_body_effect",
+    "dc/device_bsim3_pmos",
+    "dc/device_bsim3_temp",
+    "op/device_bsim3",
     # transients: RC networks and MOS1 under PULSE sources
     "tran/bench_tran_rc_pulse",
     "tran/bench_medium_rc_ladder_50",

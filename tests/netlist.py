@@ -191,7 +191,14 @@ class Deck:
             elif kind == "m":
                 kindm, prm = self.models[t[5].lower()]
                 prm = dict(prm)
-                prm.pop("level", None)
+                level = prm.pop("level", 1.0)
+                if level in (8.0, 49.0):  # BSIM3v3
+                    prm.pop("version", None)
+                    prm.setdefault("tnom", tnom)
+                    prm["type"] = 1.0 if kindm == "nmos" else -1.0
+                    prm.update(_kv(t[6:]))
+                    c.B3(name, t[1], t[2], t[3], t[4], **prm)
+                    continue
                 prm.setdefault("tnom", tnom)
                 prm["type"] = 1.0 if kindm == "nmos" else -1.0
                 prm.update(_kv(t[6:]))
