@@ -20,6 +20,7 @@ SOURCES = [
     "csrc/host/schedule.cpp",
     "csrc/host/records.cpp",
     "csrc/host/api.cpp",
+    "csrc/host/lu_jit.cpp",
     "csrc/kernels/newton.cu",
     "csrc/kernels/mlp.cu",
     "csrc/host/mlp_host.cu",
@@ -51,7 +52,7 @@ def build(force=False, verbose=False):
     cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3",
            "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
            "-Xptxas", "-v" if verbose else "-O3",
-           "-shared", "-o", LIB] + sources() + ["-lcudart"]
+           "-shared", "-o", LIB] + sources() + ["-lcudart", "-ldl"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)

@@ -18,6 +18,7 @@
 
 #include "../../../include/espice_lanes.h"
 #include "../kernels/launch.h"
+#include "lu_jit.hpp"
 #include "records.hpp"
 #include "schedule.hpp"
 #include "sparse.hpp"
@@ -236,6 +237,9 @@ struct esl_ctx {
   DevBuf d_amap, d_fill, d_prog, d_l_scaled, d_pinv, d_q, d_seq, d_sweep_values, d_meas, d_next_lane;
   uint32_t n_seq_a = 0, n_seq = 0, seq_warps = 0;  // lane-interleaved op list
   uint32_t n_seq_f = 0, mixed_warps = 0;            // its forward-only tail, the mixed kernel's warps
+  std::vector<Op> h_seq;                             // the op list, host copy (the compiled LU's input)
+  LuJitKernels lu_jit;                               // the tape-compiled lane LU of the current tape
+  int lu_jit_state = 0;                              // 0 not built, 1 built, -1 failed
   DevBuf d_row_ptr, d_row_slot, d_row_col;
   DevBuf d_group_topo, d_group_lanes, d_group_cta_ctx, d_group_cta_first, d_group_lpb;  // a group launch's tables
   DevBuf d_rec, d_lim, d_lim_active, d_status, d_iters, d_flags, d_limit, d_a_vals, d_rhs, d_dx,
@@ -616,6 +620,45 @@ GatherProgram build_companion_program(const esl_ctx* ctx, const Programs& P, uin
   return K;
 }
 
+// The sequential op list of the lane-interleaved kernels: the programs'
+// real ops in row order (padding writes the sink, nv - 1), then a copy of
+// program A's forward-solve ops (the mixed kernel's correction solves).
+std::vector<Op> lane_sequence(const Programs& P, uint32_t& n_a, uint32_t& n_all, uint32_t& n_f) {
+  std::vector<Op> seq;
+  for (const Op& o : P.a_ops)
+    if ((o.w0 & 0x0fffffffu) != P.nv - 1) seq.push_back(o);
+  n_a = uint32_t(seq.size());
+  for (const Op& o : P.b_ops)
+    if ((o.w0 & 0x0fffffffu) != P.nv - 1) seq.push_back(o);
+  n_all = uint32_t(seq.size());
+  for (uint32_t k = 0; k < n_a; ++k)
+    if ((seq[k].w0 >> 28) == kOpSubNz) seq.push_back(seq[k]);
+  n_f = uint32_t(seq.size()) - n_all;
+  return seq;
+}
+
+// The compiled lane LU's source for a factored lead tape.
+std::string compiled_lu_source(uint32_t nnz, const SparseLu& lu, const Programs& P, const std::vector<Op>& seq,
+                               uint32_t n_a, uint32_t n_all) {
+  LuJitInput in;
+  in.n = P.n;
+  in.nnz = nnz;
+  in.nu = P.nu;
+  in.nl = P.nl;
+  in.ntv = P.ntv;
+  in.nv = P.nv;
+  in.amap = &P.amap;
+  in.fill = &P.fill;
+  std::vector<uint32_t> pinv(lu.pinv.begin(), lu.pinv.begin() + P.n);
+  in.pinv = &pinv;
+  in.qcol = &lu.q;
+  in.l_scaled = &P.l_scaled;
+  in.seq = &seq;
+  in.n_seq_a = n_a;
+  in.n_seq = n_all;
+  return lu_jit_source(in);
+}
+
 // The lead lane's pivot tape, compiled and uploaded.
 int32_t upload_tape(esl_ctx* ctx) {
   cudaStream_t s = ctx->stream;
@@ -691,17 +734,11 @@ int32_t upload_tape(esl_ctx* ctx) {
   // The sequential op list of the lane-interleaved kernel: the programs'
   // real ops in row order (padding writes the sink, nv - 1).
   {
-    std::vector<Op> seq;
-    for (const Op& o : P.a_ops)
-      if ((o.w0 & 0x0fffffffu) != P.nv - 1) seq.push_back(o);
-    ctx->n_seq_a = uint32_t(seq.size());
-    for (const Op& o : P.b_ops)
-      if ((o.w0 & 0x0fffffffu) != P.nv - 1) seq.push_back(o);
-    ctx->n_seq = uint32_t(seq.size());
-    for (uint32_t k = 0; k < ctx->n_seq_a; ++k)
-      if ((seq[k].w0 >> 28) == kOpSubNz) seq.push_back(seq[k]);
-    ctx->n_seq_f = uint32_t(seq.size()) - ctx->n_seq;
+    std::vector<Op> seq = lane_sequence(P, ctx->n_seq_a, ctx->n_seq, ctx->n_seq_f);
     ESL_CUDA(upload(ctx->d_seq, seq, s));
+    ctx->h_seq = seq;
+    lu_jit_release(ctx->lu_jit);  // a new tape needs its own compiled LU
+    ctx->lu_jit_state = 0;
     ctx->mixed_warps = 0;
     for (uint32_t w = 8; w >= 1; --w)
       if (lu_lanes_mixed_smem(T, ctx->n_seq + ctx->n_seq_f, w) <= room) {
@@ -888,6 +925,7 @@ int32_t esl_destroy(esl_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  lu_jit_release(ctx->lu_jit);
   cudaStream_t s = ctx->stream;
   delete ctx;
   if (s) cudaStreamDestroy(s);
@@ -1505,6 +1543,32 @@ int32_t esl_compile_tape(uint32_t n, const uint32_t* col_ptr, const uint32_t* ro
   return ESL_OK;
 }
 
+int32_t esl_lu_compiled_source(uint32_t n, const uint32_t* col_ptr, const uint32_t* row_idx, const double* lead,
+                               char* buf, size_t cap, size_t* len) {
+  if (!col_ptr || !row_idx || !lead || !len || n == 0) return ESL_INVALID_ARGUMENT;
+  Csc pat;
+  pat.n = n;
+  pat.col_ptr.assign(col_ptr, col_ptr + n + 1);
+  pat.row_idx.assign(row_idx, row_idx + col_ptr[n]);
+  SparseLu lu;
+  lu.init(&pat, order_columns(pat));
+  lu.fill_cap = kRepivotFillCap;
+  lu.keep_min = kGrowthLimit;
+  if (!lu.factor(lead, kPivotTol)) return ESL_NOT_ELIGIBLE;
+  Programs P = compile_tape(lu);
+  if (P.has_void) return ESL_NOT_ELIGIBLE;
+  uint32_t n_a = 0, n_all = 0, n_f = 0;
+  const std::vector<Op> seq = lane_sequence(P, n_a, n_all, n_f);
+  const std::string src = compiled_lu_source(col_ptr[n], lu, P, seq, n_a, n_all);
+  *len = src.size();
+  if (buf && cap > 0) {
+    const size_t k = std::min(cap - 1, src.size());
+    std::memcpy(buf, src.data(), k);
+    buf[k] = '\0';
+  }
+  return ESL_OK;
+}
+
 int32_t esl_tape(const esl_ctx* ctx, uint32_t* q, uint32_t* pinv, uint32_t* counts) {
   if (!ctx || !ctx->have_tape) return ESL_INVALID_ARGUMENT;
   const uint32_t n = ctx->pat.n;
@@ -1535,6 +1599,40 @@ int32_t esl_lu_lanes_device(esl_ctx* ctx, const double* lead, uint32_t n_lanes, 
   ESL_CUDA(cudaEventSynchronize(ctx->ev1));
   if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
   return ESL_OK;
+}
+
+// Tapes beyond this many ops compile slowly and gain nothing over the
+// interpreted kernel (their lanes no longer fit registers either).
+constexpr uint32_t kLuJitMaxOps = 60000;
+
+int32_t esl_lu_lanes_compiled_device(esl_ctx* ctx, const double* lead, uint32_t n_lanes, const double* d_a,
+                                     const double* d_rhs, double* d_dx, uint8_t* d_bad, double* d_tv, float* ms) {
+  if (!ctx || !d_a || !d_rhs || !d_dx || !d_bad || n_lanes == 0) return ESL_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  if (!ctx->have_tape) {
+    if (!lead) return ESL_INVALID_ARGUMENT;
+    if (int32_t rc = build_tape_from(ctx, lead)) return rc;
+  }
+  if (ctx->lu_jit_state == 0) {
+    ctx->lu_jit_state = -1;
+    if (ctx->n_seq > kLuJitMaxOps) return ctx->fail(ESL_NOT_ELIGIBLE, "the tape is too long to compile");
+    const std::string src =
+        compiled_lu_source(ctx->topo.nnz, ctx->lead, ctx->prog, ctx->h_seq, ctx->n_seq_a, ctx->n_seq);
+    if (!lu_jit_build(src, ctx->lu_jit))
+      return ctx->fail(ESL_NOT_ELIGIBLE, "compiling the tape failed: " + ctx->lu_jit.log);
+    ctx->lu_jit_state = 1;
+  }
+  if (ctx->lu_jit_state < 0) return ctx->fail(ESL_NOT_ELIGIBLE, "the tape could not be compiled");
+  ESL_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  ESL_CUDA(lu_jit_launch(ctx->lu_jit, n_lanes, d_a, d_rhs, d_tv, d_dx, d_bad, ctx->stream));
+  ESL_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  ESL_CUDA(cudaEventSynchronize(ctx->ev1));
+  if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
+  return ESL_OK;
+}
+
+const char* esl_lu_compiled_log(const esl_ctx* ctx) {
+  return ctx && ctx->lu_jit_state == 1 ? ctx->lu_jit.log.c_str() : "";
 }
 
 int32_t esl_lu_lanes_mixed_device(esl_ctx* ctx, const double* lead, uint32_t n_lanes, const double* d_a,

@@ -318,6 +318,27 @@ int32_t esl_lu_replay_device(esl_ctx *ctx, const double *lead, uint32_t n_lanes,
 int32_t esl_lu_lanes_device(esl_ctx *ctx, const double *lead, uint32_t n_lanes, const double *d_a,
                             const double *d_rhs, double *d_dx, uint8_t *d_bad, double *d_tv, float *ms);
 
+/* esl_lu_lanes_device with the tape compiled into code: on its first call
+ * the lead tape becomes one straight-line sm_100a kernel (each op one
+ * statement on values held in registers, A and rhs read at first use, tape
+ * values and dx written after their last update), built with NVRTC and
+ * kept for the context's tape. Same arguments and results, bitwise;
+ * ESL_NOT_ELIGIBLE when NVRTC is missing or the tape is too long to
+ * compile (the interpreted esl_lu_lanes_device serves it). */
+int32_t esl_lu_lanes_compiled_device(esl_ctx *ctx, const double *lead, uint32_t n_lanes,
+                                     const double *d_a, const double *d_rhs, double *d_dx,
+                                     uint8_t *d_bad, double *d_tv, float *ms);
+
+/* Host-only: the CUDA source esl_lu_lanes_compiled_device compiles for the
+ * tape of `lead` on this pattern (NUL-terminated in buf when cap > 0; *len
+ * = its length without the NUL). */
+int32_t esl_lu_compiled_source(uint32_t n, const uint32_t *col_ptr, const uint32_t *row_idx,
+                               const double *lead, char *buf, size_t cap, size_t *len);
+
+/* The compiler's log of the context's compiled LU (ptxas register and spill
+ * lines), "" before the first esl_lu_lanes_compiled_device call. */
+const char *esl_lu_compiled_log(const esl_ctx *ctx);
+
 /* esl_lu_lanes_device in mixed precision: the refactor and the triangular
  * solves in FP32 on the same tape, then FP64 iterative refinement (residual
  * -rhs - A dx in FP64 from the FP64 planes, corrections solved on the FP32

@@ -136,6 +136,62 @@ def test_lu_lanes_kernel_bitwise(deck, seed):
     ctx.close()
 
 
+@pytest.mark.parametrize("deck,seed", [("grid", 0), ("grid", 3), ("ring", 1), ("ring", 2)])
+def test_lu_lanes_compiled_bitwise(deck, seed):
+    """The tape compiled into code (esl_lu_lanes_compiled_device): bitwise
+    the oracle's replay and the interpreted lane kernel, peel verdicts
+    included, on a lane count that is not a multiple of the CTA."""
+    torch = _torch()
+    fr = decks.grid_diodes(seed=seed + 1)[0] if deck == "grid" else decks.ring_oscillator(lanes=2)[0]
+    cp, ri = oracle.pattern(fr)
+    n, nnz = fr.n, len(ri)
+    rng = np.random.default_rng(seed)
+    lead = rng.uniform(0.5, 2.0, nnz) * np.where(rng.random(nnz) < 0.5, 1, -1)
+    diag = np.array([np.searchsorted(ri[cp[j]:cp[j + 1]], j) + cp[j] for j in range(n)])
+    lead[diag] += 8.0
+    n_lanes = 333
+    vals = np.stack([lead * rng.uniform(0.8, 1.2, nnz) for _ in range(n_lanes)])
+    vals[0] = lead
+    vals[5, diag[3]] = 0.0
+    vals[7] *= 1e-9
+    rhs = rng.normal(size=(n_lanes, n))
+    ref = oracle.lane_refactor_solve(n, cp, ri, lead, vals, rhs)
+    ctx = lanes.DcLanes(fr)
+    d_a = torch.tensor(vals.T.copy(), dtype=torch.float64, device="cuda")
+    d_r = torch.tensor(rhs.T.copy(), dtype=torch.float64, device="cuda")
+    d_dx = torch.zeros((n, n_lanes), dtype=torch.float64, device="cuda")
+    d_bad = torch.zeros(n_lanes, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    ctx.lu_lanes_compiled(lead, d_a.data_ptr(), d_r.data_ptr(), d_dx.data_ptr(), d_bad.data_ptr(), n_lanes)
+    nu, nl, ntv = ctx.tape_size()
+    d_tv = torch.zeros((ntv, n_lanes), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    ctx.lu_lanes_compiled(lead, d_a.data_ptr(), d_r.data_ptr(), d_dx.data_ptr(), d_bad.data_ptr(), n_lanes,
+                          d_tv.data_ptr())
+    torch.cuda.synchronize()
+    assert "registers" in ctx.lu_compiled_log()
+    bad = d_bad.cpu().numpy()
+    assert np.array_equal(bad, ref["bad"])
+    dx = d_dx.cpu().numpy().T
+    tv = d_tv.cpu().numpy().T
+    good = bad == 0
+    assert good.sum() > n_lanes // 2
+    assert np.array_equal(dx[good].view(np.uint64), ref["dx"][good].view(np.uint64))
+    assert np.array_equal(tv[good, :nu].view(np.uint64), ref["ux"][good].view(np.uint64))
+    assert np.array_equal(tv[good, nu:nu + n].view(np.uint64), ref["udiag"][good].view(np.uint64))
+    assert np.array_equal(tv[good, nu + n:nu + n + nl].view(np.uint64), ref["lx"][good].view(np.uint64))
+    # the interpreted kernel on the same lanes: the same bits everywhere
+    i_dx = torch.zeros_like(d_dx)
+    i_tv = torch.zeros_like(d_tv)
+    i_bad = torch.zeros_like(d_bad)
+    ctx.lu_lanes(lead, d_a.data_ptr(), d_r.data_ptr(), i_dx.data_ptr(), i_bad.data_ptr(), n_lanes, i_tv.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(i_bad, d_bad)
+    assert torch.equal(i_dx[:, torch.tensor(good, device="cuda")].view(torch.int64),
+                       d_dx[:, torch.tensor(good, device="cuda")].view(torch.int64))
+    ctx.close()
+
+
 @pytest.mark.parametrize("deck,seed", [("grid", 0), ("ring", 1)])
 def test_lu_lanes_mixed_refines_to_fp64(deck, seed):
     """FP32 refactor and solves with FP64 refinement: dx within 1e-9 of the
