@@ -237,8 +237,8 @@ struct esl_ctx {
   DevBuf d_amap, d_fill, d_prog, d_l_scaled, d_pinv, d_q, d_seq, d_sweep_values, d_meas, d_next_lane;
   uint32_t n_seq_a = 0, n_seq = 0, seq_warps = 0;  // lane-interleaved op list
   uint32_t n_seq_f = 0, mixed_warps = 0;            // its forward-only tail, the mixed kernel's warps
-  std::vector<Op> h_seq;                             // the op list, host copy (the compiled LU's input)
   LuJitKernels lu_jit;                               // the tape-compiled lane LU of the current tape
+  DevBuf d_lu_scratch;                               // its tape-value plane when the caller passes none
   int lu_jit_state = 0;                              // 0 not built, 1 built, -1 failed
   DevBuf d_row_ptr, d_row_slot, d_row_col;
   DevBuf d_group_topo, d_group_lanes, d_group_cta_ctx, d_group_cta_first, d_group_lpb;  // a group launch's tables
@@ -637,9 +637,15 @@ std::vector<Op> lane_sequence(const Programs& P, uint32_t& n_a, uint32_t& n_all,
   return seq;
 }
 
-// The compiled lane LU's source for a factored lead tape.
-std::string compiled_lu_source(uint32_t nnz, const SparseLu& lu, const Programs& P, const std::vector<Op>& seq,
-                               uint32_t n_a, uint32_t n_all) {
+// The compiled lane LU's source for a factored lead tape: the ops in the
+// replay's own sequential order (column by column; every value's updates in
+// the same order as the warp programs', so the same bits), which keeps
+// fewer values live at once than the programs' level-packed rows.
+std::string compiled_lu_source(uint32_t nnz, const SparseLu& lu, const Programs& P, uint32_t reload_gap = 0) {
+  std::vector<Op> seq = P.a_list;
+  const uint32_t n_a = uint32_t(seq.size());
+  seq.insert(seq.end(), P.b_list.begin(), P.b_list.end());
+  const uint32_t n_all = uint32_t(seq.size());
   LuJitInput in;
   in.n = P.n;
   in.nnz = nnz;
@@ -656,6 +662,7 @@ std::string compiled_lu_source(uint32_t nnz, const SparseLu& lu, const Programs&
   in.seq = &seq;
   in.n_seq_a = n_a;
   in.n_seq = n_all;
+  if (reload_gap) in.reload_gap = reload_gap;
   return lu_jit_source(in);
 }
 
@@ -736,7 +743,6 @@ int32_t upload_tape(esl_ctx* ctx) {
   {
     std::vector<Op> seq = lane_sequence(P, ctx->n_seq_a, ctx->n_seq, ctx->n_seq_f);
     ESL_CUDA(upload(ctx->d_seq, seq, s));
-    ctx->h_seq = seq;
     lu_jit_release(ctx->lu_jit);  // a new tape needs its own compiled LU
     ctx->lu_jit_state = 0;
     ctx->mixed_warps = 0;
@@ -1544,7 +1550,7 @@ int32_t esl_compile_tape(uint32_t n, const uint32_t* col_ptr, const uint32_t* ro
 }
 
 int32_t esl_lu_compiled_source(uint32_t n, const uint32_t* col_ptr, const uint32_t* row_idx, const double* lead,
-                               char* buf, size_t cap, size_t* len) {
+                               uint32_t reload_gap, char* buf, size_t cap, size_t* len) {
   if (!col_ptr || !row_idx || !lead || !len || n == 0) return ESL_INVALID_ARGUMENT;
   Csc pat;
   pat.n = n;
@@ -1557,9 +1563,7 @@ int32_t esl_lu_compiled_source(uint32_t n, const uint32_t* col_ptr, const uint32
   if (!lu.factor(lead, kPivotTol)) return ESL_NOT_ELIGIBLE;
   Programs P = compile_tape(lu);
   if (P.has_void) return ESL_NOT_ELIGIBLE;
-  uint32_t n_a = 0, n_all = 0, n_f = 0;
-  const std::vector<Op> seq = lane_sequence(P, n_a, n_all, n_f);
-  const std::string src = compiled_lu_source(col_ptr[n], lu, P, seq, n_a, n_all);
+  const std::string src = compiled_lu_source(col_ptr[n], lu, P, reload_gap);
   *len = src.size();
   if (buf && cap > 0) {
     const size_t k = std::min(cap - 1, src.size());
@@ -1615,14 +1619,18 @@ int32_t esl_lu_lanes_compiled_device(esl_ctx* ctx, const double* lead, uint32_t 
   }
   if (ctx->lu_jit_state == 0) {
     ctx->lu_jit_state = -1;
-    if (ctx->n_seq > kLuJitMaxOps) return ctx->fail(ESL_NOT_ELIGIBLE, "the tape is too long to compile");
-    const std::string src =
-        compiled_lu_source(ctx->topo.nnz, ctx->lead, ctx->prog, ctx->h_seq, ctx->n_seq_a, ctx->n_seq);
+    if (ctx->prog.a_nops + ctx->prog.b_nops > kLuJitMaxOps)
+      return ctx->fail(ESL_NOT_ELIGIBLE, "the tape is too long to compile");
+    const std::string src = compiled_lu_source(ctx->topo.nnz, ctx->lead, ctx->prog);
     if (!lu_jit_build(src, ctx->lu_jit))
       return ctx->fail(ESL_NOT_ELIGIBLE, "compiling the tape failed: " + ctx->lu_jit.log);
     ctx->lu_jit_state = 1;
   }
   if (ctx->lu_jit_state < 0) return ctx->fail(ESL_NOT_ELIGIBLE, "the tape could not be compiled");
+  if (!d_tv) {
+    ESL_CUDA(ctx->d_lu_scratch.ensure(size_t(ctx->prog.ntv) * n_lanes * 8));
+    d_tv = ctx->d_lu_scratch.as<double>();
+  }
   ESL_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
   ESL_CUDA(lu_jit_launch(ctx->lu_jit, n_lanes, d_a, d_rhs, d_tv, d_dx, d_bad, ctx->stream));
   ESL_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));

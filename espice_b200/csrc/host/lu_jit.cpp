@@ -26,7 +26,12 @@ namespace esl {
 
 namespace {
 
+// 128 threads, at least 4 CTAs per SM: 128 registers a thread, 16 warps
+// per SM. On the B200 this beat the unbounded form (about 240 registers,
+// 8 warps) by 20% on the ring's tape and the grid's, and an L2 prefetch of
+// every A row at the start gained nothing.
 constexpr uint32_t kThreads = 128;
+constexpr uint32_t kMinBlocks = 4;
 
 struct Gen {
   const LuJitInput& in;
@@ -34,39 +39,48 @@ struct Gen {
   std::vector<uint8_t> defined;
   std::vector<int64_t> slot_of;  // tape value -> the last pattern slot that loads it, -1 none
   std::vector<int64_t> row_of;   // y value -> its rhs row, -1 none
-  std::vector<uint8_t> is_fill;
+  std::vector<int64_t> last_ref; // statement of each value's latest reference
+  std::vector<uint8_t> stored;   // written to the tape-value plane (final)
+  int64_t at = 0;                // the current statement
 
   explicit Gen(const LuJitInput& i) : in(i) {
     defined.assign(in.nv, 0);
     slot_of.assign(in.nv, -1);
     row_of.assign(in.nv, -1);
-    is_fill.assign(in.nv, 0);
+    last_ref.assign(in.nv, -1);
+    stored.assign(in.nv, 0);
     for (uint32_t p = 0; p < in.nnz; ++p) slot_of[(*in.amap)[p]] = p;
     for (uint32_t r = 0; r < in.n; ++r) row_of[in.ntv + (*in.pinv)[r]] = r;
-    for (uint32_t f : *in.fill) is_fill[f] = 1;
   }
 
-  // The value's start, emitted at its first use: A, -rhs (y = P(-rhs)), the
-  // constants 0.0 and 1.0, a fill-in zero.
-  void def(uint32_t v) {
-    if (defined[v]) return;
-    defined[v] = 1;
-    os << "  double v" << v << " = ";
-    if (v == in.nv - 2) os << "1.0";
-    else if (v >= in.nv - 3) os << "0.0";
-    else if (slot_of[v] >= 0) os << "__ldg(al + " << slot_of[v] << " * N)";
-    else if (row_of[v] >= 0) os << "-__ldg(rl + " << row_of[v] << " * N)";
-    else os << "0.0";  // fill-in (and an entry no slot or op sets)
-    os << ";\n";
+  // A reference to value v: its start at first use (A, -rhs for y = P(-rhs),
+  // the constants 0.0 and 1.0, a fill-in zero), or, for a final tape value
+  // last touched long ago, a reload from the tape-value plane, so that the
+  // register file holds the values in use and not every value still needed.
+  void use(uint32_t v) {
+    if (!defined[v]) {
+      defined[v] = 1;
+      os << "  double v" << v << " = ";
+      if (v == in.nv - 2) os << "1.0";
+      else if (v >= in.nv - 3) os << "0.0";
+      else if (slot_of[v] >= 0) os << "__ldg(al + " << slot_of[v] << " * N)";
+      else if (row_of[v] >= 0) os << "-__ldg(rl + " << row_of[v] << " * N)";
+      else os << "0.0";  // fill-in (and an entry no slot or op sets)
+      os << ";\n";
+    } else if (stored[v] && at - last_ref[v] > int64_t(in.reload_gap)) {
+      os << "  v" << v << " = __ldcg(tl + " << v << " * N);\n";
+    }
+    last_ref[v] = at;
   }
 
   void op(uint32_t k, const Op& o) {
     const uint32_t kind = o.w0 >> 28, d = o.w0 & 0x0fffffffu, a = o.w1 & 0xffffu, b = o.w1 >> 16;
     if (kind == kOpNop) return;
-    def(a);
-    def(b);
+    ++at;
+    use(a);
+    use(b);
     if (kind == kOpFlop || kind == kOpSubNz) {
-      def(d);
+      use(d);
       if (kind == kOpSubNz) os << "  if (v" << b << " != 0.0)";
       os << "  v" << d << " = __dsub_rn(v" << d << ", __dmul_rn(v" << a << ", v" << b << "));\n";
       return;
@@ -80,6 +94,24 @@ struct Gen {
     } else {
       defined[d] = 1;
       os << "  double v" << d << " = q" << k << ";\n";
+    }
+    last_ref[d] = at;
+  }
+
+  // A tape value is final: out to its plane, then the refactor's peel test
+  // on it (a non-finite U entry, a dead or non-finite pivot, an unscaled L
+  // multiplier past 1 / pivot_tol).
+  void finish(uint32_t v) {
+    if (v >= in.ntv - 1) return;  // the discard entry holds nothing
+    use(v);
+    os << "  tl[" << v << " * N] = v" << v << ";\n";
+    stored[v] = 1;
+    if (v < in.nu) {
+      os << "  bad |= __double_as_longlong(v" << v << " - v" << v << ") != 0;\n";
+    } else if (v < in.nu + in.n) {
+      os << "  bad |= v" << v << " == 0.0 || !(fabs(v" << v << ") < kInf);\n";
+    } else if (!(*in.l_scaled)[v - in.nu - in.n]) {
+      os << "  bad |= !(fabs(v" << v << ") <= 1e3);\n";
     }
   }
 };
@@ -100,48 +132,25 @@ std::string lu_jit_source(const LuJitInput& in) {
   std::ostringstream& os = g.os;
   os << "// generated: the lane refactor + solve of one pivot tape (" << in.n << " unknowns, " << in.ntv
      << " tape values, " << in.n_seq << " ops)\n"
-     << "template <bool kTv>\n"
-     << "__device__ __forceinline__ void body(const double* __restrict__ a, const double* __restrict__ rhs,\n"
-     << "    double* __restrict__ tv, double* __restrict__ dx, unsigned char* __restrict__ bad_out,\n"
-     << "    unsigned n_lanes) {\n"
+     << "extern \"C\" __global__ void __launch_bounds__(" << kThreads << ", " << kMinBlocks << ") lu_tape(\n"
+     << "    const double* __restrict__ a, const double* __restrict__ rhs, double* __restrict__ tv,\n"
+     << "    double* __restrict__ dx, unsigned char* __restrict__ bad_out, unsigned n_lanes) {\n"
      << "  const unsigned lane = blockIdx.x * " << kThreads << "u + threadIdx.x;\n"
      << "  if (lane >= n_lanes) return;\n"
      << "  const size_t N = n_lanes;\n"
      << "  const double* al = a + lane;\n"
      << "  const double* rl = rhs + lane;\n"
+     << "  double* tl = tv + lane;\n"
      << "  const double kInf = __longlong_as_double(0x7ff0000000000000ll);\n"
      << "  bool bad = false;\n";
-  // tape values (U, diagonal, L) are final after program A: each is written
-  // out after its last update there (or at once when program A never writes it)
-  auto store_tv = [&](uint32_t v) {
-    if (v >= in.ntv - 1) return;  // the discard entry holds nothing
-    os << "  if (kTv) tv[" << v << " * N + lane] = v" << v << ";\n";
-  };
+  // tape values (U, diagonal, L) are final after their last update in
+  // program A (at once when program A never writes them)
   for (uint32_t v = 0; v + 1 < in.ntv; ++v)
-    if (last_a[v] < 0) {
-      g.def(v);
-      store_tv(v);
-    }
+    if (last_a[v] < 0) g.finish(v);
   for (uint32_t k = 0; k < in.n_seq_a; ++k) {
     g.op(k, seq[k]);
     const uint32_t d = seq[k].w0 & 0x0fffffffu;
-    if (last_a[d] == int64_t(k) && d < in.ntv) store_tv(d);
-  }
-  // the refactor's peel tests: a non-finite U entry, a dead or non-finite
-  // pivot, an unscaled L multiplier past 1 / pivot_tol
-  for (uint32_t s = 0; s < in.nu; ++s) {
-    g.def(s);
-    os << "  bad |= __double_as_longlong(v" << s << " - v" << s << ") != 0;\n";
-  }
-  for (uint32_t k = 0; k < in.n; ++k) {
-    const uint32_t v = in.nu + k;
-    g.def(v);
-    os << "  bad |= v" << v << " == 0.0 || !(fabs(v" << v << ") < kInf);\n";
-  }
-  for (uint32_t s = 0; s < in.nl; ++s) {
-    const uint32_t v = in.nu + in.n + s;
-    g.def(v);
-    if (!(*in.l_scaled)[s]) os << "  bad |= !(fabs(v" << v << ") <= 1e3);\n";
+    if (last_a[d] == int64_t(k) && d < in.ntv) g.finish(d);
   }
   // dx is final after its last update; a y entry no op writes goes out as loaded
   auto store_dx = [&](uint32_t j) {
@@ -154,17 +163,11 @@ std::string lu_jit_source(const LuJitInput& in) {
   }
   for (uint32_t j = 0; j < in.n; ++j)
     if (last_all[in.ntv + j] < int64_t(in.n_seq_a)) {
-      g.def(in.ntv + j);
+      g.use(in.ntv + j);
       store_dx(j);
     }
   os << "  bad_out[lane] = bad;\n"
-     << "}\n\n"
-     << "extern \"C\" __global__ void __launch_bounds__(" << kThreads << ") lu_tape_tv(const double* a, "
-     << "const double* rhs, double* tv, double* dx, unsigned char* bad, unsigned n_lanes) {\n"
-     << "  body<true>(a, rhs, tv, dx, bad, n_lanes);\n}\n"
-     << "extern \"C\" __global__ void __launch_bounds__(" << kThreads << ") lu_tape(const double* a, "
-     << "const double* rhs, double* tv, double* dx, unsigned char* bad, unsigned n_lanes) {\n"
-     << "  body<false>(a, rhs, tv, dx, bad, n_lanes);\n}\n";
+     << "}\n";
   return os.str();
 }
 
@@ -239,8 +242,7 @@ bool lu_jit_build(const std::string& src, LuJitKernels& out) {
     out.lib = nullptr;
     return false;
   }
-  if (cudaLibraryGetKernel(&out.with_tv, out.lib, "lu_tape_tv") != cudaSuccess ||
-      cudaLibraryGetKernel(&out.without_tv, out.lib, "lu_tape") != cudaSuccess) {
+  if (cudaLibraryGetKernel(&out.kernel, out.lib, "lu_tape") != cudaSuccess) {
     cudaGetLastError();
     out.log += "\ncudaLibraryGetKernel failed";
     lu_jit_release(out);
@@ -252,13 +254,13 @@ bool lu_jit_build(const std::string& src, LuJitKernels& out) {
 void lu_jit_release(LuJitKernels& k) {
   if (k.lib) cudaLibraryUnload(k.lib);
   k.lib = nullptr;
-  k.with_tv = k.without_tv = nullptr;
+  k.kernel = nullptr;
 }
 
 cudaError_t lu_jit_launch(const LuJitKernels& k, uint32_t n_lanes, const double* a, const double* rhs, double* tv,
                           double* dx, uint8_t* bad, cudaStream_t s) {
   void* args[] = {&a, &rhs, &tv, &dx, &bad, &n_lanes};
-  const void* fn = reinterpret_cast<const void*>(tv ? k.with_tv : k.without_tv);
+  const void* fn = reinterpret_cast<const void*>(k.kernel);
   return cudaLaunchKernel(fn, dim3((n_lanes + kThreads - 1) / kThreads), dim3(kThreads), args, 0, s);
 }
 

@@ -23,16 +23,19 @@ struct LuJitInput {
   const std::vector<uint8_t>* l_scaled = nullptr; // per L entry: scaled pivot column
   const std::vector<Op>* seq = nullptr;           // real ops, program A then program B
   uint32_t n_seq_a = 0, n_seq = 0;
+  uint32_t reload_gap = 48;  // a final tape value unused for this many ops is re-read from its plane
 };
 
-// CUDA C++ source of the two kernels `lu_tape_tv` (tape values written) and
-// `lu_tape` (not): one thread per lane over [entry][lane] planes, every tape
-// value a local variable, each op one statement in the programs' order.
+// CUDA C++ source of the kernel `lu_tape`: one thread per lane over
+// [entry][lane] planes, every tape value a local variable, each op one
+// statement in the given order; the tape values go to their plane `tv`
+// (the caller's, or scratch) as they become final and come back from it
+// when their next use is far off.
 std::string lu_jit_source(const LuJitInput& in);
 
 struct LuJitKernels {
   cudaLibrary_t lib = nullptr;
-  cudaKernel_t with_tv = nullptr, without_tv = nullptr;
+  cudaKernel_t kernel = nullptr;
   std::string log;  // NVRTC's log (ptxas register and spill lines included)
 };
 
@@ -43,6 +46,7 @@ struct LuJitKernels {
 bool lu_jit_build(const std::string& src, LuJitKernels& out);
 void lu_jit_release(LuJitKernels& k);
 
+// tv: [ntv][n_lanes], never NULL (the kernel re-reads values from it).
 cudaError_t lu_jit_launch(const LuJitKernels& k, uint32_t n_lanes, const double* a, const double* rhs, double* tv,
                           double* dx, uint8_t* bad, cudaStream_t s);
 

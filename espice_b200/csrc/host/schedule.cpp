@@ -159,6 +159,7 @@ Programs compile_tape(const SparseLu& lu) {
     for (uint32_t q = lu.lp[k]; q < lu.lp[k + 1]; ++q) a.push_back({kOpSubNz, y0 + lu.li[q], lx0 + q, y0 + k});
   }
   P.nv = P.ntv + n + 3;
+  for (const SeqOp& s : a) P.a_list.push_back(encode(s.kind, s.dst, s.a, s.b));
   pack(a, P.nv, P.a_ops, P.a_rows, P.a_levels);
   P.a_nops = uint32_t(a.size());
 
@@ -177,6 +178,7 @@ Programs compile_tape(const SparseLu& lu) {
     b.push_back({kOpDivY, y0 + k, P.nu + k, y0 + k});
     for (uint32_t p = lu.up[k]; p < lu.up[k + 1]; ++p) b.push_back({kOpSubNz, y0 + lu.ui[p], p, y0 + k});
   }
+  for (const SeqOp& s : b) P.b_list.push_back(encode(s.kind, s.dst, s.a, s.b));
   pack(b, P.nv, P.b_ops, P.b_rows, P.b_levels);
   P.b_nops = uint32_t(b.size());
   return P;

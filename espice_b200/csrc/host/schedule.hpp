@@ -31,6 +31,7 @@ struct Programs {
   std::vector<uint32_t> fill;      // tape values no pattern slot writes
   std::vector<Op> a_ops;           // rows x 32: refactor + forward solve
   std::vector<Op> b_ops;           // rows x 32: back solve
+  std::vector<Op> a_list, b_list;  // the same ops in the replay's sequential order (column by column)
   uint32_t a_rows = 0, b_rows = 0, a_levels = 0, b_levels = 0;  // levels: longest chain
   uint32_t a_nops = 0, b_nops = 0; // real ops (no padding)
   std::vector<uint8_t> l_scaled;   // per L entry: its column took the row-scaled pivot

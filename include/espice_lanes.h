@@ -321,8 +321,10 @@ int32_t esl_lu_lanes_device(esl_ctx *ctx, const double *lead, uint32_t n_lanes, 
 /* esl_lu_lanes_device with the tape compiled into code: on its first call
  * the lead tape becomes one straight-line sm_100a kernel (each op one
  * statement on values held in registers, A and rhs read at first use, tape
- * values and dx written after their last update), built with NVRTC and
- * kept for the context's tape. Same arguments and results, bitwise;
+ * values written to their plane as they become final and re-read from it
+ * when next needed far off, dx written after its last update), built with
+ * NVRTC and kept for the context's tape. With d_tv NULL a context-owned
+ * plane stands in. Same arguments and results, bitwise;
  * ESL_NOT_ELIGIBLE when NVRTC is missing or the tape is too long to
  * compile (the interpreted esl_lu_lanes_device serves it). */
 int32_t esl_lu_lanes_compiled_device(esl_ctx *ctx, const double *lead, uint32_t n_lanes,
@@ -331,9 +333,12 @@ int32_t esl_lu_lanes_compiled_device(esl_ctx *ctx, const double *lead, uint32_t 
 
 /* Host-only: the CUDA source esl_lu_lanes_compiled_device compiles for the
  * tape of `lead` on this pattern (NUL-terminated in buf when cap > 0; *len
- * = its length without the NUL). */
+ * = its length without the NUL). reload_gap: a final tape value unused for
+ * this many ops is re-read from its plane instead of held (0: the library's
+ * default, 48). */
 int32_t esl_lu_compiled_source(uint32_t n, const uint32_t *col_ptr, const uint32_t *row_idx,
-                               const double *lead, char *buf, size_t cap, size_t *len);
+                               const double *lead, uint32_t reload_gap, char *buf, size_t cap,
+                               size_t *len);
 
 /* The compiler's log of the context's compiled LU (ptxas register and spill
  * lines), "" before the first esl_lu_lanes_compiled_device call. */

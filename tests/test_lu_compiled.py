@@ -34,6 +34,7 @@ static inline double __ddiv_rn(double a, double b) { return a / b; }
 static inline double __dmul_rn(double a, double b) { return a * b; }
 static inline double __dsub_rn(double a, double b) { return a - b; }
 static inline double __ldg(const double* p) { return *p; }
+static inline double __ldcg(const double* p) { return *p; }
 static inline double __longlong_as_double(long long x) { double d; std::memcpy(&d, &x, 8); return d; }
 static inline long long __double_as_longlong(double d) { long long x; std::memcpy(&x, &d, 8); return x; }
 using std::fabs;
@@ -45,7 +46,7 @@ extern "C" void run_lanes(const double* a, const double* rhs, double* tv, double
   for (unsigned l = 0; l < n_lanes; ++l) {
     blockIdx.x = l / 128;
     threadIdx.x = l % 128;
-    lu_tape_tv(a, rhs, tv, dx, bad, n_lanes);
+    lu_tape(a, rhs, tv, dx, bad, n_lanes);
   }
 }
 """
@@ -67,11 +68,14 @@ def _case(deck, seed, n_lanes=67):
     return fr, cp, ri, lead, vals, rhs
 
 
-@pytest.mark.parametrize("deck,seed", [("ring", 1), ("ring", 2), ("grid", 0)])
-def test_compiled_source_matches_oracle_replay(deck, seed, tmp_path):
+@pytest.mark.parametrize("deck,seed,gap", [("ring", 1, 0), ("ring", 2, 0), ("grid", 0, 0), ("ring", 1, 4),
+                                           ("grid", 3, 8)])
+def test_compiled_source_matches_oracle_replay(deck, seed, gap, tmp_path):
+    """gap: the reload distance (0: the library's default); short ones make
+    most reads come back from the tape-value plane."""
     fr, cp, ri, lead, vals, rhs = _case(deck, seed)
     n, n_lanes = fr.n, vals.shape[0]
-    src = lanes.lu_compiled_source(n, cp, ri, lead)
+    src = lanes.lu_compiled_source(n, cp, ri, lead, reload_gap=gap)
     cpp = tmp_path / "lu_tape.cpp"
     cpp.write_text(PRELUDE + src + DRIVER)
     so = tmp_path / "lu_tape.so"
