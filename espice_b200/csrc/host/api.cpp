@@ -641,7 +641,7 @@ std::vector<Op> lane_sequence(const Programs& P, uint32_t& n_a, uint32_t& n_all,
 // replay's own sequential order (column by column; every value's updates in
 // the same order as the warp programs', so the same bits), which keeps
 // fewer values live at once than the programs' level-packed rows.
-std::string compiled_lu_source(uint32_t nnz, const SparseLu& lu, const Programs& P, uint32_t reload_gap = 0) {
+std::string compiled_lu_source(uint32_t nnz, const SparseLu& lu, const Programs& P, uint32_t resident = 0) {
   std::vector<Op> seq = P.a_list;
   const uint32_t n_a = uint32_t(seq.size());
   seq.insert(seq.end(), P.b_list.begin(), P.b_list.end());
@@ -662,7 +662,7 @@ std::string compiled_lu_source(uint32_t nnz, const SparseLu& lu, const Programs&
   in.seq = &seq;
   in.n_seq_a = n_a;
   in.n_seq = n_all;
-  if (reload_gap) in.reload_gap = reload_gap;
+  if (resident) in.resident_values = resident;
   return lu_jit_source(in);
 }
 
@@ -1550,7 +1550,7 @@ int32_t esl_compile_tape(uint32_t n, const uint32_t* col_ptr, const uint32_t* ro
 }
 
 int32_t esl_lu_compiled_source(uint32_t n, const uint32_t* col_ptr, const uint32_t* row_idx, const double* lead,
-                               uint32_t reload_gap, char* buf, size_t cap, size_t* len) {
+                               uint32_t resident, char* buf, size_t cap, size_t* len) {
   if (!col_ptr || !row_idx || !lead || !len || n == 0) return ESL_INVALID_ARGUMENT;
   Csc pat;
   pat.n = n;
@@ -1563,7 +1563,7 @@ int32_t esl_lu_compiled_source(uint32_t n, const uint32_t* col_ptr, const uint32
   if (!lu.factor(lead, kPivotTol)) return ESL_NOT_ELIGIBLE;
   Programs P = compile_tape(lu);
   if (P.has_void) return ESL_NOT_ELIGIBLE;
-  const std::string src = compiled_lu_source(col_ptr[n], lu, P, reload_gap);
+  const std::string src = compiled_lu_source(col_ptr[n], lu, P, resident);
   *len = src.size();
   if (buf && cap > 0) {
     const size_t k = std::min(cap - 1, src.size());

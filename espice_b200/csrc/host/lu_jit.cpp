@@ -16,6 +16,8 @@
 
 #include <dlfcn.h>
 
+#include <algorithm>
+
 #include <cstdio>
 #include <mutex>
 #include <sstream>
@@ -32,6 +34,13 @@ namespace {
 // every A row at the start gained nothing.
 constexpr uint32_t kThreads = 128;
 constexpr uint32_t kMinBlocks = 4;
+// The A and rhs entries a lane reads arrive through shared memory in
+// stages of kStage entries in first-use order, two stages in flight
+// (cp.async into a per-thread double buffer: 2 x 24 x 128 x 8 B = 48 KB a
+// CTA), so each warp keeps dozens of loads outstanding without holding
+// registers for them: the kernel was bound by load latency, with about 2.4
+// MB in flight over the GPU at 16 warps per SM.
+constexpr uint32_t kStage = 24;
 
 struct Gen {
   const LuJitInput& in;
@@ -39,50 +48,149 @@ struct Gen {
   std::vector<uint8_t> defined;
   std::vector<int64_t> slot_of;  // tape value -> the last pattern slot that loads it, -1 none
   std::vector<int64_t> row_of;   // y value -> its rhs row, -1 none
-  std::vector<int64_t> last_ref; // statement of each value's latest reference
-  std::vector<uint8_t> stored;   // written to the tape-value plane (final)
-  int64_t at = 0;                // the current statement
+  // Register residency. Every value has a home in HBM: a tape value its
+  // entry of the tape-value plane, y[j] its dx entry (the final dx store
+  // overwrites it). The first pass records every use of every value; the
+  // second keeps a model of which values sit in registers. Over the budget,
+  // the value whose next use is farthest ahead leaves (Belady): written home
+  // first when its home is stale, re-read at its next use. A tape value is
+  // written home once anyway when final, so most evictions cost no store.
+  std::vector<std::vector<uint32_t>> uses;
+  std::vector<uint32_t> next;
+  std::vector<uint8_t> resident, clean;
+  uint32_t uc = 0, n_res = 0;
+  // staging: the loaded values (A or rhs) in first-use order, recorded by the
+  // first pass; each value's position in it; the stage being read
+  bool record = true;
+  std::vector<uint32_t> order;
+  std::vector<int64_t> pos;
+  int64_t cur_stage = -1;
+  uint32_t n_stages = 0;
 
   explicit Gen(const LuJitInput& i) : in(i) {
     defined.assign(in.nv, 0);
     slot_of.assign(in.nv, -1);
     row_of.assign(in.nv, -1);
-    last_ref.assign(in.nv, -1);
-    stored.assign(in.nv, 0);
+    pos.assign(in.nv, -1);
+    uses.assign(in.nv, {});
+    next.assign(in.nv, 0);
+    resident.assign(in.nv, 0);
+    clean.assign(in.nv, 0);
     for (uint32_t p = 0; p < in.nnz; ++p) slot_of[(*in.amap)[p]] = p;
     for (uint32_t r = 0; r < in.n; ++r) row_of[in.ntv + (*in.pinv)[r]] = r;
   }
 
-  // A reference to value v: its start at first use (A, -rhs for y = P(-rhs),
-  // the constants 0.0 and 1.0, a fill-in zero), or, for a final tape value
-  // last touched long ago, a reload from the tape-value plane, so that the
-  // register file holds the values in use and not every value still needed.
+  static constexpr uint32_t kNever = 0xffffffffu;
+  uint32_t next_use(uint32_t v) const { return next[v] < uses[v].size() ? uses[v][next[v]] : kNever; }
+  bool constant(uint32_t v) const { return v >= in.nv - 3; }
+
+  // The home of value v, as an expression for this lane.
+  std::string home(uint32_t v) const {
+    std::ostringstream h;
+    if (v < in.ntv) h << "tl[" << v << " * N]";
+    else h << "dx[" << (*in.qcol)[v - in.ntv] << " * N + lane]";
+    return h.str();
+  }
+
+  // The residency model's bookkeeping for one reference at position u.
+  void touch(uint32_t v) {
+    if (!resident[v]) {
+      resident[v] = 1;
+      ++n_res;
+    }
+    ++next[v];
+    if (next_use(v) == kNever) {  // dead after this reference
+      resident[v] = 0;
+      --n_res;
+    }
+  }
+
+  // A read of value v: its start at first use (A, -rhs for y = P(-rhs), the
+  // constants 0.0 and 1.0, a fill-in zero), or a reload from its home when
+  // the model let it go.
   void use(uint32_t v) {
+    const uint32_t u = uc++;
+    if (record) {
+      uses[v].push_back(u);
+    } else if (!constant(v)) {
+      if (defined[v] && !resident[v]) os << "  v" << v << " = __ldcg(&" << home(v) << ");\n";
+      touch(v);
+    }
     if (!defined[v]) {
       defined[v] = 1;
+      const bool loaded = !constant(v) && (slot_of[v] >= 0 || row_of[v] >= 0);
+      if (loaded && record) {
+        pos[v] = int64_t(order.size());
+        order.push_back(v);
+      }
+      if (loaded && !record) enter_stage(uint32_t(pos[v] / kStage));
       os << "  double v" << v << " = ";
       if (v == in.nv - 2) os << "1.0";
-      else if (v >= in.nv - 3) os << "0.0";
-      else if (slot_of[v] >= 0) os << "__ldg(al + " << slot_of[v] << " * N)";
-      else if (row_of[v] >= 0) os << "-__ldg(rl + " << row_of[v] << " * N)";
+      else if (constant(v)) os << "0.0";
+      else if (loaded)
+        os << (slot_of[v] >= 0 ? "" : "-") << "stage_read(sb, " << (pos[v] / kStage) % 2 << ", " << pos[v] % kStage
+           << ")";
       else os << "0.0";  // fill-in (and an entry no slot or op sets)
       os << ";\n";
-    } else if (stored[v] && at - last_ref[v] > int64_t(in.reload_gap)) {
-      os << "  v" << v << " = __ldcg(tl + " << v << " * N);\n";
     }
-    last_ref[v] = at;
+  }
+
+  // A write of value d by the current op (its home is now stale).
+  void wrote(uint32_t d) {
+    clean[d] = 0;
+    if (record) return;
+  }
+
+  // After each op: back under the register budget.
+  void settle() {
+    if (record) return;
+    while (n_res > in.resident_values) {
+      uint32_t best = kNever, far = 0;
+      for (uint32_t v = 0; v < in.nv - 3; ++v)
+        if (resident[v] && next_use(v) >= far && (next_use(v) > far || clean[v])) {
+          far = next_use(v);
+          best = v;
+        }
+      if (best == kNever) return;
+      if (!clean[best]) {
+        os << "  " << home(best) << " = v" << best << ";\n";
+        clean[best] = 1;
+      }
+      resident[best] = 0;
+      --n_res;
+    }
+  }
+
+  // Stage t's copies into buffer t % 2, as one commit group.
+  void issue(uint32_t t) {
+    for (uint32_t j = t * kStage; j < std::min<uint32_t>(uint32_t(order.size()), (t + 1) * kStage); ++j) {
+      const uint32_t v = order[j];
+      os << "  stage_copy(sb, " << t % 2 << ", " << j % kStage << ", ";
+      if (slot_of[v] >= 0) os << "al + " << slot_of[v] << " * N);\n";
+      else os << "rl + " << row_of[v] << " * N);\n";
+    }
+    os << "  stage_commit();\n";
+  }
+
+  // The first read of stage s: stage s - 1 is consumed, so stage s + 1 goes
+  // into its buffer; then wait until stage s has landed.
+  void enter_stage(uint32_t s) {
+    if (int64_t(s) == cur_stage) return;
+    cur_stage = s;
+    if (s >= 1 && s + 1 < n_stages) issue(s + 1);
+    os << "  stage_wait<" << (s + 1 < n_stages ? 1 : 0) << ">();\n";
   }
 
   void op(uint32_t k, const Op& o) {
     const uint32_t kind = o.w0 >> 28, d = o.w0 & 0x0fffffffu, a = o.w1 & 0xffffu, b = o.w1 >> 16;
     if (kind == kOpNop) return;
-    ++at;
     use(a);
     use(b);
     if (kind == kOpFlop || kind == kOpSubNz) {
       use(d);
       if (kind == kOpSubNz) os << "  if (v" << b << " != 0.0)";
       os << "  v" << d << " = __dsub_rn(v" << d << ", __dmul_rn(v" << a << ", v" << b << "));\n";
+      wrote(d);
       return;
     }
     os << "  const double q" << k << " = __ddiv_rn(v" << b << ", v" << a << ");\n";
@@ -95,7 +203,12 @@ struct Gen {
       defined[d] = 1;
       os << "  double v" << d << " = q" << k << ";\n";
     }
-    last_ref[d] = at;
+    // a division's destination is a new value in a register: counted as a
+    // reference, with no load
+    const uint32_t u = uc++;
+    if (record) uses[d].push_back(u);
+    else touch(d);
+    wrote(d);
   }
 
   // A tape value is final: out to its plane, then the refactor's peel test
@@ -104,8 +217,8 @@ struct Gen {
   void finish(uint32_t v) {
     if (v >= in.ntv - 1) return;  // the discard entry holds nothing
     use(v);
-    os << "  tl[" << v << " * N] = v" << v << ";\n";
-    stored[v] = 1;
+    os << "  " << home(v) << " = v" << v << ";\n";
+    clean[v] = 1;
     if (v < in.nu) {
       os << "  bad |= __double_as_longlong(v" << v << " - v" << v << ") != 0;\n";
     } else if (v < in.nu + in.n) {
@@ -114,12 +227,18 @@ struct Gen {
       os << "  bad |= !(fabs(v" << v << ") <= 1e3);\n";
     }
   }
+
+  // y[j] is final: out to dx (its home).
+  void store_dx(uint32_t j) {
+    use(in.ntv + j);
+    os << "  " << home(in.ntv + j) << " = v" << (in.ntv + j) << ";\n";
+    clean[in.ntv + j] = 1;
+  }
 };
 
 }  // namespace
 
 std::string lu_jit_source(const LuJitInput& in) {
-  Gen g(in);
   const std::vector<Op>& seq = *in.seq;
   // the last op that writes each value, per program
   std::vector<int64_t> last_a(in.nv, -1), last_all(in.nv, -1);
@@ -129,43 +248,78 @@ std::string lu_jit_source(const LuJitInput& in) {
     if (k < in.n_seq_a) last_a[d] = k;
     last_all[d] = k;
   }
+  // The op stream: tape values (U, diagonal, L) are final after their last
+  // update in program A (at once when program A never writes them); dx is
+  // final after its last update (a y entry no op writes goes out as loaded).
+  auto walk = [&](Gen& g) {
+    for (uint32_t v = 0; v + 1 < in.ntv; ++v)
+      if (last_a[v] < 0) {
+        g.finish(v);
+        g.settle();
+      }
+    for (uint32_t k = 0; k < in.n_seq_a; ++k) {
+      g.op(k, seq[k]);
+      const uint32_t d = seq[k].w0 & 0x0fffffffu;
+      if (last_a[d] == int64_t(k) && d < in.ntv) g.finish(d);
+      g.settle();
+    }
+    for (uint32_t k = in.n_seq_a; k < in.n_seq; ++k) {
+      g.op(k, seq[k]);
+      const uint32_t d = seq[k].w0 & 0x0fffffffu;
+      if (d >= in.ntv && d < in.ntv + in.n && last_all[d] == int64_t(k)) g.store_dx(d - in.ntv);
+      g.settle();
+    }
+    for (uint32_t j = 0; j < in.n; ++j)
+      if (last_all[in.ntv + j] < int64_t(in.n_seq_a)) {
+        g.store_dx(j);
+        g.settle();
+      }
+  };
+  // pass 1: the loaded values' first-use order
+  Gen first(in);
+  walk(first);
+  Gen g(in);
+  g.record = false;
+  g.order = first.order;
+  g.pos = first.pos;
+  g.uses = first.uses;
+  g.n_stages = uint32_t((g.order.size() + kStage - 1) / kStage);
   std::ostringstream& os = g.os;
   os << "// generated: the lane refactor + solve of one pivot tape (" << in.n << " unknowns, " << in.ntv
      << " tape values, " << in.n_seq << " ops)\n"
+     << "#ifndef ESL_LU_HOST_EMULATION\n"
+     << "__device__ __forceinline__ void stage_copy(unsigned sb, unsigned b, unsigned i, const double* src) {\n"
+     << "  asm volatile(\"cp.async.ca.shared.global [%0], [%1], 8;\" :: \"r\"(sb + (b * " << kStage << "u + i) * "
+     << kThreads * 8 << "u), \"l\"(src) : \"memory\");\n"
+     << "}\n"
+     << "__device__ __forceinline__ void stage_commit() { asm volatile(\"cp.async.commit_group;\" ::: \"memory\"); }\n"
+     << "template <int P> __device__ __forceinline__ void stage_wait() {\n"
+     << "  asm volatile(\"cp.async.wait_group %0;\" :: \"n\"(P) : \"memory\");\n"
+     << "}\n"
+     << "__device__ __forceinline__ double stage_read(unsigned sb, unsigned b, unsigned i) {\n"
+     << "  double v;\n"
+     << "  asm volatile(\"ld.shared.f64 %0, [%1];\" : \"=d\"(v) : \"r\"(sb + (b * " << kStage << "u + i) * "
+     << kThreads * 8 << "u) : \"memory\");\n"
+     << "  return v;\n"
+     << "}\n"
+     << "#endif\n"
      << "extern \"C\" __global__ void __launch_bounds__(" << kThreads << ", " << kMinBlocks << ") lu_tape(\n"
      << "    const double* __restrict__ a, const double* __restrict__ rhs, double* __restrict__ tv,\n"
      << "    double* __restrict__ dx, unsigned char* __restrict__ bad_out, unsigned n_lanes) {\n"
+     << "  __shared__ __align__(16) double stage_buf[2 * " << kStage << " * " << kThreads << "];\n"
      << "  const unsigned lane = blockIdx.x * " << kThreads << "u + threadIdx.x;\n"
      << "  if (lane >= n_lanes) return;\n"
      << "  const size_t N = n_lanes;\n"
      << "  const double* al = a + lane;\n"
      << "  const double* rl = rhs + lane;\n"
      << "  double* tl = tv + lane;\n"
+     << "  const unsigned sb = unsigned(__cvta_generic_to_shared(stage_buf + threadIdx.x));\n"
      << "  const double kInf = __longlong_as_double(0x7ff0000000000000ll);\n"
      << "  bool bad = false;\n";
-  // tape values (U, diagonal, L) are final after their last update in
-  // program A (at once when program A never writes them)
-  for (uint32_t v = 0; v + 1 < in.ntv; ++v)
-    if (last_a[v] < 0) g.finish(v);
-  for (uint32_t k = 0; k < in.n_seq_a; ++k) {
-    g.op(k, seq[k]);
-    const uint32_t d = seq[k].w0 & 0x0fffffffu;
-    if (last_a[d] == int64_t(k) && d < in.ntv) g.finish(d);
-  }
-  // dx is final after its last update; a y entry no op writes goes out as loaded
-  auto store_dx = [&](uint32_t j) {
-    os << "  dx[" << (*in.qcol)[j] << " * N + lane] = v" << (in.ntv + j) << ";\n";
-  };
-  for (uint32_t k = in.n_seq_a; k < in.n_seq; ++k) {
-    g.op(k, seq[k]);
-    const uint32_t d = seq[k].w0 & 0x0fffffffu;
-    if (d >= in.ntv && d < in.ntv + in.n && last_all[d] == int64_t(k)) store_dx(d - in.ntv);
-  }
-  for (uint32_t j = 0; j < in.n; ++j)
-    if (last_all[in.ntv + j] < int64_t(in.n_seq_a)) {
-      g.use(in.ntv + j);
-      store_dx(j);
-    }
+  // the first two stages in flight before any op
+  if (g.n_stages > 0) g.issue(0);
+  if (g.n_stages > 1) g.issue(1);
+  walk(g);
   os << "  bad_out[lane] = bad;\n"
      << "}\n";
   return os.str();

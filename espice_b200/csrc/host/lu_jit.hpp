@@ -23,7 +23,9 @@ struct LuJitInput {
   const std::vector<uint8_t>* l_scaled = nullptr; // per L entry: scaled pivot column
   const std::vector<Op>* seq = nullptr;           // real ops, program A then program B
   uint32_t n_seq_a = 0, n_seq = 0;
-  uint32_t reload_gap = 48;  // a final tape value unused for this many ops is re-read from its plane
+  // register budget, in values: beyond it the final tape values needed
+  // farthest ahead are let go and re-read from their plane at next use
+  uint32_t resident_values = 48;
 };
 
 // CUDA C++ source of the kernel `lu_tape`: one thread per lane over

@@ -132,7 +132,7 @@ class TapeInfo(ctypes.Structure):
 _lib = None
 
 
-def lu_compiled_source(n, cp, ri, lead, reload_gap=0):
+def lu_compiled_source(n, cp, ri, lead, resident=0):
     """The CUDA source the compiled lane LU builds for lead's tape (host only)."""
     L = lib()
     cp = np.ascontiguousarray(cp, np.uint32)
@@ -140,12 +140,12 @@ def lu_compiled_source(n, cp, ri, lead, reload_gap=0):
     lead = np.ascontiguousarray(lead, np.float64)
     size = ctypes.c_size_t(0)
     rc = L.esl_lu_compiled_source(ctypes.c_uint32(n), _p(cp, u32p), _p(ri, u32p), _p(lead, f64p),
-                                  ctypes.c_uint32(reload_gap), None, ctypes.c_size_t(0), ctypes.byref(size))
+                                  ctypes.c_uint32(resident), None, ctypes.c_size_t(0), ctypes.byref(size))
     if rc:
         raise LaneError(rc, "esl_lu_compiled_source")
     buf = ctypes.create_string_buffer(size.value + 1)
     L.esl_lu_compiled_source(ctypes.c_uint32(n), _p(cp, u32p), _p(ri, u32p), _p(lead, f64p),
-                             ctypes.c_uint32(reload_gap), buf, ctypes.c_size_t(size.value + 1), ctypes.byref(size))
+                             ctypes.c_uint32(resident), buf, ctypes.c_size_t(size.value + 1), ctypes.byref(size))
     return buf.value.decode()
 
 

@@ -333,11 +333,11 @@ int32_t esl_lu_lanes_compiled_device(esl_ctx *ctx, const double *lead, uint32_t 
 
 /* Host-only: the CUDA source esl_lu_lanes_compiled_device compiles for the
  * tape of `lead` on this pattern (NUL-terminated in buf when cap > 0; *len
- * = its length without the NUL). reload_gap: a final tape value unused for
- * this many ops is re-read from its plane instead of held (0: the library's
- * default, 48). */
+ * = its length without the NUL). resident: the register budget in values;
+ * beyond it the final tape values needed farthest ahead are re-read from
+ * their plane at their next use (0: the library's default, 48). */
 int32_t esl_lu_compiled_source(uint32_t n, const uint32_t *col_ptr, const uint32_t *row_idx,
-                               const double *lead, uint32_t reload_gap, char *buf, size_t cap,
+                               const double *lead, uint32_t resident, char *buf, size_t cap,
                                size_t *len);
 
 /* The compiler's log of the context's compiled LU (ptxas register and spill
