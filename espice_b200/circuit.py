@@ -35,7 +35,8 @@ M_PARAMS = ["type", "vto", "kp", "gamma", "phi", "lambda", "rd", "rs", "cbd", "c
             "is", "pb", "cgso", "cgdo", "cgbo", "cj", "mj", "cjsw", "mjsw", "tox",
             "ld", "u0", "fc", "w", "l", "ad", "as", "pd", "ps", "delvto", "m", "gmin",
             "tnom", "temp"]
-M_DEFAULTS = {"type": 1.0, "vto": 0.0, "kp": 2e-5, "gamma": 0.0, "phi": 0.6, "lambda": 0.0,
+# KP NaN: not given (its default is u0 * Cox' with TOX given, else 2e-5).
+M_DEFAULTS = {"type": 1.0, "vto": 0.0, "kp": float("nan"), "gamma": 0.0, "phi": 0.6, "lambda": 0.0,
               "rd": 0.0, "rs": 0.0, "cbd": 0.0, "cbs": 0.0, "is": 1e-14, "pb": 0.8,
               "cgso": 0.0, "cgdo": 0.0, "cgbo": 0.0, "cj": 0.0, "mj": 0.5, "cjsw": 0.0,
               "mjsw": 0.5, "tox": 0.0, "ld": 0.0, "u0": 600.0, "fc": 0.5, "w": 1e-4,

@@ -229,6 +229,7 @@ struct esl_ctx {
   std::vector<double> rec_lanes;
 
   bool have_tape = false;
+  bool has_meyer = false;  // a MOS1 instance gives TOX: DC only
   SparseLu lead;
   Programs prog;
 
@@ -890,7 +891,7 @@ int32_t esl_create(const esl_circuit* circuit, const esl_options* opts, esl_ctx*
   for (const auto& B : ctx->bats) {
     if (B.type == kM)
       for (uint32_t id = 0; id < B.count; ++id)
-        if (B.params[size_t(id) * B.np + kMParamTox] > 0.0) return ESL_NOT_ELIGIBLE;
+        if (B.params[size_t(id) * B.np + kMParamTox] > 0.0) ctx->has_meyer = true;
     ctx->n_stage += B.stride * B.count;
     ctx->rec_size += B.nfields * B.count;
     ctx->nlim += lim_count(B.type) * B.count;
@@ -1198,6 +1199,8 @@ int32_t ensure_tape_cold(esl_ctx* ctx) {
 
 int32_t tran_view(esl_ctx* ctx, const esl_tran_opts* o, TranDev& P, LaneOpts& lo) {
   if (!o || !(o->t_stop > 0) || !(o->t_step > 0)) return ctx->fail(ESL_INVALID_ARGUMENT, "t_stop and t_step must be positive");
+  if (ctx->has_meyer)
+    return ctx->fail(ESL_NOT_ELIGIBLE, "MOS1 with TOX: the bias-dependent Meyer gate capacitance is not built");
   P = TranDev{};
   P.t_stop = o->t_stop;
   P.t_step = o->t_step;

@@ -94,8 +94,8 @@ static void diode_record(const double* p, double* rec, uint32_t stride) {
   rec[kDHasQ * stride] = (p[5] > 0.0 || p[9] > 0.0) ? 1.0 : 0.0;
 }
 
-// models/mos1.va:150-271 with KP given (no TOX: no derived KP, no Meyer
-// halves), NSUB/NSS/JS/RSH left out: temperature, geometry, junction sizing,
+// models/mos1.va:150-271 (no Meyer halves: a circuit with TOX runs DC
+// only), NSUB/NSS/JS/RSH left out: KP's default, temperature, geometry, junction sizing,
 // the forward-region charge constants, vcrit and the MODEINITJCT vgs seed.
 static void mos1_record(const double* p, double* rec, uint32_t stride) {
   const double type = p[0];
@@ -105,7 +105,9 @@ static void mos1_record(const double* p, double* rec, uint32_t stride) {
   const double phix = p[4];
   const double gammax = p[3];
   const double vtox = p[1] + p[29];
-  const double kpx = p[2];
+  // KP: the card's, else u0 * Cox' with TOX given, else 2e-5 (mos1.va:159-192)
+  const double coxp = p[kMParamTox] > 0.0 ? 3.9 * 8.854214871e-12 / p[kMParamTox] : 0.0;
+  const double kpx = !std::isnan(p[2]) ? p[2] : coxp > 0.0 ? p[21] * coxp * 1.0e-4 : 2.0e-5;
   const double tk = p[33];
   const double vt = tk * (kBoltz / kCharge);
   const double fact1 = tnomk / 300.15;

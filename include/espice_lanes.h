@@ -42,7 +42,9 @@ enum {
     ESL_V = 2, /* nodes p n br;       params dc wave v1 v2 td tr tf pw per phase */
     ESL_I = 3, /* nodes p n;          params dc                              */
     ESL_D = 4, /* nodes a c ai;       params is n rs bv ibv cjo vj m fc tt area gmin xti eg tnom temp */
-    ESL_M = 5, /* nodes d g s b di si; params (MOS1, models/mos1.va)         */
+    ESL_M = 5, /* nodes d g s b di si; params (MOS1, models/mos1.va; kp NaN =
+                  not given: u0 * Cox' with tox > 0, else 2e-5; a circuit with
+                  tox > 0 runs DC only, its transients ESL_NOT_ELIGIBLE)    */
     ESL_B3 = 6 /* nodes d g s b di si; params (BSIM3v3 DC core, models/bsim3.va) */
 };
 

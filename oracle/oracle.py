@@ -263,5 +263,7 @@ def tran(frozen, slots, values, opts, probes=(), max_pts=0):
                         _p(probes, u32p) if npr else None, ctypes.c_uint32(npr),
                         ctypes.c_uint32(max_pts), _p(t, f64p) if rec else None,
                         _p(v, f64p) if rec else None, _p(npts, u32p), _p(stats, u32p), _p(xf, f64p))
+    if rc == -2:
+        raise ValueError("MOS1 with TOX: the Meyer gate capacitance is not restated (DC only)")
     assert rc == 0
     return t, v, npts, stats, xf

@@ -10,7 +10,9 @@
  *   :347-350  junction depletion charges
  *   :351-441  Meyer gate capacitance: only its overlap part (CGSO, CGDO,
  *             CGBO) is supported; with TOX given the bias-dependent halves
- *             and their $prev averaging are refused (orc_mos1_supported).
+ *             and their $prev averaging are not built, so such a circuit's
+ *             transient is refused (orc_mos1_supported); its DC runs, TOX
+ *             entering only through the KP default (:159-192).
  *
  * Frame: the model runs on type-frame voltages v = type * V (PMOS negated).
  * Limited images, three per instance: vgs, vds, vbs in the type frame.
@@ -43,7 +45,9 @@ void mos1_derive(const double *p, double *d) {
     const double phix = p[ORC_M_PHI];
     const double gammax = p[ORC_M_GAMMA];
     const double vtox = p[ORC_M_VTO] + p[ORC_M_DELVTO];
-    const double kpx = p[ORC_M_KP];
+    /* KP: the card's, else u0 * Cox' with TOX given, else 2e-5 (mos1.va:159-192) */
+    const double coxp = p[ORC_M_TOX] > 0.0 ? 3.9 * 8.854214871e-12 / p[ORC_M_TOX] : 0.0;
+    const double kpx = !isnan(p[ORC_M_KP]) ? p[ORC_M_KP] : coxp > 0.0 ? p[ORC_M_U0] * coxp * 1.0e-4 : 2.0e-5;
     const double tk = p[ORC_M_TEMP];
     const double vt = tk * (KB / QE);
     const double fact1 = tnomk / 300.15;

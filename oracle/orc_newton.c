@@ -59,7 +59,6 @@ int ckt_init(ckt_t *k, const orc_circuit *c) {
         for (uint32_t id = 0; id < src->count; id++) {
             const uint32_t *nd = bt->nodes + (size_t)id * bt->nt;
             layout_t *l = &bt->lay[id];
-            if (bt->type == ORC_M && !orc_mos1_supported(bt->prm + (size_t)id * bt->np)) return 1;
             dev_layout(bt->type, bt->prm + (size_t)id * bt->np, l);
             dev_derive(bt->type, bt->prm + (size_t)id * bt->np, bt->der + (size_t)id * ORC_NDER);
             for (int e = 0; e < l->nj; e++)

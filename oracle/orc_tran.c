@@ -351,12 +351,27 @@ static void tran_lane(ckt_t *k, const orc_tran_opts *o, rec_t *rec, uint32_t *st
     free(ip_row); free(ip_st); free(cur); free(prev); free(trial);
 }
 
+/* MOS1 with TOX given carries the bias-dependent Meyer halves and their
+ * $prev averaging (mos1.va:351-441), which this restatement leaves out: a
+ * transient of such a circuit is refused (DC runs, TOX affecting only the
+ * KP default there). */
+static int orc_tran_supported(const orc_circuit *c) {
+    for (uint32_t b = 0; b < c->n_batches; b++) {
+        const orc_batch *bt = &c->batches[b];
+        if (bt->type != ORC_M) continue;
+        for (uint32_t id = 0; id < bt->count; id++)
+            if (!orc_mos1_supported(bt->params + (size_t)id * ORC_M_NP)) return 0;
+    }
+    return 1;
+}
+
 int orc_tran(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
              const double *values, uint32_t n_lanes, const orc_tran_opts *topts,
              const uint32_t *probe_nodes, uint32_t n_probes, uint32_t max_pts,
              double *out_t, double *out_v, uint32_t *n_pts_out, uint32_t *stats,
              double *x_final) {
     ckt_t k;
+    if (!orc_tran_supported(c)) return -2;
     if (ckt_init(&k, c) != 0) return -1;
     for (uint32_t l = 0; l < n_lanes; l++) {
         for (uint32_t s = 0; s < n_slots; s++) ckt_set(&k, slots[s], values[(size_t)l * n_slots + s]);
@@ -376,6 +391,7 @@ int orc_tran_meas(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
                   const orc_measure *meas, uint32_t n_meas, int early_stop, double *meas_out,
                   uint32_t *stats, double *x_final) {
     ckt_t k;
+    if (!orc_tran_supported(c)) return -2;
     if (ckt_init(&k, c) != 0) return -1;
     orc_meas_state *ms = (orc_meas_state *)calloc(n_meas ? n_meas : 1, sizeof(orc_meas_state));
     for (uint32_t l = 0; l < n_lanes; l++) {

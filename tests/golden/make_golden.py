@@ -39,6 +39,7 @@ FIXTURES = [
     "dc/device_mos1_pmos",
     "dc/device_mos1_subthreshold",
     "dc/bench_sweep_cmos_inv_sizing",
+    "dc/device_mos1_temp",
     # BSIM3v3 DC core (LEVEL 49)
     "dc/device_bsim3_transfer",
     "dc/device_bsim3_output",

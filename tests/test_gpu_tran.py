@@ -126,3 +126,27 @@ def test_golden_transients_as_gpu_lanes(name):
     n = int(ng[0])
     for col, worst in gu.score_tran(g, tg[0, :n], vg[0, :n], cols):
         assert worst <= 1.0, f"{name} {col}: {worst:.3g}x the fixture tolerance"
+
+
+def test_mos1_tox_runs_dc_and_refuses_transient():
+    """MOS1 with TOX: the DC lanes solve (KP from U0 and TOX) and match the
+    oracle; a transient is refused with ESL_NOT_ELIGIBLE, as the oracle
+    refuses it (the bias-dependent Meyer halves are not built)."""
+    from espice_b200.circuit import Circuit
+    c = Circuit()
+    c.V("vdd", "d", "0", dc=1.8)
+    c.V("vg", "g", "0", dc=1.2)
+    c.M("m1", "d", "g", "0", "0", type=1.0, vto=0.5, tox=20e-9, u0=400.0, w=2e-6, l=1e-6)
+    fr = c.freeze()
+    slot = fr.slot("vg", "dc")
+    values = np.linspace(0.0, 1.8, 64).reshape(-1, 1)
+    xo, ito, cvo = oracle.dc_points(fr, [slot], values, warm=None)
+    ctx = lanes.DcLanes(fr)
+    ctx.set_lanes([slot], values)
+    x, it, st, _ = ctx.solve(x0=None)
+    assert np.array_equal(st == lanes.LANE_CONVERGED, cvo.astype(bool)) and cvo.all()
+    assert _close(x, xo).all()
+    with pytest.raises(lanes.LaneError) as e:
+        ctx.tran(lanes.tran_opts(1e-9, 1e-11))
+    assert e.value.code == lanes.ESL_NOT_ELIGIBLE
+    ctx.close()

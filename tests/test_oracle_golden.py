@@ -52,3 +52,25 @@ def test_oracle_measures_match_golden(name):
     assert st[0] == 0, st
     for nm, worst in gu.score_meas(g, values):
         assert worst <= 1.0, f"{name} {nm}: error {worst:.3g}x the allowed tolerance"
+
+
+def test_mos1_tox_is_dc_only():
+    """MOS1 with TOX: DC solves (TOX enters only KP's default: u0 * Cox'),
+    the transient is refused, as the library refuses it (the bias-dependent
+    Meyer halves and their $prev averaging are not built)."""
+    import numpy as np
+    from espice_b200.circuit import Circuit
+    c = Circuit()
+    c.V("vdd", "d", "0", dc=1.8)
+    c.V("vg", "g", "0", dc=1.2)
+    c.M("m1", "d", "g", "0", "0", type=1.0, vto=0.5, tox=20e-9, u0=400.0, w=2e-6, l=1e-6)
+    fr = c.freeze()
+    x, it, cv = oracle.dc_points(fr, [], np.zeros((1, 1)), warm=None)
+    assert cv[0]
+    # the drain current at KP = u0 * 3.9 eps0 / tox * 1e-4 (saturation, lambda
+    # 0), beside the drain junction's gmin leak (1e-12 S at 1.8 V)
+    kp = 400.0 * 3.9 * 8.854214871e-12 / 20e-9 * 1e-4
+    want = 0.5 * kp * 2.0 * (1.2 - 0.5) ** 2
+    assert abs(-x[0, fr.unknown("i(vdd)")] - want) <= 1e-6 * want
+    with pytest.raises(ValueError):
+        oracle.tran(fr, [], np.zeros((1, 1)), oracle.tran_opts(1e-9, 1e-11))
