@@ -28,6 +28,20 @@ FIXTURES = [
     "convergence/diode_stack_8",
     "convergence/bench_diode_bridge",
     "convergence/diode_knee",
+    "convergence/diode_emission_two",
+    "convergence/diode_forward",
+    "convergence/diode_high_current",
+    "convergence/diode_large_is",
+    "convergence/diode_reverse",
+    "convergence/diode_small_is",
+    "convergence/diode_stack_2",
+    "convergence/diode_stack_32",
+    "convergence/diode_weak_current",
+    "convergence/diode_zero",
+    "convergence/resistor_chain_8",
+    "convergence/resistor_chain_31",
+    "convergence/resistor_chain_64",
+    "convergence/resistor_chain_257",
     "op/bench_medium_resistor_mesh",
     "stress/scaling_resistor_grid_32x32",
     # MOS1
