@@ -110,19 +110,23 @@ B3_PMOS = dict(type=-1.0, tox=4.1e-9, vth0=-0.4, k1=0.55, k2=-0.05, k3=80.0, vsa
 
 
 def bsim3_inverters(seed: int = 1, stages: int = 6, lanes: int = 256, sigma: float = 0.02,
-                    vdd: float = 1.8, r_load: float = 50e3):
+                    vdd: float = 1.8, r_load: float = 50e3, c_load: float = 0.0, pulse=None):
     """Returns (frozen circuit, [input dc slot] + per-device delvto slots,
-    values [lanes][1 + 2 * stages])."""
+    values [lanes][1 + 2 * stages]). c_load > 0 adds a capacitor to ground
+    on every output and `pulse` (a PULSE list) drives the input, for a
+    transient (the BSIM3 DC core has no charges of its own)."""
     rng = np.random.default_rng(seed)
     c = Circuit()
     c.V("vdd", "vdd", "0", dc=vdd)
-    c.V("vin", "s_in", "0", dc=0.0)
+    c.V("vin", "s_in", "0", dc=0.0, pulse=pulse)
     prev = "s_in"
     for k in range(stages):
         out = f"s{k}"
         c.B3(f"mn{k}", out, prev, "0", "0", w=2e-6, l=0.18e-6, **B3_NMOS[k % len(B3_NMOS)])
         c.B3(f"mp{k}", out, prev, "vdd", "vdd", w=4e-6, l=0.18e-6, **B3_PMOS)
         c.R(f"rl{k}", out, "0", r_load)
+        if c_load > 0.0:
+            c.C(f"cl{k}", out, "0", c_load)
         prev = out
     fr = c.freeze()
     from .circuit import V

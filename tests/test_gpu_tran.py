@@ -150,3 +150,16 @@ def test_mos1_tox_runs_dc_and_refuses_transient():
         ctx.tran(lanes.tran_opts(1e-9, 1e-11))
     assert e.value.code == lanes.ESL_NOT_ELIGIBLE
     ctx.close()
+
+
+def test_bsim3_inverter_chain_transient_lanes():
+    """Eight lanes of a 4-stage BSIM3 inverter chain (20 fF per output, a
+    PULSE input, each lane with its own DELVTO per device) through the BSIM3
+    instantiation of the transient kernel: the oracle's step decisions,
+    waveform and end state."""
+    fr, slots, values = decks.bsim3_inverters(seed=5, stages=4, lanes=8, c_load=20e-15,
+                                              pulse=[0.0, 1.8, 0.1e-9, 50e-12, 50e-12, 0.4e-9, 1e-9])
+    probes = [fr.unknown("v(s0)"), fr.unknown("v(s3)")]
+    res_g, res_o = _run_both(fr, slots[1:], values[:, 1:], 2e-9, 10e-12, probes=probes, max_pts=4000)
+    _check_parity(res_g, res_o)
+    assert (res_g[3][:, 0] == lanes.TRAN_DONE).all()
