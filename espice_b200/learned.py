@@ -21,6 +21,20 @@ class LearnedWarmStart:
     def __init__(self, n_params, n_unknowns, hidden=256, layers=3, device=0, seed=1):
         self.net = mlp.Mlp(n_params, hidden, layers, n_unknowns, device=device, seed=seed)
         self.n_params, self.n = n_params, n_unknowns
+        self._bufs = {}
+
+    def buffers(self, n_points):
+        """Device work buffers for a batch of n_points, kept across calls: the
+        FP32 guesses, the FP64 unknowns, and the solver's status and
+        iteration words (one [2][N] int32 tensor, read back in one copy)."""
+        import torch
+        b = self._bufs.get(n_points)
+        if b is None:
+            b = (torch.empty((n_points, self.n), dtype=torch.float32, device="cuda"),
+                 torch.empty((n_points, self.n), dtype=torch.float64, device="cuda"),
+                 torch.zeros((2, n_points), dtype=torch.int32, device="cuda"))
+            self._bufs[n_points] = b
+        return b
 
     def close(self):
         self.net.close()
@@ -57,20 +71,22 @@ def solve(ctx, fallback, ws, slots, values, x_nominal, k=8, opts=None, d_values=
     circuit). `d_values`: the values already on the device as float32 (as the
     lanes' records are), else they are uploaded. Returns (x [N][n] device
     tensor, iterations [N] (both passes), converged mask [N] host, number of
-    fallback lanes)."""
+    fallback lanes). The returned x is the learned start's work buffer for
+    this batch size: valid until its next solve of the same size."""
     import torch
     opts = opts or lanes.newton_opts()
     N = values.shape[0]
     d_vals = d_values if d_values is not None else torch.tensor(values, dtype=torch.float32, device="cuda")
-    d_x = ws.predict(d_vals, N)
-    d_it = torch.zeros(N, dtype=torch.int32, device="cuda")
-    d_st = torch.zeros(N, dtype=torch.int32, device="cuda")
+    guess, d_x, words = ws.buffers(N)
+    ws.net.predict(d_vals.data_ptr(), N, guess.data_ptr())  # returns with its stream drained
+    d_x.copy_(guess)
     capped = lanes.newton_opts(opts.reltol, opts.abstol, opts.vntol, opts.residual_tol, opts.gmin,
                                opts.max_iter, bool(opts.init_fix), iter_cap=k)
-    torch.cuda.synchronize()
-    ctx.solve_device(d_x.data_ptr(), d_it.data_ptr(), d_st.data_ptr(), cold=False, opts=capped)
-    st = d_st.cpu().numpy()
-    it = d_it.cpu().numpy().astype(np.int64)
+    torch.cuda.current_stream().synchronize()
+    ctx.solve_device(d_x.data_ptr(), words[1].data_ptr(), words[0].data_ptr(), cold=False, opts=capped)
+    host = words.cpu().numpy()
+    st = host[0]
+    it = host[1].astype(np.int64)
     failed = np.flatnonzero(st != lanes.LANE_CONVERGED)
     if len(failed):
         fallback.set_lanes(slots, values[failed])
