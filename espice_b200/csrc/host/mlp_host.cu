@@ -143,13 +143,16 @@ int32_t ensure_batch(esl_mlp* m, int rows) {
 }
 
 // Forward over `rows` rows whose BF16 input is in hb[0]; output in z.back().
-int32_t forward(esl_mlp* m, int rows) {
+// keep_z: store every layer's FP32 pre-activation (the backward pass reads
+// them); inference stores only the last layer's.
+int32_t forward(esl_mlp* m, int rows, bool keep_z = true) {
   const size_t L = m->layers.size();
   for (size_t l = 0; l < L; ++l) {
     Layer& ly = *m->layers[l];
     const bool last = l + 1 == L;
     __nv_bfloat16* next = last ? nullptr : m->hb[l + 1]->p;
-    MLP_CUDA(esl::launch_gemm_bf16(m->hb[l]->p, ly.k, ly.wb.p, ly.k, rows, ly.n, ly.k, ly.b.p, m->z[l]->p, ly.n, next,
+    float* z = (keep_z || last) ? m->z[l]->p : nullptr;
+    MLP_CUDA(esl::launch_gemm_bf16(m->hb[l]->p, ly.k, ly.wb.p, ly.k, rows, ly.n, ly.k, ly.b.p, z, ly.n, next,
                                    ly.n, last ? 0 : 1, m->gerr.p, m->stream));
   }
   return ESL_MLP_OK;
@@ -345,7 +348,7 @@ int32_t esl_mlp_predict(esl_mlp* m, const float* d_x, uint32_t n, float* d_y) {
     scale_rows<<<(rows * kin + 255) / 256, 256, 0, s>>>(d_x + size_t(r0) * m->n_in, nullptr, rows, m->n_in, kin,
                                                          m->d_in_mu.p, m->d_in_sig.p, m->hb[0]->p, nullptr);
     MLP_CUDA(cudaGetLastError());
-    if (int32_t rc = forward(m, rows)) return rc;
+    if (int32_t rc = forward(m, rows, false)) return rc;
     unscale_rows<<<(rows * m->n_out + 255) / 256, 256, 0, s>>>(m->z.back()->p, rows, m->n_out, last.n,
                                                                 m->d_out_mu.p, m->d_out_sig.p,
                                                                 d_y + size_t(r0) * m->n_out);

@@ -166,26 +166,40 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tc(const __nv_bfloat16* __
   }
   if (!ok && tid == 0) atomicExch(err, 1);
 
-  // epilogue: warp w reads accumulator rows 32w + lane, eight columns a time
-  const int m = m0 + warp * 32 + lane;
-  for (int c0 = 0; c0 < bn; c0 += 8) {
-    uint32_t r[8];
+  // epilogue: warp w owns accumulator rows 32w .. 32w + 31 (thread = row in
+  // TMEM). Each 32-column block goes through the warp's 32 x 33 float
+  // patch of the (now idle) staging buffer, so the global stores run along
+  // rows: lane j writes column c0 + j of each row, 128 B per row per store
+  // instead of 32 rows of 4 B. The MMAs that read the staging buffer are
+  // complete (the last mbarrier wait above). Columns c0 .. c0 + 31 stay
+  // inside the allocation: ncols is a power of two >= max(bn, 32).
+  float* patch = reinterpret_cast<float*>(smem) + warp * 32 * 33;
+  for (int c0 = 0; c0 < bn; c0 += 32) {
+    uint32_t r[32];
     const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0);
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;");
-    if (m < M && ok) {
 #pragma unroll
-      for (int t = 0; t < 8; ++t) {
-        const int n = n0 + c0 + t;
-        float v = __uint_as_float(r[t]);
-        if (bias) v += bias[n];
+    for (int j = 0; j < 4; ++j)
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+          : "=r"(r[8 * j]), "=r"(r[8 * j + 1]), "=r"(r[8 * j + 2]), "=r"(r[8 * j + 3]), "=r"(r[8 * j + 4]),
+            "=r"(r[8 * j + 5]), "=r"(r[8 * j + 6]), "=r"(r[8 * j + 7])
+          : "r"(taddr + uint32_t(8 * j)));
+    asm volatile("tcgen05.wait::ld.sync.aligned;");
+#pragma unroll
+    for (int t = 0; t < 32; ++t) patch[lane * 33 + t] = __uint_as_float(r[t]);
+    __syncwarp();
+    const int n = n0 + c0 + lane;
+    const bool col = c0 + lane < bn;
+    const float bv = (bias && col) ? bias[n] : 0.0f;
+    for (int rr = 0; rr < 32; ++rr) {
+      const int m = m0 + warp * 32 + rr;
+      if (m < M && col && ok) {
+        const float v = patch[rr * 33 + lane] + bv;
         if (c) c[size_t(m) * ldc + n] = v;
         if (h) h[size_t(m) * ldh + n] = __float2bfloat16_rn(act == 1 ? tanhf(v) : v);
       }
     }
+    __syncwarp();
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
