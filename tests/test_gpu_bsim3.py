@@ -80,10 +80,12 @@ def test_bsim3_sweep_lanes_match_oracle():
 
 
 OP_FIXTURES = [n for n in gu.names() if n.split("__")[0] in ("op", "convergence", "stress")]
-# The 32x32 resistor grid (1,027 unknowns, 22,568 tape values, 235k
-# program ops) does not fit one CTA's shared memory: the library refuses it
-# (ESL_NOT_ELIGIBLE) and the reference's CPU path serves it.
-TOO_BIG = {"stress__scaling_resistor_grid_32x32"}
+# Circuits whose warp programs and one lane's working set do not fit one
+# CTA's shared memory are refused (ESL_NOT_ELIGIBLE) and the reference's CPU
+# path serves them: the 32x32 resistor grid (1,027 unknowns, 22,568 tape
+# values, 235k program ops) and the 257-section resistor chain (259
+# unknowns).
+TOO_BIG = {"stress__scaling_resistor_grid_32x32", "convergence__resistor_chain_257"}
 
 
 @pytest.mark.parametrize("name", OP_FIXTURES)
