@@ -294,6 +294,19 @@ def lu_lanes_roofline(fr, ctx, hbm_peak, peak_src, lanes_n=131072, reps=5):
                                       refine.data_ptr()))
     tm = float(np.mean(msm[2:])) / 1e3
     rel = float(((dxm - dx).abs() / dx.abs().clamp_min(1e-300)).max())
+    # the mixed form compiled into code, on the same lanes
+    dxc2 = torch.empty_like(rhs)
+    msc2 = []
+    for _ in range(reps + 2):
+        torch.cuda.synchronize()
+        msc2.append(ctx.lu_lanes_mixed_compiled(lead, a.data_ptr(), rhs.data_ptr(), dxc2.data_ptr(), bad.data_ptr(),
+                                                lanes_n, refine.data_ptr()))
+    tmc = float(np.mean(msc2[2:])) / 1e3
+    out["mixed_compiled"] = {"kernel": "lu_tape_mixed (FP32 factors in registers, FP64 refinement, NVRTC)",
+                             "ms": tmc * 1e3, "speedup_vs_fp64_compiled": t / tmc,
+                             "achieved_gbs": lanes_n * 8 * (nnz + 2 * n) / tmc / 1e9,
+                             "mean_corrections": float(refine.double().mean()),
+                             "max_rel_dev_vs_fp64": float(((dxc2 - dx).abs() / dx.abs().clamp_min(1e-300)).max())}
     out["mixed"] = {"kernel": "lu_lanes_mixed_kernel", "ms": tm * 1e3, "speedup_vs_fp64": t / tm,
                     "bytes_per_lane": 8 * (nnz + 2 * n), "achieved_gbs": lanes_n * 8 * (nnz + 2 * n) / tm / 1e9,
                     "mean_corrections": float(refine.double().mean()), "max_rel_dev_vs_fp64": rel}

@@ -240,6 +240,9 @@ struct esl_ctx {
   uint32_t n_seq_f = 0, mixed_warps = 0;            // its forward-only tail, the mixed kernel's warps
   LuJitKernels lu_jit;                               // the tape-compiled lane LU of the current tape
   DevBuf d_lu_scratch;                               // its tape-value plane when the caller passes none
+  LuJitKernels lu_jit_mixed;                         // the compiled mixed-precision form
+  int lu_jit_mixed_state = 0;
+  DevBuf d_lu_scratch32;                             // its FP32 factor plane
   int lu_jit_state = 0;                              // 0 not built, 1 built, -1 failed
   DevBuf d_row_ptr, d_row_slot, d_row_col;
   DevBuf d_group_topo, d_group_lanes, d_group_cta_ctx, d_group_cta_first, d_group_lpb;  // a group launch's tables
@@ -642,7 +645,8 @@ std::vector<Op> lane_sequence(const Programs& P, uint32_t& n_a, uint32_t& n_all,
 // replay's own sequential order (column by column; every value's updates in
 // the same order as the warp programs', so the same bits), which keeps
 // fewer values live at once than the programs' level-packed rows.
-std::string compiled_lu_source(uint32_t nnz, const SparseLu& lu, const Programs& P, uint32_t resident = 0) {
+std::string compiled_lu_source(uint32_t nnz, const SparseLu& lu, const Programs& P, uint32_t resident = 0,
+                               bool mixed = false) {
   std::vector<Op> seq = P.a_list;
   const uint32_t n_a = uint32_t(seq.size());
   seq.insert(seq.end(), P.b_list.begin(), P.b_list.end());
@@ -663,6 +667,10 @@ std::string compiled_lu_source(uint32_t nnz, const SparseLu& lu, const Programs&
   in.seq = &seq;
   in.n_seq_a = n_a;
   in.n_seq = n_all;
+  in.mixed = mixed;
+  in.col_ptr = &lu.a->col_ptr;
+  in.row_idx = &lu.a->row_idx;
+  if (mixed) in.resident_values = 48;  // the refinement loop needs the registers (more spilled)
   if (resident) in.resident_values = resident;
   return lu_jit_source(in);
 }
@@ -746,6 +754,8 @@ int32_t upload_tape(esl_ctx* ctx) {
     ESL_CUDA(upload(ctx->d_seq, seq, s));
     lu_jit_release(ctx->lu_jit);  // a new tape needs its own compiled LU
     ctx->lu_jit_state = 0;
+    lu_jit_release(ctx->lu_jit_mixed);
+    ctx->lu_jit_mixed_state = 0;
     ctx->mixed_warps = 0;
     for (uint32_t w = 8; w >= 1; --w)
       if (lu_lanes_mixed_smem(T, ctx->n_seq + ctx->n_seq_f, w) <= room) {
@@ -933,6 +943,7 @@ int32_t esl_destroy(esl_ctx* ctx) {
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   lu_jit_release(ctx->lu_jit);
+  lu_jit_release(ctx->lu_jit_mixed);
   cudaStream_t s = ctx->stream;
   delete ctx;
   if (s) cudaStreamDestroy(s);
@@ -1639,6 +1650,59 @@ int32_t esl_lu_lanes_compiled_device(esl_ctx* ctx, const double* lead, uint32_t 
   ESL_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
   ESL_CUDA(cudaEventSynchronize(ctx->ev1));
   if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
+  return ESL_OK;
+}
+
+int32_t esl_lu_lanes_mixed_compiled_device(esl_ctx* ctx, const double* lead, uint32_t n_lanes, const double* d_a,
+                                           const double* d_rhs, double* d_dx, uint8_t* d_bad, uint8_t* d_refine,
+                                           float* ms) {
+  if (!ctx || !d_a || !d_rhs || !d_dx || !d_bad || n_lanes == 0) return ESL_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  if (!ctx->have_tape) {
+    if (!lead) return ESL_INVALID_ARGUMENT;
+    if (int32_t rc = build_tape_from(ctx, lead)) return rc;
+  }
+  if (ctx->lu_jit_mixed_state == 0) {
+    ctx->lu_jit_mixed_state = -1;
+    if (ctx->prog.a_nops + ctx->prog.b_nops > kLuJitMaxOps)
+      return ctx->fail(ESL_NOT_ELIGIBLE, "the tape is too long to compile");
+    const std::string src = compiled_lu_source(ctx->topo.nnz, ctx->lead, ctx->prog, 0, true);
+    if (!lu_jit_build(src, ctx->lu_jit_mixed, "lu_tape_mixed"))
+      return ctx->fail(ESL_NOT_ELIGIBLE, "compiling the tape failed: " + ctx->lu_jit_mixed.log);
+    ctx->lu_jit_mixed_state = 1;
+  }
+  if (ctx->lu_jit_mixed_state < 0) return ctx->fail(ESL_NOT_ELIGIBLE, "the tape could not be compiled");
+  ESL_CUDA(ctx->d_lu_scratch32.ensure(size_t(ctx->prog.ntv) * n_lanes * 4));
+  ESL_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  ESL_CUDA(lu_jit_launch_mixed(ctx->lu_jit_mixed, n_lanes, d_a, d_rhs, ctx->d_lu_scratch32.as<float>(), d_dx, d_bad,
+                               d_refine, ctx->stream));
+  ESL_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  ESL_CUDA(cudaEventSynchronize(ctx->ev1));
+  if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
+  return ESL_OK;
+}
+
+int32_t esl_lu_compiled_mixed_source(uint32_t n, const uint32_t* col_ptr, const uint32_t* row_idx,
+                                     const double* lead, char* buf, size_t cap, size_t* len) {
+  if (!col_ptr || !row_idx || !lead || !len || n == 0) return ESL_INVALID_ARGUMENT;
+  Csc pat;
+  pat.n = n;
+  pat.col_ptr.assign(col_ptr, col_ptr + n + 1);
+  pat.row_idx.assign(row_idx, row_idx + col_ptr[n]);
+  SparseLu lu;
+  lu.init(&pat, order_columns(pat));
+  lu.fill_cap = kRepivotFillCap;
+  lu.keep_min = kGrowthLimit;
+  if (!lu.factor(lead, kPivotTol)) return ESL_NOT_ELIGIBLE;
+  Programs P = compile_tape(lu);
+  if (P.has_void) return ESL_NOT_ELIGIBLE;
+  const std::string src = compiled_lu_source(col_ptr[n], lu, P, 0, true);
+  *len = src.size();
+  if (buf && cap > 0) {
+    const size_t k = std::min(cap - 1, src.size());
+    std::memcpy(buf, src.data(), k);
+    buf[k] = '\0';
+  }
   return ESL_OK;
 }
 

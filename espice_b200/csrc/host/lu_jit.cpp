@@ -80,6 +80,14 @@ struct Gen {
     for (uint32_t r = 0; r < in.n; ++r) row_of[in.ntv + (*in.pinv)[r]] = r;
   }
 
+  // FP64 form (double values, __d*_rn) or mixed form (float factors and y,
+  // __f*_rn, FP32 peel tests as the interpreted mixed kernel takes them)
+  const char* ty() const { return in.mixed ? "float" : "double"; }
+  const char* sub_rn() const { return in.mixed ? "__fsub_rn" : "__dsub_rn"; }
+  const char* mul_rn() const { return in.mixed ? "__fmul_rn" : "__dmul_rn"; }
+  const char* div_rn() const { return in.mixed ? "__fdiv_rn" : "__ddiv_rn"; }
+  const char* zero() const { return in.mixed ? "0.0f" : "0.0"; }
+
   static constexpr uint32_t kNever = 0xffffffffu;
   uint32_t next_use(uint32_t v) const { return next[v] < uses[v].size() ? uses[v][next[v]] : kNever; }
   bool constant(uint32_t v) const { return v >= in.nv - 3; }
@@ -124,13 +132,13 @@ struct Gen {
         order.push_back(v);
       }
       if (loaded && !record) enter_stage(uint32_t(pos[v] / kStage));
-      os << "  double v" << v << " = ";
-      if (v == in.nv - 2) os << "1.0";
-      else if (constant(v)) os << "0.0";
+      os << "  " << ty() << " v" << v << " = ";
+      if (v == in.nv - 2) os << (in.mixed ? "1.0f" : "1.0");
+      else if (constant(v)) os << zero();
       else if (loaded)
-        os << (slot_of[v] >= 0 ? "" : "-") << "stage_read(sb, " << (pos[v] / kStage) % 2 << ", " << pos[v] % kStage
-           << ")";
-      else os << "0.0";  // fill-in (and an entry no slot or op sets)
+        os << (in.mixed ? "float(" : "") << (slot_of[v] >= 0 ? "" : "-") << "stage_read(sb, " << (pos[v] / kStage) % 2
+           << ", " << pos[v] % kStage << ")" << (in.mixed ? ")" : "");
+      else os << zero();  // fill-in (and an entry no slot or op sets)
       os << ";\n";
     }
   }
@@ -188,20 +196,22 @@ struct Gen {
     use(b);
     if (kind == kOpFlop || kind == kOpSubNz) {
       use(d);
-      if (kind == kOpSubNz) os << "  if (v" << b << " != 0.0)";
-      os << "  v" << d << " = __dsub_rn(v" << d << ", __dmul_rn(v" << a << ", v" << b << "));\n";
+      if (kind == kOpSubNz) os << "  if (v" << b << " != " << zero() << ")";
+      os << "  v" << d << " = " << sub_rn() << "(v" << d << ", " << mul_rn() << "(v" << a << ", v" << b << "));\n";
       wrote(d);
       return;
     }
-    os << "  const double q" << k << " = __ddiv_rn(v" << b << ", v" << a << ");\n";
-    if (kind == kOpDivGrowth)
-      os << "  bad |= !(fabs(v" << a << ") >= __dmul_rn(1e-12, fabs(v" << b << ")));\n";
+    os << "  const " << ty() << " q" << k << " = " << div_rn() << "(v" << b << ", v" << a << ");\n";
+    if (kind == kOpDivGrowth) {
+      if (in.mixed) os << "  bad |= !(fabsf(v" << a << ") >= __fmul_rn(1e-12f, fabsf(v" << b << ")));\n";
+      else os << "  bad |= !(fabs(v" << a << ") >= __dmul_rn(1e-12, fabs(v" << b << ")));\n";
+    }
     if (kind == kOpDivScaled) os << "  bad |= !(fabs(q" << k << ") < kInf);\n";
     if (defined[d]) {
       os << "  v" << d << " = q" << k << ";\n";
     } else {
       defined[d] = 1;
-      os << "  double v" << d << " = q" << k << ";\n";
+      os << "  " << ty() << " v" << d << " = q" << k << ";\n";
     }
     // a division's destination is a new value in a register: counted as a
     // reference, with no load
@@ -219,6 +229,12 @@ struct Gen {
     use(v);
     os << "  " << home(v) << " = v" << v << ";\n";
     clean[v] = 1;
+    if (in.mixed) {  // the interpreted mixed kernel's FP32 tests
+      if (v < in.nu) os << "  bad |= !(fabsf(v" << v << ") < kInf);\n";
+      else if (v < in.nu + in.n) os << "  bad |= v" << v << " == 0.0f || !(fabsf(v" << v << ") < kInf);\n";
+      else if (!(*in.l_scaled)[v - in.nu - in.n]) os << "  bad |= !(fabsf(v" << v << ") <= 1e3f);\n";
+      return;
+    }
     if (v < in.nu) {
       os << "  bad |= __double_as_longlong(v" << v << " - v" << v << ") != 0;\n";
     } else if (v < in.nu + in.n) {
@@ -237,6 +253,59 @@ struct Gen {
 };
 
 }  // namespace
+
+// The mixed form's FP64 refinement, after dx = the FP32 solve: the residual
+// res = -rhs - A dx in FP64 (A and rhs re-read, the pattern by rows, columns
+// ascending), then, unless max |res| <= 1e-12 max |rhs| or 6 corrections
+// are done, the correction solved on the FP32 factors (the forward
+// substitution's ops of program A, then program B, all in their sequential
+// order, the factors read from their FP32 plane) and added to dx, as the
+// interpreted mixed kernel does it.
+static void refinement(const LuJitInput& in, std::ostringstream& os) {
+  const std::vector<Op>& seq = *in.seq;
+  std::vector<std::vector<std::pair<uint32_t, uint32_t>>> rows(in.n);
+  for (uint32_t j = 0; j < in.n; ++j)
+    for (uint32_t p = (*in.col_ptr)[j]; p < (*in.col_ptr)[j + 1]; ++p) rows[(*in.row_idx)[p]].push_back({p, j});
+  auto y = [&](uint32_t v) { return "r" + std::to_string(v - in.ntv); };
+  auto fac = [&](uint32_t v) { return "__ldcg(&tl[" + std::to_string(v) + " * N])"; };
+  os << "  unsigned char refined = 0;\n"
+     << "  #pragma unroll 1\n"
+     << "  for (int it = 0; it <= 6; ++it) {\n"
+     << "    double rmax = 0.0, bmax = 0.0;\n    float";
+  for (uint32_t j = 0; j < in.n; ++j) os << (j ? ", r" : " r") << j;
+  os << ";\n";
+  for (uint32_t i = 0; i < in.n; ++i) {
+    os << "    {\n      const double b = __ldg(rl + " << i << " * N);\n      double res = -b;\n";
+    for (const auto& e : rows[i])
+      os << "      res = __dsub_rn(res, __dmul_rn(__ldg(al + " << e.first << " * N), __ldcg(&dx[" << e.second
+         << " * N + lane])));\n";
+    os << "      rmax = fmax(rmax, fabs(res));\n      bmax = fmax(bmax, fabs(b));\n"
+       << "      r" << (*in.pinv)[i] << " = float(res);\n    }\n";
+  }
+  os << "    if (!(rmax > 1e-12 * bmax) || it == 6) break;\n";
+  for (uint32_t k = 0; k < in.n_seq_a; ++k) {
+    const Op& o = seq[k];
+    if ((o.w0 >> 28) != kOpSubNz) continue;
+    const uint32_t d = o.w0 & 0x0fffffffu, a = o.w1 & 0xffffu, b = o.w1 >> 16;
+    os << "    if (" << y(b) << " != 0.0f) " << y(d) << " = __fsub_rn(" << y(d) << ", __fmul_rn(" << fac(a) << ", " << y(b)
+       << "));\n";
+  }
+  for (uint32_t k = in.n_seq_a; k < in.n_seq; ++k) {
+    const Op& o = seq[k];
+    const uint32_t kind = o.w0 >> 28, d = o.w0 & 0x0fffffffu, a = o.w1 & 0xffffu, b = o.w1 >> 16;
+    if (kind == kOpNop) continue;
+    if (kind == kOpSubNz)
+      os << "    if (" << y(b) << " != 0.0f) " << y(d) << " = __fsub_rn(" << y(d) << ", __fmul_rn(" << fac(a) << ", "
+         << y(b) << "));\n";
+    else  // the back substitution's divisions (kOpDivY)
+      os << "    " << y(d) << " = __fdiv_rn(" << y(b) << ", " << fac(a) << ");\n";
+  }
+  for (uint32_t j = 0; j < in.n; ++j)
+    os << "    dx[" << (*in.qcol)[j] << " * N + lane] = __ldcg(&dx[" << (*in.qcol)[j] << " * N + lane]) + double(r" << j
+       << ");\n";
+  os << "    ++refined;\n  }\n"
+     << "  if (refine_out) refine_out[lane] = refined;\n";
+}
 
 std::string lu_jit_source(const LuJitInput& in) {
   const std::vector<Op>& seq = *in.seq;
@@ -302,24 +371,33 @@ std::string lu_jit_source(const LuJitInput& in) {
      << kThreads * 8 << "u) : \"memory\");\n"
      << "  return v;\n"
      << "}\n"
-     << "#endif\n"
-     << "extern \"C\" __global__ void __launch_bounds__(" << kThreads << ", " << kMinBlocks << ") lu_tape(\n"
-     << "    const double* __restrict__ a, const double* __restrict__ rhs, double* __restrict__ tv,\n"
-     << "    double* __restrict__ dx, unsigned char* __restrict__ bad_out, unsigned n_lanes) {\n"
+     << "#endif\n";
+  if (in.mixed)
+    os << "extern \"C\" __global__ void __launch_bounds__(" << kThreads << ", " << kMinBlocks << ") lu_tape_mixed(\n"
+       << "    const double* __restrict__ a, const double* __restrict__ rhs, float* __restrict__ tv,\n"
+       << "    double* __restrict__ dx, unsigned char* __restrict__ bad_out, unsigned char* __restrict__ refine_out,\n"
+       << "    unsigned n_lanes) {\n";
+  else
+    os << "extern \"C\" __global__ void __launch_bounds__(" << kThreads << ", " << kMinBlocks << ") lu_tape(\n"
+       << "    const double* __restrict__ a, const double* __restrict__ rhs, double* __restrict__ tv,\n"
+       << "    double* __restrict__ dx, unsigned char* __restrict__ bad_out, unsigned n_lanes) {\n";
+  os
      << "  __shared__ __align__(16) double stage_buf[2 * " << kStage << " * " << kThreads << "];\n"
      << "  const unsigned lane = blockIdx.x * " << kThreads << "u + threadIdx.x;\n"
      << "  if (lane >= n_lanes) return;\n"
      << "  const size_t N = n_lanes;\n"
      << "  const double* al = a + lane;\n"
      << "  const double* rl = rhs + lane;\n"
-     << "  double* tl = tv + lane;\n"
+     << "  " << g.ty() << "* tl = tv + lane;\n"
      << "  const unsigned sb = unsigned(__cvta_generic_to_shared(stage_buf + threadIdx.x));\n"
-     << "  const double kInf = __longlong_as_double(0x7ff0000000000000ll);\n"
+     << (in.mixed ? "  const float kInf = __int_as_float(0x7f800000);\n"
+                  : "  const double kInf = __longlong_as_double(0x7ff0000000000000ll);\n")
      << "  bool bad = false;\n";
   // the first two stages in flight before any op
   if (g.n_stages > 0) g.issue(0);
   if (g.n_stages > 1) g.issue(1);
   walk(g);
+  if (in.mixed) refinement(in, os);
   os << "  bad_out[lane] = bad;\n"
      << "}\n";
   return os.str();
@@ -363,7 +441,7 @@ const Nvrtc& nvrtc() {
 
 }  // namespace
 
-bool lu_jit_build(const std::string& src, LuJitKernels& out) {
+bool lu_jit_build(const std::string& src, LuJitKernels& out, const char* name) {
   const Nvrtc& nv = nvrtc();
   if (!nv.ok) {
     out.log = "NVRTC (libnvrtc.so.12) is not available";
@@ -396,7 +474,7 @@ bool lu_jit_build(const std::string& src, LuJitKernels& out) {
     out.lib = nullptr;
     return false;
   }
-  if (cudaLibraryGetKernel(&out.kernel, out.lib, "lu_tape") != cudaSuccess) {
+  if (cudaLibraryGetKernel(&out.kernel, out.lib, name) != cudaSuccess) {
     cudaGetLastError();
     out.log += "\ncudaLibraryGetKernel failed";
     lu_jit_release(out);
@@ -416,6 +494,17 @@ cudaError_t lu_jit_launch(const LuJitKernels& k, uint32_t n_lanes, const double*
   void* args[] = {&a, &rhs, &tv, &dx, &bad, &n_lanes};
   const void* fn = reinterpret_cast<const void*>(k.kernel);
   return cudaLaunchKernel(fn, dim3((n_lanes + kThreads - 1) / kThreads), dim3(kThreads), args, 0, s);
+}
+
+}  // namespace esl
+
+namespace esl {
+
+cudaError_t lu_jit_launch_mixed(const LuJitKernels& k, uint32_t n_lanes, const double* a, const double* rhs,
+                                float* tf, double* dx, uint8_t* bad, uint8_t* refine, cudaStream_t s) {
+  void* args[] = {&a, &rhs, &tf, &dx, &bad, &refine, &n_lanes};
+  return cudaLaunchKernel(reinterpret_cast<const void*>(k.kernel), dim3((n_lanes + kThreads - 1) / kThreads),
+                          dim3(kThreads), args, 0, s);
 }
 
 }  // namespace esl

@@ -26,6 +26,11 @@ struct LuJitInput {
   // register budget, in values: beyond it the final tape values needed
   // farthest ahead are let go and re-read from their plane at next use
   uint32_t resident_values = 48;
+  // the mixed form: FP32 factors and solves, then FP64 refinement on the
+  // residual over the pattern (col_ptr, row_idx), kernel `lu_tape_mixed`
+  bool mixed = false;
+  const std::vector<uint32_t>* col_ptr = nullptr;
+  const std::vector<uint32_t>* row_idx = nullptr;
 };
 
 // CUDA C++ source of the kernel `lu_tape`: one thread per lane over
@@ -45,11 +50,15 @@ struct LuJitKernels {
 // each multiply and subtract rounds on its own) and loads the cubin on the
 // current device. Returns false with `out.log` set when NVRTC is missing or
 // the compile or load fails.
-bool lu_jit_build(const std::string& src, LuJitKernels& out);
+bool lu_jit_build(const std::string& src, LuJitKernels& out, const char* name = "lu_tape");
 void lu_jit_release(LuJitKernels& k);
 
 // tv: [ntv][n_lanes], never NULL (the kernel re-reads values from it).
 cudaError_t lu_jit_launch(const LuJitKernels& k, uint32_t n_lanes, const double* a, const double* rhs, double* tv,
                           double* dx, uint8_t* bad, cudaStream_t s);
+
+// The mixed form: tf [ntv][n_lanes] FP32 plane (never NULL), refine may be NULL.
+cudaError_t lu_jit_launch_mixed(const LuJitKernels& k, uint32_t n_lanes, const double* a, const double* rhs,
+                                float* tf, double* dx, uint8_t* bad, uint8_t* refine, cudaStream_t s);
 
 }  // namespace esl

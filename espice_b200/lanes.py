@@ -30,7 +30,7 @@ EXPORTS = ["esl_create", "esl_destroy", "esl_last_error", "esl_dims", "esl_set_l
            "esl_tape_size", "esl_pattern", "esl_compile_tape", "esl_tran", "esl_tran_device", "esl_lu_lanes_device",
            "esl_lu_lanes_mixed_device", "esl_group_dc_solve_device", "esl_autotune", "esl_dc_sweep_device",
            "esl_tran_meas_device", "esl_lu_lanes_compiled_device", "esl_lu_compiled_log",
-           "esl_lu_compiled_source"]
+           "esl_lu_compiled_source", "esl_lu_lanes_mixed_compiled_device", "esl_lu_compiled_mixed_source"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 f64p = ctypes.POINTER(ctypes.c_double)
@@ -130,6 +130,23 @@ class TapeInfo(ctypes.Structure):
 
 
 _lib = None
+
+
+def lu_compiled_mixed_source(n, cp, ri, lead):
+    """The mixed form's CUDA source for lead's tape (host only)."""
+    L = lib()
+    cp = np.ascontiguousarray(cp, np.uint32)
+    ri = np.ascontiguousarray(ri, np.uint32)
+    lead = np.ascontiguousarray(lead, np.float64)
+    size = ctypes.c_size_t(0)
+    rc = L.esl_lu_compiled_mixed_source(ctypes.c_uint32(n), _p(cp, u32p), _p(ri, u32p), _p(lead, f64p), None,
+                                        ctypes.c_size_t(0), ctypes.byref(size))
+    if rc:
+        raise LaneError(rc, "esl_lu_compiled_mixed_source")
+    buf = ctypes.create_string_buffer(size.value + 1)
+    L.esl_lu_compiled_mixed_source(ctypes.c_uint32(n), _p(cp, u32p), _p(ri, u32p), _p(lead, f64p), buf,
+                                   ctypes.c_size_t(size.value + 1), ctypes.byref(size))
+    return buf.value.decode()
 
 
 def lu_compiled_source(n, cp, ri, lead, resident=0):
@@ -437,6 +454,16 @@ class DcLanes:
                                                          ctypes.c_void_p(d_dx), ctypes.c_void_p(d_bad),
                                                          ctypes.c_void_p(d_tv) if d_tv else None,
                                                          ctypes.byref(ms)), "esl_lu_lanes_compiled_device")
+        return ms.value
+
+    def lu_lanes_mixed_compiled(self, lead, d_a, d_rhs, d_dx, d_bad, n_lanes, d_refine=0):
+        """lu_lanes_mixed through the tape compiled into code; the kernel's ms."""
+        lead = np.ascontiguousarray(lead, np.float64)
+        ms = ctypes.c_float(0)
+        self._check(self._L.esl_lu_lanes_mixed_compiled_device(
+            self._ctx, _p(lead, f64p), ctypes.c_uint32(n_lanes), ctypes.c_void_p(d_a), ctypes.c_void_p(d_rhs),
+            ctypes.c_void_p(d_dx), ctypes.c_void_p(d_bad), ctypes.c_void_p(d_refine) if d_refine else None,
+            ctypes.byref(ms)), "esl_lu_lanes_mixed_compiled_device")
         return ms.value
 
     def lu_compiled_log(self):

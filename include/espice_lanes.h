@@ -342,6 +342,20 @@ int32_t esl_lu_compiled_source(uint32_t n, const uint32_t *col_ptr, const uint32
                                const double *lead, uint32_t resident, char *buf, size_t cap,
                                size_t *len);
 
+/* esl_lu_lanes_mixed_device with the tape compiled into code (NVRTC, first
+ * call): FP32 factors and solves in registers (an FP32 factor plane, owned
+ * by the context, holds the values let go and serves the corrections), then
+ * the same FP64 refinement on the residual -rhs - A dx until it falls below
+ * 1e-12 of rhs, at most 6 corrections. Same arguments as
+ * esl_lu_lanes_mixed_device; ESL_NOT_ELIGIBLE without NVRTC. */
+int32_t esl_lu_lanes_mixed_compiled_device(esl_ctx *ctx, const double *lead, uint32_t n_lanes,
+                                           const double *d_a, const double *d_rhs, double *d_dx,
+                                           uint8_t *d_bad, uint8_t *d_refine, float *ms);
+
+/* Host-only: the mixed form's CUDA source (as esl_lu_compiled_source). */
+int32_t esl_lu_compiled_mixed_source(uint32_t n, const uint32_t *col_ptr, const uint32_t *row_idx,
+                                     const double *lead, char *buf, size_t cap, size_t *len);
+
 /* The compiler's log of the context's compiled LU (ptxas register and spill
  * lines), "" before the first esl_lu_lanes_compiled_device call. */
 const char *esl_lu_compiled_log(const esl_ctx *ctx);

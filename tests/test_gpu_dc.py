@@ -193,6 +193,45 @@ def test_lu_lanes_compiled_bitwise(deck, seed):
 
 
 @pytest.mark.parametrize("deck,seed", [("grid", 0), ("ring", 1)])
+def test_lu_lanes_mixed_compiled_matches_interpreted(deck, seed):
+    """The mixed form compiled into code against the interpreted mixed
+    kernel on the same lanes: the same peel verdicts and correction counts,
+    dx within 1e-12 (the FP32 ops and the FP64 refinement run in the same
+    per-value order)."""
+    torch = _torch()
+    fr = decks.grid_diodes(seed=seed + 1)[0] if deck == "grid" else decks.ring_oscillator(lanes=2)[0]
+    cp, ri = oracle.pattern(fr)
+    n, nnz = fr.n, len(ri)
+    rng = np.random.default_rng(seed)
+    lead = rng.uniform(0.5, 2.0, nnz) * np.where(rng.random(nnz) < 0.5, 1, -1)
+    diag = np.array([np.searchsorted(ri[cp[j]:cp[j + 1]], j) + cp[j] for j in range(n)])
+    lead[diag] += 8.0
+    n_lanes = 333
+    vals = np.stack([lead * rng.uniform(0.8, 1.2, nnz) for _ in range(n_lanes)])
+    vals[5, diag[3]] = 0.0
+    rhs = rng.normal(size=(n_lanes, n))
+    ctx = lanes.DcLanes(fr)
+    d_a = torch.tensor(vals.T.copy(), dtype=torch.float64, device="cuda")
+    d_r = torch.tensor(rhs.T.copy(), dtype=torch.float64, device="cuda")
+    out = []
+    for call in (ctx.lu_lanes_mixed, ctx.lu_lanes_mixed_compiled):
+        d_dx = torch.zeros((n, n_lanes), dtype=torch.float64, device="cuda")
+        d_bad = torch.zeros(n_lanes, dtype=torch.uint8, device="cuda")
+        d_ref = torch.zeros(n_lanes, dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        call(lead, d_a.data_ptr(), d_r.data_ptr(), d_dx.data_ptr(), d_bad.data_ptr(), n_lanes, d_ref.data_ptr())
+        torch.cuda.synchronize()
+        out.append((d_dx.cpu().numpy().T, d_bad.cpu().numpy(), d_ref.cpu().numpy()))
+    ctx.close()
+    (dx_i, bad_i, ref_i), (dx_c, bad_c, ref_c) = out
+    assert np.array_equal(bad_i, bad_c)
+    good = bad_i == 0
+    assert good.sum() > n_lanes // 2
+    assert np.array_equal(ref_i[good], ref_c[good])
+    assert np.all(np.abs(dx_c[good] - dx_i[good]) <= 1e-12 * np.abs(dx_i[good]).max(axis=1, keepdims=True))
+
+
+@pytest.mark.parametrize("deck,seed", [("grid", 0), ("ring", 1)])
 def test_lu_lanes_mixed_refines_to_fp64(deck, seed):
     """FP32 refactor and solves with FP64 refinement: dx within 1e-9 of the
     oracle's FP64 replay (the refinement drives the residual below 1e-12 of
