@@ -121,10 +121,11 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_tran(fr, slots, values, threads, seconds):
+def cpu_tran(fr, slots, values, threads, seconds, keep=None):
     """The oracle's transient lanes on `threads` host threads (ctypes calls
     release the GIL), one lane per task, until `seconds` have passed (the
-    lanes started by then finish). Returns (lanes done, wall seconds)."""
+    lanes started by then finish). Returns (lanes done, wall seconds); with
+    keep a dict, keep[lane] = (step statistics, final x) of each lane run."""
     from oracle import oracle
     _, oo = tran_opts_pair()
     done = 0
@@ -133,13 +134,54 @@ def cpu_tran(fr, slots, values, threads, seconds):
     def run(i):
         if time.perf_counter() - t0 > seconds:
             return 0
-        _, _, _, st, _ = oracle.tran(fr, slots, values[i:i + 1], oo)
+        _, _, _, st, x = oracle.tran(fr, slots, values[i:i + 1], oo)
+        if keep is not None:
+            keep[i] = (st[0].copy(), x[0].copy())
         return int(st[0, 0] == 0)
 
     with cf.ThreadPoolExecutor(max_workers=threads) as ex:
         for c in ex.map(run, range(values.shape[0])):
             done += c
     return done, time.perf_counter() - t0
+
+
+def parity_block(keep, stats, x):
+    """The GPU lanes (stats [lanes][8], x [lanes][n] of the e2e run) against
+    the oracle's runs of the same lanes (keep, from the CPU baseline): how many
+    lanes took every step decision the oracle took, and the largest deviation
+    of their final solutions."""
+    idx = sorted(keep)
+    if not idx:
+        return {"lanes": 0}
+    so = np.stack([keep[i][0] for i in idx]).astype(np.int64)
+    xo = np.stack([keep[i][1] for i in idx])
+    sg = stats[idx].astype(np.int64)
+    xg = x[idx]
+    d = np.abs(xg - xo)
+    scale = np.maximum(np.abs(xg), np.abs(xo))
+    within = d <= 1e-12 + 1e-9 * scale
+    rel = np.where(d > 1e-12, d / np.maximum(scale, 1e-300), 0.0)
+    return {"lanes": len(idx), "decisions_equal": int((sg == so).all(axis=1).sum()),
+            "bitwise_equal": int((xg.view(np.uint64) == xo.view(np.uint64)).all(axis=1).sum()),
+            "within_tolerance": bool(within.all()), "max_abs_dev": float(d.max()),
+            "max_rel_dev": float(rel.max()),
+            "checked": "the step statistics (status, accepted, attempts, Newton iterations, Newton and LTE "
+                       "rejections, breakpoint landings, operating-point iterations) and the final solution "
+                       "of the lanes the CPU baseline ran, against the e2e run's; tolerance 1e-9 relative "
+                       "or 1e-12 absolute"}
+
+
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), for the baseline records."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
 
 
 def reference_arm(args, rank, world):
@@ -163,7 +205,7 @@ def reference_arm(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": cfg,
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "cpu": cpu_model(),
                          "sample": f"{args.steps} steps of {per_step} of the {values.shape[0]} lanes"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -591,9 +633,11 @@ def our_arm(args, rank, world):
     out["lu_roofline_warp_per_lane"] = lu_replay_roofline(fr, ctx, hbm_peak, peak_src)
     if args.cpu_baseline:
         threads = os.cpu_count() or 1
-        d, dt = cpu_tran(fr, slots, values, threads, args.cpu_seconds)
-        out["cpu_baseline"] = {"value": d / dt, "unit": UNIT, "cores": threads, "kind": "port",
+        keep = {}
+        d, dt = cpu_tran(fr, slots, values, threads, args.cpu_seconds, keep=keep)
+        out["cpu_baseline"] = {"value": d / dt, "unit": UNIT, "cores": threads, "kind": "port", "cpu": cpu_model(),
                                "sample": f"{d} of the {N} lanes in {dt:.1f} s"}
+        out["parity"] = parity_block(keep, sth, xh)
     print(json.dumps(out), flush=True)
     ctx.close()
 

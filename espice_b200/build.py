@@ -46,19 +46,40 @@ def stale():
     return any(os.path.getmtime(f) > t for f in sources() + headers())
 
 
+def _flags(verbose):
+    return [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3",
+            "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
+            "-Xptxas", "-v" if verbose else "-O3"]
+
+
 def build(force=False, verbose=False):
+    """Compiles each source to an object in _build/ (in parallel), then links
+    the shared library."""
     if not force and not stale():
         return LIB
-    cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3",
-           "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
-           "-Xptxas", "-v" if verbose else "-O3",
-           "-shared", "-o", LIB] + sources() + ["-lcudart", "-ldl"]
-    r = subprocess.run(cmd, capture_output=True, text=True)
+    from concurrent.futures import ThreadPoolExecutor
+
+    obj_dir = os.path.join(HERE, "_build")
+    os.makedirs(obj_dir, exist_ok=True)
+    objs = [os.path.join(obj_dir, os.path.basename(s) + ".o") for s in sources()]
+
+    def compile_one(i):
+        return subprocess.run(_flags(verbose) + ["-c", sources()[i], "-o", objs[i]],
+                              capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=len(objs)) as ex:
+        results = list(ex.map(compile_one, range(len(objs))))
+    for r in results:
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("nvcc failed building libespice_lanes.so")
+        if verbose:
+            sys.stderr.write(r.stderr)
+    r = subprocess.run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB] + objs
+                       + ["-lcudart", "-ldl"], capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libespice_lanes.so")
-    if verbose:
-        sys.stderr.write(r.stderr)
+        raise RuntimeError("nvcc failed linking libespice_lanes.so")
     return LIB
 
 

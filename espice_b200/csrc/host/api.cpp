@@ -833,7 +833,10 @@ int32_t ensure_lane_buffers(esl_ctx* ctx) {
 // Host factor + solve of the paused lanes (lane_solver.zig peel), then
 // resume. A lane's first host factor is its own fresh factor when it paused
 // at its first iterate; later it continues the lead tape's replay history.
-int32_t serve_pauses(esl_ctx* ctx, esl_stats* st, bool* any) {
+// The status and iteration words are the launch's own (L.status, L.iters:
+// the caller's device arrays for esl_dc_solve_device), the other hand-off
+// planes the context's.
+int32_t serve_pauses(esl_ctx* ctx, const LaneDev& L, esl_stats* st, bool* any) {
   cudaStream_t s = ctx->stream;
   uint32_t paused = 0;
   ESL_CUDA(cudaMemcpyAsync(&paused, ctx->d_paused.p, 4, cudaMemcpyDeviceToHost, s));
@@ -842,8 +845,8 @@ int32_t serve_pauses(esl_ctx* ctx, esl_stats* st, bool* any) {
   if (!paused) return ESL_OK;
   const uint32_t N = ctx->n_lanes, n = ctx->pat.n, nnz = ctx->pat.nnz();
   std::vector<uint32_t> status(N), iters(N), flags(N);
-  ESL_CUDA(cudaMemcpyAsync(status.data(), ctx->d_status.p, N * 4, cudaMemcpyDeviceToHost, s));
-  ESL_CUDA(cudaMemcpyAsync(iters.data(), ctx->d_iters.p, N * 4, cudaMemcpyDeviceToHost, s));
+  ESL_CUDA(cudaMemcpyAsync(status.data(), L.status, N * 4, cudaMemcpyDeviceToHost, s));
+  ESL_CUDA(cudaMemcpyAsync(iters.data(), L.iters, N * 4, cudaMemcpyDeviceToHost, s));
   ESL_CUDA(cudaMemcpyAsync(flags.data(), ctx->d_flags.p, N * 4, cudaMemcpyDeviceToHost, s));
   ESL_CUDA(cudaStreamSynchronize(s));
   std::vector<double> a(nnz), r(n), dx(n);
@@ -871,8 +874,8 @@ int32_t serve_pauses(esl_ctx* ctx, esl_stats* st, bool* any) {
     ESL_CUDA(cudaMemcpy(ctx->d_dx.as<double>() + size_t(l) * n, dx.data(), n * 8, cudaMemcpyHostToDevice));
     if (ds.lu.same_tape(ctx->lead)) flags[l] &= ~2u;
   }
-  ESL_CUDA(cudaMemcpyAsync(ctx->d_status.p, status.data(), N * 4, cudaMemcpyHostToDevice, s));
-  ESL_CUDA(cudaMemcpyAsync(ctx->d_iters.p, iters.data(), N * 4, cudaMemcpyHostToDevice, s));
+  ESL_CUDA(cudaMemcpyAsync(L.status, status.data(), N * 4, cudaMemcpyHostToDevice, s));
+  ESL_CUDA(cudaMemcpyAsync(L.iters, iters.data(), N * 4, cudaMemcpyHostToDevice, s));
   ESL_CUDA(cudaMemcpyAsync(ctx->d_flags.p, flags.data(), N * 4, cudaMemcpyHostToDevice, s));
   ESL_CUDA(cudaMemsetAsync(ctx->d_paused.p, 0, 4, s));
   return ESL_OK;
@@ -1069,7 +1072,7 @@ int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d
   uint32_t launches = 1;
   for (;;) {
     bool any = false;
-    if (int32_t rc = serve_pauses(ctx, st, &any)) return rc;
+    if (int32_t rc = serve_pauses(ctx, L, st, &any)) return rc;
     if (!any) break;
     LaneDev R = L;
     R.resume = 1;
@@ -1444,7 +1447,7 @@ int32_t esl_group_dc_solve_device(esl_ctx* const* ctxs, uint32_t n_ctx, const es
     uint32_t launches = 1;
     for (;;) {
       bool any = false;
-      if (int32_t rc = serve_pauses(x, stats ? &stats[c] : nullptr, &any)) return rc;
+      if (int32_t rc = serve_pauses(x, lanes[c], stats ? &stats[c] : nullptr, &any)) return rc;
       if (!any) break;
       LaneDev R = lanes[c];
       R.resume = 1;

@@ -413,20 +413,26 @@ int32_t esl_mlp_weights(esl_mlp* m, float* out) {
   return ESL_MLP_OK;
 }
 
-int32_t esl_gemm_bf16(const void* d_a, int lda, const void* d_b, int ldb, int M, int N, int K, const float* d_bias,
-                      float* d_c, int ldc, void* d_h, int ldh, int act) {
+int32_t esl_gemm_bf16_bounded(const void* d_a, int lda, const void* d_b, int ldb, int M, int N, int K,
+                              const float* d_bias, float* d_c, int ldc, void* d_h, int ldh, int act,
+                              uint32_t wait_rounds) {
   int* err = nullptr;
   if (cudaMalloc(&err, 4) != cudaSuccess) return ESL_MLP_OUT_OF_MEMORY;
   cudaMemset(err, 0, 4);
   cudaError_t e = esl::launch_gemm_bf16(static_cast<const __nv_bfloat16*>(d_a), lda,
                                         static_cast<const __nv_bfloat16*>(d_b), ldb, M, N, K, d_bias, d_c, ldc,
-                                        static_cast<__nv_bfloat16*>(d_h), ldh, act, err, nullptr);
+                                        static_cast<__nv_bfloat16*>(d_h), ldh, act, err, nullptr, wait_rounds);
   int h = 0;
   if (e == cudaSuccess) e = cudaMemcpy(&h, err, 4, cudaMemcpyDeviceToHost);
   cudaFree(err);
   if (e == cudaErrorInvalidValue) return ESL_MLP_INVALID_ARGUMENT;
   if (e != cudaSuccess) return ESL_MLP_DEVICE_FAULT;
   return h ? ESL_MLP_TIMEOUT : ESL_MLP_OK;
+}
+
+int32_t esl_gemm_bf16(const void* d_a, int lda, const void* d_b, int ldb, int M, int N, int K, const float* d_bias,
+                      float* d_c, int ldc, void* d_h, int ldh, int act) {
+  return esl_gemm_bf16_bounded(d_a, lda, d_b, ldb, M, N, K, d_bias, d_c, ldc, d_h, ldh, act, 0);
 }
 
 }  // extern "C"

@@ -48,11 +48,11 @@ __device__ __forceinline__ Dual dsqrt(Dual a) {
   return {s, a.g * h, a.d * h, a.b * h};
 }
 __device__ __forceinline__ Dual dexp(Dual a) {
-  const double e = exp(a.v);
+  const double e = esl_exp(a.v);
   return {e, a.g * e, a.d * e, a.b * e};
 }
 __device__ __forceinline__ Dual dlog(Dual a) {
-  return {log(a.v), div_rn(a.g, a.v), div_rn(a.d, a.v), div_rn(a.b, a.v)};
+  return {esl_log(a.v), div_rn(a.g, a.v), div_rn(a.d, a.v), div_rn(a.b, a.v)};
 }
 // a + c and c - a, c a constant
 __device__ __forceinline__ Dual daddk(Dual a, double c) { return {a.v + c, a.g, a.d, a.b}; }
@@ -343,7 +343,7 @@ __device__ __forceinline__ void b3_jcur(double v, double isat, double nvt, doubl
     g = div_rn(isevjm, nvt) + gmin;
   } else {
     const double u = fmin(div_rn(v, nvt), 80.0);
-    const double e = exp(u);
+    const double e = esl_exp(u);
     i = isat * (e * (1.0 + (div_rn(v, nvt) - u)) - 1.0) + gmin * v;
     g = div_rn(isat * e, nvt) + gmin;
   }

@@ -53,8 +53,8 @@ __device__ __forceinline__ uint32_t core_offset(uint32_t r, uint32_t k) {
   return ((r >> 3) * (kTileK / 8) + (k >> 3)) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_t limit) {
+  for (uint32_t i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -86,7 +86,8 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32
 __global__ void __launch_bounds__(kThreads) gemm_bf16_tc(const __nv_bfloat16* __restrict__ a, int lda,
                                                          const __nv_bfloat16* __restrict__ b, int ldb, int M, int K,
                                                          int bn, const float* __restrict__ bias, float* c, int ldc,
-                                                         __nv_bfloat16* h, int ldh, int act, int* err) {
+                                                         __nv_bfloat16* h, int ldh, int act, int* err,
+                                                         uint32_t wait_limit) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const uint32_t a_bytes = kTileM * kTileK * 2, b_bytes = uint32_t(bn) * kTileK * 2;
   unsigned char* buf[2] = {smem, smem + a_bytes + b_bytes};
@@ -160,7 +161,14 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tc(const __nv_bfloat16* __
     }
     // the other buffer's last reader (chunk q - 1) completed at the previous wait
     if (q + 1 < n_chunks) stage(q + 1);
-    ok = mbar_wait(smem_u32(&bar), parity) && ok;
+    if (!mbar_wait(smem_u32(&bar), parity, wait_limit)) {
+      // The wait ran out: the result is not stored (err is raised), but the
+      // MMAs still read the staging buffer and write the accumulator, so
+      // drain them (again bounded) before the buffer is refilled or the
+      // tensor memory freed.
+      ok = false;
+      mbar_wait(smem_u32(&bar), parity, kWaitLimit);
+    }
     parity ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;");
   }
@@ -290,7 +298,7 @@ __global__ void to_bf16(const float* in, int n, __nv_bfloat16* out) {
 
 cudaError_t launch_gemm_bf16(const __nv_bfloat16* a, int lda, const __nv_bfloat16* b, int ldb, int M, int N, int K,
                              const float* bias, float* c, int ldc, __nv_bfloat16* h, int ldh, int act, int* err,
-                             cudaStream_t s) {
+                             cudaStream_t s, uint32_t wait_rounds) {
   if (M <= 0 || N <= 0 || K <= 0 || K % 16 || N % 16 || lda % 8 || ldb % 8) return cudaErrorInvalidValue;
   int bn = N <= 256 ? N : 128;
   while (N % bn) bn -= 16;
@@ -301,7 +309,8 @@ cudaError_t launch_gemm_bf16(const __nv_bfloat16* a, int lda, const __nv_bfloat1
   cudaError_t e = cudaFuncSetAttribute(gemm_bf16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   dim3 grid((M + kTileM - 1) / kTileM, N / bn);
-  gemm_bf16_tc<<<grid, kThreads, smem, s>>>(a, lda, b, ldb, M, K, bn, bias, c, ldc, h, ldh, act, err);
+  gemm_bf16_tc<<<grid, kThreads, smem, s>>>(a, lda, b, ldb, M, K, bn, bias, c, ldc, h, ldh, act, err,
+                                            wait_rounds == 0 ? kWaitLimit : wait_rounds == ~0u ? 0u : wait_rounds);
   return cudaGetLastError();
 }
 

@@ -12,6 +12,7 @@
 #include <math_constants.h>
 
 #include "../common.h"
+#include "../esl_math.h"
 
 namespace esl {
 
@@ -65,12 +66,12 @@ __device__ __forceinline__ void diode_iv(const double* r, int s, double vd, doub
   if (vd >= -3.0 * vte) {
     const double u = div_rn(vd, vte);
     const double ulim = fmin(u, 80.0);
-    const double e = exp(ulim);
+    const double e = esl_exp(ulim);
     id = is * ((e * (1.0 + (u - ulim))) - 1.0);
     gd = div_rn(is * e, vte);
   } else {
     const double a = div_rn(3.0 * vte, vd * 2.718281828459045);
-    const double a3 = pow(a, 3.0);
+    const double a3 = esl_pow(a, 3.0);
     id = -is * (1.0 + a3);
     gd = div_rn(3.0 * is * a3, vd);
   }
@@ -79,7 +80,7 @@ __device__ __forceinline__ void diode_iv(const double* r, int s, double vd, doub
     const double vtb = r[kDVtebrk * s];
     const double wb = div_rn(-(xbv + vd), vtb);
     const double wlim = fmin(wb, 80.0);
-    const double e = exp(wlim);
+    const double e = esl_exp(wlim);
     id = -is * e * (1.0 + (wb - wlim));
     gd = div_rn(is * e, vtb);
   }
@@ -98,11 +99,11 @@ __device__ __forceinline__ void diode_qc(const double* r, int s, double vd, doub
     const double vfc = fc * vj;
     if (vd < vfc) {
       const double b = 1.0 - div_rn(vd, vj);
-      qj = div_rn(cjo * vj * (1.0 - pow(b, 1.0 - mt)), 1.0 - mt);
-      cj = cjo * pow(b, -mt);
+      qj = div_rn(cjo * vj * (1.0 - esl_pow(b, 1.0 - mt)), 1.0 - mt);
+      cj = cjo * esl_pow(b, -mt);
     } else {
-      const double f1 = vj * (1.0 - pow(1.0 - fc, 1.0 - mt)) / (1.0 - mt);
-      const double f2 = pow(1.0 - fc, 1.0 + mt);
+      const double f1 = vj * (1.0 - esl_pow(1.0 - fc, 1.0 - mt)) / (1.0 - mt);
+      const double f2 = esl_pow(1.0 - fc, 1.0 + mt);
       const double f3 = 1.0 - fc * (1.0 + mt);
       qj = cjo * (f1 + (1.0 / f2) * (f3 * (vd - vfc) + (mt / (2.0 * vj)) * (vd * vd - vfc * vfc)));
       cj = cjo * ((1.0 / f2) * (f3 + (mt / vj) * vd));
@@ -122,10 +123,10 @@ __device__ __forceinline__ double pnjlim_dev(double vnew, double vold, double vt
   if (vnew > vcrit && fabs(vnew - vold) > vt + vt) {
     if (vold > 0) {
       const double arg = div_rn(vnew - vold, vt);
-      if (arg > 0) vnew = vold + vt * (2 + log(arg - 2));
-      else vnew = vold - vt * (2 + log(2 - arg));
+      if (arg > 0) vnew = vold + vt * (2 + esl_log(arg - 2));
+      else vnew = vold - vt * (2 + esl_log(2 - arg));
     } else {
-      vnew = vt * log(div_rn(vnew, vt));
+      vnew = vt * esl_log(div_rn(vnew, vt));
     }
     lim = true;
   } else if (vnew < 0) {
@@ -240,7 +241,7 @@ __device__ __forceinline__ double limvds_dev(double vnew, double vold) {
 __device__ __forceinline__ void mos_jcur(double v, double isat, double vtx, double gm, double& i, double& g) {
   if (v > -3.0 * vtx) {
     const double u = fmin(div_rn(v, vtx), 80.0);
-    const double e = exp(u);
+    const double e = esl_exp(u);
     i = isat * (e * (1.0 + (div_rn(v, vtx) - u)) - 1.0) + gm * v;
     g = div_rn(isat * e, vtx) + gm;
   } else {
@@ -266,8 +267,8 @@ __device__ __forceinline__ void mos_jchg(double v, double cz, double czsw, doubl
     c = 0.0;
   } else if (v < fcx * pbx) {
     const double a = 1.0 - div_rn(v, pbx);
-    q = pbx * (div_rn(cz * (1.0 - pow(a, 1.0 - mjx)), 1.0 - mjx) + div_rn(czsw * (1.0 - pow(a, 1.0 - mjswx)), 1.0 - mjswx));
-    c = cz * pow(a, -mjx) + czsw * pow(a, -mjswx);
+    q = pbx * (div_rn(cz * (1.0 - esl_pow(a, 1.0 - mjx)), 1.0 - mjx) + div_rn(czsw * (1.0 - esl_pow(a, 1.0 - mjswx)), 1.0 - mjswx));
+    c = cz * esl_pow(a, -mjx) + czsw * esl_pow(a, -mjswx);
   } else {
     q = f4 + v * (f2 + 0.5 * f3 * v);
     c = f2 + f3 * v;

@@ -38,9 +38,10 @@ u8p = ctypes.POINTER(ctypes.c_uint8)
 
 
 class LaneError(RuntimeError):
-    def __init__(self, code, what):
+    def __init__(self, code, what, paused=0):
         super().__init__(f"espice_lanes error {code}: {what}")
         self.code = code
+        self.paused = paused  # esl_dc_solve_device_static: lanes left paused
 
 
 class NewtonOpts(ctypes.Structure):
@@ -322,11 +323,12 @@ class DcLanes:
         a nonzero count raises with ESL_NOT_ELIGIBLE)."""
         opts = opts or newton_opts()
         paused = ctypes.c_uint32(0)
-        self._check(self._L.esl_dc_solve_device_static(self._ctx, ctypes.byref(opts),
-                                                       ctypes.c_void_p(d_x), ctypes.c_int(int(cold)),
-                                                       ctypes.c_void_p(d_iters), ctypes.c_void_p(d_status),
-                                                       ctypes.byref(paused)),
-                    "esl_dc_solve_device_static")
+        rc = self._L.esl_dc_solve_device_static(self._ctx, ctypes.byref(opts), ctypes.c_void_p(d_x),
+                                                ctypes.c_int(int(cold)), ctypes.c_void_p(d_iters),
+                                                ctypes.c_void_p(d_status), ctypes.byref(paused))
+        if rc:
+            raise LaneError(rc, "esl_dc_solve_device_static: " + self._L.esl_last_error(self._ctx).decode(),
+                            paused=paused.value)
         return paused.value
 
     def tran(self, opts, probes=(), max_pts=0):

@@ -13,7 +13,11 @@ import numpy as np
 from . import lanes
 
 EXPORTS = ["esl_mlp_create", "esl_mlp_destroy", "esl_mlp_last_error", "esl_mlp_set_scaling", "esl_mlp_train",
-           "esl_mlp_predict", "esl_mlp_gradients", "esl_mlp_shapes", "esl_mlp_weights", "esl_gemm_bf16"]
+           "esl_mlp_predict", "esl_mlp_gradients", "esl_mlp_shapes", "esl_mlp_weights", "esl_gemm_bf16",
+           "esl_gemm_bf16_bounded"]
+
+GEMM_NO_WAIT = 0xFFFFFFFF  # ESL_GEMM_NO_WAIT: every completion wait runs out at once
+MLP_TIMEOUT = 7
 
 f32p = ctypes.POINTER(ctypes.c_float)
 i32p = ctypes.POINTER(ctypes.c_int)
@@ -40,10 +44,13 @@ class MlpError(RuntimeError):
         self.code = code
 
 
-def gemm_bf16(d_a, lda, d_b, ldb, M, N, K, d_c, ldc, d_bias=0, d_h=0, ldh=0, act=0):
-    rc = _lib().esl_gemm_bf16(ctypes.c_void_p(d_a), lda, ctypes.c_void_p(d_b), ldb, M, N, K,
-                              ctypes.c_void_p(d_bias) if d_bias else None, ctypes.c_void_p(d_c), ldc,
-                              ctypes.c_void_p(d_h) if d_h else None, ldh, act)
+def gemm_bf16(d_a, lda, d_b, ldb, M, N, K, d_c, ldc, d_bias=0, d_h=0, ldh=0, act=0, wait_rounds=0):
+    """esl_gemm_bf16 (wait_rounds 0), or esl_gemm_bf16_bounded with that
+    bound on the tensor-core completion waits."""
+    rc = _lib().esl_gemm_bf16_bounded(ctypes.c_void_p(d_a), lda, ctypes.c_void_p(d_b), ldb, M, N, K,
+                                      ctypes.c_void_p(d_bias) if d_bias else None, ctypes.c_void_p(d_c), ldc,
+                                      ctypes.c_void_p(d_h) if d_h else None, ldh, act,
+                                      ctypes.c_uint32(wait_rounds))
     if rc:
         raise MlpError(rc, "esl_gemm_bf16")
 

@@ -7,8 +7,8 @@
  * src/analysis/gpu_lanes.zig (GpuLanes.init / newton / deinit,
  * gpu_lanes.zig:349-845) under tran.runGpuLanes (tran.zig:1654) and, on the
  * CPU, sweep/lanes.solveBatch (sweep/lanes.zig:186-233). A Zig host would
- * call these entry points where gpu_lanes.zig launches its kernels; the
- * bindings a maintainer adds are in INTEGRATION.md.
+ * call these entry points where gpu_lanes.zig launches its kernels, through
+ * an `extern` block that declares them with the same C types.
  *
  * Threading: calls on one context must be serialized (the rule of
  * include/espice.h:139-156 for a problem handle). Each context owns one CUDA
@@ -167,7 +167,11 @@ int32_t esl_dc_solve_device(esl_ctx *ctx, const esl_newton_opts *opts, double *d
  *
  * Set-up: the first call on a device looks up the array's address, and the
  * first call on a context reserves its error-message buffer; make that
- * first call before any stream capture begins. The context needs its pivot
+ * first call before any stream capture begins. The address is kept for the
+ * life of the process: a cudaDeviceReset on that device (which also frees
+ * every context's device memory) is not supported while the library is
+ * loaded. Each call waits for its stream before it returns (it reads the
+ * paused-lane count back to the host). The context needs its pivot
  * tape (one esl_dc_solve_device call on it first) and its lanes (esl_set_lanes).
  * Nothing has to start at zero: the call writes every lane's start state and
  * clears the counter itself. Calls overlapping in time on one device (any

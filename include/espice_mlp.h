@@ -68,6 +68,18 @@ int32_t esl_mlp_weights(esl_mlp *m, float *out);
 int32_t esl_gemm_bf16(const void *d_a, int lda, const void *d_b, int ldb, int M, int N, int K,
                       const float *d_bias, float *d_c, int ldc, void *d_h, int ldh, int act);
 
+/* esl_gemm_bf16 with its tensor-core completion wait bounded by wait_rounds
+ * mbarrier try_wait rounds per K chunk (0: the library's bound, 2^20;
+ * ESL_GEMM_NO_WAIT: no round, so every wait runs out at once). When a wait
+ * runs out the kernel drains the chunk's MMAs (under the library's bound)
+ * before it reuses their staging buffer or frees the accumulator's tensor
+ * memory, stores nothing, and the call returns ESL_MLP_TIMEOUT. The tests
+ * use ESL_GEMM_NO_WAIT to check that path. */
+#define ESL_GEMM_NO_WAIT 0xffffffffu
+int32_t esl_gemm_bf16_bounded(const void *d_a, int lda, const void *d_b, int ldb, int M, int N, int K,
+                              const float *d_bias, float *d_c, int ldc, void *d_h, int ldh, int act,
+                              uint32_t wait_rounds);
+
 #ifdef __cplusplus
 }
 #endif

@@ -118,6 +118,8 @@ int orc_params_per(uint32_t type);
  * k of the instance is xloc[k]), no limiting: residuals f[6] and Jacobian
  * J[6][6] over its local nodes, row-major. A test hook for the models'
  * derivatives. Returns 0, or 1 for an unknown type. */
+/* The model code's exp (which 0), log (1) or pow (2) over n arguments. */
+void orc_math(int which, uint32_t n, const double *x, const double *y, double *out);
 int orc_dev_stamp(uint32_t type, const double *prm, const double *xloc, double *f, double *J);
 
 /* Pattern (Circuit.freeze): CSC with every diagonal, rows ascending.
@@ -160,6 +162,13 @@ int orc_dc_points(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
                   const double *values, uint32_t n_lanes, const double *warm,
                   const orc_newton_opts *opts, double *x_out, uint32_t *iters,
                   uint8_t *conv);
+/* orc_dc_points recording each lane's gate inputs per iterate: trace
+ * [n_lanes][cap][3] = (delta score, max |rhs_i| / residual gate, limited
+ * flag), NaN past the lane's last iterate. */
+int orc_dc_points_trace(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
+                        const double *values, uint32_t n_lanes, const double *warm,
+                        const orc_newton_opts *opts, double *x_out, uint32_t *iters,
+                        uint8_t *conv, double *trace, uint32_t cap);
 
 /* Sequential .dc sweep (dc.zig Sweep): point 0 cold, later points warm
  * from the 2*last - prev predictor limited against the last point; a failed

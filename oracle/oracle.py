@@ -16,8 +16,12 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
+# The same restatement with the host C library's exp, log and pow in the
+# model code (liboracle.so uses the kernels' shared esl_math.h functions).
+LIB_LIBM = os.path.join(HERE, "liboracle_libm.so")
 
 _lib = None
+_lib_libm = None
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 f64p = ctypes.POINTER(ctypes.c_double)
@@ -39,8 +43,16 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-def lib():
-    global _lib
+def lib(libm=False):
+    """The oracle library; libm=True: the variant with the C library's
+    transcendentals in the model code."""
+    global _lib, _lib_libm
+    if libm:
+        if _lib_libm is None:
+            if not os.path.exists(LIB_LIBM):
+                build()
+            _lib_libm = ctypes.CDLL(LIB_LIBM)
+        return _lib_libm
     if _lib is None:
         if not os.path.exists(LIB):
             build()
@@ -144,6 +156,41 @@ def dc_points(frozen, slots, values, warm=None, opts=None):
                              _p(x, f64p), _p(it, u32p), _p(cv, u8p))
     assert rc == 0
     return x, it, cv
+
+
+def math(which, x, y=None, libm=False):
+    """The model code's exp ("exp"), log ("log") or pow ("pow") over arrays."""
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.ascontiguousarray(np.zeros_like(x) if y is None else y, np.float64)
+    out = np.zeros_like(x)
+    lib(libm).orc_math(ctypes.c_int({"exp": 0, "log": 1, "pow": 2}[which]), ctypes.c_uint32(x.size),
+                       _p(x, f64p), _p(y, f64p), _p(out, f64p))
+    return out
+
+
+def dc_points_trace(frozen, slots, values, warm=None, opts=None, cap=100, libm=False):
+    """dc_points with every lane's gate inputs per iterate: trace
+    [lanes][cap][3] = (delta score, max |rhs_i| / residual gate, limited),
+    NaN past the lane's last iterate. libm=True runs the variant with the C
+    library's exp, log and pow."""
+    opts = opts or newton_opts()
+    values = np.ascontiguousarray(values, np.float64).reshape(-1, max(1, len(slots)))
+    lanes = values.shape[0]
+    x = np.zeros((lanes, frozen.n))
+    it = np.zeros(lanes, np.uint32)
+    cv = np.zeros(lanes, np.uint8)
+    tr = np.zeros((lanes, cap, 3))
+    sa = frozen.slots_array(slots)
+    wp = None
+    if warm is not None:
+        warm = np.ascontiguousarray(warm, np.float64)
+        wp = _p(warm, f64p)
+    rc = lib(libm).orc_dc_points_trace(ctypes.byref(frozen.struct()), sa, ctypes.c_uint32(len(slots)),
+                                       _p(values, f64p), ctypes.c_uint32(lanes), wp, ctypes.byref(opts),
+                                       _p(x, f64p), _p(it, u32p), _p(cv, u8p), _p(tr, f64p),
+                                       ctypes.c_uint32(cap))
+    assert rc == 0
+    return x, it, cv, tr
 
 
 def dc_sweep(frozen, slot, values, opts=None):

@@ -343,12 +343,12 @@ static dual dsqrt(dual a) {
     return r;
 }
 static dual dexp(dual a) {
-    const double e = exp(a.v);
+    const double e = esl_exp(a.v);
     dual r = {e, a.g * e, a.d * e, a.b * e};
     return r;
 }
 static dual dlog(dual a) {
-    dual r = {log(a.v), a.g / a.v, a.d / a.v, a.b / a.v};
+    dual r = {esl_log(a.v), a.g / a.v, a.d / a.v, a.b / a.v};
     return r;
 }
 /* a + c and c - a, c a constant */
@@ -372,7 +372,7 @@ static void b3_jcur(double v, double isat, double nvt, double vjm, double isevjm
         *g = isevjm / nvt + gmin;
     } else {
         const double u = fmin(v / nvt, 80.0);
-        const double e = exp(u);
+        const double e = esl_exp(u);
         *i = isat * (e * (1.0 + (v / nvt - u)) - 1.0) + gmin * v;
         *g = isat * e / nvt + gmin;
     }

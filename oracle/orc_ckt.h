@@ -26,6 +26,8 @@ typedef struct {
     double *st;                 /* committed state, then staged state */
     double *dx, *x_old;
     double last_scaled;
+    double *trace;              /* optional per-iterate gate inputs (orc_dc_points_trace) */
+    uint32_t trace_cap;
     sim_t sim;
     dsv_t dsv;
     /* transient companion hook (integrator.zig Hook): when `tran`, the

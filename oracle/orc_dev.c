@@ -164,10 +164,10 @@ double pnjlim(double vnew, double vold, double vt, double vcrit, int *lim) {
     if (vnew > vcrit && fabs(vnew - vold) > vt + vt) {
         if (vold > 0) {
             double arg = (vnew - vold) / vt;
-            if (arg > 0) vnew = vold + vt * (2 + log(arg - 2));
-            else vnew = vold - vt * (2 + log(2 - arg));
+            if (arg > 0) vnew = vold + vt * (2 + esl_log(arg - 2));
+            else vnew = vold - vt * (2 + esl_log(2 - arg));
         } else {
-            vnew = vt * log(vnew / vt);
+            vnew = vt * esl_log(vnew / vt);
         }
         *lim = 1;
     } else if (vnew < 0) {
@@ -297,19 +297,19 @@ static void diode_iv(const double *d, double vd, double *i, double *g) {
     if (vd >= -3.0 * vte) {
         double u = vd / vte;
         double ulim = u < 80.0 ? u : 80.0;
-        double e = exp(ulim);
+        double e = esl_exp(ulim);
         id = is * ((e * (1.0 + (u - ulim))) - 1.0);
         gd = is * e / vte;
     } else {
         double a = 3.0 * vte / (vd * 2.718281828459045);
-        double a3 = pow(a, 3.0);
+        double a3 = esl_pow(a, 3.0);
         id = -is * (1.0 + a3);
         gd = 3.0 * is * a3 / vd;
     }
     if (d[DD_BV] > 0.0 && vd < -3.0 * vte && vd < -d[DD_XBV]) {
         double wb = -(d[DD_XBV] + vd) / d[DD_VTEBRK];
         double wlim = wb < 80.0 ? wb : 80.0;
-        double e = exp(wlim);
+        double e = esl_exp(wlim);
         id = -is * e * (1.0 + (wb - wlim));
         gd = is * e / d[DD_VTEBRK];
     }
@@ -325,11 +325,11 @@ static void diode_qc(const double *d, double vd, double itot, double gtot, doubl
         double vfc = fc * vj;
         if (vd < vfc) {
             double b = 1.0 - vd / vj;
-            qj = cjo * vj * (1.0 - pow(b, 1.0 - mt)) / (1.0 - mt);
-            cj = cjo * pow(b, -mt);
+            qj = cjo * vj * (1.0 - esl_pow(b, 1.0 - mt)) / (1.0 - mt);
+            cj = cjo * esl_pow(b, -mt);
         } else {
-            double f1 = vj * (1.0 - pow(1.0 - fc, 1.0 - mt)) / (1.0 - mt);
-            double f2 = pow(1.0 - fc, 1.0 + mt);
+            double f1 = vj * (1.0 - esl_pow(1.0 - fc, 1.0 - mt)) / (1.0 - mt);
+            double f2 = esl_pow(1.0 - fc, 1.0 + mt);
             double f3 = 1.0 - fc * (1.0 + mt);
             qj = cjo * (f1 + (1.0 / f2) * (f3 * (vd - vfc) + (mt / (2.0 * vj)) * (vd * vd - vfc * vfc)));
             cj = cjo * ((1.0 / f2) * (f3 + (mt / vj) * vd));
@@ -525,4 +525,12 @@ int orc_dev_stamp(uint32_t type, const double *prm, const double *xloc, double *
         for (int c = 0; c < ORC_MAX_U; c++) J[r * ORC_MAX_U + c] = o.J[r][c];
     }
     return 0;
+}
+
+/* The model code's exp, log and pow (esl_math.h's, or the C library's in
+ * the libm build) for the accuracy tests: which 0 exp(x), 1 log(x),
+ * 2 pow(x, y); n values from x (and y) into out. */
+void orc_math(int which, uint32_t n, const double *x, const double *y, double *out) {
+    for (uint32_t i = 0; i < n; i++)
+        out[i] = which == 0 ? esl_exp(x[i]) : which == 1 ? esl_log(x[i]) : esl_pow(x[i], y[i]);
 }

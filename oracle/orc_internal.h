@@ -4,6 +4,21 @@
 
 #include "espice_oracle.h"
 
+/* exp, log and pow of the bias-dependent model code: the functions the CUDA
+ * kernels use (espice_b200/csrc/esl_math.h), so that the oracle's model
+ * evaluations are bitwise the device's. Built with ORC_LIBM_TRANSCENDENTALS
+ * (liboracle_libm.so) they are the host C library's instead, which shows
+ * what the choice changes: only last-ulp differences that move a Newton
+ * gate sitting at its threshold. */
+#ifdef ORC_LIBM_TRANSCENDENTALS
+#include <math.h>
+#define esl_exp exp
+#define esl_log log
+#define esl_pow pow
+#else
+#include "../espice_b200/csrc/esl_math.h"
+#endif
+
 #define NONE 0xffffffffu
 #define ORC_MAX_U 6
 #define ORC_MAX_E 40

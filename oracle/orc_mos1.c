@@ -132,7 +132,7 @@ int mos1_has_charge(const double *der) { return der[MD_HASQ] != 0.0; }
 static void jcur(double v, double isat, double vtx, double gm, double *i, double *g) {
     if (v > -3.0 * vtx) {
         double u = fmin(v / vtx, 80.0);
-        double e = exp(u);
+        double e = esl_exp(u);
         *i = isat * (e * (1.0 + (v / vtx - u)) - 1.0) + gm * v;
         *g = isat * e / vtx + gm;
     } else {
@@ -159,8 +159,8 @@ static void jchg(double v, double cz, double czsw, double pbx, double mjx, doubl
         *c = 0.0;
     } else if (v < fcx * pbx) {
         double a = 1.0 - v / pbx;
-        *q = pbx * (cz * (1.0 - pow(a, 1.0 - mjx)) / (1.0 - mjx) + czsw * (1.0 - pow(a, 1.0 - mjswx)) / (1.0 - mjswx));
-        *c = cz * pow(a, -mjx) + czsw * pow(a, -mjswx);
+        *q = pbx * (cz * (1.0 - esl_pow(a, 1.0 - mjx)) / (1.0 - mjx) + czsw * (1.0 - esl_pow(a, 1.0 - mjswx)) / (1.0 - mjswx));
+        *c = cz * esl_pow(a, -mjx) + czsw * esl_pow(a, -mjswx);
     } else {
         *q = f4 + v * (f2 + 0.5 * f3 * v);
         *c = f2 + f3 * v;

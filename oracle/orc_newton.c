@@ -288,6 +288,18 @@ int ckt_newton(ckt_t *k, double *x, const orc_newton_opts *opts, int init_fix, u
                 }
         }
         k->last_scaled = scaled;
+        if (k->trace && iter < k->trace_cap) {
+            /* the gate inputs of this iterate: the delta score, the largest
+               |rhs_i| / residual gate, whether a junction was limited */
+            double worst_res = 0;
+            for (uint32_t i = 0; i < n; i++) {
+                double r = fabs(k->rhs[i]) / residual_gate(opts, v[k->diag[i]], x[i]);
+                if (r > worst_res || r != r) worst_res = r;
+            }
+            k->trace[3 * iter] = scaled;
+            k->trace[3 * iter + 1] = worst_res;
+            k->trace[3 * iter + 2] = limited;
+        }
         if (ok) {
             if (init_fix) {
                 init_fix = 0;
@@ -348,6 +360,34 @@ int orc_dc_points(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
         int rc = ckt_run(&k, x, opts, 0, &it);
         conv[l] = rc == 0;
         iters[l] = rc == 2 ? 0 : it;
+        ckt_free(&k);
+    }
+    return 0;
+}
+
+/* orc_dc_points with each lane's gate inputs per iterate: trace
+ * [n_lanes][cap][3] = (delta score, max |rhs_i| / residual gate, limited),
+ * NaN past the lane's last iterate. */
+int orc_dc_points_trace(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
+                        const double *values, uint32_t n_lanes, const double *warm,
+                        const orc_newton_opts *opts, double *x_out, uint32_t *iters,
+                        uint8_t *conv, double *trace, uint32_t cap) {
+    uint32_t n = c->n;
+    for (size_t i = 0; i < (size_t)n_lanes * cap * 3; i++) trace[i] = NAN;
+    for (uint32_t l = 0; l < n_lanes; l++) {
+        ckt_t k;
+        if (ckt_init(&k, c)) return 1;
+        k.trace = trace + (size_t)l * cap * 3;
+        k.trace_cap = cap;
+        for (uint32_t s = 0; s < n_slots; s++) ckt_set(&k, slots[s], values[(size_t)l * n_slots + s]);
+        double *x = x_out + (size_t)l * n;
+        if (warm) memcpy(x, warm, sizeof(double) * n);
+        else ckt_cold_start(&k, x);
+        uint32_t it = 0;
+        int rc = ckt_run(&k, x, opts, 0, &it);
+        conv[l] = rc == 0;
+        iters[l] = rc == 2 ? 0 : it;
+        k.trace = NULL;
         ckt_free(&k);
     }
     return 0;

@@ -7,6 +7,9 @@
   which rounds to BF16 where the GPU does: relative error of each gradient
   tensor below 1e-3 (FP32 summation order, and a BF16 rounding it flips).
 - Training on the GPU fits a smooth map.
+- A completion wait that runs out (every wait bounded to no rounds) raises
+  the timeout status and stores nothing; the next unbounded GEMM on the same
+  device is correct (the drained MMAs left the context usable).
 """
 
 import numpy as np
@@ -103,3 +106,22 @@ def test_training_fits_a_smooth_map():
     err = np.abs(out.cpu().numpy() - y).mean()
     assert err < 0.1
     net.close()
+
+
+def test_gemm_wait_runs_out_and_stores_nothing():
+    torch = _torch()
+    M, N, K = 256, 128, 192
+    g = torch.Generator().manual_seed(7)
+    a = torch.randn(M, K, generator=g).to(torch.bfloat16).cuda()
+    b = torch.randn(N, K, generator=g).to(torch.bfloat16).cuda()
+    c = torch.full((M, N), 12345.0, device="cuda")
+    torch.cuda.synchronize()
+    with pytest.raises(mlp.MlpError) as err:
+        mlp.gemm_bf16(a.data_ptr(), K, b.data_ptr(), K, M, N, K, c.data_ptr(), N, wait_rounds=mlp.GEMM_NO_WAIT)
+    assert err.value.code == mlp.MLP_TIMEOUT
+    torch.cuda.synchronize()
+    assert bool((c == 12345.0).all()), "a timed-out GEMM stored results"
+    mlp.gemm_bf16(a.data_ptr(), K, b.data_ptr(), K, M, N, K, c.data_ptr(), N)
+    torch.cuda.synchronize()
+    ref = a.double().cpu() @ b.double().cpu().T
+    assert torch.allclose(c.double().cpu(), ref, rtol=1e-5, atol=1e-4)

@@ -96,6 +96,44 @@ def test_ring_oscillator_short_window():
     assert (res_g[3][:, 0] == lanes.TRAN_DONE).all()
 
 
+def test_ring_oscillator_headline_window():
+    """The bench's headline workload at its own window: 64 of its 1,024
+    Monte-Carlo ring samples (seed 1, every 16th lane), each over the full
+    20 ns with the 1 ps maximum step (about 20,000 accepted steps and 40,000
+    Newton iterations a lane). Every step decision equal to the oracle's
+    (accepted steps, attempts, Newton and LTE rejections, breakpoint
+    landings, operating-point and transient Newton iterations) and the final
+    solution within 1e-9 relative or 1e-12 absolute. The oracle's lanes run on
+    all host threads."""
+    import concurrent.futures as cf
+    import os
+
+    fr, slots, values = decks.ring_oscillator(seed=1, lanes=1024)
+    values = values[::16]
+    go = lanes.tran_opts(decks.RING_T_STOP, decks.RING_T_STEP, decks.RING_T_MAX, max_steps=200_000)
+    oo = oracle.tran_opts(decks.RING_T_STOP, decks.RING_T_STEP, decks.RING_T_MAX, max_steps=200_000)
+    ctx = lanes.DcLanes(fr)
+    ctx.set_lanes(slots, values)
+    _, _, _, sg, xg, _ = ctx.tran(go)
+    ctx.close()
+
+    def one(i):
+        _, _, _, so, xo = oracle.tran(fr, slots, values[i:i + 1], oo)
+        return so[0], xo[0]
+
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        res = list(ex.map(one, range(len(values))))
+    so = np.stack([r[0] for r in res])
+    xo = np.stack([r[1] for r in res])
+    for k, name in enumerate(lanes.TS_FIELDS):
+        if name in DECISIONS:
+            bad = np.flatnonzero(sg[:, k] != so[:, k])
+            assert len(bad) == 0, f"{name} differs on lanes {bad}: gpu {sg[bad, k]} oracle {so[bad, k]}"
+    assert (sg[:, 0] == lanes.TRAN_DONE).all()
+    assert (sg[:, 1] > 15_000).all(), sg[:, 1]
+    assert _close(xg, xo).all(), float(np.max(np.abs(xg - xo)))
+
+
 TRAN_FIXTURES = [n for n in gu.names("tran__") if gu.load(n)["plots"]]
 
 

@@ -76,6 +76,48 @@ def test_static_entry_matches_device_entry(cold):
     ctx.close()
 
 
+def test_static_entry_leaves_paused_lanes_to_the_caller():
+    """A zener regulator swept into breakdown: some lanes leave the lead
+    pivot tape. Twice in a row, the allocation-free call refuses with
+    ESL_NOT_ELIGIBLE, reports exactly the lanes it left at
+    ESL_LANE_NEED_SOLVE, and every other lane ends as the allocating entry
+    point's does, bit for bit."""
+    import golden_util as gu
+    from netlist import Deck, sweep_values
+
+    torch = _torch()
+    g = gu.load("dc__bench_power_zener_reg")
+    deck = Deck(g["deck"])
+    fr = deck.circuit().freeze()
+    an = deck.analysis
+    values = np.array(sweep_values(an[2], an[3], an[4])).reshape(-1, 1)
+    slots = [fr.slot(an[1], "dc")]
+    opts = lanes.newton_opts(**deck.newton_opts())
+    ctx = lanes.DcLanes(fr)
+    ctx.set_lanes(slots, values)
+    x0 = np.zeros((len(values), fr.n))
+    ref_bufs = _buffers(torch, x0)
+    torch.cuda.synchronize()
+    stats = ctx.solve_device(*_ptrs(ref_bufs), cold=True, opts=opts)
+    xr, itr, str_ = _host(torch, ref_bufs)
+    assert stats["peeled"] > 0, stats
+    for call in range(2):
+        bufs = _buffers(torch, x0)
+        torch.cuda.synchronize()
+        with pytest.raises(lanes.LaneError) as err:
+            ctx.solve_device_static(*_ptrs(bufs), cold=True, opts=opts)
+        assert err.value.code == lanes.ESL_NOT_ELIGIBLE
+        xs, its, sts = _host(torch, bufs)
+        paused = sts == lanes.LANE_NEED_SOLVE
+        assert err.value.paused == int(paused.sum()) > 0, f"call {call}"
+        assert int(paused.sum()) <= stats["peeled"], f"call {call}"
+        ok = ~paused
+        assert np.array_equal(sts[ok], str_[ok]), f"call {call}"
+        assert np.array_equal(its[ok], itr[ok]), f"call {call}"
+        assert np.array_equal(xs[ok].view(np.uint64), xr[ok].view(np.uint64)), f"call {call}"
+    ctx.close()
+
+
 def test_static_entry_needs_a_tape_first():
     torch = _torch()
     fr, slots, values = decks.grid_diodes(seed=3, points=32)
