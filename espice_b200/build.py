@@ -22,6 +22,7 @@ SOURCES = [
     "csrc/host/api.cpp",
     "csrc/host/lu_jit.cpp",
     "csrc/kernels/newton.cu",
+    "csrc/kernels/block.cu",
     "csrc/kernels/mlp.cu",
     "csrc/host/mlp_host.cu",
 ]
@@ -76,7 +77,7 @@ def build(force=False, verbose=False):
         if verbose:
             sys.stderr.write(r.stderr)
     r = subprocess.run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB] + objs
-                       + ["-lcudart", "-ldl"], capture_output=True, text=True)
+                       + ["-lcudart", "-ldl", "-Xlinker", "--no-undefined"], capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("nvcc failed linking libespice_lanes.so")

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <thread>
 #include <limits>
 #include <memory>
 #include <string>
@@ -17,6 +18,7 @@
 #include <vector>
 
 #include "../../../include/espice_lanes.h"
+#include "../kernels/block.h"
 #include "../kernels/launch.h"
 #include "lu_jit.hpp"
 #include "records.hpp"
@@ -229,7 +231,21 @@ struct esl_ctx {
   std::vector<double> rec_lanes;
 
   bool have_tape = false;
+  bool warp_ok = false;    // the tape's warp programs fit (16-bit value indices, a warp's shared memory)
   bool has_meyer = false;  // a MOS1 instance gives TOX: DC only
+  // Block lanes (block.cu): the solve mode, the block programs of the
+  // current tape and their device copies, the per-CTA working-set slab.
+  uint32_t precision = ESL_PREC_FP64;
+  uint32_t path = ESL_PATH_AUTO;
+  uint32_t block_width = 256;
+  double refine_tol = 1e-12;
+  uint32_t refine_max = 6;
+  bool have_block = false;
+  bool profile = false;  // block lanes: accumulate the phase cycles (esl_solve_mode.profile)
+  BlockPrograms bprog;
+  uint32_t block_op_bytes = 8;     // 8: 16-bit value indices; 16: 32-bit
+  uint32_t block_g_len = 0, block_g_ncells = 0;
+  DevBuf d_ba, d_bb, d_bf, d_slab, d_refine, d_prof, d_bg_terms, d_bg_cells;
   SparseLu lead;
   Programs prog;
 
@@ -246,6 +262,7 @@ struct esl_ctx {
   int lu_jit_state = 0;                              // 0 not built, 1 built, -1 failed
   DevBuf d_row_ptr, d_row_slot, d_row_col;
   DevBuf d_group_topo, d_group_lanes, d_group_cta_ctx, d_group_cta_first, d_group_lpb;  // a group launch's tables
+  DevBuf d_group_blocks, d_group_items, d_group_slab;  // a block-lane group launch's tables and slabs
   DevBuf d_rec, d_lim, d_lim_active, d_status, d_iters, d_flags, d_limit, d_a_vals, d_rhs, d_dx,
       d_diag, d_paused, d_x;
   TopoDev topo{};
@@ -681,7 +698,6 @@ int32_t upload_tape(esl_ctx* ctx) {
   TopoDev& T = ctx->topo;
   Programs& P = ctx->prog;
   if (P.has_void) return ctx->fail(ESL_NOT_ELIGIBLE, "the lead factor fabricated a pivot for a void unknown");
-  if (P.nv >= 65536) return ctx->fail(ESL_NOT_ELIGIBLE, "tape too large for one lane's shared memory");
   ESL_CUDA(upload(ctx->d_amap, P.amap, s));
   ESL_CUDA(upload(ctx->d_fill, P.fill, s));
   ESL_CUDA(upload(ctx->d_l_scaled, P.l_scaled, s));
@@ -694,6 +710,20 @@ int32_t upload_tape(esl_ctx* ctx) {
   T.amap = ctx->d_amap.as<uint32_t>();
   T.fill = ctx->d_fill.as<uint32_t>();
   T.n_fill = uint32_t(P.fill.size());
+  T.l_scaled = ctx->d_l_scaled.as<uint8_t>();
+  T.pinv = ctx->d_pinv.as<uint32_t>();
+  T.qcol = ctx->d_q.as<uint32_t>();
+  ctx->have_block = false;  // a new tape needs its own block programs
+  lu_jit_release(ctx->lu_jit);  // and its own compiled LU
+  ctx->lu_jit_state = 0;
+  lu_jit_release(ctx->lu_jit_mixed);
+  ctx->lu_jit_mixed_state = 0;
+  ctx->have_tape = true;
+  // The warp lanes: programs with 16-bit value indices, the programs and one
+  // lane's working set in a CTA's shared memory. A tape beyond them runs on
+  // the block lanes only.
+  ctx->warp_ok = false;
+  if (P.nv >= 65536) return ESL_OK;
   {
     // One blob: A ops, B ops, gather depth/off/src/dst, each section
     // 16-byte aligned.
@@ -725,17 +755,11 @@ int32_t upload_tape(esl_ctx* ctx) {
     T.g_nseg = G.nseg;
     T.g_seg_blocks = G.seg_len / kGatherBlock;
   }
-  T.l_scaled = ctx->d_l_scaled.as<uint8_t>();
-  T.pinv = ctx->d_pinv.as<uint32_t>();
-  T.qcol = ctx->d_q.as<uint32_t>();
   T.smem_doubles = lane_layout(T.n, T.ntv, T.n_stage, T.nlim).total;
-  if (size_t(T.smem_doubles) * 8 > 227 * 1024)
-    return ctx->fail(ESL_NOT_ELIGIBLE, "one lane's working set exceeds a CTA's shared memory");
   // Every CTA stages the programs; as many lanes per CTA as fit beside them.
   const size_t lane_bytes = size_t(T.smem_doubles) * 8;
   const size_t room = size_t(227) * 1024;
-  if (T.prog_bytes + lane_bytes > room)
-    return ctx->fail(ESL_NOT_ELIGIBLE, "programs and one lane exceed a CTA's shared memory");
+  if (T.prog_bytes + lane_bytes > room) return ESL_OK;
   ctx->lanes_eff = std::max<uint32_t>(1, std::min<uint32_t>(8, uint32_t((room - T.prog_bytes) / lane_bytes)));
   // Transient lanes add the accepted points, the charge rings and dynamic
   // currents over the rows and the LTE states: cur | prev | q[4] | ip over
@@ -752,10 +776,6 @@ int32_t upload_tape(esl_ctx* ctx) {
   {
     std::vector<Op> seq = lane_sequence(P, ctx->n_seq_a, ctx->n_seq, ctx->n_seq_f);
     ESL_CUDA(upload(ctx->d_seq, seq, s));
-    lu_jit_release(ctx->lu_jit);  // a new tape needs its own compiled LU
-    ctx->lu_jit_state = 0;
-    lu_jit_release(ctx->lu_jit_mixed);
-    ctx->lu_jit_mixed_state = 0;
     ctx->mixed_warps = 0;
     for (uint32_t w = 8; w >= 1; --w)
       if (lu_lanes_mixed_smem(T, ctx->n_seq + ctx->n_seq_f, w) <= room) {
@@ -769,8 +789,198 @@ int32_t upload_tape(esl_ctx* ctx) {
         break;
       }
   }
-  ctx->have_tape = true;
+  ctx->warp_ok = true;
   return ESL_OK;
+}
+
+// The block lanes' program rows in their device format: 8-byte words
+// {dst | kind << 28, a | b << 16} when the value space has 16-bit indices,
+// else the 16-byte words as built.
+std::vector<uint32_t> block_words(const std::vector<Op4>& ops, bool short_ops) {
+  std::vector<uint32_t> w;
+  w.reserve(ops.size() * (short_ops ? 2 : 4));
+  for (const Op4& o : ops) {
+    if (short_ops) {
+      w.push_back(o.w0);
+      w.push_back(o.a | (o.b << 16));
+    } else {
+      w.push_back(o.w0);
+      w.push_back(o.a);
+      w.push_back(o.b);
+      w.push_back(0u);
+    }
+  }
+  return w;
+}
+
+// The block lanes' assembly streams (block.cu block_assemble): every
+// residual row and pattern slot is a cell summing its staging terms in list
+// order; cells go to the CTA's threads longest first, each to the least
+// loaded thread; a thread's terms follow one another in its stream
+// (terms[k * W + t]), the last term of each cell flagged, and its cells'
+// destinations in its cell stream (cells[c * W + t]).
+void build_block_gather(const esl_ctx* ctx, uint32_t W, std::vector<uint32_t>& terms, std::vector<uint32_t>& cells,
+                        uint32_t& len, uint32_t& ncells) {
+  struct Cell {
+    std::vector<uint32_t> src;
+    uint32_t w0, w1, w2;
+  };
+  auto code = [](uint32_t s) { return s == kSrcOne ? kGSrcOne : s == kSrcX0 ? kGSrcX0 : s; };
+  std::vector<Cell> all;
+  const uint32_t n = ctx->pat.n, nnz = ctx->pat.nnz();
+  for (uint32_t i = 0; i < n; ++i) {
+    Cell c{{}, i | kGCellRow, ctx->lead.pinv[i], 0u};
+    for (uint32_t e = ctx->rhs_ptr[i]; e < ctx->rhs_ptr[i + 1]; ++e) c.src.push_back(code(ctx->rhs_src[e]));
+    all.push_back(std::move(c));
+  }
+  for (uint32_t p = 0; p < nnz; ++p) {
+    Cell c{{}, p, ctx->prog.amap[p], ctx->slot_row[p]};
+    for (uint32_t e = ctx->a_ptr[p]; e < ctx->a_ptr[p + 1]; ++e) c.src.push_back(code(ctx->a_src[e]));
+    all.push_back(std::move(c));
+  }
+  for (Cell& c : all) {
+    if (c.src.empty()) c.src.push_back(kGSrcZero);
+    c.src.back() |= kGTermEnd;
+  }
+  std::stable_sort(all.begin(), all.end(), [](const Cell& a, const Cell& b) { return a.src.size() > b.src.size(); });
+  std::vector<std::vector<uint32_t>> t_terms(W), t_cells(W);
+  std::vector<size_t> load(W, 0);
+  for (const Cell& c : all) {
+    const uint32_t t = uint32_t(std::min_element(load.begin(), load.end()) - load.begin());
+    t_terms[t].insert(t_terms[t].end(), c.src.begin(), c.src.end());
+    t_cells[t].insert(t_cells[t].end(), {c.w0, c.w1, c.w2, 0u});
+    load[t] += c.src.size();
+  }
+  len = 0;
+  ncells = 0;
+  for (uint32_t t = 0; t < W; ++t) {
+    len = std::max(len, uint32_t(t_terms[t].size()));
+    ncells = std::max(ncells, uint32_t(t_cells[t].size() / 4));
+  }
+  terms.assign(size_t(std::max(len, 1u)) * W, kGSrcZero);
+  cells.assign(size_t(std::max(ncells, 1u)) * W * 4, 0u);
+  for (uint32_t t = 0; t < W; ++t) {
+    for (size_t k = 0; k < t_terms[t].size(); ++k) terms[k * W + t] = t_terms[t][k];
+    for (size_t c = 0; c < t_cells[t].size() / 4; ++c)
+      for (int j = 0; j < 4; ++j) cells[(c * W + t) * 4 + j] = t_cells[t][4 * c + j];
+  }
+}
+
+// The block lanes' programs and assembly streams of the current tape.
+int32_t ensure_block(esl_ctx* ctx) {
+  if (ctx->have_block) return ESL_OK;
+  cudaStream_t s = ctx->stream;
+  ctx->bprog = compile_block(ctx->prog, kBlockThreads);
+  const bool short_ops = ctx->prog.nv < 65536;
+  ctx->block_op_bytes = short_ops ? 8 : 16;
+  ESL_CUDA(upload(ctx->d_ba, block_words(ctx->bprog.a_ops, short_ops), s));
+  ESL_CUDA(upload(ctx->d_bb, block_words(ctx->bprog.b_ops, short_ops), s));
+  ESL_CUDA(upload(ctx->d_bf, block_words(ctx->bprog.f_ops, short_ops), s));
+  std::vector<uint32_t> terms, cells;
+  build_block_gather(ctx, kBlockThreads, terms, cells, ctx->block_g_len, ctx->block_g_ncells);
+  ESL_CUDA(upload(ctx->d_bg_terms, terms, s));
+  ESL_CUDA(upload(ctx->d_bg_cells, cells, s));
+  ctx->have_block = true;
+  return ESL_OK;
+}
+
+// The op ring a block-lane CTA streams its programs through: kDepth + 1
+// slots of one op word per thread (block.cu OpFormat).
+uint32_t block_ring_bytes(uint32_t op_bytes) { return (op_bytes == 8 ? 17u : 9u) * kBlockThreads * op_bytes; }
+
+// A block lane's working set (block.cu carves the same): x, xo, rhs, diag,
+// dx (FP64, n each), staging, limited images, the FP64 matrix (mixed form),
+// the value space (nv values, FP64 or FP32), each 16-byte aligned.
+void block_layout(const TopoDev& T, uint32_t nv, bool mixed, BlockDev& D) {
+  size_t at = 0;
+  auto take = [&at](size_t bytes) {
+    const size_t o = at;
+    at += (bytes + 15) & ~size_t(15);
+    return uint32_t(o);
+  };
+  D.o_x = take(8 * size_t(T.n));
+  D.o_xo = take(8 * size_t(T.n));
+  D.o_rhs = take(8 * size_t(T.n));
+  D.o_diag = take(8 * size_t(T.n));
+  D.o_dx = take(8 * size_t(T.n));
+  D.o_st = take(8 * size_t(T.n_stage));
+  D.o_lim = take(8 * size_t(std::max<uint32_t>(T.nlim, 1)));
+  D.o_a64 = take(mixed ? 8 * size_t(T.nnz) : 0);
+  D.o_v = take(size_t(mixed ? 4 : 8) * nv);
+  D.lane_bytes = uint32_t(at);
+}
+
+// Shared memory a block lane may take (a CTA's 227 KB, less the static
+// reduction words).
+constexpr size_t kBlockSmemRoom = size_t(227) * 1024 - 256;
+
+// The launch view of the block lanes for n_lanes lanes: programs, layout,
+// where the working set lives, the persistent grid and its slab.
+int32_t block_view(esl_ctx* ctx, bool mixed, uint32_t n_lanes, BlockDev& D) {
+  if (int32_t rc = ensure_block(ctx)) return rc;
+  const TopoDev& T = ctx->topo;
+  D = BlockDev{};
+  D.T = T;
+  D.a_ops = ctx->d_ba.p;
+  D.b_ops = ctx->d_bb.p;
+  D.f_ops = ctx->d_bf.p;
+  D.a_rows = ctx->bprog.a_rows;
+  D.b_rows = ctx->bprog.b_rows;
+  D.f_rows = ctx->bprog.f_rows;
+  D.op_bytes = ctx->block_op_bytes;
+  D.ring_bytes = block_ring_bytes(D.op_bytes);
+  D.g_terms = ctx->d_bg_terms.as<uint32_t>();
+  D.g_cells = ctx->d_bg_cells.as<uint4>();
+  D.g_len = ctx->block_g_len;
+  D.g_ncells = ctx->block_g_ncells;
+  block_layout(T, T.nv, mixed, D);
+  D.in_smem = D.lane_bytes + D.ring_bytes <= kBlockSmemRoom;
+  const int per_sm = block_occupancy(mixed, D.op_bytes == 16, topo_has_b3(T),
+                                     (D.in_smem ? D.lane_bytes : 0) + D.ring_bytes);
+  const uint32_t cap = uint32_t(ctx->sms) * uint32_t(std::max(per_sm, 1));
+  D.grid = std::max<uint32_t>(1, std::min(n_lanes, cap));
+  ESL_CUDA(ctx->d_slab.ensure(size_t(D.in_smem ? 1 : D.grid) * D.lane_bytes));
+  D.slab = ctx->d_slab.as<unsigned char>();
+  D.refine_tol = ctx->refine_tol;
+  D.refine_max = ctx->refine_max;
+  ESL_CUDA(ctx->d_refine.ensure(size_t(n_lanes) * 4));
+  D.refine_out = mixed ? ctx->d_refine.as<uint32_t>() : nullptr;
+  D.prof = nullptr;
+  if (ctx->profile) {
+    ESL_CUDA(ctx->d_prof.ensure(kBlockPhases * sizeof(unsigned long long)));
+    D.prof = ctx->d_prof.as<unsigned long long>();
+  }
+  return ESL_OK;
+}
+
+// Whether a DC solve of this context runs on the block lanes: asked for,
+// mixed precision (the warp lanes are FP64), or a tape beyond the warp
+// lanes.
+bool use_block(const esl_ctx* ctx) {
+  return ctx->path == ESL_PATH_BLOCK || ctx->precision == ESL_PREC_MIXED || !ctx->warp_ok;
+}
+
+// The lead lane's first Jacobian in pattern order: the warp assembly kernel
+// when its working set fits a CTA's shared memory, else the block lanes'
+// (global scratch). The same gathers in the same order: the same bits.
+cudaError_t lead_jacobian(esl_ctx* ctx, const LaneDev& L, double* out) {
+  const TopoDev& T = ctx->topo;
+  const size_t smem = size_t(4 * T.n + T.nv + T.n_stage + T.nlim + 2) * sizeof(double);
+  if (smem <= size_t(227) * 1024) return launch_assemble(T, L, 0, out, ctx->stream);
+  BlockDev D{};
+  D.T = T;
+  block_layout(T, 0, false, D);
+  cudaError_t e = ctx->d_slab.ensure(D.lane_bytes);
+  if (e != cudaSuccess) return e;
+  D.slab = ctx->d_slab.as<unsigned char>();
+  return launch_block_lead(D, L, 0, out, topo_has_b3(T), ctx->stream);
+}
+
+int32_t warp_only(esl_ctx* ctx) {
+  if (ctx->warp_ok) return ESL_OK;
+  return ctx->fail(ESL_NOT_ELIGIBLE,
+                   "the circuit's tape exceeds the warp lanes (16-bit value indices or a warp's shared memory); "
+                   "its DC solves run on the block lanes, this call has no block form");
 }
 
 int32_t build_tape_from(esl_ctx* ctx, const double* lead_vals) {
@@ -974,20 +1184,53 @@ int32_t esl_set_lanes(esl_ctx* ctx, const esl_slot* slots, uint32_t n_slots, con
   ctx->n_lanes = n_lanes;
   const size_t R = ctx->rec_size;
   ctx->rec_lanes.resize(size_t(n_lanes) * R);
-  std::vector<double> prm;
-  for (uint32_t l = 0; l < n_lanes; ++l) {
-    double* rec = &ctx->rec_lanes[size_t(l) * R];
-    std::copy(ctx->rec_nominal.begin(), ctx->rec_nominal.end(), rec);
+  // The instances the slots touch, each with its slots: a lane re-derives
+  // every touched instance once, with all of its overrides in place.
+  struct Touched {
+    uint32_t batch, inst;
+    std::vector<uint32_t> slots;
+  };
+  std::vector<Touched> touched;
+  {
+    std::unordered_map<uint64_t, size_t> at;
     for (uint32_t k = 0; k < n_slots; ++k) {
-      // Instances touched by several slots are re-derived once per slot,
-      // the last time with every override in place.
-      const esl_slot& sl = slots[k];
-      const HostBatch& B = ctx->bats[sl.batch];
-      prm.assign(B.params.begin() + size_t(sl.inst) * B.np, B.params.begin() + size_t(sl.inst + 1) * B.np);
-      for (uint32_t j = 0; j < n_slots; ++j)
-        if (slots[j].batch == sl.batch && slots[j].inst == sl.inst) prm[slots[j].param] = values[size_t(l) * n_slots + j];
-      derive_instance(B.type, prm.data(), rec + B.rec_off + sl.inst, B.count);
+      const uint64_t key = (uint64_t(slots[k].batch) << 32) | slots[k].inst;
+      auto it = at.find(key);
+      if (it == at.end()) {
+        it = at.emplace(key, touched.size()).first;
+        touched.push_back(Touched{slots[k].batch, slots[k].inst, {}});
+      }
+      touched[it->second].slots.push_back(k);
     }
+  }
+  auto derive_lanes = [&](uint32_t l0, uint32_t l1) {
+    std::vector<double> prm;
+    for (uint32_t l = l0; l < l1; ++l) {
+      double* rec = &ctx->rec_lanes[size_t(l) * R];
+      std::copy(ctx->rec_nominal.begin(), ctx->rec_nominal.end(), rec);
+      for (const Touched& t : touched) {
+        const HostBatch& B = ctx->bats[t.batch];
+        prm.assign(B.params.begin() + size_t(t.inst) * B.np, B.params.begin() + size_t(t.inst + 1) * B.np);
+        for (uint32_t k : t.slots) prm[slots[k].param] = values[size_t(l) * n_slots + k];
+        derive_instance(B.type, prm.data(), rec + B.rec_off + t.inst, B.count);
+      }
+    }
+  };
+  // Lanes are independent: derive them on the host's threads when there is
+  // enough work to share.
+  const size_t work = size_t(n_lanes) * touched.size();
+  const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const uint32_t n_thr = work < 4096 ? 1u : std::min<uint32_t>(hw, n_lanes);
+  if (n_thr <= 1) {
+    derive_lanes(0, n_lanes);
+  } else {
+    std::vector<std::thread> pool;
+    const uint32_t per = (n_lanes + n_thr - 1) / n_thr;
+    for (uint32_t t = 0; t < n_thr; ++t) {
+      const uint32_t l0 = t * per, l1 = std::min(n_lanes, l0 + per);
+      if (l0 < l1) pool.emplace_back(derive_lanes, l0, l1);
+    }
+    for (auto& th : pool) th.join();
   }
   ESL_CUDA(upload(ctx->d_rec, ctx->rec_lanes, ctx->stream));
   ctx->topo.rec_size = ctx->rec_size;
@@ -1046,7 +1289,7 @@ int32_t prepare_dc(esl_ctx* ctx, const esl_newton_opts* opts, double* d_x, int c
   L.status = d_status;
   if (!ctx->have_tape) {
     // The lead lane's first Jacobian, factored on the host into the tape.
-    ESL_CUDA(launch_assemble(ctx->topo, L, 0, ctx->d_a_vals.as<double>(), s));
+    ESL_CUDA(lead_jacobian(ctx, L, ctx->d_a_vals.as<double>()));
     std::vector<double> a0(ctx->pat.nnz());
     ESL_CUDA(cudaMemcpyAsync(a0.data(), ctx->d_a_vals.p, a0.size() * 8, cudaMemcpyDeviceToHost, s));
     ESL_CUDA(cudaStreamSynchronize(s));
@@ -1067,8 +1310,24 @@ int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d
   if (int32_t rc = prepare_dc(ctx, opts, d_x, cold, d_iters, d_status, st, L)) return rc;
   LaneOpts o{opts->reltol, opts->abstol, opts->vntol, opts->residual_tol, opts->gmin, opts->max_iter, opts->init_fix,
              opts->iter_cap};
+  const bool block = use_block(ctx);
+  if (!block && !ctx->warp_ok) return warp_only(ctx);
+  if (ctx->path == ESL_PATH_WARP && block)
+    return ctx->fail(ESL_NOT_ELIGIBLE, ctx->warp_ok ? "the warp lanes solve in FP64 only" : "the tape exceeds the warp lanes");
+  const bool mixed = ctx->precision == ESL_PREC_MIXED;
+  BlockDev D{};
+  if (block) {
+    if (int32_t rc = block_view(ctx, mixed, N, D)) return rc;
+    if (D.refine_out) ESL_CUDA(cudaMemsetAsync(D.refine_out, 0, size_t(N) * 4, s));
+    if (D.prof) ESL_CUDA(cudaMemsetAsync(D.prof, 0, kBlockPhases * sizeof(unsigned long long), s));
+  }
+  const bool b3 = topo_has_b3(ctx->topo);
+  auto launch = [&](const LaneDev& LL) {
+    return block ? launch_dc_block(D, LL, o, mixed, b3, s)
+                 : launch_dc_newton(ctx->topo, LL, o, lanes_per_cta(ctx, N, ctx->lanes_eff), s);
+  };
   ESL_CUDA(cudaEventRecord(ctx->ev0, s));
-  ESL_CUDA(launch_dc_newton(ctx->topo, L, o, lanes_per_cta(ctx, N, ctx->lanes_eff), s));
+  ESL_CUDA(launch(L));
   uint32_t launches = 1;
   for (;;) {
     bool any = false;
@@ -1076,7 +1335,7 @@ int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d
     if (!any) break;
     LaneDev R = L;
     R.resume = 1;
-    ESL_CUDA(launch_dc_newton(ctx->topo, R, o, lanes_per_cta(ctx, N, ctx->lanes_eff), s));
+    ESL_CUDA(launch(R));
     ++launches;
   }
   ESL_CUDA(cudaEventRecord(ctx->ev1, s));
@@ -1087,9 +1346,15 @@ int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d
     st->kernel_ms = ms;
     st->launches = launches;
     st->lanes = N;
+    st->path = block ? ESL_PATH_BLOCK : ESL_PATH_WARP;
     std::vector<uint32_t> status(N);
     ESL_CUDA(cudaMemcpy(status.data(), d_status, N * 4, cudaMemcpyDeviceToHost));
     for (uint32_t v : status) st->converged += v == kConverged;
+    if (D.refine_out) {
+      std::vector<uint32_t> ref(N);
+      ESL_CUDA(cudaMemcpy(ref.data(), D.refine_out, N * 4, cudaMemcpyDeviceToHost));
+      for (uint32_t v : ref) st->refinements += v;
+    }
   }
   return ESL_OK;
 }
@@ -1118,6 +1383,8 @@ int32_t esl_dc_solve_device_static(esl_ctx* ctx, const esl_newton_opts* opts, do
     return fail(ESL_INVALID_ARGUMENT, "null argument or no lanes set");
   if (!ctx->have_tape)
     return fail(ESL_NOT_ELIGIBLE, "no pivot tape yet: the first solve of a context must be esl_dc_solve_device");
+  if (!ctx->warp_ok || use_block(ctx))
+    return fail(ESL_NOT_ELIGIBLE, "the allocation-free entry runs the warp lanes in FP64 only");
   if (cudaError_t e = cudaSetDevice(ctx->device)) return cuda(e, "cudaSetDevice");
   void* base = nullptr;
   if (cudaError_t e = static_scratch(&base)) return cuda(e, "cudaGetSymbolAddress(lane scratch)");
@@ -1204,7 +1471,7 @@ int32_t ensure_tape_cold(esl_ctx* ctx) {
   ESL_CUDA(cudaMemcpyAsync(ctx->d_lim.p, lim.data(), lim.size() * 8, cudaMemcpyHostToDevice, s));
   ESL_CUDA(cudaMemcpyAsync(ctx->d_lim_active.p, &act, 4, cudaMemcpyHostToDevice, s));
   LaneDev L = lane_view(ctx, 0);
-  ESL_CUDA(launch_assemble(ctx->topo, L, 0, ctx->d_a_vals.as<double>(), s));
+  ESL_CUDA(lead_jacobian(ctx, L, ctx->d_a_vals.as<double>()));
   std::vector<double> a0(ctx->pat.nnz());
   ESL_CUDA(cudaMemcpyAsync(a0.data(), ctx->d_a_vals.p, a0.size() * 8, cudaMemcpyDeviceToHost, s));
   ESL_CUDA(cudaStreamSynchronize(s));
@@ -1243,6 +1510,7 @@ int32_t esl_tran_device(esl_ctx* ctx, const esl_tran_opts* opts, double* d_x, ui
   LaneOpts lo;
   if (int32_t rc = tran_view(ctx, opts, P, lo)) return rc;
   if (int32_t rc = ensure_tape_cold(ctx)) return rc;
+  if (int32_t rc = warp_only(ctx)) return rc;
   if (ctx->tran_lanes_eff == 0) return ctx->fail(ESL_NOT_ELIGIBLE, "a transient lane exceeds a CTA's shared memory");
   P.stats = d_stats;
   P.n_probes = max_pts ? n_probes : 0;
@@ -1289,6 +1557,7 @@ int32_t esl_dc_sweep_device(esl_ctx* ctx, const esl_slot* slot, const double* va
     ESL_CUDA(cudaStreamSynchronize(s));
     if (rc) return rc;
   }
+  if (int32_t rc = warp_only(ctx)) return rc;
   const TopoDev& T = ctx->topo;
   const size_t lane_bytes = size_t(sweep_doubles(T)) * 8, room = size_t(227) * 1024;
   if (T.prog_bytes + lane_bytes > room) return ctx->fail(ESL_NOT_ELIGIBLE, "a sweep lane exceeds a CTA's shared memory");
@@ -1334,6 +1603,7 @@ int32_t esl_tran_meas_device(esl_ctx* ctx, const esl_tran_opts* opts, const esl_
   LaneOpts lo;
   if (int32_t rc = tran_view(ctx, opts, P, lo)) return rc;
   if (int32_t rc = ensure_tape_cold(ctx)) return rc;
+  if (int32_t rc = warp_only(ctx)) return rc;
   const TopoDev& T = ctx->topo;
   const size_t lane_bytes = (size_t(T.tran_doubles) + size_t(kMeasDoubles) * n_meas) * 8, room = size_t(227) * 1024;
   if (T.prog_bytes + lane_bytes > room) return ctx->fail(ESL_NOT_ELIGIBLE, "a transient lane exceeds a CTA's shared memory");
@@ -1391,6 +1661,120 @@ int32_t esl_tran(esl_ctx* ctx, const esl_tran_opts* opts, const uint32_t* probes
   return ESL_OK;
 }
 
+namespace {
+
+// Shared memory a topology's working set may take in a group launch (the
+// group kernel keeps the work item's tables in static shared memory too).
+constexpr size_t kGroupSmemRoom = size_t(227) * 1024 - 2048;
+
+// The uneven batch on the block lanes: every context's lanes in one
+// persistent launch (work items largest topology first), then each
+// context's paused lanes served on the host and resumed on its own.
+int32_t group_block(esl_ctx* const* ctxs, uint32_t n_ctx, const esl_newton_opts* opts,
+                    const std::vector<LaneDev>& lanes, uint32_t* const* d_status, esl_stats* stats) {
+  esl_ctx* c0 = ctxs[0];
+  esl_ctx* ctx = c0;  // ESL_CUDA reports on the first context
+  const bool mixed = c0->precision == ESL_PREC_MIXED;
+  for (uint32_t c = 0; c < n_ctx; ++c)
+    if ((ctxs[c]->precision == ESL_PREC_MIXED) != mixed || ctxs[c]->path == ESL_PATH_WARP)
+      return c0->fail(ESL_INVALID_ARGUMENT, "a block-lane group runs every context in one precision");
+  std::vector<BlockDev> Ds(n_ctx);
+  bool b3 = false;
+  size_t smem = 0, stride = 16;
+  for (uint32_t c = 0; c < n_ctx; ++c) {
+    esl_ctx* x = ctxs[c];
+    if (int32_t rc = block_view(x, mixed, x->n_lanes, Ds[c])) return rc;
+    if (Ds[c].refine_out) ESL_CUDA(cudaMemsetAsync(Ds[c].refine_out, 0, size_t(x->n_lanes) * 4, x->stream));
+    ESL_CUDA(cudaStreamSynchronize(x->stream));
+    b3 |= topo_has_b3(x->topo);
+  }
+  // the group's own placement: the op ring of the widest op format after
+  // the working sets that fit shared memory within the group room
+  bool long_ops = false;
+  for (uint32_t c = 0; c < n_ctx; ++c) long_ops |= Ds[c].op_bytes == 16;
+  if (long_ops)
+    for (uint32_t c = 0; c < n_ctx; ++c)
+      if (Ds[c].op_bytes != 16) {
+        // one op format per launch: the long words for every topology
+        esl_ctx* x = ctxs[c];
+        ESL_CUDA(upload(x->d_ba, block_words(x->bprog.a_ops, false), x->stream));
+        ESL_CUDA(upload(x->d_bb, block_words(x->bprog.b_ops, false), x->stream));
+        ESL_CUDA(upload(x->d_bf, block_words(x->bprog.f_ops, false), x->stream));
+        ESL_CUDA(cudaStreamSynchronize(x->stream));
+        x->block_op_bytes = 16;
+        if (int32_t rc = block_view(x, mixed, x->n_lanes, Ds[c])) return rc;
+      }
+  const uint32_t ring = block_ring_bytes(long_ops ? 16 : 8);
+  std::vector<BlockDev> Dg = Ds;
+  for (uint32_t c = 0; c < n_ctx; ++c) {
+    Dg[c].in_smem = Dg[c].lane_bytes + ring <= kGroupSmemRoom;
+    if (Dg[c].in_smem) smem = std::max<size_t>(smem, Dg[c].lane_bytes);
+    else stride = std::max<size_t>(stride, Dg[c].lane_bytes);
+  }
+  const uint32_t ring_at = uint32_t((smem + 15) & ~size_t(15));
+  smem = ring_at + ring;
+  std::vector<uint32_t> order(n_ctx);
+  for (uint32_t c = 0; c < n_ctx; ++c) order[c] = c;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    return ctxs[a]->prog.a_nops > ctxs[b]->prog.a_nops;
+  });
+  std::vector<uint2> items;
+  for (uint32_t c : order)
+    for (uint32_t l = 0; l < ctxs[c]->n_lanes; ++l) items.push_back(make_uint2(c, l));
+  const int per_sm = block_group_occupancy(mixed, long_ops, b3, smem);
+  const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(items.size()),
+                                                                 uint32_t(c0->sms) * uint32_t(std::max(per_sm, 1))));
+  cudaStream_t s = c0->stream;
+  ESL_CUDA(upload(c0->d_group_blocks, Dg, s));
+  ESL_CUDA(upload(c0->d_group_lanes, lanes, s));
+  ESL_CUDA(upload(c0->d_group_items, items, s));
+  ESL_CUDA(c0->d_next_lane.ensure(sizeof(uint32_t)));
+  ESL_CUDA(c0->d_group_slab.ensure(size_t(grid) * stride));
+  const LaneOpts o{opts->reltol, opts->abstol, opts->vntol, opts->residual_tol, opts->gmin, opts->max_iter,
+                   opts->init_fix, opts->iter_cap};
+  ESL_CUDA(cudaEventRecord(c0->ev0, s));
+  ESL_CUDA(launch_dc_block_group(c0->d_group_blocks.as<BlockDev>(), c0->d_group_lanes.as<LaneDev>(),
+                                 c0->d_group_items.as<uint2>(), uint32_t(items.size()),
+                                 c0->d_next_lane.as<uint32_t>(), o, c0->d_group_slab.as<unsigned char>(), stride,
+                                 smem, ring_at, grid, mixed, long_ops, b3, s));
+  ESL_CUDA(cudaEventRecord(c0->ev1, s));
+  ESL_CUDA(cudaEventSynchronize(c0->ev1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c0->ev0, c0->ev1);
+  for (uint32_t c = 0; c < n_ctx; ++c) {
+    esl_ctx* x = ctxs[c];
+    ctx = x;
+    uint32_t launches = 1;
+    for (;;) {
+      bool any = false;
+      if (int32_t rc = serve_pauses(x, lanes[c], stats ? &stats[c] : nullptr, &any)) return rc;
+      if (!any) break;
+      LaneDev R = lanes[c];
+      R.resume = 1;
+      ESL_CUDA(launch_dc_block(Ds[c], R, o, mixed, topo_has_b3(x->topo), x->stream));
+      ++launches;
+    }
+    ESL_CUDA(cudaStreamSynchronize(x->stream));
+    if (stats) {
+      stats[c].kernel_ms = ms;
+      stats[c].launches = launches;
+      stats[c].lanes = x->n_lanes;
+      stats[c].path = ESL_PATH_BLOCK;
+      std::vector<uint32_t> status(x->n_lanes);
+      ESL_CUDA(cudaMemcpy(status.data(), d_status[c], x->n_lanes * 4, cudaMemcpyDeviceToHost));
+      for (uint32_t v : status) stats[c].converged += v == kConverged;
+      if (Ds[c].refine_out) {
+        std::vector<uint32_t> ref(x->n_lanes);
+        ESL_CUDA(cudaMemcpy(ref.data(), Ds[c].refine_out, x->n_lanes * 4, cudaMemcpyDeviceToHost));
+        for (uint32_t v : ref) stats[c].refinements += v;
+      }
+    }
+  }
+  return ESL_OK;
+}
+
+}  // namespace
+
 int32_t esl_group_dc_solve_device(esl_ctx* const* ctxs, uint32_t n_ctx, const esl_newton_opts* opts,
                                   double* const* d_x, const int* cold, uint32_t* const* d_iters,
                                   uint32_t* const* d_status, esl_stats* stats) {
@@ -1407,12 +1791,19 @@ int32_t esl_group_dc_solve_device(esl_ctx* const* ctxs, uint32_t n_ctx, const es
   std::vector<uint32_t> cta_ctx, cta_first, lpb(n_ctx);
   size_t smem = 0;
   uint32_t max_lpb = 1;
+  bool block = false;
   for (uint32_t c = 0; c < n_ctx; ++c) {
     esl_ctx* x = ctxs[c];
     if (int32_t rc = prepare_dc(x, opts, d_x[c], cold ? cold[c] : 0, d_iters[c], d_status[c],
                                 stats ? &stats[c] : nullptr, lanes[c]))
       return rc;
     ESL_CUDA(cudaStreamSynchronize(x->stream));
+    block |= use_block(x);
+  }
+  if (block) return group_block(ctxs, n_ctx, opts, lanes, d_status, stats);
+  for (uint32_t c = 0; c < n_ctx; ++c) {
+    esl_ctx* x = ctxs[c];
+    if (int32_t rc = warp_only(x)) return rc;
     topos[c] = x->topo;
     lpb[c] = lanes_per_cta(x, x->n_lanes, x->lanes_eff);
     max_lpb = std::max(max_lpb, lpb[c]);
@@ -1463,6 +1854,55 @@ int32_t esl_group_dc_solve_device(esl_ctx* const* ctxs, uint32_t n_ctx, const es
       ESL_CUDA(cudaMemcpy(status.data(), d_status[c], x->n_lanes * 4, cudaMemcpyDeviceToHost));
       for (uint32_t v : status) stats[c].converged += v == kConverged;
     }
+  }
+  return ESL_OK;
+}
+
+int32_t esl_set_mode(esl_ctx* ctx, const esl_solve_mode* mode) {
+  if (!ctx || !mode) return ESL_INVALID_ARGUMENT;
+  if (mode->precision > ESL_PREC_MIXED || mode->path > ESL_PATH_BLOCK)
+    return ctx->fail(ESL_INVALID_ARGUMENT, "unknown precision or path");
+  const uint32_t width = mode->block_threads ? mode->block_threads : kBlockThreads;
+  if (width != kBlockThreads) return ctx->fail(ESL_INVALID_ARGUMENT, "block_threads: 256 (or 0)");
+  ctx->precision = mode->precision;
+  ctx->path = mode->path;
+  ctx->block_width = width;
+  ctx->refine_tol = mode->refine_tol > 0.0 ? mode->refine_tol : 1e-12;
+  ctx->refine_max = mode->refine_max ? mode->refine_max : 6;
+  ctx->profile = mode->profile != 0;
+  return ESL_OK;
+}
+
+int32_t esl_block_profile(esl_ctx* ctx, uint64_t* cycles) {
+  if (!ctx || !cycles) return ESL_INVALID_ARGUMENT;
+  if (!ctx->profile || !ctx->d_prof.p) return ctx->fail(ESL_INVALID_ARGUMENT, "no profiled block-lane solve yet");
+  cudaSetDevice(ctx->device);
+  ESL_CUDA(cudaMemcpy(cycles, ctx->d_prof.p, kBlockPhases * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  return ESL_OK;
+}
+
+int32_t esl_block_info(esl_ctx* ctx, esl_block_info_t* info) {
+  if (!ctx || !info || !ctx->have_tape) return ESL_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  if (int32_t rc = ensure_block(ctx)) return rc;
+  std::memset(info, 0, sizeof(*info));
+  info->width = kBlockThreads;
+  info->a_rows = ctx->bprog.a_rows;
+  info->b_rows = ctx->bprog.b_rows;
+  info->f_rows = ctx->bprog.f_rows;
+  info->a_levels = ctx->bprog.a_levels;
+  info->a_nops = ctx->prog.a_nops;
+  info->b_nops = ctx->prog.b_nops;
+  info->ntv = ctx->prog.ntv;
+  info->warp_ok = ctx->warp_ok;
+  for (int m = 0; m < 2; ++m) {
+    BlockDev D{};
+    if (int32_t rc = block_view(ctx, m == 1, ctx->n_lanes ? ctx->n_lanes : 1, D)) return rc;
+    info->lane_bytes[m] = D.lane_bytes;
+    info->in_smem[m] = D.in_smem;
+    info->ctas_per_sm[m] = uint32_t(std::max(
+        0, block_occupancy(m == 1, D.op_bytes == 16, topo_has_b3(ctx->topo),
+                           (D.in_smem ? D.lane_bytes : 0) + D.ring_bytes)));
   }
   return ESL_OK;
 }
@@ -1612,6 +2052,7 @@ int32_t esl_lu_lanes_device(esl_ctx* ctx, const double* lead, uint32_t n_lanes, 
     if (!lead) return ESL_INVALID_ARGUMENT;
     if (int32_t rc = build_tape_from(ctx, lead)) return rc;
   }
+  if (int32_t rc = warp_only(ctx)) return rc;
   if (ctx->seq_warps == 0) return ctx->fail(ESL_NOT_ELIGIBLE, "a warp's interleaved lane values exceed shared memory");
   ESL_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
   ESL_CUDA(launch_lu_lanes(ctx->topo, ctx->d_seq.as<uint2>(), ctx->n_seq_a, ctx->n_seq, n_lanes, d_a, d_rhs, d_tv,
@@ -1634,6 +2075,7 @@ int32_t esl_lu_lanes_compiled_device(esl_ctx* ctx, const double* lead, uint32_t 
     if (!lead) return ESL_INVALID_ARGUMENT;
     if (int32_t rc = build_tape_from(ctx, lead)) return rc;
   }
+  if (int32_t rc = warp_only(ctx)) return rc;
   if (ctx->lu_jit_state == 0) {
     ctx->lu_jit_state = -1;
     if (ctx->prog.a_nops + ctx->prog.b_nops > kLuJitMaxOps)
@@ -1665,6 +2107,7 @@ int32_t esl_lu_lanes_mixed_compiled_device(esl_ctx* ctx, const double* lead, uin
     if (!lead) return ESL_INVALID_ARGUMENT;
     if (int32_t rc = build_tape_from(ctx, lead)) return rc;
   }
+  if (int32_t rc = warp_only(ctx)) return rc;
   if (ctx->lu_jit_mixed_state == 0) {
     ctx->lu_jit_mixed_state = -1;
     if (ctx->prog.a_nops + ctx->prog.b_nops > kLuJitMaxOps)
@@ -1721,6 +2164,7 @@ int32_t esl_lu_lanes_mixed_device(esl_ctx* ctx, const double* lead, uint32_t n_l
     if (!lead) return ESL_INVALID_ARGUMENT;
     if (int32_t rc = build_tape_from(ctx, lead)) return rc;
   }
+  if (int32_t rc = warp_only(ctx)) return rc;
   if (ctx->mixed_warps == 0) return ctx->fail(ESL_NOT_ELIGIBLE, "a warp's interleaved lane values exceed shared memory");
   ESL_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
   ESL_CUDA(launch_lu_lanes_mixed(ctx->topo, ctx->d_seq.as<uint2>(), ctx->n_seq_a, ctx->n_seq, ctx->n_seq_f, n_lanes,
@@ -1747,6 +2191,7 @@ int32_t esl_lu_replay_device(esl_ctx* ctx, const double* lead, uint32_t n_lanes,
     if (!lead) return ESL_INVALID_ARGUMENT;
     if (int32_t rc = build_tape_from(ctx, lead)) return rc;
   }
+  if (int32_t rc = warp_only(ctx)) return rc;
   ESL_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
   ESL_CUDA(launch_lu_replay(ctx->topo, n_lanes, d_a, d_rhs, d_tv, d_dx, d_bad, lanes_per_cta(ctx, n_lanes, ctx->lanes_eff), ctx->stream));
   ESL_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));

@@ -36,8 +36,9 @@ bool is_div(uint32_t kind) { return kind == kOpDivGrowth || kind == kOpDivScaled
 // Padding ops write the sink slot (space - 1) from the constants 1.0
 // (space - 2) and 0.0 (space - 3): 1.0 / 1.0 in a division row, a
 // zero-skipped 1.0 * 0.0 in a multiply-subtract row.
-void pack(const std::vector<SeqOp>& seq, uint32_t space, std::vector<Op>& rows, uint32_t& n_rows,
-          uint32_t& n_levels) {
+template <class Enc, class OpT>
+void pack_rows(const std::vector<SeqOp>& seq, uint32_t space, uint32_t width, Enc enc, const OpT& pad_div,
+               const OpT& pad_flop, std::vector<OpT>& rows, uint32_t& n_rows, uint32_t& n_levels) {
   const size_t n = seq.size();
   std::vector<int32_t> last_write(space, -1);
   std::vector<std::vector<uint32_t>> readers(space);
@@ -89,19 +90,14 @@ void pack(const std::vector<SeqOp>& seq, uint32_t space, std::vector<Op>& rows, 
     else c = later(ready[0].front(), ready[1].front()) ? 1 : 0;
     auto& q = ready[c];
     row.clear();
-    while (!q.empty() && row.size() < kRow) {
+    while (!q.empty() && row.size() < width) {
       std::pop_heap(q.begin(), q.end(), later);
       row.push_back(q.back());
       q.pop_back();
     }
-    for (uint32_t t = 0; t < kRow; ++t) {
-      if (t < row.size()) {
-        const SeqOp& s = seq[row[t]];
-        rows.push_back(encode(s.kind, s.dst, s.a, s.b));
-      } else {
-        rows.push_back(c ? encode(kOpDivY, space - 1, space - 2, space - 2)
-                         : encode(kOpSubNz, space - 1, space - 2, space - 3));
-      }
+    for (uint32_t t = 0; t < width; ++t) {
+      if (t < row.size()) rows.push_back(enc(seq[row[t]]));
+      else rows.push_back(c ? pad_div : pad_flop);
     }
     ++n_rows;
     for (uint32_t i : row)
@@ -114,6 +110,18 @@ void pack(const std::vector<SeqOp>& seq, uint32_t space, std::vector<Op>& rows, 
         }
       }
   }
+}
+
+void pack(const std::vector<SeqOp>& seq, uint32_t space, std::vector<Op>& rows, uint32_t& n_rows,
+          uint32_t& n_levels) {
+  auto enc = [](const SeqOp& s) { return encode(s.kind, s.dst, s.a, s.b); };
+  pack_rows(seq, space, kRow, enc, encode(kOpDivY, space - 1, space - 2, space - 2),
+            encode(kOpSubNz, space - 1, space - 2, space - 3), rows, n_rows, n_levels);
+}
+
+// Block-lane ops: 32-bit value indices, padding as no-ops.
+Op4 encode4(const SeqOp& s) {
+  return Op4{s.dst | (s.kind << 28), s.a == kNone ? 0u : s.a, s.b == kNone ? 0u : s.b, 0u};
 }
 
 }  // namespace
@@ -159,8 +167,11 @@ Programs compile_tape(const SparseLu& lu) {
     for (uint32_t q = lu.lp[k]; q < lu.lp[k + 1]; ++q) a.push_back({kOpSubNz, y0 + lu.li[q], lx0 + q, y0 + k});
   }
   P.nv = P.ntv + n + 3;
-  for (const SeqOp& s : a) P.a_list.push_back(encode(s.kind, s.dst, s.a, s.b));
-  pack(a, P.nv, P.a_ops, P.a_rows, P.a_levels);
+  for (const SeqOp& s : a) {
+    P.a_list.push_back(encode(s.kind, s.dst, s.a, s.b));
+    P.a_seq.push_back(Op4{s.dst | (s.kind << 28), s.a == kNone ? 0u : s.a, s.b == kNone ? 0u : s.b, 0u});
+  }
+  if (P.nv < 65536) pack(a, P.nv, P.a_ops, P.a_rows, P.a_levels);
   P.a_nops = uint32_t(a.size());
 
   std::vector<uint8_t> written(P.ntv, 0);
@@ -178,10 +189,49 @@ Programs compile_tape(const SparseLu& lu) {
     b.push_back({kOpDivY, y0 + k, P.nu + k, y0 + k});
     for (uint32_t p = lu.up[k]; p < lu.up[k + 1]; ++p) b.push_back({kOpSubNz, y0 + lu.ui[p], p, y0 + k});
   }
-  for (const SeqOp& s : b) P.b_list.push_back(encode(s.kind, s.dst, s.a, s.b));
-  pack(b, P.nv, P.b_ops, P.b_rows, P.b_levels);
+  for (const SeqOp& s : b) {
+    P.b_list.push_back(encode(s.kind, s.dst, s.a, s.b));
+    P.b_seq.push_back(Op4{s.dst | (s.kind << 28), s.a, s.b, 0u});
+  }
+  if (P.nv < 65536) pack(b, P.nv, P.b_ops, P.b_rows, P.b_levels);
   P.b_nops = uint32_t(b.size());
   return P;
+}
+
+}  // namespace esl
+
+namespace esl {
+
+namespace {
+
+std::vector<SeqOp> unpack(const std::vector<Op4>& ops) {
+  std::vector<SeqOp> out;
+  out.reserve(ops.size());
+  for (const Op4& o : ops) {
+    const uint32_t kind = o.w0 >> 28;
+    // a multiply-subtract reads a and b; a division reads a (divisor) and b
+    out.push_back(SeqOp{kind, o.w0 & 0x0fffffffu, o.a, o.b});
+  }
+  return out;
+}
+
+}  // namespace
+
+BlockPrograms compile_block(const Programs& P, uint32_t width) {
+  BlockPrograms B;
+  B.width = width;
+  const Op4 nop{uint32_t(kOpNop) << 28, 0u, 0u, 0u};
+  const std::vector<SeqOp> a = unpack(P.a_seq), b = unpack(P.b_seq);
+  uint32_t lv = 0;
+  pack_rows(a, P.nv, width, encode4, nop, nop, B.a_ops, B.a_rows, B.a_levels);
+  pack_rows(b, P.nv, width, encode4, nop, nop, B.b_ops, B.b_rows, lv);
+  // the forward substitution alone (program A's solve ops), for the mixed
+  // form's refinement corrections on the finished factors
+  std::vector<SeqOp> f;
+  for (const SeqOp& s : a)
+    if (s.kind == kOpSubNz) f.push_back(s);
+  pack_rows(f, P.nv, width, encode4, nop, nop, B.f_ops, B.f_rows, lv);
+  return B;
 }
 
 }  // namespace esl

@@ -1,0 +1,692 @@
+// Block lanes for sm_100a: the DC Newton solve of circuits whose lane working
+// set is too large for one warp's share of shared memory (hundreds to
+// thousands of unknowns). One CTA owns a lane for its whole solve, every
+// phase in one persistent launch, as the warp lanes do (newton.cu); what
+// changes is the width: eval strides over the CTA's threads, the tape
+// programs are rows of one op per thread (a CTA barrier between rows), and
+// reductions run across the CTA. Nothing per topology is staged: the
+// programs (L2-resident, shared by every lane of the topology) stream in,
+// each thread copying its own op words 16 rows ahead (8 for 16-byte ops)
+// into a private ring in shared memory with cp.async, and the assembly is a
+// per-thread stream of staging indices read eight terms ahead, so neither
+// waits on an L2 round trip per row or per term.
+//
+// Where the working set lives: x | xo | rhs | diag | dx | staging | limited
+// images | (mixed: the FP64 matrix) | v = [tape values | y | 0.0 | 1.0 |
+// sink], in the CTA's shared memory when it fits, else in a per-CTA slab of
+// global memory (L2-resident for the lane's solve; one CTA writes and reads
+// it, ordered by its barriers).
+//
+// Two precisions. FP64: the refactor and solves are bitwise the CPU replay
+// (sparse_lu.zig refactor + solve), as the warp programs are. Mixed: the
+// tape values and y are FP32 (the refactor and both triangular solves in
+// FP32), the assembled matrix is kept in FP64, and each Newton step is
+// refined in FP64 on the residual -rhs - A dx (A and rhs FP64, corrections
+// solved on the FP32 factors) until max |res| <= tol * max |rhs|. Device
+// evaluation, assembly, the refinement residual, the update and the Newton
+// gates stay FP64 in both.
+//
+// Reference path: src/solver/lane_kernels.zig:49-143 (refactor, solveNeg),
+// sparse_lu.zig:918-1184, converger.zig newtonLanes / finalizeStep
+// (:199-522); the refinement has no reference counterpart (the reference's
+// lane LU is FP64 only).
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include "block.h"
+#include "lane_eval.cuh"
+
+namespace esl {
+
+namespace {
+
+__device__ __forceinline__ uint64_t warp_max_bits(uint64_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint64_t w = __shfl_xor_sync(kFull, v, o);
+    v = w > v ? w : v;
+  }
+  return v;
+}
+
+// Maximum over the CTA of a non-negative double's bit pattern (the order of
+// non-negative doubles); red holds one word per warp.
+template <uint32_t kW>
+__device__ __forceinline__ uint64_t block_max_bits(uint64_t v, uint64_t* red) {
+  v = warp_max_bits(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  uint64_t r = 0;
+#pragma unroll
+  for (uint32_t w = 0; w < kW / 32; ++w) r = red[w] > r ? red[w] : r;
+  __syncthreads();
+  return r;
+}
+
+template <uint32_t kW>
+__device__ __forceinline__ double block_max_abs(double v, uint64_t* red) {
+  return from_bits(block_max_bits<kW>(dbits(fabs(v)), red));
+}
+
+// fmax over the CTA (NaN ignored, as fmax does).
+template <uint32_t kW>
+__device__ __forceinline__ double block_fmax(double v, uint64_t* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dbits(v);
+  __syncthreads();
+  double r = from_bits(red[0]);
+#pragma unroll
+  for (uint32_t w = 1; w < kW / 32; ++w) r = fmax(r, from_bits(red[w]));
+  __syncthreads();
+  return r;
+}
+
+// The op's arithmetic in the lane's precision, rounded as the CPU replay
+// rounds (FP64: bitwise; FP32: the same order in FP32).
+__device__ __forceinline__ double op_div(double b, double a) { return div_rn(b, a); }
+__device__ __forceinline__ float op_div(float b, float a) { return __fdiv_rn(b, a); }
+__device__ __forceinline__ double op_msub(double d, double a, double b) { return __dsub_rn(d, __dmul_rn(a, b)); }
+__device__ __forceinline__ float op_msub(float d, float a, float b) { return __fsub_rn(d, __fmul_rn(a, b)); }
+__device__ __forceinline__ double growth(double) { return 1e-12; }
+__device__ __forceinline__ float growth(float) { return 1e-12f; }
+__device__ __forceinline__ double inf_of(double) { return CUDART_INF; }
+__device__ __forceinline__ float inf_of(float) { return CUDART_INF_F; }
+
+// One op of a row (thread-local): a division with its pivot checks, or a
+// multiply-subtract (the solves skip a zero multiplier, the refactor never
+// does); no-ops pad the row. Returns true on a failed pivot test.
+template <typename V>
+__device__ __forceinline__ bool run_op(const uint4& op, V* v) {
+  const uint32_t kind = op.x >> 28;
+  if (kind == kOpNop) return false;
+  V* pd = v + (op.x & 0x0fffffffu);
+  const V a = v[op.y], b = v[op.z];
+  if (kind == kOpDivGrowth || kind == kOpDivScaled || kind == kOpDivY) {
+    const V q = op_div(b, a);
+    *pd = q;
+    if (kind == kOpDivGrowth) return !(fabs(a) >= growth(a) * fabs(b));
+    if (kind == kOpDivScaled) return !(fabs(q) < inf_of(q));
+    return false;
+  }
+  const V d = *pd;
+  if (kind == kOpFlop || b != V(0)) *pd = op_msub(d, a, b);
+  return false;
+}
+
+// Op words: 8 bytes {dst | kind << 28, a | b << 16} when the value space
+// has 16-bit indices, 16 bytes {dst | kind << 28, a, b, 0} otherwise. A
+// thread's ring holds kDepth + 1 op words (16 + 1 short or 8 + 1 long: about
+// 34 or 36 KB a CTA): kDepth rows in flight, and the slot being refilled is
+// never the one being read.
+template <typename OpT>
+struct OpFormat;
+template <>
+struct OpFormat<uint2> {
+  static constexpr uint32_t kDepth = 16;
+  __device__ static uint4 decode(uint2 o) { return make_uint4(o.x, o.y & 0xffffu, o.y >> 16, 0u); }
+};
+template <>
+struct OpFormat<uint4> {
+  static constexpr uint32_t kDepth = 8;
+  __device__ static uint4 decode(uint4 o) { return o; }
+};
+
+__device__ __forceinline__ void ring_copy(uint32_t dst, const void* src, uint32_t bytes) {
+  if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+  else asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void ring_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void ring_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ uint2 ld_ring(uint32_t a, uint2*) {
+  uint2 r;
+  asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(r.x), "=r"(r.y) : "r"(a));
+  return r;
+}
+__device__ __forceinline__ uint4 ld_ring(uint32_t a, uint4*) {
+  uint4 r;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w) : "r"(a));
+  return r;
+}
+
+// Runs a program over v: row r's op for this thread is ops[r * kW + tid];
+// a CTA barrier after each row. Each thread keeps its next kDepth ops in
+// flight through its ring (slot s at ring + s * kW * sizeof(OpT), one commit
+// group per row), so a row waits only for its own op word, copied kDepth rows
+// earlier. Returns this thread's pivot-test failures.
+template <typename V, typename OpT, uint32_t kW>
+__device__ bool block_rows(const OpT* __restrict__ ops, uint32_t rows, V* v, uint32_t ring, int tid) {
+  constexpr uint32_t D = OpFormat<OpT>::kDepth, kSlot = kW * sizeof(OpT);
+  for (uint32_t d = 0; d < D; ++d) {
+    if (d < rows) ring_copy(ring + d * kSlot, ops + size_t(d) * kW + tid, sizeof(OpT));
+    ring_commit();
+  }
+  bool bad = false;
+  uint32_t slot = 0, fill = D;  // the slot of row r, of row r + D
+  for (uint32_t r = 0; r < rows; ++r) {
+    ring_wait<D - 1>();  // row r's group has landed
+    const uint4 op = OpFormat<OpT>::decode(ld_ring(ring + slot * kSlot, static_cast<OpT*>(nullptr)));
+    if (r + D < rows) ring_copy(ring + fill * kSlot, ops + size_t(r + D) * kW + tid, sizeof(OpT));
+    ring_commit();
+    slot = slot == D ? 0 : slot + 1;
+    fill = fill == D ? 0 : fill + 1;
+    bad |= run_op(op, v);
+    __syncthreads();
+  }
+  ring_wait<0>();
+  return bad;
+}
+
+// The lane's views into its working set.
+template <typename V>
+struct BlockMem {
+  LaneMem m;    // x, xo, rhs, diag, staging, limited images (the shared evaluation's view)
+  double* dx;   // n: the FP64 step, in unknown order
+  double* a64;  // nnz: the assembled matrix in FP64 (mixed form only)
+  V* v;         // tape values | y | 0.0 | 1.0 | sink
+  V* y;
+  uint32_t ring;  // this thread's op ring (shared address of its slot 0)
+};
+
+template <typename V>
+__device__ __forceinline__ BlockMem<V> block_carve(const BlockDev& D, unsigned char* base, unsigned char* ring = nullptr,
+                                                  uint32_t op_bytes = 8) {
+  BlockMem<V> b;
+  b.m.base = reinterpret_cast<double*>(base);
+  b.m.x = reinterpret_cast<double*>(base + D.o_x);
+  b.m.xo = reinterpret_cast<double*>(base + D.o_xo);
+  b.m.rhs = reinterpret_cast<double*>(base + D.o_rhs);
+  b.m.diag = reinterpret_cast<double*>(base + D.o_diag);
+  b.m.st = reinterpret_cast<double*>(base + D.o_st);
+  b.m.lim = reinterpret_cast<double*>(base + D.o_lim);
+  b.m.v = nullptr;
+  b.m.y = nullptr;
+  b.dx = reinterpret_cast<double*>(base + D.o_dx);
+  b.a64 = reinterpret_cast<double*>(base + D.o_a64);
+  b.v = reinterpret_cast<V*>(base + D.o_v);
+  b.y = b.v + D.T.ntv;
+  b.ring = ring ? static_cast<uint32_t>(__cvta_generic_to_shared(ring)) + threadIdx.x * op_bytes : 0u;
+  return b;
+}
+
+// Assembly as one streamed gather: thread t walks its term stream
+// (D.g_terms[k * kW + t], k < D.g_len) summing staging cells (or x[0], 1.0,
+// +0.0) from +0.0 in each cell's list order (the CSR order: the same bits as
+// the warp lanes' gather and the host factor's pattern copy); a term with
+// kGTermEnd closes a cell, whose destinations come from the thread's cell
+// stream (D.g_cells[c * kW + t]): a pattern slot (its tape value, FP32 in the
+// mixed form which also keeps the FP64 sum, and the diagonal copy for the
+// gates) or a residual row (rhs and y = P(-rhs)). Terms and cells arrive
+// eight terms and two cells ahead. gmin > 0 adds loadExtras' diagonal and
+// residual terms. Fill-in tape values are zeroed.
+template <typename V, uint32_t kW>
+__device__ __forceinline__ double gather_term(const BlockMem<V>& b, uint32_t w) {
+  const uint32_t src = w & ~kGTermEnd;
+  return src < kGSrcZero ? b.m.st[src] : src == kGSrcOne ? 1.0 : src == kGSrcX0 ? b.m.x[0] : 0.0;
+}
+
+template <typename V, uint32_t kW>
+__device__ __forceinline__ void gather_store(const BlockDev& D, const BlockMem<V>& b, const uint4& c, double s,
+                                             double gmin) {
+  constexpr bool kMixed = sizeof(V) == 4;
+  if (c.x & kGCellRow) {
+    const uint32_t i = c.x & ~kGCellRow;
+    if (gmin > 0.0) s = __dadd_rn(s, __dmul_rn(gmin, b.m.x[i]));
+    b.m.rhs[i] = s;
+    b.y[c.y] = V(-s);
+  } else {
+    if (c.z != kNoDiag) {
+      if (gmin > 0.0) s = __dadd_rn(s, gmin);
+      b.m.diag[c.z] = s;
+    }
+    b.v[c.y] = V(s);
+    if constexpr (kMixed) b.a64[c.x] = s;
+  }
+}
+
+template <typename V, uint32_t kW>
+__device__ void block_assemble(const BlockDev& D, const BlockMem<V>& b, double gmin, int tid) {
+  const TopoDev& T = D.T;
+  const uint32_t* terms = D.g_terms + tid;
+  const uint4* cells = D.g_cells + tid;
+  const uint32_t K = D.g_len;
+  uint32_t w[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) w[j] = uint32_t(j) < K ? __ldg(terms + size_t(j) * kW) : kGSrcZero;
+  const uint4 none = make_uint4(0u, 0u, 0u, 0u);
+  uint4 cell = D.g_ncells > 0 ? __ldg(cells) : none;
+  uint4 cell1 = D.g_ncells > 1 ? __ldg(cells + kW) : none;
+  uint32_t c_next = 2;
+  double s = 0.0;
+  for (uint32_t k0 = 0; k0 < K; k0 += 8) {
+    uint32_t nx[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) nx[j] = k0 + 8 + j < K ? __ldg(terms + size_t(k0 + 8 + j) * kW) : kGSrcZero;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      s = __dadd_rn(s, gather_term<V, kW>(b, w[j]));
+      if (w[j] & kGTermEnd) {
+        gather_store<V, kW>(D, b, cell, s, gmin);
+        s = 0.0;
+        cell = cell1;
+        cell1 = c_next < D.g_ncells ? __ldg(cells + size_t(c_next) * kW) : none;
+        ++c_next;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) w[j] = nx[j];
+  }
+  for (uint32_t j = tid; j < T.n_fill; j += kW) b.v[T.fill[j]] = V(0);
+}
+
+// Refactor + forward solve (program A), then the lane kernels' peel tests on
+// the finished tape values (lane_kernels.zig Bodies.refactor and
+// LaneSolver.wideMultipliers). CTA-uniform verdict.
+template <typename V, typename OpT, uint32_t kW>
+__device__ bool block_refactor(const BlockDev& D, V* v, uint32_t ring, int tid) {
+  const TopoDev& T = D.T;
+  bool bad = block_rows<V, OpT, kW>(static_cast<const OpT*>(D.a_ops), D.a_rows, v, ring, tid);
+  const uint32_t l0 = T.nu + T.n;
+  for (uint32_t s = tid; s < T.nu; s += kW)
+    if (!(fabs(v[s]) < inf_of(v[s]))) bad = true;
+  for (uint32_t k = tid; k < T.n; k += kW) {
+    const V d = v[T.nu + k];
+    if (d == V(0) || !(fabs(d) < inf_of(d))) bad = true;
+  }
+  for (uint32_t s = tid; s < T.nl; s += kW)
+    if (!T.l_scaled[s] && !(fabs(v[l0 + s]) <= V(1e3))) bad = true;
+  return __syncthreads_or(bad) != 0;
+}
+
+// The mixed form's FP64 iterative refinement of the step in dx (unknown
+// order): res = -rhs - A dx with A and rhs in FP64 (the pattern by rows),
+// stop when max |res| <= tol * max |rhs| or after refine_max corrections;
+// each correction solved on the FP32 factors (program F then program B)
+// and added to dx in FP64. Returns the corrections made.
+template <typename OpT, uint32_t kW>
+__device__ uint32_t block_refine(const BlockDev& D, const BlockMem<float>& b, uint64_t* red, int tid) {
+  const TopoDev& T = D.T;
+  uint32_t made = 0;
+  for (uint32_t it = 0;; ++it) {
+    double rmax = 0.0, bmax = 0.0;
+    for (uint32_t i = tid; i < T.n; i += kW) {
+      const double rb = b.m.rhs[i];
+      double res = -rb;
+      for (uint32_t e = T.row_ptr[i]; e < T.row_ptr[i + 1]; ++e)
+        res = __dsub_rn(res, __dmul_rn(b.a64[T.row_slot[e]], b.dx[T.row_col[e]]));
+      rmax = fmax(rmax, fabs(res));
+      bmax = fmax(bmax, fabs(rb));
+      b.y[T.pinv[i]] = float(res);
+    }
+    rmax = block_max_abs<kW>(rmax, red);
+    bmax = block_max_abs<kW>(bmax, red);
+    if (!(rmax > D.refine_tol * bmax) || it >= D.refine_max) break;
+    block_rows<float, OpT, kW>(static_cast<const OpT*>(D.f_ops), D.f_rows, b.v, b.ring, tid);
+    block_rows<float, OpT, kW>(static_cast<const OpT*>(D.b_ops), D.b_rows, b.v, b.ring, tid);
+    for (uint32_t j = tid; j < T.n; j += kW) {
+      const uint32_t i = T.qcol[j];
+      b.dx[i] = __dadd_rn(b.dx[i], double(b.y[j]));
+    }
+    __syncthreads();
+    ++made;
+  }
+  return made;
+}
+
+// Phase profile: thread 0 adds the cycles since `t` to prof[phase] and
+// restarts the clock (nothing when profiling is off).
+__device__ __forceinline__ void phase_mark(unsigned long long* prof, uint32_t phase, long long& t) {
+  if (prof && threadIdx.x == 0) {
+    const long long now = clock64();
+    atomicAdd(prof + phase, static_cast<unsigned long long>(now - t));
+    t = now;
+  }
+}
+
+// One lane's DC Newton solve (converger.zig newtonLanes at W = 1 with the
+// lane's own direct solver), by the CTA that owns it: the warp lanes'
+// dc_solve_lane step for step, reductions across the CTA.
+template <typename V, typename OpT, bool kHasB3, uint32_t kW>
+__device__ void block_lane(const BlockDev& D, const LaneDev& L, const LaneOpts& o, unsigned char* base,
+                           unsigned char* ring, uint64_t* red, uint32_t lane) {
+  constexpr bool kMixed = sizeof(V) == 4;
+  const TopoDev& T = D.T;
+  const int tid = threadIdx.x;
+  const uint32_t status = L.status[lane];
+  const bool resuming = L.resume && status == kNeedSolve;
+  if (!(status == kRunning || resuming)) return;
+
+  const uint32_t n = T.n;
+  const BlockMem<V> b = block_carve<V>(D, base, ring, sizeof(OpT));
+  const LaneMem& m = b.m;
+  const double* rec = L.rec + size_t(lane) * T.rec_size;
+  for (uint32_t i = tid; i < n; i += kW) m.x[i] = L.x[size_t(lane) * n + i];
+  for (uint32_t i = tid; i < T.nlim; i += kW) m.lim[i] = L.lim[size_t(lane) * T.nlim + i];
+  if (tid == 0) {
+    b.v[T.ntv + n] = V(0);
+    b.v[T.ntv + n + 1] = V(1);
+    b.v[T.ntv + n + 2] = V(0);
+  }
+  bool lim_active = L.lim_active[lane] != 0;
+  uint32_t flags = L.flags[lane];
+  uint32_t iter = L.iters[lane];
+  double limit = L.limit[lane];
+  uint32_t max_iter = o.max_iter < 100 ? 100 : o.max_iter;
+  if (o.iter_cap && o.iter_cap < max_iter) max_iter = o.iter_cap;
+  uint32_t refinements = 0;
+  SimDev sim;
+  sim.t = 0.0;
+  sim.src_scale = 1.0;
+  sim.kind = 0;
+  bool have_step = false;
+  if (resuming) {
+    for (uint32_t i = tid; i < n; i += kW) {
+      m.rhs[i] = L.rhs[size_t(lane) * n + i];
+      m.diag[i] = L.diag[size_t(lane) * n + i];
+      b.dx[i] = L.dx[size_t(lane) * n + i];
+    }
+    have_step = true;
+  }
+  __syncthreads();
+
+  long long t0 = D.prof && tid == 0 ? clock64() : 0;
+  for (; iter < max_iter; ++iter) {
+    if (D.prof && tid == 0) atomicAdd(D.prof + kBlockPhaseIters, 1ull);
+    if (!have_step) {
+      eval_all<kHasB3, kW>(T, rec, m, lim_active, sim, tid, false, nullptr, true);
+      __syncthreads();
+      phase_mark(D.prof, kBlockPhaseEval, t0);
+      block_assemble<V, kW>(D, b, o.gmin, tid);
+      __syncthreads();
+      phase_mark(D.prof, kBlockPhaseAssemble, t0);
+      if (iter == 0) {
+        // plausibleLimit: 1e3 x the start's scale, at least x_plausible
+        double g = 1.0;
+        uint64_t xm = 0, fm = 0;
+        for (uint32_t i = tid; i < n; i += kW) {
+          g = fmax(g, fabs(m.diag[i]));
+          const uint64_t bx = dbits(fabs(m.x[i])), bf = dbits(fabs(m.rhs[i]));
+          xm = bx > xm ? bx : xm;
+          fm = bf > fm ? bf : fm;
+        }
+        const double gd = block_fmax<kW>(g, red);
+        xm = block_max_bits<kW>(xm, red);
+        fm = block_max_bits<kW>(fm, red);
+        const double scale = fmin(fmax(from_bits(xm), from_bits(fm) * gd), 1e18);
+        limit = !(1e3 * scale > kXPlausible) ? kXPlausible : 1e3 * scale;
+      }
+      const bool host_mode = (flags & 2u) != 0;
+      bool bad = true;
+      if (!host_mode) bad = block_refactor<V, OpT, kW>(D, b.v, b.ring, tid);
+      phase_mark(D.prof, kBlockPhaseRefactor, t0);
+      if (bad) {
+        // Pause: the host factors this lane with its own FP64 direct solver.
+        const size_t at = size_t(lane) * n;
+        gather_pattern<kW>(T, m, L.a_vals + size_t(lane) * T.nnz, tid);
+        for (uint32_t i = tid; i < n; i += kW) {
+          L.x[at + i] = m.x[i];
+          L.rhs[at + i] = m.rhs[i];
+          L.diag[at + i] = m.diag[i];
+        }
+        for (uint32_t i = tid; i < T.nlim; i += kW) L.lim[size_t(lane) * T.nlim + i] = m.lim[i];
+        if (tid == 0) {
+          L.lim_active[lane] = lim_active;
+          L.flags[lane] = flags | 2u;
+          L.iters[lane] = iter;
+          L.limit[lane] = limit;
+          L.status[lane] = kNeedSolve;
+          if (D.refine_out) D.refine_out[lane] += refinements;
+          atomicAdd(L.n_paused, 1u);
+        }
+        return;
+      }
+      block_rows<V, OpT, kW>(static_cast<const OpT*>(D.b_ops), D.b_rows, b.v, b.ring, tid);
+      for (uint32_t j = tid; j < n; j += kW) b.dx[T.qcol[j]] = double(b.y[j]);
+      __syncthreads();
+      phase_mark(D.prof, kBlockPhaseSolve, t0);
+      if constexpr (kMixed) {
+        refinements += block_refine<OpT, kW>(D, b, red, tid);
+        phase_mark(D.prof, kBlockPhaseRefine, t0);
+      }
+    }
+    have_step = false;
+
+    // finalizeStep: x_old = x, x += dx, delta score (updateAndNorm)
+    uint64_t worst = 0;
+    for (uint32_t i = tid; i < n; i += kW) {
+      const double d = b.dx[i];
+      const double xold = m.x[i];
+      const double xn = xold + d;
+      m.xo[i] = xold;
+      m.x[i] = xn;
+      const double tol = o.reltol * fmax(fabs(xn), fabs(xold)) + (T.cur_row[i] ? o.abstol : o.vntol);
+      const bool finite = fabs(xn) < CUDART_INF && fabs(d) < CUDART_INF;
+      const double qv = div_rn(fabs(d), tol);
+      const double score = !finite ? CUDART_INF : (qv == qv ? qv : 0.0);
+      const uint64_t sb = dbits(score);
+      worst = sb > worst ? sb : worst;
+    }
+    worst = block_max_bits<kW>(worst, red);
+    const bool limited = __syncthreads_or(apply_limits<kHasB3, kW>(T, rec, m, lim_active, tid)) != 0;
+    if (T.nlim) lim_active = true;
+
+    bool ok = !limited && iter != 0 && !(from_bits(worst) >= 1.0);
+    if (ok) {
+      bool p = true;
+      for (uint32_t i = tid; i < n; i += kW) p &= fabs(m.x[i]) <= limit;
+      ok = __syncthreads_and(p) != 0;
+    }
+    if (ok) {
+      bool p = true;
+      for (uint32_t i = tid; i < n; i += kW) p &= fabs(m.rhs[i]) <= residual_gate(o, m.diag[i], m.x[i]);
+      ok = __syncthreads_and(p) != 0;
+    }
+    phase_mark(D.prof, kBlockPhaseGates, t0);
+    if (ok) {
+      if (flags & 1u) {
+        flags &= ~1u;  // INITFIX -> INITFLOAT: one more passing iterate
+      } else {
+        for (uint32_t i = tid; i < n; i += kW) L.x[size_t(lane) * n + i] = m.xo[i];
+        if (tid == 0) {
+          L.iters[lane] = iter + 1;
+          L.status[lane] = kConverged;
+          L.lim_active[lane] = 0;
+          if (D.refine_out) D.refine_out[lane] += refinements;
+        }
+        return;
+      }
+    }
+    __syncthreads();
+  }
+  for (uint32_t i = tid; i < n; i += kW) L.x[size_t(lane) * n + i] = m.x[i];
+  if (tid == 0) {
+    L.iters[lane] = max_iter;
+    L.status[lane] = kMaxIter;
+    L.lim_active[lane] = 0;
+    if (D.refine_out) D.refine_out[lane] += refinements;
+  }
+}
+
+// Persistent grid: each CTA takes lanes blockIdx.x, + gridDim.x, ...; its
+// working set in dynamic shared memory or in its slab of D.slab.
+// Dynamic shared memory: the working set (when in_smem), then the op ring.
+template <typename V, typename OpT, bool kHasB3, uint32_t kW>
+__global__ void __launch_bounds__(kW) dc_block_kernel(BlockDev D, LaneDev L, LaneOpts o) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint64_t red[kW / 32];
+  unsigned char* base = D.in_smem ? smem_raw : D.slab + size_t(blockIdx.x) * D.lane_bytes;
+  unsigned char* ring = smem_raw + (D.in_smem ? D.lane_bytes : 0u);
+  for (uint32_t lane = blockIdx.x; lane < L.n_lanes; lane += gridDim.x) {
+    block_lane<V, OpT, kHasB3, kW>(D, L, o, base, ring, red, lane);
+    __syncthreads();
+  }
+}
+
+// Uneven batching on the block lanes: the lanes of several topologies in one
+// persistent launch. Work items are (topology, lane) pairs; each CTA takes
+// the next item from a counter (items ordered largest topology first, so
+// the long solves start early and the short ones fill in behind them),
+// copies that topology's tables into shared memory and solves the lane with
+// its working set in dynamic shared memory (when the topology's fits) or in
+// the CTA's slab. Every topology of a group runs in one precision and width.
+template <typename V, typename OpT, bool kHasB3, uint32_t kW>
+__global__ void __launch_bounds__(kW) dc_block_group_kernel(const BlockDev* __restrict__ Ds,
+                                                            const LaneDev* __restrict__ Ls, const uint2* items,
+                                                            uint32_t n_items, uint32_t* next, LaneOpts o,
+                                                            unsigned char* slab, size_t slab_stride,
+                                                            uint32_t ring_at) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint64_t red[kW / 32];
+  __shared__ BlockDev D;
+  __shared__ LaneDev L;
+  __shared__ uint32_t item;
+  unsigned char* own_slab = slab + size_t(blockIdx.x) * slab_stride;
+  for (;;) {
+    if (threadIdx.x == 0) item = atomicAdd(next, 1u);
+    __syncthreads();
+    const uint32_t it = item;
+    if (it >= n_items) break;
+    const uint2 w = items[it];
+    if (threadIdx.x == 0) {
+      D = Ds[w.x];
+      L = Ls[w.x];
+    }
+    __syncthreads();
+    block_lane<V, OpT, kHasB3, kW>(D, L, o, D.in_smem ? smem_raw : own_slab, smem_raw + ring_at, red, w.y);
+    __syncthreads();
+  }
+}
+
+template <typename V, bool kHasB3, uint32_t kW>
+cudaError_t launch_group_t(const BlockDev* Ds, const LaneDev* Ls, const uint2* items, uint32_t n_items,
+                           uint32_t* next, const LaneOpts& o, unsigned char* slab, size_t slab_stride, size_t smem,
+                           uint32_t grid, cudaStream_t s) {
+  auto* k = dc_block_group_kernel<V, kHasB3, kW>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(next, 0, sizeof(uint32_t), s);
+  if (e != cudaSuccess) return e;
+  k<<<grid, kW, smem, s>>>(Ds, Ls, items, n_items, next, o, slab, slab_stride);
+  return cudaGetLastError();
+}
+
+template <typename V, bool kHasB3, uint32_t kW>
+int group_occupancy_t(size_t smem) {
+  int per_sm = 0;
+  auto* k = dc_block_group_kernel<V, kHasB3, kW>;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) return 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, int(kW), smem);
+  return per_sm;
+}
+
+// The lead lane's first Jacobian in pattern order (its device evaluation at
+// the lane's start point), with the working set in global scratch: the
+// block lanes' counterpart of assemble_kernel, for any circuit size.
+template <bool kHasB3, uint32_t kW>
+__global__ void __launch_bounds__(kW) block_lead_kernel(BlockDev D, LaneDev L, uint32_t lane, double* out) {
+  const TopoDev& T = D.T;
+  const int tid = threadIdx.x;
+  const BlockMem<double> b = block_carve<double>(D, D.slab);
+  for (uint32_t i = tid; i < T.n; i += kW) b.m.x[i] = L.x[size_t(lane) * T.n + i];
+  for (uint32_t i = tid; i < T.nlim; i += kW) b.m.lim[i] = L.lim[size_t(lane) * T.nlim + i];
+  SimDev sim;
+  sim.t = 0.0;
+  sim.src_scale = 1.0;
+  sim.kind = 0;
+  __syncthreads();
+  eval_all<kHasB3, kW>(T, L.rec + size_t(lane) * T.rec_size, b.m, L.lim_active[lane] != 0, sim, tid, false, nullptr,
+                       true);
+  __syncthreads();
+  gather_pattern<kW>(T, b.m, out, tid);
+}
+
+template <typename V, typename OpT, bool kHasB3>
+cudaError_t launch_t(const BlockDev& D, const LaneDev& L, const LaneOpts& o, cudaStream_t s) {
+  auto* k = dc_block_kernel<V, OpT, kHasB3, kBlockThreads>;
+  const size_t smem = (D.in_smem ? D.lane_bytes : 0) + D.ring_bytes;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  const uint32_t grid = D.grid < L.n_lanes ? D.grid : L.n_lanes;
+  k<<<grid > 0 ? grid : 1, kBlockThreads, smem, s>>>(D, L, o);
+  return cudaGetLastError();
+}
+
+template <typename V, typename OpT, bool kHasB3>
+int occupancy_t(size_t smem) {
+  int per_sm = 0;
+  auto* k = dc_block_kernel<V, OpT, kHasB3, kBlockThreads>;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) return 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, int(kBlockThreads), smem);
+  return per_sm;
+}
+
+template <typename V, typename OpT, bool kHasB3>
+cudaError_t launch_group_t(const BlockDev* Ds, const LaneDev* Ls, const uint2* items, uint32_t n_items,
+                           uint32_t* next, const LaneOpts& o, unsigned char* slab, size_t slab_stride, size_t smem,
+                           uint32_t ring_at, uint32_t grid, cudaStream_t s) {
+  auto* k = dc_block_group_kernel<V, OpT, kHasB3, kBlockThreads>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(next, 0, sizeof(uint32_t), s);
+  if (e != cudaSuccess) return e;
+  k<<<grid, kBlockThreads, smem, s>>>(Ds, Ls, items, n_items, next, o, slab, slab_stride, ring_at);
+  return cudaGetLastError();
+}
+
+template <typename V, typename OpT, bool kHasB3>
+int group_occupancy_t(size_t smem) {
+  int per_sm = 0;
+  auto* k = dc_block_group_kernel<V, OpT, kHasB3, kBlockThreads>;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) return 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, int(kBlockThreads), smem);
+  return per_sm;
+}
+
+// The eight instantiations: precision x op format x BSIM3.
+#define ESL_BLOCK_DISPATCH(F, ...)                                                     \
+  do {                                                                                 \
+    if (mixed) {                                                                       \
+      if (long_ops) return has_b3 ? F<float, uint4, true>(__VA_ARGS__) : F<float, uint4, false>(__VA_ARGS__); \
+      return has_b3 ? F<float, uint2, true>(__VA_ARGS__) : F<float, uint2, false>(__VA_ARGS__);               \
+    }                                                                                  \
+    if (long_ops) return has_b3 ? F<double, uint4, true>(__VA_ARGS__) : F<double, uint4, false>(__VA_ARGS__); \
+    return has_b3 ? F<double, uint2, true>(__VA_ARGS__) : F<double, uint2, false>(__VA_ARGS__);               \
+  } while (0)
+
+}  // namespace
+
+cudaError_t launch_dc_block(const BlockDev& D, const LaneDev& L, const LaneOpts& o, bool mixed, bool has_b3,
+                            cudaStream_t s) {
+  const bool long_ops = D.op_bytes == 16;
+  ESL_BLOCK_DISPATCH(launch_t, D, L, o, s);
+}
+
+int block_occupancy(bool mixed, bool long_ops, bool has_b3, size_t smem) {
+  ESL_BLOCK_DISPATCH(occupancy_t, smem);
+}
+
+cudaError_t launch_dc_block_group(const BlockDev* d_Ds, const LaneDev* d_Ls, const uint2* d_items, uint32_t n_items,
+                                  uint32_t* d_next, const LaneOpts& o, unsigned char* slab, size_t slab_stride,
+                                  size_t smem, uint32_t ring_at, uint32_t grid, bool mixed, bool long_ops, bool has_b3,
+                                  cudaStream_t s) {
+  ESL_BLOCK_DISPATCH(launch_group_t, d_Ds, d_Ls, d_items, n_items, d_next, o, slab, slab_stride, smem, ring_at, grid,
+                     s);
+}
+
+int block_group_occupancy(bool mixed, bool long_ops, bool has_b3, size_t smem) {
+  ESL_BLOCK_DISPATCH(group_occupancy_t, smem);
+}
+
+#undef ESL_BLOCK_DISPATCH
+
+cudaError_t launch_block_lead(const BlockDev& D, const LaneDev& L, uint32_t lane, double* out, bool has_b3,
+                              cudaStream_t s) {
+  if (has_b3) block_lead_kernel<true, kBlockThreads><<<1, kBlockThreads, 0, s>>>(D, L, lane, out);
+  else block_lead_kernel<false, kBlockThreads><<<1, kBlockThreads, 0, s>>>(D, L, lane, out);
+  return cudaGetLastError();
+}
+
+}  // namespace esl

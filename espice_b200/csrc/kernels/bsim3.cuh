@@ -352,7 +352,7 @@ __device__ __forceinline__ void b3_jcur(double v, double isat, double nvt, doubl
 // BSIM3 stamp into its 23 staging cells (layout in common.h). `lim` is the
 // instance's three images (vgs, vds, vbs) when limiting is live; a limited
 // instance is linearised back to x.
-__device__ __noinline__ void bsim3_stamp(const double* r, int s, double xd, double xg, double xs, double xb,
+static __device__ __noinline__ void bsim3_stamp(const double* r, int s, double xd, double xg, double xs, double xb,
                                          double xdi, double xsi, const double* lim, double* st) {
   auto F = [&](int f) { return r[f * s]; };
   const double type = F(kB3Type), m = F(kB3M);
@@ -437,7 +437,7 @@ __device__ __noinline__ void bsim3_stamp(const double* r, int s, double xd, doub
 // vcrit, against `old` (images, or x_old's voltages before the first
 // pass); true when pnjlim limited. Images within 16 ulps of the raw value
 // snap to it.
-__device__ __noinline__ bool bsim3_limit(const double* r, int s, double xg, double xb, double xdi, double xsi,
+static __device__ __noinline__ bool bsim3_limit(const double* r, int s, double xg, double xb, double xdi, double xsi,
                                          const double* old, double* img) {
   const double type = r[kB3Type * s];
   const double vgs_n = type * (xg - xsi), vds_n = type * (xdi - xsi), vbs_n = type * (xb - xsi);

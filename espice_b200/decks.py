@@ -23,6 +23,28 @@ and the vfb/vth0 defaults derived, RSH series resistance (internal drain and
 source nodes), impact ionisation (ALPHA0) and poly depletion (NGATE) under
 MOBMOD 2, and a MOBMOD 3 card. Each lane draws the input voltage from
 U(0, VDD) and every device's DELVTO from N(0, 20 mV).
+
+analog_block (the learned warm start's workload): a seeded BSIM3 analog
+block of 120 MOSFETs on a 20 x 21 RC mesh (R log-uniform in [100, 10k] ohm
+between neighbours, C log-uniform in [1, 100] fF to ground, the mesh's edge
+nodes tied to VREF through 1 kohm): twenty 5-transistor OTAs (an NMOS
+differential pair with a PMOS current-mirror load and an NMOS tail mirror),
+each a unity-gain follower whose input is a seeded mesh node and whose output
+drives another seeded mesh node through 2 kohm; a bias network of six current
+sources, each into a diode-connected NMOS (the tails' mirror gates) and
+mirrored into a diode-connected PMOS; an NMOS source follower on the last
+OTA. About 500 unknowns. 16 parameters per point, uniform from seed: VDD in
+[1.6, 2.0] V, VREF in [0.8, 1.0] V, the six bias currents log-uniform in
+[1, 100] uA, the temperature in [-40, 125] C (every device), and seven DELVTO
+shifts in [-50, 50] mV (device k takes shift k mod 7).
+
+mesh_gates (the uneven batch): eight seeded topologies of about 50 to 2,000
+unknowns, each a planar RC mesh (R log-uniform in [10, 10k] ohm, C in
+[1, 100] fF to ground) with BSIM3 (LEVEL 49 card defaults, L = 0.18 um,
+W log-uniform in [0.2, 2] um) inverters and NAND2 gates, one per twelve
+unknowns, each at a seeded mesh node (its output) with its inputs on mesh
+nodes within two rows and columns of it; two mesh nodes tied to ground and to
+the supply through 1 kohm. Each lane is one supply value in [0.8, 1.8] V.
 """
 
 from __future__ import annotations
@@ -135,3 +157,150 @@ def bsim3_inverters(seed: int = 1, stages: int = 6, lanes: int = 256, sigma: flo
     values[:, 0] = rng.uniform(0.0, vdd, lanes)
     values[:, 1:] = rng.normal(0.0, sigma, size=(lanes, len(slots) - 1))
     return fr, slots, values
+
+
+ANALOG_PARAMS = ["vdd", "vref"] + [f"ibias{k}" for k in range(6)] + ["temp_c"] + [f"dvto{k}" for k in range(7)]
+
+
+def analog_block(seed: int = 1, rows: int = 20, cols: int = 21, n_ota: int = 20):
+    """The analog block at its nominal parameters. Returns (frozen circuit,
+    expand) where expand(params [points][16]) gives the lane values for the
+    slots expand.slots (the two sources' dc, the six bias currents, then
+    every device's temperature in K and its DELVTO)."""
+    rng = np.random.default_rng(seed)
+    c = Circuit()
+    c.V("vdd", "vdd", "0", dc=1.8)
+    c.V("vref", "vref", "0", dc=0.9)
+    mesh = lambda r, k: f"m{r}_{k}"  # noqa: E731
+    for r in range(rows):
+        for k in range(cols):
+            if k + 1 < cols:
+                c.R(f"rh{r}_{k}", mesh(r, k), mesh(r, k + 1), float(np.exp(rng.uniform(np.log(100), np.log(1e4)))))
+            if r + 1 < rows:
+                c.R(f"rv{r}_{k}", mesh(r, k), mesh(r + 1, k), float(np.exp(rng.uniform(np.log(100), np.log(1e4)))))
+            c.C(f"cm{r}_{k}", mesh(r, k), "0", float(np.exp(rng.uniform(np.log(1e-15), np.log(1e-13)))))
+            if r in (0, rows - 1) or k in (0, cols - 1):
+                c.R(f"re{r}_{k}", mesh(r, k), "vref", 1e3)
+    nm = dict(B3_NMOS[0])
+    pm = dict(B3_PMOS)
+
+    def nmos(name, d, g, s_, w):
+        c.B3(name, d, g, s_, "0", w=w, l=0.18e-6, **nm)
+
+    def pmos(name, d, g, s_, w):
+        c.B3(name, d, g, s_, "vdd", w=w, l=0.18e-6, **pm)
+
+    # bias network: I_k into a diode NMOS (nb_k), mirrored into a diode PMOS (pb_k)
+    for k in range(6):
+        c.I(f"ib{k}", "vdd", f"nb{k}", dc=10e-6)
+        nmos(f"mbn{k}", f"nb{k}", f"nb{k}", "0", 2e-6)
+        nmos(f"mbm{k}", f"pb{k}", f"nb{k}", "0", 2e-6)
+        pmos(f"mbp{k}", f"pb{k}", f"pb{k}", "vdd", 4e-6)
+    interior = [(r, k) for r in range(1, rows - 1) for k in range(1, cols - 1)]
+    picks = rng.choice(len(interior), size=2 * n_ota, replace=False)
+    for o in range(n_ota):
+        a = mesh(*interior[picks[2 * o]])
+        b = mesh(*interior[picks[2 * o + 1]])
+        t, mm, out = f"t{o}", f"l{o}", f"o{o}"
+        nmos(f"m1_{o}", mm, a, t, 4e-6)      # + input
+        nmos(f"m2_{o}", out, out, t, 4e-6)   # - input tied to the output
+        pmos(f"m3_{o}", mm, mm, "vdd", 8e-6)
+        pmos(f"m4_{o}", out, mm, "vdd", 8e-6)
+        nmos(f"m5_{o}", t, f"nb{o % 6}", "0", 4e-6)
+        c.R(f"ro{o}", out, b, 2e3)
+    # source follower on the last OTA's output
+    nmos("msf", "vdd", f"o{n_ota - 1}", "sf", 4e-6)
+    nmos("msk", "sf", "nb0", "0", 2e-6)
+    fr = c.freeze()
+    from .circuit import I as I_, V as V_
+    vsl = fr.slots_of(V_, "dc")
+    isl = fr.slots_of(I_, "dc")
+    tsl = fr.slots_of(B3, "temp")
+    dsl = fr.slots_of(B3, "delvto")
+    n_dev = len(tsl)
+    group = np.arange(n_dev) % 7
+
+    def expand(params):
+        params = np.atleast_2d(np.asarray(params, np.float64))
+        out = np.empty((params.shape[0], 2 + 6 + 2 * n_dev))
+        out[:, 0:2] = params[:, 0:2]
+        out[:, 2:8] = params[:, 2:8]
+        out[:, 8:8 + n_dev] = params[:, 8:9] + 273.15
+        out[:, 8 + n_dev:] = params[:, 9 + group]
+        return out
+
+    expand.slots = list(vsl) + list(isl) + list(tsl) + list(dsl)
+    expand.n_devices = n_dev
+    return fr, expand
+
+
+def analog_block_params(seed: int = 1, points: int = 65536):
+    """The 16 parameters of `points` analog-block points, uniform from seed:
+    [points][16] in ANALOG_PARAMS order, and the nominal point [16]."""
+    rng = np.random.default_rng(seed + 4000)
+    p = np.empty((points, 16))
+    p[:, 0] = rng.uniform(1.6, 2.0, points)
+    p[:, 1] = rng.uniform(0.8, 1.0, points)
+    p[:, 2:8] = np.exp(rng.uniform(np.log(1e-6), np.log(100e-6), size=(points, 6)))
+    p[:, 8] = rng.uniform(-40.0, 125.0, points)
+    p[:, 9:16] = rng.uniform(-0.05, 0.05, size=(points, 7))
+    nominal = np.array([1.8, 0.9] + [10e-6] * 6 + [27.0] + [0.0] * 7)
+    return p, nominal
+
+
+MESH_GATES_SIZES = [50, 100, 200, 400, 700, 1000, 1500, 2000]
+
+
+def mesh_gates(size: int, seed: int = 1):
+    """One uneven-batch topology of about `size` unknowns. Returns (frozen
+    circuit, [supply dc slot])."""
+    rng = np.random.default_rng(seed * 7919 + size)
+    n_gates = max(2, size // 12)
+    # mesh nodes: the size less the NAND2 internal nodes and the supply's node and branch
+    n_mesh = max(9, size - n_gates // 2 - 2)
+    cols = int(np.ceil(np.sqrt(n_mesh)))
+    c = Circuit()
+    c.V("vdd", "vdd", "0", dc=1.8)
+    mesh = lambda i: f"m{i}"  # noqa: E731
+    for i in range(n_mesh):
+        r, k = divmod(i, cols)
+        if k + 1 < cols and i + 1 < n_mesh:
+            c.R(f"rh{i}", mesh(i), mesh(i + 1), float(np.exp(rng.uniform(np.log(10), np.log(1e4)))))
+        if i + cols < n_mesh:
+            c.R(f"rv{i}", mesh(i), mesh(i + cols), float(np.exp(rng.uniform(np.log(10), np.log(1e4)))))
+        c.C(f"cm{i}", mesh(i), "0", float(np.exp(rng.uniform(np.log(1e-15), np.log(1e-13)))))
+    c.R("rtie0", mesh(0), "0", 1e3)
+    c.R("rtie1", mesh(n_mesh - 1), "vdd", 1e3)
+    card_n = dict(type=1.0)
+    card_p = dict(type=-1.0)
+    def near(i):
+        # a mesh node within two rows and columns of node i (a gate's pins
+        # are near each other on the layout), not i itself
+        r, k = divmod(i, cols)
+        while True:
+            rr = int(np.clip(r + rng.integers(-2, 3), 0, (n_mesh - 1) // cols))
+            kk = int(np.clip(k + rng.integers(-2, 3), 0, cols - 1))
+            j = rr * cols + kk
+            if j != i and j < n_mesh:
+                return j
+
+    for g in range(n_gates):
+        w = float(np.exp(rng.uniform(np.log(0.2e-6), np.log(2e-6))))
+        centre = int(rng.integers(n_mesh))
+        a1 = near(centre)
+        a2 = near(centre)
+        while a2 == a1:
+            a2 = near(centre)
+        ins = [mesh(a1), mesh(a2), mesh(centre)]
+        out = ins[2]
+        if g % 2 == 0:  # inverter
+            c.B3(f"mn{g}", out, ins[0], "0", "0", w=w, l=0.18e-6, **card_n)
+            c.B3(f"mp{g}", out, ins[0], "vdd", "vdd", w=2 * w, l=0.18e-6, **card_p)
+        else:  # NAND2
+            mid = f"x{g}"
+            c.B3(f"mna{g}", out, ins[0], mid, "0", w=w, l=0.18e-6, **card_n)
+            c.B3(f"mnb{g}", mid, ins[1], "0", "0", w=w, l=0.18e-6, **card_n)
+            c.B3(f"mpa{g}", out, ins[0], "vdd", "vdd", w=2 * w, l=0.18e-6, **card_p)
+            c.B3(f"mpb{g}", out, ins[1], "vdd", "vdd", w=2 * w, l=0.18e-6, **card_p)
+    fr = c.freeze()
+    return fr, [fr.slot("vdd", "dc")]

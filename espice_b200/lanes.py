@@ -30,7 +30,8 @@ EXPORTS = ["esl_create", "esl_destroy", "esl_last_error", "esl_dims", "esl_set_l
            "esl_tape_size", "esl_pattern", "esl_compile_tape", "esl_tran", "esl_tran_device", "esl_lu_lanes_device",
            "esl_lu_lanes_mixed_device", "esl_group_dc_solve_device", "esl_autotune", "esl_dc_sweep_device",
            "esl_tran_meas_device", "esl_lu_lanes_compiled_device", "esl_lu_compiled_log",
-           "esl_lu_compiled_source", "esl_lu_lanes_mixed_compiled_device", "esl_lu_compiled_mixed_source"]
+           "esl_lu_compiled_source", "esl_lu_lanes_mixed_compiled_device", "esl_lu_compiled_mixed_source",
+           "esl_set_mode", "esl_block_info", "esl_block_profile"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 f64p = ctypes.POINTER(ctypes.c_double)
@@ -58,10 +59,31 @@ class Options(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("lanes", ctypes.c_uint32), ("converged", ctypes.c_uint32),
                 ("peeled", ctypes.c_uint32), ("host_solves", ctypes.c_uint32),
-                ("launches", ctypes.c_uint32), ("kernel_ms", ctypes.c_double)]
+                ("launches", ctypes.c_uint32), ("kernel_ms", ctypes.c_double),
+                ("path", ctypes.c_uint32), ("refinements", ctypes.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+PREC_FP64, PREC_MIXED = 0, 1
+PATH_AUTO, PATH_WARP, PATH_BLOCK = 0, 1, 2
+
+
+class SolveMode(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_uint32), ("path", ctypes.c_uint32), ("block_threads", ctypes.c_uint32),
+                ("refine_max", ctypes.c_uint32), ("refine_tol", ctypes.c_double), ("profile", ctypes.c_uint32),
+                ("pad", ctypes.c_uint32)]
+
+
+BLOCK_PHASES = ["eval", "assemble", "refactor", "solve", "refine", "gates", "iterations"]
+
+
+class BlockInfo(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint32) for k in ("width", "a_rows", "b_rows", "f_rows", "a_levels", "a_nops",
+                                                 "b_nops", "ntv", "warp_ok")] + \
+               [("lane_bytes", ctypes.c_uint32 * 2), ("in_smem", ctypes.c_uint32 * 2),
+                ("ctas_per_sm", ctypes.c_uint32 * 2)]
 
 
 class TranOpts(ctypes.Structure):
@@ -315,6 +337,28 @@ class DcLanes:
                                                 ctypes.byref(stats)),
                     "esl_dc_solve_device")
         return stats.as_dict()
+
+    def set_mode(self, precision=PREC_FP64, path=PATH_AUTO, block_threads=0, refine_tol=0.0, refine_max=0,
+                 profile=False):
+        """esl_set_mode: FP64 or mixed precision; the warp lanes, the block
+        lanes, or either (PATH_AUTO); profile: count the block lanes' phase
+        cycles (block_profile)."""
+        m = SolveMode(precision, path, block_threads, refine_max, refine_tol, int(profile), 0)
+        self._check(self._L.esl_set_mode(self._ctx, ctypes.byref(m)), "esl_set_mode")
+
+    def block_profile(self):
+        """The last profiled block-lane solve's cycles by phase (BLOCK_PHASES)."""
+        c = (ctypes.c_uint64 * len(BLOCK_PHASES))()
+        self._check(self._L.esl_block_profile(self._ctx, c), "esl_block_profile")
+        return dict(zip(BLOCK_PHASES, [int(v) for v in c]))
+
+    def block_info(self):
+        info = BlockInfo()
+        self._check(self._L.esl_block_info(self._ctx, ctypes.byref(info)), "esl_block_info")
+        out = {k: getattr(info, k) for k, _ in info._fields_[:9]}
+        for k in ("lane_bytes", "in_smem", "ctas_per_sm"):
+            out[k] = list(getattr(info, k))
+        return out
 
     def solve_device_static(self, d_x, d_iters, d_status, cold=False, opts=None):
         """solve_device through the allocation-free entry point (fixed lane

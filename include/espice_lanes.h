@@ -114,7 +114,37 @@ typedef struct {
     uint32_t host_solves;  /* host factor+solve calls (lane_solver.zig peels) */
     uint32_t launches;     /* kernel launches in the call */
     double kernel_ms;      /* device time of the Newton launches */
+    uint32_t path;         /* the lanes that ran: ESL_PATH_WARP or ESL_PATH_BLOCK */
+    uint32_t refinements;  /* mixed precision: FP64 refinement corrections, all lanes */
 } esl_stats;
+
+/* How a context's DC solves run (esl_set_mode). No reference counterpart:
+ * the reference's lane LU is FP64 and one thread per lane.
+ *
+ * precision: ESL_PREC_FP64 (the default), or ESL_PREC_MIXED: the refactor
+ * and the triangular solves in FP32 on the same pivot tape, each Newton step
+ * then refined in FP64 (residual -F - J dx from the FP64 Jacobian, the
+ * correction solved on the FP32 factors) until max |res| <= refine_tol *
+ * max |F| or refine_max corrections; device evaluation, assembly, the
+ * update and the Newton gates stay FP64. A lane the FP32 factors cannot
+ * stand in for (the pivot tests on them) takes the host's FP64 factor.
+ * path: ESL_PATH_AUTO picks the warp lanes (a warp per lane, its working
+ * set in shared memory) for FP64 when the tape fits them, else the block
+ * lanes (a CTA per lane, block_threads wide: 128 or 256, 0 = 256; the
+ * working set in shared memory when it fits, else in global memory, for any
+ * circuit size); ESL_PATH_WARP / ESL_PATH_BLOCK force one (the warp lanes
+ * are FP64 only). refine_tol 0 takes 1e-12, refine_max 0 takes 6. */
+enum { ESL_PREC_FP64 = 0, ESL_PREC_MIXED = 1 };
+enum { ESL_PATH_AUTO = 0, ESL_PATH_WARP = 1, ESL_PATH_BLOCK = 2 };
+typedef struct {
+    uint32_t precision;
+    uint32_t path;
+    uint32_t block_threads;
+    uint32_t refine_max;
+    double refine_tol;
+    uint32_t profile;  /* != 0: block-lane solves count their phase cycles (esl_block_profile) */
+    uint32_t pad;
+} esl_solve_mode;
 
 /* Builds the pattern, column order and stamp tables of `circuit` on
  * `opts->device` (NULL: device 0). Replaces GpuLanes.init's pattern and
@@ -148,7 +178,8 @@ int32_t esl_dc_solve(esl_ctx *ctx, const esl_newton_opts *opts, const double *x0
 /* esl_dc_solve on device buffers: d_x [n_lanes][n] start points in place of
  * x0 (overwritten with the solutions), d_iters/d_status device arrays.
  * cold != 0 seeds the junctions and starts from zero. Returns once the
- * lanes are done (host peels included). */
+ * lanes are done (host peels included). Runs on the warp or the block lanes
+ * in the context's precision (esl_set_mode). */
 int32_t esl_dc_solve_device(esl_ctx *ctx, const esl_newton_opts *opts, double *d_x, int cold,
                             uint32_t *d_iters, uint32_t *d_status, esl_stats *stats);
 
@@ -293,6 +324,28 @@ int32_t esl_dc_sweep_device(esl_ctx *ctx, const esl_slot *slot, const double *va
 int32_t esl_group_dc_solve_device(esl_ctx *const *ctxs, uint32_t n_ctx, const esl_newton_opts *opts,
                                   double *const *d_x, const int *cold, uint32_t *const *d_iters,
                                   uint32_t *const *d_status, esl_stats *stats);
+
+/* Sets how the context's later DC solves (esl_dc_solve, esl_dc_solve_device)
+ * run. */
+int32_t esl_set_mode(esl_ctx *ctx, const esl_solve_mode *mode);
+
+/* The block lanes' programs and working set for the context's tape (after
+ * its first solve): rows of `width` ops in programs A (refactor + forward
+ * solve, a_levels its longest dependence chain), B and F; the tape's
+ * values and ops; per precision (0 FP64, 1 mixed) a lane's working-set
+ * bytes, whether it sits in shared memory, and CTAs per SM. */
+typedef struct {
+    uint32_t width, a_rows, b_rows, f_rows, a_levels, a_nops, b_nops, ntv, warp_ok;
+    uint32_t lane_bytes[2], in_smem[2], ctas_per_sm[2];
+} esl_block_info_t;
+int32_t esl_block_info(esl_ctx *ctx, esl_block_info_t *info);
+
+/* The SM cycles of the last block-lane solve by phase, summed over its
+ * CTAs (each CTA's thread 0 reads clock64 between phases), when the mode
+ * asked for a profile: cycles[0] device evaluation, [1] assembly, [2]
+ * refactor + forward solve, [3] back solve and step, [4] mixed refinement,
+ * [5] update, limiting and gates, [6] the Newton iterations counted. */
+int32_t esl_block_profile(esl_ctx *ctx, uint64_t *cycles);
 
 /* Picks the context's lanes per CTA (1, 2, 4 or 8, as shared memory allows)
  * by timing its DC solve from x0 (NULL: cold) on its current lanes; keeps
