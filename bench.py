@@ -455,75 +455,208 @@ def ring_period_early_stop(args, local, flush):
             "period_s_median": float(np.nanmedian(v[:, 0]))}
 
 
-def learned_dc(args, local, flush):
-    """The learned warm start against the plain FP64 lanes on the 16-parameter
-    grid-with-diodes deck: 65536 seeded points, the network trained on the
-    first 32768 (their plain-solver solutions, from the nominal warm start),
-    both paths timed on the other 32768: plain from the nominal start, learned
-    from the network's guesses (inference included) with an 8-iteration cap
-    and the nominal fallback."""
+# The accuracy setting of the metric's configurations: Newton stops when a
+# step is below 1e-9 of the unknown (and 1e-12 V / 1e-15 A), so every start
+# converges to the same solution within the parity tolerance (at reltol 1e-3
+# a point's result depends on its start at the 1e-3 level).
+TIGHT = dict(reltol=1e-9, vntol=1e-12, abstol=1e-15)
+
+
+def _dev(a, b):
+    """(max relative deviation of a from b, fraction of points within 1e-9
+    relative or 1e-12 absolute on every unknown)."""
+    d = np.abs(a - b)
+    scale = np.maximum(np.abs(a), np.abs(b))
+    rel = np.where(d > 1e-12, d / np.maximum(scale, 1e-300), 0.0)
+    within = np.all(d <= 1e-12 + 1e-9 * scale, axis=1)
+    return float(rel.max()), float(within.mean())
+
+
+def learned_mixed_c4(args, local, flush, points=65536, n_train=32768):
+    """The metric on its configuration: the learned warm start with the
+    mixed-precision lanes against the plain FP64 lanes, on the 500-unknown
+    BSIM3 analog block (120 MOSFETs, 16 parameters), 65,536 seeded points at
+    the 1e-9 setting. The network (16 -> 512 -> 512 -> n, tanh, BF16
+    tcgen05 GEMMs with FP32 accumulation) is trained on the GPU on 32,768
+    other points' plain-solver solutions. Plain: FP64 block lanes from the
+    nominal operating point. Learned + mixed: the network's guesses
+    (inference included), the mixed-precision lanes capped at 8 Newton
+    iterations, the lanes that did not converge again from the nominal point.
+    Each path is timed by wall clock with the device synchronised on both
+    sides, every point's lane state resident."""
     import torch
     from espice_b200 import decks, lanes, learned
-    fr, slots, values, nominal = decks.grid_diodes_16(points=65536)
-    train, test = values[:32768], values[32768:]
-    ctx = lanes.DcLanes(fr, device=local)
-    fb = lanes.DcLanes(fr, device=local)
-    ctx.set_lanes(slots, nominal[None, :])
-    x_nom = ctx.solve(x0=None)[0][0]
-    ctx.set_lanes(slots, train)
-    x_tr, _, st_tr, _ = ctx.solve(x0=x_nom)
+    from oracle import oracle
+    fr, expand = decks.analog_block()
+    p_train, nominal = decks.analog_block_params(seed=1, points=n_train)
+    p_test, _ = decks.analog_block_params(seed=2, points=points)
+    opts = lanes.newton_opts(**TIGHT)
+    oo = oracle.newton_opts(**TIGHT)
+    plain = lanes.DcLanes(fr, device=local)
+    plain.set_mode(precision=lanes.PREC_FP64, path=lanes.PATH_BLOCK)
+    plain.set_lanes(expand.slots, expand(nominal))
+    x_nom = plain.solve(x0=None, opts=opts)[0][0]
+    t0 = time.perf_counter()
+    plain.set_lanes(expand.slots, expand(p_train))
+    x_tr, _, st_tr, _ = plain.solve(x0=np.broadcast_to(x_nom, (n_train, fr.n)), opts=opts)
+    t_data = time.perf_counter() - t0
     ok = st_tr == lanes.LANE_CONVERGED
-    ws = learned.LearnedWarmStart(len(slots), fr.n, hidden=256, layers=3)
+    ws = learned.LearnedWarmStart(16, fr.n, hidden=512, layers=3)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    loss = ws.fit(train[ok], x_tr[ok], epochs=60, batch=256, lr=2e-3)
+    loss = ws.fit(p_train[ok], x_tr[ok], epochs=60, batch=256, lr=2e-3, lr_end=2e-5)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
-    ctx.set_lanes(slots, test)
-    N, n = test.shape[0], fr.n
+    vals = expand(p_test)
+    t0 = time.perf_counter()
+    plain.set_lanes(expand.slots, vals)
+    t_set = time.perf_counter() - t0
+    mixed = lanes.DcLanes(fr, device=local)
+    mixed.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK)
+    mixed.set_lanes(expand.slots, vals)
+    fb = lanes.DcLanes(fr, device=local)
+    fb.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK)
+    N, n = points, fr.n
     d_x = torch.empty((N, n), dtype=torch.float64, device="cuda")
     d_it = torch.zeros(N, dtype=torch.int32, device="cuda")
     d_st = torch.zeros(N, dtype=torch.int32, device="cuda")
     x_nom_d = torch.tensor(x_nom, device="cuda")
-    d_vals = torch.tensor(test, dtype=torch.float32, device="cuda")  # resident, as the lanes' records are
-    opts = lanes.newton_opts()
-    plain_t, learned_t, it_p, it_l, conv_p, conv_l, fallback = [], [], 0.0, 0.0, 0, 0, 0
-    for i in range(args.warmup + args.steps):
+    d_p = torch.tensor(p_test, dtype=torch.float32, device="cuda")
+    steps = max(1, min(args.steps, 3))
+    plain_t, mixed_t, it_p, it_l, conv_p, conv_l, fallback, refine = [], [], 0.0, 0.0, 0, 0, 0, 0
+    for i in range(1 + steps):
         flush.zero_()
+        d_x.copy_(x_nom_d.expand(N, n))
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        d_x.copy_(x_nom_d.expand(N, n))
-        ctx.solve_device(d_x.data_ptr(), d_it.data_ptr(), d_st.data_ptr(), cold=False, opts=opts)
+        st_p = plain.solve_device(d_x.data_ptr(), d_it.data_ptr(), d_st.data_ptr(), cold=False, opts=opts)
         torch.cuda.synchronize()
         t2 = time.perf_counter()
-        if i >= args.warmup:
+        if i >= 1:
             plain_t.append(t2 - t1)
             it_p += float(d_it.double().mean())
             conv_p += int((d_st == lanes.LANE_CONVERGED).sum())
+        x_plain = d_x.cpu().numpy() if i == steps else None
         flush.zero_()
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        _, it, conv, nfb = learned.solve(ctx, fb, ws, slots, test, x_nom, k=8, opts=opts, d_values=d_vals)
+        xl, it, conv, nfb = learned.solve(mixed, fb, ws, expand.slots, vals, x_nom, k=8, opts=opts, d_values=d_p)
         torch.cuda.synchronize()
         t2 = time.perf_counter()
-        if i >= args.warmup:
-            learned_t.append(t2 - t1)
+        if i >= 1:
+            mixed_t.append(t2 - t1)
             it_l += float(it.mean())
             conv_l += int(conv.sum())
             fallback += nfb
+        if i == steps:
+            x_learned = xl.cpu().numpy()
+    # attribution: the learned start on the FP64 lanes, and the mixed lanes
+    # from the nominal start (device time of one solve each)
+    guess = ws.predict(d_p, N).cpu().numpy()
+    _, it_lf, _, s_lf = plain.solve(x0=guess, opts=opts)
+    _, it_mn, _, s_mn = mixed.solve(x0=np.broadcast_to(x_nom, (N, n)), opts=opts)
+    s_pn = plain.solve(x0=np.broadcast_to(x_nom, (N, n)), opts=opts)[3]
+    # accuracy: every point against the plain FP64 lanes, a sample against
+    # the CPU oracle (FP64, from the nominal start)
+    idx = np.arange(0, N, 1024)
+    xo, ito, cvo = oracle.dc_points(fr, expand.slots, vals[idx], warm=x_nom, opts=oo)
+    dev_plain_oracle = _dev(x_plain[idx], xo)
+    dev_learned_oracle = _dev(x_learned[idx], xo)
+    dev_learned_plain = _dev(x_learned, x_plain)
+    for c in (plain, mixed, fb):
+        c.close()
     ws.close()
-    fb.close()
-    ctx.close()
-    k = args.steps
-    return {"workload": "grid_diodes_16: the grid-with-diodes deck, 16 swept parameters (source 0..5 V, 15 "
-                        "resistors x exp(U(-0.7, 0.7))), 32768 held-out points; network 16->256->256->82 "
-                        "(tanh, BF16 tcgen05 GEMMs, FP32 accumulation) trained on 32768 plain-solver points",
-            "plain_points_per_s": conv_p / sum(plain_t), "learned_points_per_s": conv_l / sum(learned_t),
-            "speedup": (conv_l / sum(learned_t)) / (conv_p / sum(plain_t)),
-            "newton_iters_plain": it_p / k, "newton_iters_learned": it_l / k, "fallback_lanes": fallback / k,
-            "train_s": t_train, "train_loss_first_last": [float(loss[0]), float(loss[-1])],
-            "timing": "wall clock around each path with device synchronisation (inference, solve and "
-                      "fallback included)"}
+    k = len(plain_t)
+    pp = conv_p / sum(plain_t)
+    pl = conv_l / sum(mixed_t)
+    return {"workload": f"analog_block: 500-unknown BSIM3 analog block ({fr.n} unknowns incl. ground, 120 MOSFETs: "
+                        "20 five-transistor OTA followers on a 20x21 RC mesh, a 6-branch bias network, a source "
+                        "follower), 16 parameters (VDD, VREF, 6 bias currents 1-100 uA log-uniform, temperature "
+                        "-40..125 C, 7 DELVTO shifts +-50 mV); 65,536 test points, 32,768 training points",
+            "newton": "reltol 1e-9, vntol 1e-12, abstol 1e-15 (every start converges to the same solution within "
+                      "1e-9; at reltol 1e-3 a point's result depends on its start at the 1e-3 level)",
+            "plain_points_per_s": pp, "learned_mixed_points_per_s": pl,
+            "learned_mixed_over_plain": pl / pp,
+            "attribution_device_ms": {"plain_fp64_nominal": s_pn["kernel_ms"],
+                                      "learned_fp64": s_lf["kernel_ms"], "mixed_nominal": s_mn["kernel_ms"],
+                                      "learned_over_plain_fp64": s_pn["kernel_ms"] / s_lf["kernel_ms"],
+                                      "mixed_over_fp64_nominal": s_pn["kernel_ms"] / s_mn["kernel_ms"]},
+            "newton_iters_plain": it_p / k, "newton_iters_learned": it_l / k,
+            "newton_iters_learned_fp64": float(it_lf.mean()), "fallback_lanes": fallback / k,
+            "max_rel_dev": {"plain_vs_cpu_oracle": dev_plain_oracle[0],
+                            "learned_mixed_vs_cpu_oracle": dev_learned_oracle[0],
+                            "learned_mixed_vs_plain_all_points": dev_learned_plain[0]},
+            "within_1e-9": {"plain_vs_cpu_oracle": dev_plain_oracle[1],
+                            "learned_mixed_vs_cpu_oracle": dev_learned_oracle[1],
+                            "learned_mixed_vs_plain_all_points": dev_learned_plain[1]},
+            "oracle_sample": f"{len(idx)} points (every 1024th)",
+            "setup_s": {"record_derivation_65536": t_set, "training_solutions_32768": t_data,
+                        "training_60_epochs": t_train},
+            "train_loss_first_last": [float(loss[0]), float(loss[-1])],
+            "timing": "wall clock around each path with device synchronisation (inference, solves and fallback "
+                      f"included), {k} steps after one warm-up, L2 flushed before each path"}
+
+
+def uneven_c3(args, local, flush, lanes_per_topo=512):
+    """Uneven batching on its configuration: 4,096 DC lanes over the eight
+    mesh-with-gates topologies (50 to 2,000 unknowns, 512 supply values each
+    in [0.8, 1.8] V) in one launch of the block lanes, cold starts, plain FP64
+    against mixed precision (refinement to 1e-12 of the residual)."""
+    import torch
+    from espice_b200 import decks, lanes
+    from oracle import oracle
+    sizes = decks.MESH_GATES_SIZES
+    vals = np.linspace(0.8, 1.8, lanes_per_topo).reshape(-1, 1)
+    out = {"workload": "mesh_gates: 8 seeded topologies of " + ", ".join(str(s) for s in sizes) +
+                       f" unknowns (RC mesh + BSIM3 INV/NAND2), {lanes_per_topo} supply values each, one launch",
+           "newton": "reltol 1e-3, vntol 1e-6 (the deck defaults), cold starts"}
+    res = {}
+    for prec, name in ((lanes.PREC_FP64, "fp64"), (lanes.PREC_MIXED, "mixed")):
+        ctxs, bufs = [], []
+        for sz in sizes:
+            fr, slots = decks.mesh_gates(sz)
+            c = lanes.DcLanes(fr, device=local)
+            c.set_mode(precision=prec, path=lanes.PATH_BLOCK)
+            c.set_lanes(slots, vals)
+            ctxs.append(c)
+            bufs.append((torch.zeros((lanes_per_topo, fr.n), dtype=torch.float64, device="cuda"),
+                         torch.zeros(lanes_per_topo, dtype=torch.int32, device="cuda"),
+                         torch.zeros(lanes_per_topo, dtype=torch.int32, device="cuda")))
+        times, conv = [], 0
+        for i in range(2):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            st = lanes.group_solve_device(ctxs, [b[0].data_ptr() for b in bufs], [b[1].data_ptr() for b in bufs],
+                                          [b[2].data_ptr() for b in bufs], cold=[True] * len(ctxs))
+            torch.cuda.synchronize()
+            if i == 1:
+                times.append(time.perf_counter() - t1)
+                conv = sum(int((b[2] == lanes.LANE_CONVERGED).sum()) for b in bufs)
+        res[name] = {"points_per_s": conv / times[0], "converged": conv, "device_ms": st[0]["kernel_ms"],
+                     "x": [b[0].cpu().numpy() for b in bufs],
+                     "refinements_per_lane": sum(s["refinements"] for s in st) / (lanes_per_topo * len(sizes))}
+        for c in ctxs:
+            c.close()
+    out["plain_points_per_s"] = res["fp64"]["points_per_s"]
+    out["mixed_points_per_s"] = res["mixed"]["points_per_s"]
+    out["mixed_over_plain"] = res["mixed"]["points_per_s"] / res["fp64"]["points_per_s"]
+    out["device_ms"] = {k: res[k]["device_ms"] for k in res}
+    out["refinements_per_lane"] = res["mixed"]["refinements_per_lane"]
+    devs, worst = [], 0.0
+    for t, sz in enumerate(sizes):
+        fr, slots = decks.mesh_gates(sz)
+        idx = np.arange(0, lanes_per_topo, 128)
+        xo, _, cvo = oracle.dc_points(fr, slots, vals[idx], warm=None)
+        ok = cvo.astype(bool)
+        dp, wp = _dev(res["fp64"]["x"][t][idx][ok], xo[ok])
+        dm, wm = _dev(res["mixed"]["x"][t][idx][ok], xo[ok])
+        worst = max(worst, dm)
+        devs.append({"unknowns": fr.n, "plain_vs_oracle": dp, "mixed_vs_oracle": dm, "mixed_within": wm})
+    out["per_topology_max_rel_dev"] = devs
+    out["mixed_max_rel_dev_vs_cpu_oracle"] = worst
+    out["oracle_sample"] = "4 lanes per topology (every 128th)"
+    return out
 
 
 def our_arm(args, rank, world):
@@ -628,7 +761,8 @@ def our_arm(args, rank, world):
     out["dc_sweep_lanes"] = dc_sweep_lanes(args, local, flush)
     out["ring_period_early_stop"] = ring_period_early_stop(args, local, flush)
     if args.learned:
-        out["learned_warm_start"] = learned_dc(args, local, flush)
+        out["learned_mixed_c4"] = learned_mixed_c4(args, local, flush)
+        out["uneven_c3"] = uneven_c3(args, local, flush)
     out["lu_roofline"] = lu_lanes_roofline(fr, ctx, hbm_peak, peak_src)
     out["lu_roofline_warp_per_lane"] = lu_replay_roofline(fr, ctx, hbm_peak, peak_src)
     if args.cpu_baseline:

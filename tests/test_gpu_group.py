@@ -57,3 +57,46 @@ def test_autotune_keeps_results():
     assert np.array_equal(x1.view(np.uint64), x2.view(np.uint64))
     assert np.array_equal(it1, it2) and np.array_equal(st1, st2)
     ctx.close()
+
+
+@pytest.mark.parametrize("precision", [lanes.PREC_FP64, lanes.PREC_MIXED])
+def test_block_group_uneven_batch_against_oracle(precision):
+    """The uneven batch on the block lanes: the eight mesh-with-gates
+    topologies (50 to 2,000 unknowns), six supply values each, in one launch
+    (work items largest topology first; the two largest keep their working
+    set in global memory). FP64: every lane bitwise the oracle, the same
+    iteration counts. Mixed: the oracle's convergence, values within 1e-9
+    relative or 1e-12 absolute."""
+    import torch
+    import parity
+    from oracle import oracle
+    vals = np.linspace(0.8, 1.8, 6).reshape(-1, 1)
+    ctxs, bufs, decks_ = [], [], []
+    for size in decks.MESH_GATES_SIZES:
+        fr, slots = decks.mesh_gates(size)
+        c = lanes.DcLanes(fr)
+        c.set_mode(precision=precision, path=lanes.PATH_BLOCK)
+        c.set_lanes(slots, vals)
+        ctxs.append(c)
+        decks_.append((fr, slots))
+        bufs.append((torch.zeros((len(vals), fr.n), dtype=torch.float64, device="cuda"),
+                     torch.zeros(len(vals), dtype=torch.int32, device="cuda"),
+                     torch.zeros(len(vals), dtype=torch.int32, device="cuda")))
+    torch.cuda.synchronize()
+    stats = lanes.group_solve_device(ctxs, [b[0].data_ptr() for b in bufs], [b[1].data_ptr() for b in bufs],
+                                     [b[2].data_ptr() for b in bufs], cold=[True] * len(ctxs))
+    torch.cuda.synchronize()
+    for (fr, slots), b, s, c in zip(decks_, bufs, stats, ctxs):
+        assert s["path"] == lanes.PATH_BLOCK
+        x = b[0].cpu().numpy()
+        it = b[1].cpu().numpy().astype(np.uint32)
+        st = b[2].cpu().numpy().astype(np.uint32)
+        xo, ito, cvo = oracle.dc_points(fr, slots, vals, warm=None)
+        conv = st == lanes.LANE_CONVERGED
+        if precision == lanes.PREC_FP64:
+            assert parity.assert_dc_parity(fr, slots, vals, None, oracle.newton_opts(), x, it, conv, xo, ito, cvo,
+                                           f"group n={fr.n}") == 1.0
+        else:
+            assert np.array_equal(conv, cvo.astype(bool))
+            assert parity.close(x[conv], xo[conv]).all(), float(np.max(np.abs(x[conv] - xo[conv])))
+        c.close()
