@@ -252,6 +252,7 @@ struct esl_ctx {
   DevBuf d_nodes[kMaxBatches], d_rhs_ptr, d_rhs_src, d_a_ptr, d_a_src, d_slot_row, d_cur;
   DevBuf d_q_ptr, d_q_src, d_c_ptr, d_c_src, d_probes, d_tran_t, d_tran_v, d_tran_n, d_tran_stats;
   DevBuf d_amap, d_fill, d_prog, d_l_scaled, d_pinv, d_q, d_seq, d_sweep_values, d_meas, d_next_lane;
+  DevBuf d_sweep_state, d_sweep_rows;  // paused sweep lanes' state
   uint32_t n_seq_a = 0, n_seq = 0, seq_warps = 0;  // lane-interleaved op list
   uint32_t n_seq_f = 0, mixed_warps = 0;            // its forward-only tail, the mixed kernel's warps
   LuJitKernels lu_jit;                               // the tape-compiled lane LU of the current tape
@@ -1573,11 +1574,31 @@ int32_t esl_dc_sweep_device(esl_ctx* ctx, const esl_slot* slot, const double* va
   P.conv = d_conv;
   P.status = d_status;
   const LaneOpts o{opts->reltol, opts->abstol, opts->vntol, opts->residual_tol, opts->gmin, opts->max_iter, 0, 0};
+  const uint32_t N = ctx->n_lanes;
+  ESL_CUDA(ctx->d_sweep_state.ensure(size_t(N) * kSweepStateN * 4));
+  ESL_CUDA(ctx->d_sweep_rows.ensure(size_t(N) * 2 * T.n * 8));
+  P.state = ctx->d_sweep_state.as<uint32_t>();
+  P.rows = ctx->d_sweep_rows.as<double>();
+  // every lane running on the lead tape; lanes that pause are served on
+  // the host (serve_pauses) and resumed where they stopped
   LaneDev L = lane_view(ctx, 0);
+  ESL_CUDA(cudaMemsetAsync(L.status, 0, size_t(N) * 4, s));
+  ESL_CUDA(cudaMemsetAsync(L.flags, 0, size_t(N) * 4, s));
+  ESL_CUDA(cudaMemsetAsync(L.n_paused, 0, 4, s));
+  ctx->peel.clear();
   ESL_CUDA(ctx->d_next_lane.ensure(sizeof(uint32_t)));
   P.next_lane = ctx->d_next_lane.as<uint32_t>();
+  const uint32_t lpb = lanes_per_cta(ctx, N, fit);
   ESL_CUDA(cudaEventRecord(ctx->ev0, s));
-  ESL_CUDA(launch_sweep(T, L, P, o, lanes_per_cta(ctx, ctx->n_lanes, fit), s));
+  ESL_CUDA(launch_sweep(T, L, P, o, lpb, s));
+  for (;;) {
+    bool any = false;
+    if (int32_t rc = serve_pauses(ctx, L, nullptr, &any)) return rc;
+    if (!any) break;
+    LaneDev R = L;
+    R.resume = 1;
+    ESL_CUDA(launch_sweep(T, R, P, o, lpb, s));
+  }
   ESL_CUDA(cudaEventRecord(ctx->ev1, s));
   ESL_CUDA(cudaEventSynchronize(ctx->ev1));
   if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);

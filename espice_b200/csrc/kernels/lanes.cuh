@@ -142,6 +142,28 @@ struct SweepDev {
   uint8_t* conv;     // [lane][n_pts]
   uint32_t* status;  // [lane]
   uint32_t* next_lane;  // the lane-refill counter, zero at launch
+  // A lane paused for a host factor (LaneDev's pause protocol): where its
+  // sweep stands, [lane][kSweepStateN] words, and its predictor rows, the
+  // last solution and the one before, [lane][2 n].
+  uint32_t* state;
+  double* rows;
+};
+
+// A paused sweep lane's state words.
+enum SweepStateWord : uint32_t {
+  kSwPoint, kSwPhase, kSwItTotal, kSwCold, kSwIter, kSwInitFix, kSwLimActive, kSweepStateN
+};
+
+// A Newton solve's loop state across a pause (sweep lanes): the iteration
+// reached, the runaway bound, the INITFIX flag; on resume, whether the
+// host's step (in y, permuted) or its singular verdict stands for the
+// iteration, and whether every factor of the lane is the host's.
+struct NewtonCarry {
+  uint32_t iter;
+  double limit;
+  uint32_t init_fix;
+  uint32_t resume;     // 0 none, 1 the host's step, 2 the host's factor was singular
+  uint32_t host_mode;  // the lane's factor left the lead tape: pause before every factor
 };
 
 // Shared-memory doubles per lane of sweep_kernel: the lane working set,

@@ -1073,11 +1073,25 @@ __device__ void fill_sources(const TopoDev& T, const double* rec, const SimDev& 
 template <bool kHasB3>
 __device__ int lane_newton(const TopoDev& T, uint32_t prog, const LaneMem& m, const double* rec, const LaneOpts& o,
                            const SimDev& sim, const Companion* cp, bool& lim_active, bool init_fix,
-                           uint32_t& iters, const double* vcache, int tid) {
+                           uint32_t& iters, const double* vcache, int tid, NewtonCarry* carry = nullptr) {
   const uint32_t n = T.n;
   const uint32_t max_iter = o.max_iter < 100 ? 100 : o.max_iter;
   double limit = kXPlausible;
-  for (uint32_t iter = 0; iter < max_iter; ++iter) {
+  uint32_t iter0 = 0;
+  bool have_step = false;
+  if (carry && carry->resume) {
+    // resumed after a host factor: the step for iteration `iter` is the host's
+    iter0 = carry->iter;
+    limit = carry->limit;
+    init_fix = carry->init_fix != 0;
+    if (carry->resume == 2) {
+      iters = iter0 + 1;
+      return 2;
+    }
+    have_step = true;
+  }
+  for (uint32_t iter = iter0; iter < max_iter; ++iter) {
+   if (!have_step) {
     eval_all<kHasB3>(T, rec, m, lim_active, sim, tid, false, vcache);
     __syncwarp();
     assemble(T, prog, m, tid);
@@ -1116,11 +1130,21 @@ __device__ int lane_newton(const TopoDev& T, uint32_t prog, const LaneMem& m, co
       const double scale = fmin(fmax(from_bits(xm), from_bits(fm) * g), 1e18);
       limit = !(1e3 * scale > kXPlausible) ? kXPlausible : 1e3 * scale;
     }
-    if (refactor_forward(T, prog, m.v, tid)) {
+    const bool bad = (carry && carry->host_mode) || refactor_forward(T, prog, m.v, tid);
+    if (bad) {
+      if (carry) {
+        // pause: the caller hands the lane to the host at this iteration
+        carry->iter = iter;
+        carry->limit = limit;
+        carry->init_fix = init_fix;
+        return 3;
+      }
       iters = iter + 1;
       return 2;
     }
     back_solve(T, prog, m.v, tid);
+   }
+    have_step = false;
     __syncwarp();
     uint64_t worst = 0;
     for (uint32_t j = tid; j < n; j += 32) {
@@ -1715,93 +1739,184 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
 // and Newton with MODEINITFIX at the operating point's 100 iterations, the
 // ladder's plain rung (endPoint, dc.zig:361-365). Point 0, once converged,
 // is also `prev` (dc.zig:376-379, after dctrcurv.c). A factor that leaves
-// the lead tape ends the lane's sweep (kSweepLeftTape); its later points
-// read not converged.
+// the lead tape pauses the lane for the host (sweep_lane below).
+//
+// The cold start of a sweep point (op.zig coldStart): x = 0, every junction
+// image at its seed.
+template <bool kHasB3>
+__device__ void sweep_seed(const TopoDev& T, const double* rec, const LaneMem& m, int tid) {
+  for (uint32_t i = tid; i < T.n; i += 32) m.x[i] = 0.0;
+  for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
+    const BatchDev& B = T.b[bi];
+    for (uint32_t i = tid; i < B.count; i += 32) {
+      if (B.type == kD) m.lim[B.lim_off + i] = rec[B.rec_off + kDVcrit * B.count + i];
+      if (B.type == kM) {
+        m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kMSeedVgs * B.count + i];
+        m.lim[B.lim_off + 3 * i + 1] = 0.0;
+        m.lim[B.lim_off + 3 * i + 2] = -1.0;
+      }
+      if (B.type == kB3) {
+        m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kB3SeedVgs * B.count + i];
+        m.lim[B.lim_off + 3 * i + 1] = 0.1;
+        m.lim[B.lim_off + 3 * i + 2] = 0.0;
+      }
+    }
+  }
+}
+
+// A sweep lane (dc.zig Sweep, one per lane): per point, the predictor
+// limited against the last point and a warm Newton; on its failure, or
+// before any point has converged, the cold rung (op.zig's plain rung at 100
+// iterations with MODEINITFIX). A factor the lead tape cannot stand in for
+// pauses the lane (the DC lanes' protocol: the matrix, residual and
+// diagonal to the hand-off planes, L.status kNeedSolve); the host factors it
+// on the lane's own direct solver and a resume launch continues the lane at
+// that point, phase and iteration with the host's step (or its singular
+// verdict). The lane keeps pausing before every factor until its own factor
+// is the lead tape again (the host clears the host-mode flag).
 template <bool kHasB3>
 __device__ void sweep_lane(const TopoDev& T, const LaneDev& L, const SweepDev& P, const LaneOpts& o, uint32_t prog,
                            double* block, uint32_t lane, int tid) {
   const uint32_t n = T.n;
+  const uint32_t lstat = L.status[lane];
+  const bool resuming = L.resume && (lstat == kNeedSolve || lstat == kSingular);
+  if (!(lstat == kRunning || resuming)) return;
   LaneMem m = carve(T, block);
   double* sol = block + T.smem_doubles;
   double* prev = sol + n;
   double* vsrc = prev + n;  // T.n_src
   const double* rec = L.rec + size_t(lane) * T.rec_size;
+  uint32_t* sw = P.state + size_t(lane) * kSweepStateN;
   init_consts(T, m.v, tid);
   SimDev sim;
   sim.t = 0.0;
   sim.src_scale = 1.0;
   sim.kind = 0;
   fill_sources(T, rec, sim, vsrc, tid);
-  for (uint32_t i = tid; i < n; i += 32) {
-    sol[i] = 0.0;
-    prev[i] = 0.0;
-  }
   LaneOpts cold_o = o;
   cold_o.max_iter = 100;
   uint32_t status = kSweepDone;
   bool cold = true;
-  for (uint32_t pt = 0; pt < P.n_pts; ++pt) {
-    const size_t row = size_t(lane) * P.n_pts + pt;
-    if (status != kSweepDone) {
-      for (uint32_t i = tid; i < n; i += 32) P.x_out[row * n + i] = 0.0;
-      if (tid == 0) {
-        P.iters[row] = 0;
-        P.conv[row] = 0;
-      }
-      continue;
-    }
-    if (tid == 0) vsrc[P.src] = P.values[pt];
+  uint32_t pt0 = 0, phase0 = 0, it_total0 = 0;
+  bool lim_active = false;
+  NewtonCarry carry{0u, kXPlausible, 0u, 0u, (L.flags[lane] & 2u) ? 1u : 0u};
+  if (resuming) {
+    pt0 = sw[kSwPoint];
+    phase0 = sw[kSwPhase];
+    it_total0 = sw[kSwItTotal];
+    cold = sw[kSwCold] != 0;
+    lim_active = sw[kSwLimActive] != 0;
+    carry.iter = sw[kSwIter];
+    carry.init_fix = sw[kSwInitFix];
+    carry.limit = L.limit[lane];
+    carry.resume = lstat == kSingular ? 2u : 1u;
+    const size_t at = size_t(lane) * n;
     for (uint32_t i = tid; i < n; i += 32) {
-      const double last = sol[i];
-      sol[i] = 2.0 * last - prev[i];
-      prev[i] = last;
+      sol[i] = P.rows[2 * at + i];
+      prev[i] = P.rows[2 * at + n + i];
+      m.x[i] = L.x[at + i];
+      m.rhs[i] = L.rhs[at + i];
+      m.diag[i] = L.diag[at + i];
+    }
+    for (uint32_t i = tid; i < T.nlim; i += 32) m.lim[i] = L.lim[size_t(lane) * T.nlim + i];
+    for (uint32_t j = tid; j < n; j += 32) m.y[j] = L.dx[at + T.qcol[j]];
+  } else {
+    for (uint32_t i = tid; i < n; i += 32) {
+      sol[i] = 0.0;
+      prev[i] = 0.0;
+    }
+  }
+  // Pause: the lane's state for the host and for the resume launch.
+  auto pause = [&](uint32_t pt, uint32_t phase, uint32_t it_total) {
+    const size_t at = size_t(lane) * n;
+    gather_pattern(T, m, L.a_vals + size_t(lane) * T.nnz, tid);
+    for (uint32_t i = tid; i < n; i += 32) {
+      L.x[at + i] = m.x[i];
+      L.rhs[at + i] = m.rhs[i];
+      L.diag[at + i] = m.diag[i];
+      P.rows[2 * at + i] = sol[i];
+      P.rows[2 * at + n + i] = prev[i];
+    }
+    for (uint32_t i = tid; i < T.nlim; i += 32) L.lim[size_t(lane) * T.nlim + i] = m.lim[i];
+    if (tid == 0) {
+      sw[kSwPoint] = pt;
+      sw[kSwPhase] = phase;
+      sw[kSwItTotal] = it_total;
+      sw[kSwCold] = cold;
+      sw[kSwIter] = carry.iter;
+      sw[kSwInitFix] = carry.init_fix;
+      sw[kSwLimActive] = lim_active;
+      L.limit[lane] = carry.limit;
+      L.flags[lane] |= 2u;
+      // the lane's first factor of all is its own fresh factor; a later
+      // one continues the lead tape's history
+      L.iters[lane] = (pt == 0 && carry.iter == 0) ? 0u : 1u;
+      L.status[lane] = kNeedSolve;
+      atomicAdd(L.n_paused, 1u);
+    }
+  };
+  __syncwarp();
+  for (uint32_t pt = pt0; pt < P.n_pts; ++pt) {
+    const size_t row = size_t(lane) * P.n_pts + pt;
+    const bool res_here = resuming && pt == pt0;
+    if (tid == 0) vsrc[P.src] = P.values[pt];
+    uint32_t it_total = res_here ? it_total0 : 0u;
+    if (!res_here) {
+      for (uint32_t i = tid; i < n; i += 32) {
+        const double last = sol[i];
+        sol[i] = 2.0 * last - prev[i];
+        prev[i] = last;
+      }
     }
     __syncwarp();
-    uint32_t it_total = 0;
     int rc = 1;
-    bool lim_active = false;
-    if (!cold) {
-      for (uint32_t i = tid; i < n; i += 32) {
-        m.x[i] = sol[i];
-        m.xo[i] = prev[i];
-      }
-      __syncwarp();
-      apply_limits<kHasB3>(T, rec, m, false, tid);
-      lim_active = T.nlim != 0;
-      __syncwarp();
-      uint32_t it = 0;
-      rc = lane_newton<kHasB3>(T, prog, m, rec, o, sim, nullptr, lim_active, false, it, vsrc, tid);
-      it_total += it;
-      for (uint32_t i = tid; i < n; i += 32) sol[i] = m.x[i];
-      __syncwarp();
-    }
-    if (rc == 1) {
-      for (uint32_t i = tid; i < n; i += 32) m.x[i] = 0.0;
-      for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
-        const BatchDev& B = T.b[bi];
-        for (uint32_t i = tid; i < B.count; i += 32) {
-          if (B.type == kD) m.lim[B.lim_off + i] = rec[B.rec_off + kDVcrit * B.count + i];
-          if (B.type == kM) {
-            m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kMSeedVgs * B.count + i];
-            m.lim[B.lim_off + 3 * i + 1] = 0.0;
-            m.lim[B.lim_off + 3 * i + 2] = -1.0;
-          }
-          if (B.type == kB3) {
-            m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kB3SeedVgs * B.count + i];
-            m.lim[B.lim_off + 3 * i + 1] = 0.1;
-            m.lim[B.lim_off + 3 * i + 2] = 0.0;
-          }
+    if (res_here ? phase0 == 0 : !cold) {
+      if (!res_here) {
+        for (uint32_t i = tid; i < n; i += 32) {
+          m.x[i] = sol[i];
+          m.xo[i] = prev[i];
         }
+        __syncwarp();
+        apply_limits<kHasB3>(T, rec, m, false, tid);
+        lim_active = T.nlim != 0;
+        carry.iter = 0;
+        carry.resume = 0;
+        __syncwarp();
       }
-      __syncwarp();
-      lim_active = T.nlim != 0;
       uint32_t it = 0;
-      rc = lane_newton<kHasB3>(T, prog, m, rec, cold_o, sim, nullptr, lim_active, true, it, vsrc, tid);
+      rc = lane_newton<kHasB3>(T, prog, m, rec, o, sim, nullptr, lim_active, false, it, vsrc, tid, &carry);
+      if (rc == 3) {
+        pause(pt, 0, it_total);
+        return;
+      }
+      carry.resume = 0;
       it_total += it;
       for (uint32_t i = tid; i < n; i += 32) sol[i] = m.x[i];
       __syncwarp();
     }
-    if (rc == 2) status = kSweepLeftTape;
+    if (rc != 0) {
+      // cold rung: on a failed warm point, before any point has converged,
+      // or when resumed inside it
+      const bool res_cold = res_here && phase0 == 1;
+      if (!res_cold) {
+        sweep_seed<kHasB3>(T, rec, m, tid);
+        __syncwarp();
+        lim_active = T.nlim != 0;
+        carry.iter = 0;
+        carry.init_fix = 1;
+        carry.resume = 0;
+      }
+      uint32_t it = 0;
+      rc = lane_newton<kHasB3>(T, prog, m, rec, cold_o, sim, nullptr, lim_active, true, it, vsrc, tid, &carry);
+      if (rc == 3) {
+        pause(pt, 1, it_total);
+        return;
+      }
+      carry.resume = 0;
+      it_total += it;
+      for (uint32_t i = tid; i < n; i += 32) sol[i] = m.x[i];
+      __syncwarp();
+    }
     const bool converged = rc == 0;
     for (uint32_t i = tid; i < n; i += 32) P.x_out[row * n + i] = sol[i];
     if (tid == 0) {
@@ -1817,7 +1932,10 @@ __device__ void sweep_lane(const TopoDev& T, const LaneDev& L, const SweepDev& P
     }
     __syncwarp();
   }
-  if (tid == 0) P.status[lane] = status;
+  if (tid == 0) {
+    P.status[lane] = status;
+    L.status[lane] = kConverged;  // this lane's sweep is done
+  }
 }
 
 // Uneven batching: lanes of several topologies (circuits of different sizes)

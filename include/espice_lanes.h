@@ -305,12 +305,13 @@ int32_t esl_tran_meas_device(esl_ctx *ctx, const esl_tran_opts *opts, const esl_
  * warm Newton; on its failure, or before a point has converged, a cold start
  * with MODEINITFIX at 100 iterations (op.zig's plain rung). Device buffers:
  * d_x [n_lanes][n_pts][n], d_iters [n_lanes][n_pts] (both solves of a
- * point), d_conv [n_lanes][n_pts], d_status [n_lanes] (ESL_SWEEP_*). A lane
- * whose factor leaves the lead pivot tape stops there with
- * ESL_SWEEP_LEFT_TAPE (its later points read 0 and not converged; its
- * sweep is the CPU's). ESL_NOT_ELIGIBLE for a slot that is not a source's
- * DC value. ms: the kernel's device time (may be NULL). */
-enum { ESL_SWEEP_DONE = 0, ESL_SWEEP_LEFT_TAPE = 4 };
+ * point), d_conv [n_lanes][n_pts], d_status [n_lanes] (ESL_SWEEP_DONE). A
+ * lane whose factor leaves the lead pivot tape pauses and takes the host's
+ * factor on its own direct solver, then continues where it stopped, until
+ * its own factor is the lead tape again (lane_solver.zig peels); the call
+ * returns once every lane's sweep is done. ESL_NOT_ELIGIBLE for a slot that
+ * is not a source's DC value. ms: the device time of the launches (may be
+ * NULL). ESL_SWEEP_LEFT_TAPE is not returned since the peels. */
 int32_t esl_dc_sweep_device(esl_ctx *ctx, const esl_slot *slot, const double *values, uint32_t n_pts,
                             const esl_newton_opts *opts, double *d_x, uint32_t *d_iters, uint8_t *d_conv,
                             uint32_t *d_status, float *ms);

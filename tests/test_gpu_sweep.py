@@ -64,10 +64,9 @@ def _op(fr, opts):
 DC_FIXTURES = [n for n in gu.names("dc__")]
 
 # Sweeps that cross into reverse breakdown need other pivots than the lead
-# tape built at their first point: their lanes stop with SWEEP_LEFT_TAPE
-# (the reference's lane solver would re-pivot per lane on the host; the rest
-# of such a sweep is the CPU's), here already within their first point.
-# Their points before the stop, if any, are checked.
+# tape built at their first point: their lanes pause there and take the
+# host's factor on their own direct solver (lane_solver.zig peels), then
+# continue on the device where they stopped.
 LEAVES_TAPE = {"dc__bench_ensemble_sweep_lanes", "dc__bench_power_zener_reg", "dc__device_diode_breakdown"}
 
 
@@ -75,20 +74,39 @@ LEAVES_TAPE = {"dc__bench_ensemble_sweep_lanes", "dc__bench_power_zener_reg", "d
 def test_golden_fixtures_as_sweep_lanes(name):
     """Every reference DC sweep fixture as sweep lanes (one lane per outer
     value): the oracle's points, iterations and convergence, and the
-    reference's golden values at its tolerances."""
+    reference's golden values at its tolerances. The sweeps that leave the
+    lead tape finish through host peels with the same results."""
     g = gu.load(name)
     _gpu_sweep.status = []
     fr, rows, conv = gu.solve_deck(g, _gpu_sweep, _op)
     fro, rows_o, conv_o = gu.solve_deck(g, _oracle_sweep, _op)
-    if name in LEAVES_TAPE:
-        assert lanes.SWEEP_LEFT_TAPE in _gpu_sweep.status
-        stop = int(np.argmin(conv)) if not conv.all() else len(conv)
-        assert conv_o[:stop].all()
-        assert _close(rows[:stop], rows_o[:stop]).all()
-        return
     assert all(s == lanes.SWEEP_DONE for s in _gpu_sweep.status)
     assert np.array_equal(conv.astype(bool), conv_o.astype(bool))
     assert conv.all()
     assert _close(rows, rows_o).all(), float(np.max(np.abs(rows - rows_o)))
     for col, worst, count in gu.score(g, fr, rows):
         assert worst <= 1.0, f"{name} {col}: {worst:.3g}x the fixture tolerance"
+
+
+@pytest.mark.parametrize("name", sorted(LEAVES_TAPE))
+def test_sweep_lanes_peel_and_match_oracle_exactly(name):
+    """The sweeps that leave the lead tape: every point's iteration count and
+    convergence equal to the oracle's per-lane sweep, the solutions bitwise."""
+    g = gu.load(name)
+    deck = Deck(g["deck"])
+    fr = deck.circuit().freeze()
+    an = deck.analysis
+    from netlist import sweep_values
+    pts = np.array(sweep_values(an[2], an[3], an[4]))
+    slot = fr.slot(an[1], "dc")
+    opts = deck.newton_opts()
+    ctx = lanes.DcLanes(fr)
+    ctx.set_lanes([], np.zeros((2, 1)))
+    x, it, cv, st, _ = ctx.sweep(slot, pts, lanes.newton_opts(**opts))
+    ctx.close()
+    assert (st == lanes.SWEEP_DONE).all()
+    xo, ito, cvo = oracle.dc_sweep(fr, slot, pts, oracle.newton_opts(**opts))
+    for lane in range(2):
+        assert np.array_equal(cv[lane], cvo.astype(bool)), lane
+        assert np.array_equal(it[lane], ito), (lane, np.flatnonzero(it[lane] != ito))
+        assert np.array_equal(x[lane].view(np.uint64), xo.view(np.uint64)), lane
