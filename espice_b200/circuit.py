@@ -82,11 +82,54 @@ B3_DEFAULTS = {
 # ngspice card spellings that name the same parameter
 B3_ALIASES = {"npeak": "nch", "uo": "u0"}
 
-V_PARAMS = ["dc", "wave", "v1", "v2", "td", "tr", "tf", "pw", "per", "phase"]
-PARAMS_PER = {R: 1, C: 1, V: len(V_PARAMS), I: 1, D: len(D_PARAMS), M: len(M_PARAMS),
+# V and I sources (models/vsource.va, isource.va): dc, wave (0 DC, 1 PULSE,
+# 2 SIN, 3 EXP, 4 PWL), the wave's eight parameters in slots 2..9 (named for
+# PULSE: v1 v2 td tr tf pw per phase; SIN: vo va freq td theta phase; EXP: v1
+# v2 td1 tau1 td2 tau2; PWL: len repeat td), then the PWL table: 64 times and
+# 64 values.
+PWL_MAX = 64
+SRC_PARAMS = (["dc", "wave", "v1", "v2", "td", "tr", "tf", "pw", "per", "phase"]
+              + [f"pwl_t{k}" for k in range(PWL_MAX)] + [f"pwl_v{k}" for k in range(PWL_MAX)])
+V_PARAMS = SRC_PARAMS
+WAVE = {"dc": 0, "pulse": 1, "sin": 2, "exp": 3, "pwl": 4}
+PARAMS_PER = {R: 1, C: 1, V: len(SRC_PARAMS), I: len(SRC_PARAMS), D: len(D_PARAMS), M: len(M_PARAMS),
               B3: len(B3_PARAMS)}
-PARAM_NAMES = {R: ["r"], C: ["c"], V: V_PARAMS, I: ["dc"], D: D_PARAMS, M: M_PARAMS,
+PARAM_NAMES = {R: ["r"], C: ["c"], V: SRC_PARAMS, I: SRC_PARAMS, D: D_PARAMS, M: M_PARAMS,
                B3: B3_PARAMS}
+
+
+def source_params(dc=0.0, pulse=None, sin=None, exp=None, pwl=None):
+    """The 138 source parameters: dc and at most one wave. pulse: [v1 v2 td
+    tr tf pw per phase] (missing ones take the model's -1 / 0 sentinels);
+    sin: [vo va freq td theta phase]; exp: [v1 v2 td1 tau1 td2 tau2]; pwl:
+    (times, values[, repeat, td]) with at most 64 points (repeat < 0: none)."""
+    prm = [float(dc), 0.0] + [0.0] * 8 + [0.0] * (2 * PWL_MAX)
+    if pulse is not None:
+        prm[1] = 1.0
+        vals = list(pulse) + [None] * (8 - len(pulse))
+        defaults = [0.0, 0.0, 0.0, -1.0, -1.0, -1.0, -1.0, 0.0]
+        for k in range(8):
+            prm[2 + k] = float(vals[k]) if vals[k] is not None else defaults[k]
+    elif sin is not None:
+        prm[1] = 2.0
+        vals = list(sin) + [0.0] * (6 - len(sin))
+        prm[2:8] = [float(v) for v in vals[:6]]
+    elif exp is not None:
+        prm[1] = 3.0
+        defaults = [0.0, 0.0, 0.0, 1.0e-9, 0.0, 1.0e-9]
+        vals = list(exp) + [None] * (6 - len(exp))
+        prm[2:8] = [float(v) if v is not None else d for v, d in zip(vals[:6], defaults)]
+    elif pwl is not None:
+        times, values = list(pwl[0]), list(pwl[1])
+        repeat = float(pwl[2]) if len(pwl) > 2 else -1.0
+        td = float(pwl[3]) if len(pwl) > 3 else 0.0
+        if len(times) != len(values) or not 0 < len(times) <= PWL_MAX:
+            raise ValueError(f"a PWL source takes 1 to {PWL_MAX} points")
+        prm[1] = 4.0
+        prm[2:5] = [float(len(times)), repeat, td]
+        prm[10:10 + len(times)] = [float(v) for v in times]
+        prm[10 + PWL_MAX:10 + PWL_MAX + len(values)] = [float(v) for v in values]
+    return prm
 TYPE_ORDER = [R, C, V, I, D, M, B3]
 TYPE_LETTER = {R: "R", C: "C", V: "V", I: "I", D: "D", M: "M", B3: "M"}
 
@@ -127,18 +170,13 @@ class Circuit:
     def C(self, name, p, n, c):
         self._add(name, C, [p, n], [float(c)])
 
-    def V(self, name, p, n, dc=0.0, pulse=None):
-        prm = [float(dc), 0.0, 0, 0, 0, -1.0, -1.0, -1.0, -1.0, 0.0]
-        if pulse is not None:
-            prm[1] = 1.0
-            vals = list(pulse) + [None] * (8 - len(pulse))
-            defaults = [0.0, 0.0, 0.0, -1.0, -1.0, -1.0, -1.0, 0.0]
-            for k in range(8):
-                prm[2 + k] = float(vals[k]) if vals[k] is not None else defaults[k]
-        self._add(name, V, [p, n], prm)
+    def V(self, name, p, n, dc=0.0, pulse=None, sin=None, exp=None, pwl=None):
+        """A voltage source: dc and at most one wave (source_params)."""
+        self._add(name, V, [p, n], source_params(dc, pulse, sin, exp, pwl))
 
-    def I(self, name, p, n, dc=0.0):
-        self._add(name, I, [p, n], [float(dc)])
+    def I(self, name, p, n, dc=0.0, pulse=None, sin=None, exp=None, pwl=None):
+        """A current source from p to n through the source (source_params)."""
+        self._add(name, I, [p, n], source_params(dc, pulse, sin, exp, pwl))
 
     def D(self, name, a, c, area=1.0, **model):
         kw = dict(D_DEFAULTS)

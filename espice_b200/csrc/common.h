@@ -34,7 +34,17 @@ enum DiodeField {
   kDVte, kDIs, kDVcrit, kDRs, kDGmin, kDBv, kDXbv, kDVtebrk, kDCjo, kDVj, kDMt, kDFc, kDTt,
   kDHasRs, kDHasQ, kDiodeFields
 };
-constexpr int kRFields = 1, kCFields = 1, kVFields = 10, kIFields = 1;
+constexpr int kRFields = 1, kCFields = 1;
+// V and I sources (models/vsource.va, isource.va): the parameters as given,
+// one record field each: dc, wave (kWave*), the wave's eight parameters at
+// kSrcShape (PULSE v1 v2 td tr tf pw per phase; SIN vo va freq td theta
+// phase; EXP v1 v2 td1 tau1 td2 tau2; PWL len repeat td), then the PWL table,
+// kPwlMax times at kSrcPwlT and values at kSrcPwlV.
+enum SourceWave { kWaveDc = 0, kWavePulse = 1, kWaveSin = 2, kWaveExp = 3, kWavePwl = 4 };
+constexpr int kPwlMax = 64;
+constexpr int kSrcShape = 2, kSrcPwlT = 10, kSrcPwlV = kSrcPwlT + kPwlMax;
+constexpr int kSrcParams = kSrcPwlV + kPwlMax;
+constexpr int kVFields = kSrcParams, kIFields = kSrcParams;
 
 // MOS1 record fields: the bias-independent part of models/mos1.va
 // (temperature, geometry, junction sizing), in the type frame.

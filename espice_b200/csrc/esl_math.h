@@ -158,6 +158,47 @@ ESL_MATH_ENTRY double esl_exp(double x) { return em_exp(x); }
 
 ESL_MATH_ENTRY double esl_log(double x) { return em_log(x); }
 
+/* sin x: x = k pi/2 + r with pi/2 split in three (33, 33 and 53 bits: the
+ * first two products exact for |k| < 2^20), |r| <= pi/4, then by the
+ * quadrant k mod 4 the Taylor series of sin r (to r^17/17!) or cos r (to
+ * r^18/18!), each below 1e-19 truncation on |r| <= pi/4, by Estrin's scheme
+ * in r^2. Error about 1 ulp for |x| below 1e6 (a source's 2 pi f t). */
+#define EM_PIO2_1 1.5707963267341256
+#define EM_PIO2_2 6.077100506303966e-11
+#define EM_PIO2_3 2.0222662487959506e-21
+#define EM_TWO_OVER_PI 0.6366197723675814
+
+ESL_MATH_FN double em_sin(double x) {
+  if (x != x || x - x != 0.0) return EM_SUB(x, x); /* NaN for NaN and infinities */
+  const double kd = EM_SUB(EM_ADD(EM_MUL(x, EM_TWO_OVER_PI), EM_SHIFTER), EM_SHIFTER);
+  const double r = EM_SUB(EM_SUB(EM_SUB(x, EM_MUL(kd, EM_PIO2_1)), EM_MUL(kd, EM_PIO2_2)), EM_MUL(kd, EM_PIO2_3));
+  const double z = EM_MUL(r, r), z2 = EM_MUL(z, z), z4 = EM_MUL(z2, z2);
+  const int64_t k = (int64_t)kd;
+  double out;
+  if ((k & 1) == 0) {
+    /* sin r = r + r z P(z), P = -1/3! + z/5! - ... + z^7/17! */
+    const double a0 = EM_ADD(-0.16666666666666666, EM_MUL(z, 0.008333333333333333));
+    const double a1 = EM_ADD(-0.0001984126984126984, EM_MUL(z, 2.7557319223985893e-06));
+    const double a2 = EM_ADD(-2.505210838544172e-08, EM_MUL(z, 1.6059043836821613e-10));
+    const double a3 = EM_ADD(-7.647163731819816e-13, EM_MUL(z, 2.8114572543455206e-15));
+    const double p = EM_ADD(EM_ADD(a0, EM_MUL(z2, a1)), EM_MUL(z4, EM_ADD(a2, EM_MUL(z2, a3))));
+    out = EM_ADD(r, EM_MUL(EM_MUL(r, z), p));
+  } else {
+    /* cos r = 1 + z Q(z), Q = -1/2! + z/4! - ... + z^8/18! */
+    const double b0 = EM_ADD(-0.5, EM_MUL(z, 0.041666666666666664));
+    const double b1 = EM_ADD(-0.001388888888888889, EM_MUL(z, 2.48015873015873e-05));
+    const double b2 = EM_ADD(-2.755731922398589e-07, EM_MUL(z, 2.08767569878681e-09));
+    const double b3 = EM_ADD(-1.1470745597729725e-11, EM_MUL(z, 4.779477332387385e-14));
+    const double z8 = EM_MUL(z4, z4);
+    const double q = EM_ADD(EM_ADD(EM_ADD(b0, EM_MUL(z2, b1)), EM_MUL(z4, EM_ADD(b2, EM_MUL(z2, b3)))),
+                            EM_MUL(z8, -1.5619206968586225e-16));
+    out = EM_ADD(1.0, EM_MUL(z, q));
+  }
+  return (k & 2) ? -out : out;
+}
+
+ESL_MATH_ENTRY double esl_sin(double x) { return em_sin(x); }
+
 ESL_MATH_ENTRY double esl_pow(double x, double y) {
   if (y == 0.0 || x == 1.0) return 1.0;
   if (x != x || y != y) return EM_ADD(x, y);

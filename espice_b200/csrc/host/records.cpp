@@ -29,7 +29,7 @@ uint32_t record_fields(uint32_t type) {
 }
 
 uint32_t param_count(uint32_t type) {
-  static const uint32_t n[kNumTypes] = {1, 1, 10, 1, kDiodeParams, kMosParams, kB3Params};
+  static const uint32_t n[kNumTypes] = {1, 1, kSrcParams, kSrcParams, kDiodeParams, kMosParams, kB3Params};
   return type < kNumTypes ? n[type] : 0;
 }
 
@@ -422,11 +422,11 @@ void derive_instance(uint32_t type, const double* params, double* rec, uint32_t 
   switch (type) {
     case kR:
     case kC:
-    case kI:
       rec[0] = params[0];
       break;
     case kV:
-      for (int f = 0; f < kVFields; ++f) rec[f * stride] = params[f];
+    case kI:
+      for (int f = 0; f < kSrcParams; ++f) rec[f * stride] = params[f];
       break;
     case kD:
       diode_record(params, rec, stride);

@@ -96,7 +96,7 @@ __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, 
           break;
         }
         case kV: {
-          const double v = vcache ? vcache[B.src_off + i] : vsource_value(r, s, sim);
+          const double v = vcache ? vcache[B.src_off + i] : source_value(r, s, sim);
           const double ib = m.x[nd[2]];
           st[0] = ib;
           st[1] = -ib;
@@ -108,7 +108,7 @@ __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, 
           break;
         }
         case kI: {
-          const double v = vcache ? vcache[B.src_off + i] : r[0] * sim.src_scale;
+          const double v = vcache ? vcache[B.src_off + i] : source_value(r, s, sim);
           st[0] = v;
           st[1] = -v;
           break;

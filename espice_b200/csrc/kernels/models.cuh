@@ -32,7 +32,7 @@ struct SimDev {
   int kind;          // 0 static (.op / .dc), 1 transient, 2 transient op
 };
 
-// PULSE (vsource.va:211-222); p = the 10 V-source fields.
+// PULSE (vsource.va:211-222); p = the source's record fields.
 __device__ __forceinline__ double pulse_value(const double* p, int stride, double t) {
   const double v1 = p[2 * stride], v2 = p[3 * stride], td = p[4 * stride];
   const double tr = fmax(p[5 * stride], 1.0e-12);
@@ -51,11 +51,71 @@ __device__ __forceinline__ double pulse_value(const double* p, int stride, doubl
   return v1;
 }
 
-// V source value: static analyses (kind 0) bias at `dc`; the transient and
-// its own operating point (kinds 1, 2) at the wave.
-__device__ __forceinline__ double vsource_value(const double* p, int stride, const SimDev& sim) {
+constexpr double kPiD = 3.141592653589793;
+constexpr double kTwoPiD = 6.283185307179586;
+
+// SIN (vsource.va:224-236): before TD the wave's own t = 0 value; the
+// damping applies after TD, its exponent clamped at 80. The operations and
+// their order are the oracle's (esl_sin / esl_exp are shared with it).
+__device__ __forceinline__ double sin_value(const double* p, int s, double t) {
+  const double vo = p[2 * s], va = p[3 * s], freq = p[4 * s], td = p[5 * s], theta = p[6 * s], phase = p[7 * s];
+  const double t_sin = t - td;
+  const double ph = div_rn(phase * kPiD, 180.0);
+  if (t_sin < 0.0) return vo + va * esl_sin(ph);
+  return vo + va * esl_sin(kTwoPiD * freq * t_sin + ph) * esl_exp(fmin(-theta * t_sin, 80.0));
+}
+
+// EXP (vsource.va:238-246): two one-sided exponentials on V1.
+__device__ __forceinline__ double exp_value(const double* p, int s, double t) {
+  const double v1 = p[2 * s], v2 = p[3 * s], td1 = p[4 * s], tau1 = p[5 * s], td2 = p[6 * s], tau2 = p[7 * s];
+  const double t_e1 = t - td1, t_e2 = t - td2;
+  double out = v1;
+  if (t_e1 > 0.0) out = out + (v2 - v1) * (1.0 - esl_exp(fmin(div_rn(-t_e1, fmax(tau1, 1.0e-15)), 80.0)));
+  if (t_e2 > 0.0) out = out + (v1 - v2) * (1.0 - esl_exp(fmin(div_rn(-t_e2, fmax(tau2, 1.0e-15)), 80.0)));
+  return out;
+}
+
+// PWL (vsource.va:248-290): the repeat wraps [r, t_last]; bisection over the
+// sorted times for the segment holding t.
+__device__ __forceinline__ double pwl_value(const double* p, int s, double t) {
+  const int len = static_cast<int>(p[2 * s]);
+  if (len <= 0) return p[0];
+  const double repeat = p[3 * s], td = p[4 * s];
+  const double* tt = p + kSrcPwlT * s;
+  const double* vv = p + kSrcPwlV * s;
+  double t_e = t - td;
+  const double t_first = tt[0], v_first = vv[0], t_last = tt[(len - 1) * s], v_last = vv[(len - 1) * s];
+  if (repeat >= 0.0 && len > 1 && t_e > t_last && t_last > repeat) {
+    const double span = t_last - repeat;
+    if (span > 0.0) {
+      const double excess = t_e - repeat;
+      t_e = repeat + (excess - floor(div_rn(excess, span)) * span);
+    }
+  }
+  if (t_e < 0.0 || t_e <= t_first) return v_first;
+  if (t_e >= t_last) return v_last;
+  int klo = 0, khi = len - 1;
+  while (khi - klo > 1) {
+    const int k = (klo + khi) / 2;
+    if (tt[k * s] > t_e) khi = k;
+    else klo = k;
+  }
+  const double tp = tt[klo * s], vp = vv[klo * s], tk = tt[khi * s], vk = vv[khi * s];
+  return vp + div_rn((vk - vp) * (t_e - tp), fmax(tk - tp, 1.0e-15));
+}
+
+// A V or I source's value (vsource.va:198-290): static analyses (kind 0)
+// bias at `dc`; the transient and its own operating point (kinds 1, 2) at
+// the wave; times the source-stepping factor.
+__device__ __forceinline__ double source_value(const double* p, int stride, const SimDev& sim) {
   double out = p[0];
-  if (sim.kind != 0 && p[stride] == 1.0) out = pulse_value(p, stride, sim.t);
+  if (sim.kind != 0) {
+    const double w = p[stride];
+    if (w == 1.0) out = pulse_value(p, stride, sim.t);
+    else if (w == 2.0) out = sin_value(p, stride, sim.t);
+    else if (w == 3.0) out = exp_value(p, stride, sim.t);
+    else if (w == 4.0) out = pwl_value(p, stride, sim.t);
+  }
   return out * sim.src_scale;
 }
 

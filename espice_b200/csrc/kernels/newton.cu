@@ -1059,8 +1059,7 @@ __device__ void fill_sources(const TopoDev& T, const double* rec, const SimDev& 
     const BatchDev& B = T.b[bi];
     if (B.type != kV && B.type != kI) continue;
     for (uint32_t i = tid; i < B.count; i += 32)
-      vcache[B.src_off + i] = B.type == kV ? vsource_value(rec + B.rec_off + i, static_cast<int>(B.count), sim)
-                                           : rec[B.rec_off + i] * sim.src_scale;
+      vcache[B.src_off + i] = source_value(rec + B.rec_off + i, static_cast<int>(B.count), sim);
   }
   __syncwarp();
 }
@@ -1242,7 +1241,7 @@ __device__ __forceinline__ bool almost_equal_ulps(double a, double b, long long 
 __device__ void pulse_timers(const TopoDev& T, const double* rec, double* tm, int tid) {
   for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
     const BatchDev& B = T.b[bi];
-    if (B.type != kV) continue;
+    if (B.type != kV && B.type != kI) continue;
     const int s = static_cast<int>(B.count);
     for (uint32_t i = tid; i < B.count; i += 32) {
       const double* p = rec + B.rec_off + i;
@@ -1273,8 +1272,11 @@ __device__ void pulse_timers(const TopoDev& T, const double* rec, double* tm, in
 }
 
 // The first timer event at or after `after` (tran.zig nextBp), the timers
-// spread over the warp and the earliest taken by a warp minimum.
-__device__ bool next_bp(const TopoDev& T, const double* tm, double after, double& bp) {
+// spread over the warp and the earliest taken by a warp minimum: the PULSE
+// corners from the lane's timer table, and each PWL source's one-shot
+// corners (its table times plus TD, and TD itself when the table leaves
+// slots unused, vsource.va:137-200) found in its record.
+__device__ bool next_bp(const TopoDev& T, const double* rec, const double* tm, double after, double& bp) {
   const int tid = threadIdx.x & 31;
   double best = CUDART_INF;
   for (uint32_t k = tid; k < 4 * T.n_src; k += 32) {
@@ -1287,6 +1289,25 @@ __device__ bool next_bp(const TopoDev& T, const double* tm, double after, double
       if (t < after) t += per;
     }
     if (t < best) best = t;
+  }
+  for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
+    const BatchDev& B = T.b[bi];
+    if (B.type != kV && B.type != kI) continue;
+    const int s = static_cast<int>(B.count);
+    for (uint32_t i = tid; i < B.count; i += 32) {
+      const double* p = rec + B.rec_off + i;
+      if (p[s] != 4.0) continue;
+      const int len = static_cast<int>(p[2 * s]);
+      const double td = p[4 * s];
+      if (len < kPwlMax && td >= after && td < best) best = td;
+      for (int j = 0; j < len; ++j) {
+        const double c = p[(kSrcPwlT + j) * s] + td;
+        if (c >= after) {
+          if (c < best) best = c;
+          break;  // the table is sorted: the first corner at or after `after`
+        }
+      }
+    }
   }
   best = warp_fmin(best);
   if (best == CUDART_INF) return false;
@@ -1571,7 +1592,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
     const double min_break = 10.0 * delmin;
     double dt = fmin(div_rn(fmin(P.t_step, div_rn(P.t_stop, 100.0)), 10.0), dt_max);
     double bp0;
-    if (next_bp(T, tmr, min_break, bp0)) dt = fmin(dt, 0.1 * bp0);
+    if (next_bp(T, rec, tmr, min_break, bp0)) dt = fmin(dt, 0.1 * bp0);
     dt = div_rn(dt, 10.0);
     double dt_old[6];
     for (int k = 0; k < 6; ++k) dt_old[k] = dt_max;
@@ -1696,7 +1717,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
           stat[kTsBpLandings] += 1;
           order = 1;
           double shrink = bp_save_dt, nb;
-          if (next_bp(T, tmr, t_new + min_break, nb)) shrink = fmin(shrink, nb - t_new);
+          if (next_bp(T, rec, tmr, t_new + min_break, nb)) shrink = fmin(shrink, nb - t_new);
           dt_next = fmin(dt_next, 0.1 * shrink);
         }
         have_bp = false;
@@ -1707,7 +1728,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
         stat[kTsStatus] = kTranResolved;
         break;
       }
-      have_bp = next_bp(T, tmr, t_new + min_break, bp_next);
+      have_bp = next_bp(T, rec, tmr, t_new + min_break, bp_next);
       bp_clamped = false;
       if (have_bp) {
         const double dt_to_bp = bp_next - t_new;

@@ -208,7 +208,7 @@ def lib():
     return _lib
 
 
-RECORD_FIELDS = {0: 1, 1: 1, 2: 10, 3: 1, 4: 15, 5: 33}
+RECORD_FIELDS = {0: 1, 1: 1, 2: 138, 3: 138, 4: 15, 5: 33}
 
 
 def record_size(frozen: Frozen) -> int:

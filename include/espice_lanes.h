@@ -39,14 +39,25 @@ enum {
 enum {
     ESL_R = 0, /* nodes p n;          params r                               */
     ESL_C = 1, /* nodes p n;          params c                               */
-    ESL_V = 2, /* nodes p n br;       params dc wave v1 v2 td tr tf pw per phase */
-    ESL_I = 3, /* nodes p n;          params dc                              */
+    ESL_V = 2, /* nodes p n br;       params: ESL_SRC_PARAMS (below)         */
+    ESL_I = 3, /* nodes p n;          params: ESL_SRC_PARAMS (below)         */
     ESL_D = 4, /* nodes a c ai;       params is n rs bv ibv cjo vj m fc tt area gmin xti eg tnom temp */
     ESL_M = 5, /* nodes d g s b di si; params (MOS1, models/mos1.va; kp NaN =
                   not given: u0 * Cox' with tox > 0, else 2e-5; a circuit with
                   tox > 0 runs DC only, its transients ESL_NOT_ELIGIBLE)    */
     ESL_B3 = 6 /* nodes d g s b di si; params (BSIM3v3 DC core, models/bsim3.va) */
 };
+
+/* ESL_V and ESL_I parameters (models/vsource.va, isource.va): dc; wave (0
+ * DC, 1 PULSE, 2 SIN, 3 EXP, 4 PWL); the wave's eight parameters (PULSE v1
+ * v2 td tr tf pw per phase, the -1 sentinels of the .va for tr tf pw per;
+ * SIN vo va freq td theta phase; EXP v1 v2 td1 tau1 td2 tau2; PWL len
+ * repeat td, repeat < 0 for none); then the PWL table: ESL_PWL_MAX times
+ * (non-decreasing) and ESL_PWL_MAX values. Static analyses bias at dc, the
+ * transient and its operating point at the wave; PULSE and PWL corners are
+ * breakpoints of the transient. */
+#define ESL_PWL_MAX 64
+#define ESL_SRC_PARAMS 138
 
 /* ESL_B3 parameter slots: the model card of models/bsim3.va:26-138 in its
  * order (type mobmod tnom tox toxm xj nch nsub ngate gamma1 gamma2 xt vbx

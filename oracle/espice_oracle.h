@@ -38,8 +38,8 @@ extern "C" {
 enum {
     ORC_R = 0,  /* nodes p n;          params r                          */
     ORC_C = 1,  /* nodes p n;          params c                          */
-    ORC_V = 2,  /* nodes p n br;       params dc wave v1 v2 td tr tf pw per phase */
-    ORC_I = 3,  /* nodes p n;          params dc                         */
+    ORC_V = 2,  /* nodes p n br;       params: the source layout below   */
+    ORC_I = 3,  /* nodes p n;          params: the source layout below   */
     ORC_D = 4,  /* nodes a c ai;       params see ORC_D_* (ai == a: RS collapsed) */
     ORC_M = 5,  /* nodes d g s b di si; params see ORC_M_*               */
     ORC_B3 = 6, /* nodes d g s b di si; params see ORC_B3_* (BSIM3v3 DC) */
@@ -112,6 +112,15 @@ typedef struct {
     uint32_t max_iter;      /* before the max(itl, 100) raise */
 } orc_newton_opts;
 
+/* V and I source parameters (models/vsource.va, isource.va): dc, wave
+ * (0 DC, 1 PULSE, 2 SIN, 3 EXP, 4 PWL), the wave's eight parameters (PULSE
+ * v1 v2 td tr tf pw per phase; SIN vo va freq td theta phase; EXP v1 v2 td1
+ * tau1 td2 tau2; PWL len repeat td), then the PWL table: 64 times, 64
+ * values. */
+#define ORC_SRC_NP 138
+#define ORC_SRC_PWL_T 10
+#define ORC_SRC_PWL_V 74
+#define ORC_PWL_MAX 64
 int orc_nodes_per(uint32_t type);
 int orc_params_per(uint32_t type);
 /* One instance's static stamp at local voltages xloc[nodes_per(type)] (node

@@ -30,7 +30,7 @@ int orc_nodes_per(uint32_t type) {
 }
 
 int orc_params_per(uint32_t type) {
-    static const int t[ORC_NTYPES] = {1, 1, 10, 1, ORC_D_NP, ORC_M_NP, ORC_B3_NP};
+    static const int t[ORC_NTYPES] = {1, 1, ORC_SRC_NP, ORC_SRC_NP, ORC_D_NP, ORC_M_NP, ORC_B3_NP};
     return type < ORC_NTYPES ? t[type] : 0;
 }
 
@@ -370,10 +370,67 @@ static double pulse(const double *p, double t) {
     return v1;
 }
 
+#define ORC_PI 3.141592653589793
+#define ORC_TWO_PI 6.283185307179586
+
+/* SIN (vsource.va:224-236): before TD the wave's own t = 0 value; the
+ * damping applies after TD, its exponent clamped at 80. */
+static double sine(const double *p, double t) {
+    double vo = p[2], va = p[3], freq = p[4], td = p[5], theta = p[6], phase = p[7];
+    double t_sin = t - td;
+    if (t_sin < 0.0) return vo + va * esl_sin(phase * ORC_PI / 180.0);
+    return vo + va * esl_sin(ORC_TWO_PI * freq * t_sin + phase * ORC_PI / 180.0) * esl_exp(fmin(-theta * t_sin, 80.0));
+}
+
+/* EXP (vsource.va:238-246): two one-sided exponentials on V1. */
+static double expo(const double *p, double t) {
+    double v1 = p[2], v2 = p[3], td1 = p[4], tau1 = p[5], td2 = p[6], tau2 = p[7];
+    double t_e1 = t - td1, t_e2 = t - td2;
+    double out = v1;
+    if (t_e1 > 0.0) out = out + (v2 - v1) * (1.0 - esl_exp(fmin(-t_e1 / fmax(tau1, 1.0e-15), 80.0)));
+    if (t_e2 > 0.0) out = out + (v1 - v2) * (1.0 - esl_exp(fmin(-t_e2 / fmax(tau2, 1.0e-15), 80.0)));
+    return out;
+}
+
+/* PWL (vsource.va:248-290): the repeat wraps [r, t_last]; bisection for the
+ * segment holding t. */
+static double pwl(const double *p, double t) {
+    const int len = (int)p[2];
+    if (len <= 0) return p[0];
+    const double repeat = p[3], td = p[4];
+    const double *tt = p + ORC_SRC_PWL_T, *vv = p + ORC_SRC_PWL_V;
+    double t_e = t - td;
+    const double t_first = tt[0], v_first = vv[0], t_last = tt[len - 1], v_last = vv[len - 1];
+    if (repeat >= 0.0 && len > 1 && t_e > t_last && t_last > repeat) {
+        double span = t_last - repeat;
+        if (span > 0.0) {
+            double excess = t_e - repeat;
+            t_e = repeat + (excess - floor(excess / span) * span);
+        }
+    }
+    if (t_e < 0.0 || t_e <= t_first) return v_first;
+    if (t_e >= t_last) return v_last;
+    int klo = 0, khi = len - 1;
+    while (khi - klo > 1) {
+        int k = (klo + khi) / 2;
+        if (tt[k] > t_e) khi = k;
+        else klo = k;
+    }
+    const double tp = tt[klo], vp = vv[klo], tk = tt[khi], vk = vv[khi];
+    return vp + (vk - vp) * (t_e - tp) / fmax(tk - tp, 1.0e-15);
+}
+
+/* The source's value (vsource.va:198-290): static analyses at `dc`, the
+ * transient and its own operating point at the wave; times the source-
+ * stepping factor. */
 double source_value(const double *p, const sim_t *sim) {
     double out = p[0];
-    if (sim->kind == 0) out = p[0];
-    else if (p[1] == 1.0) out = pulse(p, sim->t);
+    if (sim->kind != 0) {
+        if (p[1] == 1.0) out = pulse(p, sim->t);
+        else if (p[1] == 2.0) out = sine(p, sim->t);
+        else if (p[1] == 3.0) out = expo(p, sim->t);
+        else if (p[1] == 4.0) out = pwl(p, sim->t);
+    }
     return out * sim->src_scale;
 }
 
@@ -407,7 +464,7 @@ void dev_eval(uint32_t type, const uint32_t *nd, const double *prm, const double
         break;
     }
     case ORC_I: {
-        double v = prm[0] * sim->src_scale;
+        double v = source_value(prm, sim);
         o->f[0] = v;
         o->f[1] = -v;
         break;

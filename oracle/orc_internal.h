@@ -4,7 +4,7 @@
 
 #include "espice_oracle.h"
 
-/* exp, log and pow of the bias-dependent model code: the functions the CUDA
+/* exp, log, pow and sin of the model code: the functions the CUDA
  * kernels use (espice_b200/csrc/esl_math.h), so that the oracle's model
  * evaluations are bitwise the device's. Built with ORC_LIBM_TRANSCENDENTALS
  * (liboracle_libm.so) they are the host C library's instead, which shows
@@ -15,6 +15,7 @@
 #define esl_exp exp
 #define esl_log log
 #define esl_pow pow
+#define esl_sin sin
 #else
 #include "../espice_b200/csrc/esl_math.h"
 #endif

@@ -11,7 +11,8 @@
  *                                        breakpoint landing and clamping
  *   src/analysis/tran/integrator.zig:40-53 coeffs, :166-212 companionAt,
  *                                        :348-424 stepBound / minDel (CKTterr)
- *   models/vsource.va:133-136            PULSE corners as periodic timers
+ *   models/vsource.va:133-200            PULSE corners as periodic timers,
+ *                                        PWL corners as one-shot timers
  * Left out (no device on this path uses them): uic, VPI callbacks, state
  * flips and reject_at, bound_step, stateful-charge rebase, delay-line
  * echoes, gear orders above 2 and tangents. Measures (orc_meas.c) are fed
@@ -31,17 +32,35 @@
 #define LTE_TRAP 0.08333333333
 
 typedef struct {
-    double start, per;
+    double start, per; /* per 0: a one-shot timer */
 } timer_t_;
 
-/* The PULSE corner timers of every V source with a PULSE wave. */
-static uint32_t pulse_timers(const ckt_t *k, timer_t_ *out, uint32_t cap) {
+/* The corner timers of the circuit's sources (vsource.va / isource.va):
+ * the 4 periodic PULSE corners of each PULSE source (:133-136), and for a
+ * PWL source one one-shot timer per table time plus TD, and TD itself when
+ * the table leaves slots unused (their times read 0). Timers at or before
+ * the first step never act (breakpoints are sought after t + min_break). */
+static uint32_t source_timers(const ckt_t *k, timer_t_ *out, uint32_t cap) {
     uint32_t m = 0;
     for (uint32_t b = 0; b < k->nb; b++) {
         const bat_t *bt = &k->bt[b];
-        if (bt->type != ORC_V) continue;
+        if (bt->type != ORC_V && bt->type != ORC_I) continue;
         for (uint32_t id = 0; id < bt->count; id++) {
             const double *p = bt->prm + (size_t)id * bt->np;
+            if (p[1] == 4.0) {
+                const int len = (int)p[2];
+                for (int j = 0; j < len && m < cap; j++) {
+                    out[m].start = p[ORC_SRC_PWL_T + j] + p[4];
+                    out[m].per = 0.0;
+                    m++;
+                }
+                if (len < ORC_PWL_MAX && m < cap) {
+                    out[m].start = 0.0 + p[4];
+                    out[m].per = 0.0;
+                    m++;
+                }
+                continue;
+            }
             if (p[1] != 1.0) continue;
             double tr = p[5] > 1.0e-12 ? p[5] : 1.0e-12;
             double tf = p[6] > 1.0e-12 ? p[6] : 1.0e-12;
@@ -67,6 +86,7 @@ static int next_bp(const timer_t_ *tm, uint32_t nt, double after, double *bp) {
     for (uint32_t i = 0; i < nt; i++) {
         double t = tm[i].start;
         if (t < after) {
+            if (tm[i].per == 0.0) continue;
             double kk = ceil((after - tm[i].start) / tm[i].per);
             t = tm[i].start + kk * tm[i].per;
             if (t < after) t += tm[i].per;
@@ -210,8 +230,11 @@ static void tran_lane(ckt_t *k, const orc_tran_opts *o, rec_t *rec, uint32_t *st
     const double dt_max = o->tmax > 0 ? o->tmax : fmin(o->tstep, o->tstop / 50.0);
     const double delmin = 1e-11 * dt_max;
     const double min_break = 10.0 * delmin;
-    timer_t_ tm[64];
-    uint32_t nt = pulse_timers(k, tm, 64);
+    uint32_t cap_tm = 0;
+    for (uint32_t b = 0; b < k->nb; b++)
+        if (k->bt[b].type == ORC_V || k->bt[b].type == ORC_I) cap_tm += k->bt[b].count * (ORC_PWL_MAX + 4);
+    timer_t_ *tm = (timer_t_ *)calloc(cap_tm + 1, sizeof(timer_t_));
+    uint32_t nt = source_timers(k, tm, cap_tm);
     double dt = fmin(fmin(o->tstep, o->tstop / 100.0) / 10.0, dt_max);
     double bp0;
     if (next_bp(tm, nt, min_break, &bp0)) dt = fmin(dt, 0.1 * bp0);
@@ -349,6 +372,7 @@ static void tran_lane(ckt_t *k, const orc_tran_opts *o, rec_t *rec, uint32_t *st
         free(qt[i]);
     }
     free(ip_row); free(ip_st); free(cur); free(prev); free(trial);
+    free(tm);
 }
 
 /* MOS1 with TOX given carries the bias-dependent Meyer halves and their

@@ -69,6 +69,15 @@ FIXTURES = [
     "tran/bench_mosfet_nmos_cs",
     "tran/rc_pulse_history_trap",
     "tran/finite_rise_positive",
+    # transients under SIN, EXP and PWL sources (V and I)
+    "tran/sine",
+    "tran/sine_offset_phase",
+    "tran/rc_sinusoidal_startup",
+    "tran/bench_tran_exp_source",
+    "tran/source_exp_defaults_ngspice",
+    "tran/pwl_triangle",
+    "tran/pwl_nonzero_start",
+    "tran/pwl_isource_breakpoints",
     # transient measures (FIND .. AT=) against ngspice's printed values
     "tran/zero_abstol_vntol",
     "tran/zero_vntol_chgtol",

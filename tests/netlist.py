@@ -6,6 +6,7 @@ covers only what the committed fixtures use.
 
 from __future__ import annotations
 
+import math
 import re
 
 from espice_b200.circuit import Circuit
@@ -145,35 +146,74 @@ class Deck:
             elif kind == "c":
                 c.C(name, t[1], t[2], num(t[3]))
             elif kind in "vi":
+                c_src = c.V if kind == "v" else c.I
                 rest = " ".join(t[3:])
-                dc = 0.0
-                pulse = None
-                m = re.search(r"pulse\s*\(([^)]*)\)", rest, re.I)
-                if m:
-                    pulse = [num(v) for v in m.group(1).replace(",", " ").split()]
-                    rest = rest[: m.start()] + rest[m.end():]
-                toks = rest.split()
+                waves = {}
+                for w in ("pulse", "sin", "exp", "pwl"):
+                    m = re.search(w + r"\s*\(([^)]*)\)", rest, re.I)
+                    if m:
+                        waves[w] = [num(v) for v in m.group(1).replace(",", " ").split()]
+                        rest = rest[: m.start()] + rest[m.end():]
+                opts = {}
+                toks = []
+                for tok in rest.split():
+                    if "=" in tok:
+                        k, v = tok.split("=", 1)
+                        opts[k.lower()] = num(v)
+                    else:
+                        toks.append(tok)
+                dc = None
                 if toks and toks[0].lower() == "dc":
                     dc = num(toks[1])
                 elif toks:
                     dc = num(toks[0])
-                if kind == "v":
-                    if pulse is not None and not m.group(0).lower().startswith("dc"):
-                        if not (toks and toks[0].lower() == "dc"):
-                            dc = pulse[0]
-                    if pulse is not None and self.analysis and self.analysis[0] == "tran":
+                tran = self.analysis and self.analysis[0] == "tran"
+                tstep, tstop = (self.analysis[1], self.analysis[2]) if tran else (0.0, 0.0)
+                kw = {}
+                if "pulse" in waves:
+                    pulse = waves["pulse"]
+                    if dc is None:
+                        dc = pulse[0]
+                    if tran:
                         # PULSE defaults from the .tran card (ngspice TRANinit, the
                         # reference's resolvePulseDefaults): TR = TF = TSTEP,
                         # PW = PER = TSTOP
-                        tstep, tstop = self.analysis[1], self.analysis[2]
                         full = list(pulse) + [None] * (7 - len(pulse))
                         for k, dflt in ((3, tstep), (4, tstep), (5, tstop), (6, tstop)):
                             if full[k] is None:
                                 full[k] = dflt
                         pulse = [0.0 if v is None else v for v in full]
-                    c.V(name, t[1], t[2], dc=dc, pulse=pulse)
-                else:
-                    c.I(name, t[1], t[2], dc=dc)
+                    kw["pulse"] = pulse
+                elif "sin" in waves:
+                    sn = waves["sin"] + [0.0] * (6 - len(waves["sin"]))
+                    if sn[2] == 0.0 and tran:
+                        sn[2] = 1.0 / tstop  # SIN's frequency defaults to 1 / TSTOP
+                    if dc is None:
+                        dc = sn[0] + sn[1] * math.sin(sn[5] * math.pi / 180.0)
+                    kw["sin"] = sn[:6]
+                elif "exp" in waves:
+                    ex = waves["exp"] + [0.0] * (6 - len(waves["exp"]))
+                    if tran:
+                        # EXP's omitted (or 0) TD1, TAU1, TAU2 take TSTEP and TD2
+                        # TD1 + TSTEP (the reference builder's defaults)
+                        if ex[2] == 0.0:
+                            ex[2] = tstep
+                        if ex[3] == 0.0:
+                            ex[3] = tstep
+                        if ex[4] == 0.0:
+                            ex[4] = ex[2] + tstep
+                        if ex[5] == 0.0:
+                            ex[5] = tstep
+                    if dc is None:
+                        dc = ex[0]
+                    kw["exp"] = ex[:6]
+                elif "pwl" in waves:
+                    pts = waves["pwl"]
+                    times, values = pts[0::2], pts[1::2]
+                    if dc is None:
+                        dc = values[0]
+                    kw["pwl"] = (times, values, opts.get("r", -1.0), opts.get("td", 0.0))
+                c_src(name, t[1], t[2], dc=0.0 if dc is None else dc, **kw)
             elif kind == "d":
                 kindm, prm = self.models[t[3].lower()]
                 prm = dict(prm)

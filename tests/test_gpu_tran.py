@@ -134,6 +134,40 @@ def test_ring_oscillator_headline_window():
     assert _close(xg, xo).all(), float(np.max(np.abs(xg - xo)))
 
 
+def test_source_waves_vary_per_lane():
+    """An RC network driven by a SIN, an EXP and a PWL voltage source and a
+    PWL current source, twelve lanes each with its own wave parameters (SIN
+    amplitude and frequency, EXP time constant, PWL corner values and a
+    shifted PWL delay): the oracle's step decisions, breakpoint landings
+    included (each lane's own PWL corners), and its waveforms."""
+    from espice_b200.circuit import Circuit, I, V
+    c = Circuit()
+    c.V("vs", "a", "0", dc=0.0, sin=[0.2, 1.0, 5e8, 0.0, 1e7, 30.0])
+    c.V("ve", "b", "0", dc=0.0, exp=[0.0, 1.5, 1e-10, 4e-10, 1.2e-9, 3e-10])
+    c.V("vp", "c", "0", dc=0.0, pwl=([0.0, 3e-10, 7e-10, 1.1e-9, 1.6e-9], [0.0, 1.0, 1.0, -0.5, 0.2], -1.0, 0.0))
+    c.I("ip", "0", "d", dc=0.0, pwl=([0.0, 2e-10, 9e-10], [0.0, 1e-3, -5e-4], -1.0, 1e-10))
+    c.R("r1", "a", "x", 1e3)
+    c.R("r2", "b", "x", 2e3)
+    c.R("r3", "c", "x", 1.5e3)
+    c.R("r4", "d", "x", 500.0)
+    c.C("c1", "x", "0", 1e-13)
+    c.R("r5", "d", "0", 3e3)
+    c.C("c2", "d", "0", 5e-14)
+    fr = c.freeze()
+    slots = [fr.slot("vs", "v2"), fr.slot("vs", "td"), fr.slot("ve", "tr"), fr.slot("vp", "pwl_v1"),
+             fr.slot("vp", "pwl_v3"), fr.slot("ip", "td")]
+    rng = np.random.default_rng(11)
+    lanes_n = 12
+    values = np.stack([rng.uniform(0.5, 1.5, lanes_n), rng.uniform(3e8, 9e8, lanes_n),
+                       rng.uniform(2e-10, 6e-10, lanes_n), rng.uniform(0.5, 1.5, lanes_n),
+                       rng.uniform(-1.0, 0.0, lanes_n), rng.uniform(0.0, 3e-10, lanes_n)], axis=1)
+    probes = [fr.unknown("v(x)"), fr.unknown("v(d)")]
+    res_g, res_o = _run_both(fr, slots, values, 2e-9, 1e-11, 2e-11, probes=probes, max_pts=4000)
+    _check_parity(res_g, res_o)
+    assert (res_g[3][:, 0] == lanes.TRAN_DONE).all()
+    assert (res_g[3][:, 6] >= 4).all()  # every lane landed on its PWL corners
+
+
 TRAN_FIXTURES = [n for n in gu.names("tran__") if gu.load(n)["plots"]]
 
 
