@@ -189,9 +189,9 @@ def test_golden_transients_as_gpu_lanes(name):
     values = np.zeros((2, 1))
     ctx = lanes.DcLanes(fr)
     ctx.set_lanes([], values)
-    res_g = ctx.tran(go, probes, 20_000)
+    res_g = ctx.tran(go, probes, 60_000)
     ctx.close()
-    res_o = oracle.tran(fr, [], values, oo, probes, 20_000)
+    res_o = oracle.tran(fr, [], values, oo, probes, 60_000)
     _check_parity(res_g, res_o)
     tg, vg, ng, sg, _, _ = res_g
     assert (sg[:, 0] == lanes.TRAN_DONE).all()
