@@ -21,6 +21,7 @@ SOURCES = [
     "csrc/host/records.cpp",
     "csrc/host/api.cpp",
     "csrc/host/lu_jit.cpp",
+    "csrc/host/points.cpp",
     "csrc/kernels/newton.cu",
     "csrc/kernels/block.cu",
     "csrc/kernels/mlp.cu",
@@ -33,7 +34,8 @@ def sources():
 
 
 def headers():
-    out = [os.path.join(ROOT, "include", "espice_lanes.h")]
+    inc = os.path.join(ROOT, "include")
+    out = [os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h")]
     for d in ("csrc", "csrc/host", "csrc/kernels"):
         p = os.path.join(HERE, d)
         out += [os.path.join(p, f) for f in os.listdir(p) if f.endswith((".h", ".hpp", ".cuh"))]
