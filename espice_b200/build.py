@@ -24,6 +24,7 @@ SOURCES = [
     "csrc/host/points.cpp",
     "csrc/kernels/newton.cu",
     "csrc/kernels/block.cu",
+    "csrc/kernels/derive.cu",
     "csrc/kernels/mlp.cu",
     "csrc/host/mlp_host.cu",
 ]

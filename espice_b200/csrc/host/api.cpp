@@ -20,6 +20,7 @@
 #include "../../../include/espice_lanes.h"
 #include "../kernels/block.h"
 #include "../kernels/launch.h"
+#include "../kernels/derive.h"
 #include "lu_jit.hpp"
 #include "records.hpp"
 #include "schedule.hpp"
@@ -228,7 +229,9 @@ struct esl_ctx {
   std::vector<double> rec_nominal;
 
   uint32_t n_lanes = 0;
-  std::vector<double> rec_lanes;
+  std::vector<double> rec_lane0;   // lane 0's records (the lead lane's, for the host-side tape builds)
+  std::vector<uint32_t> prm_off;   // each batch's first parameter in d_params
+  DevBuf d_rec_nominal, d_params, d_derive_items, d_derive_slots, d_values;
 
   bool have_tape = false;
   bool warp_ok = false;    // the tape's warp programs fit (16-bit value indices, a warp's shared memory)
@@ -1139,9 +1142,22 @@ int32_t esl_create(const esl_circuit* circuit, const esl_options* opts, esl_ctx*
   build_gather(ctx.get());
   ctx->order = order_columns(ctx->pat);
   ctx->rec_nominal.assign(rec, 0.0);
-  for (const auto& B : ctx->bats)
+  std::vector<double> params;
+  for (const auto& B : ctx->bats) {
+    ctx->prm_off.push_back(uint32_t(params.size()));
+    params.insert(params.end(), B.params.begin(), B.params.end());
     for (uint32_t id = 0; id < B.count; ++id)
       derive_instance(B.type, &B.params[size_t(id) * B.np], &ctx->rec_nominal[B.rec_off + id], B.count);
+  }
+  ctx->rec_lane0 = ctx->rec_nominal;
+  if (cudaError_t e = upload(ctx->d_rec_nominal, ctx->rec_nominal, ctx->stream)) {
+    *out = ctx.release();
+    return (*out)->cuda_fail(e, "nominal records");
+  }
+  if (cudaError_t e = upload(ctx->d_params, params, ctx->stream)) {
+    *out = ctx.release();
+    return (*out)->cuda_fail(e, "nominal parameters");
+  }
   if (int32_t rc = upload_topology(ctx.get())) {
     *out = ctx.release();
     return rc;
@@ -1182,58 +1198,49 @@ int32_t esl_set_lanes(esl_ctx* ctx, const esl_slot* slots, uint32_t n_slots, con
     if (slots[k].inst >= B.count || slots[k].param >= B.np) return ESL_INVALID_ARGUMENT;
   }
   cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
   ctx->n_lanes = n_lanes;
   const size_t R = ctx->rec_size;
-  ctx->rec_lanes.resize(size_t(n_lanes) * R);
   // The instances the slots touch, each with its slots: a lane re-derives
-  // every touched instance once, with all of its overrides in place.
-  struct Touched {
-    uint32_t batch, inst;
-    std::vector<uint32_t> slots;
-  };
-  std::vector<Touched> touched;
+  // every touched instance once, with all of its overrides in place; the
+  // device derives every lane's (derive.cu) from the nominal records.
+  std::vector<DeriveItem> items;
+  std::vector<DeriveSlot> dslots;
   {
-    std::unordered_map<uint64_t, size_t> at;
-    for (uint32_t k = 0; k < n_slots; ++k) {
-      const uint64_t key = (uint64_t(slots[k].batch) << 32) | slots[k].inst;
-      auto it = at.find(key);
-      if (it == at.end()) {
-        it = at.emplace(key, touched.size()).first;
-        touched.push_back(Touched{slots[k].batch, slots[k].inst, {}});
-      }
-      touched[it->second].slots.push_back(k);
+    std::vector<std::pair<uint64_t, uint32_t>> keyed;  // (batch, inst) key, slot
+    for (uint32_t k = 0; k < n_slots; ++k) keyed.push_back({(uint64_t(slots[k].batch) << 32) | slots[k].inst, k});
+    std::stable_sort(keyed.begin(), keyed.end(),
+                     [](const auto& a, const auto& b) { return a.first < b.first; });
+    for (size_t i = 0; i < keyed.size();) {
+      const uint32_t b = uint32_t(keyed[i].first >> 32), inst = uint32_t(keyed[i].first);
+      const HostBatch& B = ctx->bats[b];
+      DeriveItem it{};
+      it.type = B.type;
+      it.np = B.np;
+      it.rec_at = B.rec_off + inst;
+      it.stride = B.count;
+      it.prm_at = ctx->prm_off[b] + inst * B.np;
+      it.slot0 = uint32_t(dslots.size());
+      for (; i < keyed.size() && keyed[i].first == ((uint64_t(b) << 32) | inst); ++i)
+        dslots.push_back({slots[keyed[i].second].param, keyed[i].second});
+      it.slot1 = uint32_t(dslots.size());
+      items.push_back(it);
     }
   }
-  auto derive_lanes = [&](uint32_t l0, uint32_t l1) {
-    std::vector<double> prm;
-    for (uint32_t l = l0; l < l1; ++l) {
-      double* rec = &ctx->rec_lanes[size_t(l) * R];
-      std::copy(ctx->rec_nominal.begin(), ctx->rec_nominal.end(), rec);
-      for (const Touched& t : touched) {
-        const HostBatch& B = ctx->bats[t.batch];
-        prm.assign(B.params.begin() + size_t(t.inst) * B.np, B.params.begin() + size_t(t.inst + 1) * B.np);
-        for (uint32_t k : t.slots) prm[slots[k].param] = values[size_t(l) * n_slots + k];
-        derive_instance(B.type, prm.data(), rec + B.rec_off + t.inst, B.count);
-      }
-    }
-  };
-  // Lanes are independent: derive them on the host's threads when there is
-  // enough work to share.
-  const size_t work = size_t(n_lanes) * touched.size();
-  const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
-  const uint32_t n_thr = work < 4096 ? 1u : std::min<uint32_t>(hw, n_lanes);
-  if (n_thr <= 1) {
-    derive_lanes(0, n_lanes);
-  } else {
-    std::vector<std::thread> pool;
-    const uint32_t per = (n_lanes + n_thr - 1) / n_thr;
-    for (uint32_t t = 0; t < n_thr; ++t) {
-      const uint32_t l0 = t * per, l1 = std::min(n_lanes, l0 + per);
-      if (l0 < l1) pool.emplace_back(derive_lanes, l0, l1);
-    }
-    for (auto& th : pool) th.join();
+  ESL_CUDA(ctx->d_rec.ensure(size_t(n_lanes) * R * 8));
+  if (!items.empty()) {
+    ESL_CUDA(upload(ctx->d_derive_items, items, s));
+    ESL_CUDA(upload(ctx->d_derive_slots, dslots, s));
+    ESL_CUDA(ctx->d_values.ensure(size_t(n_lanes) * n_slots * 8));
+    ESL_CUDA(cudaMemcpyAsync(ctx->d_values.p, values, size_t(n_lanes) * n_slots * 8, cudaMemcpyHostToDevice, s));
   }
-  ESL_CUDA(upload(ctx->d_rec, ctx->rec_lanes, ctx->stream));
+  ESL_CUDA(launch_derive_lanes(ctx->d_rec_nominal.as<double>(), uint32_t(R), ctx->d_derive_items.as<DeriveItem>(),
+                               uint32_t(items.size()), ctx->d_derive_slots.as<DeriveSlot>(),
+                               ctx->d_params.as<double>(), ctx->d_values.as<double>(), n_slots, n_lanes,
+                               ctx->d_rec.as<double>(), s));
+  ctx->rec_lane0.resize(R);
+  ESL_CUDA(cudaMemcpyAsync(ctx->rec_lane0.data(), ctx->d_rec.p, R * 8, cudaMemcpyDeviceToHost, s));
+  ESL_CUDA(cudaStreamSynchronize(s));
   ctx->topo.rec_size = ctx->rec_size;
   ctx->peel.clear();
   return ensure_lane_buffers(ctx);
@@ -1247,47 +1254,16 @@ namespace {
 int32_t prepare_dc(esl_ctx* ctx, const esl_newton_opts* opts, double* d_x, int cold, uint32_t* d_iters,
                    uint32_t* d_status, esl_stats* st, LaneDev& L) {
   cudaStream_t s = ctx->stream;
-  const uint32_t N = ctx->n_lanes, n = ctx->pat.n;
   if (st) std::memset(st, 0, sizeof(*st));
-  // Per-lane start state: cold lanes start at zero with the junction seeds
-  // (op.zig coldStart), warm lanes at x with limiting off.
-  std::vector<uint32_t> flags(N, opts->init_fix ? 1u : 0u), act(N, cold && ctx->nlim ? 1u : 0u);
-  std::vector<double> limit(N, 1e9), lim(size_t(N) * std::max<uint32_t>(ctx->nlim, 1), 0.0);
-  if (cold) {
-    for (uint32_t l = 0; l < N; ++l)
-      for (const auto& B : ctx->bats) {
-        const double* rec = &ctx->rec_lanes[size_t(l) * ctx->rec_size + B.rec_off];
-        double* li = &lim[size_t(l) * ctx->nlim + B.lim_off];
-        if (B.type == kD)
-          for (uint32_t i = 0; i < B.count; ++i) li[i] = rec[kDVcrit * B.count + i];
-        if (B.type == kM)
-          for (uint32_t i = 0; i < B.count; ++i) {
-            li[3 * i] = rec[kMSeedVgs * B.count + i];
-            li[3 * i + 1] = 0.0;
-            li[3 * i + 2] = -1.0;
-          }
-        if (B.type == kB3)
-          for (uint32_t i = 0; i < B.count; ++i) {
-            li[3 * i] = rec[kB3SeedVgs * B.count + i];
-            li[3 * i + 1] = 0.1;
-            li[3 * i + 2] = 0.0;
-          }
-      }
-    ESL_CUDA(cudaMemsetAsync(d_x, 0, size_t(N) * n * 8, s));
-  }
-  ESL_CUDA(cudaMemcpyAsync(ctx->d_flags.p, flags.data(), N * 4, cudaMemcpyHostToDevice, s));
-  ESL_CUDA(cudaMemcpyAsync(ctx->d_lim_active.p, act.data(), N * 4, cudaMemcpyHostToDevice, s));
-  ESL_CUDA(cudaMemcpyAsync(ctx->d_limit.p, limit.data(), N * 8, cudaMemcpyHostToDevice, s));
-  ESL_CUDA(cudaMemcpyAsync(ctx->d_lim.p, lim.data(), lim.size() * 8, cudaMemcpyHostToDevice, s));
-  ESL_CUDA(cudaMemsetAsync(d_status, 0, N * 4, s));
-  ESL_CUDA(cudaMemsetAsync(d_iters, 0, N * 4, s));
-  ESL_CUDA(cudaMemsetAsync(ctx->d_paused.p, 0, 4, s));
+  // Per-lane start state, set on the device (lane_init_kernel): cold lanes
+  // start at zero with the junction seeds (op.zig coldStart), warm lanes at
+  // x with limiting off.
   ctx->peel.clear();
-
   L = lane_view(ctx, 0);
   L.x = d_x;
   L.iters = d_iters;
   L.status = d_status;
+  ESL_CUDA(launch_lane_init(ctx->topo, L, cold != 0, opts->init_fix != 0, s));
   if (!ctx->have_tape) {
     // The lead lane's first Jacobian, factored on the host into the tape.
     ESL_CUDA(lead_jacobian(ctx, L, ctx->d_a_vals.as<double>()));
@@ -1451,7 +1427,7 @@ int32_t ensure_tape_cold(esl_ctx* ctx) {
   const uint32_t n = ctx->pat.n;
   std::vector<double> lim(std::max<uint32_t>(ctx->nlim, 1), 0.0);
   for (const auto& B : ctx->bats) {
-    const double* rec = &ctx->rec_lanes[B.rec_off];
+    const double* rec = &ctx->rec_lane0[B.rec_off];
     if (B.type == kD)
       for (uint32_t i = 0; i < B.count; ++i) lim[B.lim_off + i] = rec[kDVcrit * B.count + i];
     if (B.type == kM)
@@ -1551,7 +1527,7 @@ int32_t esl_dc_sweep_device(esl_ctx* ctx, const esl_slot* slot, const double* va
     // (the first Jacobian the sweep solves), its source set there for the
     // assembly and restored after.
     double* src = ctx->d_rec.as<double>() + SB.rec_off + slot->inst;
-    const double first = values[0], keep = ctx->rec_lanes[SB.rec_off + slot->inst];
+    const double first = values[0], keep = ctx->rec_lane0[SB.rec_off + slot->inst];
     ESL_CUDA(cudaMemcpyAsync(src, &first, 8, cudaMemcpyHostToDevice, s));
     const int32_t rc = ensure_tape_cold(ctx);
     ESL_CUDA(cudaMemcpyAsync(src, &keep, 8, cudaMemcpyHostToDevice, s));

@@ -64,7 +64,7 @@ class LearnedWarmStart:
         return out.double()
 
 
-def solve(ctx, fallback, ws, slots, values, x_nominal, k=8, opts=None, d_values=None):
+def solve(ctx, fallback, ws, slots, values, x_nominal, k=8, opts=None, d_values=None, stats_out=None):
     """Solves every lane of `ctx` (lanes already set to `values`) from the
     learned guess with at most `k` Newton iterations, then the lanes that did
     not converge again from `x_nominal` on `fallback` (a DcLanes of the same
@@ -72,7 +72,9 @@ def solve(ctx, fallback, ws, slots, values, x_nominal, k=8, opts=None, d_values=
     lanes' records are), else they are uploaded. Returns (x [N][n] device
     tensor, iterations [N] (both passes), converged mask [N] host, number of
     fallback lanes). The returned x is the learned start's work buffer for
-    this batch size: valid until its next solve of the same size."""
+    this batch size: valid until its next solve of the same size. With
+    stats_out a list, the solves' statistics (esl_stats dicts) are appended
+    to it."""
     import torch
     opts = opts or lanes.newton_opts()
     N = values.shape[0]
@@ -83,14 +85,18 @@ def solve(ctx, fallback, ws, slots, values, x_nominal, k=8, opts=None, d_values=
     capped = lanes.newton_opts(opts.reltol, opts.abstol, opts.vntol, opts.residual_tol, opts.gmin,
                                opts.max_iter, bool(opts.init_fix), iter_cap=k)
     torch.cuda.current_stream().synchronize()
-    ctx.solve_device(d_x.data_ptr(), words[1].data_ptr(), words[0].data_ptr(), cold=False, opts=capped)
+    s = ctx.solve_device(d_x.data_ptr(), words[1].data_ptr(), words[0].data_ptr(), cold=False, opts=capped)
+    if stats_out is not None:
+        stats_out.append(s)
     host = words.cpu().numpy()
     st = host[0]
     it = host[1].astype(np.int64)
     failed = np.flatnonzero(st != lanes.LANE_CONVERGED)
     if len(failed):
         fallback.set_lanes(slots, values[failed])
-        xf, itf, stf, _ = fallback.solve(x0=np.broadcast_to(x_nominal, (len(failed), len(x_nominal))), opts=opts)
+        xf, itf, stf, sf = fallback.solve(x0=np.broadcast_to(x_nominal, (len(failed), len(x_nominal))), opts=opts)
+        if stats_out is not None:
+            stats_out.append(sf)
         d_x[torch.as_tensor(failed, device="cuda")] = torch.tensor(xf, device="cuda")
         it[failed] += itf
         st[failed] = stf

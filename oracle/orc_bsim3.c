@@ -57,14 +57,14 @@ void bsim3_derive(const double *p, double *d) {
     const double vt = 8.617087e-5 * tk;
     const double eg0 = 1.16 - 7.02e-4 * tnomk * tnomk / (tnomk + 1108.0);
     const double eg = 1.16 - 7.02e-4 * tk * tk / (tk + 1108.0);
-    const double ni = 1.45e10 * (tnomk / 300.15) * sqrt(tnomk / 300.15) * exp(21.5565981 - eg0 / (2.0 * vtnom));
+    const double ni = 1.45e10 * (tnomk / 300.15) * sqrt(tnomk / 300.15) * esl_exp(21.5565981 - eg0 / (2.0 * vtnom));
     const double cox = 3.453133e-11 / tox;
     const double factor1 = sqrt(1.03594e-10 / 3.453133e-11 * tox);
     const double vt0 = 1.38064852e-23 * 300.15 / 1.6021766208e-19;
-    const double vcrit = vt0 * log(vt0 / (1.4142135623730951 * 1.0e-14));
+    const double vcrit = vt0 * esl_log(vt0 / (1.4142135623730951 * 1.0e-14));
     double jst, jswt;
     if (tk != tnomk) {
-        const double jtmp = exp((eg0 / vtnom - eg / vt + p[ORC_B3_XTI] * log(tratio)) / p[ORC_B3_NJ]);
+        const double jtmp = esl_exp((eg0 / vtnom - eg / vt + p[ORC_B3_XTI] * esl_log(tratio)) / p[ORC_B3_NJ]);
         jst = p[ORC_B3_JS] * jtmp;
         jswt = p[ORC_B3_JSW] * jtmp;
     } else {
@@ -76,11 +76,11 @@ void bsim3_derive(const double *p, double *d) {
 
     /* geometry (:214-229) */
     const double l = p[ORC_B3_L], w = p[ORC_B3_W];
-    double t0 = pow(l, p[ORC_B3_LLN]);
-    double t1 = pow(w, p[ORC_B3_LWN]);
+    double t0 = esl_pow(l, p[ORC_B3_LLN]);
+    double t1 = esl_pow(w, p[ORC_B3_LWN]);
     const double dl = p[ORC_B3_LINT] + p[ORC_B3_LL] / t0 + p[ORC_B3_LW] / t1 + p[ORC_B3_LWL] / (t0 * t1);
-    double t2 = pow(l, p[ORC_B3_WLN]);
-    double t3 = pow(w, p[ORC_B3_WWN]);
+    double t2 = esl_pow(l, p[ORC_B3_WLN]);
+    double t3 = esl_pow(w, p[ORC_B3_WWN]);
     const double dwx = p[ORC_B3_WINT] + p[ORC_B3_WL] / t2 + p[ORC_B3_WW] / t3 + p[ORC_B3_WWL] / (t2 * t3);
     double leff = l + p[ORC_B3_XL] - 2.0 * dl;
     double weff = w + p[ORC_B3_XW] - 2.0 * dwx;
@@ -103,9 +103,9 @@ void bsim3_derive(const double *p, double *d) {
     else if (type > 0.0) u0x = 0.067;
     else u0x = 0.025;
     if (u0x > 1.0) u0x = u0x / 1.0e4;
-    const double u0temp = u0x * pow(tratio, p[ORC_B3_UTE]) * p[ORC_B3_MULU0];
+    const double u0temp = u0x * esl_pow(tratio, p[ORC_B3_UTE]) * p[ORC_B3_MULU0];
     const double vsattemp = p[ORC_B3_VSAT] - p[ORC_B3_AT] * (tratio - 1.0);
-    const double rds0 = (p[ORC_B3_RDSW] + p[ORC_B3_PRT] * (tratio - 1.0)) / pow(weff * 1.0e6, p[ORC_B3_WR]);
+    const double rds0 = (p[ORC_B3_RDSW] + p[ORC_B3_PRT] * (tratio - 1.0)) / esl_pow(weff * 1.0e6, p[ORC_B3_WR]);
 
     /* doping-derived quantities (:249-268) */
     double npeakx;
@@ -120,12 +120,12 @@ void bsim3_derive(const double *p, double *d) {
     }
     double ngatex = p[ORC_B3_NGATE];
     if (ngatex > 1.000001e24) ngatex = ngatex * 1.0e-6;
-    const double phi = 2.0 * vtnom * log(npeakx / ni);
+    const double phi = 2.0 * vtnom * esl_log(npeakx / ni);
     const double sqrtphi = sqrt(phi);
     const double phis3 = sqrtphi * phi;
     const double xdep0 = sqrt(2.0 * 1.03594e-10 / (1.60219e-19 * npeakx * 1.0e6)) * sqrtphi;
     const double litl = sqrt(3.0 * p[ORC_B3_XJ] * tox);
-    const double vbi = vtnom * log(1.0e20 * npeakx / (ni * ni));
+    const double vbi = vtnom * esl_log(1.0e20 * npeakx / (ni * ni));
     const double cdep0 = sqrt(1.60219e-19 * 1.03594e-10 * npeakx * 1.0e6 / 2.0 / phi);
 
     /* k1/k2 ladder (:270-290) */
@@ -172,9 +172,9 @@ void bsim3_derive(const double *p, double *d) {
 
     const double dsubx = GIVEN(ORC_B3_DSUB) ? p[ORC_B3_DSUB] : p[ORC_B3_DROUT];
     const double lt0 = factor1 * sqrt(xdep0);
-    t0 = exp(-0.5 * dsubx * leff / lt0);
+    t0 = esl_exp(-0.5 * dsubx * leff / lt0);
     const double theta0vb0 = t0 + 2.0 * t0 * t0;
-    t0 = exp(-0.5 * p[ORC_B3_DROUT] * leff / lt0);
+    t0 = esl_exp(-0.5 * p[ORC_B3_DROUT] * leff / lt0);
     const double thetarout = p[ORC_B3_PDIBLC1] * (t0 + 2.0 * t0 * t0) + p[ORC_B3_PDIBLC2];
 
     /* junction sizing (:323-338) */
@@ -185,12 +185,12 @@ void bsim3_derive(const double *p, double *d) {
     const double isatd = (ad <= 0.0 && pd <= 0.0) ? 1.0e-14 : ad * jst + pd * jswt;
     double vjsm = 0.0, isevjsm = 0.0, vjdm = 0.0, isevjdm = 0.0;
     if (isats > 0.0 && ijth > 0.0) {
-        vjsm = nvtmj * log(ijth / isats + 1.0);
-        isevjsm = isats * exp(vjsm / nvtmj);
+        vjsm = nvtmj * esl_log(ijth / isats + 1.0);
+        isevjsm = isats * esl_exp(vjsm / nvtmj);
     }
     if (isatd > 0.0 && ijth > 0.0) {
-        vjdm = nvtmj * log(ijth / isatd + 1.0);
-        isevjdm = isatd * exp(vjdm / nvtmj);
+        vjdm = nvtmj * esl_log(ijth / isatd + 1.0);
+        isevjdm = isatd * esl_exp(vjdm / nvtmj);
     }
 
     /* series resistance (:340-346) */

@@ -255,8 +255,8 @@ static void diode_derive(const double *p, double *d) {
     double fact1 = tnomk / 300.15, fact2 = tk / 300.15;
     double arg1 = -egfet1 / (2.0 * KB * tnomk) + 1.1150877 / (2.0 * KB * 300.15);
     double argt = -egfet / (2.0 * KB * tk) + 1.1150877 / (2.0 * KB * 300.15);
-    double pbfact1 = -2.0 * vtnom * (1.5 * log(fact1) + QE * arg1);
-    double pbfact = -2.0 * vt * (1.5 * log(fact2) + QE * argt);
+    double pbfact1 = -2.0 * vtnom * (1.5 * esl_log(fact1) + QE * arg1);
+    double pbfact = -2.0 * vt * (1.5 * esl_log(fact2) + QE * argt);
     double vj = p[ORC_D_VJ];
     double pbo = (vj - pbfact1) / fact1;
     double gmaold = (vj - pbo) / pbo;
@@ -265,19 +265,19 @@ static void diode_derive(const double *p, double *d) {
     double cjo_t = p[ORC_D_CJO] * (1.0 + mt * (400e-6 * (tk - 300.15) - gmanew)) /
                    (1.0 + mt * (400e-6 * (tnomk - 300.15) - gmaold));
     cjo_t = cjo_t * ae;
-    double is_t = p[ORC_D_IS] * ae * exp((ratio - 1.0) * egp / vte + (p[ORC_D_XTI] / n) * log(ratio));
+    double is_t = p[ORC_D_IS] * ae * esl_exp((ratio - 1.0) * egp / vte + (p[ORC_D_XTI] / n) * esl_log(ratio));
     double bv_t = p[ORC_D_BV];
     double ibvx = p[ORC_D_IBV];
     double xbv = bv_t;
     if (p[ORC_D_BV] > 0.0 && ibvx >= is_t * bv_t / vt) {
-        xbv = bv_t - vtebrk * log(1.0 + ibvx / is_t);
-        xbv = bv_t - vtebrk * log(ibvx / is_t + 1.0 - xbv / vt);
+        xbv = bv_t - vtebrk * esl_log(1.0 + ibvx / is_t);
+        xbv = bv_t - vtebrk * esl_log(ibvx / is_t + 1.0 - xbv / vt);
     }
     double rs_t = p[ORC_D_RS] / ae;
     if (rs_t < 1.0e-9) rs_t = 1.0e-9;
     d[DD_VTE] = vte;
     d[DD_IS] = is_t;
-    d[DD_VCRIT] = vte * log(vte / (1.4142135623730951 * is_t));
+    d[DD_VCRIT] = vte * esl_log(vte / (1.4142135623730951 * is_t));
     d[DD_RS] = rs_t;
     d[DD_GMIN] = p[ORC_D_GMIN];
     d[DD_BV] = p[ORC_D_BV];

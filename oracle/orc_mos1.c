@@ -55,14 +55,14 @@ void mos1_derive(const double *p, double *d) {
     const double egfet = 1.16 - (7.02e-4 * tk * tk) / (tk + 1108.0);
     const double arg1 = -egfet1 / (2.0 * KB * tnomk) + 1.1150877 / (2.0 * KB * 300.15);
     const double argt = -egfet / (2.0 * KB * tk) + 1.1150877 / (2.0 * KB * 300.15);
-    const double pbfact1 = -2.0 * vtnom * (1.5 * log(fact1) + QE * arg1);
-    const double pbfact = -2.0 * vt * (1.5 * log(fact2) + QE * argt);
+    const double pbfact1 = -2.0 * vtnom * (1.5 * esl_log(fact1) + QE * arg1);
+    const double pbfact = -2.0 * vt * (1.5 * esl_log(fact2) + QE * argt);
     const double ratio4 = (tk / tnomk) * sqrt(tk / tnomk);
     const double kpt = kpx / ratio4;
     const double phio = (phix - pbfact1) / fact1;
     const double phit = fact2 * phio + pbfact;
     const double vbit = vtox - type * (gammax * sqrt(phix)) + 0.5 * (egfet1 - egfet) + type * 0.5 * (phit - phix);
-    const double ist = p[ORC_M_IS] * exp(-egfet / vt + egfet1 / vtnom);
+    const double ist = p[ORC_M_IS] * esl_exp(-egfet / vt + egfet1 / vtnom);
     const double pb = p[ORC_M_PB], mj = p[ORC_M_MJ], mjsw = p[ORC_M_MJSW];
     const double pbo = (pb - pbfact1) / fact1;
     const double pbt = fact2 * pbo + pbfact;
@@ -85,8 +85,8 @@ void mos1_derive(const double *p, double *d) {
     const double fc = p[ORC_M_FC];
     const double depcap = fc * pbt;
     const double argf = 1.0 - fc;
-    const double sargb = pow(argf, -mj);
-    const double sargs = pow(argf, -mjsw);
+    const double sargb = esl_pow(argf, -mj);
+    const double sargs = esl_pow(argf, -mjsw);
     const double f2d = czbd * (1.0 - fc * (1.0 + mj)) * sargb / argf + czbdsw * (1.0 - fc * (1.0 + mjsw)) * sargs / argf;
     const double f3d = czbd * mj * sargb / (argf * pbt) + czbdsw * mjsw * sargs / (argf * pbt);
     const double f4d = czbd * pbt * (1.0 - argf * sargb) / (1.0 - mj) + czbdsw * pbt * (1.0 - argf * sargs) / (1.0 - mjsw) -
@@ -104,8 +104,8 @@ void mos1_derive(const double *p, double *d) {
     d[MD_LAMBDA] = p[ORC_M_LAMBDA];
     d[MD_ISATS] = isats;
     d[MD_ISATD] = isatd;
-    d[MD_VCRITS] = vt * log(vt / (1.4142135623730951 * isats));
-    d[MD_VCRITD] = vt * log(vt / (1.4142135623730951 * isatd));
+    d[MD_VCRITS] = vt * esl_log(vt / (1.4142135623730951 * isats));
+    d[MD_VCRITD] = vt * esl_log(vt / (1.4142135623730951 * isatd));
     d[MD_GDRAIN] = p[ORC_M_RD] > 0.0 ? m / p[ORC_M_RD] : 0.0;
     d[MD_GSOURCE] = p[ORC_M_RS] > 0.0 ? m / p[ORC_M_RS] : 0.0;
     d[MD_CZBD] = czbd;
