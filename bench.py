@@ -1,25 +1,39 @@
-"""Benchmark: converged sweep points/s of the sweep-lane Newton path on B200.
+"""Benchmark: converged sweep points/s of the sweep-lane Newton path on B200,
+learned warm start + mixed precision against plain FP64, at 1e-9.
 
     python bench.py --gpus N --steps K --warmup W [--impl reference]
 
-Workload (one GPU): Monte-Carlo transient lanes of a 31-stage MOS1 CMOS ring
-oscillator (1024 lanes, per-device VTO ~ N(nominal, 30 mV), trapezoidal to
-20 ns with a 1 ps maximum step). A point is one lane's whole transient (its
-operating point, then about 20,000 accepted steps); a step of the benchmark
-is one pass over all lanes, one launch of the fused transient kernel.
-`value` is device-timed (CUDA events on the library's stream, the lanes'
-records resident in HBM, L2 flushed between steps); `e2e` is the same metric
-through the public C ABI with host buffers (esl_set_lanes uploads each
-step's per-lane records, esl_tran returns solutions and step statistics),
-copies inside the timed region. The DC sweep of the grid-with-diodes deck is
-reported beside it (`dc_grid_diodes`). Under torchrun each rank runs its own
-lane batch (independent samples, no collective on the data path, weak
-scaling); times are the max over ranks.
+Workload (one GPU): the 500-unknown BSIM3 analog block (498 unknowns with
+ground, 120 MOSFETs: twenty five-transistor OTA followers on a 20 x 21 RC
+mesh, a six-branch bias network and a source follower), 65,536 seeded sweep
+points of its 16 parameters (two supplies, six bias currents 1-100 uA
+log-uniform, temperature -40..125 C, seven VTO shifts of +-50 mV), each an
+independent DC operating point solved to reltol 1e-9, vntol 1e-12 V, abstol
+1e-15 A. A step is one pass over all 65,536 points:
+- learned + mixed (`value`): the tanh MLP (16 -> 512 -> 512 -> 498, BF16
+  tcgen05 GEMMs with FP32 accumulation, trained on the GPU on 32,768 other
+  points' plain-solver solutions before timing) predicts every point's
+  start; the mixed-precision block lanes (FP32 refactor and solves, FP64
+  evaluation, residual, refinement and gates) run at most 8 Newton
+  iterations from it; the points that did not converge are solved again from
+  the nominal operating point;
+- plain FP64 (`plain_fp64`): the FP64 block lanes from the nominal point.
+`value` is converged points / device time (CUDA events around each step on
+the launching stream, the lanes' records resident in HBM, L2 flushed before
+each step). `e2e` is the same metric through the public API with host
+buffers: each step uploads the points' parameter values (esl_set_lanes,
+records derived on the device) and the network's inputs, and reads every
+point's solution back. Side blocks: the 31-stage ring-oscillator transient
+lanes (`ring_transient`), the grid-with-diodes DC sweep, sequential sweep
+lanes, the ring's early-stopping period measure, the uneven batch of eight
+topologies (plain and mixed) and the lane LU against the HBM roofline.
+Under torchrun each rank runs its own points (independent seeds, no
+collective on the data path, weak scaling); times are the max over ranks.
 
 --impl reference times the reference's CPU algorithm on this host's cores
 (the C restatement under oracle/, since the Zig reference cannot be built
-here): independent lanes, one per worker thread, as the reference's sweep
-pool runs them.
+here): plain FP64 Newton from the nominal operating point, one point per
+worker thread, as the reference's sweep pool runs them.
 """
 
 from __future__ import annotations
@@ -184,19 +198,66 @@ def cpu_model():
     return platform.processor() or "unknown"
 
 
+C4_POINTS = 65536
+C4_TRAIN = 32768
+
+
+def c4_workload(seed=2, points=C4_POINTS):
+    """The metric's configuration: the analog block and `points` seeded
+    points of its 16 parameters (seed 1 is the training set's)."""
+    from espice_b200 import decks
+    fr, expand = decks.analog_block()
+    params, nominal = decks.analog_block_params(seed=seed, points=points)
+    cfg = {"workload": "analog_block: 500-unknown BSIM3 analog block (498 unknowns incl. ground, 120 MOSFETs: "
+                       "20 five-transistor OTA followers on a 20x21 RC mesh, a 6-branch bias network, a source "
+                       "follower), 16 parameters (VDD, VREF, 6 bias currents 1-100 uA log-uniform, temperature "
+                       "-40..125 C, 7 DELVTO shifts +-50 mV); a point = one independent DC operating point; "
+                       "learned warm start + mixed-precision block lanes",
+           "points": int(points), "unknowns": int(fr.n), "parameters": 16, "seed": seed,
+           "training_points": C4_TRAIN, "training_seed": 1,
+           "reltol": TIGHT["reltol"], "vntol": TIGHT["vntol"], "abstol": TIGHT["abstol"],
+           "l2": "flushed before each timed step (256 MiB write); the lanes' records alone exceed L2"}
+    return fr, expand, params, nominal, cfg
+
+
+def cpu_dc(fr, slots, values, x0, opts, threads, seconds, keep=None):
+    """The oracle's DC points (plain FP64 Newton from x0) on `threads` host
+    threads (ctypes calls release the GIL), one point per task, until
+    `seconds` have passed (the points started by then finish). Returns
+    (converged points, wall seconds); with keep a dict, keep[i] = (x,
+    iterations, converged) of each point run."""
+    from oracle import oracle
+    t0 = time.perf_counter()
+
+    def run(i):
+        if time.perf_counter() - t0 > seconds:
+            return 0
+        x, it, cv = oracle.dc_points(fr, slots, values[i:i + 1], warm=x0, opts=opts)
+        if keep is not None:
+            keep[i] = (x[0].copy(), int(it[0]), bool(cv[0]))
+        return int(cv[0])
+
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        done = sum(ex.map(run, range(values.shape[0])))
+    return done, time.perf_counter() - t0
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return
-    fr, slots, values, cfg = workload()
+    from oracle import oracle
+    fr, expand, params, nominal, cfg = c4_workload()
+    oo = oracle.newton_opts(**TIGHT)
+    xn, _, cvn = oracle.dc_points(fr, expand.slots, expand(nominal), warm=None, opts=oo)
     threads = os.cpu_count() or 1
-    per_step = max(threads, 2 * threads)  # a bounded sample of the batch
-    sample = values[:per_step]
+    per_step = 128 * threads  # a bounded sample of the 65,536 points
+    vals = expand(params[:per_step])
     for _ in range(args.warmup):
-        cpu_tran(fr, slots, sample[:threads], threads, 1e9)
+        cpu_dc(fr, expand.slots, vals[:threads], xn[0], oo, threads, 1e9)
     t0 = time.perf_counter()
     pts = 0
     for _ in range(args.steps):
-        d, _ = cpu_tran(fr, slots, sample, threads, 1e9)
+        d, _ = cpu_dc(fr, expand.slots, vals, xn[0], oo, threads, 1e9)
         pts += d
     dt = time.perf_counter() - t0
     v = pts / dt
@@ -206,10 +267,15 @@ def reference_arm(args, rank, world):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": cfg,
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "cpu": cpu_model(),
-                         "sample": f"{args.steps} steps of {per_step} of the {values.shape[0]} lanes"},
+                         "sample": f"{args.steps} steps of the first {per_step} of the {C4_POINTS} points, "
+                                   "plain FP64 Newton from the nominal operating point"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
+
+# DRAM bytes per point of one mixed dc_block_kernel launch on the analog
+# block, from an ncu capture (None until one is recorded).
+C4_BLOCK_DRAM_BYTES_PER_LANE = None
 
 # DRAM bytes per lane of one tran_kernel launch, from an ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum, --set full) of 148 ring
@@ -472,131 +538,6 @@ def _dev(a, b):
     return float(rel.max()), float(within.mean())
 
 
-def learned_mixed_c4(args, local, flush, points=65536, n_train=32768):
-    """The metric on its configuration: the learned warm start with the
-    mixed-precision lanes against the plain FP64 lanes, on the 500-unknown
-    BSIM3 analog block (120 MOSFETs, 16 parameters), 65,536 seeded points at
-    the 1e-9 setting. The network (16 -> 512 -> 512 -> n, tanh, BF16
-    tcgen05 GEMMs with FP32 accumulation) is trained on the GPU on 32,768
-    other points' plain-solver solutions. Plain: FP64 block lanes from the
-    nominal operating point. Learned + mixed: the network's guesses
-    (inference included), the mixed-precision lanes capped at 8 Newton
-    iterations, the lanes that did not converge again from the nominal point.
-    Each path is timed by wall clock with the device synchronised on both
-    sides, every point's lane state resident."""
-    import torch
-    from espice_b200 import decks, lanes, learned
-    from oracle import oracle
-    fr, expand = decks.analog_block()
-    p_train, nominal = decks.analog_block_params(seed=1, points=n_train)
-    p_test, _ = decks.analog_block_params(seed=2, points=points)
-    opts = lanes.newton_opts(**TIGHT)
-    oo = oracle.newton_opts(**TIGHT)
-    plain = lanes.DcLanes(fr, device=local)
-    plain.set_mode(precision=lanes.PREC_FP64, path=lanes.PATH_BLOCK)
-    plain.set_lanes(expand.slots, expand(nominal))
-    x_nom = plain.solve(x0=None, opts=opts)[0][0]
-    t0 = time.perf_counter()
-    plain.set_lanes(expand.slots, expand(p_train))
-    x_tr, _, st_tr, _ = plain.solve(x0=np.broadcast_to(x_nom, (n_train, fr.n)), opts=opts)
-    t_data = time.perf_counter() - t0
-    ok = st_tr == lanes.LANE_CONVERGED
-    ws = learned.LearnedWarmStart(16, fr.n, hidden=512, layers=3)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    loss = ws.fit(p_train[ok], x_tr[ok], epochs=60, batch=256, lr=2e-3, lr_end=2e-5)
-    torch.cuda.synchronize()
-    t_train = time.perf_counter() - t0
-    vals = expand(p_test)
-    t0 = time.perf_counter()
-    plain.set_lanes(expand.slots, vals)
-    t_set = time.perf_counter() - t0
-    mixed = lanes.DcLanes(fr, device=local)
-    mixed.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK)
-    mixed.set_lanes(expand.slots, vals)
-    fb = lanes.DcLanes(fr, device=local)
-    fb.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK)
-    N, n = points, fr.n
-    d_x = torch.empty((N, n), dtype=torch.float64, device="cuda")
-    d_it = torch.zeros(N, dtype=torch.int32, device="cuda")
-    d_st = torch.zeros(N, dtype=torch.int32, device="cuda")
-    x_nom_d = torch.tensor(x_nom, device="cuda")
-    d_p = torch.tensor(p_test, dtype=torch.float32, device="cuda")
-    steps = max(1, min(args.steps, 3))
-    plain_t, mixed_t, it_p, it_l, conv_p, conv_l, fallback, refine = [], [], 0.0, 0.0, 0, 0, 0, 0
-    for i in range(1 + steps):
-        flush.zero_()
-        d_x.copy_(x_nom_d.expand(N, n))
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        st_p = plain.solve_device(d_x.data_ptr(), d_it.data_ptr(), d_st.data_ptr(), cold=False, opts=opts)
-        torch.cuda.synchronize()
-        t2 = time.perf_counter()
-        if i >= 1:
-            plain_t.append(t2 - t1)
-            it_p += float(d_it.double().mean())
-            conv_p += int((d_st == lanes.LANE_CONVERGED).sum())
-        x_plain = d_x.cpu().numpy() if i == steps else None
-        flush.zero_()
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        xl, it, conv, nfb = learned.solve(mixed, fb, ws, expand.slots, vals, x_nom, k=8, opts=opts, d_values=d_p)
-        torch.cuda.synchronize()
-        t2 = time.perf_counter()
-        if i >= 1:
-            mixed_t.append(t2 - t1)
-            it_l += float(it.mean())
-            conv_l += int(conv.sum())
-            fallback += nfb
-        if i == steps:
-            x_learned = xl.cpu().numpy()
-    # attribution: the learned start on the FP64 lanes, and the mixed lanes
-    # from the nominal start (device time of one solve each)
-    guess = ws.predict(d_p, N).cpu().numpy()
-    _, it_lf, _, s_lf = plain.solve(x0=guess, opts=opts)
-    _, it_mn, _, s_mn = mixed.solve(x0=np.broadcast_to(x_nom, (N, n)), opts=opts)
-    s_pn = plain.solve(x0=np.broadcast_to(x_nom, (N, n)), opts=opts)[3]
-    # accuracy: every point against the plain FP64 lanes, a sample against
-    # the CPU oracle (FP64, from the nominal start)
-    idx = np.arange(0, N, 1024)
-    xo, ito, cvo = oracle.dc_points(fr, expand.slots, vals[idx], warm=x_nom, opts=oo)
-    dev_plain_oracle = _dev(x_plain[idx], xo)
-    dev_learned_oracle = _dev(x_learned[idx], xo)
-    dev_learned_plain = _dev(x_learned, x_plain)
-    for c in (plain, mixed, fb):
-        c.close()
-    ws.close()
-    k = len(plain_t)
-    pp = conv_p / sum(plain_t)
-    pl = conv_l / sum(mixed_t)
-    return {"workload": f"analog_block: 500-unknown BSIM3 analog block ({fr.n} unknowns incl. ground, 120 MOSFETs: "
-                        "20 five-transistor OTA followers on a 20x21 RC mesh, a 6-branch bias network, a source "
-                        "follower), 16 parameters (VDD, VREF, 6 bias currents 1-100 uA log-uniform, temperature "
-                        "-40..125 C, 7 DELVTO shifts +-50 mV); 65,536 test points, 32,768 training points",
-            "newton": "reltol 1e-9, vntol 1e-12, abstol 1e-15 (every start converges to the same solution within "
-                      "1e-9; at reltol 1e-3 a point's result depends on its start at the 1e-3 level)",
-            "plain_points_per_s": pp, "learned_mixed_points_per_s": pl,
-            "learned_mixed_over_plain": pl / pp,
-            "attribution_device_ms": {"plain_fp64_nominal": s_pn["kernel_ms"],
-                                      "learned_fp64": s_lf["kernel_ms"], "mixed_nominal": s_mn["kernel_ms"],
-                                      "learned_over_plain_fp64": s_pn["kernel_ms"] / s_lf["kernel_ms"],
-                                      "mixed_over_fp64_nominal": s_pn["kernel_ms"] / s_mn["kernel_ms"]},
-            "newton_iters_plain": it_p / k, "newton_iters_learned": it_l / k,
-            "newton_iters_learned_fp64": float(it_lf.mean()), "fallback_lanes": fallback / k,
-            "max_rel_dev": {"plain_vs_cpu_oracle": dev_plain_oracle[0],
-                            "learned_mixed_vs_cpu_oracle": dev_learned_oracle[0],
-                            "learned_mixed_vs_plain_all_points": dev_learned_plain[0]},
-            "within_1e-9": {"plain_vs_cpu_oracle": dev_plain_oracle[1],
-                            "learned_mixed_vs_cpu_oracle": dev_learned_oracle[1],
-                            "learned_mixed_vs_plain_all_points": dev_learned_plain[1]},
-            "oracle_sample": f"{len(idx)} points (every 1024th)",
-            "setup_s": {"record_derivation_65536": t_set, "training_solutions_32768": t_data,
-                        "training_60_epochs": t_train},
-            "train_loss_first_last": [float(loss[0]), float(loss[-1])],
-            "timing": "wall clock around each path with device synchronisation (inference, solves and fallback "
-                      f"included), {k} steps after one warm-up, L2 flushed before each path"}
-
-
 def uneven_c3(args, local, flush, lanes_per_topo=512):
     """Uneven batching on its configuration: 4,096 DC lanes over the eight
     mesh-with-gates topologies (50 to 2,000 unknowns, 512 supply values each
@@ -659,67 +600,7 @@ def uneven_c3(args, local, flush, lanes_per_topo=512):
     return out
 
 
-def our_arm(args, rank, world):
-    import torch
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    from espice_b200 import lanes
-    fr, slots, values, cfg = workload(seed=1 + rank, lanes_n=args.lanes, t_stop=args.t_stop)
-    go, _ = tran_opts_pair(args.t_stop)
-    ctx = lanes.DcLanes(fr, device=local)
-    ctx.set_lanes(slots, values)
-    N, n = values.shape[0], fr.n
-    d_x = torch.zeros((N, n), dtype=torch.float64, device="cuda")
-    d_st = torch.zeros((N, len(lanes.TS_FIELDS)), dtype=torch.int32, device="cuda")
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-
-    def step():
-        torch.cuda.synchronize()
-        return ctx.tran_device(go, d_x.data_ptr(), d_st.data_ptr())
-
-    for _ in range(args.warmup):
-        step()
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    ms, done, steps_acc, nr_iters = [], 0, 0, 0
-    with ClockSampler(local) as clk:
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            flush.zero_()
-            ms.append(step())
-            st = d_st.cpu().numpy()
-            done += int((st[:, 0] == lanes.TRAN_DONE).sum())
-            steps_acc += int(st[:, 1].sum())
-            nr_iters += int(st[:, 3].sum())
-        torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
-    dev_s = sum(ms) / 1e3
-
-    # e2e through the public API with host buffers: each step uploads the
-    # lanes' parameters (esl_set_lanes) and reads back solutions and stats.
-    e2e_t, e2e_done = [], 0
-    for i in range(args.warmup + args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        ctx.set_lanes(slots, values)
-        _, _, _, sth, xh, _ = ctx.tran(go)
-        t2 = time.perf_counter()
-        if i >= args.warmup:
-            e2e_t.append(t2 - t1)
-            e2e_done += int((sth[:, 0] == lanes.TRAN_DONE).sum())
-    e2e_s = sum(e2e_t)
-
-    # weak scaling: every rank ran its own batch; the job's time is the
-    # slowest rank's, its count the sum
-    from espice_b200 import shard
-    dev_s, done = shard.reduce_run(dev_s, done)
-    e2e_s, e2e_done = shard.reduce_run(e2e_s, e2e_done)
-    if rank != 0:
-        ctx.close()
-        return
-
+def load_peaks():
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -727,53 +608,310 @@ def our_arm(args, rank, world):
     except OSError:
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    step_s = dev_s / args.steps
+    return hbm_peak, "measured" if "hbm_gbs" in peaks else "fallback"
+
+
+def ring_transient(args, rank, world, local, flush):
+    """The transient Monte-Carlo lanes: the 31-stage MOS1 ring oscillator,
+    1024 lanes, trapezoidal to 20 ns with a 1 ps maximum step; a point is one
+    lane's whole transient, one tran_kernel launch per step. Device-timed,
+    end to end (esl_set_lanes + esl_tran with host buffers), the CPU
+    oracle's lanes/s on the host cores, and the lanes the CPU ran checked
+    decision for decision against the e2e run."""
+    import torch
+    from espice_b200 import lanes, shard
+    fr, slots, values, cfg = workload(seed=1 + rank, lanes_n=args.lanes, t_stop=args.t_stop)
+    go, _ = tran_opts_pair(args.t_stop)
+    ctx = lanes.DcLanes(fr, device=local)
+    ctx.set_lanes(slots, values)
+    N, n = values.shape[0], fr.n
+    d_x = torch.zeros((N, n), dtype=torch.float64, device="cuda")
+    d_st = torch.zeros((N, len(lanes.TS_FIELDS)), dtype=torch.int32, device="cuda")
+
+    def step():
+        torch.cuda.synchronize()
+        return ctx.tran_device(go, d_x.data_ptr(), d_st.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    ms, done, steps_acc, nr_iters = [], 0, 0, 0
+    ring_steps = max(1, args.steps // 2)
+    for _ in range(ring_steps):
+        flush.zero_()
+        ms.append(step())
+        st = d_st.cpu().numpy()
+        done += int((st[:, 0] == lanes.TRAN_DONE).sum())
+        steps_acc += int(st[:, 1].sum())
+        nr_iters += int(st[:, 3].sum())
+    dev_s = sum(ms) / 1e3
+    e2e_t, e2e_done = [], 0
+    for i in range(1 + ring_steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        ctx.set_lanes(slots, values)
+        _, _, _, sth, xh, _ = ctx.tran(go)
+        t2 = time.perf_counter()
+        if i >= 1:
+            e2e_t.append(t2 - t1)
+            e2e_done += int((sth[:, 0] == lanes.TRAN_DONE).sum())
+    e2e_s = sum(e2e_t)
+    dev_s, done = shard.reduce_run(dev_s, done)
+    e2e_s, e2e_done = shard.reduce_run(e2e_s, e2e_done)
+    if rank != 0:
+        ctx.close()
+        return None
+    hbm_peak, peak_src = load_peaks()
+    step_s = dev_s / ring_steps
     rec_bytes = lanes.record_size(fr) * 8
     hbm_bytes = N * (rec_bytes + 8 * n + 4 * len(lanes.TS_FIELDS))
     achieved = hbm_bytes / step_s / 1e9
-    alg = lane_major_bytes(fr, nr_iters / args.steps)
-    out = {
-        "metric": METRIC, "value": done / dev_s, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * step_s,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": cfg,
-        "e2e": {"value": e2e_done / e2e_s, "unit": UNIT,
-                "h2d_bytes_per_step": int(N * rec_bytes),
-                "d2h_bytes_per_step": int(N * n * 8 + N * 4 * len(lanes.TS_FIELDS))},
-        "gpu_launches": args.steps,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": TRAN_DRAM_BYTES_PER_LANE * N,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                       "tran_kernel launch on 148 ring lanes, scaled by lanes",
-                     "peak_source": peak_src,
-                     "note": "fused tran_kernel: unavoidable HBM bytes (records in, solution and "
-                             "step statistics out) per launch / device time; every lane's Newton "
-                             "working set stays in shared memory for its whole transient, so the "
-                             "kernel is bound by dependent shared-memory latency, not by HBM",
-                     "alg_bytes_lane_major_per_step": alg,
-                     "alg_equivalent_gbs": alg / step_s / 1e9},
-        "accepted_steps_per_point": steps_acc / max(1, args.steps * N),
-        "newton_iters_per_point": nr_iters / max(1, args.steps * N),
-        "clocks": clk.summary(), "wall_s_timed": wall,
-    }
-    out["dc_grid_diodes"] = dc_grid_diodes(args, local, flush)
-    out["dc_sweep_lanes"] = dc_sweep_lanes(args, local, flush)
-    out["ring_period_early_stop"] = ring_period_early_stop(args, local, flush)
-    if args.learned:
-        out["learned_mixed_c4"] = learned_mixed_c4(args, local, flush)
-        out["uneven_c3"] = uneven_c3(args, local, flush)
+    alg = lane_major_bytes(fr, nr_iters / ring_steps)
+    out = {"config": cfg, "value": done / dev_s, "unit": "points/s (a point = one lane's whole transient)",
+           "ms_per_step": 1e3 * step_s, "steps": ring_steps, "dtype": "f64",
+           "e2e": {"value": e2e_done / e2e_s, "h2d_bytes_per_step": int(values.nbytes),
+                   "d2h_bytes_per_step": int(N * n * 8 + N * 4 * len(lanes.TS_FIELDS))},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                        "frac": achieved / hbm_peak, "traffic": TRAN_DRAM_BYTES_PER_LANE * N,
+                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                          "tran_kernel launch on 148 ring lanes, scaled by lanes",
+                        "peak_source": peak_src,
+                        "note": "fused tran_kernel: unavoidable HBM bytes (records in, solution and step "
+                                "statistics out) per launch / device time; every lane's working set stays in "
+                                "shared memory for its whole transient (latency bound, not HBM bound)",
+                        "alg_bytes_lane_major_per_step": alg, "alg_equivalent_gbs": alg / step_s / 1e9},
+           "accepted_steps_per_point": steps_acc / max(1, ring_steps * N),
+           "newton_iters_per_point": nr_iters / max(1, ring_steps * N)}
     out["lu_roofline"] = lu_lanes_roofline(fr, ctx, hbm_peak, peak_src)
     out["lu_roofline_warp_per_lane"] = lu_replay_roofline(fr, ctx, hbm_peak, peak_src)
     if args.cpu_baseline:
         threads = os.cpu_count() or 1
         keep = {}
         d, dt = cpu_tran(fr, slots, values, threads, args.cpu_seconds, keep=keep)
-        out["cpu_baseline"] = {"value": d / dt, "unit": UNIT, "cores": threads, "kind": "port", "cpu": cpu_model(),
-                               "sample": f"{d} of the {N} lanes in {dt:.1f} s"}
+        out["cpu_baseline"] = {"value": d / dt, "unit": "points/s", "cores": threads, "kind": "port",
+                               "cpu": cpu_model(), "sample": f"{d} of the {N} lanes in {dt:.1f} s"}
         out["parity"] = parity_block(keep, sth, xh)
-    print(json.dumps(out), flush=True)
     ctx.close()
+    return out
+
+
+def our_arm(args, rank, world):
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    from espice_b200 import decks, lanes, learned, shard
+    fr, expand, p_test, nominal, cfg = c4_workload(seed=2 + 2 * rank, points=args.points)
+    opts = lanes.newton_opts(**TIGHT)
+    N, n = p_test.shape[0], fr.n
+    slots = expand.slots
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    setup = {}
+
+    # the nominal operating point (the plain path's start and the fallback's)
+    plain = lanes.DcLanes(fr, device=local)
+    plain.set_mode(precision=lanes.PREC_FP64, path=lanes.PATH_BLOCK)
+    plain.set_lanes(slots, expand(nominal))
+    x_nom = plain.solve(x0=None, opts=opts)[0][0]
+    # the network, trained on the GPU on other points' plain-solver solutions
+    t0 = time.perf_counter()
+    p_train, _ = decks.analog_block_params(seed=1 + 2 * rank, points=C4_TRAIN)
+    plain.set_lanes(slots, expand(p_train))
+    x_tr, _, st_tr, _ = plain.solve(x0=np.broadcast_to(x_nom, (C4_TRAIN, n)), opts=opts)
+    setup["training_solutions_s"] = time.perf_counter() - t0
+    ok = st_tr == lanes.LANE_CONVERGED
+    ws = learned.LearnedWarmStart(16, n, hidden=512, layers=3, device=local)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss = ws.fit(p_train[ok], x_tr[ok], epochs=60, batch=256, lr=2e-3, lr_end=2e-5)
+    torch.cuda.synchronize()
+    setup["training_60_epochs_s"] = time.perf_counter() - t0
+    vals = expand(p_test)
+    t0 = time.perf_counter()
+    plain.set_lanes(slots, vals)
+    setup["set_lanes_s"] = time.perf_counter() - t0
+    mixed = lanes.DcLanes(fr, device=local)
+    mixed.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK)
+    mixed.set_lanes(slots, vals)
+    fb = lanes.DcLanes(fr, device=local)
+    fb.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK)
+    d_x = torch.empty((N, n), dtype=torch.float64, device="cuda")
+    d_it = torch.zeros(N, dtype=torch.int32, device="cuda")
+    d_st = torch.zeros(N, dtype=torch.int32, device="cuda")
+    x_nom_d = torch.tensor(x_nom, device="cuda")
+    d_p = torch.tensor(p_test, dtype=torch.float32, device="cuda")
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ev0.record()
+        r = fn()
+        ev1.record()
+        ev1.synchronize()
+        return r, ev0.elapsed_time(ev1) / 1e3
+
+    def learned_step(stats):
+        return learned.solve(mixed, fb, ws, slots, vals, x_nom, k=8, opts=opts, d_values=d_p, stats_out=stats)
+
+    def plain_step():
+        d_x.copy_(x_nom_d.expand(N, n))
+        return plain.solve_device(d_x.data_ptr(), d_it.data_ptr(), d_st.data_ptr(), cold=False, opts=opts)
+
+    for _ in range(args.warmup):
+        timed(lambda: learned_step([]))
+        timed(plain_step)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    lt, lconv, lit, lfb, lstats = 0.0, 0, 0.0, 0, []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            st_list = []
+            (xl, it, conv, nfb), dt = timed(lambda: learned_step(st_list))
+            lt += dt
+            lconv += int(conv.sum())
+            lit += float(it.mean())
+            lfb += nfb
+            lstats.append(st_list)
+        x_learned = xl.cpu().numpy()
+        pt, pconv, pit, pstats = 0.0, 0, 0.0, []
+        for _ in range(args.steps):
+            sp, dt = timed(plain_step)
+            pt += dt
+            pconv += int((d_st == lanes.LANE_CONVERGED).sum())
+            pit += float(d_it.double().mean())
+            pstats.append(sp)
+    x_plain = d_x.cpu().numpy()
+    it_plain = d_it.cpu().numpy().astype(np.int64)
+    K = args.steps
+
+    # e2e through the public API with host buffers: the points' parameters
+    # in, every point's solution out
+    p_pin = torch.empty((N, p_test.shape[1]), dtype=torch.float32).pin_memory()
+    x_host = torch.empty((N, n), dtype=torch.float64).pin_memory()
+    d_p_e = torch.empty((N, p_test.shape[1]), dtype=torch.float32, device="cuda")
+    e2e_t, e2e_conv, e2e_fb, h2d, d2h = 0.0, 0, 0, 0, 0
+    for i in range(1 + K):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        vals_h = expand(p_test)
+        mixed.set_lanes(slots, vals_h)
+        p_pin.copy_(torch.from_numpy(p_test))
+        d_p_e.copy_(p_pin)
+        xl, it, conv, nfb = learned.solve(mixed, fb, ws, slots, vals_h, x_nom, k=8, opts=opts, d_values=d_p_e)
+        x_host.copy_(xl)
+        t2 = time.perf_counter()
+        if i >= 1:
+            e2e_t += t2 - t1
+            e2e_conv += int(conv.sum())
+            e2e_fb += nfb
+            h2d += vals_h.nbytes + p_pin.numel() * 4 + nfb * (vals_h.shape[1] + n) * 8
+            d2h += N * n * 8 + 2 * N * 4 + nfb * n * 8
+
+    # the mixed lanes' phase cycles (one untimed, profiled pass)
+    mixed.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK, profile=True)
+    prof_stats = []
+    learned_step(prof_stats)
+    prof = mixed.block_profile()
+    info = mixed.block_info()
+    mixed.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK)
+
+    lt, lconv = shard.reduce_run(lt, lconv)
+    pt, pconv = shard.reduce_run(pt, pconv)
+    e2e_t, e2e_conv = shard.reduce_run(e2e_t, e2e_conv)
+    ring = ring_transient(args, rank, world, local, flush) if args.side else None
+    if rank != 0:
+        for c in (plain, mixed, fb):
+            c.close()
+        ws.close()
+        return
+
+    hbm_peak, peak_src = load_peaks()
+    rec_bytes = lanes.record_size(fr) * 8
+    lane_bytes = rec_bytes + 16 * n + 32  # records in, start in, solution out, lane words
+    k_ms = lstats[-1][0]["kernel_ms"]
+    achieved = N * lane_bytes / (k_ms / 1e3) / 1e9
+    iters = max(prof["iterations"], 1)
+    ref_per_iter = prof_stats[0]["refinements"] / iters
+    rows_per_iter = info["a_rows"] + info["b_rows"] + ref_per_iter * (info["f_rows"] + info["b_rows"])
+    cyc = {k: prof[k] / iters for k in ("eval", "assemble", "refactor", "solve", "refine", "gates")}
+    launches = sum(sum(x["launches"] + 1 for x in st) for st in lstats) + K * 10
+    out = {
+        "metric": METRIC, "value": lconv / lt, "unit": UNIT, "n_gpus": world,
+        "steps": K, "warmup": args.warmup, "ms_per_step": 1e3 * lt / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+        "data": "synthetic", "config": cfg,
+        "e2e": {"value": e2e_conv / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(h2d / K),
+                "d2h_bytes_per_step": int(d2h / K)},
+        "gpu_launches": int(launches),
+        "plain_fp64": {"value": pconv / pt, "unit": UNIT, "ms_per_step": 1e3 * pt / K,
+                       "newton_iters_per_point": pit / K, "gpu_launches": int(sum(x["launches"] + 1 for x in pstats))},
+        "learned_mixed_over_plain": (lconv / lt) / (pconv / pt),
+        "newton_iters_per_point": lit / K, "fallback_points_per_step": lfb / K,
+        "e2e_fallback_points_per_step": e2e_fb / K,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": C4_BLOCK_DRAM_BYTES_PER_LANE and
+                     C4_BLOCK_DRAM_BYTES_PER_LANE * N,
+                     "kernel": "dc_block_kernel (mixed precision, BSIM3): the learned step's Newton launch",
+                     "kernel_ms": k_ms, "alg_bytes_per_lane": lane_bytes,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one mixed "
+                                       "dc_block_kernel launch on a reduced point count, scaled by points",
+                     "peak_source": peak_src,
+                     "note": "each lane's working set stays in its CTA's shared memory for the whole solve, so "
+                             "HBM carries only records, starts and solutions: the kernel is bound by the "
+                             "latency of its dependent program rows (the latency block)"},
+        "latency": {"cycles_per_newton_iter": {k: round(v) for k, v in cyc.items()},
+                    "rows_per_newton_iter": rows_per_iter,
+                    "refactor_cycles_per_row": cyc["refactor"] / info["a_rows"],
+                    "program_a": {"rows": info["a_rows"], "dependency_levels": info["a_levels"],
+                                  "ops": info["a_nops"], "levels_over_rows": info["a_levels"] / info["a_rows"]},
+                    "program_b_rows": info["b_rows"], "program_f_rows": info["f_rows"],
+                    "refinements_per_newton_iter": ref_per_iter,
+                    "ctas_per_sm": info["ctas_per_sm"], "lane_bytes": info["lane_bytes"],
+                    "note": "cycles of one CTA (one lane) per Newton iteration by phase, thread 0's clock64; "
+                            "rows are CTA-wide steps of the tape programs, each ending in a barrier; "
+                            "levels_over_rows: the dependency bound of program A over its scheduled rows"},
+        "setup": dict(setup, train_loss_first_last=[float(loss[0]), float(loss[-1])]),
+        "clocks": clk.summary(),
+    }
+    if args.cpu_baseline:
+        from oracle import oracle
+        oo = oracle.newton_opts(**TIGHT)
+        xo_nom, _, _ = oracle.dc_points(fr, slots, expand(nominal), warm=None, opts=oo)
+        threads = os.cpu_count() or 1
+        keep = {}
+        d, dt = cpu_dc(fr, slots, vals, xo_nom[0], oo, threads, args.cpu_seconds, keep=keep)
+        out["cpu_baseline"] = {"value": d / dt, "unit": UNIT, "cores": threads, "kind": "port", "cpu": cpu_model(),
+                               "sample": f"the first {len(keep)} of the {N} points in {dt:.1f} s, plain FP64 "
+                                         "Newton from the nominal operating point, one point per thread"}
+        idx = np.array(sorted(keep), dtype=np.int64)
+        xo = np.stack([keep[i][0] for i in idx])
+        ito = np.array([keep[i][1] for i in idx])
+        cvo = np.array([keep[i][2] for i in idx])
+        dp = _dev(x_plain[idx][cvo], xo[cvo])
+        dl = _dev(x_learned[idx][cvo], xo[cvo])
+        out["parity"] = {
+            "points": int(len(idx)), "oracle_converged": int(cvo.sum()),
+            "plain_fp64": {"bitwise_equal": int((x_plain[idx].view(np.uint64) == xo.view(np.uint64)).all(1).sum()),
+                           "iterations_equal": int((it_plain[idx] == ito).sum()), "max_rel_dev": dp[0]},
+            "learned_mixed": {"max_rel_dev": dl[0], "within_1e-9_rel_or_1e-12_abs": dl[1]},
+            "checked": "every point the CPU baseline solved: the plain FP64 lanes' solution bitwise and their "
+                       "Newton iteration count against the oracle's; the learned + mixed lanes' solution within "
+                       "1e-9 relative or 1e-12 absolute of it"}
+    out["learned_vs_plain_points_all"] = dict(zip(("max_rel_dev", "within_1e-9"), _dev(x_learned, x_plain)))
+    for c in (plain, mixed, fb):
+        c.close()
+    ws.close()
+    if args.side:
+        out["ring_transient"] = ring
+        out["dc_grid_diodes"] = dc_grid_diodes(args, local, flush)
+        out["dc_sweep_lanes"] = dc_sweep_lanes(args, local, flush)
+        out["ring_period_early_stop"] = ring_period_early_stop(args, local, flush)
+        out["uneven_c3"] = uneven_c3(args, local, flush)
+    print(json.dumps(out), flush=True)
+
+
 
 
 def main():
@@ -786,7 +924,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     # a reduced case for profiler captures (the benchmark itself uses the defaults)
     ap.add_argument("--lanes", type=int, default=RING_LANES)
-    ap.add_argument("--no-learned", dest="learned", action="store_false")
+    ap.add_argument("--points", type=int, default=C4_POINTS)
+    ap.add_argument("--no-side", dest="side", action="store_false")
     ap.add_argument("--t-stop", type=float, default=None)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

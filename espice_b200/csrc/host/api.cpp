@@ -890,12 +890,14 @@ int32_t ensure_block(esl_ctx* ctx) {
 
 // The op ring a block-lane CTA streams its programs through: kDepth + 1
 // slots of one op word per thread (block.cu OpFormat).
-uint32_t block_ring_bytes(uint32_t op_bytes) { return (op_bytes == 8 ? 17u : 9u) * kBlockThreads * op_bytes; }
+uint32_t block_ring_bytes(uint32_t op_bytes) { return 5u * kBlockThreads * op_bytes; }
 
-// A block lane's working set (block.cu carves the same): x, xo, rhs, diag,
-// dx (FP64, n each), staging, limited images, the FP64 matrix (mixed form),
-// the value space (nv values, FP64 or FP32), each 16-byte aligned.
-void block_layout(const TopoDev& T, uint32_t nv, bool mixed, BlockDev& D) {
+// A block lane's working set (block.cu carves the same): the hot part x,
+// rhs, diag, dx (FP64, n each), limited images, the FP64 matrix (mixed
+// form), the value space (nv values, FP64 or FP32); the cold part xo and
+// the staging cells; each 16-byte aligned. split: the cold part's offsets
+// start again from 0 (it lives in the CTA's slab).
+void block_layout(const TopoDev& T, uint32_t nv, bool mixed, bool split, BlockDev& D) {
   size_t at = 0;
   auto take = [&at](size_t bytes) {
     const size_t o = at;
@@ -903,15 +905,19 @@ void block_layout(const TopoDev& T, uint32_t nv, bool mixed, BlockDev& D) {
     return uint32_t(o);
   };
   D.o_x = take(8 * size_t(T.n));
-  D.o_xo = take(8 * size_t(T.n));
   D.o_rhs = take(8 * size_t(T.n));
   D.o_diag = take(8 * size_t(T.n));
   D.o_dx = take(8 * size_t(T.n));
-  D.o_st = take(8 * size_t(T.n_stage));
   D.o_lim = take(8 * size_t(std::max<uint32_t>(T.nlim, 1)));
   D.o_a64 = take(mixed ? 8 * size_t(T.nnz) : 0);
   D.o_v = take(size_t(mixed ? 4 : 8) * nv);
-  D.lane_bytes = uint32_t(at);
+  const size_t hot = at;
+  if (split) at = 0;
+  D.o_xo = take(8 * size_t(T.n));
+  D.o_st = take(8 * size_t(T.n_stage));
+  D.split = split ? 1u : 0u;
+  D.lane_bytes = uint32_t(split ? hot : at);
+  D.cold_bytes = uint32_t(split ? at : 0);
 }
 
 // Shared memory a block lane may take (a CTA's 227 KB, less the static
@@ -937,13 +943,26 @@ int32_t block_view(esl_ctx* ctx, bool mixed, uint32_t n_lanes, BlockDev& D) {
   D.g_cells = ctx->d_bg_cells.as<uint4>();
   D.g_len = ctx->block_g_len;
   D.g_ncells = ctx->block_g_ncells;
-  block_layout(T, T.nv, mixed, D);
-  D.in_smem = D.lane_bytes + D.ring_bytes <= kBlockSmemRoom;
-  const int per_sm = block_occupancy(mixed, D.op_bytes == 16, topo_has_b3(T),
-                                     (D.in_smem ? D.lane_bytes : 0) + D.ring_bytes);
-  const uint32_t cap = uint32_t(ctx->sms) * uint32_t(std::max(per_sm, 1));
+  // The placement with the most CTAs an SM: the whole working set in shared
+  // memory, its hot part there (the cold part in the slab), or all of it in
+  // the slab; on a tie, the most in shared memory.
+  const bool long_ops = D.op_bytes == 16, b3 = topo_has_b3(T);
+  int best = -1;
+  uint32_t place = 2;
+  for (uint32_t p = 0; p < 3; ++p) {
+    block_layout(T, T.nv, mixed, p == 1, D);
+    if (p < 2 && D.lane_bytes + D.ring_bytes > kBlockSmemRoom) continue;
+    const int per_sm = block_occupancy(mixed, long_ops, b3, (p < 2 ? D.lane_bytes : 0) + D.ring_bytes);
+    if (per_sm > best) {
+      best = per_sm;
+      place = p;
+    }
+  }
+  block_layout(T, T.nv, mixed, place == 1, D);
+  D.in_smem = place < 2;
+  const uint32_t cap = uint32_t(ctx->sms) * uint32_t(std::max(best, 1));
   D.grid = std::max<uint32_t>(1, std::min(n_lanes, cap));
-  ESL_CUDA(ctx->d_slab.ensure(size_t(D.in_smem ? 1 : D.grid) * D.lane_bytes));
+  ESL_CUDA(ctx->d_slab.ensure(size_t(D.in_smem && !D.split ? 1 : D.grid) * (D.split ? D.cold_bytes : D.lane_bytes)));
   D.slab = ctx->d_slab.as<unsigned char>();
   D.refine_tol = ctx->refine_tol;
   D.refine_max = ctx->refine_max;
@@ -973,7 +992,7 @@ cudaError_t lead_jacobian(esl_ctx* ctx, const LaneDev& L, double* out) {
   if (smem <= size_t(227) * 1024) return launch_assemble(T, L, 0, out, ctx->stream);
   BlockDev D{};
   D.T = T;
-  block_layout(T, 0, false, D);
+  block_layout(T, 0, false, false, D);
   cudaError_t e = ctx->d_slab.ensure(D.lane_bytes);
   if (e != cudaSuccess) return e;
   D.slab = ctx->d_slab.as<unsigned char>();
@@ -1591,7 +1610,7 @@ int32_t esl_tran_meas_device(esl_ctx* ctx, const esl_tran_opts* opts, const esl_
   if (n_meas > kMaxMeas) return ctx->fail(ESL_INVALID_ARGUMENT, "at most 32 measure cards");
   for (uint32_t c = 0; c < n_meas; ++c) {
     const esl_measure& m = meas[c];
-    if (m.kind > ESL_MEAS_PP) return ctx->fail(ESL_INVALID_ARGUMENT, "unknown measure kind");
+    if (m.kind > ESL_MEAS_DERIV) return ctx->fail(ESL_INVALID_ARGUMENT, "unknown measure kind");
     if (m.a.unknown >= ctx->pat.n || (m.kind == ESL_MEAS_TRIG_TARG && m.b.unknown >= ctx->pat.n))
       return ctx->fail(ESL_INVALID_ARGUMENT, "measure probe out of range");
   }
@@ -1704,9 +1723,12 @@ int32_t group_block(esl_ctx* const* ctxs, uint32_t n_ctx, const esl_newton_opts*
   const uint32_t ring = block_ring_bytes(long_ops ? 16 : 8);
   std::vector<BlockDev> Dg = Ds;
   for (uint32_t c = 0; c < n_ctx; ++c) {
-    Dg[c].in_smem = Dg[c].lane_bytes + ring <= kGroupSmemRoom;
+    // each topology keeps its own placement (block_view's), the whole
+    // working set in the CTA's slab when its shared part misses the room
+    Dg[c].in_smem = Dg[c].in_smem && Dg[c].lane_bytes + ring <= kGroupSmemRoom;
+    if (!Dg[c].in_smem && Dg[c].split) block_layout(ctxs[c]->topo, ctxs[c]->topo.nv, mixed, false, Dg[c]);
     if (Dg[c].in_smem) smem = std::max<size_t>(smem, Dg[c].lane_bytes);
-    else stride = std::max<size_t>(stride, Dg[c].lane_bytes);
+    stride = std::max<size_t>(stride, Dg[c].split ? Dg[c].cold_bytes : Dg[c].in_smem ? 0 : Dg[c].lane_bytes);
   }
   const uint32_t ring_at = uint32_t((smem + 15) & ~size_t(15));
   smem = ring_at + ring;
@@ -1900,6 +1922,8 @@ int32_t esl_block_info(esl_ctx* ctx, esl_block_info_t* info) {
     info->ctas_per_sm[m] = uint32_t(std::max(
         0, block_occupancy(m == 1, D.op_bytes == 16, topo_has_b3(ctx->topo),
                            (D.in_smem ? D.lane_bytes : 0) + D.ring_bytes)));
+    info->split[m] = D.split;
+    info->cold_bytes[m] = D.cold_bytes;
   }
   return ESL_OK;
 }

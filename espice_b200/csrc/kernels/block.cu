@@ -6,16 +6,19 @@
 // programs are rows of one op per thread (a CTA barrier between rows), and
 // reductions run across the CTA. Nothing per topology is staged: the
 // programs (L2-resident, shared by every lane of the topology) stream in,
-// each thread copying its own op words 16 rows ahead (8 for 16-byte ops)
+// each thread copying its own op words 4 rows ahead
 // into a private ring in shared memory with cp.async, and the assembly is a
 // per-thread stream of staging indices read eight terms ahead, so neither
 // waits on an L2 round trip per row or per term.
 //
-// Where the working set lives: x | xo | rhs | diag | dx | staging | limited
-// images | (mixed: the FP64 matrix) | v = [tape values | y | 0.0 | 1.0 |
-// sink], in the CTA's shared memory when it fits, else in a per-CTA slab of
-// global memory (L2-resident for the lane's solve; one CTA writes and reads
-// it, ordered by its barriers).
+// Where the working set lives: x | rhs | diag | dx | limited images |
+// (mixed: the FP64 matrix) | v = [tape values | y | 0.0 | 1.0 | sink] |
+// xo | staging, in the CTA's shared memory when it fits; or its hot part
+// (up to v) there and xo and the staging cells (written once and read once
+// an iteration, by the evaluation and the assembly) in a per-CTA slab of
+// global memory, when that lets more CTAs share an SM; else all of it in
+// the slab (L2-resident for the lane's solve; one CTA writes and reads it,
+// ordered by its barriers).
 //
 // Two precisions. FP64: the refactor and solves are bitwise the CPU replay
 // (sparse_lu.zig refactor + solve), as the warp programs are. Mixed: the
@@ -116,19 +119,20 @@ __device__ __forceinline__ bool run_op(const uint4& op, V* v) {
 
 // Op words: 8 bytes {dst | kind << 28, a | b << 16} when the value space
 // has 16-bit indices, 16 bytes {dst | kind << 28, a, b, 0} otherwise. A
-// thread's ring holds kDepth + 1 op words (16 + 1 short or 8 + 1 long: about
-// 34 or 36 KB a CTA): kDepth rows in flight, and the slot being refilled is
+// thread's ring holds kDepth + 1 op words (10 or 20 KB a CTA): kDepth rows
+// in flight (about 1,500 cycles ahead, past an L2 round trip), and the slot
+// being refilled is
 // never the one being read.
 template <typename OpT>
 struct OpFormat;
 template <>
 struct OpFormat<uint2> {
-  static constexpr uint32_t kDepth = 16;
+  static constexpr uint32_t kDepth = 4;
   __device__ static uint4 decode(uint2 o) { return make_uint4(o.x, o.y & 0xffffu, o.y >> 16, 0u); }
 };
 template <>
 struct OpFormat<uint4> {
-  static constexpr uint32_t kDepth = 8;
+  static constexpr uint32_t kDepth = 4;
   __device__ static uint4 decode(uint4 o) { return o; }
 };
 
@@ -191,16 +195,19 @@ struct BlockMem {
   uint32_t ring;  // this thread's op ring (shared address of its slot 0)
 };
 
+// base: the working set (its hot part when split); cold: the CTA's slab
+// for a split layout's cold part.
 template <typename V>
-__device__ __forceinline__ BlockMem<V> block_carve(const BlockDev& D, unsigned char* base, unsigned char* ring = nullptr,
-                                                  uint32_t op_bytes = 8) {
+__device__ __forceinline__ BlockMem<V> block_carve(const BlockDev& D, unsigned char* base, unsigned char* cold,
+                                                  unsigned char* ring = nullptr, uint32_t op_bytes = 8) {
   BlockMem<V> b;
+  unsigned char* cbase = D.split ? cold : base;
   b.m.base = reinterpret_cast<double*>(base);
   b.m.x = reinterpret_cast<double*>(base + D.o_x);
-  b.m.xo = reinterpret_cast<double*>(base + D.o_xo);
+  b.m.xo = reinterpret_cast<double*>(cbase + D.o_xo);
   b.m.rhs = reinterpret_cast<double*>(base + D.o_rhs);
   b.m.diag = reinterpret_cast<double*>(base + D.o_diag);
-  b.m.st = reinterpret_cast<double*>(base + D.o_st);
+  b.m.st = reinterpret_cast<double*>(cbase + D.o_st);
   b.m.lim = reinterpret_cast<double*>(base + D.o_lim);
   b.m.v = nullptr;
   b.m.y = nullptr;
@@ -351,7 +358,7 @@ __device__ __forceinline__ void phase_mark(unsigned long long* prof, uint32_t ph
 // dc_solve_lane step for step, reductions across the CTA.
 template <typename V, typename OpT, bool kHasB3, uint32_t kW>
 __device__ void block_lane(const BlockDev& D, const LaneDev& L, const LaneOpts& o, unsigned char* base,
-                           unsigned char* ring, uint64_t* red, uint32_t lane) {
+                           unsigned char* cold, unsigned char* ring, uint64_t* red, uint32_t lane) {
   constexpr bool kMixed = sizeof(V) == 4;
   const TopoDev& T = D.T;
   const int tid = threadIdx.x;
@@ -360,7 +367,7 @@ __device__ void block_lane(const BlockDev& D, const LaneDev& L, const LaneOpts& 
   if (!(status == kRunning || resuming)) return;
 
   const uint32_t n = T.n;
-  const BlockMem<V> b = block_carve<V>(D, base, ring, sizeof(OpT));
+  const BlockMem<V> b = block_carve<V>(D, base, cold, ring, sizeof(OpT));
   const LaneMem& m = b.m;
   const double* rec = L.rec + size_t(lane) * T.rec_size;
   for (uint32_t i = tid; i < n; i += kW) m.x[i] = L.x[size_t(lane) * n + i];
@@ -511,16 +518,20 @@ __device__ void block_lane(const BlockDev& D, const LaneDev& L, const LaneOpts& 
 }
 
 // Persistent grid: each CTA takes lanes blockIdx.x, + gridDim.x, ...; its
-// working set in dynamic shared memory or in its slab of D.slab.
-// Dynamic shared memory: the working set (when in_smem), then the op ring.
+// working set in dynamic shared memory, split between shared memory and its
+// slab of D.slab, or all in its slab. Dynamic shared memory: the working set
+// (its hot part when split; nothing when all in the slab), then the op ring.
+// Two CTAs an SM by registers (the BSIM3 instantiation spills a few words
+// of its evaluation for it), as many as shared memory then allows.
 template <typename V, typename OpT, bool kHasB3, uint32_t kW>
-__global__ void __launch_bounds__(kW) dc_block_kernel(BlockDev D, LaneDev L, LaneOpts o) {
+__global__ void __launch_bounds__(kW, 2) dc_block_kernel(BlockDev D, LaneDev L, LaneOpts o) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint64_t red[kW / 32];
-  unsigned char* base = D.in_smem ? smem_raw : D.slab + size_t(blockIdx.x) * D.lane_bytes;
+  unsigned char* own = D.slab + size_t(blockIdx.x) * (D.split ? D.cold_bytes : D.lane_bytes);
+  unsigned char* base = D.in_smem ? smem_raw : own;
   unsigned char* ring = smem_raw + (D.in_smem ? D.lane_bytes : 0u);
   for (uint32_t lane = blockIdx.x; lane < L.n_lanes; lane += gridDim.x) {
-    block_lane<V, OpT, kHasB3, kW>(D, L, o, base, ring, red, lane);
+    block_lane<V, OpT, kHasB3, kW>(D, L, o, base, own, ring, red, lane);
     __syncthreads();
   }
 }
@@ -533,7 +544,7 @@ __global__ void __launch_bounds__(kW) dc_block_kernel(BlockDev D, LaneDev L, Lan
 // its working set in dynamic shared memory (when the topology's fits) or in
 // the CTA's slab. Every topology of a group runs in one precision and width.
 template <typename V, typename OpT, bool kHasB3, uint32_t kW>
-__global__ void __launch_bounds__(kW) dc_block_group_kernel(const BlockDev* __restrict__ Ds,
+__global__ void __launch_bounds__(kW, 2) dc_block_group_kernel(const BlockDev* __restrict__ Ds,
                                                             const LaneDev* __restrict__ Ls, const uint2* items,
                                                             uint32_t n_items, uint32_t* next, LaneOpts o,
                                                             unsigned char* slab, size_t slab_stride,
@@ -555,7 +566,8 @@ __global__ void __launch_bounds__(kW) dc_block_group_kernel(const BlockDev* __re
       L = Ls[w.x];
     }
     __syncthreads();
-    block_lane<V, OpT, kHasB3, kW>(D, L, o, D.in_smem ? smem_raw : own_slab, smem_raw + ring_at, red, w.y);
+    block_lane<V, OpT, kHasB3, kW>(D, L, o, D.in_smem ? smem_raw : own_slab, own_slab, smem_raw + ring_at, red,
+                                   w.y);
     __syncthreads();
   }
 }
@@ -589,7 +601,7 @@ template <bool kHasB3, uint32_t kW>
 __global__ void __launch_bounds__(kW) block_lead_kernel(BlockDev D, LaneDev L, uint32_t lane, double* out) {
   const TopoDev& T = D.T;
   const int tid = threadIdx.x;
-  const BlockMem<double> b = block_carve<double>(D, D.slab);
+  const BlockMem<double> b = block_carve<double>(D, D.slab, D.slab);
   for (uint32_t i = tid; i < T.n; i += kW) b.m.x[i] = L.x[size_t(lane) * T.n + i];
   for (uint32_t i = tid; i < T.nlim; i += kW) b.m.lim[i] = L.lim[size_t(lane) * T.nlim + i];
   SimDev sim;

@@ -40,14 +40,18 @@ struct BlockDev {
   const uint32_t* g_terms;
   const uint4* g_cells;
   uint32_t g_len, g_ncells;
-  // A lane's working set, byte offsets from its base: x, xo, rhs, diag, dx
-  // (FP64, n each), staging cells, limited images, the FP64 matrix (mixed
-  // form: nnz), the value space v (FP64, or FP32 in the mixed form).
+  // A lane's working set, byte offsets: the hot part x, rhs, diag, dx (FP64,
+  // n each), limited images, the FP64 matrix (mixed form: nnz), the value
+  // space v (FP64, or FP32 in the mixed form); then the cold part xo (n) and
+  // the staging cells. Split: the cold part lives apart, in the CTA's slab
+  // (its offsets from there), so that more CTAs fit an SM's shared memory.
   uint32_t o_x, o_xo, o_rhs, o_diag, o_dx, o_st, o_lim, o_a64, o_v;
-  uint32_t lane_bytes;  // the whole working set, 16-byte aligned
-  uint32_t in_smem;     // 1: in the CTA's shared memory; 0: in its slab of `slab`
+  uint32_t lane_bytes;  // the working set (split: its hot part), 16-byte aligned
+  uint32_t in_smem;     // 1: (the hot part) in the CTA's shared memory; 0: all in its slab of `slab`
+  uint32_t split;       // 1: the cold part in the CTA's slab, cold_bytes each
+  uint32_t cold_bytes;
   uint32_t grid;        // CTAs of a launch (persistent)
-  unsigned char* slab;  // grid x lane_bytes of global memory (and the lead assembly's scratch)
+  unsigned char* slab;  // per CTA: the working set (in_smem 0) or its cold part (split), and the lead assembly's scratch
   // Mixed form: refinement stops at max |res| <= refine_tol * max |rhs| or
   // after refine_max corrections; refine_out [lane] accumulates them.
   double refine_tol;

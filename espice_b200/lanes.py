@@ -83,7 +83,8 @@ class BlockInfo(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint32) for k in ("width", "a_rows", "b_rows", "f_rows", "a_levels", "a_nops",
                                                  "b_nops", "ntv", "warp_ok")] + \
                [("lane_bytes", ctypes.c_uint32 * 2), ("in_smem", ctypes.c_uint32 * 2),
-                ("ctas_per_sm", ctypes.c_uint32 * 2)]
+                ("ctas_per_sm", ctypes.c_uint32 * 2), ("split", ctypes.c_uint32 * 2),
+                ("cold_bytes", ctypes.c_uint32 * 2)]
 
 
 class TranOpts(ctypes.Structure):
@@ -113,11 +114,12 @@ class MeasClause(ctypes.Structure):
 
 
 class Measure(ctypes.Structure):
-    """esl_measure: MEAS_WHEN (a), MEAS_TRIG_TARG (a = TRIG, b = TARG) or MEAS_FIND_AT (a)."""
+    """esl_measure: MEAS_TRIG_TARG (a = TRIG, b = TARG), else clause a alone."""
     _fields_ = [("kind", ctypes.c_uint32), ("pad", ctypes.c_uint32), ("a", MeasClause), ("b", MeasClause)]
 
 
 MEAS_WHEN, MEAS_TRIG_TARG, MEAS_FIND_AT, MEAS_MIN, MEAS_MAX, MEAS_AVG, MEAS_PP = 0, 1, 2, 3, 4, 5, 6
+MEAS_INTEG, MEAS_RMS, MEAS_DERIV = 7, 8, 9
 MEAS_UNSET, MEAS_LAST = -1, -2
 
 
@@ -138,8 +140,13 @@ def find_at(unknown, at):
     return Measure(MEAS_FIND_AT, 0, meas_clause(unknown, at=at), meas_clause(0))
 
 
+def deriv_at(unknown, at):
+    """DERIV .. AT=: the slope of the first segment holding AT."""
+    return Measure(MEAS_DERIV, 0, meas_clause(unknown, at=at), meas_clause(0))
+
+
 def window(kind, unknown, from_=0.0, to=0.0):
-    """MIN, MAX, AVG or PP (MEAS_*) of `unknown` over FROM..TO (TO 0: to the end)."""
+    """MIN, MAX, AVG, PP, INTEG or RMS (MEAS_*) of `unknown` over FROM..TO (TO 0: to the end)."""
     return Measure(kind, 0, meas_clause(unknown, from_=from_, to=to), meas_clause(0))
 
 
@@ -208,7 +215,7 @@ def lib():
     return _lib
 
 
-RECORD_FIELDS = {0: 1, 1: 1, 2: 138, 3: 138, 4: 15, 5: 33}
+RECORD_FIELDS = {0: 1, 1: 1, 2: 138, 3: 138, 4: 15, 5: 33, 6: 88}
 
 
 def record_size(frozen: Frozen) -> int:
@@ -356,7 +363,7 @@ class DcLanes:
         info = BlockInfo()
         self._check(self._L.esl_block_info(self._ctx, ctypes.byref(info)), "esl_block_info")
         out = {k: getattr(info, k) for k, _ in info._fields_[:9]}
-        for k in ("lane_bytes", "in_smem", "ctas_per_sm"):
+        for k in ("lane_bytes", "in_smem", "ctas_per_sm", "split", "cold_bytes"):
             out[k] = list(getattr(info, k))
         return out
 

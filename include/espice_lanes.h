@@ -282,13 +282,19 @@ int32_t esl_tran_device(esl_ctx *ctx, const esl_tran_opts *opts, double *d_x, ui
  * targ - trig (each clause with its own TD); FIND .. AT=: the value at a
  * time; MIN, MAX, AVG (trapezoidal mean) and PP of clause a's unknown over
  * its FROM..TO window (the samples inside it, ends not interpolated; MIN
- * and MAX read 0 when no sample falls inside, as the reference's do). A
+ * and MAX read 0 when no sample falls inside, as the reference's do);
+ * INTEG and RMS of clause a's unknown over FROM..TO with interpolated ends,
+ * by Simpson's 3/8 rule, Simpson's rule or the trapezoid panel by panel as
+ * the sample spacing allows (measure.zig Integ, ngspice
+ * measure_rms_integral); DERIV .. AT=: the slope of the first segment
+ * holding AT (measure.zig At with slope). A
  * clause: the probed unknown, the level VAL, RISE/FALL/CROSS counts
  * (ESL_MEAS_UNSET, ESL_MEAS_LAST or k >= 1), TD, FROM, TO (0: none), AT. An
  * event is counted from the clause's second sample and its time is the
  * level crossing interpolated on the last segment, as ngspice does. */
 enum { ESL_MEAS_WHEN = 0, ESL_MEAS_TRIG_TARG = 1, ESL_MEAS_FIND_AT = 2,
-       ESL_MEAS_MIN = 3, ESL_MEAS_MAX = 4, ESL_MEAS_AVG = 5, ESL_MEAS_PP = 6 };
+       ESL_MEAS_MIN = 3, ESL_MEAS_MAX = 4, ESL_MEAS_AVG = 5, ESL_MEAS_PP = 6,
+       ESL_MEAS_INTEG = 7, ESL_MEAS_RMS = 8, ESL_MEAS_DERIV = 9 };
 enum { ESL_MEAS_UNSET = -1, ESL_MEAS_LAST = -2 };
 typedef struct {
     uint32_t unknown;
@@ -345,10 +351,12 @@ int32_t esl_set_mode(esl_ctx *ctx, const esl_solve_mode *mode);
  * its first solve): rows of `width` ops in programs A (refactor + forward
  * solve, a_levels its longest dependence chain), B and F; the tape's
  * values and ops; per precision (0 FP64, 1 mixed) a lane's working-set
- * bytes, whether it sits in shared memory, and CTAs per SM. */
+ * bytes in shared memory (all of it, or its hot part when split), whether
+ * it sits in shared memory, CTAs per SM, and whether it is split (its
+ * previous iterate and staging cells, cold_bytes, in global memory). */
 typedef struct {
     uint32_t width, a_rows, b_rows, f_rows, a_levels, a_nops, b_nops, ntv, warp_ok;
-    uint32_t lane_bytes[2], in_smem[2], ctas_per_sm[2];
+    uint32_t lane_bytes[2], in_smem[2], ctas_per_sm[2], split[2], cold_bytes[2];
 } esl_block_info_t;
 int32_t esl_block_info(esl_ctx *ctx, esl_block_info_t *info);
 
