@@ -110,7 +110,8 @@ enum SweepStatus : uint32_t {
 };
 // Streamed measure cards and clause counts (esl_measure).
 enum MeasKind : uint32_t {
-  kMeasWhen = 0, kMeasTrigTarg = 1, kMeasFindAt = 2, kMeasMin = 3, kMeasMax = 4, kMeasAvg = 5, kMeasPp = 6
+  kMeasWhen = 0, kMeasTrigTarg = 1, kMeasFindAt = 2, kMeasMin = 3, kMeasMax = 4, kMeasAvg = 5, kMeasPp = 6,
+  kMeasInteg = 7, kMeasRms = 8, kMeasDeriv = 9
 };
 constexpr int32_t kMeasUnset = -1;
 constexpr int32_t kMeasLast = -2;

@@ -112,6 +112,16 @@ struct CrossDev {
   int32_t pad;
 };
 constexpr uint32_t kMeasDoubles = 2 * sizeof(CrossDev) / sizeof(double);
+// INTEG and RMS (measure.zig Integ) in the same card state: the window's
+// points not folded into a panel yet, the three rules' sums, the last raw
+// sample and the window's ends.
+struct IntegDev {
+  double p[4][2];
+  double sum[3];
+  double px, py, first_x, cut_x;
+  uint32_t rows, np, count, inside, cut, over;
+};
+static_assert(sizeof(IntegDev) <= 2 * sizeof(CrossDev), "a card's state holds INTEG");
 
 struct TranDev {
   double t_stop, t_step, dt_max, dt_min;

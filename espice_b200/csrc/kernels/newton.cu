@@ -1337,6 +1337,14 @@ __device__ void meas_start(const MeasDev& mc, CrossDev* x) {
       s.td = 0.0;   // its span
     }
   }
+  if (mc.kind == kMeasInteg || mc.kind == kMeasRms) {
+    IntegDev& g = *reinterpret_cast<IntegDev*>(x);
+    for (int j = 0; j < 4; ++j) g.p[j][0] = g.p[j][1] = 0.0;
+    g.sum[0] = g.sum[1] = g.sum[2] = 0.0;
+    g.px = g.py = 0.0;
+    g.first_x = g.cut_x = CUDART_NAN;
+    g.rows = g.np = g.count = g.inside = g.cut = g.over = 0;
+  }
 }
 
 // Extremum.feed (measure.zig:1401-1449, not DC): op 0 MIN, 1 MAX (the last
@@ -1442,9 +1450,123 @@ __device__ bool at_feed(CrossDev& s, const MeasClauseDev& c, double xv, double v
   return false;
 }
 
+// At.feed with slope (DERIV .. AT=): the slope of the first segment
+// holding AT.
+__device__ bool slope_feed(CrossDev& s, const MeasClauseDev& c, double xv, double v) {
+  if (s.over) return true;
+  if (s.first > 0 && s.prev_x <= c.at && xv >= c.at) {
+    s.hit = div_rn(v - s.prev, xv - s.prev_x);
+    s.found = 1;
+    s.over = 1;
+    return true;
+  }
+  s.first += 1;
+  s.prev_x = xv;
+  s.prev = v;
+  return false;
+}
+
+// almostEqualUlps (measure.zig:1699-1708): within 100 units in the last
+// place, on the doubles' order-preserving integer images.
+__device__ __forceinline__ bool almost_equal_ulps(double a, double b) {
+  if (a == b) return true;
+  long long ia = __double_as_longlong(a), ib = __double_as_longlong(b);
+  if (ia < 0) ia = (long long)(0x8000000000000000ull - (unsigned long long)ia);
+  if (ib < 0) ib = (long long)(0x8000000000000000ull - (unsigned long long)ib);
+  const unsigned long long d = (unsigned long long)ia - (unsigned long long)ib;
+  const unsigned long long mag = (long long)d < 0 ? 0ull - d : d;
+  return mag <= 100ull;
+}
+
+// measure.zig line (:1257-1261).
+__device__ __forceinline__ double line_at(double x0, double y0, double x1, double y1, double at) {
+  const double slope = div_rn(y1 - y0, x1 - x0);
+  const double intercept = y0 - slope * x0;
+  return slope * at + intercept;
+}
+
+// Integ.panel (measure.zig:1568-1586): folds the oldest points into one
+// panel by Simpson's 3/8 rule, Simpson's rule or the trapezoid, as the next
+// spacings agree; `avail` of p are points, the rest read zero.
+__device__ void integ_panel(IntegDev& s, uint32_t avail) {
+  double p[4][2];
+  for (uint32_t j = 0; j < 4; ++j) {
+    p[j][0] = j < avail ? s.p[j][0] : 0.0;
+    p[j][1] = j < avail ? s.p[j][1] : 0.0;
+  }
+  double w[3];
+  for (uint32_t j = 0; j < 3; ++j) w[j] = j + 1 < avail ? p[j + 1][0] - p[j][0] : 0.0;
+  uint32_t used;
+  if (almost_equal_ulps(w[0], w[1]) && almost_equal_ulps(w[0], w[2])) {
+    s.sum[0] = s.sum[0] + div_rn(3.0 * w[0] * (p[0][1] + 3.0 * (p[1][1] + p[2][1]) + p[3][1]), 8.0);
+    used = 3;
+  } else if (almost_equal_ulps(w[0], w[1])) {
+    s.sum[1] = s.sum[1] + div_rn(w[0] * (p[0][1] + 4.0 * p[1][1] + p[2][1]), 3.0);
+    used = 2;
+  } else {
+    s.sum[2] = s.sum[2] + div_rn(w[0] * (p[0][1] + p[1][1]), 2.0);
+    used = 1;
+  }
+  s.np = avail > used ? avail - used : 0u;
+  for (uint32_t j = 0; j < s.np; ++j) {
+    s.p[j][0] = p[avail - s.np + j][0];
+    s.p[j][1] = p[avail - s.np + j][1];
+  }
+}
+
+// Integ.feed (measure.zig:1538-1563): the window's points from the first
+// sample at or past FROM (read as the value at a nonzero FROM) to the first
+// past a nonzero TO (read as the value at TO); true once past TO.
+__device__ bool integ_feed(IntegDev& s, const MeasClauseDev& c, bool rms, double xv, double v) {
+  if (s.over) return true;
+  bool ret = false;
+  if (s.inside || !(xv < c.from)) {
+    s.inside = 1;
+    s.cut = c.to != 0.0 && xv > c.to;
+    double p0 = xv, p1 = v;
+    if (s.cut) {
+      if (s.rows > 0 && !almost_equal_ulps(xv, c.to)) {
+        p0 = c.to;
+        p1 = line_at(s.px, s.py, xv, v, c.to);
+      }
+    } else if (s.count == 0 && c.from != 0.0 && s.rows > 0 && !almost_equal_ulps(xv, c.from)) {
+      p0 = c.from;
+      p1 = line_at(s.px, s.py, xv, v, c.from);
+    }
+    if (rms) p1 = p1 * p1;
+    if (s.count == 0) s.first_x = p0;
+    if (s.cut) s.cut_x = p0;
+    s.count += 1;
+    s.p[s.np][0] = p0;
+    s.p[s.np][1] = p1;
+    s.np += 1;
+    if (s.np == 4) integ_panel(s, s.np);
+    ret = s.cut != 0;
+    if (ret) s.over = 1;
+  }
+  s.rows += 1;
+  s.px = xv;
+  s.py = v;
+  return ret;
+}
+
+// Integ.result (measure.zig:1588-1595): the integral, or the RMS over the
+// window's span.
+__device__ double integ_result(IntegDev s, bool rms) {
+  if (s.rows == 0) return CUDART_NAN;
+  while (s.np > 1) integ_panel(s, s.np);
+  const double from = s.count > (s.cut ? 1u : 0u) ? s.first_x : CUDART_NAN;
+  const double to = s.cut ? s.cut_x : s.px;
+  const double total = s.sum[0] + s.sum[1] + s.sum[2];
+  return rms ? sqrt(div_rn(total, to - from)) : total;
+}
+
 // Feeds the row (t, x) to card c; true once the card has resolved.
 __device__ bool meas_feed(const MeasDev& mc, CrossDev* x, double t, const double* xs) {
   if (mc.kind == kMeasFindAt) return at_feed(x[0], mc.a, t, xs[mc.a.unknown]);
+  if (mc.kind == kMeasDeriv) return slope_feed(x[0], mc.a, t, xs[mc.a.unknown]);
+  if (mc.kind == kMeasInteg || mc.kind == kMeasRms)
+    return integ_feed(*reinterpret_cast<IntegDev*>(x), mc.a, mc.kind == kMeasRms, t, xs[mc.a.unknown]);
   if (mc.kind == kMeasMin || mc.kind == kMeasMax || mc.kind == kMeasAvg)
     return ext_feed(x[0], mc.a, int(mc.kind - kMeasMin), t, xs[mc.a.unknown]);
   if (mc.kind == kMeasPp) {
@@ -1463,8 +1585,10 @@ __device__ bool meas_feed(const MeasDev& mc, CrossDev* x, double t, const double
 // MIN/MAX the extreme, AVG the trapezoidal mean, PP max - min.
 __device__ double meas_value(const MeasDev& mc, const CrossDev* x) {
   double v;
-  if (mc.kind == kMeasFindAt) {
+  if (mc.kind == kMeasFindAt || mc.kind == kMeasDeriv) {
     v = x[0].found ? x[0].hit : CUDART_NAN;
+  } else if (mc.kind == kMeasInteg || mc.kind == kMeasRms) {
+    v = integ_result(*reinterpret_cast<const IntegDev*>(x), mc.kind == kMeasRms);
   } else if (mc.kind == kMeasMin || mc.kind == kMeasMax) {
     v = x[0].hit;  // 0 when no sample fell in the window
   } else if (mc.kind == kMeasAvg) {

@@ -232,7 +232,8 @@ enum {
  * VAL, RISE/FALL/CROSS counts (ORC_MEAS_UNSET, ORC_MEAS_LAST or k >= 1),
  * TD, FROM, TO (0: none) and AT. */
 enum { ORC_MEAS_WHEN = 0, ORC_MEAS_TRIG_TARG = 1, ORC_MEAS_FIND_AT = 2,
-       ORC_MEAS_MIN = 3, ORC_MEAS_MAX = 4, ORC_MEAS_AVG = 5, ORC_MEAS_PP = 6 };
+       ORC_MEAS_MIN = 3, ORC_MEAS_MAX = 4, ORC_MEAS_AVG = 5, ORC_MEAS_PP = 6,
+       ORC_MEAS_INTEG = 7, ORC_MEAS_RMS = 8, ORC_MEAS_DERIV = 9 };
 enum { ORC_MEAS_UNSET = -1, ORC_MEAS_LAST = -2 };
 typedef struct {
     uint32_t unknown;

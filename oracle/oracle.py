@@ -238,6 +238,7 @@ class Measure(ctypes.Structure):
 
 
 MEAS_WHEN, MEAS_TRIG_TARG, MEAS_FIND_AT, MEAS_MIN, MEAS_MAX, MEAS_AVG, MEAS_PP = 0, 1, 2, 3, 4, 5, 6
+MEAS_INTEG, MEAS_RMS, MEAS_DERIV = 7, 8, 9
 MEAS_UNSET, MEAS_LAST = -1, -2
 TRAN_RESOLVED = 5
 

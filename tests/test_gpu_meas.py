@@ -40,14 +40,17 @@ def _cards(fr, mod):
         mod.Measure(mod.MEAS_MIN, 0, mod.meas_clause(s5, from_=0.5e-9, to=2.5e-9), mod.meas_clause(0)),
         mod.Measure(mod.MEAS_AVG, 0, mod.meas_clause(s0, from_=1e-9), mod.meas_clause(0)),
         mod.Measure(mod.MEAS_PP, 0, mod.meas_clause(s5, from_=1e-9), mod.meas_clause(0)),
+        mod.Measure(mod.MEAS_INTEG, 0, mod.meas_clause(s0, from_=0.3e-9, to=2.2e-9), mod.meas_clause(0)),
+        mod.Measure(mod.MEAS_RMS, 0, mod.meas_clause(s5, from_=0.5e-9), mod.meas_clause(0)),
+        mod.Measure(mod.MEAS_DERIV, 0, mod.meas_clause(s0, at=1.1e-9), mod.meas_clause(0)),
     ]
 
 
 @pytest.mark.parametrize("early", [False, True])
 def test_ring_measures_match_oracle(early):
     """24 ring-oscillator samples over 3 ns: a period, a stage delay, a
-    delayed fall, a LAST crossing, a FIND, a windowed rise, and MAX, MIN,
-    AVG and PP over windows."""
+    delayed fall, a LAST crossing, a FIND, a windowed rise, MAX, MIN, AVG
+    and PP over windows, a windowed INTEGRAL, an RMS and a DERIVATIVE."""
     fr, slots, values = decks.ring_oscillator(lanes=24)
     go = lanes.tran_opts(3e-9, decks.RING_T_STEP, decks.RING_T_MAX, max_steps=200_000)
     oo = oracle.tran_opts(3e-9, decks.RING_T_STEP, decks.RING_T_MAX, max_steps=200_000)
@@ -111,3 +114,38 @@ def test_golden_measures_as_gpu_lanes(name):
     values = {m["name"]: float(vg[0, k]) for k, m in enumerate(deck.measures)}
     for nm, worst in gu.score_meas(g, values):
         assert worst <= 1.0, f"{name} {nm}: {worst:.3g}x the fixture tolerance"
+
+
+def test_integral_rms_derivative_on_rc_lanes():
+    """16 RC charging lanes (R from 0.5 to 2 kohm, 1 nF, a 1 V step; the
+    reference's hspice/meas_forms deck without its E source): INTEGRAL over
+    0..5 us and over the whole run, DERIVATIVE at 1 us, RMS over 1..2 us,
+    against the oracle."""
+    from espice_b200.circuit import Circuit
+    c = Circuit()
+    c.V("v1", "in", "0", pulse=[0.0, 1.0, 0.0, 1e-12, 1e-12, 1.0, 2.0])
+    c.R("r1", "in", "out", 1e3)
+    c.C("c1", "out", "0", 1e-9)
+    fr = c.freeze()
+    out = fr.unknown("v(out)")
+    slots = [fr.slot("r1", "r")]
+    values = np.linspace(500.0, 2000.0, 16).reshape(-1, 1)
+
+    def cards(mod):
+        cl = mod.meas_clause
+        return [mod.Measure(mod.MEAS_INTEG, 0, cl(out, from_=0.0, to=5e-6), cl(0)),
+                mod.Measure(mod.MEAS_INTEG, 0, cl(out), cl(0)),
+                mod.Measure(mod.MEAS_DERIV, 0, cl(out, at=1e-6), cl(0)),
+                mod.Measure(mod.MEAS_RMS, 0, cl(out, from_=1e-6, to=2e-6), cl(0))]
+
+    go = lanes.tran_opts(5e-6, 10e-9, 0.0, max_steps=200_000)
+    oo = oracle.tran_opts(5e-6, 10e-9, 0.0, max_steps=200_000)
+    ctx = lanes.DcLanes(fr)
+    ctx.set_lanes(slots, values)
+    vg, sg, _, _ = ctx.tran_meas(go, cards(lanes))
+    ctx.close()
+    vo, so, _ = oracle.tran_meas(fr, slots, values, oo, cards(oracle))
+    assert np.array_equal(sg, so)
+    same = _same(vg, vo)
+    assert same.all(), (vg[~same], vo[~same])
+    assert np.isfinite(vg).all()
