@@ -256,6 +256,8 @@ struct esl_ctx {
   DevBuf d_q_ptr, d_q_src, d_c_ptr, d_c_src, d_probes, d_tran_t, d_tran_v, d_tran_n, d_tran_stats;
   DevBuf d_amap, d_fill, d_prog, d_l_scaled, d_pinv, d_q, d_seq, d_sweep_values, d_meas, d_next_lane;
   DevBuf d_sweep_state, d_sweep_rows;  // paused sweep lanes' state
+  DevBuf d_tran_state, d_tran_save;    // paused transient lanes' state
+  esl_stats last_peels{};              // the last call's peel counts (esl_peel_stats)
   uint32_t n_seq_a = 0, n_seq = 0, seq_warps = 0;  // lane-interleaved op list
   uint32_t n_seq_f = 0, mixed_warps = 0;            // its forward-only tail, the mixed kernel's warps
   LuJitKernels lu_jit;                               // the tape-compiled lane LU of the current tape
@@ -1496,6 +1498,48 @@ int32_t tran_view(esl_ctx* ctx, const esl_tran_opts* o, TranDev& P, LaneOpts& lo
 
 }  // namespace
 
+}  // extern "C"
+
+namespace {
+
+// One transient launch over every lane, then the host factors of the lanes
+// that paused (serve_pauses) and resume launches until none pauses.
+int32_t run_tran(esl_ctx* ctx, LaneDev L, TranDev P, const LaneOpts& lo, uint32_t lpb) {
+  cudaStream_t s = ctx->stream;
+  const uint32_t N = ctx->n_lanes;
+  const size_t bd = size_t(ctx->topo.tran_doubles) + size_t(kMeasDoubles) * P.n_meas + kTranSaveRegs;
+  ESL_CUDA(ctx->d_tran_state.ensure(size_t(N) * kTranStateN * 4));
+  ESL_CUDA(ctx->d_tran_save.ensure(size_t(N) * bd * 8));
+  P.tstate = ctx->d_tran_state.as<uint32_t>();
+  P.tsave = ctx->d_tran_save.as<double>();
+  ESL_CUDA(cudaMemsetAsync(L.status, 0, size_t(N) * 4, s));
+  ESL_CUDA(cudaMemsetAsync(L.flags, 0, size_t(N) * 4, s));
+  ESL_CUDA(cudaMemsetAsync(L.n_paused, 0, 4, s));
+  ctx->peel.clear();
+  std::memset(&ctx->last_peels, 0, sizeof(ctx->last_peels));
+  ESL_CUDA(ctx->d_next_lane.ensure(sizeof(uint32_t)));
+  P.next_lane = ctx->d_next_lane.as<uint32_t>();
+  ESL_CUDA(cudaEventRecord(ctx->ev0, s));
+  ESL_CUDA(launch_tran(ctx->topo, L, P, lo, lpb, s));
+  ctx->last_peels.launches = 1;
+  for (;;) {
+    bool any = false;
+    if (int32_t rc = serve_pauses(ctx, L, &ctx->last_peels, &any)) return rc;
+    if (!any) break;
+    LaneDev R = L;
+    R.resume = 1;
+    ESL_CUDA(launch_tran(ctx->topo, R, P, lo, lpb, s));
+    ++ctx->last_peels.launches;
+  }
+  ESL_CUDA(cudaEventRecord(ctx->ev1, s));
+  ESL_CUDA(cudaEventSynchronize(ctx->ev1));
+  return ESL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int32_t esl_tran_device(esl_ctx* ctx, const esl_tran_opts* opts, double* d_x, uint32_t* d_stats,
                         const uint32_t* d_probes, uint32_t n_probes, uint32_t max_pts, double* d_t,
                         double* d_v, uint32_t* d_n_pts, float* ms) {
@@ -1517,13 +1561,7 @@ int32_t esl_tran_device(esl_ctx* ctx, const esl_tran_opts* opts, double* d_x, ui
   P.n_pts = max_pts ? d_n_pts : nullptr;
   LaneDev L = lane_view(ctx, 0);
   L.x = d_x;
-  cudaStream_t s = ctx->stream;
-  ESL_CUDA(ctx->d_next_lane.ensure(sizeof(uint32_t)));
-  P.next_lane = ctx->d_next_lane.as<uint32_t>();
-  ESL_CUDA(cudaEventRecord(ctx->ev0, s));
-  ESL_CUDA(launch_tran(ctx->topo, L, P, lo, lanes_per_cta(ctx, ctx->n_lanes, ctx->tran_lanes_eff), s));
-  ESL_CUDA(cudaEventRecord(ctx->ev1, s));
-  ESL_CUDA(cudaEventSynchronize(ctx->ev1));
+  if (int32_t rc = run_tran(ctx, L, P, lo, lanes_per_cta(ctx, ctx->n_lanes, ctx->tran_lanes_eff))) return rc;
   if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
   return ESL_OK;
 }
@@ -1585,14 +1623,17 @@ int32_t esl_dc_sweep_device(esl_ctx* ctx, const esl_slot* slot, const double* va
   P.next_lane = ctx->d_next_lane.as<uint32_t>();
   const uint32_t lpb = lanes_per_cta(ctx, N, fit);
   ESL_CUDA(cudaEventRecord(ctx->ev0, s));
+  std::memset(&ctx->last_peels, 0, sizeof(ctx->last_peels));
   ESL_CUDA(launch_sweep(T, L, P, o, lpb, s));
+  ctx->last_peels.launches = 1;
   for (;;) {
     bool any = false;
-    if (int32_t rc = serve_pauses(ctx, L, nullptr, &any)) return rc;
+    if (int32_t rc = serve_pauses(ctx, L, &ctx->last_peels, &any)) return rc;
     if (!any) break;
     LaneDev R = L;
     R.resume = 1;
     ESL_CUDA(launch_sweep(T, R, P, o, lpb, s));
+    ++ctx->last_peels.launches;
   }
   ESL_CUDA(cudaEventRecord(ctx->ev1, s));
   ESL_CUDA(cudaEventSynchronize(ctx->ev1));
@@ -1634,12 +1675,7 @@ int32_t esl_tran_meas_device(esl_ctx* ctx, const esl_tran_opts* opts, const esl_
   P.meas_out = d_values;
   LaneDev L = lane_view(ctx, 0);
   L.x = d_x;
-  ESL_CUDA(ctx->d_next_lane.ensure(sizeof(uint32_t)));
-  P.next_lane = ctx->d_next_lane.as<uint32_t>();
-  ESL_CUDA(cudaEventRecord(ctx->ev0, s));
-  ESL_CUDA(launch_tran(T, L, P, lo, lanes_per_cta(ctx, ctx->n_lanes, fit), s));
-  ESL_CUDA(cudaEventRecord(ctx->ev1, s));
-  ESL_CUDA(cudaEventSynchronize(ctx->ev1));
+  if (int32_t rc = run_tran(ctx, L, P, lo, lanes_per_cta(ctx, ctx->n_lanes, fit))) return rc;
   if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
   return ESL_OK;
 }
@@ -1892,6 +1928,14 @@ int32_t esl_set_mode(esl_ctx* ctx, const esl_solve_mode* mode) {
   return ESL_OK;
 }
 
+int32_t esl_peel_counts(const esl_ctx* ctx, uint32_t* lanes, uint32_t* host_solves, uint32_t* launches) {
+  if (!ctx) return ESL_INVALID_ARGUMENT;
+  if (lanes) *lanes = ctx->last_peels.peeled;
+  if (host_solves) *host_solves = ctx->last_peels.host_solves;
+  if (launches) *launches = ctx->last_peels.launches;
+  return ESL_OK;
+}
+
 int32_t esl_block_profile(esl_ctx* ctx, uint64_t* cycles) {
   if (!ctx || !cycles) return ESL_INVALID_ARGUMENT;
   if (!ctx->profile || !ctx->d_prof.p) return ctx->fail(ESL_INVALID_ARGUMENT, "no profiled block-lane solve yet");
@@ -1924,6 +1968,8 @@ int32_t esl_block_info(esl_ctx* ctx, esl_block_info_t* info) {
                            (D.in_smem ? D.lane_bytes : 0) + D.ring_bytes)));
     info->split[m] = D.split;
     info->cold_bytes[m] = D.cold_bytes;
+    info->gather_terms = D.g_len;
+    info->gather_cells = D.g_ncells;
   }
   return ESL_OK;
 }

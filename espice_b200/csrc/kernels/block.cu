@@ -226,9 +226,10 @@ __device__ __forceinline__ BlockMem<V> block_carve(const BlockDev& D, unsigned c
 // kGTermEnd closes a cell, whose destinations come from the thread's cell
 // stream (D.g_cells[c * kW + t]): a pattern slot (its tape value, FP32 in the
 // mixed form which also keeps the FP64 sum, and the diagonal copy for the
-// gates) or a residual row (rhs and y = P(-rhs)). Terms and cells arrive
-// eight terms and two cells ahead. gmin > 0 adds loadExtras' diagonal and
-// residual terms. Fill-in tape values are zeroed.
+// gates) or a residual row (rhs and y = P(-rhs)). Term words arrive two
+// batches of eight ahead, staging values one batch ahead, cells two ahead.
+// gmin > 0 adds loadExtras' diagonal and residual terms. Fill-in tape
+// values are zeroed.
 template <typename V, uint32_t kW>
 __device__ __forceinline__ double gather_term(const BlockMem<V>& b, uint32_t w) {
   const uint32_t src = w & ~kGTermEnd;
@@ -260,21 +261,33 @@ __device__ void block_assemble(const BlockDev& D, const BlockMem<V>& b, double g
   const uint32_t* terms = D.g_terms + tid;
   const uint4* cells = D.g_cells + tid;
   const uint32_t K = D.g_len;
-  uint32_t w[8];
+  // Term words two batches ahead and staging values one batch ahead: every
+  // load of a batch is issued before the stores of the batch before it, so
+  // none waits behind them (the staging cells are only read here).
+  uint32_t w[8], nx[8];
+  double val[8];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) w[j] = uint32_t(j) < K ? __ldg(terms + size_t(j) * kW) : kGSrcZero;
+  for (int j = 0; j < 8; ++j) {
+    w[j] = uint32_t(j) < K ? __ldg(terms + size_t(j) * kW) : kGSrcZero;
+    nx[j] = uint32_t(8 + j) < K ? __ldg(terms + size_t(8 + j) * kW) : kGSrcZero;
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) val[j] = gather_term<V, kW>(b, w[j]);
   const uint4 none = make_uint4(0u, 0u, 0u, 0u);
   uint4 cell = D.g_ncells > 0 ? __ldg(cells) : none;
   uint4 cell1 = D.g_ncells > 1 ? __ldg(cells + kW) : none;
   uint32_t c_next = 2;
   double s = 0.0;
   for (uint32_t k0 = 0; k0 < K; k0 += 8) {
-    uint32_t nx[8];
+    uint32_t nnx[8];
+    double nv[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) nx[j] = k0 + 8 + j < K ? __ldg(terms + size_t(k0 + 8 + j) * kW) : kGSrcZero;
+    for (int j = 0; j < 8; ++j) nnx[j] = k0 + 16 + j < K ? __ldg(terms + size_t(k0 + 16 + j) * kW) : kGSrcZero;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) nv[j] = gather_term<V, kW>(b, nx[j]);
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      s = __dadd_rn(s, gather_term<V, kW>(b, w[j]));
+      s = __dadd_rn(s, val[j]);
       if (w[j] & kGTermEnd) {
         gather_store<V, kW>(D, b, cell, s, gmin);
         s = 0.0;
@@ -284,7 +297,11 @@ __device__ void block_assemble(const BlockDev& D, const BlockMem<V>& b, double g
       }
     }
 #pragma unroll
-    for (int j = 0; j < 8; ++j) w[j] = nx[j];
+    for (int j = 0; j < 8; ++j) {
+      w[j] = nx[j];
+      nx[j] = nnx[j];
+      val[j] = nv[j];
+    }
   }
   for (uint32_t j = tid; j < T.n_fill; j += kW) b.v[T.fill[j]] = V(0);
 }

@@ -137,7 +137,28 @@ struct TranDev {
   uint32_t n_meas, early_stop;
   double* meas_out;        // [lane][n_meas] card values (NaN: unresolved)
   uint32_t* next_lane;     // the lane-refill counter, zero at launch
+  // A lane paused for a host factor (LaneDev's pause protocol): its state
+  // words [lane][kTranStateN] and its shared memory and double state
+  // [lane][tran_doubles + kMeasDoubles n_meas + kTranSaveRegs].
+  uint32_t* tstate;
+  double* tsave;
 };
+// A paused transient lane's state words.
+enum TranStateWord : uint32_t {
+  kTrPhase = 0,      // 1 paused in the operating point, 2 in a step
+  kTrIter = 1,       // the Newton iteration it paused in
+  kTrInitFix = 2,
+  kTrOrder = 3,
+  kTrSteps = 4,
+  kTrHaveBp = 5,
+  kTrBpClamped = 6,
+  kTrHb = 7,         // the charge rings' base slot
+  kTrNRec = 8,       // rows recorded
+  kTrLimActive = 9,
+  kTrStat = 10,      // kTsN step statistics
+  kTranStateN = 10 + kTsN
+};
+constexpr uint32_t kTranSaveRegs = 10;  // t, dt, the breakpoint and its saved step, six past steps
 
 // Sequential .dc sweeps, one per lane (dc.zig Sweep): the swept source
 // (its index among the V and I sources' cached values) takes values[pt] at

@@ -1606,9 +1606,33 @@ __device__ double meas_value(const MeasDev& mc, const CrossDev* x) {
 
 }  // namespace
 
+// A paused transient lane's matrix for the host factor: every pattern slot's
+// G from the staging cells, plus ag0 C on the slots with capacitance cells
+// (the same sums in the same order as the assembly and the companion
+// gather, so the same bits as the lane's own assembled matrix).
+__device__ void gather_pattern_tran(const TopoDev& T, const LaneMem& m, double ag0, bool dynamic, double* out,
+                                    int tid) {
+  for (uint32_t p = tid; p < T.nnz; p += 32) {
+    double g = 0.0;
+    for (uint32_t e = T.a_ptr[p]; e < T.a_ptr[p + 1]; ++e) {
+      const uint32_t src = T.a_src[e];
+      g = __dadd_rn(g, src == kSrcOne ? 1.0 : src == kSrcX0 ? m.x[0] : m.st[src]);
+    }
+    if (dynamic && T.c_ptr[p + 1] != T.c_ptr[p]) {
+      double c = 0.0;
+      for (uint32_t e = T.c_ptr[p]; e < T.c_ptr[p + 1]; ++e) c = __dadd_rn(c, m.st[T.c_src[e]]);
+      g = __dadd_rn(g, __dmul_rn(ag0, c));
+    }
+    out[p] = g;
+  }
+}
+
 template <bool kHasB3>
 __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, const LaneOpts& o, uint32_t prog,
                           double* block, uint32_t lane, int tid) {
+  const uint32_t lstat = L.status[lane];
+  const bool resuming = L.resume && (lstat == kNeedSolve || lstat == kSingular);
+  if (!(lstat == kRunning || resuming)) return;
   const uint32_t n = T.n, nq = T.n_qt;
   LaneMem m = carve(T, block);
   double* cur = block + T.smem_doubles;
@@ -1622,144 +1646,241 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
   // past the lane's tran_doubles: kMeasDoubles per measure card
   CrossDev* mstate = reinterpret_cast<CrossDev*>(block + T.tran_doubles) + 2 * tid;
   const bool card = P.meas && uint32_t(tid) < P.n_meas;
-  if (card) meas_start(P.meas[tid], mstate);
+  const uint32_t bd = T.tran_doubles + kMeasDoubles * P.n_meas;  // the lane's shared-memory doubles
+  uint32_t* ts = P.tstate + size_t(lane) * kTranStateN;
+  double* sv = P.tsave + size_t(lane) * (size_t(bd) + kTranSaveRegs);
   const double* rec = L.rec + size_t(lane) * T.rec_size;
+  const size_t at = size_t(lane) * n;
   uint32_t stat[kTsN];
   for (int k = 0; k < kTsN; ++k) stat[k] = 0;
-  init_consts(T, m.v, tid);
 
-  // operating point: cold start with the junction seeds, MODEINITFIX; the
-  // source waves at t = 0 (kind 2: vsource.va:214-219)
+  // The run's state outside shared memory (saved with it on a pause).
+  const double dt_max = P.dt_max;
+  const double delmin = 1e-11 * dt_max;
+  const double min_break = 10.0 * delmin;
+  double dt = 0.0, t = 0.0, bp_next = 0.0, bp_save_dt = div_rn(P.t_stop, 50.0);
+  double dt_old[6];
+  for (int k = 0; k < 6; ++k) dt_old[k] = dt_max;
+  int order = 1;
+  uint32_t steps = 0, hb = 0, n_rec = 0;
+  bool have_bp = false, bp_clamped = false, lim_active = false;
+  NewtonCarry carry{0u, kXPlausible, 0u, 0u, (L.flags[lane] & 2u) ? 1u : 0u};
+  uint32_t phase0 = 0;  // 0 a fresh lane, 1 resumed in the operating point, 2 in a step
+
   SimDev sim;
   sim.t = 0.0;
   sim.src_scale = 1.0;
   sim.kind = 2;
-  for (uint32_t i = tid; i < n; i += 32) m.x[i] = 0.0;
-  for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
-    const BatchDev& B = T.b[bi];
-    for (uint32_t i = tid; i < B.count; i += 32) {
-      if (B.type == kD) m.lim[B.lim_off + i] = rec[B.rec_off + kDVcrit * B.count + i];
-      if (B.type == kM) {
-        m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kMSeedVgs * B.count + i];
-        m.lim[B.lim_off + 3 * i + 1] = 0.0;
-        m.lim[B.lim_off + 3 * i + 2] = -1.0;
-      }
-      if (B.type == kB3) {
-        m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kB3SeedVgs * B.count + i];
-        m.lim[B.lim_off + 3 * i + 1] = 0.1;
-        m.lim[B.lim_off + 3 * i + 2] = 0.0;
-      }
-    }
+  if (resuming) {
+    for (uint32_t i = tid; i < bd; i += 32) block[i] = sv[i];
+    phase0 = ts[kTrPhase];
+    carry.iter = ts[kTrIter];
+    carry.init_fix = ts[kTrInitFix];
+    carry.limit = L.limit[lane];
+    carry.resume = lstat == kSingular ? 2u : 1u;
+    order = int(ts[kTrOrder]);
+    steps = ts[kTrSteps];
+    have_bp = ts[kTrHaveBp] != 0;
+    bp_clamped = ts[kTrBpClamped] != 0;
+    hb = ts[kTrHb];
+    n_rec = ts[kTrNRec];
+    lim_active = ts[kTrLimActive] != 0;
+    for (int k = 0; k < kTsN; ++k) stat[k] = ts[kTrStat + k];
+    const double* r = sv + bd;
+    t = r[0];
+    dt = r[1];
+    bp_next = r[2];
+    bp_save_dt = r[3];
+    for (int k = 0; k < 6; ++k) dt_old[k] = r[4 + k];
+    __syncwarp();
+    // the host's step for the iteration the lane paused in
+    if (carry.resume == 1)
+      for (uint32_t j = tid; j < n; j += 32) m.y[j] = L.dx[at + T.qcol[j]];
+  } else {
+    if (card) meas_start(P.meas[tid], mstate);
+    init_consts(T, m.v, tid);
   }
-  __syncwarp();
-  bool lim_active = T.nlim != 0;
-  LaneOpts op = o;
-  op.residual_tol = 1e-9;
-  op.gmin = 0.0;
-  op.max_iter = 100;
-  uint32_t it = 0;
-  fill_sources(T, rec, sim, vsrc, tid);
-  int rc = lane_newton<kHasB3>(T, prog, m, rec, op, sim, nullptr, lim_active, true, it, vsrc, tid);
-  lim_active = false;
-  stat[kTsOpIters] = it;
-  uint32_t n_rec = 0;
+  // Pause: the host factors this lane's matrix (G, plus ag0 C in a step)
+  // with the lane's own direct solver; the resume launch restores the
+  // lane's shared memory and state and continues the Newton solve with the
+  // host's step (lane_solver.zig's per-lane peel).
+  auto pause = [&](uint32_t phase, double ag0) {
+    gather_pattern_tran(T, m, ag0, phase == 2, L.a_vals + size_t(lane) * T.nnz, tid);
+    for (uint32_t i = tid; i < n; i += 32) {
+      L.x[at + i] = m.x[i];
+      L.rhs[at + i] = m.rhs[i];
+      L.diag[at + i] = m.diag[i];
+    }
+    __syncwarp();
+    for (uint32_t i = tid; i < bd; i += 32) sv[i] = block[i];
+    if (tid == 0) {
+      double* r = sv + bd;
+      r[0] = t;
+      r[1] = dt;
+      r[2] = bp_next;
+      r[3] = bp_save_dt;
+      for (int k = 0; k < 6; ++k) r[4 + k] = dt_old[k];
+      ts[kTrPhase] = phase;
+      ts[kTrIter] = carry.iter;
+      ts[kTrInitFix] = carry.init_fix;
+      ts[kTrOrder] = uint32_t(order);
+      ts[kTrSteps] = steps;
+      ts[kTrHaveBp] = have_bp;
+      ts[kTrBpClamped] = bp_clamped;
+      ts[kTrHb] = hb;
+      ts[kTrNRec] = n_rec;
+      ts[kTrLimActive] = lim_active;
+      for (int k = 0; k < kTsN; ++k) ts[kTrStat + k] = stat[k];
+      L.limit[lane] = carry.limit;
+      L.flags[lane] |= 2u;
+      // the lane's first factor of all is its own fresh factor; a later
+      // one continues the lead tape's history
+      L.iters[lane] = (phase == 1 && carry.iter == 0) ? 0u : 1u;
+      L.status[lane] = kNeedSolve;
+      atomicAdd(L.n_paused, 1u);
+    }
+  };
   // Records the row (t, m.x) and feeds it to the measure cards; true while
   // a card is still open.
-  auto record = [&](double t) {
+  auto record = [&](double tr) {
     bool open = false;
     if (P.meas) {
-      const bool done = card ? meas_feed(P.meas[tid], mstate, t, m.x) : true;
+      const bool done = card ? meas_feed(P.meas[tid], mstate, tr, m.x) : true;
       open = __any_sync(kFull, !done);
     }
     if (P.out_t && n_rec < P.max_pts) {
-      if (tid == 0) P.out_t[size_t(lane) * P.max_pts + n_rec] = t;
+      if (tid == 0) P.out_t[size_t(lane) * P.max_pts + n_rec] = tr;
       for (uint32_t k = tid; k < P.n_probes; k += 32)
         P.out_v[(size_t(lane) * P.max_pts + n_rec) * P.n_probes + k] = m.x[P.probes[k]];
       ++n_rec;
     }
     return open;
   };
-  if (rc != 0) {
-    stat[kTsStatus] = rc == 2 ? kTranLeftTape : kTranOpFailed;
-  } else {
-    for (uint32_t i = tid; i < n; i += 32) {
-      cur[i] = m.x[i];
-      prev[i] = m.x[i];
-    }
-    // charge histories, flat at q(x_op); no dynamic current yet
-    sim.kind = 1;
-    eval_all<kHasB3>(T, rec, m, false, sim, tid, true);
-    __syncwarp();
-    for (uint32_t i = tid; i < 4 * n; i += 32) qh[i] = 0.0;
-    __syncwarp();
-    row_charges(T, prog, m, qh + n, tid);
-    state_charges(T, rec, m.x, qt + nq, tid);
-    __syncwarp();
-    for (uint32_t i = tid; i < n; i += 32) {
-      qh[2 * n + i] = qh[n + i];
-      qh[3 * n + i] = qh[n + i];
-      ipr[i] = 0.0;
-    }
-    for (uint32_t j = tid; j < nq; j += 32) {
-      qt[2 * nq + j] = qt[nq + j];
-      qt[3 * nq + j] = qt[nq + j];
-      ipt[j] = 0.0;
-    }
-    __syncwarp();
-    const bool has_charge = T.q_ptr[n] != 0 || T.c_ptr[T.nnz] != 0;
-    uint32_t hb = 0;  // ring slot r lives at (hb + r) & 3
-    auto slot = [&](double* base, uint32_t len, uint32_t r) { return base + size_t((hb + r) & 3u) * len; };
 
-    pulse_timers(T, rec, tmr, tid);
-    const double dt_max = P.dt_max;
-    const double delmin = 1e-11 * dt_max;
-    const double min_break = 10.0 * delmin;
-    double dt = fmin(div_rn(fmin(P.t_step, div_rn(P.t_stop, 100.0)), 10.0), dt_max);
-    double bp0;
-    if (next_bp(T, rec, tmr, min_break, bp0)) dt = fmin(dt, 0.1 * bp0);
-    dt = div_rn(dt, 10.0);
-    double dt_old[6];
-    for (int k = 0; k < 6; ++k) dt_old[k] = dt_max;
-    double t = 0.0;
-    int order = 1;
-    uint32_t steps = 0;
-    bool have_bp = false, bp_clamped = false;
-    double bp_next = 0.0, bp_save_dt = div_rn(P.t_stop, 50.0);
-    record(0.0);
+  // operating point: cold start with the junction seeds, MODEINITFIX; the
+  // source waves at t = 0 (kind 2: vsource.va:214-219)
+  int rc = 0;
+  if (phase0 != 2) {
+    if (phase0 == 0) {
+      for (uint32_t i = tid; i < n; i += 32) m.x[i] = 0.0;
+      for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
+        const BatchDev& B = T.b[bi];
+        for (uint32_t i = tid; i < B.count; i += 32) {
+          if (B.type == kD) m.lim[B.lim_off + i] = rec[B.rec_off + kDVcrit * B.count + i];
+          if (B.type == kM) {
+            m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kMSeedVgs * B.count + i];
+            m.lim[B.lim_off + 3 * i + 1] = 0.0;
+            m.lim[B.lim_off + 3 * i + 2] = -1.0;
+          }
+          if (B.type == kB3) {
+            m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kB3SeedVgs * B.count + i];
+            m.lim[B.lim_off + 3 * i + 1] = 0.1;
+            m.lim[B.lim_off + 3 * i + 2] = 0.0;
+          }
+        }
+      }
+      __syncwarp();
+      lim_active = T.nlim != 0;
+      carry.init_fix = 1;
+    }
+    LaneOpts op = o;
+    op.residual_tol = 1e-9;
+    op.gmin = 0.0;
+    op.max_iter = 100;
+    uint32_t it = 0;
+    fill_sources(T, rec, sim, vsrc, tid);
+    rc = lane_newton<kHasB3>(T, prog, m, rec, op, sim, nullptr, lim_active, carry.init_fix != 0, it, vsrc, tid,
+                             &carry);
+    if (rc == 3) {
+      pause(1, 0.0);
+      return;
+    }
+    carry.resume = 0;
+    lim_active = false;
+    stat[kTsOpIters] = it;
+  }
+  if (rc != 0) {
+    stat[kTsStatus] = kTranOpFailed;
+  } else {
+    const bool has_charge = T.q_ptr[n] != 0 || T.c_ptr[T.nnz] != 0;
+    auto slot = [&](double* base, uint32_t len, uint32_t r) { return base + size_t((hb + r) & 3u) * len; };
+    if (phase0 != 2) {
+      // the operating point converged here (fresh, or resumed in it): the
+      // run's start
+      for (uint32_t i = tid; i < n; i += 32) {
+        cur[i] = m.x[i];
+        prev[i] = m.x[i];
+      }
+      // charge histories, flat at q(x_op); no dynamic current yet
+      sim.kind = 1;
+      eval_all<kHasB3>(T, rec, m, false, sim, tid, true);
+      __syncwarp();
+      for (uint32_t i = tid; i < 4 * n; i += 32) qh[i] = 0.0;
+      __syncwarp();
+      row_charges(T, prog, m, qh + n, tid);
+      state_charges(T, rec, m.x, qt + nq, tid);
+      __syncwarp();
+      for (uint32_t i = tid; i < n; i += 32) {
+        qh[2 * n + i] = qh[n + i];
+        qh[3 * n + i] = qh[n + i];
+        ipr[i] = 0.0;
+      }
+      for (uint32_t j = tid; j < nq; j += 32) {
+        qt[2 * nq + j] = qt[nq + j];
+        qt[3 * nq + j] = qt[nq + j];
+        ipt[j] = 0.0;
+      }
+      __syncwarp();
+      pulse_timers(T, rec, tmr, tid);
+      dt = fmin(div_rn(fmin(P.t_step, div_rn(P.t_stop, 100.0)), 10.0), dt_max);
+      double bp0;
+      if (next_bp(T, rec, tmr, min_break, bp0)) dt = fmin(dt, 0.1 * bp0);
+      dt = div_rn(dt, 10.0);
+      record(0.0);
+    }
     LaneOpts nr = o;
     nr.residual_tol = CUDART_INF;
     nr.gmin = 0.0;
     nr.max_iter = 100;
+    bool res_step = phase0 == 2;  // the first pass continues the paused step's Newton solve
     for (;;) {
-      if (!(t < P.t_stop && !almost_equal_ulps(t, P.t_stop, 100) && steps < P.max_steps)) break;
+      if (!res_step && !(t < P.t_stop && !almost_equal_ulps(t, P.t_stop, 100) && steps < P.max_steps)) break;
       const double t_dev = t + dt;
       sim.kind = 1;
       sim.t = t_dev;
       const bool trap = order == 2;
       const double ag0 = trap ? div_rn(div_rn(1.0, dt), 1.0 - 0.5) : div_rn(1.0, dt);
       const double ag1 = trap ? div_rn(0.5, 1.0 - 0.5) : 1.0;
-      // predictor, limited against the accepted point
-      const double xfact = div_rn(dt, dt_old[0]);
-      for (uint32_t i = tid; i < n; i += 32) {
-        m.x[i] = cur[i] + xfact * (cur[i] - prev[i]);
-        m.xo[i] = cur[i];
+      if (!res_step) {
+        // predictor, limited against the accepted point
+        const double xfact = div_rn(dt, dt_old[0]);
+        for (uint32_t i = tid; i < n; i += 32) {
+          m.x[i] = cur[i] + xfact * (cur[i] - prev[i]);
+          m.xo[i] = cur[i];
+        }
+        __syncwarp();
+        apply_limits<kHasB3>(T, rec, m, false, tid);
+        lim_active = T.nlim != 0;
+        carry.iter = 0;
+        carry.init_fix = 0;
+        carry.resume = 0;
+        __syncwarp();
       }
-      __syncwarp();
-      apply_limits<kHasB3>(T, rec, m, false, tid);
-      lim_active = T.nlim != 0;
-      __syncwarp();
+      res_step = false;
       Companion c{ag0, ag1, trap, slot(qh, n, 1), ipr};
       uint32_t iters = 0;
       fill_sources(T, rec, sim, vsrc, tid);
-      rc = lane_newton<kHasB3>(T, prog, m, rec, nr, sim, &c, lim_active, false, iters, vsrc, tid);
+      rc = lane_newton<kHasB3>(T, prog, m, rec, nr, sim, &c, lim_active, false, iters, vsrc, tid, &carry);
+      if (rc == 3) {
+        pause(2, ag0);
+        return;
+      }
+      carry.resume = 0;
       lim_active = false;
       stat[kTsAttempts] += 1;
       stat[kTsNrIters] += iters;
-      if (rc == 2) {
-        stat[kTsStatus] = kTranLeftTape;
-        break;
-      }
       if (rc != 0) {
+        // out of iterations, or the host's factor of this lane was singular
         stat[kTsRejNewton] += 1;
         order = 1;
         dt = div_rn(dt, 8.0);
@@ -1873,7 +1994,10 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
   for (uint32_t i = tid; i < n; i += 32) L.x[size_t(lane) * n + i] = m.x[i];
   if (card) P.meas_out[size_t(lane) * P.n_meas + tid] = meas_value(P.meas[tid], mstate);
   if (tid < kTsN) P.stats[size_t(lane) * kTsN + tid] = stat[tid];
-  if (tid == 0 && P.n_pts) P.n_pts[lane] = n_rec;
+  if (tid == 0) {
+    if (P.n_pts) P.n_pts[lane] = n_rec;
+    L.status[lane] = kConverged;  // done: a resume launch passes it by
+  }
 }
 
 // One lane's sequential .dc sweep over the points of one swept source

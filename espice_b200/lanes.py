@@ -31,7 +31,7 @@ EXPORTS = ["esl_create", "esl_destroy", "esl_last_error", "esl_dims", "esl_set_l
            "esl_lu_lanes_mixed_device", "esl_group_dc_solve_device", "esl_autotune", "esl_dc_sweep_device",
            "esl_tran_meas_device", "esl_lu_lanes_compiled_device", "esl_lu_compiled_log",
            "esl_lu_compiled_source", "esl_lu_lanes_mixed_compiled_device", "esl_lu_compiled_mixed_source",
-           "esl_set_mode", "esl_block_info", "esl_block_profile"]
+           "esl_set_mode", "esl_block_info", "esl_block_profile", "esl_peel_counts"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 f64p = ctypes.POINTER(ctypes.c_double)
@@ -84,7 +84,8 @@ class BlockInfo(ctypes.Structure):
                                                  "b_nops", "ntv", "warp_ok")] + \
                [("lane_bytes", ctypes.c_uint32 * 2), ("in_smem", ctypes.c_uint32 * 2),
                 ("ctas_per_sm", ctypes.c_uint32 * 2), ("split", ctypes.c_uint32 * 2),
-                ("cold_bytes", ctypes.c_uint32 * 2)]
+                ("cold_bytes", ctypes.c_uint32 * 2), ("gather_terms", ctypes.c_uint32),
+                ("gather_cells", ctypes.c_uint32)]
 
 
 class TranOpts(ctypes.Structure):
@@ -359,12 +360,21 @@ class DcLanes:
         self._check(self._L.esl_block_profile(self._ctx, c), "esl_block_profile")
         return dict(zip(BLOCK_PHASES, [int(v) for v in c]))
 
+    def peel_counts(self):
+        """esl_peel_counts: (lanes peeled, host solves, launches) of the last
+        transient or sequential sweep call."""
+        a, b, c = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(self._L.esl_peel_counts(self._ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+                    "esl_peel_counts")
+        return a.value, b.value, c.value
+
     def block_info(self):
         info = BlockInfo()
         self._check(self._L.esl_block_info(self._ctx, ctypes.byref(info)), "esl_block_info")
         out = {k: getattr(info, k) for k, _ in info._fields_[:9]}
         for k in ("lane_bytes", "in_smem", "ctas_per_sm", "split", "cold_bytes"):
             out[k] = list(getattr(info, k))
+        out["gather_terms"], out["gather_cells"] = info.gather_terms, info.gather_cells
         return out
 
     def solve_device_static(self, d_x, d_iters, d_status, cold=False, opts=None):

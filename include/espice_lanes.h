@@ -253,14 +253,17 @@ enum {
     ESL_TRAN_UNDERFLOW = 1,  /* TimestepTooSmall */
     ESL_TRAN_OP_FAILED = 2,  /* the operating point did not converge */
     ESL_TRAN_MAX_STEPS = 3,
-    ESL_TRAN_LEFT_TAPE = 4   /* a factor left the lead pivot tape: run the lane on the CPU */
+    ESL_TRAN_LEFT_TAPE = 4   /* unused: a lane that leaves the lead tape is peeled to the host */
 };
 
 /* Monte-Carlo transient lanes (tran.runGpuLanes, tran.zig:1654, driving
  * gpu_lanes.zig predictRound/newton/apply per tick): each lane solves its
  * operating point from a cold start, then steps trapezoidally (BE first
  * step, order promotion, LTE control over the charge states, Newton
- * rejection, PULSE breakpoints) to t_stop, all inside one launch. Host
+ * rejection, PULSE and PWL breakpoints) to t_stop, all inside one launch.
+ * A lane whose factor leaves the lead pivot tape pauses, takes a factor
+ * of its own on the host (lane_solver.zig's peel) and resumes where it
+ * stopped, in a further launch (esl_peel_counts). Host
  * buffers: x_out [n_lanes][n] the last accepted solution, stats
  * [n_lanes][ESL_TS_N]; with max_pts > 0, probes [n_probes] unknowns
  * recorded at t = 0 and every accepted step into t_out [n_lanes][max_pts],
@@ -357,6 +360,7 @@ int32_t esl_set_mode(esl_ctx *ctx, const esl_solve_mode *mode);
 typedef struct {
     uint32_t width, a_rows, b_rows, f_rows, a_levels, a_nops, b_nops, ntv, warp_ok;
     uint32_t lane_bytes[2], in_smem[2], ctas_per_sm[2], split[2], cold_bytes[2];
+    uint32_t gather_terms, gather_cells; /* the assembly's terms and cells a thread walks */
 } esl_block_info_t;
 int32_t esl_block_info(esl_ctx *ctx, esl_block_info_t *info);
 
@@ -366,6 +370,12 @@ int32_t esl_block_info(esl_ctx *ctx, esl_block_info_t *info);
  * refactor + forward solve, [3] back solve and step, [4] mixed refinement,
  * [5] update, limiting and gates, [6] the Newton iterations counted. */
 int32_t esl_block_profile(esl_ctx *ctx, uint64_t *cycles);
+
+/* The peels of the context's last transient (esl_tran*, esl_tran_meas_device)
+ * or sequential sweep (esl_dc_sweep_device) call: lanes that paused for a
+ * host factor at least once, host factor + solve calls, and kernel launches
+ * (the first and every resume). Any pointer may be NULL. */
+int32_t esl_peel_counts(const esl_ctx *ctx, uint32_t *lanes, uint32_t *host_solves, uint32_t *launches);
 
 /* Picks the context's lanes per CTA (1, 2, 4 or 8, as shared memory allows)
  * by timing its DC solve from x0 (NULL: cold) on its current lanes; keeps

@@ -235,3 +235,41 @@ def test_bsim3_inverter_chain_transient_lanes():
     res_g, res_o = _run_both(fr, slots[1:], values[:, 1:], 2e-9, 10e-12, probes=probes, max_pts=4000)
     _check_parity(res_g, res_o)
     assert (res_g[3][:, 0] == lanes.TRAN_DONE).all()
+
+
+ZENER_TRAN = """* the reference's shunt regulator (power/zener_reg) driven by a supply ramp
+Vsupply sup 0 PULSE(6 18 10n 200n 200n 200n 1u)
+Rseries sup out 220
+Dz out ref DZ
+Vref ref 0 DC 5.1
+Rload out 0 1k
+Cout out 0 100p
+.model DZ D(IS=1e-12 N=1)
+.tran 1n 600n
+.end
+"""
+
+
+def test_lanes_that_leave_the_tape_are_peeled():
+    """The reference's shunt regulator with its supply ramped from 6 to 18 V
+    and back (the ramp its DC sweep takes, whose breakdown points leave the
+    lead pivot tape): the transient lanes that leave the tape pause, take the
+    host's factor and resume, and every lane keeps the oracle's step
+    decisions and waveforms."""
+    deck = Deck(ZENER_TRAN)
+    fr = deck.circuit().freeze()
+    slots = [fr.slot("rseries", "r")]
+    values = np.linspace(150.0, 330.0, 6).reshape(-1, 1)
+    probes = [fr.unknown("v(out)")]
+    go = lanes.tran_opts(600e-9, 1e-9, 0.0, max_steps=200_000)
+    oo = oracle.tran_opts(600e-9, 1e-9, 0.0, max_steps=200_000)
+    ctx = lanes.DcLanes(fr)
+    ctx.set_lanes(slots, values)
+    g = ctx.tran(go, probes, 5_000)
+    peeled, solves, launches = ctx.peel_counts()
+    ctx.close()
+    o = oracle.tran(fr, slots, values, oo, probes, 5_000)
+    print(f"peeled lanes {peeled}, host solves {solves}, launches {launches}")
+    _check_parity(g, o)
+    assert (g[3][:, 0] == lanes.TRAN_DONE).all()
+    assert peeled > 0 and launches > 1
