@@ -831,7 +831,8 @@ void build_block_gather(const esl_ctx* ctx, uint32_t W, std::vector<uint32_t>& t
     std::vector<uint32_t> src;
     uint32_t w0, w1, w2;
   };
-  auto code = [](uint32_t s) { return s == kSrcOne ? kGSrcOne : s == kSrcX0 ? kGSrcX0 : s; };
+  const uint32_t ns = ctx->n_stage;
+  auto code = [ns](uint32_t s) { return s == kSrcOne ? ns + kGCellOne : s == kSrcX0 ? ns + kGCellX0 : s; };
   std::vector<Cell> all;
   const uint32_t n = ctx->pat.n, nnz = ctx->pat.nnz();
   for (uint32_t i = 0; i < n; ++i) {
@@ -845,7 +846,7 @@ void build_block_gather(const esl_ctx* ctx, uint32_t W, std::vector<uint32_t>& t
     all.push_back(std::move(c));
   }
   for (Cell& c : all) {
-    if (c.src.empty()) c.src.push_back(kGSrcZero);
+    if (c.src.empty()) c.src.push_back(ns + kGCellZero);
     c.src.back() |= kGTermEnd;
   }
   std::stable_sort(all.begin(), all.end(), [](const Cell& a, const Cell& b) { return a.src.size() > b.src.size(); });
@@ -863,7 +864,7 @@ void build_block_gather(const esl_ctx* ctx, uint32_t W, std::vector<uint32_t>& t
     len = std::max(len, uint32_t(t_terms[t].size()));
     ncells = std::max(ncells, uint32_t(t_cells[t].size() / 4));
   }
-  terms.assign(size_t(std::max(len, 1u)) * W, kGSrcZero);
+  terms.assign(size_t(std::max(len, 1u)) * W, ns + kGCellZero);
   cells.assign(size_t(std::max(ncells, 1u)) * W * 4, 0u);
   for (uint32_t t = 0; t < W; ++t) {
     for (size_t k = 0; k < t_terms[t].size(); ++k) terms[k * W + t] = t_terms[t][k];
@@ -916,7 +917,7 @@ void block_layout(const TopoDev& T, uint32_t nv, bool mixed, bool split, BlockDe
   const size_t hot = at;
   if (split) at = 0;
   D.o_xo = take(8 * size_t(T.n));
-  D.o_st = take(8 * size_t(T.n_stage));
+  D.o_st = take(8 * size_t(T.n_stage + kGConstCells));
   D.split = split ? 1u : 0u;
   D.lane_bytes = uint32_t(split ? hot : at);
   D.cold_bytes = uint32_t(split ? at : 0);

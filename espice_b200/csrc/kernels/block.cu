@@ -220,8 +220,8 @@ __device__ __forceinline__ BlockMem<V> block_carve(const BlockDev& D, unsigned c
 }
 
 // Assembly as one streamed gather: thread t walks its term stream
-// (D.g_terms[k * kW + t], k < D.g_len) summing staging cells (or x[0], 1.0,
-// +0.0) from +0.0 in each cell's list order (the CSR order: the same bits as
+// (D.g_terms[k * kW + t], k < D.g_len) summing staging cells (the constant
+// cells for x[0], 1.0 and +0.0) from +0.0 in each cell's list order (the CSR order: the same bits as
 // the warp lanes' gather and the host factor's pattern copy); a term with
 // kGTermEnd closes a cell, whose destinations come from the thread's cell
 // stream (D.g_cells[c * kW + t]): a pattern slot (its tape value, FP32 in the
@@ -232,8 +232,7 @@ __device__ __forceinline__ BlockMem<V> block_carve(const BlockDev& D, unsigned c
 // values are zeroed.
 template <typename V, uint32_t kW>
 __device__ __forceinline__ double gather_term(const BlockMem<V>& b, uint32_t w) {
-  const uint32_t src = w & ~kGTermEnd;
-  return src < kGSrcZero ? b.m.st[src] : src == kGSrcOne ? 1.0 : src == kGSrcX0 ? b.m.x[0] : 0.0;
+  return b.m.st[w & ~kGTermEnd];
 }
 
 template <typename V, uint32_t kW>
@@ -260,7 +259,7 @@ __device__ void block_assemble(const BlockDev& D, const BlockMem<V>& b, double g
   const TopoDev& T = D.T;
   const uint32_t* terms = D.g_terms + tid;
   const uint4* cells = D.g_cells + tid;
-  const uint32_t K = D.g_len;
+  const uint32_t K = D.g_len, pad = T.n_stage + kGCellZero;
   // Term words two batches ahead and staging values one batch ahead: every
   // load of a batch is issued before the stores of the batch before it, so
   // none waits behind them (the staging cells are only read here).
@@ -268,8 +267,8 @@ __device__ void block_assemble(const BlockDev& D, const BlockMem<V>& b, double g
   double val[8];
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
-    w[j] = uint32_t(j) < K ? __ldg(terms + size_t(j) * kW) : kGSrcZero;
-    nx[j] = uint32_t(8 + j) < K ? __ldg(terms + size_t(8 + j) * kW) : kGSrcZero;
+    w[j] = uint32_t(j) < K ? __ldg(terms + size_t(j) * kW) : pad;
+    nx[j] = uint32_t(8 + j) < K ? __ldg(terms + size_t(8 + j) * kW) : pad;
   }
 #pragma unroll
   for (int j = 0; j < 8; ++j) val[j] = gather_term<V, kW>(b, w[j]);
@@ -282,7 +281,7 @@ __device__ void block_assemble(const BlockDev& D, const BlockMem<V>& b, double g
     uint32_t nnx[8];
     double nv[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) nnx[j] = k0 + 16 + j < K ? __ldg(terms + size_t(k0 + 16 + j) * kW) : kGSrcZero;
+    for (int j = 0; j < 8; ++j) nnx[j] = k0 + 16 + j < K ? __ldg(terms + size_t(k0 + 16 + j) * kW) : pad;
 #pragma unroll
     for (int j = 0; j < 8; ++j) nv[j] = gather_term<V, kW>(b, nx[j]);
 #pragma unroll
@@ -393,6 +392,8 @@ __device__ void block_lane(const BlockDev& D, const LaneDev& L, const LaneOpts& 
     b.v[T.ntv + n] = V(0);
     b.v[T.ntv + n + 1] = V(1);
     b.v[T.ntv + n + 2] = V(0);
+    m.st[T.n_stage + kGCellZero] = 0.0;
+    m.st[T.n_stage + kGCellOne] = 1.0;
   }
   bool lim_active = L.lim_active[lane] != 0;
   uint32_t flags = L.flags[lane];
@@ -421,6 +422,7 @@ __device__ void block_lane(const BlockDev& D, const LaneDev& L, const LaneOpts& 
     if (D.prof && tid == 0) atomicAdd(D.prof + kBlockPhaseIters, 1ull);
     if (!have_step) {
       eval_all<kHasB3, kW>(T, rec, m, lim_active, sim, tid, false, nullptr, true);
+      if (tid == 0) m.st[T.n_stage + kGCellX0] = m.x[0];
       __syncthreads();
       phase_mark(D.prof, kBlockPhaseEval, t0);
       block_assemble<V, kW>(D, b, o.gmin, tid);

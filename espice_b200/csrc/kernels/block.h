@@ -15,14 +15,15 @@ namespace esl {
 constexpr uint32_t kBlockThreads = 256;
 
 // The block lanes' assembly streams (see block_assemble): a term word is a
-// staging index or one of the three constants below, with kGTermEnd on a
-// cell's last term; a cell word {index | kGCellRow, tape value or y index,
+// staging index, with kGTermEnd on a cell's last term. Three cells past the
+// device stamps hold constants, so every term is a plain load: n_stage +
+// kGCellZero (+0.0: a cell without terms, padding), + kGCellOne (1.0: the
+// ground pin on g) and + kGCellX0 (x[0]: the ground pin on rhs, refreshed
+// each iteration). A cell word {index | kGCellRow, tape value or y index,
 // diagonal row or kNoDiag, 0} is a pattern slot (index p) or, with
 // kGCellRow, a residual row (index i).
 constexpr uint32_t kGTermEnd = 0x80000000u;
-constexpr uint32_t kGSrcZero = 0x3ffffffcu;  // + 0.0 (a cell without terms; padding)
-constexpr uint32_t kGSrcX0 = 0x3ffffffdu;    // + x[0] (the ground pin on rhs)
-constexpr uint32_t kGSrcOne = 0x3ffffffeu;   // + 1.0 (the ground pin on g)
+constexpr uint32_t kGCellZero = 0, kGCellOne = 1, kGCellX0 = 2, kGConstCells = 3;
 constexpr uint32_t kGCellRow = 0x80000000u;
 
 struct BlockDev {
