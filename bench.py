@@ -529,6 +529,10 @@ def ring_period_early_stop(args, local, flush):
 # converges to the same solution within the parity tolerance (at reltol 1e-3
 # a point's result depends on its start at the 1e-3 level).
 TIGHT = dict(reltol=1e-9, vntol=1e-12, abstol=1e-15)
+# Mixed precision refines the Newton steps within this many tolerances of
+# convergence (esl_solve_mode.refine_skip); the steps farther out go
+# unrefined, their FP32 error corrected by the iterations after them.
+REFINE_SKIP = 1e3
 
 
 def _dev(a, b):
@@ -734,10 +738,10 @@ def our_arm(args, rank, world):
     plain.set_lanes(slots, vals)
     setup["set_lanes_s"] = time.perf_counter() - t0
     mixed = lanes.DcLanes(fr, device=local)
-    mixed.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK)
+    mixed.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK, refine_skip=REFINE_SKIP)
     mixed.set_lanes(slots, vals)
     fb = lanes.DcLanes(fr, device=local)
-    fb.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK)
+    fb.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK, refine_skip=REFINE_SKIP)
     d_x = torch.empty((N, n), dtype=torch.float64, device="cuda")
     d_it = torch.zeros(N, dtype=torch.int32, device="cuda")
     d_st = torch.zeros(N, dtype=torch.int32, device="cuda")
@@ -794,6 +798,16 @@ def our_arm(args, rank, world):
     x_plain = d_x.cpu().numpy()
     it_plain = d_it.cpu().numpy().astype(np.int64)
     K = args.steps
+    # attribution: the same learned + mixed steps refining every Newton step
+    mixed.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK)
+    fb.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK)
+    at, aconv = 0.0, 0
+    for _ in range(K):
+        (_, _, conv, _), dt = timed(lambda: learned_step([]))
+        at += dt
+        aconv += int(conv.sum())
+    mixed.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK, refine_skip=REFINE_SKIP)
+    fb.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK, refine_skip=REFINE_SKIP)
 
     # e2e through the public API with host buffers: the points' parameters
     # in, every point's solution out
@@ -820,12 +834,12 @@ def our_arm(args, rank, world):
             d2h += N * n * 8 + 2 * N * 4 + nfb * n * 8
 
     # the mixed lanes' phase cycles (one untimed, profiled pass)
-    mixed.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK, profile=True)
+    mixed.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK, profile=True, refine_skip=REFINE_SKIP)
     prof_stats = []
     learned_step(prof_stats)
     prof = mixed.block_profile()
     info = mixed.block_info()
-    mixed.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK)
+    mixed.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK, refine_skip=REFINE_SKIP)
 
     lt, lconv = shard.reduce_run(lt, lconv)
     pt, pconv = shard.reduce_run(pt, pconv)
@@ -844,6 +858,7 @@ def our_arm(args, rank, world):
     achieved = N * lane_bytes / (k_ms / 1e3) / 1e9
     iters = max(prof["iterations"], 1)
     ref_per_iter = prof_stats[0]["refinements"] / iters
+    at, aconv = shard.reduce_run(at, aconv)
     rows_per_iter = info["a_rows"] + info["b_rows"] + ref_per_iter * (info["f_rows"] + info["b_rows"])
     cyc = {k: prof[k] / iters for k in ("eval", "assemble", "refactor", "solve", "refine", "gates")}
     launches = sum(sum(x["launches"] + 1 for x in st) for st in lstats) + K * 10
@@ -858,6 +873,12 @@ def our_arm(args, rank, world):
         "plain_fp64": {"value": pconv / pt, "unit": UNIT, "ms_per_step": 1e3 * pt / K,
                        "newton_iters_per_point": pit / K, "gpu_launches": int(sum(x["launches"] + 1 for x in pstats))},
         "learned_mixed_over_plain": (lconv / lt) / (pconv / pt),
+        "mixed_refinement": {"refine_tol": 1e-12, "refine_skip": REFINE_SKIP,
+                             "note": "FP32 refactor and solves; a Newton step whose FP32 solution is within "
+                                     f"{REFINE_SKIP:g} tolerances of convergence is refined in FP64 on the residual "
+                                     "to 1e-12 of it, a step farther out is taken as an inexact Newton step",
+                             "refine_every_step_points_per_s": aconv / at,
+                             "refinements_per_newton_iter": ref_per_iter},
         "newton_iters_per_point": lit / K, "fallback_points_per_step": lfb / K,
         "e2e_fallback_points_per_step": e2e_fb / K,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",

@@ -243,6 +243,7 @@ struct esl_ctx {
   uint32_t block_width = 256;
   double refine_tol = 1e-12;
   uint32_t refine_max = 6;
+  double refine_skip = 0.0;  // mixed: steps above this many tolerances go unrefined (0: none)
   bool have_block = false;
   bool profile = false;  // block lanes: accumulate the phase cycles (esl_solve_mode.profile)
   BlockPrograms bprog;
@@ -969,6 +970,7 @@ int32_t block_view(esl_ctx* ctx, bool mixed, uint32_t n_lanes, BlockDev& D) {
   D.slab = ctx->d_slab.as<unsigned char>();
   D.refine_tol = ctx->refine_tol;
   D.refine_max = ctx->refine_max;
+  D.refine_skip = ctx->refine_skip;
   ESL_CUDA(ctx->d_refine.ensure(size_t(n_lanes) * 4));
   D.refine_out = mixed ? ctx->d_refine.as<uint32_t>() : nullptr;
   D.prof = nullptr;
@@ -1925,6 +1927,7 @@ int32_t esl_set_mode(esl_ctx* ctx, const esl_solve_mode* mode) {
   ctx->block_width = width;
   ctx->refine_tol = mode->refine_tol > 0.0 ? mode->refine_tol : 1e-12;
   ctx->refine_max = mode->refine_max ? mode->refine_max : 6;
+  ctx->refine_skip = mode->refine_skip > 0.0 ? mode->refine_skip : 0.0;
   ctx->profile = mode->profile != 0;
   return ESL_OK;
 }

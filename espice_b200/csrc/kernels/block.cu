@@ -474,7 +474,22 @@ __device__ void block_lane(const BlockDev& D, const LaneDev& L, const LaneOpts& 
       __syncthreads();
       phase_mark(D.prof, kBlockPhaseSolve, t0);
       if constexpr (kMixed) {
-        refinements += block_refine<OpT, kW>(D, b, red, tid);
+        bool refine = true;
+        if (D.refine_skip > 0.0) {
+          // an inexact Newton step far from convergence keeps its FP32 error
+          // (about 1e-7 of the step, far below what the next iterate
+          // corrects); the steps nearer convergence are refined
+          uint64_t q = 0;
+          for (uint32_t i = tid; i < n; i += kW) {
+            const double d = b.dx[i], xo = m.x[i], xn = xo + d;
+            const double tol = o.reltol * fmax(fabs(xn), fabs(xo)) + (T.cur_row[i] ? o.abstol : o.vntol);
+            const double s = div_rn(fabs(d), tol);
+            const uint64_t bits = dbits(s == s ? s : CUDART_INF);
+            q = bits > q ? bits : q;
+          }
+          refine = !(from_bits(block_max_bits<kW>(q, red)) > D.refine_skip);
+        }
+        if (refine) refinements += block_refine<OpT, kW>(D, b, red, tid);
         phase_mark(D.prof, kBlockPhaseRefine, t0);
       }
     }

@@ -58,6 +58,9 @@ struct BlockDev {
   double refine_tol;
   uint32_t refine_max;
   uint32_t* refine_out;
+  // Mixed form: a step whose FP32 solution scores above refine_skip
+  // tolerances (the Newton delta score) is taken unrefined (0: never).
+  double refine_skip;
   // Optional phase profile (null: off): thread 0 of each CTA adds the SM
   // cycles (clock64) of each phase of each Newton iteration to
   // prof[kBlockPhase*], and counts the iterations in prof[kBlockPhaseIters].

@@ -73,7 +73,7 @@ PATH_AUTO, PATH_WARP, PATH_BLOCK = 0, 1, 2
 class SolveMode(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_uint32), ("path", ctypes.c_uint32), ("block_threads", ctypes.c_uint32),
                 ("refine_max", ctypes.c_uint32), ("refine_tol", ctypes.c_double), ("profile", ctypes.c_uint32),
-                ("pad", ctypes.c_uint32)]
+                ("pad", ctypes.c_uint32), ("refine_skip", ctypes.c_double)]
 
 
 BLOCK_PHASES = ["eval", "assemble", "refactor", "solve", "refine", "gates", "iterations"]
@@ -347,11 +347,12 @@ class DcLanes:
         return stats.as_dict()
 
     def set_mode(self, precision=PREC_FP64, path=PATH_AUTO, block_threads=0, refine_tol=0.0, refine_max=0,
-                 profile=False):
+                 profile=False, refine_skip=0.0):
         """esl_set_mode: FP64 or mixed precision; the warp lanes, the block
         lanes, or either (PATH_AUTO); profile: count the block lanes' phase
-        cycles (block_profile)."""
-        m = SolveMode(precision, path, block_threads, refine_max, refine_tol, int(profile), 0)
+        cycles (block_profile); refine_skip: take mixed steps above that many
+        tolerances unrefined (0: refine every step)."""
+        m = SolveMode(precision, path, block_threads, refine_max, refine_tol, int(profile), 0, refine_skip)
         self._check(self._L.esl_set_mode(self._ctx, ctypes.byref(m)), "esl_set_mode")
 
     def block_profile(self):

@@ -141,10 +141,16 @@ typedef struct {
  * stand in for (the pivot tests on them) takes the host's FP64 factor.
  * path: ESL_PATH_AUTO picks the warp lanes (a warp per lane, its working
  * set in shared memory) for FP64 when the tape fits them, else the block
- * lanes (a CTA per lane, block_threads wide: 128 or 256, 0 = 256; the
+ * lanes (a CTA per lane, block_threads wide: 256, or 0 for 256; the
  * working set in shared memory when it fits, else in global memory, for any
  * circuit size); ESL_PATH_WARP / ESL_PATH_BLOCK force one (the warp lanes
- * are FP64 only). refine_tol 0 takes 1e-12, refine_max 0 takes 6. */
+ * are FP64 only). refine_tol 0 takes 1e-12, refine_max 0 takes 6.
+ * refine_skip > 0 (mixed precision): a Newton step whose FP32 solution is
+ * still more than refine_skip times its convergence tolerance (the delta
+ * score, max |dx_i| / (reltol max(|x_i|, |x_i + dx_i|) + vntol or abstol))
+ * is taken unrefined, as an inexact Newton step; the steps nearer
+ * convergence, the accepted one among them, are refined. 0: every step is
+ * refined. */
 enum { ESL_PREC_FP64 = 0, ESL_PREC_MIXED = 1 };
 enum { ESL_PATH_AUTO = 0, ESL_PATH_WARP = 1, ESL_PATH_BLOCK = 2 };
 typedef struct {
@@ -155,6 +161,7 @@ typedef struct {
     double refine_tol;
     uint32_t profile;  /* != 0: block-lane solves count their phase cycles (esl_block_profile) */
     uint32_t pad;
+    double refine_skip;
 } esl_solve_mode;
 
 /* Builds the pattern, column order and stamp tables of `circuit` on

@@ -154,3 +154,28 @@ def test_block_lanes_serve_pauses():
     xo, ito, cvo = oracle.dc_points(fr, slots, values, warm=None, opts=oracle.newton_opts(**opts))
     parity.assert_dc_parity(fr, slots, values, None, oracle.newton_opts(**opts), xb, itb,
                             stb == lanes.LANE_CONVERGED, xo, ito, cvo, "zener block")
+
+
+def test_analog_block_mixed_adaptive_refinement():
+    """Mixed precision with refine_skip: steps more than 1e3 tolerances from
+    convergence go unrefined (inexact Newton), the rest are refined. Every
+    point still converges as the oracle's does, within 1e-9 relative or
+    1e-12 absolute of the FP64 oracle at the 1e-9 setting, with fewer
+    refinement corrections than refining every step."""
+    tight = dict(reltol=1e-9, vntol=1e-12, abstol=1e-15)
+    fr, slots, values, x_nom = _analog(48, seed=4)
+    refs = {}
+    for skip in (0.0, 1e3):
+        ctx = lanes.DcLanes(fr)
+        ctx.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK, refine_skip=skip)
+        ctx.set_lanes(slots, values)
+        xm, itm, stm, stats = ctx.solve(x0=x_nom, opts=lanes.newton_opts(**tight))
+        ctx.close()
+        refs[skip] = stats["refinements"]
+        xo, ito, cvo = oracle.dc_points(fr, slots, values, warm=x_nom, opts=oracle.newton_opts(**tight))
+        assert np.array_equal(stm == lanes.LANE_CONVERGED, cvo.astype(bool))
+        ok = parity.close(xm, xo)
+        assert ok.all(), float(np.max(np.abs(xm - xo) / (1e-12 + np.abs(xo))))
+        print(f"refine_skip {skip:g}: {stats['refinements']} corrections, iterations {itm.mean():.2f} "
+              f"(oracle {ito.mean():.2f})")
+    assert refs[1e3] < refs[0.0]
