@@ -224,6 +224,7 @@ struct esl_ctx {
   std::vector<HostBatch> bats;
   uint32_t n_stage = 0, rec_size = 0, nlim = 0;
   std::vector<uint32_t> rhs_ptr, rhs_src, a_ptr, a_src, slot_row;
+  std::vector<uint32_t> gst;  // gmin-stepping stamps (slot, row, column)
   std::vector<uint32_t> q_ptr, q_src, c_ptr, c_src;  // transient charge rows, capacitance slots
   uint32_t n_qt = 0;
   std::vector<double> rec_nominal;
@@ -272,6 +273,7 @@ struct esl_ctx {
   DevBuf d_group_blocks, d_group_items, d_group_slab;  // a block-lane group launch's tables and slabs
   DevBuf d_rec, d_lim, d_lim_active, d_status, d_iters, d_flags, d_limit, d_a_vals, d_rhs, d_dx,
       d_diag, d_paused, d_x;
+  DevBuf d_gst, d_ladder, d_x_good;  // operating-point lanes: stamps, ladder states, stepping points
   TopoDev topo{};
 
   std::unordered_map<uint32_t, DirectSolver> peel;
@@ -830,19 +832,26 @@ void build_block_gather(const esl_ctx* ctx, uint32_t W, std::vector<uint32_t>& t
                         uint32_t& len, uint32_t& ncells) {
   struct Cell {
     std::vector<uint32_t> src;
-    uint32_t w0, w1, w2;
+    uint32_t w0, w1, w2, w3;
   };
   const uint32_t ns = ctx->n_stage;
   auto code = [ns](uint32_t s) { return s == kSrcOne ? ns + kGCellOne : s == kSrcX0 ? ns + kGCellX0 : s; };
   std::vector<Cell> all;
   const uint32_t n = ctx->pat.n, nnz = ctx->pat.nnz();
+  // the gmin-stepping stamps: the column + 1 on a stamped row, 1 on a
+  // stamped slot (block.cu gather_store)
+  std::vector<uint32_t> row_w(n, 0u), slot_w(nnz, 0u);
+  for (size_t k = 0; k + 2 < ctx->gst.size(); k += 3) {
+    slot_w[ctx->gst[k]] = 1u;
+    row_w[ctx->gst[k + 1]] = ctx->gst[k + 2] + 1u;
+  }
   for (uint32_t i = 0; i < n; ++i) {
-    Cell c{{}, i | kGCellRow, ctx->lead.pinv[i], 0u};
+    Cell c{{}, i | kGCellRow, ctx->lead.pinv[i], 0u, row_w[i]};
     for (uint32_t e = ctx->rhs_ptr[i]; e < ctx->rhs_ptr[i + 1]; ++e) c.src.push_back(code(ctx->rhs_src[e]));
     all.push_back(std::move(c));
   }
   for (uint32_t p = 0; p < nnz; ++p) {
-    Cell c{{}, p, ctx->prog.amap[p], ctx->slot_row[p]};
+    Cell c{{}, p, ctx->prog.amap[p], ctx->slot_row[p], slot_w[p]};
     for (uint32_t e = ctx->a_ptr[p]; e < ctx->a_ptr[p + 1]; ++e) c.src.push_back(code(ctx->a_src[e]));
     all.push_back(std::move(c));
   }
@@ -856,7 +865,7 @@ void build_block_gather(const esl_ctx* ctx, uint32_t W, std::vector<uint32_t>& t
   for (const Cell& c : all) {
     const uint32_t t = uint32_t(std::min_element(load.begin(), load.end()) - load.begin());
     t_terms[t].insert(t_terms[t].end(), c.src.begin(), c.src.end());
-    t_cells[t].insert(t_cells[t].end(), {c.w0, c.w1, c.w2, 0u});
+    t_cells[t].insert(t_cells[t].end(), {c.w0, c.w1, c.w2, c.w3});
     load[t] += c.src.size();
   }
   len = 0;
@@ -1018,7 +1027,14 @@ int32_t build_tape_from(esl_ctx* ctx, const double* lead_vals) {
   if (!ctx->lead.factor(lead_vals, kPivotTol))
     return ctx->fail(ESL_NOT_ELIGIBLE, "the lead lane's first Jacobian is singular");
   ctx->prog = compile_tape(ctx->lead);
-  return upload_tape(ctx);
+  if (int32_t rc = upload_tape(ctx)) return rc;
+  // The gmin-stepping rung's stamps: the V-source incidence (+-1) and the
+  // zero branch diagonals decide them, the same in every lane.
+  ctx->gst = gmin_stamps(ctx->pat, ctx->cur, lead_vals);
+  ESL_CUDA(upload(ctx->d_gst, ctx->gst, ctx->stream));
+  ctx->topo.gst = ctx->d_gst.as<uint32_t>();
+  ctx->topo.n_gst = uint32_t(ctx->gst.size() / 3);
+  return ESL_OK;
 }
 
 // Lanes per CTA for a launch over n_lanes: the caller's choice when given,
@@ -1096,7 +1112,9 @@ int32_t serve_pauses(esl_ctx* ctx, const LaneDev& L, esl_stats* st, bool* any) {
     if (it == ctx->peel.end()) {
       DirectSolver ds;
       ds.init(&ctx->pat, ctx->order);
-      if (iters[l] != 0) ds.adopt(ctx->lead, nullptr);
+      // a lane that factored before (an earlier iteration, or an earlier
+      // run of the ladder) holds the lead tape in its solver
+      if (iters[l] != 0 || (flags[l] & 4u)) ds.adopt(ctx->lead, nullptr);
       it = ctx->peel.emplace(l, std::move(ds)).first;
       it->second.lu.a = &ctx->pat;
       if (st) st->peeled++;
@@ -1276,17 +1294,26 @@ namespace {
 // coldStart; warm: x with limiting off) and, on a context's first solve,
 // the lead tape from lane 0's first Jacobian. Leaves the lane view in L.
 int32_t prepare_dc(esl_ctx* ctx, const esl_newton_opts* opts, double* d_x, int cold, uint32_t* d_iters,
-                   uint32_t* d_status, esl_stats* st, LaneDev& L) {
+                   uint32_t* d_status, esl_stats* st, LaneDev& L, uint32_t* d_rung = nullptr) {
   cudaStream_t s = ctx->stream;
   if (st) std::memset(st, 0, sizeof(*st));
   // Per-lane start state, set on the device (lane_init_kernel): cold lanes
   // start at zero with the junction seeds (op.zig coldStart), warm lanes at
-  // x with limiting off.
+  // x with limiting off; operating-point lanes (d_rung given) on the
+  // ladder's first rung.
   ctx->peel.clear();
   L = lane_view(ctx, 0);
   L.x = d_x;
   L.iters = d_iters;
   L.status = d_status;
+  if (d_rung) {
+    const size_t N = ctx->n_lanes;
+    ESL_CUDA(ctx->d_ladder.ensure(N * sizeof(LadderDev)));
+    ESL_CUDA(ctx->d_x_good.ensure(N * ctx->pat.n * 8));
+    L.ladder = ctx->d_ladder.as<LadderDev>();
+    L.x_good = ctx->d_x_good.as<double>();
+    L.rung_out = d_rung;
+  }
   ESL_CUDA(launch_lane_init(ctx->topo, L, cold != 0, opts->init_fix != 0, s));
   if (!ctx->have_tape) {
     // The lead lane's first Jacobian, factored on the host into the tape.
@@ -1301,21 +1328,27 @@ int32_t prepare_dc(esl_ctx* ctx, const esl_newton_opts* opts, double* d_x, int c
 
 }  // namespace
 
-int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d_x, int cold,
-                            uint32_t* d_iters, uint32_t* d_status, esl_stats* st) {
-  if (!ctx || !opts || !d_x || ctx->n_lanes == 0) return ESL_INVALID_ARGUMENT;
-  cudaSetDevice(ctx->device);
+}  // extern "C"
+
+namespace {
+
+// The DC lanes' solve: every lane's Newton run (a plain DC solve), or every
+// lane's operating point through op.zig's ladder (d_rung given), with the
+// host serving the lanes that pause for a factor of their own.
+int32_t dc_solve(esl_ctx* ctx, const esl_newton_opts* opts, double* d_x, int cold, uint32_t* d_iters,
+                 uint32_t* d_status, uint32_t* d_rung, esl_stats* st) {
   cudaStream_t s = ctx->stream;
   const uint32_t N = ctx->n_lanes;
   LaneDev L;
-  if (int32_t rc = prepare_dc(ctx, opts, d_x, cold, d_iters, d_status, st, L)) return rc;
+  if (int32_t rc = prepare_dc(ctx, opts, d_x, cold, d_iters, d_status, st, L, d_rung)) return rc;
   LaneOpts o{opts->reltol, opts->abstol, opts->vntol, opts->residual_tol, opts->gmin, opts->max_iter, opts->init_fix,
-             opts->iter_cap};
-  const bool block = use_block(ctx);
+             opts->iter_cap, d_rung ? 1u : 0u};
+  // operating-point lanes run the FP64 form (warp or block lanes)
+  const bool block = d_rung ? (ctx->path == ESL_PATH_BLOCK || !ctx->warp_ok) : use_block(ctx);
   if (!block && !ctx->warp_ok) return warp_only(ctx);
   if (ctx->path == ESL_PATH_WARP && block)
     return ctx->fail(ESL_NOT_ELIGIBLE, ctx->warp_ok ? "the warp lanes solve in FP64 only" : "the tape exceeds the warp lanes");
-  const bool mixed = ctx->precision == ESL_PREC_MIXED;
+  const bool mixed = ctx->precision == ESL_PREC_MIXED && !d_rung;
   BlockDev D{};
   if (block) {
     if (int32_t rc = block_view(ctx, mixed, N, D)) return rc;
@@ -1357,6 +1390,46 @@ int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d
       for (uint32_t v : ref) st->refinements += v;
     }
   }
+  return ESL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t esl_dc_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d_x, int cold,
+                            uint32_t* d_iters, uint32_t* d_status, esl_stats* st) {
+  if (!ctx || !opts || !d_x || ctx->n_lanes == 0) return ESL_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  return dc_solve(ctx, opts, d_x, cold, d_iters, d_status, nullptr, st);
+}
+
+int32_t esl_op_solve_device(esl_ctx* ctx, const esl_newton_opts* opts, double* d_x, uint32_t* d_iters,
+                            uint32_t* d_status, uint32_t* d_rung, esl_stats* st) {
+  if (!ctx || !opts || !d_x || !d_iters || !d_status || !d_rung || ctx->n_lanes == 0) return ESL_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  // the plain rung is a cold operating point: MODEINITJCT seeds, then INITFIX
+  esl_newton_opts o = *opts;
+  o.init_fix = 1;
+  return dc_solve(ctx, &o, d_x, 1, d_iters, d_status, d_rung, st);
+}
+
+int32_t esl_op_solve(esl_ctx* ctx, const esl_newton_opts* opts, double* x_out, uint32_t* iters,
+                     uint32_t* status, uint32_t* rung, esl_stats* st) {
+  if (!ctx || !opts || !x_out || ctx->n_lanes == 0) return ESL_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  const size_t N = ctx->n_lanes, n = ctx->pat.n;
+  if (int32_t rc = ensure_lane_buffers(ctx)) return rc;
+  DevBuf d_rung;
+  ESL_CUDA(d_rung.ensure(N * 4));
+  if (int32_t rc = esl_op_solve_device(ctx, opts, ctx->d_x.as<double>(), ctx->d_iters.as<uint32_t>(),
+                                       ctx->d_status.as<uint32_t>(), d_rung.as<uint32_t>(), st))
+    return rc;
+  ESL_CUDA(cudaMemcpyAsync(x_out, ctx->d_x.p, N * n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (iters) ESL_CUDA(cudaMemcpyAsync(iters, ctx->d_iters.p, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  if (status) ESL_CUDA(cudaMemcpyAsync(status, ctx->d_status.p, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  if (rung) ESL_CUDA(cudaMemcpyAsync(rung, d_rung.p, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  ESL_CUDA(cudaStreamSynchronize(ctx->stream));
   return ESL_OK;
 }
 

@@ -362,6 +362,75 @@ uint32_t Csc::slot(uint32_t row, uint32_t col) const {
   return (it != e && *it == row) ? uint32_t(it - row_idx.begin()) : nnz();
 }
 
+// op.zig gminStamps (:531-608): LoadGmin adds gmin to the diagonal that
+// Sparse holds after spMNA_Preorder, which gives each branch-current column
+// without a diagonal (its row's G and C both zero: no device here stamps a
+// capacitance there, so G decides) the position of a +-1 twin: the column
+// is exchanged with the row r whose entry (r, column) and transposed entry
+// (column's position, column r) are both +-1, single twins first, then the
+// first column with several. The ground row takes no load.
+std::vector<uint32_t> gmin_stamps(const Csc& a, const std::vector<uint8_t>& cur_row, const double* g) {
+  const uint32_t n = a.n, none = ~0u;
+  std::vector<uint32_t> perm(n), dcol(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    perm[i] = i;
+    const uint32_t d = a.slot(i, i);
+    const bool zero = d == a.nnz() || g[d] == 0.0;
+    dcol[i] = (i != 0 && cur_row[i] && zero) ? none : i;
+  }
+  // the twins of column position j: how many (stopping at two) and the first
+  auto twins = [&](uint32_t j, uint32_t& first) {
+    uint32_t count = 0;
+    const uint32_t col = perm[j];
+    for (uint32_t p = a.col_ptr[col]; p < a.col_ptr[col + 1]; ++p) {
+      const uint32_t r = a.row_idx[p];
+      if (r == 0 || std::fabs(g[p]) != 1.0) continue;
+      const uint32_t q = a.slot(j, perm[r]);
+      if (q == a.nnz() || std::fabs(g[q]) != 1.0) continue;
+      if (++count == 1)
+        first = r;
+      else
+        break;
+    }
+    return count;
+  };
+  auto exchange = [&](uint32_t j, uint32_t r) {
+    dcol[j] = perm[r];
+    dcol[r] = perm[j];
+    std::swap(perm[j], perm[r]);
+  };
+  uint32_t start = 1;
+  for (;;) {
+    bool swapped = false, again = false;
+    for (uint32_t j = start; j < n; ++j) {
+      if (dcol[j] != none) continue;
+      uint32_t r = 0;
+      const uint32_t t = twins(j, r);
+      if (t == 1) {
+        exchange(j, r);
+        swapped = true;
+      } else if (t > 1 && !again) {
+        again = true;
+        start = j;
+      }
+    }
+    if (!again) break;
+    for (uint32_t j = start; !swapped && j < n; ++j) {
+      if (dcol[j] != none) continue;
+      uint32_t r = 0;
+      if (twins(j, r) > 0) {
+        exchange(j, r);
+        swapped = true;
+      }
+    }
+    if (!swapped) break;
+  }
+  std::vector<uint32_t> out;
+  for (uint32_t i = 1; i < n; ++i)
+    if (dcol[i] != none) out.insert(out.end(), {a.slot(i, dcol[i]), i, dcol[i]});
+  return out;
+}
+
 // order.zig order: Tarjan SCCs of j -> i for A(i, j) != 0 (sink block
 // first), each non-singleton block in AMD or natural order, whichever gives
 // the smaller Cholesky factor of the block's A + A^T.

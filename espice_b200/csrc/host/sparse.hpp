@@ -34,6 +34,11 @@ struct Csc {
 // Column order q[k] = column eliminated at step k (order.zig `order`).
 std::vector<uint32_t> order_columns(const Csc& a);
 
+// The gmin-stepping rung's loads (op.zig gminStamps): (slot, row, column)
+// triples for rows 1 .. n-1 after ngspice's spMNA_Preorder, from the
+// pattern, the current-row flags and an assembled G.
+std::vector<uint32_t> gmin_stamps(const Csc& a, const std::vector<uint8_t>& cur_row, const double* g);
+
 // One sparse LU (sparse_lu.zig SparseLu). L row indices are pivot steps once
 // a factor returns; U columns keep the order the triangular solve visited.
 struct SparseLu {

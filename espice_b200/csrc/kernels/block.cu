@@ -38,6 +38,7 @@
 
 #include "block.h"
 #include "lane_eval.cuh"
+#include "ladder.cuh"
 
 namespace esl {
 
@@ -228,8 +229,9 @@ __device__ __forceinline__ BlockMem<V> block_carve(const BlockDev& D, unsigned c
 // mixed form which also keeps the FP64 sum, and the diagonal copy for the
 // gates) or a residual row (rhs and y = P(-rhs)). Term words arrive two
 // batches of eight ahead, staging values one batch ahead, cells two ahead.
-// gmin > 0 adds loadExtras' diagonal and residual terms. Fill-in tape
-// values are zeroed.
+// gmin > 0 adds loadExtras' diagonal and residual terms; gs > 0 the
+// gmin-stepping rung's at the cells that carry a stamp (c.w: 1 on a stamped
+// slot, the column + 1 on a stamped row). Fill-in tape values are zeroed.
 template <typename V, uint32_t kW>
 __device__ __forceinline__ double gather_term(const BlockMem<V>& b, uint32_t w) {
   return b.m.st[w & ~kGTermEnd];
@@ -237,25 +239,25 @@ __device__ __forceinline__ double gather_term(const BlockMem<V>& b, uint32_t w) 
 
 template <typename V, uint32_t kW>
 __device__ __forceinline__ void gather_store(const BlockDev& D, const BlockMem<V>& b, const uint4& c, double s,
-                                             double gmin) {
+                                             double gmin, double gs) {
   constexpr bool kMixed = sizeof(V) == 4;
   if (c.x & kGCellRow) {
     const uint32_t i = c.x & ~kGCellRow;
     if (gmin > 0.0) s = __dadd_rn(s, __dmul_rn(gmin, b.m.x[i]));
+    if (gs > 0.0 && c.w) s = __dadd_rn(s, __dmul_rn(gs, b.m.x[c.w - 1]));
     b.m.rhs[i] = s;
     b.y[c.y] = V(-s);
   } else {
-    if (c.z != kNoDiag) {
-      if (gmin > 0.0) s = __dadd_rn(s, gmin);
-      b.m.diag[c.z] = s;
-    }
+    if (c.z != kNoDiag && gmin > 0.0) s = __dadd_rn(s, gmin);
+    if (gs > 0.0 && c.w) s = __dadd_rn(s, gs);
+    if (c.z != kNoDiag) b.m.diag[c.z] = s;
     b.v[c.y] = V(s);
     if constexpr (kMixed) b.a64[c.x] = s;
   }
 }
 
 template <typename V, uint32_t kW>
-__device__ void block_assemble(const BlockDev& D, const BlockMem<V>& b, double gmin, int tid) {
+__device__ void block_assemble(const BlockDev& D, const BlockMem<V>& b, double gmin, double gs, int tid) {
   const TopoDev& T = D.T;
   const uint32_t* terms = D.g_terms + tid;
   const uint4* cells = D.g_cells + tid;
@@ -288,7 +290,7 @@ __device__ void block_assemble(const BlockDev& D, const BlockMem<V>& b, double g
     for (int j = 0; j < 8; ++j) {
       s = __dadd_rn(s, val[j]);
       if (w[j] & kGTermEnd) {
-        gather_store<V, kW>(D, b, cell, s, gmin);
+        gather_store<V, kW>(D, b, cell, s, gmin, gs);
         s = 0.0;
         cell = cell1;
         cell1 = c_next < D.g_ncells ? __ldg(cells + size_t(c_next) * kW) : none;
@@ -372,9 +374,10 @@ __device__ __forceinline__ void phase_mark(unsigned long long* prof, uint32_t ph
 // One lane's DC Newton solve (converger.zig newtonLanes at W = 1 with the
 // lane's own direct solver), by the CTA that owns it: the warp lanes'
 // dc_solve_lane step for step, reductions across the CTA.
-template <typename V, typename OpT, bool kHasB3, uint32_t kW>
+template <typename V, typename OpT, bool kHasB3, uint32_t kW, bool kLadder = false>
 __device__ void block_lane(const BlockDev& D, const LaneDev& L, const LaneOpts& o, unsigned char* base,
-                           unsigned char* cold, unsigned char* ring, uint64_t* red, uint32_t lane) {
+                           unsigned char* cold, unsigned char* ring, uint64_t* red, uint32_t lane,
+                           const LadderDev* ld = nullptr) {
   constexpr bool kMixed = sizeof(V) == 4;
   const TopoDev& T = D.T;
   const int tid = threadIdx.x;
@@ -399,13 +402,14 @@ __device__ void block_lane(const BlockDev& D, const LaneDev& L, const LaneOpts& 
   uint32_t flags = L.flags[lane];
   uint32_t iter = L.iters[lane];
   double limit = L.limit[lane];
-  uint32_t max_iter = o.max_iter < 100 ? 100 : o.max_iter;
-  if (o.iter_cap && o.iter_cap < max_iter) max_iter = o.iter_cap;
+  const LadderRun run = ladder_run(o, kLadder ? ld : nullptr);
+  const uint32_t max_iter = run.max_iter;
   uint32_t refinements = 0;
   SimDev sim;
   sim.t = 0.0;
-  sim.src_scale = 1.0;
+  sim.src_scale = run.src;
   sim.kind = 0;
+  sim.gmin = run.gmin_dev;
   bool have_step = false;
   if (resuming) {
     for (uint32_t i = tid; i < n; i += kW) {
@@ -425,7 +429,7 @@ __device__ void block_lane(const BlockDev& D, const LaneDev& L, const LaneOpts& 
       if (tid == 0) m.st[T.n_stage + kGCellX0] = m.x[0];
       __syncthreads();
       phase_mark(D.prof, kBlockPhaseEval, t0);
-      block_assemble<V, kW>(D, b, o.gmin, tid);
+      block_assemble<V, kW>(D, b, o.gmin, run.gs, tid);
       __syncthreads();
       phase_mark(D.prof, kBlockPhaseAssemble, t0);
       if (iter == 0) {
@@ -557,7 +561,7 @@ __device__ void block_lane(const BlockDev& D, const LaneDev& L, const LaneOpts& 
 // (its hot part when split; nothing when all in the slab), then the op ring.
 // Two CTAs an SM by registers (the BSIM3 instantiation spills a few words
 // of its evaluation for it), as many as shared memory then allows.
-template <typename V, typename OpT, bool kHasB3, uint32_t kW>
+template <typename V, typename OpT, bool kHasB3, uint32_t kW, bool kLadder>
 __global__ void __launch_bounds__(kW, 2) dc_block_kernel(BlockDev D, LaneDev L, LaneOpts o) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint64_t red[kW / 32];
@@ -565,7 +569,23 @@ __global__ void __launch_bounds__(kW, 2) dc_block_kernel(BlockDev D, LaneDev L, 
   unsigned char* base = D.in_smem ? smem_raw : own;
   unsigned char* ring = smem_raw + (D.in_smem ? D.lane_bytes : 0u);
   for (uint32_t lane = blockIdx.x; lane < L.n_lanes; lane += gridDim.x) {
-    block_lane<V, OpT, kHasB3, kW>(D, L, o, base, own, ring, red, lane);
+    if constexpr (!kLadder) {
+      block_lane<V, OpT, kHasB3, kW>(D, L, o, base, own, ring, red, lane);
+    } else {
+      // an operating-point lane runs Newton until the ladder is done or the
+      // lane pauses for a host factor (a singular host factor ends a run)
+      for (;;) {
+        const uint32_t st = *(volatile uint32_t*)(L.status + lane);
+        if (st == kRunning || (L.resume && st == kNeedSolve)) {
+          block_lane<V, OpT, kHasB3, kW, true>(D, L, o, base, own, ring, red, lane, L.ladder + lane);
+          __syncthreads();
+          if (*(volatile uint32_t*)(L.status + lane) == kNeedSolve) break;
+        } else if (!(st == kSingular && L.ladder[lane].rung != kRungDone)) {
+          break;
+        }
+        if (!ladder_step(D.T, L, lane, threadIdx.x, kW)) break;
+      }
+    }
     __syncthreads();
   }
 }
@@ -601,7 +621,7 @@ __global__ void __launch_bounds__(kW, 2) dc_block_group_kernel(const BlockDev* _
     }
     __syncthreads();
     block_lane<V, OpT, kHasB3, kW>(D, L, o, D.in_smem ? smem_raw : own_slab, own_slab, smem_raw + ring_at, red,
-                                   w.y);
+                                   w.y, nullptr);
     __syncthreads();
   }
 }
@@ -651,7 +671,14 @@ __global__ void __launch_bounds__(kW) block_lead_kernel(BlockDev D, LaneDev L, u
 
 template <typename V, typename OpT, bool kHasB3>
 cudaError_t launch_t(const BlockDev& D, const LaneDev& L, const LaneOpts& o, cudaStream_t s) {
-  auto* k = dc_block_kernel<V, OpT, kHasB3, kBlockThreads>;
+  // operating-point lanes: the FP64 form with the ladder between runs
+  auto* k = dc_block_kernel<V, OpT, kHasB3, kBlockThreads, false>;
+  if (o.ladder) {
+    if constexpr (sizeof(V) == 8)
+      k = dc_block_kernel<V, OpT, kHasB3, kBlockThreads, true>;
+    else
+      return cudaErrorNotSupported;
+  }
   const size_t smem = (D.in_smem ? D.lane_bytes : 0) + D.ring_bytes;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
@@ -663,7 +690,7 @@ cudaError_t launch_t(const BlockDev& D, const LaneDev& L, const LaneOpts& o, cud
 template <typename V, typename OpT, bool kHasB3>
 int occupancy_t(size_t smem) {
   int per_sm = 0;
-  auto* k = dc_block_kernel<V, OpT, kHasB3, kBlockThreads>;
+  auto* k = dc_block_kernel<V, OpT, kHasB3, kBlockThreads, false>;
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) return 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, int(kBlockThreads), smem);
   return per_sm;

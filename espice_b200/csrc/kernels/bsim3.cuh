@@ -351,9 +351,10 @@ __device__ __forceinline__ void b3_jcur(double v, double isat, double nvt, doubl
 
 // BSIM3 stamp into its 23 staging cells (layout in common.h). `lim` is the
 // instance's three images (vgs, vds, vbs) when limiting is live; a limited
-// instance is linearised back to x.
+// instance is linearised back to x. `gmin` >= 0 replaces the card's junction
+// gmin (the gmin-stepping rung).
 static __device__ __noinline__ void bsim3_stamp(const double* r, int s, double xd, double xg, double xs, double xb,
-                                         double xdi, double xsi, const double* lim, double* st) {
+                                         double xdi, double xsi, const double* lim, double* st, double gmin) {
   auto F = [&](int f) { return r[f * s]; };
   const double type = F(kB3Type), m = F(kB3M);
   const double vgs_r = type * (xg - xsi), vds_r = type * (xdi - xsi), vbs_r = type * (xb - xsi);
@@ -361,9 +362,12 @@ static __device__ __noinline__ void bsim3_stamp(const double* r, int s, double x
   const Dual vds = {lim ? lim[1] : vds_r, 0.0, 1.0, 0.0};
   const Dual vbs = {lim ? lim[2] : vbs_r, 0.0, 0.0, 1.0};
   const Dual vgd = dsub(vgs, vds), vbd = dsub(vbs, vds);
+  // gminx = $simparam("gmin", 1e-12) (bsim3.va:353): the stepping rung's
+  // gmin while it runs, else the card's
+  if (!(gmin >= 0.0)) gmin = F(kB3Gmin);
   double ibs, gbs, ibd, gbd;
-  b3_jcur(vbs.v, F(kB3Isats), F(kB3Nvtmj), F(kB3Vjsm), F(kB3Isevjsm), F(kB3Ijth), F(kB3Gmin), ibs, gbs);
-  b3_jcur(vbd.v, F(kB3Isatd), F(kB3Nvtmj), F(kB3Vjdm), F(kB3Isevjdm), F(kB3Ijth), F(kB3Gmin), ibd, gbd);
+  b3_jcur(vbs.v, F(kB3Isats), F(kB3Nvtmj), F(kB3Vjsm), F(kB3Isevjsm), F(kB3Ijth), gmin, ibs, gbs);
+  b3_jcur(vbd.v, F(kB3Isatd), F(kB3Nvtmj), F(kB3Vjdm), F(kB3Isevjdm), F(kB3Ijth), gmin, ibd, gbd);
   const bool fwd = vds.v >= 0.0;
   Dual id, isub;
   b3_channel(r, s, fwd ? vgs : vgd, fwd ? vds : dneg(vds), fwd ? vbs : vbd, id, isub);

@@ -123,7 +123,7 @@ __device__ void eval_all(const TopoDev& T, const double* rec, const LaneMem& m, 
         case kB3:
           if constexpr (kHasB3)
             bsim3_stamp(r, s, m.x[nd[0]], m.x[nd[1]], m.x[nd[2]], m.x[nd[3]], m.x[nd[4]], m.x[nd[5]],
-                        lim_active ? m.lim + B.lim_off + 3 * i : nullptr, st);
+                        lim_active ? m.lim + B.lim_off + 3 * i : nullptr, st, sim.gmin);
           break;
         default:
           break;

@@ -86,6 +86,11 @@ struct TopoDev {
   const uint32_t* row_ptr;
   const uint32_t* row_slot;
   const uint32_t* row_col;
+  // The gmin-stepping rung's loads (op.zig gminStamps): n_gst triples
+  // (pattern slot, row, column); gmin goes on the slot and gmin x[column]
+  // on the row's residual.
+  const uint32_t* gst;
+  uint32_t n_gst;
 };
 
 // One transient over every lane (tran.zig Sim): options, the probe trace
@@ -203,6 +208,28 @@ __host__ __device__ inline uint32_t sweep_doubles(const TopoDev& T) {
   return (T.smem_doubles + 2 * T.n + T.n_src + 1) & ~1u;
 }
 
+// An operating-point lane's place on op.zig's ladder (solveLadder /
+// afterPlain), in global memory across Newton runs and pauses: the rung of
+// the run in flight, the runs of the stepping loop, the iterations summed
+// over every run, and the stepping state (the gmin descent and the source
+// factor with their last good values).
+struct LadderDev {
+  uint32_t rung;       // LadderRung of the run in flight
+  uint32_t solves;     // runs of the current stepping loop
+  uint32_t total;      // iterations over every run, saturating at 65535
+  uint32_t have_good;  // the gmin loop has a converged point in x_good
+  double factor, good_gmin, gmin_val;
+  double lambda, lambda_good, delta;
+};
+enum LadderRung : uint32_t {
+  kRungPlain = 0,   // rung 1: plain Newton from the cold start (MODEINITFIX)
+  kRungGmin = 1,    // rung 2: a gmin-stepping run
+  kRungClean = 2,   // rung 2's last run, without the shunt
+  kRungSource = 3,  // rung 3: a source-stepping run
+  kRungFinal = 4,   // the full-source Newton after rung 3
+  kRungDone = 5
+};
+
 struct LaneDev {
   uint32_t n_lanes;
   uint32_t resume;        // 1: lanes paused at the solve take the host's dx
@@ -212,7 +239,8 @@ struct LaneDev {
   uint32_t* lim_active;   // [lane]
   uint32_t* status;       // [lane] LaneStatus
   uint32_t* iters;        // [lane]
-  uint32_t* flags;        // [lane] bit 0 INITFIX pending, bit 1 every solve on the host
+  uint32_t* flags;        // [lane] bit 0 INITFIX pending, bit 1 every solve on the host,
+                          // bit 2 the lane's solver factored in an earlier run
   double* limit;          // [lane] runaway bound of this solve
   double* xo;             // [lane][n]  (pause state)
   double* a_vals;         // [lane][nnz] (pause: matrix for the host factor)
@@ -220,6 +248,9 @@ struct LaneDev {
   double* dx;             // [lane][n]   (resume: the host's step)
   double* diag;           // [lane][n]   (pause: assembled diagonal for the gate)
   uint32_t* n_paused;     // device counter
+  LadderDev* ladder;      // [lane] operating-point lanes: the ladder's state
+  double* x_good;         // [lane][n] its last converged stepping point
+  uint32_t* rung_out;     // [lane] the rung that converged (0 plain, 1 gmin, 2 source; 3 none)
 };
 
 }  // namespace esl

@@ -30,6 +30,9 @@ struct SimDev {
   double t;          // time (transient)
   double src_scale;  // source-stepping factor
   int kind;          // 0 static (.op / .dc), 1 transient, 2 transient op
+  // $simparam("gmin") read inside an analog block (BSIM3's junction gminx):
+  // the gmin-stepping rung's value while it runs, negative for the card's
+  double gmin = -1.0;
 };
 
 // PULSE (vsource.va:211-222); p = the source's record fields.

@@ -34,6 +34,7 @@
 #include "models.cuh"
 #include "bsim3.cuh"
 #include "lane_eval.cuh"
+#include "ladder.cuh"
 
 namespace esl {
 
@@ -275,9 +276,11 @@ __device__ __forceinline__ void init_consts(const TopoDev& T, double* v, int tid
 
 // One lane's DC Newton solve (converger.zig newtonLanes at W = 1 with the
 // lane's own direct solver), by the warp that owns it.
-template <bool kHasB3>
+// `ld`: an operating-point lane's ladder state (the run's gmin stamps,
+// source factor and cap), null for a plain DC solve.
+template <bool kHasB3, bool kLadder = false>
 __device__ void dc_solve_lane(const TopoDev& T, const LaneDev& L, const LaneOpts& o, uint32_t prog, double* block,
-                              uint32_t lane, int tid) {
+                              uint32_t lane, int tid, const LadderDev* ld = nullptr) {
   const uint32_t status = L.status[lane];
   const bool resuming = L.resume && status == kNeedSolve;
   if (!(status == kRunning || resuming)) return;
@@ -292,12 +295,13 @@ __device__ void dc_solve_lane(const TopoDev& T, const LaneDev& L, const LaneOpts
   uint32_t flags = L.flags[lane];
   uint32_t iter = L.iters[lane];
   double limit = L.limit[lane];
-  uint32_t max_iter = o.max_iter < 100 ? 100 : o.max_iter;
-  if (o.iter_cap && o.iter_cap < max_iter) max_iter = o.iter_cap;
+  const LadderRun run = ladder_run(o, kLadder ? ld : nullptr);
+  const uint32_t max_iter = run.max_iter;
   SimDev sim;
   sim.t = 0.0;
-  sim.src_scale = 1.0;
+  sim.src_scale = run.src;
   sim.kind = 0;
+  sim.gmin = run.gmin_dev;
   bool have_step = false;
   if (resuming) {
     for (uint32_t i = tid; i < n; i += 32) {
@@ -327,6 +331,21 @@ __device__ void dc_solve_lane(const TopoDev& T, const LaneDev& L, const LaneOpts
           }
         }
         for (uint32_t i = tid; i < n; i += 32) m.rhs[i] += o.gmin * m.x[i];
+        __syncwarp();
+        load_y(T, m.rhs, m.y, tid);
+        __syncwarp();
+      }
+      if (run.gs > 0.0) {
+        // loadGmin at the gmin-stepping stamps (converger.zig:696-713);
+        // every stamp its own row and slot
+        for (uint32_t k = tid; k < T.n_gst; k += 32) {
+          const uint32_t slot = T.gst[3 * k], row = T.gst[3 * k + 1], col = T.gst[3 * k + 2];
+          const uint32_t at = T.amap[slot], dr = T.slot_row[slot];
+          const double d = m.v[at] + run.gs;
+          m.v[at] = d;
+          if (dr != kNoDiag) m.diag[dr] = d;
+          m.rhs[row] += run.gs * m.x[col];
+        }
         __syncwarp();
         load_y(T, m.rhs, m.y, tid);
         __syncwarp();
@@ -433,7 +452,7 @@ __device__ void dc_solve_lane(const TopoDev& T, const LaneDev& L, const LaneOpts
 // DC Newton over independent sweep points (sweep/lanes.zig solveBatch:
 // each lane bitwise its own converger.run), one warp per lane; a persistent
 // grid, each CTA staging the programs once and taking lanes in turn.
-template <bool kHasB3>
+template <bool kHasB3, bool kLadder>
 __global__ void __launch_bounds__(256) dc_newton_kernel(TopoDev T, LaneDev L, LaneOpts o) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* lanes_smem = stage_programs(T, smem_raw);
@@ -442,7 +461,24 @@ __global__ void __launch_bounds__(256) dc_newton_kernel(TopoDev T, LaneDev L, La
   const uint32_t warps = blockDim.x >> 5, w = threadIdx.x >> 5;
   double* block = lanes_smem + size_t(w) * T.smem_doubles;
   for (uint32_t lane = blockIdx.x * warps + w; lane < L.n_lanes; lane += gridDim.x * warps) {
-    dc_solve_lane<kHasB3>(T, L, o, prog, block, lane, tid);
+    if constexpr (!kLadder) {
+      dc_solve_lane<kHasB3>(T, L, o, prog, block, lane, tid);
+      __syncwarp();
+      continue;
+    }
+    // an operating-point lane: Newton runs until the ladder is done or the
+    // lane pauses for a host factor (a singular host factor ends a run)
+    for (;;) {
+      const uint32_t st = *(volatile uint32_t*)(L.status + lane);
+      if (st == kRunning || (L.resume && st == kNeedSolve)) {
+        dc_solve_lane<kHasB3, true>(T, L, o, prog, block, lane, tid, L.ladder + lane);
+        __syncwarp();
+        if (*(volatile uint32_t*)(L.status + lane) == kNeedSolve) break;
+      } else if (!(st == kSingular && L.ladder[lane].rung != kRungDone)) {
+        break;
+      }
+      if (!ladder_step(T, L, lane, tid, 32)) break;
+    }
     __syncwarp();
   }
 }
@@ -533,7 +569,7 @@ template <bool kHasB3>
 static cudaError_t launch_dc_newton_t(const TopoDev& T, const LaneDev& L, const LaneOpts& o, uint32_t lanes_per_block,
                                       cudaStream_t s) {
   const size_t smem = T.prog_bytes + lanes_per_block * lane_smem_bytes(T);
-  auto* k = dc_newton_kernel<kHasB3>;
+  auto* k = o.ladder ? dc_newton_kernel<kHasB3, true> : dc_newton_kernel<kHasB3, false>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   k<<<persistent_grid(k, L.n_lanes, lanes_per_block, smem), 32 * lanes_per_block, smem, s>>>(T, L, o);
@@ -919,26 +955,14 @@ __global__ void lane_init_kernel(TopoDev T, LaneDev L, uint32_t cold, uint32_t i
   L.limit[lane] = 1e9;
   double* lim = L.lim + size_t(lane) * T.nlim;
   for (uint32_t i = 0; i < T.nlim; ++i) lim[i] = 0.0;
+  if (L.ladder) {
+    LadderDev z{};
+    z.rung = kRungPlain;
+    L.ladder[lane] = z;
+  }
   if (!cold) return;
   for (uint32_t i = 0; i < T.n; ++i) L.x[size_t(lane) * T.n + i] = 0.0;
-  const double* rec = L.rec + size_t(lane) * T.rec_size;
-  for (uint32_t b = 0; b < T.n_batches; ++b) {
-    const BatchDev& B = T.b[b];
-    if (B.type == kD)
-      for (uint32_t i = 0; i < B.count; ++i) lim[B.lim_off + i] = rec[B.rec_off + kDVcrit * B.count + i];
-    if (B.type == kM)
-      for (uint32_t i = 0; i < B.count; ++i) {
-        lim[B.lim_off + 3 * i] = rec[B.rec_off + kMSeedVgs * B.count + i];
-        lim[B.lim_off + 3 * i + 1] = 0.0;
-        lim[B.lim_off + 3 * i + 2] = -1.0;
-      }
-    if (B.type == kB3)
-      for (uint32_t i = 0; i < B.count; ++i) {
-        lim[B.lim_off + 3 * i] = rec[B.rec_off + kB3SeedVgs * B.count + i];
-        lim[B.lim_off + 3 * i + 1] = 0.1;
-        lim[B.lim_off + 3 * i + 2] = 0.0;
-      }
-  }
+  cold_images(T, L.rec + size_t(lane) * T.rec_size, lim, 0, 1);
 }
 
 cudaError_t launch_lane_init(const TopoDev& T, const LaneDev& L, bool cold, bool init_fix, cudaStream_t s) {

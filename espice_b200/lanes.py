@@ -23,6 +23,8 @@ LIB_PATH = os.path.join(HERE, "libespice_lanes.so")
 ESL_OK, ESL_INVALID_ARGUMENT, ESL_OUT_OF_MEMORY = 0, 1, 3
 ESL_NOT_ELIGIBLE, ESL_NO_DEVICE, ESL_DEVICE_FAULT, ESL_TIMEOUT = 4, 5, 6, 7
 LANE_CONVERGED, LANE_MAX_ITER, LANE_SINGULAR, LANE_NEED_SOLVE = 1, 2, 3, 4
+# the rung an operating-point lane converged on (esl_op_solve)
+RUNG_PLAIN, RUNG_GMIN, RUNG_SOURCE, RUNG_NONE = 0, 1, 2, 3
 
 # Every entry point include/espice_lanes.h declares.
 EXPORTS = ["esl_create", "esl_destroy", "esl_last_error", "esl_dims", "esl_set_lanes",
@@ -31,7 +33,8 @@ EXPORTS = ["esl_create", "esl_destroy", "esl_last_error", "esl_dims", "esl_set_l
            "esl_lu_lanes_mixed_device", "esl_group_dc_solve_device", "esl_autotune", "esl_dc_sweep_device",
            "esl_tran_meas_device", "esl_lu_lanes_compiled_device", "esl_lu_compiled_log",
            "esl_lu_compiled_source", "esl_lu_lanes_mixed_compiled_device", "esl_lu_compiled_mixed_source",
-           "esl_set_mode", "esl_block_info", "esl_block_profile", "esl_peel_counts"]
+           "esl_set_mode", "esl_block_info", "esl_block_profile", "esl_peel_counts", "esl_op_solve",
+           "esl_op_solve_device"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 f64p = ctypes.POINTER(ctypes.c_double)
@@ -334,6 +337,21 @@ class DcLanes:
                                          _p(it, u32p), _p(st, u32p), ctypes.byref(stats)),
                     "esl_dc_solve")
         return x, it, st, stats.as_dict()
+
+    def op(self, opts=None):
+        """Operating-point lanes (esl_op_solve): every lane's operating point
+        from the cold start through op.zig's ladder. Returns x [lanes][n],
+        iters, status, rung (RUNG_*) and stats."""
+        opts = opts or newton_opts()
+        x = np.zeros((self.n_lanes, self.n))
+        it = np.zeros(self.n_lanes, np.uint32)
+        st = np.zeros(self.n_lanes, np.uint32)
+        rung = np.zeros(self.n_lanes, np.uint32)
+        stats = Stats()
+        self._check(self._L.esl_op_solve(self._ctx, ctypes.byref(opts), _p(x, f64p), _p(it, u32p),
+                                         _p(st, u32p), _p(rung, u32p), ctypes.byref(stats)),
+                    "esl_op_solve")
+        return x, it, st, rung, stats.as_dict()
 
     def solve_device(self, d_x, d_iters, d_status, cold=False, opts=None):
         """Device-buffer solve: pointers (ints) to [lanes][n] f64 and [lanes] u32."""

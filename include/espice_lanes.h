@@ -201,6 +201,30 @@ int32_t esl_dc_solve(esl_ctx *ctx, const esl_newton_opts *opts, const double *x0
 int32_t esl_dc_solve_device(esl_ctx *ctx, const esl_newton_opts *opts, double *d_x, int cold,
                             uint32_t *d_iters, uint32_t *d_status, esl_stats *stats);
 
+/* Operating-point lanes: every lane's operating point from the cold start
+ * through op.zig's continuation ladder (src/analysis/dc/op.zig:84-320,
+ * solveLadder and afterPlain), the batched form of op.solve without holds.
+ * Rung 1 is plain Newton with MODEINITFIX (opts->init_fix is implied);
+ * a lane it leaves unconverged goes on, on the device and without the
+ * host, to dynamic gmin stepping (gmin from 1e-2 down to 1e-12 at ngspice's
+ * diagonal placement, the BSIM3 junction gmin following it; a clean solve
+ * at the end) and then source stepping (V and I sources scaled by an
+ * adaptive lambda) and the full-source Newton. Each stepping run has a
+ * cap of max(itl2, 100) = 100 iterations, the others opts->max_iter (at
+ * least 100); opts->iter_cap caps every run. Rungs 4 (JFNK) and 5 (OPtran)
+ * are not built: a lane that needs them reads ESL_LANE_MAX_ITER. iters:
+ * the plain run's iterations, or the sum over every run once the lane
+ * entered the ladder (saturating at 65535, op.zig's u16); rung: 0 plain,
+ * 1 gmin stepping, 2 source stepping, 3 not converged. Lanes whose factor
+ * leaves the lead tape pause for the host's factor as in esl_dc_solve. */
+int32_t esl_op_solve(esl_ctx *ctx, const esl_newton_opts *opts, double *x_out, uint32_t *iters,
+                     uint32_t *status, uint32_t *rung, esl_stats *stats);
+
+/* esl_op_solve on device buffers: d_x [n_lanes][n] (the solutions out),
+ * d_iters, d_status and d_rung [n_lanes]. */
+int32_t esl_op_solve_device(esl_ctx *ctx, const esl_newton_opts *opts, double *d_x, uint32_t *d_iters,
+                            uint32_t *d_status, uint32_t *d_rung, esl_stats *stats);
+
 /* esl_dc_solve_device without allocating. No counterpart in the reference:
  * its lane solver allocates its lane planes per call.
  *

@@ -195,6 +195,13 @@ int orc_dc_sweep_lanes(const orc_circuit *c, const orc_slot *slots, uint32_t n_s
                        double *x_out, uint32_t *iters, uint8_t *conv);
 
 /* Operating point (op.zig solve, plain rung, cold start). */
+/* Operating points of independent lanes through op.zig's ladder (plain,
+ * gmin stepping, source stepping) from the cold start; rung per lane: 0
+ * plain, 1 gmin, 2 source, 3 not converged. iter_cap (0: none) caps every
+ * Newton run. */
+int orc_op_points(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots, const double *values,
+                  uint32_t n_lanes, const orc_newton_opts *opts, uint32_t iter_cap, double *x_out,
+                  uint32_t *iters, uint8_t *conv, uint8_t *rung);
 int orc_op(const orc_circuit *c, const orc_newton_opts *opts, double *x_out,
            uint32_t *iters);
 

@@ -158,6 +158,26 @@ def dc_points(frozen, slots, values, warm=None, opts=None):
     return x, it, cv
 
 
+def op_points(frozen, slots, values, opts=None, iter_cap=0):
+    """Operating points of independent lanes through op.zig's ladder from the
+    cold start: x [lanes][n], iters, conv, rung (0 plain, 1 gmin stepping,
+    2 source stepping, 3 not converged). iter_cap > 0 caps every Newton run."""
+    opts = opts or newton_opts(max_iter=100)
+    values = np.ascontiguousarray(values, np.float64).reshape(-1, max(1, len(slots)))
+    lanes = values.shape[0]
+    x = np.zeros((lanes, frozen.n))
+    it = np.zeros(lanes, np.uint32)
+    cv = np.zeros(lanes, np.uint8)
+    rung = np.zeros(lanes, np.uint8)
+    sa = frozen.slots_array(slots)
+    rc = lib().orc_op_points(ctypes.byref(frozen.struct()), sa, ctypes.c_uint32(len(slots)),
+                             _p(values, f64p), ctypes.c_uint32(lanes), ctypes.byref(opts),
+                             ctypes.c_uint32(iter_cap), _p(x, f64p), _p(it, u32p), _p(cv, u8p),
+                             _p(rung, u8p))
+    assert rc == 0
+    return x, it, cv, rung
+
+
 def math(which, x, y=None, libm=False):
     """The model code's exp ("exp"), log ("log") or pow ("pow") over arrays."""
     x = np.ascontiguousarray(x, np.float64)

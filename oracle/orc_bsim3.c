@@ -652,7 +652,8 @@ static void b3_channel(const double *q, dual vgsx, dual vdsx, dual vbsx, dual *i
     }
 }
 
-void bsim3_eval(const uint32_t *nd, const double *der, const double *x, const double *lim, devout_t *o) {
+void bsim3_eval(const uint32_t *nd, const double *der, const double *x, const double *lim, double gmin,
+                devout_t *o) {
     memset(o, 0, sizeof(*o));
     const double *q = der;
     const double type = q[BD_TYPE], m = q[BD_M];
@@ -664,9 +665,12 @@ void bsim3_eval(const uint32_t *nd, const double *der, const double *x, const do
     const dual vbs = {vbs_v, 0.0, 0.0, 1.0};
     const dual vgd = dsub(vgs, vds), vbd = dsub(vbs, vds);
 
+    /* gminx = $simparam("gmin", 1e-12) (bsim3.va:353): the stepping rung's
+     * gmin while it runs, else the card's */
+    if (!(gmin >= 0.0)) gmin = q[BD_GMIN];
     double ibs, gbs, ibd, gbd;
-    b3_jcur(vbs.v, q[BD_ISATS], q[BD_NVTMJ], q[BD_VJSM], q[BD_ISEVJSM], q[BD_IJTH], q[BD_GMIN], &ibs, &gbs);
-    b3_jcur(vbd.v, q[BD_ISATD], q[BD_NVTMJ], q[BD_VJDM], q[BD_ISEVJDM], q[BD_IJTH], q[BD_GMIN], &ibd, &gbd);
+    b3_jcur(vbs.v, q[BD_ISATS], q[BD_NVTMJ], q[BD_VJSM], q[BD_ISEVJSM], q[BD_IJTH], gmin, &ibs, &gbs);
+    b3_jcur(vbd.v, q[BD_ISATD], q[BD_NVTMJ], q[BD_VJDM], q[BD_ISEVJDM], q[BD_IJTH], gmin, &ibd, &gbd);
 
     const int fwd = vds.v >= 0.0;
     const dual vdsx = fwd ? vds : dneg(vds);

@@ -37,6 +37,12 @@ typedef struct {
     double ag0, ag1;
     const double *q1, *ip;
     double *av;
+    /* op.zig gmin stepping: gmin `gs` loaded at the n_gst stamps
+     * (slot, row, col) instead of every diagonal, when gs > 0 */
+    double gs;
+    uint32_t iter_cap;          /* 0, or a cap on every Newton run below max_iter */
+    uint32_t n_gst;
+    uint32_t *gst;
 } ckt_t;
 
 int ckt_init(ckt_t *k, const orc_circuit *c);
@@ -49,6 +55,8 @@ void ckt_cold_start(ckt_t *k, double *x);
 int ckt_newton(ckt_t *k, double *x, const orc_newton_opts *opts, int init_fix, uint32_t *iters);
 uint32_t ckt_qtape(ckt_t *k, const double *x, double *out);
 int ckt_run(ckt_t *k, double *x, const orc_newton_opts *opts, int init_fix, uint32_t *iters);
+uint32_t ckt_gmin_stamps(const ckt_t *k, uint32_t *out);
+int ckt_ladder(ckt_t *k, double *x, const orc_newton_opts *opts, uint32_t *iters, uint32_t *rung);
 double update_and_norm(uint32_t n, double *x, const double *dx, double *x_old, const uint8_t *cur,
                        double reltol, double abstol, double vntol);
 

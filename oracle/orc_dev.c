@@ -510,7 +510,7 @@ void dev_eval(uint32_t type, const uint32_t *nd, const double *prm, const double
         mos1_eval(nd, prm, der, x, lim, st, sim, o);
         break;
     case ORC_B3:
-        bsim3_eval(nd, der, x, lim, o);
+        bsim3_eval(nd, der, x, lim, sim->gmin, o);
         break;
     default:
         break;
@@ -574,6 +574,7 @@ int orc_dev_stamp(uint32_t type, const double *prm, const double *xloc, double *
     sim_t sim;
     memset(&sim, 0, sizeof(sim));
     sim.src_scale = 1.0;
+    sim.gmin = -1.0;
     sim.iteration = 1;
     devout_t o;
     dev_eval(type, nd, prm, der, xloc, NULL, NULL, &sim, &o);

@@ -95,6 +95,9 @@ typedef struct {
     int kind;          /* 0 static (.op/.dc), 1 transient, 2 transient op (ic) */
     double t;
     double src_scale;
+    double gmin;        /* $simparam("gmin") read in an analog block (BSIM3's
+                           junction gminx): the gmin-stepping rung's value,
+                           negative for the card's */
     uint32_t iteration; /* $simparam("iteration"), 1 on a solve's first */
     int initial_tran;   /* first transient step (MODEINITTRAN) */
 } sim_t;
@@ -154,7 +157,8 @@ void mos1_derive(const double *prm, double *der);
 void mos1_eval(const uint32_t *nd, const double *prm, const double *der, const double *x,
                const double *lim, const double *st, const sim_t *sim, devout_t *o);
 void bsim3_derive(const double *prm, double *der);
-void bsim3_eval(const uint32_t *nd, const double *der, const double *x, const double *lim, devout_t *o);
+void bsim3_eval(const uint32_t *nd, const double *der, const double *x, const double *lim, double gmin,
+                devout_t *o);
 int bsim3_limit(const uint32_t *nd, const double *der, const double *x, const double *x_old,
                 const double *lim_old, double *lim_new);
 int bsim3_seed(const double *der, double *lim);

@@ -83,6 +83,7 @@ int ckt_init(ckt_t *k, const orc_circuit *c) {
     k->av = (double *)calloc(k->nnz + 1, sizeof(double));
     k->sim.kind = 0;
     k->sim.src_scale = 1.0;
+    k->sim.gmin = -1.0;
     k->sim.iteration = 1;
     dsv_init(&k->dsv, n, k->cp, k->ri);
     return 0;
@@ -99,6 +100,7 @@ void ckt_free(ckt_t *k) {
     free(k->bt);
     free(k->cp); free(k->ri); free(k->diag); free(k->lim); free(k->lim_new); free(k->st);
     free(k->g); free(k->cv); free(k->rhs); free(k->q); free(k->dx); free(k->x_old); free(k->av);
+    free(k->gst);
     dsv_free(&k->dsv);
     memset(k, 0, sizeof(*k));
 }
@@ -240,6 +242,7 @@ static double residual_gate(const orc_newton_opts *o, double diag, double xi) {
 int ckt_newton(ckt_t *k, double *x, const orc_newton_opts *opts, int init_fix, uint32_t *iters) {
     uint32_t n = k->n;
     uint32_t max_iter = opts->max_iter < 100 ? 100 : opts->max_iter;
+    if (k->iter_cap && k->iter_cap < max_iter) max_iter = k->iter_cap;
     double limit = X_PLAUSIBLE;
     k->sim.iteration = 1;
     for (uint32_t iter = 0; iter < max_iter; iter++) {
@@ -259,6 +262,11 @@ int ckt_newton(ckt_t *k, double *x, const orc_newton_opts *opts, int init_fix, u
         if (opts->gmin > 0) {
             for (uint32_t i = 0; i < n; i++) v[k->diag[i]] += opts->gmin;
             for (uint32_t i = 0; i < n; i++) k->rhs[i] += opts->gmin * x[i];
+        }
+        if (k->gs > 0) {
+            /* converger.loadGmin with gmin_stamps (converger.zig:696-713) */
+            for (uint32_t e = 0; e < k->n_gst; e++) v[k->gst[3 * e]] += k->gs;
+            for (uint32_t e = 0; e < k->n_gst; e++) k->rhs[k->gst[3 * e + 1]] += k->gs * x[k->gst[3 * e + 2]];
         }
         if (iter == 0) limit = plausible_limit(k, x, k->rhs, v);
         if (dsv_factor(&k->dsv, v) != 0) {
@@ -340,6 +348,209 @@ int ckt_run(ckt_t *k, double *x, const orc_newton_opts *opts, int init_fix, uint
 }
 
 /* ------------------------------------------------------------------ */
+/* the operating-point ladder (op.zig solveLadder / afterPlain)        */
+
+#define LADDER_GMIN_START 1e-2   /* Tolerances.gmin_start (numerics.zig:389) */
+#define LADDER_GMIN_TARGET 1e-12 /* Tolerances.gmin */
+#define LADDER_ITL2 50u          /* Tolerances.itl2 */
+
+/* CountTwins of op.zig gminStamps (:560-575): in column position j, the
+ * +-1 entries (ground row skipped) whose transposed entry, row j at
+ * original column perm[r], is +-1 too; counting stops at two. */
+static uint32_t count_twins(const ckt_t *k, const uint32_t *perm, uint32_t j, uint32_t *twin) {
+    uint32_t col = perm[j], count = 0;
+    for (uint32_t p = k->cp[col]; p < k->cp[col + 1]; p++) {
+        uint32_t r = k->ri[p];
+        if (r == 0 || fabs(k->g[p]) != 1.0) continue;
+        uint32_t q = find_slot(k->cp, k->ri, k->nnz, j, perm[r]);
+        if (q == k->nnz || fabs(k->g[q]) != 1.0) continue;
+        count++;
+        if (count == 1) *twin = r;
+        else break;
+    }
+    return count;
+}
+
+/* op.zig gminStamps (:531-608): ngspice's diagonal-gmin placement. Rows
+ * whose unknown is a branch current with nothing on the diagonal (G and C
+ * both zero in the current planes) have no diagonal; spMNA_Preorder swaps
+ * such a column with the twin of a +-1 pair, lone twins first, then the
+ * first column with several. Writes (slot, row, col) triples for rows 1..n-1
+ * that end with a diagonal; returns their count. */
+uint32_t ckt_gmin_stamps(const ckt_t *k, uint32_t *out) {
+    const uint32_t n = k->n, none = 0xffffffffu;
+    uint32_t *perm = (uint32_t *)malloc(sizeof(uint32_t) * (n ? n : 1));
+    uint32_t *dcol = (uint32_t *)malloc(sizeof(uint32_t) * (n ? n : 1));
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t d = k->diag[i];
+        perm[i] = i;
+        dcol[i] = (k->c->current_row[i] && k->g[d] == 0.0 && k->cv[d] == 0.0) ? none : i;
+    }
+    uint32_t start = 1;
+    for (;;) {
+        int swapped = 0, again = 0;
+        for (uint32_t j = start; j < n; j++) {
+            if (dcol[j] != none) continue;
+            uint32_t r = 0, t = count_twins(k, perm, j, &r);
+            if (t == 1) {
+                dcol[j] = perm[r]; dcol[r] = perm[j];
+                uint32_t tmp = perm[j]; perm[j] = perm[r]; perm[r] = tmp;
+                swapped = 1;
+            } else if (t > 1 && !again) {
+                again = 1;
+                start = j;
+            }
+        }
+        if (!again) break;
+        for (uint32_t j = start; !swapped && j < n; j++) {
+            if (dcol[j] != none) continue;
+            uint32_t r = 0, t = count_twins(k, perm, j, &r);
+            if (t > 0) {
+                dcol[j] = perm[r]; dcol[r] = perm[j];
+                uint32_t tmp = perm[j]; perm[j] = perm[r]; perm[r] = tmp;
+                swapped = 1;
+            }
+        }
+        if (!swapped) break;
+    }
+    uint32_t m = 0;
+    for (uint32_t i = 1; i < n; i++) {
+        if (dcol[i] == none) continue;
+        out[3 * m] = find_slot(k->cp, k->ri, k->nnz, i, dcol[i]);
+        out[3 * m + 1] = i;
+        out[3 * m + 2] = dcol[i];
+        m++;
+    }
+    free(perm);
+    free(dcol);
+    return m;
+}
+
+/* op.zig newtonRun: one converger.run with the rung's gmin stamps, source
+ * factor and Newton cap; a singular Jacobian is a failed solve of zero
+ * iterations. Returns 1 converged. */
+static int ladder_run(ckt_t *k, double *x, const orc_newton_opts *opts, uint32_t max_iter, double gs,
+                      double src, int init_fix, uint32_t *iters) {
+    orc_newton_opts o = *opts;
+    o.gmin = 0.0;
+    o.max_iter = max_iter;
+    k->gs = gs;
+    k->sim.gmin = gs > 0 ? gs : -1.0;
+    k->sim.src_scale = src;
+    uint32_t it = 0;
+    int rc = ckt_run(k, x, &o, init_fix, &it);
+    k->gs = 0.0;
+    k->sim.gmin = -1.0;
+    k->sim.src_scale = 1.0;
+    *iters = rc == 2 ? 0 : it;
+    return rc == 0;
+}
+
+static uint32_t sat_add16(uint32_t a, uint32_t b) {
+    uint32_t s = a + b;
+    return s > 65535u ? 65535u : s;
+}
+
+/* op.zig solveLadder from a cold start, without holds: rung 1 plain Newton
+ * (MODEINITFIX), rung 2 dynamic gmin stepping (cktop.c dynamic_gmin: the
+ * descent, the 4th-root back-off toward the last good gmin, the clean solve
+ * at the target), rung 3 adaptive source stepping, then the full-source
+ * Newton. Rungs 4 (JFNK) and 5 (OPtran) are not restated: a point that
+ * needs them reads not converged. `x` holds the cold start. Returns 1
+ * converged; *iters the plain run's iterations, or the sum over every run
+ * (saturating at 65535) once the ladder is entered; *rung the rung that
+ * converged (0 plain, 1 gmin, 2 source; 3 none). */
+int ckt_ladder(ckt_t *k, double *x, const orc_newton_opts *opts, uint32_t *iters, uint32_t *rung) {
+    const uint32_t n = k->n;
+    const uint32_t itl1 = opts->max_iter, itl2 = LADDER_ITL2;
+    uint32_t it = 0;
+    *rung = 0;
+    if (ladder_run(k, x, opts, itl1, 0.0, 1.0, 1, &it)) {
+        *iters = it;
+        return 1;
+    }
+    uint32_t total = it;
+    double *x_good = (double *)malloc(sizeof(double) * (n ? n : 1));
+    if (!k->gst) k->gst = (uint32_t *)malloc(sizeof(uint32_t) * 3 * (n ? n : 1));
+    k->n_gst = ckt_gmin_stamps(k, k->gst);
+
+    /* rung 2: dynamic gmin stepping (op.zig:158-227) */
+    {
+        ckt_cold_start(k, x);
+        double factor = 10.0, good = LADDER_GMIN_START, g = good / factor;
+        int have_good = 0;
+        for (uint32_t solves = 0; solves < 100; solves++) {
+            int conv = ladder_run(k, x, opts, itl2, g, 1.0, !have_good, &it);
+            total = sat_add16(total, it);
+            if (conv) {
+                if (g <= LADDER_GMIN_TARGET) {
+                    conv = ladder_run(k, x, opts, itl1, 0.0, 1.0, 0, &it);
+                    total = sat_add16(total, it);
+                    if (conv) {
+                        free(x_good);
+                        *iters = total;
+                        *rung = 1;
+                        return 1;
+                    }
+                    break;
+                }
+                memcpy(x_good, x, sizeof(double) * n);
+                have_good = 1;
+                good = g;
+                if (it <= itl2 / 4) {
+                    double f = factor * sqrt(factor);
+                    factor = f < 10.0 ? f : 10.0;
+                } else if (it > 3 * itl2 / 4) {
+                    double f = sqrt(factor);
+                    factor = f > 1.00005 ? f : 1.00005;
+                }
+                if (g < factor * LADDER_GMIN_TARGET) {
+                    factor = g / LADDER_GMIN_TARGET;
+                    g = LADDER_GMIN_TARGET;
+                } else {
+                    g = g / factor;
+                }
+            } else {
+                if (factor < 1.00005) break;
+                factor = sqrt(sqrt(factor));
+                g = good / factor;
+                if (have_good) memcpy(x, x_good, sizeof(double) * n);
+                else ckt_cold_start(k, x);
+            }
+        }
+    }
+
+    /* rung 3: source stepping (op.zig:229-279) */
+    ckt_cold_start(k, x);
+    {
+        double lambda = 0.0, lambda_good = -1.0, delta = 0.25;
+        for (uint32_t solves = 0; solves < 100; solves++) {
+            int conv = ladder_run(k, x, opts, itl2, 0.0, lambda, lambda_good < 0.0, &it);
+            total = sat_add16(total, it);
+            if (conv) {
+                if (lambda >= 1.0) break;
+                lambda_good = lambda;
+                memcpy(x_good, x, sizeof(double) * n);
+                delta *= 1.5;
+                lambda = lambda + delta < 1.0 ? lambda + delta : 1.0;
+            } else {
+                delta *= 0.5;
+                if (delta < 1e-4) break;
+                if (lambda_good < 0.0) break;
+                memcpy(x, x_good, sizeof(double) * n);
+                lambda = lambda_good + delta < 1.0 ? lambda_good + delta : 1.0;
+            }
+        }
+    }
+    int conv = ladder_run(k, x, opts, itl1, 0.0, 1.0, 0, &it);
+    total = sat_add16(total, it);
+    free(x_good);
+    *iters = total;
+    *rung = conv ? 2 : 3;
+    return conv;
+}
+
+/* ------------------------------------------------------------------ */
 /* entry points                                                        */
 
 int orc_dc_points(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots,
@@ -393,13 +604,40 @@ int orc_dc_points_trace(const orc_circuit *c, const orc_slot *slots, uint32_t n_
     return 0;
 }
 
+/* Operating-point lanes: every lane's parameters installed, then op.zig's
+ * ladder from the cold start (ckt_ladder), each lane with its own solver.
+ * iter_cap (0: none) caps every Newton run of the ladder, as the lanes'
+ * iter_cap option does. */
+int orc_op_points(const orc_circuit *c, const orc_slot *slots, uint32_t n_slots, const double *values,
+                  uint32_t n_lanes, const orc_newton_opts *opts, uint32_t iter_cap, double *x_out,
+                  uint32_t *iters, uint8_t *conv, uint8_t *rung) {
+    uint32_t n = c->n;
+    for (uint32_t l = 0; l < n_lanes; l++) {
+        ckt_t k;
+        if (ckt_init(&k, c)) return 1;
+        k.iter_cap = iter_cap;
+        for (uint32_t s = 0; s < n_slots; s++) ckt_set(&k, slots[s], values[(size_t)l * n_slots + s]);
+        double *x = x_out + (size_t)l * n;
+        ckt_cold_start(&k, x);
+        uint32_t it = 0, r = 0;
+        conv[l] = (uint8_t)ckt_ladder(&k, x, opts, &it, &r);
+        iters[l] = it;
+        rung[l] = (uint8_t)r;
+        ckt_free(&k);
+    }
+    return 0;
+}
+
+/* op.solve without holds: the ladder from the cold start. Returns 0
+ * converged, 1 not. */
 int orc_op(const orc_circuit *c, const orc_newton_opts *opts, double *x_out, uint32_t *iters) {
     ckt_t k;
     if (ckt_init(&k, c)) return -1;
     ckt_cold_start(&k, x_out);
-    int rc = ckt_run(&k, x_out, opts, 1, iters);
+    uint32_t rung = 0;
+    int conv = ckt_ladder(&k, x_out, opts, iters, &rung);
     ckt_free(&k);
-    return rc;
+    return conv ? 0 : 1;
 }
 
 /* One sequential sweep on an initialized circuit (dc.zig Sweep :163-386). */

@@ -23,6 +23,7 @@ FIXTURES = [
     "dc/diode_reverse",
     "dc/diode_reverse_continuation",
     "dc/bench_power_zener_reg",
+    "convergence/bench_mos_latch_ladder",
     "dc/device_diode_temp",
     # operating points
     "convergence/diode_stack_8",

@@ -179,3 +179,20 @@ def test_analog_block_mixed_adaptive_refinement():
         print(f"refine_skip {skip:g}: {stats['refinements']} corrections, iterations {itm.mean():.2f} "
               f"(oracle {ito.mean():.2f})")
     assert refs[1e3] < refs[0.0]
+
+
+def test_mesh_gates_20k_unknowns_slab_lanes():
+    """A 20,001-unknown mesh with 1,666 BSIM3 gates (the large transient
+    configuration's size) as 16 DC lanes with the working set in the per-CTA
+    global slab: every lane converges, two lanes bitwise the oracle's with
+    the same iteration counts."""
+    fr, slots = decks.mesh_gates(20000)
+    values = np.linspace(0.8, 1.8, 16).reshape(-1, 1)
+    xb, itb, stb, stats, info = _solve(fr, slots, values)
+    assert fr.n == 20001 and not info["in_smem"][0]
+    assert (stb == lanes.LANE_CONVERGED).all()
+    xo, ito, cvo = oracle.dc_points(fr, slots, values[:2], warm=None)
+    assert cvo.all() and np.array_equal(itb[:2], ito)
+    assert np.array_equal(xb[:2].view(np.uint64), xo.view(np.uint64))
+    print(f"20k lanes: {stats['kernel_ms']:.1f} ms for 16 lanes, {itb.mean():.2f} iterations, "
+          f"{info['a_rows']} rows in program A over {info['a_levels']} levels")

@@ -61,7 +61,9 @@ def _op(fr, opts):
     return oracle.op(fr, oracle.newton_opts(max_iter=100, **opts))
 
 
-DC_FIXTURES = [n for n in gu.names("dc__")]
+# every DC sweep fixture, and the reference's ladder deck (a MOS1 latch whose
+# sweep restarts cold three times)
+DC_FIXTURES = [n for n in gu.names("dc__")] + ["convergence__bench_mos_latch_ladder"]
 
 # Sweeps that cross into reverse breakdown need other pivots than the lead
 # tape built at their first point: their lanes pause there and take the
