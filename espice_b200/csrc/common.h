@@ -136,6 +136,7 @@ struct LaneOpts {
   uint32_t init_fix;
   uint32_t iter_cap;  // 0 or a hard cap below max_iter
   uint32_t ladder;    // 1: operating-point lanes, op.zig's ladder between Newton runs
+  double gstamp;      // lane_newton: the gmin-stepping rung's gmin at the stamps (0: none)
 };
 
 // Lane status words (device -> host).

@@ -1694,6 +1694,11 @@ int32_t esl_dc_sweep_device(esl_ctx* ctx, const esl_slot* slot, const double* va
   ESL_CUDA(cudaMemsetAsync(L.status, 0, size_t(N) * 4, s));
   ESL_CUDA(cudaMemsetAsync(L.flags, 0, size_t(N) * 4, s));
   ESL_CUDA(cudaMemsetAsync(L.n_paused, 0, 4, s));
+  // a cold point's ladder: its state across pauses, its last good point
+  ESL_CUDA(ctx->d_ladder.ensure(size_t(N) * sizeof(LadderDev)));
+  ESL_CUDA(ctx->d_x_good.ensure(size_t(N) * T.n * 8));
+  L.ladder = ctx->d_ladder.as<LadderDev>();
+  L.x_good = ctx->d_x_good.as<double>();
   ctx->peel.clear();
   ESL_CUDA(ctx->d_next_lane.ensure(sizeof(uint32_t)));
   P.next_lane = ctx->d_next_lane.as<uint32_t>();

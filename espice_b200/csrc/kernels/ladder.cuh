@@ -84,32 +84,31 @@ __device__ __forceinline__ void ladder_sync(uint32_t width) {
     __syncthreads();
 }
 
-// The lane's Newton run has ended (status kConverged, kMaxIter or kSingular,
-// its end point in L.x): the ladder's next step, by every thread of the
-// lane's warp (width 32) or CTA. Returns true when it set up another run
-// (status kRunning, its start in L.x and L.lim), false when the lane is
-// done (its iterations: the plain run's, or the sum over every run once the
-// ladder was entered; rung_out the rung that converged).
-static __device__ __noinline__ bool ladder_step(const TopoDev& T, const LaneDev& L, uint32_t lane, int tid,
-                                         uint32_t width) {
-  ladder_sync(width);
-  LadderDev s = L.ladder[lane];
-  const uint32_t st = *(volatile uint32_t*)(L.status + lane);
-  const bool conv = st == kConverged;
-  // a singular Jacobian is a failed run of zero iterations (newtonRun)
-  const uint32_t it = st == kSingular ? 0u : *(volatile uint32_t*)(L.iters + lane);
-  const uint32_t n = T.n;
-  double* x = L.x + size_t(lane) * n;
-  double* xg = L.x_good + size_t(lane) * n;
-  enum { kKeep, kCold, kGood } start = kKeep;
-  bool save = false, done = false, to_source = false, to_final = false, init_fix = false;
-  uint32_t result = 3, report = 0;
+// Where the ladder's next run starts: the run's own end point, the cold
+// start (zero, junction seeds), or the last converged stepping point.
+enum LadderStart : uint32_t { kStartKeep = 0, kStartCold = 1, kStartGood = 2 };
+
+// The ladder's step after a run (converged or not, `it` its iterations, 0
+// for a singular Jacobian), on the lane's state `s`: the next run's start
+// and INITFIX, whether the run's end point becomes the last good point, or
+// that the lane is done (result: 0 plain, 1 gmin, 2 source, 3 none; report:
+// the plain run's iterations, or the sum over every run once the ladder
+// was entered). Pure: every thread of the lane computes the same move.
+struct LadderMove {
+  uint32_t start;
+  bool save, done, init_fix;
+  uint32_t result, report;
+};
+
+__device__ __forceinline__ LadderMove ladder_decide(LadderDev& s, bool conv, uint32_t it) {
+  LadderMove mv{kStartKeep, false, false, false, 3u, 0u};
+  bool to_source = false, to_final = false;
   switch (s.rung) {
     case kRungPlain:
       if (conv) {
-        done = true;
-        result = 0;
-        report = it;
+        mv.done = true;
+        mv.result = 0;
+        mv.report = it;
         break;
       }
       // rung 2 from the cold start: gmin_start / 10 first
@@ -120,8 +119,8 @@ static __device__ __noinline__ bool ladder_step(const TopoDev& T, const LaneDev&
       s.gmin_val = div_rn(kLadderGminStart, 10.0);
       s.have_good = 0;
       s.solves = 0;
-      start = kCold;
-      init_fix = true;
+      mv.start = kStartCold;
+      mv.init_fix = true;
       break;
     case kRungGmin:
       s.total = ladder_sat(s.total, it);
@@ -131,7 +130,7 @@ static __device__ __noinline__ bool ladder_step(const TopoDev& T, const LaneDev&
           s.rung = kRungClean;
           break;
         }
-        save = true;
+        mv.save = true;
         s.have_good = 1;
         s.good_gmin = s.gmin_val;
         // an easy step accelerates (capped at 10), a hard one slows down
@@ -155,20 +154,20 @@ static __device__ __noinline__ bool ladder_step(const TopoDev& T, const LaneDev&
         }
         s.factor = sqrt(sqrt(s.factor));
         s.gmin_val = div_rn(s.good_gmin, s.factor);
-        start = s.have_good ? kGood : kCold;
+        mv.start = s.have_good ? kStartGood : kStartCold;
       }
       if (++s.solves >= 100) {
         to_source = true;  // rung 3 starts cold whatever x holds
         break;
       }
-      init_fix = !s.have_good;
+      mv.init_fix = !s.have_good;
       break;
     case kRungClean:
       s.total = ladder_sat(s.total, it);
       if (conv) {
-        done = true;
-        result = 1;
-        report = s.total;
+        mv.done = true;
+        mv.result = 1;
+        mv.report = s.total;
         break;
       }
       to_source = true;
@@ -181,7 +180,7 @@ static __device__ __noinline__ bool ladder_step(const TopoDev& T, const LaneDev&
           break;
         }
         s.lambda_good = s.lambda;
-        save = true;
+        mv.save = true;
         s.delta *= 1.5;
         s.lambda = s.lambda + s.delta < 1.0 ? s.lambda + s.delta : 1.0;
       } else {
@@ -190,20 +189,20 @@ static __device__ __noinline__ bool ladder_step(const TopoDev& T, const LaneDev&
           to_final = true;
           break;
         }
-        start = kGood;
+        mv.start = kStartGood;
         s.lambda = s.lambda_good + s.delta < 1.0 ? s.lambda_good + s.delta : 1.0;
       }
       if (++s.solves >= 100) {
         to_final = true;  // from x as the last run left it, or the restored good point
         break;
       }
-      init_fix = s.lambda_good < 0.0;
+      mv.init_fix = s.lambda_good < 0.0;
       break;
     default:  // kRungFinal
       s.total = ladder_sat(s.total, it);
-      done = true;
-      result = conv ? 2 : 3;
-      report = s.total;
+      mv.done = true;
+      mv.result = conv ? 2 : 3;
+      mv.report = s.total;
       break;
   }
   if (to_source) {
@@ -213,39 +212,58 @@ static __device__ __noinline__ bool ladder_step(const TopoDev& T, const LaneDev&
     s.lambda_good = -1.0;
     s.delta = 0.25;
     s.solves = 0;
-    start = kCold;
-    init_fix = true;
+    mv.start = kStartCold;
+    mv.init_fix = true;
   }
   if (to_final) {
     // the full-source Newton from where the stepping left x
     s.rung = kRungFinal;
-    init_fix = false;
+    mv.init_fix = false;
   }
-  if (done) s.rung = kRungDone;
-  if (save)
+  if (mv.done) s.rung = kRungDone;
+  return mv;
+}
+
+// The lane's Newton run has ended (status kConverged, kMaxIter or kSingular,
+// its end point in L.x): the ladder's next step, by every thread of the
+// lane's warp (width 32) or CTA. Returns true when it set up another run
+// (status kRunning, its start in L.x and L.lim), false when the lane is
+// done (its iterations the move's report, rung_out its result).
+static __device__ __noinline__ bool ladder_step(const TopoDev& T, const LaneDev& L, uint32_t lane, int tid,
+                                                uint32_t width) {
+  ladder_sync(width);
+  LadderDev s = L.ladder[lane];
+  const uint32_t st = *(volatile uint32_t*)(L.status + lane);
+  // a singular Jacobian is a failed run of zero iterations (newtonRun)
+  const uint32_t it = st == kSingular ? 0u : *(volatile uint32_t*)(L.iters + lane);
+  const LadderMove mv = ladder_decide(s, st == kConverged, it);
+  const uint32_t n = T.n;
+  double* x = L.x + size_t(lane) * n;
+  double* xg = L.x_good + size_t(lane) * n;
+  if (mv.save)
     for (uint32_t i = tid; i < n; i += width) xg[i] = x[i];
-  if (start == kGood)
+  if (mv.start == kStartGood)
     for (uint32_t i = tid; i < n; i += width) x[i] = xg[i];
-  if (start == kCold) {
+  if (mv.start == kStartCold) {
     for (uint32_t i = tid; i < n; i += width) x[i] = 0.0;
     cold_images(T, L.rec + size_t(lane) * T.rec_size, L.lim + size_t(lane) * T.nlim, tid, width);
   }
   ladder_sync(width);
   if (tid == 0) {
     L.ladder[lane] = s;
-    if (done) {
-      L.iters[lane] = report;
-      if (L.rung_out) L.rung_out[lane] = result;
+    if (mv.done) {
+      L.iters[lane] = mv.report;
+      if (L.rung_out) L.rung_out[lane] = mv.result;
     } else {
       L.status[lane] = kRunning;
       L.iters[lane] = 0;
-      L.flags[lane] = (L.flags[lane] & 2u) | 4u | (init_fix ? 1u : 0u);
-      L.lim_active[lane] = start == kCold && T.nlim ? 1u : 0u;
+      L.flags[lane] = (L.flags[lane] & 2u) | 4u | (mv.init_fix ? 1u : 0u);
+      L.lim_active[lane] = mv.start == kStartCold && T.nlim ? 1u : 0u;
       L.limit[lane] = 1e9;
     }
   }
   ladder_sync(width);
-  return !done;
+  return !mv.done;
 }
 
 }  // namespace esl

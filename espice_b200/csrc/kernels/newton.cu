@@ -1138,6 +1138,20 @@ __device__ int lane_newton(const TopoDev& T, uint32_t prog, const LaneMem& m, co
       load_y(T, m.rhs, m.y, tid);
       __syncwarp();
     }
+    if (o.gstamp > 0.0) {
+      // loadGmin at the gmin-stepping stamps (converger.zig:696-713)
+      for (uint32_t k = tid; k < T.n_gst; k += 32) {
+        const uint32_t slot = T.gst[3 * k], row = T.gst[3 * k + 1], col = T.gst[3 * k + 2];
+        const uint32_t at = T.amap[slot], dr = T.slot_row[slot];
+        const double d = m.v[at] + o.gstamp;
+        m.v[at] = d;
+        if (dr != kNoDiag) m.diag[dr] = d;
+        m.rhs[row] += o.gstamp * m.x[col];
+      }
+      __syncwarp();
+      load_y(T, m.rhs, m.y, tid);
+      __syncwarp();
+    }
     if (iter == 0) {
       double g = 1.0;
       uint64_t xm = 0, fm = 0;
@@ -2039,22 +2053,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
 template <bool kHasB3>
 __device__ void sweep_seed(const TopoDev& T, const double* rec, const LaneMem& m, int tid) {
   for (uint32_t i = tid; i < T.n; i += 32) m.x[i] = 0.0;
-  for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
-    const BatchDev& B = T.b[bi];
-    for (uint32_t i = tid; i < B.count; i += 32) {
-      if (B.type == kD) m.lim[B.lim_off + i] = rec[B.rec_off + kDVcrit * B.count + i];
-      if (B.type == kM) {
-        m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kMSeedVgs * B.count + i];
-        m.lim[B.lim_off + 3 * i + 1] = 0.0;
-        m.lim[B.lim_off + 3 * i + 2] = -1.0;
-      }
-      if (B.type == kB3) {
-        m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kB3SeedVgs * B.count + i];
-        m.lim[B.lim_off + 3 * i + 1] = 0.1;
-        m.lim[B.lim_off + 3 * i + 2] = 0.0;
-      }
-    }
-  }
+  cold_images(T, rec, m.lim, tid, 32);
 }
 
 // A sweep lane (dc.zig Sweep, one per lane): per point, the predictor
@@ -2120,7 +2119,7 @@ __device__ void sweep_lane(const TopoDev& T, const LaneDev& L, const SweepDev& P
     }
   }
   // Pause: the lane's state for the host and for the resume launch.
-  auto pause = [&](uint32_t pt, uint32_t phase, uint32_t it_total) {
+  auto pause = [&](uint32_t pt, uint32_t phase, uint32_t it_total, bool fresh) {
     const size_t at = size_t(lane) * n;
     gather_pattern(T, m, L.a_vals + size_t(lane) * T.nnz, tid);
     for (uint32_t i = tid; i < n; i += 32) {
@@ -2143,7 +2142,7 @@ __device__ void sweep_lane(const TopoDev& T, const LaneDev& L, const SweepDev& P
       L.flags[lane] |= 2u;
       // the lane's first factor of all is its own fresh factor; a later
       // one continues the lead tape's history
-      L.iters[lane] = (pt == 0 && carry.iter == 0) ? 0u : 1u;
+      L.iters[lane] = fresh ? 0u : 1u;
       L.status[lane] = kNeedSolve;
       atomicAdd(L.n_paused, 1u);
     }
@@ -2162,9 +2161,54 @@ __device__ void sweep_lane(const TopoDev& T, const LaneDev& L, const SweepDev& P
       }
     }
     __syncwarp();
+    // The point's Newton runs through one call site: the warm run (stage 0)
+    // and, when it fails or no point has converged yet, the cold ladder's
+    // runs (stage 2; dc.zig endPoint: op.nodesetLadder from the cold start,
+    // rung 1 first). in_run: resumed inside a paused run.
+    // The ladder's state stays in L.ladder (across pauses too).
+    uint32_t stage = res_here ? phase0 : (cold ? 2u : 0u);
+    bool in_run = res_here;
+    LadderMove mv{kStartCold, false, false, true, 3u, 0u};
+    if (stage == 2 && !res_here && tid == 0) L.ladder[lane] = LadderDev{kRungPlain};
+    __syncwarp();
+    bool scaled = false;  // the sources hold a source-stepping factor
     int rc = 1;
-    if (res_here ? phase0 == 0 : !cold) {
-      if (!res_here) {
+    const size_t at = size_t(lane) * n;
+    for (;;) {
+      LaneOpts ro = o;
+      SimDev rs = sim;
+      if (stage == 2) {
+        if (!in_run) {
+          if (mv.done) break;
+          // the next run's start: its own end point, the last good
+          // stepping point or the cold start
+          if (mv.save)
+            for (uint32_t i = tid; i < n; i += 32) L.x_good[at + i] = m.x[i];
+          if (mv.start == kStartGood)
+            for (uint32_t i = tid; i < n; i += 32) m.x[i] = L.x_good[at + i];
+          if (mv.start == kStartCold) sweep_seed<kHasB3>(T, rec, m, tid);
+          __syncwarp();
+          lim_active = mv.start == kStartCold && T.nlim != 0;
+          carry.iter = 0;
+          carry.init_fix = mv.init_fix ? 1u : 0u;
+          carry.resume = 0;
+        }
+        // the rung's gmin stamps, junction gmin and source factor (the
+        // swept source's value scaled with the others)
+        const LadderRun run = ladder_run(cold_o, L.ladder + lane);
+        ro = cold_o;
+        ro.gstamp = run.gs;
+        ro.max_iter = run.max_iter;
+        rs.src_scale = run.src;
+        rs.gmin = run.gmin_dev;
+        if (scaled || run.src != 1.0) {
+          fill_sources(T, rec, rs, vsrc, tid);
+          if (tid == 0) vsrc[P.src] = P.values[pt] * run.src;
+          __syncwarp();
+          scaled = run.src != 1.0;
+        }
+      } else if (!in_run) {
+        // the warm start: the predictor limited against the last point
         for (uint32_t i = tid; i < n; i += 32) {
           m.x[i] = sol[i];
           m.xo[i] = prev[i];
@@ -2176,37 +2220,42 @@ __device__ void sweep_lane(const TopoDev& T, const LaneDev& L, const SweepDev& P
         carry.resume = 0;
         __syncwarp();
       }
+      in_run = false;
       uint32_t it = 0;
-      rc = lane_newton<kHasB3>(T, prog, m, rec, o, sim, nullptr, lim_active, false, it, vsrc, tid, &carry);
-      if (rc == 3) {
-        pause(pt, 0, it_total);
+      const int r = lane_newton<kHasB3>(T, prog, m, rec, ro, rs, nullptr, lim_active,
+                                        stage == 2 && carry.init_fix != 0, it, vsrc, tid, &carry);
+      if (r == 3) {
+        pause(pt, stage, it_total, pt == 0 && carry.iter == 0 && (stage == 0 || L.ladder[lane].rung == kRungPlain));
         return;
       }
       carry.resume = 0;
-      it_total += it;
-      for (uint32_t i = tid; i < n; i += 32) sol[i] = m.x[i];
+      if (stage == 0) {
+        it_total += it;
+        for (uint32_t i = tid; i < n; i += 32) sol[i] = m.x[i];
+        __syncwarp();
+        if (r == 0) {
+          rc = 0;
+          break;
+        }
+        stage = 2;
+        if (tid == 0) L.ladder[lane] = LadderDev{kRungPlain};
+        __syncwarp();
+        mv = LadderMove{kStartCold, false, false, true, 3u, 0u};
+        continue;
+      }
+      LadderDev ls = L.ladder[lane];
+      mv = ladder_decide(ls, r == 0, r == 2 ? 0u : it);
+      __syncwarp();
+      if (tid == 0) L.ladder[lane] = ls;
       __syncwarp();
     }
-    if (rc != 0) {
-      // cold rung: on a failed warm point, before any point has converged,
-      // or when resumed inside it
-      const bool res_cold = res_here && phase0 == 1;
-      if (!res_cold) {
-        sweep_seed<kHasB3>(T, rec, m, tid);
-        __syncwarp();
-        lim_active = T.nlim != 0;
-        carry.iter = 0;
-        carry.init_fix = 1;
-        carry.resume = 0;
+    if (stage == 2) {
+      rc = mv.result < 3 ? 0 : 1;
+      it_total += mv.report;
+      if (scaled) {
+        fill_sources(T, rec, sim, vsrc, tid);
+        if (tid == 0) vsrc[P.src] = P.values[pt];
       }
-      uint32_t it = 0;
-      rc = lane_newton<kHasB3>(T, prog, m, rec, cold_o, sim, nullptr, lim_active, true, it, vsrc, tid, &carry);
-      if (rc == 3) {
-        pause(pt, 1, it_total);
-        return;
-      }
-      carry.resume = 0;
-      it_total += it;
       for (uint32_t i = tid; i < n; i += 32) sol[i] = m.x[i];
       __syncwarp();
     }

@@ -667,13 +667,14 @@ static void sweep_run(ckt_t *kp, orc_slot slot, const double *values, uint32_t n
             converged = rc == 0;
         }
         if (!converged) {
+            /* dc.zig endPoint: the cold ladder (op.nodesetLadder, no
+             * nodesets) at the deck's itl1 */
             ckt_cold_start(&k, sol);
             orc_newton_opts cold_opts = *opts;
-            cold_opts.max_iter = 100; /* the op ladder's itl1 */
-            uint32_t it = 0;
-            int rc = ckt_run(&k, sol, &cold_opts, 1, &it);
+            cold_opts.max_iter = 100;
+            uint32_t it = 0, rung = 0;
+            converged = ckt_ladder(&k, sol, &cold_opts, &it, &rung);
             it_total += it;
-            converged = rc == 0;
         }
         memcpy(x_out + (size_t)pt * n, sol, sizeof(double) * n);
         iters[pt] = it_total;

@@ -81,7 +81,8 @@ def test_bsim3_sweep_lanes_match_oracle():
     assert _close(x, xo).all(), float(np.max(np.abs(x - xo)))
 
 
-OP_FIXTURES = [n for n in gu.names() if n.split("__")[0] in ("op", "convergence", "stress")]
+OP_FIXTURES = [n for n in gu.names() if n.split("__")[0] in ("op", "convergence", "stress")
+               and Deck(gu.load(n)["deck"]).analysis[0] == "op"]
 
 
 @pytest.mark.parametrize("name", OP_FIXTURES)

@@ -112,3 +112,32 @@ def test_sweep_lanes_peel_and_match_oracle_exactly(name):
         assert np.array_equal(cv[lane], cvo.astype(bool)), lane
         assert np.array_equal(it[lane], ito), (lane, np.flatnonzero(it[lane] != ito))
         assert np.array_equal(x[lane].view(np.uint64), xo.view(np.uint64)), lane
+
+
+def test_sweep_lanes_cold_ladder():
+    """The reference's ladder deck swept at 0.5 V steps, 16 lanes over the
+    second bit line's bias: a warm point fails and its cold restart leaves
+    plain Newton on four lanes, which finish the point through gmin stepping
+    on the device (dc.zig's cold ladder); every lane's points, iteration
+    counts and convergence exactly the oracle's."""
+    g = gu.load("convergence__bench_mos_latch_ladder")
+    deck = Deck(g["deck"])
+    fr = deck.circuit().freeze()
+    an = deck.analysis
+    from netlist import sweep_values
+    pts = np.array(sweep_values(an[2], an[3], 0.5))
+    slot = fr.slot(an[1], "dc")
+    opts = deck.newton_opts()
+    lane_values = np.linspace(1.6, 2.4, 16).reshape(-1, 1)
+    slots = [fr.slot("vdb", "dc")]
+    ctx = lanes.DcLanes(fr)
+    ctx.set_lanes(slots, lane_values)
+    x, it, cv, st, _ = ctx.sweep(slot, pts, lanes.newton_opts(**opts))
+    ctx.close()
+    assert (st == lanes.SWEEP_DONE).all()
+    xo, ito, cvo = oracle.dc_sweep_lanes(fr, slots, lane_values, slot, pts, oracle.newton_opts(**opts))
+    assert np.array_equal(cv, cvo.astype(bool))
+    assert np.array_equal(it, ito), np.argwhere(it != ito)
+    assert np.array_equal(x.view(np.uint64), xo.view(np.uint64))
+    assert (it > 100).sum() >= 4, it.max()
+    print(f"cold ladder points: {int((it > 100).sum())} of {it.size}, iterations up to {int(it.max())}")
