@@ -1588,6 +1588,11 @@ int32_t run_tran(esl_ctx* ctx, LaneDev L, TranDev P, const LaneOpts& lo, uint32_
   ESL_CUDA(ctx->d_tran_save.ensure(size_t(N) * bd * 8));
   P.tstate = ctx->d_tran_state.as<uint32_t>();
   P.tsave = ctx->d_tran_save.as<double>();
+  // the operating point's ladder: its state across pauses, its last good point
+  ESL_CUDA(ctx->d_ladder.ensure(size_t(N) * sizeof(LadderDev)));
+  ESL_CUDA(ctx->d_x_good.ensure(size_t(N) * ctx->topo.n * 8));
+  L.ladder = ctx->d_ladder.as<LadderDev>();
+  L.x_good = ctx->d_x_good.as<double>();
   ESL_CUDA(cudaMemsetAsync(L.status, 0, size_t(N) * 4, s));
   ESL_CUDA(cudaMemsetAsync(L.flags, 0, size_t(N) * 4, s));
   ESL_CUDA(cudaMemsetAsync(L.n_paused, 0, 4, s));

@@ -1773,7 +1773,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
       L.flags[lane] |= 2u;
       // the lane's first factor of all is its own fresh factor; a later
       // one continues the lead tape's history
-      L.iters[lane] = (phase == 1 && carry.iter == 0) ? 0u : 1u;
+      L.iters[lane] = (phase == 1 && carry.iter == 0 && L.ladder[lane].rung == kRungPlain) ? 0u : 1u;
       L.status[lane] = kNeedSolve;
       atomicAdd(L.n_paused, 1u);
     }
@@ -1795,47 +1795,65 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
     return open;
   };
 
-  // operating point: cold start with the junction seeds, MODEINITFIX; the
-  // source waves at t = 0 (kind 2: vsource.va:214-219)
+  // operating point (op.solve with tran_op): op.zig's ladder from the cold
+  // start (the junction seeds, MODEINITFIX), the source waves at t = 0
+  // (kind 2: vsource.va:214-219); every run through one call site, the
+  // ladder's state in L.ladder (across pauses too). in_run: resumed inside a
+  // paused run.
   int rc = 0;
   if (phase0 != 2) {
-    if (phase0 == 0) {
-      for (uint32_t i = tid; i < n; i += 32) m.x[i] = 0.0;
-      for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
-        const BatchDev& B = T.b[bi];
-        for (uint32_t i = tid; i < B.count; i += 32) {
-          if (B.type == kD) m.lim[B.lim_off + i] = rec[B.rec_off + kDVcrit * B.count + i];
-          if (B.type == kM) {
-            m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kMSeedVgs * B.count + i];
-            m.lim[B.lim_off + 3 * i + 1] = 0.0;
-            m.lim[B.lim_off + 3 * i + 2] = -1.0;
-          }
-          if (B.type == kB3) {
-            m.lim[B.lim_off + 3 * i] = rec[B.rec_off + kB3SeedVgs * B.count + i];
-            m.lim[B.lim_off + 3 * i + 1] = 0.1;
-            m.lim[B.lim_off + 3 * i + 2] = 0.0;
-          }
-        }
-      }
-      __syncwarp();
-      lim_active = T.nlim != 0;
-      carry.init_fix = 1;
-    }
+    bool in_run = phase0 == 1;
+    LadderMove mv{kStartCold, false, false, true, 3u, 0u};
+    if (phase0 == 0 && tid == 0) L.ladder[lane] = LadderDev{kRungPlain};
+    __syncwarp();
     LaneOpts op = o;
     op.residual_tol = 1e-9;
     op.gmin = 0.0;
     op.max_iter = 100;
-    uint32_t it = 0;
-    fill_sources(T, rec, sim, vsrc, tid);
-    rc = lane_newton<kHasB3>(T, prog, m, rec, op, sim, nullptr, lim_active, carry.init_fix != 0, it, vsrc, tid,
-                             &carry);
-    if (rc == 3) {
-      pause(1, 0.0);
-      return;
+    for (;;) {
+      if (!in_run) {
+        if (mv.done) break;
+        if (mv.save)
+          for (uint32_t i = tid; i < n; i += 32) L.x_good[at + i] = m.x[i];
+        if (mv.start == kStartGood)
+          for (uint32_t i = tid; i < n; i += 32) m.x[i] = L.x_good[at + i];
+        if (mv.start == kStartCold) {
+          for (uint32_t i = tid; i < n; i += 32) m.x[i] = 0.0;
+          cold_images(T, rec, m.lim, tid, 32);
+        }
+        __syncwarp();
+        lim_active = mv.start == kStartCold && T.nlim != 0;
+        carry.iter = 0;
+        carry.init_fix = mv.init_fix ? 1u : 0u;
+        carry.resume = 0;
+      }
+      in_run = false;
+      // the rung's gmin stamps, junction gmin and source factor
+      const LadderRun run = ladder_run(op, L.ladder + lane);
+      LaneOpts ro = op;
+      ro.gstamp = run.gs;
+      ro.max_iter = run.max_iter;
+      SimDev rs = sim;
+      rs.src_scale = run.src;
+      rs.gmin = run.gmin_dev;
+      fill_sources(T, rec, rs, vsrc, tid);
+      uint32_t it = 0;
+      const int r = lane_newton<kHasB3>(T, prog, m, rec, ro, rs, nullptr, lim_active, carry.init_fix != 0, it, vsrc,
+                                        tid, &carry);
+      if (r == 3) {
+        pause(1, 0.0);
+        return;
+      }
+      carry.resume = 0;
+      LadderDev ls = L.ladder[lane];
+      mv = ladder_decide(ls, r == 0, r == 2 ? 0u : it);
+      __syncwarp();
+      if (tid == 0) L.ladder[lane] = ls;
+      __syncwarp();
     }
-    carry.resume = 0;
     lim_active = false;
-    stat[kTsOpIters] = it;
+    stat[kTsOpIters] = mv.report;
+    rc = mv.result < 3 ? 0 : 1;
   }
   if (rc != 0) {
     stat[kTsStatus] = kTranOpFailed;

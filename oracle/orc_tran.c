@@ -195,8 +195,9 @@ static void tran_lane(ckt_t *k, const orc_tran_opts *o, rec_t *rec, uint32_t *st
     k->sim.t = 0.0;
     k->tran = 0;
     ckt_cold_start(k, cur);
-    uint32_t it = 0;
-    if (ckt_run(k, cur, &op, 1, &it) != 0) {
+    uint32_t it = 0, rung = 0;
+    /* op.solve with tran_op: the ladder from the cold start */
+    if (!ckt_ladder(k, cur, &op, &it, &rung)) {
         st[ORC_TS_STATUS] = 2;
         st[ORC_TS_OP_ITERS] = it;
         memcpy(x_final, cur, sizeof(double) * n);

@@ -273,3 +273,32 @@ def test_lanes_that_leave_the_tape_are_peeled():
     _check_parity(g, o)
     assert (g[3][:, 0] == lanes.TRAN_DONE).all()
     assert peeled > 0 and launches > 1
+
+
+def test_operating_point_takes_the_ladder():
+    """The reference's ladder deck (a MOS1 latch) as transient lanes over its
+    swept drain bias: the operating points that plain Newton leaves
+    (op.solve with tran_op) converge through gmin stepping inside the
+    transient lane, with the oracle's iteration sums, step decisions and
+    waveforms."""
+    g = gu.load("convergence__bench_mos_latch_ladder")
+    deck = Deck(g["deck"])
+    fr = deck.circuit().freeze()
+    from netlist import sweep_values
+    an = deck.analysis
+    slots = [fr.slot("vd", "dc")]
+    values = np.array(sweep_values(an[2], an[3], an[4])).reshape(-1, 1)
+    probes = [fr.unknown("v(q)"), fr.unknown("v(qb)")]
+    go = lanes.tran_opts(1e-9, 1e-10, 1e-10)
+    oo = oracle.tran_opts(1e-9, 1e-10, 1e-10)
+    ctx = lanes.DcLanes(fr)
+    ctx.set_lanes(slots, values)
+    res_g = ctx.tran(go, probes, 200)
+    ctx.close()
+    res_o = oracle.tran(fr, slots, values, oo, probes, 200)
+    _check_parity(res_g, res_o)
+    sg = res_g[3]
+    op_iters = sg[:, lanes.TS_FIELDS.index("op_iters")]
+    assert np.array_equal(op_iters, res_o[3][:, lanes.TS_FIELDS.index("op_iters")])
+    assert (sg[:, 0] == lanes.TRAN_DONE).all()
+    assert (op_iters > 100).sum() >= 3, op_iters
