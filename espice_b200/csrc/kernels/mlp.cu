@@ -1,16 +1,19 @@
 // The learned warm start's network on the 5th-generation tensor cores:
-// a BF16 GEMM with FP32 accumulation in tensor memory (tcgen05.mma, operands
-// staged in shared memory in the canonical K-major layout, one elected
-// thread issuing, completion through an mbarrier, the accumulator read back
-// with tcgen05.ld), its fused epilogues (bias, tanh, BF16 copies), and the
-// small kernels of training (tanh backward, transposes, bias gradient, MSE
-// gradient, Adam).
+// a BF16 GEMM with FP32 accumulation in tensor memory (operand tiles moved
+// by the Tensor Memory Accelerator, cp.async.bulk.tensor with the 128-byte
+// swizzle, into a ring of shared-memory stages tracked by mbarriers;
+// tcgen05.mma issued by one thread, each stage released by tcgen05.commit;
+// the accumulator read back with tcgen05.ld), its fused epilogues (bias,
+// tanh, BF16 copies), and the small kernels of training (tanh backward,
+// transposes, bias gradient, MSE gradient, Adam).
 //
 // Descriptor layouts (bit positions of the instruction descriptor and the
 // shared-memory matrix descriptor) follow the sm100 UMMA definitions;
 // encode_idesc and encode_sdesc pack them by hand.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cstdint>
@@ -33,24 +36,20 @@ __host__ __device__ constexpr uint32_t encode_idesc(uint32_t n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | (uint32_t(kTileM >> 4) << 24);
 }
 
-// Shared-memory matrix descriptor, no swizzle (K-major canonical layout
-// ((8, m), 2) : ((16 B, SBO), LBO)): start address >> 4 at bits 0-13,
-// leading byte offset >> 4 at 16-29, stride byte offset >> 4 at 32-45,
-// version 1 at bits 46-47, base offset 0, layout type 0 at bits 61-63.
-__device__ __forceinline__ uint64_t encode_sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  return uint64_t((saddr >> 4) & 0x3fffu) | (uint64_t((lbo >> 4) & 0x3fffu) << 16) |
-         (uint64_t((sbo >> 4) & 0x3fffu) << 32) | (1ull << 46);
+// Shared-memory matrix descriptor of a K-major tile written by TMA with the
+// 128-byte swizzle (rows of 64 BF16 = 128 B, 8-row atoms of 1 KB): start
+// address >> 4 at bits 0-13, leading byte offset (unused by the swizzled
+// K-major form) 16 B at 16-29, stride byte offset 1024 B (one atom) at
+// 32-45, version 1 at bits 46-47, base offset 0 (stages are 1 KB aligned),
+// layout type 2 (128-byte swizzle) at bits 61-63. The k-th K = 16 slice of a
+// stage starts 32 k bytes in.
+__device__ __forceinline__ uint64_t encode_sdesc(uint32_t saddr) {
+  return uint64_t((saddr >> 4) & 0x3fffu) | (uint64_t(16 >> 4) << 16) | (uint64_t(1024 >> 4) << 32) | (1ull << 46) |
+         (2ull << 61);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// Canonical K-major placement of element (r, k) of a rows x kTileK chunk:
-// 8 x 8 core matrices of 128 contiguous bytes, row-group major, K groups of
-// one row group adjacent (LBO = 128 B, SBO = 1024 B).
-__device__ __forceinline__ uint32_t core_offset(uint32_t r, uint32_t k) {
-  return ((r >> 3) * (kTileK / 8) + (k >> 3)) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
 }
 
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_t limit) {
@@ -68,31 +67,56 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_
   return false;
 }
 
-// 16-byte asynchronous copy global -> shared; src_bytes 0 fills zeros.
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+// One 2-D TMA tile load global -> shared, completing bytes on `bar`.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
 }
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+constexpr int kMaxStages = 4;
 
 // C = A (M x K, row-major BF16) . B (N x K, row-major BF16)^T with FP32
 // accumulation; grid (ceil(M / 128), N / bn), block 128 threads. The
 // epilogue adds bias[n] when given, stores the FP32 result to c (ldc) when
 // given, and tanh (act = 1) or identity of it as BF16 to h (ldh) when given.
-// Rows >= M are read as zero and not stored. K is a multiple of 16 (zero
-// padded by the caller), bn a multiple of 16 in [16, 256].
+// Rows >= M are read as zero (the TMA box's out-of-bounds fill) and not
+// stored; so are K columns past K. K is a multiple of 16, bn a multiple of 16
+// in [16, 256].
 //
-// Two staging buffers: while the MMAs of K chunk k run, the cp.async copies
-// of chunk k + 1 fill the other buffer, whose previous reader (the MMAs of
-// chunk k - 1) is known complete through the mbarrier.
-__global__ void __launch_bounds__(kThreads) gemm_bf16_tc(const __nv_bfloat16* __restrict__ a, int lda,
-                                                         const __nv_bfloat16* __restrict__ b, int ldb, int M, int K,
-                                                         int bn, const float* __restrict__ bias, float* c, int ldc,
-                                                         __nv_bfloat16* h, int ldh, int act, int* err,
+// The pipeline (thread 0): `stages` shared-memory stages of one 64-wide K
+// chunk each (A 128 x 64, B bn x 64 BF16). Chunk q's two TMA loads land on
+// full[q % stages]; its four MMAs are issued once they have, and their
+// completion is committed to empty[q % stages], which frees the stage for
+// chunk q + stages. The refill of a stage waits for the MMAs of the chunk
+// before the one just issued, so one chunk's MMAs are always queued behind
+// the running ones. Every wait is bounded; one that runs out raises err,
+// stops the issue, and waits (bounded again) for the loads and MMAs in
+// flight before the tensor memory is freed.
+__global__ void __launch_bounds__(kThreads) gemm_bf16_tc(const __grid_constant__ CUtensorMap ta,
+                                                         const __grid_constant__ CUtensorMap tb, int M, int K, int bn,
+                                                         int stages, const float* __restrict__ bias, float* c,
+                                                         int ldc, __nv_bfloat16* h, int ldh, int act, int* err,
                                                          uint32_t wait_limit) {
-  extern __shared__ __align__(1024) unsigned char smem[];
+  extern __shared__ unsigned char smem_raw[];
+  // stages at a 1 KB boundary (the swizzle atom)
+  const uint32_t raw = smem_u32(smem_raw);
+  unsigned char* smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
   const uint32_t a_bytes = kTileM * kTileK * 2, b_bytes = uint32_t(bn) * kTileK * 2;
-  unsigned char* buf[2] = {smem, smem + a_bytes + b_bytes};
-  __shared__ __align__(8) uint64_t bar;
+  const uint32_t stage_bytes = a_bytes + b_bytes;
+  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], done;
   __shared__ uint32_t tmem_slot;
+  __shared__ int ok_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * bn;
   uint32_t ncols = 32;
@@ -104,50 +128,48 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tc(const __nv_bfloat16* __
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)));
+    for (int s = 0; s < stages; ++s) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[s])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[s])));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&done)));
     asm volatile("fence.mbarrier_init.release.cluster;");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&ta)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tb)) : "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = tmem_slot;
-  const uint32_t idesc = encode_idesc(uint32_t(bn));
-  const int n_chunks = (K + kTileK - 1) / kTileK;
 
-  // stage chunk q into buffer q & 1: 16 B per copy, zero beyond M and K
-  auto stage = [&](int q) {
-    const int k0 = q * kTileK, kc = min(kTileK, K - k0);
-    unsigned char* sa = buf[q & 1];
-    unsigned char* sb = sa + a_bytes;
-    for (int i = tid; i < kTileM * (kTileK / 8); i += kThreads) {
-      const int r = i / (kTileK / 8), kg = (i % (kTileK / 8)) * 8;
-      const bool in = m0 + r < M && kg < kc;
-      const __nv_bfloat16* src = a + size_t(in ? m0 + r : 0) * lda + (in ? k0 + kg : 0);
-      cp_async16(smem_u32(sa + core_offset(r, kg)), src, in ? 16u : 0u);
-    }
-    for (int i = tid; i < bn * (kTileK / 8); i += kThreads) {
-      const int r = i / (kTileK / 8), kg = (i % (kTileK / 8)) * 8;
-      const bool in = kg < kc;
-      const __nv_bfloat16* src = b + size_t(n0 + r) * ldb + (in ? k0 + kg : 0);
-      cp_async16(smem_u32(sb + core_offset(r, kg)), src, in ? 16u : 0u);
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-  };
-
-  uint32_t parity = 0;
-  bool ok = true;
-  stage(0);
-  for (int q = 0; q < n_chunks; ++q) {
-    asm volatile("cp.async.wait_group 0;" ::: "memory");  // chunk q has landed
-    asm volatile("fence.proxy.async.shared::cta;");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    const int kc = min(kTileK, K - q * kTileK);
-    if (tid == 0) {
-      const uint32_t sa = smem_u32(buf[q & 1]), sb = sa + a_bytes;
+  if (tid == 0) {
+    const uint32_t idesc = encode_idesc(uint32_t(bn));
+    const uint32_t base = smem_u32(smem);
+    const int n_chunks = (K + kTileK - 1) / kTileK;
+    int issued = 0, consumed = 0;
+    bool ok = true;
+    auto issue = [&](int q) {
+      const int s = q % stages;
+      const uint32_t sa = base + uint32_t(s) * stage_bytes, bar = smem_u32(&full[s]);
+      mbar_expect_tx(bar, stage_bytes);
+      tma_load_2d(sa, &ta, q * kTileK, m0, bar);
+      tma_load_2d(sa + a_bytes, &tb, q * kTileK, n0, bar);
+      ++issued;
+    };
+    for (int q = 0; q < n_chunks && q < stages; ++q) issue(q);
+    for (int q = 0; q < n_chunks; ++q) {
+      const int s = q % stages;
+      if (!mbar_wait(smem_u32(&full[s]), uint32_t(q / stages) & 1u, wait_limit)) {
+        ok = false;
+        break;
+      }
+      ++consumed;
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t sa = base + uint32_t(s) * stage_bytes, sb = sa + a_bytes;
+      const int kc = min(kTileK, K - q * kTileK);
       for (int j = 0; j < kc / 16; ++j) {
-        const uint64_t da = encode_sdesc(sa + j * 256, 128, 1024);
-        const uint64_t db = encode_sdesc(sb + j * 256, 128, 1024);
+        const uint64_t da = encode_sdesc(sa + uint32_t(j) * 32u);
+        const uint64_t db = encode_sdesc(sb + uint32_t(j) * 32u);
         const uint32_t acc = (q > 0 || j > 0) ? 1u : 0u;
         const uint32_t z = 0;
         asm volatile(
@@ -156,23 +178,33 @@ __global__ void __launch_bounds__(kThreads) gemm_bf16_tc(const __nv_bfloat16* __
             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
             "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-          smem_u32(&bar)));
+      umma_commit(smem_u32(&empty[s]));
+      // refill the stage of the chunk before this one once its MMAs are done
+      const int p = q - 1;
+      if (p >= 0 && p + stages < n_chunks) {
+        if (!mbar_wait(smem_u32(&empty[p % stages]), uint32_t(p / stages) & 1u, wait_limit)) {
+          ok = false;
+          break;
+        }
+        issue(p + stages);
+      }
     }
-    // the other buffer's last reader (chunk q - 1) completed at the previous wait
-    if (q + 1 < n_chunks) stage(q + 1);
-    if (!mbar_wait(smem_u32(&bar), parity, wait_limit)) {
-      // The wait ran out: the result is not stored (err is raised), but the
-      // MMAs still read the staging buffer and write the accumulator, so
-      // drain them (again bounded) before the buffer is refilled or the
-      // tensor memory freed.
+    if (!ok) {
+      // loads still in flight land before the stages are reused or freed
+      for (int q = consumed; q < issued; ++q) mbar_wait(smem_u32(&full[q % stages]), uint32_t(q / stages) & 1u, kWaitLimit);
+    }
+    // every MMA issued, complete before the accumulator is read or freed
+    umma_commit(smem_u32(&done));
+    if (!mbar_wait(smem_u32(&done), 0u, ok ? wait_limit : kWaitLimit)) {
       ok = false;
-      mbar_wait(smem_u32(&bar), parity, kWaitLimit);
+      mbar_wait(smem_u32(&done), 0u, kWaitLimit);
     }
-    parity ^= 1u;
-    asm volatile("tcgen05.fence::after_thread_sync;");
+    ok_flag = ok;
+    if (!ok) atomicExch(err, 1);
   }
-  if (!ok && tid == 0) atomicExch(err, 1);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const bool ok = ok_flag != 0;
 
   // epilogue: warp w owns accumulator rows 32w .. 32w + 31 (thread = row in
   // TMEM). Each 32-column block goes through the warp's 32 x 33 float
@@ -296,20 +328,65 @@ __global__ void to_bf16(const float* in, int n, __nv_bfloat16* out) {
 
 }  // namespace
 
+namespace {
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library), looked up once.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return static_cast<PFN_cuTensorMapEncodeTiled_v12000>(nullptr);
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// The tensor map of a row-major BF16 matrix of `rows` x `cols` (leading
+// dimension ld elements, a multiple of 8: 16-byte row strides) read in
+// boxes of box_rows x 64 with the 128-byte swizzle; out-of-bounds elements
+// read as zero.
+cudaError_t bf16_tile_map(CUtensorMap* map, const __nv_bfloat16* base, int rows, int cols, int ld, int box_rows) {
+  PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  if (!encode) return cudaErrorNotSupported;
+  const cuuint64_t dims[2] = {cuuint64_t(cols), cuuint64_t(rows)};
+  const cuuint64_t strides[1] = {cuuint64_t(ld) * 2};
+  const cuuint32_t box[2] = {cuuint32_t(kTileK), cuuint32_t(box_rows)};
+  const cuuint32_t elem[2] = {1, 1};
+  const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(base), dims, strides,
+                            box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+}  // namespace
+
 cudaError_t launch_gemm_bf16(const __nv_bfloat16* a, int lda, const __nv_bfloat16* b, int ldb, int M, int N, int K,
                              const float* bias, float* c, int ldc, __nv_bfloat16* h, int ldh, int act, int* err,
                              cudaStream_t s, uint32_t wait_rounds) {
   if (M <= 0 || N <= 0 || K <= 0 || K % 16 || N % 16 || lda % 8 || ldb % 8) return cudaErrorInvalidValue;
+  // TMA: 16-byte aligned bases (the strides are, by lda, ldb)
+  if ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b)) & 15u) return cudaErrorInvalidValue;
   int bn = N <= 256 ? N : 128;
   while (N % bn) bn -= 16;
-  // Two staging buffers of A (16 KB) and B (bn x 64 BF16, at most 32 KB);
-  // at least 100 KB per CTA, so at most two CTAs share an SM and their
-  // tensor-memory allocations (at most 256 columns each) fit in its 512.
-  const size_t smem = std::max<size_t>(100 * 1024, 2 * (size_t(kTileM) * kTileK * 2 + size_t(bn) * kTileK * 2));
-  cudaError_t e = cudaFuncSetAttribute(gemm_bf16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  CUtensorMap ta, tb;
+  cudaError_t e = bf16_tile_map(&ta, a, M, K, lda, kTileM);
+  if (e != cudaSuccess) return e;
+  e = bf16_tile_map(&tb, b, N, K, ldb, bn);
+  if (e != cudaSuccess) return e;
+  // Stages of A (16 KB) and B (bn x 64 BF16, at most 32 KB): three when B is
+  // at most 128 rows, else two, which keeps a CTA under 100 KB so two share
+  // an SM (their tensor-memory allocations, at most 256 columns each, fit
+  // in its 512); 1 KB more for the stages' alignment.
+  const int stages = bn <= 128 ? 3 : 2;
+  const size_t stage_bytes = size_t(kTileM) * kTileK * 2 + size_t(bn) * kTileK * 2;
+  const size_t smem = std::max<size_t>(100 * 1024, size_t(stages) * stage_bytes + 1024);
+  e = cudaFuncSetAttribute(gemm_bf16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   dim3 grid((M + kTileM - 1) / kTileM, N / bn);
-  gemm_bf16_tc<<<grid, kThreads, smem, s>>>(a, lda, b, ldb, M, K, bn, bias, c, ldc, h, ldh, act, err,
+  gemm_bf16_tc<<<grid, kThreads, smem, s>>>(ta, tb, M, K, bn, stages, bias, c, ldc, h, ldh, act, err,
                                             wait_rounds == 0 ? kWaitLimit : wait_rounds == ~0u ? 0u : wait_rounds);
   return cudaGetLastError();
 }

@@ -27,7 +27,10 @@ def _torch():
     return torch
 
 
-@pytest.mark.parametrize("M,N,K", [(200, 96, 48), (1000, 512, 512), (128, 16, 16), (333, 272, 80)])
+# the last: the learned step's inference shape (a 32,768-point chunk through
+# a 512-wide hidden layer)
+@pytest.mark.parametrize("M,N,K", [(200, 96, 48), (1000, 512, 512), (128, 16, 16), (333, 272, 80),
+                                   (32768, 512, 512)])
 def test_gemm_matches_float64(M, N, K):
     torch = _torch()
     g = torch.Generator().manual_seed(M + N + K)
@@ -44,8 +47,13 @@ def test_gemm_matches_float64(M, N, K):
     got = c.double().cpu()
     scale = (a.double().abs().cpu() @ b.double().abs().cpu().T).max()
     assert float((got - ref).abs().max()) <= 1e-6 * float(scale) + 1e-6
+    # the BF16 tanh copy: the device's tanhf and the host's may differ in the
+    # last FP32 bit, which flips a BF16 rounding now and then: one BF16 ulp,
+    # on a handful of the elements at most
     th = torch.tanh(c.cpu()).to(torch.bfloat16).float()
-    assert torch.equal(h.cpu().float(), th)
+    hb = h.cpu().float()
+    assert torch.allclose(hb, th, rtol=2.0 ** -7, atol=0.0)
+    assert float((hb != th).float().mean()) <= 1e-5
 
 
 def test_gemm_without_bias_or_copy():
