@@ -274,6 +274,7 @@ struct esl_ctx {
   DevBuf d_rec, d_lim, d_lim_active, d_status, d_iters, d_flags, d_limit, d_a_vals, d_rhs, d_dx,
       d_diag, d_paused, d_x;
   DevBuf d_gst, d_ladder, d_x_good;  // operating-point lanes: stamps, ladder states, stepping points
+  DevBuf d_tran_slab;                // block transient lanes: each CTA's run state
   TopoDev topo{};
 
   std::unordered_map<uint32_t, DirectSolver> peel;
@@ -1580,6 +1581,29 @@ namespace {
 
 // One transient launch over every lane, then the host factors of the lanes
 // that paused (serve_pauses) and resume launches until none pauses.
+// The transient on the block lanes (a CTA per lane, FP64): one persistent
+// launch, every lane's run state in the CTA's part of the transient slab.
+// Lanes whose factor leaves the lead tape stop (kTranLeftTape): no host
+// factor on this path.
+int32_t run_tran_block(esl_ctx* ctx, LaneDev L, TranDev P, const LaneOpts& lo) {
+  cudaStream_t s = ctx->stream;
+  const uint32_t N = ctx->n_lanes;
+  if (P.meas) return ctx->fail(ESL_NOT_ELIGIBLE, "the block transient lanes stream no measure cards");
+  BlockDev D{};
+  if (int32_t rc = block_view(ctx, false, N, D)) return rc;
+  ESL_CUDA(ctx->d_tran_slab.ensure(size_t(D.grid) * tran_block_slab(ctx->topo) * 8));
+  ESL_CUDA(ctx->d_x_good.ensure(size_t(N) * ctx->topo.n * 8));
+  L.x_good = ctx->d_x_good.as<double>();
+  ESL_CUDA(cudaMemsetAsync(L.status, 0, size_t(N) * 4, s));
+  std::memset(&ctx->last_peels, 0, sizeof(ctx->last_peels));
+  ESL_CUDA(cudaEventRecord(ctx->ev0, s));
+  ESL_CUDA(launch_tran_block(D, L, P, lo, topo_has_b3(ctx->topo), ctx->d_tran_slab.as<double>(), s));
+  ctx->last_peels.launches = 1;
+  ESL_CUDA(cudaEventRecord(ctx->ev1, s));
+  ESL_CUDA(cudaEventSynchronize(ctx->ev1));
+  return ESL_OK;
+}
+
 int32_t run_tran(esl_ctx* ctx, LaneDev L, TranDev P, const LaneOpts& lo, uint32_t lpb) {
   cudaStream_t s = ctx->stream;
   const uint32_t N = ctx->n_lanes;
@@ -1631,8 +1655,8 @@ int32_t esl_tran_device(esl_ctx* ctx, const esl_tran_opts* opts, double* d_x, ui
   LaneOpts lo;
   if (int32_t rc = tran_view(ctx, opts, P, lo)) return rc;
   if (int32_t rc = ensure_tape_cold(ctx)) return rc;
-  if (int32_t rc = warp_only(ctx)) return rc;
-  if (ctx->tran_lanes_eff == 0) return ctx->fail(ESL_NOT_ELIGIBLE, "a transient lane exceeds a CTA's shared memory");
+  // the block lanes when asked for, or when a warp lane cannot hold the run
+  const bool block = ctx->path == ESL_PATH_BLOCK || !ctx->warp_ok || ctx->tran_lanes_eff == 0;
   P.stats = d_stats;
   P.n_probes = max_pts ? n_probes : 0;
   P.max_pts = max_pts;
@@ -1642,7 +1666,11 @@ int32_t esl_tran_device(esl_ctx* ctx, const esl_tran_opts* opts, double* d_x, ui
   P.n_pts = max_pts ? d_n_pts : nullptr;
   LaneDev L = lane_view(ctx, 0);
   L.x = d_x;
-  if (int32_t rc = run_tran(ctx, L, P, lo, lanes_per_cta(ctx, ctx->n_lanes, ctx->tran_lanes_eff))) return rc;
+  if (block) {
+    if (int32_t rc = run_tran_block(ctx, L, P, lo)) return rc;
+  } else if (int32_t rc = run_tran(ctx, L, P, lo, lanes_per_cta(ctx, ctx->n_lanes, ctx->tran_lanes_eff))) {
+    return rc;
+  }
   if (ms) cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1);
   return ESL_OK;
 }

@@ -39,6 +39,7 @@
 #include "block.h"
 #include "lane_eval.cuh"
 #include "ladder.cuh"
+#include "tran_core.cuh"
 
 namespace esl {
 
@@ -718,6 +719,482 @@ int group_occupancy_t(size_t smem) {
   return per_sm;
 }
 
+// ---------------------------------------------------------------------------
+// Transient block lanes (tran.zig Sim.begin / Sim.end and the integrator.zig
+// kernels on a CTA per lane): the warp transient lanes' run, step for step,
+// for circuits whose working set leaves a warp's share of shared memory, and
+// for few lanes (a lane's rows spread over the CTA's 256 threads). FP64; no
+// streamed measures; a lane whose factor leaves the lead tape stops with
+// kTranLeftTape (no host factor).
+// ---------------------------------------------------------------------------
+
+// The transient's row charges (q of every row that carries charge cells,
+// summed from +0.0 in stamp order) into q.
+template <uint32_t kW>
+__device__ void block_row_charges(const TopoDev& T, const double* st, double* q, int tid) {
+  for (uint32_t i = tid; i < T.n; i += kW) {
+    const uint32_t e0 = T.q_ptr[i], e1 = T.q_ptr[i + 1];
+    if (e0 == e1) continue;
+    double s = 0.0;
+    for (uint32_t e = e0; e < e1; ++e) s = __dadd_rn(s, st[T.q_src[e]]);
+    q[i] = s;
+  }
+}
+
+// integrator.companionAt (accumulate) and Circuit.combineGC on the
+// assembled G: rows with charge get ag0 (q - q1) (less ag1 ip on a
+// trapezoidal step), slots with capacitance ag0 C.
+struct BlockCompanion {
+  double ag0, ag1;
+  bool trap;
+  const double* q1;
+  const double* ip;
+};
+
+template <uint32_t kW>
+__device__ void block_companion(const TopoDev& T, const BlockMem<double>& b, const BlockCompanion& c, int tid) {
+  const double* st = b.m.st;
+  for (uint32_t i = tid; i < T.n; i += kW) {
+    const uint32_t e0 = T.q_ptr[i], e1 = T.q_ptr[i + 1];
+    if (e0 == e1) continue;
+    double s = 0.0;
+    for (uint32_t e = e0; e < e1; ++e) s = __dadd_rn(s, st[T.q_src[e]]);
+    const double dq = c.ag0 * (s - c.q1[i]);
+    const double base = b.m.rhs[i] + dq;
+    const double r = c.trap ? base - c.ag1 * c.ip[i] : base;
+    b.m.rhs[i] = r;
+    b.y[T.pinv[i]] = -r;
+  }
+  for (uint32_t p = tid; p < T.nnz; p += kW) {
+    const uint32_t e0 = T.c_ptr[p], e1 = T.c_ptr[p + 1];
+    if (e0 == e1) continue;
+    double s = 0.0;
+    for (uint32_t e = e0; e < e1; ++e) s = __dadd_rn(s, st[T.c_src[e]]);
+    const uint32_t at = T.amap[p], dr = T.slot_row[p];
+    const double v = b.v[at] + c.ag0 * s;
+    b.v[at] = v;
+    if (dr != kNoDiag) b.m.diag[dr] = v;
+  }
+}
+
+// One Newton solve of a block transient lane (converger.newton at W = 1,
+// the warp lanes' lane_newton): the companion when cp is given, the
+// gmin-stepping stamps at o.gstamp. Returns 0 converged (x holds the
+// published iterate), 1 out of iterations, 2 a factor left the lead tape.
+template <typename OpT, bool kHasB3, uint32_t kW>
+__device__ int block_tran_newton(const BlockDev& D, const BlockMem<double>& b, const double* rec, const LaneOpts& o,
+                                 const SimDev& sim, const BlockCompanion* cp, bool& lim_active, bool init_fix,
+                                 uint32_t& iters, const double* vsrc, uint64_t* red, int tid) {
+  const TopoDev& T = D.T;
+  const LaneMem& m = b.m;
+  const uint32_t n = T.n;
+  uint32_t max_iter = o.max_iter < 100 ? 100 : o.max_iter;
+  if (o.iter_cap && o.iter_cap < max_iter) max_iter = o.iter_cap;
+  double limit = kXPlausible;
+  for (uint32_t iter = 0; iter < max_iter; ++iter) {
+    eval_all<kHasB3, kW>(T, rec, m, lim_active, sim, tid, false, vsrc);
+    if (tid == 0) m.st[T.n_stage + kGCellX0] = m.x[0];
+    __syncthreads();
+    block_assemble<double, kW>(D, b, o.gmin, o.gstamp, tid);
+    __syncthreads();
+    if (cp) {
+      block_companion<kW>(T, b, *cp, tid);
+      __syncthreads();
+    }
+    if (iter == 0) {
+      // plausibleLimit: 1e3 x the start's scale, at least x_plausible
+      double g = 1.0;
+      uint64_t xm = 0, fm = 0;
+      for (uint32_t i = tid; i < n; i += kW) {
+        g = fmax(g, fabs(m.diag[i]));
+        const uint64_t bx = dbits(fabs(m.x[i])), bf = dbits(fabs(m.rhs[i]));
+        xm = bx > xm ? bx : xm;
+        fm = bf > fm ? bf : fm;
+      }
+      const double gd = block_fmax<kW>(g, red);
+      xm = block_max_bits<kW>(xm, red);
+      fm = block_max_bits<kW>(fm, red);
+      const double scale = fmin(fmax(from_bits(xm), from_bits(fm) * gd), 1e18);
+      limit = !(1e3 * scale > kXPlausible) ? kXPlausible : 1e3 * scale;
+    }
+    if (block_refactor<double, OpT, kW>(D, b.v, b.ring, tid)) {
+      iters = iter + 1;
+      return 2;
+    }
+    block_rows<double, OpT, kW>(static_cast<const OpT*>(D.b_ops), D.b_rows, b.v, b.ring, tid);
+    for (uint32_t j = tid; j < n; j += kW) b.dx[T.qcol[j]] = b.y[j];
+    __syncthreads();
+    // finalizeStep: x_old = x, x += dx, delta score (updateAndNorm)
+    uint64_t worst = 0;
+    for (uint32_t i = tid; i < n; i += kW) {
+      const double d = b.dx[i];
+      const double xold = m.x[i];
+      const double xn = xold + d;
+      m.xo[i] = xold;
+      m.x[i] = xn;
+      const double tol = o.reltol * fmax(fabs(xn), fabs(xold)) + (T.cur_row[i] ? o.abstol : o.vntol);
+      const bool finite = fabs(xn) < CUDART_INF && fabs(d) < CUDART_INF;
+      const double qv = div_rn(fabs(d), tol);
+      const double score = !finite ? CUDART_INF : (qv == qv ? qv : 0.0);
+      const uint64_t sb = dbits(score);
+      worst = sb > worst ? sb : worst;
+    }
+    worst = block_max_bits<kW>(worst, red);
+    const bool limited = __syncthreads_or(apply_limits<kHasB3, kW>(T, rec, m, lim_active, tid)) != 0;
+    if (T.nlim) lim_active = true;
+    bool ok = !limited && iter != 0 && !(from_bits(worst) >= 1.0);
+    if (ok) {
+      bool p = true;
+      for (uint32_t i = tid; i < n; i += kW) p &= fabs(m.x[i]) <= limit;
+      ok = __syncthreads_and(p) != 0;
+    }
+    if (ok) {
+      bool p = true;
+      for (uint32_t i = tid; i < n; i += kW) p &= fabs(m.rhs[i]) <= residual_gate(o, m.diag[i], m.x[i]);
+      ok = __syncthreads_and(p) != 0;
+    }
+    if (ok) {
+      if (init_fix) {
+        init_fix = false;  // INITFIX -> INITFLOAT: one more passing iterate
+      } else {
+        for (uint32_t i = tid; i < n; i += kW) m.x[i] = m.xo[i];
+        __syncthreads();
+        iters = iter + 1;
+        return 0;
+      }
+    }
+    __syncthreads();
+  }
+  iters = max_iter;
+  return 1;
+}
+
+// A block transient lane's run state, in its CTA's part of the transient
+// slab (global memory): the accepted point and the one before (n each),
+// the row-charge ring (4 slots of n) and its currents (n), the LTE-state
+// ring (4 slots of nq) and its currents (nq), the sources' values (n_src)
+// and their PULSE timers (8 n_src).
+__host__ __device__ inline size_t tran_block_slab_doubles(const TopoDev& T) {
+  return (7 * size_t(T.n) + 5 * size_t(T.n_qt) + 9 * size_t(T.n_src) + 1) & ~size_t(1);
+}
+
+// One lane's whole transient on the CTA (tran_lane's run): the operating
+// point through op.zig's ladder, then the trapezoidal steps with the
+// predictor, LTE control, order promotion and source breakpoints.
+template <typename OpT, bool kHasB3, uint32_t kW>
+__device__ void block_tran_lane(const BlockDev& D, const LaneDev& L, const TranDev& P, const LaneOpts& o,
+                                unsigned char* base, unsigned char* cold, unsigned char* ring, double* tslab,
+                                uint64_t* red, uint32_t lane) {
+  const TopoDev& T = D.T;
+  const int tid = threadIdx.x;
+  const uint32_t n = T.n, nq = T.n_qt;
+  const BlockMem<double> b = block_carve<double>(D, base, cold, ring, sizeof(OpT));
+  const LaneMem& m = b.m;
+  double* cur = tslab;
+  double* prev = cur + n;
+  double* qh = prev + n;  // 4 slots of n: the row-charge ring
+  double* ipr = qh + 4 * size_t(n);
+  double* qt = ipr + n;   // 4 slots of nq: the LTE-state ring
+  double* ipt = qt + 4 * size_t(nq);
+  double* vsrc = ipt + nq;  // the V and I sources at the current time point
+  double* tmr = vsrc + T.n_src;  // 8 n_src: the PULSE corner timers
+  const double* rec = L.rec + size_t(lane) * T.rec_size;
+  const size_t at = size_t(lane) * n;
+  uint32_t stat[kTsN];
+  for (int k = 0; k < kTsN; ++k) stat[k] = 0;
+  if (tid == 0) {
+    b.v[T.ntv + n] = 0.0;
+    b.v[T.ntv + n + 1] = 1.0;
+    b.v[T.ntv + n + 2] = 0.0;
+    m.st[T.n_stage + kGCellZero] = 0.0;
+    m.st[T.n_stage + kGCellOne] = 1.0;
+  }
+
+  const double dt_max = P.dt_max;
+  const double delmin = 1e-11 * dt_max;
+  const double min_break = 10.0 * delmin;
+  double dt = 0.0, t = 0.0, bp_next = 0.0, bp_save_dt = div_rn(P.t_stop, 50.0);
+  double dt_old[6];
+  for (int k = 0; k < 6; ++k) dt_old[k] = dt_max;
+  int order = 1;
+  uint32_t steps = 0, hb = 0, n_rec = 0;
+  bool have_bp = false, bp_clamped = false, lim_active = false;
+  SimDev sim;
+  sim.t = 0.0;
+  sim.src_scale = 1.0;
+  sim.kind = 2;
+  __syncthreads();
+
+  auto record = [&](double tr) {
+    if (P.out_t && n_rec < P.max_pts) {
+      if (tid == 0) P.out_t[size_t(lane) * P.max_pts + n_rec] = tr;
+      for (uint32_t k = tid; k < P.n_probes; k += kW)
+        P.out_v[(size_t(lane) * P.max_pts + n_rec) * P.n_probes + k] = m.x[P.probes[k]];
+      ++n_rec;
+    }
+  };
+
+  // operating point (op.solve with tran_op): op.zig's ladder from the cold
+  // start, the source waves at t = 0 (kind 2), every run through one call
+  // site, the ladder's state in L.ladder
+  int rc = 0;
+  {
+    LadderMove mv{kStartCold, false, false, true, 3u, 0u};
+    LadderDev ls{kRungPlain};
+    LaneOpts op = o;
+    op.residual_tol = 1e-9;
+    op.gmin = 0.0;
+    op.max_iter = 100;
+    bool left = false;
+    for (;;) {
+      if (mv.done) break;
+      if (mv.save)
+        for (uint32_t i = tid; i < n; i += kW) L.x_good[at + i] = m.x[i];
+      if (mv.start == kStartGood)
+        for (uint32_t i = tid; i < n; i += kW) m.x[i] = L.x_good[at + i];
+      if (mv.start == kStartCold) {
+        for (uint32_t i = tid; i < n; i += kW) m.x[i] = 0.0;
+        cold_images(T, rec, m.lim, tid, kW);
+      }
+      __syncthreads();
+      lim_active = mv.start == kStartCold && T.nlim != 0;
+      const LadderRun run = ladder_run(op, &ls);
+      LaneOpts ro = op;
+      ro.gstamp = run.gs;
+      ro.max_iter = run.max_iter;
+      SimDev rs = sim;
+      rs.src_scale = run.src;
+      rs.gmin = run.gmin_dev;
+      fill_sources<kW>(T, rec, rs, vsrc, tid);
+      uint32_t it = 0;
+      const int r = block_tran_newton<OpT, kHasB3, kW>(D, b, rec, ro, rs, nullptr, lim_active, mv.init_fix, it, vsrc,
+                                                        red, tid);
+      if (r == 2) {
+        left = true;
+        break;
+      }
+      mv = ladder_decide(ls, r == 0, it);
+    }
+    lim_active = false;
+    stat[kTsOpIters] = mv.report;
+    if (left) {
+      stat[kTsStatus] = kTranLeftTape;
+      rc = 2;
+    } else {
+      rc = mv.result < 3 ? 0 : 1;
+    }
+  }
+  if (rc == 1) {
+    stat[kTsStatus] = kTranOpFailed;
+  } else if (rc == 0) {
+    const bool has_charge = T.q_ptr[n] != 0 || T.c_ptr[T.nnz] != 0;
+    auto slot = [&](double* base_, uint32_t len, uint32_t r) { return base_ + size_t((hb + r) & 3u) * len; };
+    for (uint32_t i = tid; i < n; i += kW) {
+      cur[i] = m.x[i];
+      prev[i] = m.x[i];
+    }
+    // charge histories, flat at q(x_op); no dynamic current yet
+    sim.kind = 1;
+    eval_all<kHasB3, kW>(T, rec, m, false, sim, tid, true);
+    for (uint32_t i = tid; i < 4 * n; i += kW) qh[i] = 0.0;
+    __syncthreads();
+    block_row_charges<kW>(T, m.st, qh + n, tid);
+    state_charges<kW>(T, rec, m.x, qt + nq, tid);
+    __syncthreads();
+    for (uint32_t i = tid; i < n; i += kW) {
+      qh[2 * n + i] = qh[n + i];
+      qh[3 * n + i] = qh[n + i];
+      ipr[i] = 0.0;
+    }
+    for (uint32_t j = tid; j < nq; j += kW) {
+      qt[2 * nq + j] = qt[nq + j];
+      qt[3 * nq + j] = qt[nq + j];
+      ipt[j] = 0.0;
+    }
+    __syncthreads();
+    pulse_timers<kW>(T, rec, tmr, tid);
+    dt = fmin(div_rn(fmin(P.t_step, div_rn(P.t_stop, 100.0)), 10.0), dt_max);
+    double bp0;
+    if (next_bp<kW>(T, rec, tmr, min_break, bp0, tid, red)) dt = fmin(dt, 0.1 * bp0);
+    dt = div_rn(dt, 10.0);
+    record(0.0);
+    LaneOpts nr = o;
+    nr.residual_tol = CUDART_INF;
+    nr.gmin = 0.0;
+    nr.max_iter = 100;
+    for (;;) {
+      if (!(t < P.t_stop && !almost_equal_ulps(t, P.t_stop, 100) && steps < P.max_steps)) break;
+      const double t_dev = t + dt;
+      sim.kind = 1;
+      sim.t = t_dev;
+      const bool trap = order == 2;
+      const double ag0 = trap ? div_rn(div_rn(1.0, dt), 1.0 - 0.5) : div_rn(1.0, dt);
+      const double ag1 = trap ? div_rn(0.5, 1.0 - 0.5) : 1.0;
+      // predictor, limited against the accepted point
+      const double xfact = div_rn(dt, dt_old[0]);
+      for (uint32_t i = tid; i < n; i += kW) {
+        m.x[i] = cur[i] + xfact * (cur[i] - prev[i]);
+        m.xo[i] = cur[i];
+      }
+      __syncthreads();
+      apply_limits<kHasB3, kW>(T, rec, m, false, tid);
+      lim_active = T.nlim != 0;
+      __syncthreads();
+      const BlockCompanion c{ag0, ag1, trap, slot(qh, n, 1), ipr};
+      uint32_t iters = 0;
+      fill_sources<kW>(T, rec, sim, vsrc, tid);
+      rc = block_tran_newton<OpT, kHasB3, kW>(D, b, rec, nr, sim, &c, lim_active, false, iters, vsrc, red, tid);
+      lim_active = false;
+      if (rc == 2) {
+        stat[kTsStatus] = kTranLeftTape;
+        break;
+      }
+      stat[kTsAttempts] += 1;
+      stat[kTsNrIters] += iters;
+      if (rc != 0) {
+        stat[kTsRejNewton] += 1;
+        order = 1;
+        dt = div_rn(dt, 8.0);
+        if (dt < P.dt_min) {
+          stat[kTsStatus] = kTranUnderflow;
+          break;
+        }
+        continue;
+      }
+      double dt_next = steps == 0 ? dt : fmin(dt * 2.0, dt_max);
+      if (has_charge) {
+        eval_all<kHasB3, kW>(T, rec, m, false, sim, tid, true);
+        __syncthreads();
+        block_row_charges<kW>(T, m.st, slot(qh, n, 0), tid);
+        state_charges<kW>(T, rec, m.x, slot(qt, nq, 0), tid);
+        __syncthreads();
+      }
+      const double dt1 = dt_old[0], dt2 = dt_old[1];
+      if (has_charge && steps > 0) {
+        const int mth = trap ? 2 : 1;
+        const double del = step_bound<kW>(mth, mth, nq, slot(qt, nq, 0), slot(qt, nq, 1), slot(qt, nq, 2),
+                                          slot(qt, nq, 3), ipt, ag0, ag1, dt, dt1, dt2, P, tid, red);
+        if (!(del >= 0.9 * dt)) {
+          stat[kTsRejLte] += 1;
+          if (del != del) {
+            order = 1;
+            dt = div_rn(dt, 8.0);
+          } else {
+            dt = del;
+          }
+          if (dt < P.dt_min) {
+            stat[kTsStatus] = kTranUnderflow;
+            break;
+          }
+          continue;
+        }
+        dt_next = fmin(fmin(fmax(del, P.dt_min), 2.0 * dt), dt_max);
+      }
+      if (has_charge) {
+        if (steps > 0 && order == 1) {
+          const double trial_del = step_bound<kW>(2, 1, nq, slot(qt, nq, 0), slot(qt, nq, 1), slot(qt, nq, 2),
+                                                  slot(qt, nq, 3), ipt, ag0, ag1, dt, dt1, dt2, P, tid, red);
+          if (trial_del == trial_del) {
+            const double nd2 = fmin(2.0 * dt, trial_del);
+            if (nd2 > 1.05 * dt) order = 2;
+            dt_next = fmin(fmax(nd2, P.dt_min), dt_max);
+          }
+        }
+        // integrator.advanceCurrent over rows and states, then the rotation
+        const double* q0 = slot(qh, n, 0);
+        const double* q1 = slot(qh, n, 1);
+        for (uint32_t i = tid; i < n; i += kW) {
+          const double d = ag0 * (q0[i] - q1[i]);
+          ipr[i] = trap ? d - ag1 * ipr[i] : d;
+        }
+        const double* s0 = slot(qt, nq, 0);
+        const double* s1 = slot(qt, nq, 1);
+        for (uint32_t j = tid; j < nq; j += kW) {
+          const double d = ag0 * (s0[j] - s1[j]);
+          ipt[j] = trap ? d - ag1 * ipt[j] : d;
+        }
+        hb = (hb + 3u) & 3u;
+      }
+      for (int k = 5; k > 0; --k) dt_old[k] = dt_old[k - 1];
+      dt_old[0] = dt;
+      for (uint32_t i = tid; i < n; i += kW) {
+        prev[i] = cur[i];
+        cur[i] = m.x[i];
+      }
+      __syncthreads();
+      t = t + dt;
+      steps += 1;
+      stat[kTsAccepted] += 1;
+      const double t_new = t;
+      if (have_bp) {
+        const bool landed = bp_clamped ? fabs(t_new - bp_next) <= min_break
+                                       : (bp_next - t_new <= delmin || almost_equal_ulps(t_new, bp_next, 100));
+        if (landed) {
+          stat[kTsBpLandings] += 1;
+          order = 1;
+          double shrink = bp_save_dt, nb;
+          if (next_bp<kW>(T, rec, tmr, t_new + min_break, nb, tid, red)) shrink = fmin(shrink, nb - t_new);
+          dt_next = fmin(dt_next, 0.1 * shrink);
+        }
+        have_bp = false;
+      }
+      record(t_new);
+      have_bp = next_bp<kW>(T, rec, tmr, t_new + min_break, bp_next, tid, red);
+      bp_clamped = false;
+      if (have_bp) {
+        const double dt_to_bp = bp_next - t_new;
+        if (dt_to_bp < dt_next) {
+          bp_save_dt = dt_next;
+          dt_next = dt_to_bp;
+          bp_clamped = true;
+        }
+      }
+      dt = dt_next;
+      if (t_new + dt > P.t_stop) dt = P.t_stop - t_new;
+    }
+    if (stat[kTsStatus] == kTranDone && steps >= P.max_steps && !(t >= P.t_stop || almost_equal_ulps(t, P.t_stop, 100)))
+      stat[kTsStatus] = kTranMaxSteps;
+    for (uint32_t i = tid; i < n; i += kW) m.x[i] = cur[i];
+    __syncthreads();
+  }
+  for (uint32_t i = tid; i < n; i += kW) L.x[at + i] = m.x[i];
+  if (tid < kTsN) P.stats[size_t(lane) * kTsN + tid] = stat[tid];
+  if (tid == 0) {
+    if (P.n_pts) P.n_pts[lane] = n_rec;
+    L.status[lane] = kConverged;
+  }
+}
+
+// Persistent grid over the lanes, one CTA per lane at a time; the working
+// set placed as the DC block lanes place it (shared memory, split or slab),
+// the run state in the CTA's part of tslab.
+template <typename OpT, bool kHasB3, uint32_t kW>
+__global__ void __launch_bounds__(kW, 2) tran_block_kernel(BlockDev D, LaneDev L, TranDev P, LaneOpts o,
+                                                          double* tslab, size_t tslab_stride) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint64_t red[kW / 32];
+  unsigned char* own = D.slab + size_t(blockIdx.x) * (D.split ? D.cold_bytes : D.lane_bytes);
+  unsigned char* base = D.in_smem ? smem_raw : own;
+  unsigned char* ring = smem_raw + (D.in_smem ? D.lane_bytes : 0u);
+  double* ts = tslab + size_t(blockIdx.x) * tslab_stride;
+  for (uint32_t lane = blockIdx.x; lane < L.n_lanes; lane += gridDim.x) {
+    block_tran_lane<OpT, kHasB3, kW>(D, L, P, o, base, own, ring, ts, red, lane);
+    __syncthreads();
+  }
+}
+
+template <typename OpT, bool kHasB3>
+cudaError_t launch_tran_t(const BlockDev& D, const LaneDev& L, const TranDev& P, const LaneOpts& o, double* tslab,
+                          size_t tslab_stride, cudaStream_t s) {
+  auto* k = tran_block_kernel<OpT, kHasB3, kBlockThreads>;
+  const size_t smem = (D.in_smem ? D.lane_bytes : 0) + D.ring_bytes;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  const uint32_t grid = D.grid < L.n_lanes ? D.grid : L.n_lanes;
+  k<<<grid > 0 ? grid : 1, kBlockThreads, smem, s>>>(D, L, P, o, tslab, tslab_stride);
+  return cudaGetLastError();
+}
+
 // The eight instantiations: precision x op format x BSIM3.
 #define ESL_BLOCK_DISPATCH(F, ...)                                                     \
   do {                                                                                 \
@@ -735,6 +1212,18 @@ cudaError_t launch_dc_block(const BlockDev& D, const LaneDev& L, const LaneOpts&
                             cudaStream_t s) {
   const bool long_ops = D.op_bytes == 16;
   ESL_BLOCK_DISPATCH(launch_t, D, L, o, s);
+}
+
+size_t tran_block_slab(const TopoDev& T) { return tran_block_slab_doubles(T); }
+
+cudaError_t launch_tran_block(const BlockDev& D, const LaneDev& L, const TranDev& P, const LaneOpts& o, bool has_b3,
+                              double* tslab, cudaStream_t s) {
+  const size_t stride = tran_block_slab_doubles(D.T);
+  if (D.op_bytes == 16)
+    return has_b3 ? launch_tran_t<uint4, true>(D, L, P, o, tslab, stride, s)
+                  : launch_tran_t<uint4, false>(D, L, P, o, tslab, stride, s);
+  return has_b3 ? launch_tran_t<uint2, true>(D, L, P, o, tslab, stride, s)
+                : launch_tran_t<uint2, false>(D, L, P, o, tslab, stride, s);
 }
 
 int block_occupancy(bool mixed, bool long_ops, bool has_b3, size_t smem) {

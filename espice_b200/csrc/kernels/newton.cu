@@ -35,6 +35,7 @@
 #include "bsim3.cuh"
 #include "lane_eval.cuh"
 #include "ladder.cuh"
+#include "tran_core.cuh"
 
 namespace esl {
 
@@ -463,21 +464,20 @@ __global__ void __launch_bounds__(256) dc_newton_kernel(TopoDev T, LaneDev L, La
   for (uint32_t lane = blockIdx.x * warps + w; lane < L.n_lanes; lane += gridDim.x * warps) {
     if constexpr (!kLadder) {
       dc_solve_lane<kHasB3>(T, L, o, prog, block, lane, tid);
-      __syncwarp();
-      continue;
-    }
-    // an operating-point lane: Newton runs until the ladder is done or the
-    // lane pauses for a host factor (a singular host factor ends a run)
-    for (;;) {
-      const uint32_t st = *(volatile uint32_t*)(L.status + lane);
-      if (st == kRunning || (L.resume && st == kNeedSolve)) {
-        dc_solve_lane<kHasB3, true>(T, L, o, prog, block, lane, tid, L.ladder + lane);
-        __syncwarp();
-        if (*(volatile uint32_t*)(L.status + lane) == kNeedSolve) break;
-      } else if (!(st == kSingular && L.ladder[lane].rung != kRungDone)) {
-        break;
+    } else {
+      // an operating-point lane: Newton runs until the ladder is done or the
+      // lane pauses for a host factor (a singular host factor ends a run)
+      for (;;) {
+        const uint32_t st = *(volatile uint32_t*)(L.status + lane);
+        if (st == kRunning || (L.resume && st == kNeedSolve)) {
+          dc_solve_lane<kHasB3, true>(T, L, o, prog, block, lane, tid, L.ladder + lane);
+          __syncwarp();
+          if (*(volatile uint32_t*)(L.status + lane) == kNeedSolve) break;
+        } else if (!(st == kSingular && L.ladder[lane].rung != kRungDone)) {
+          break;
+        }
+        if (!ladder_step(T, L, lane, tid, 32)) break;
       }
-      if (!ladder_step(T, L, lane, tid, 32)) break;
     }
     __syncwarp();
   }
@@ -978,20 +978,6 @@ cudaError_t launch_lane_init(const TopoDev& T, const LaneDev& L, bool cold, bool
 // ---------------------------------------------------------------------------
 namespace {
 
-constexpr double kLteBe = 0.5;            // integrator.lteCoeff, gearCoeff[0]
-constexpr double kLteTrap = 0.08333333333;  // trapCoeff[1]
-
-__device__ __forceinline__ double warp_fmin(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(kFull, v, o));
-  return v;
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = v + __shfl_xor_sync(kFull, v, o);
-  return v;
-}
 
 // One companion step's terms (integrator.zig Hook): rhs += ag0 * (q - q1)
 // (- ag1 * ip for trap), matrix G + ag0 * C.
@@ -1046,47 +1032,9 @@ __device__ __forceinline__ void row_charges(const TopoDev& T, uint32_t prog, con
 
 // The LTE charge states at x (capacitor charges, diode junction charges,
 // MOS1 overlap gate charges).
-__device__ __forceinline__ void state_charges(const TopoDev& T, const double* rec, const double* x, double* out, int tid) {
-  for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
-    const BatchDev& B = T.b[bi];
-    if (B.qt_sites == 0) continue;
-    const int s = static_cast<int>(B.count);
-    for (uint32_t i = tid; i < B.count; i += 32) {
-      const uint32_t* nd = B.nodes + size_t(i) * B.nt;
-      const double* r = rec + B.rec_off + i;
-      double* o = out + B.qt_off + i * B.qt_sites;
-      if (B.type == kC) {
-        o[0] = r[0] * (x[nd[0]] - x[nd[1]]);
-      } else if (B.type == kD) {
-        double q = 0.0, c;
-        if (r[kDHasQ * s] != 0.0) {
-          const double vd = x[nd[2]] - x[nd[1]];
-          double id, gd;
-          diode_iv(r, s, vd, id, gd);
-          diode_qc(r, s, vd, id, gd, q, c);
-        }
-        o[0] = q;
-      } else if (B.type == kM) {
-        const double xg = x[nd[1]];
-        o[0] = r[kMCgs * s] * (xg - x[nd[5]]);
-        o[1] = r[kMCgd * s] * (xg - x[nd[4]]);
-        o[2] = r[kMCgb * s] * (xg - x[nd[3]]);
-      }
-    }
-  }
-}
 
 // The V and I sources' values at `sim` (they depend on the time point and
 // the source scale alone), once for all the Newton iterations there.
-__device__ void fill_sources(const TopoDev& T, const double* rec, const SimDev& sim, double* vcache, int tid) {
-  for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
-    const BatchDev& B = T.b[bi];
-    if (B.type != kV && B.type != kI) continue;
-    for (uint32_t i = tid; i < B.count; i += 32)
-      vcache[B.src_off + i] = source_value(rec + B.rec_off + i, static_cast<int>(B.count), sim);
-  }
-  __syncwarp();
-}
 
 // Newton on one lane (converger.newton at W = 1 on the frozen tape), for
 // the transient's operating point (no companion) and its steps, and for the
@@ -1232,43 +1180,7 @@ __device__ int lane_newton(const TopoDev& T, uint32_t prog, const LaneMem& m, co
 // CKTterr's bound over the LTE states (integrator.zig minDel at w = 1, then
 // the order-2 root): `method` 1 BE / 2 trap probed after a step integrated
 // with `cur`; q0..q3 the ring slots; NaN when a read entry is not finite.
-__device__ __forceinline__ double step_bound(int method, int cur, uint32_t m, const double* q0, const double* q1, const double* q2,
-                             const double* q3, const double* ip, double ag0, double ag1, double dt, double dt1,
-                             double dt2, const TranDev& P, int tid) {
-  const double sum01 = dt + dt1, sum12 = dt1 + dt2, sum012 = dt + (dt1 + dt2);
-  const double coeff = method == 1 ? kLteBe : kLteTrap;
-  double vmin = CUDART_INF, poison = 0.0;
-  for (uint32_t j = tid; j < m; j += 32) {
-    const double qc = q0[j], qp = q1[j], qp2 = q2[j], ipj = ip[j];
-    const double i_new = cur == 2 ? ag0 * (qc - qp) - ag1 * ipj : ag0 * (qc - qp);
-    const double volttol = P.abstol + P.reltol * fmax(fabs(i_new), fabs(ipj));
-    const double chargetol = div_rn(P.reltol * fmax(fmax(fabs(qc), fabs(qp)), P.chgtol), dt);
-    const double tol = fmax(volttol, chargetol);
-    poison += (qc - qc) + (qp - qp) + (qp2 - qp2) + (ipj - ipj);
-    const double f12 = div_rn(qp - qp2, dt1);
-    double dd = div_rn(div_rn(qc - qp, dt) - f12, sum01);
-    if (method != 1) {
-      const double qp3 = q3[j];
-      poison += qp3 - qp3;
-      const double f123 = div_rn(f12 - div_rn(qp2 - qp3, dt2), sum12);
-      dd = div_rn(dd - f123, sum012);
-    }
-    const double del = div_rn(P.trtol * tol, fmax(P.abstol, coeff * fabs(dd)));
-    poison += del == del ? 0.0 : del;
-    vmin = fmin(vmin, del);
-  }
-  vmin = warp_fmin(vmin);
-  poison = warp_sum(poison);
-  if (poison != poison) return CUDART_NAN;
-  return method == 1 ? vmin : sqrt(vmin);
-}
 
-__device__ __forceinline__ bool almost_equal_ulps(double a, double b, long long ulps) {
-  if (a == b) return true;
-  if ((a < 0) != (b < 0)) return false;
-  const long long d = __double_as_longlong(a) - __double_as_longlong(b);
-  return (d < 0 ? -d : d) <= ulps;
-}
 
 // The first PULSE corner at or after `after` over every V source with a
 // PULSE wave (models/vsource.va:133-136: four periodic timers per source).
@@ -1276,82 +1188,12 @@ __device__ __forceinline__ bool almost_equal_ulps(double a, double b, long long 
 // each V source with a PULSE wave) into `tm`: timer k at tm[2 k] (start)
 // and tm[2 k + 1] (period); 4 per V source, start +inf where the source has
 // no PULSE wave. Each lane computes its table once.
-__device__ void pulse_timers(const TopoDev& T, const double* rec, double* tm, int tid) {
-  for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
-    const BatchDev& B = T.b[bi];
-    if (B.type != kV && B.type != kI) continue;
-    const int s = static_cast<int>(B.count);
-    for (uint32_t i = tid; i < B.count; i += 32) {
-      const double* p = rec + B.rec_off + i;
-      double* t = tm + 8 * (B.src_off + i);
-      if (p[1 * s] != 1.0) {
-        for (int k = 0; k < 4; ++k) {
-          t[2 * k] = CUDART_INF;
-          t[2 * k + 1] = 1.0;
-        }
-        continue;
-      }
-      const double tr = p[5 * s] > 1.0e-12 ? p[5 * s] : 1.0e-12;
-      const double tf = p[6 * s] > 1.0e-12 ? p[6 * s] : 1.0e-12;
-      const double pwr = p[7 * s];
-      const double pw = (pwr > 0.0 ? pwr : 0.0) + (-pwr > 0.0 ? -pwr : 0.0) * 1.0e30;
-      double per = p[8 * s];
-      const double per_min = tr + pw + tf + 1.0e-12;
-      if (per < per_min) per = per_min;
-      const double td = p[4 * s];
-      const double st[4] = {td, td + tr, td + tr + pw, td + tr + pw + tf};
-      for (int k = 0; k < 4; ++k) {
-        t[2 * k] = st[k];
-        t[2 * k + 1] = per;
-      }
-    }
-  }
-  __syncwarp();
-}
 
 // The first timer event at or after `after` (tran.zig nextBp), the timers
 // spread over the warp and the earliest taken by a warp minimum: the PULSE
 // corners from the lane's timer table, and each PWL source's one-shot
 // corners (its table times plus TD, and TD itself when the table leaves
 // slots unused, vsource.va:137-200) found in its record.
-__device__ bool next_bp(const TopoDev& T, const double* rec, const double* tm, double after, double& bp) {
-  const int tid = threadIdx.x & 31;
-  double best = CUDART_INF;
-  for (uint32_t k = tid; k < 4 * T.n_src; k += 32) {
-    const double start = tm[2 * k], per = tm[2 * k + 1];
-    if (!(start < CUDART_INF)) continue;
-    double t = start;
-    if (t < after) {
-      const double kk = ceil(div_rn(after - start, per));
-      t = start + kk * per;
-      if (t < after) t += per;
-    }
-    if (t < best) best = t;
-  }
-  for (uint32_t bi = 0; bi < T.n_batches; ++bi) {
-    const BatchDev& B = T.b[bi];
-    if (B.type != kV && B.type != kI) continue;
-    const int s = static_cast<int>(B.count);
-    for (uint32_t i = tid; i < B.count; i += 32) {
-      const double* p = rec + B.rec_off + i;
-      if (p[s] != 4.0) continue;
-      const int len = static_cast<int>(p[2 * s]);
-      const double td = p[4 * s];
-      if (len < kPwlMax && td >= after && td < best) best = td;
-      for (int j = 0; j < len; ++j) {
-        const double c = p[(kSrcPwlT + j) * s] + td;
-        if (c >= after) {
-          if (c < best) best = c;
-          break;  // the table is sorted: the first corner at or after `after`
-        }
-      }
-    }
-  }
-  best = warp_fmin(best);
-  if (best == CUDART_INF) return false;
-  bp = best;
-  return true;
-}
 
 // Streamed measures (src/output/measure.zig, after ngspice com_measure2.c):
 // Cross counts RISE/FALL/CROSS events from a clause's second sample and
@@ -1836,7 +1678,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
       SimDev rs = sim;
       rs.src_scale = run.src;
       rs.gmin = run.gmin_dev;
-      fill_sources(T, rec, rs, vsrc, tid);
+      fill_sources<32>(T, rec, rs, vsrc, tid);
       uint32_t it = 0;
       const int r = lane_newton<kHasB3>(T, prog, m, rec, ro, rs, nullptr, lim_active, carry.init_fix != 0, it, vsrc,
                                         tid, &carry);
@@ -1874,7 +1716,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
       for (uint32_t i = tid; i < 4 * n; i += 32) qh[i] = 0.0;
       __syncwarp();
       row_charges(T, prog, m, qh + n, tid);
-      state_charges(T, rec, m.x, qt + nq, tid);
+      state_charges<32>(T, rec, m.x, qt + nq, tid);
       __syncwarp();
       for (uint32_t i = tid; i < n; i += 32) {
         qh[2 * n + i] = qh[n + i];
@@ -1887,10 +1729,10 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
         ipt[j] = 0.0;
       }
       __syncwarp();
-      pulse_timers(T, rec, tmr, tid);
+      pulse_timers<32>(T, rec, tmr, tid);
       dt = fmin(div_rn(fmin(P.t_step, div_rn(P.t_stop, 100.0)), 10.0), dt_max);
       double bp0;
-      if (next_bp(T, rec, tmr, min_break, bp0)) dt = fmin(dt, 0.1 * bp0);
+      if (next_bp<32>(T, rec, tmr, min_break, bp0, tid, nullptr)) dt = fmin(dt, 0.1 * bp0);
       dt = div_rn(dt, 10.0);
       record(0.0);
     }
@@ -1925,7 +1767,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
       res_step = false;
       Companion c{ag0, ag1, trap, slot(qh, n, 1), ipr};
       uint32_t iters = 0;
-      fill_sources(T, rec, sim, vsrc, tid);
+      fill_sources<32>(T, rec, sim, vsrc, tid);
       rc = lane_newton<kHasB3>(T, prog, m, rec, nr, sim, &c, lim_active, false, iters, vsrc, tid, &carry);
       if (rc == 3) {
         pause(2, ag0);
@@ -1951,14 +1793,14 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
         eval_all<kHasB3>(T, rec, m, false, sim, tid, true);
         __syncwarp();
         row_charges(T, prog, m, slot(qh, n, 0), tid);
-        state_charges(T, rec, m.x, slot(qt, nq, 0), tid);
+        state_charges<32>(T, rec, m.x, slot(qt, nq, 0), tid);
         __syncwarp();
       }
       const double dt1 = dt_old[0], dt2 = dt_old[1];
       if (has_charge && steps > 0) {
         const int mth = trap ? 2 : 1;
-        const double del = step_bound(mth, mth, nq, slot(qt, nq, 0), slot(qt, nq, 1), slot(qt, nq, 2),
-                                      slot(qt, nq, 3), ipt, ag0, ag1, dt, dt1, dt2, P, tid);
+        const double del = step_bound<32>(mth, mth, nq, slot(qt, nq, 0), slot(qt, nq, 1), slot(qt, nq, 2),
+                                      slot(qt, nq, 3), ipt, ag0, ag1, dt, dt1, dt2, P, tid, nullptr);
         if (!(del >= 0.9 * dt)) {
           stat[kTsRejLte] += 1;
           if (del != del) {
@@ -1977,8 +1819,8 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
       }
       if (has_charge) {
         if (steps > 0 && order == 1) {
-          const double trial_del = step_bound(2, 1, nq, slot(qt, nq, 0), slot(qt, nq, 1), slot(qt, nq, 2),
-                                              slot(qt, nq, 3), ipt, ag0, ag1, dt, dt1, dt2, P, tid);
+          const double trial_del = step_bound<32>(2, 1, nq, slot(qt, nq, 0), slot(qt, nq, 1), slot(qt, nq, 2),
+                                              slot(qt, nq, 3), ipt, ag0, ag1, dt, dt1, dt2, P, tid, nullptr);
           if (trial_del == trial_del) {
             const double nd2 = fmin(2.0 * dt, trial_del);
             if (nd2 > 1.05 * dt) order = 2;
@@ -2018,7 +1860,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
           stat[kTsBpLandings] += 1;
           order = 1;
           double shrink = bp_save_dt, nb;
-          if (next_bp(T, rec, tmr, t_new + min_break, nb)) shrink = fmin(shrink, nb - t_new);
+          if (next_bp<32>(T, rec, tmr, t_new + min_break, nb, tid, nullptr)) shrink = fmin(shrink, nb - t_new);
           dt_next = fmin(dt_next, 0.1 * shrink);
         }
         have_bp = false;
@@ -2029,7 +1871,7 @@ __device__ void tran_lane(const TopoDev& T, const LaneDev& L, const TranDev& P, 
         stat[kTsStatus] = kTranResolved;
         break;
       }
-      have_bp = next_bp(T, rec, tmr, t_new + min_break, bp_next);
+      have_bp = next_bp<32>(T, rec, tmr, t_new + min_break, bp_next, tid, nullptr);
       bp_clamped = false;
       if (have_bp) {
         const double dt_to_bp = bp_next - t_new;
@@ -2102,7 +1944,7 @@ __device__ void sweep_lane(const TopoDev& T, const LaneDev& L, const SweepDev& P
   sim.t = 0.0;
   sim.src_scale = 1.0;
   sim.kind = 0;
-  fill_sources(T, rec, sim, vsrc, tid);
+  fill_sources<32>(T, rec, sim, vsrc, tid);
   LaneOpts cold_o = o;
   cold_o.max_iter = 100;
   uint32_t status = kSweepDone;
@@ -2220,7 +2062,7 @@ __device__ void sweep_lane(const TopoDev& T, const LaneDev& L, const SweepDev& P
         rs.src_scale = run.src;
         rs.gmin = run.gmin_dev;
         if (scaled || run.src != 1.0) {
-          fill_sources(T, rec, rs, vsrc, tid);
+          fill_sources<32>(T, rec, rs, vsrc, tid);
           if (tid == 0) vsrc[P.src] = P.values[pt] * run.src;
           __syncwarp();
           scaled = run.src != 1.0;
@@ -2271,7 +2113,7 @@ __device__ void sweep_lane(const TopoDev& T, const LaneDev& L, const SweepDev& P
       rc = mv.result < 3 ? 0 : 1;
       it_total += mv.report;
       if (scaled) {
-        fill_sources(T, rec, sim, vsrc, tid);
+        fill_sources<32>(T, rec, sim, vsrc, tid);
         if (tid == 0) vsrc[P.src] = P.values[pt];
       }
       for (uint32_t i = tid; i < n; i += 32) sol[i] = m.x[i];
