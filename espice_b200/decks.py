@@ -304,3 +304,76 @@ def mesh_gates(size: int, seed: int = 1):
             c.B3(f"mpb{g}", out, ins[1], "vdd", "vdd", w=2 * w, l=0.18e-6, **card_p)
     fr = c.freeze()
     return fr, [fr.slot("vdd", "dc")]
+
+
+C5_T_STOP = 5e-9
+
+
+def digital_block(size: int = 20000, seed: int = 5, n_cells: int = 500, n_inputs: int = 16,
+                  t_stop: float = C5_T_STOP):
+    """The large transient configuration's circuit: a seeded digital block of
+    n_cells BSIM3 NAND2 cells (4 MOSFETs each: 2,000 at the default) on a
+    planar RC parasitic mesh (R log-uniform 10 ohm - 10 kohm, C 1 - 100 fF),
+    about `size` unknowns, driven by n_inputs seeded piecewise-linear pulse
+    trains (0 to 1.8 V, 50 ps edges, through 50 ohm into mesh nodes) over
+    t_stop. Returns (frozen circuit, the MOSFETs' DELVTO slots)."""
+    rng = np.random.default_rng(seed * 104729 + size)
+    n_mesh = max(16, size - n_cells - 2 * n_inputs - 2)
+    cols = int(np.ceil(np.sqrt(n_mesh)))
+    c = Circuit()
+    c.V("vdd", "vdd", "0", dc=1.8)
+    mesh = lambda i: f"m{i}"  # noqa: E731
+    for i in range(n_mesh):
+        r, k = divmod(i, cols)
+        if k + 1 < cols and i + 1 < n_mesh:
+            c.R(f"rh{i}", mesh(i), mesh(i + 1), float(np.exp(rng.uniform(np.log(10), np.log(1e4)))))
+        if i + cols < n_mesh:
+            c.R(f"rv{i}", mesh(i), mesh(i + cols), float(np.exp(rng.uniform(np.log(10), np.log(1e4)))))
+        c.C(f"cm{i}", mesh(i), "0", float(np.exp(rng.uniform(np.log(1e-15), np.log(1e-13)))))
+    c.R("rtie0", mesh(0), "0", 1e3)
+    c.R("rtie1", mesh(n_mesh - 1), "vdd", 1e3)
+    edge = 50e-12
+    for k in range(n_inputs):
+        # a pulse train: a seeded first edge, then widths and gaps of 0.2-1 ns
+        pts, t, level = [(0.0, 0.0)], float(rng.uniform(0.02e-9, 0.5e-9)), 0.0
+        while t + edge < t_stop and len(pts) < 60:
+            pts.append((t, level))
+            level = 1.8 - level
+            pts.append((t + edge, level))
+            t += edge + float(rng.uniform(0.2e-9, 1.0e-9))
+        c.V(f"vin{k}", f"in{k}", "0", pwl=([p[0] for p in pts], [p[1] for p in pts]))
+        c.R(f"rin{k}", f"in{k}", mesh(int(rng.integers(n_mesh))), 50.0)
+
+    def near(i):
+        r, k = divmod(i, cols)
+        while True:
+            rr = int(np.clip(r + rng.integers(-2, 3), 0, (n_mesh - 1) // cols))
+            kk = int(np.clip(k + rng.integers(-2, 3), 0, cols - 1))
+            j = rr * cols + kk
+            if j != i and j < n_mesh:
+                return j
+
+    card_n = dict(type=1.0)
+    card_p = dict(type=-1.0)
+    names = []
+    for g in range(n_cells):
+        w = float(np.exp(rng.uniform(np.log(0.2e-6), np.log(2e-6))))
+        out = int(rng.integers(n_mesh))
+        a = near(out)
+        b = near(out)
+        while b == a:
+            b = near(out)
+        mid = f"x{g}"
+        c.B3(f"mna{g}", mesh(out), mesh(a), mid, "0", w=w, l=0.18e-6, **card_n)
+        c.B3(f"mnb{g}", mid, mesh(b), "0", "0", w=w, l=0.18e-6, **card_n)
+        c.B3(f"mpa{g}", mesh(out), mesh(a), "vdd", "vdd", w=2 * w, l=0.18e-6, **card_p)
+        c.B3(f"mpb{g}", mesh(out), mesh(b), "vdd", "vdd", w=2 * w, l=0.18e-6, **card_p)
+        names += [f"mna{g}", f"mnb{g}", f"mpa{g}", f"mpb{g}"]
+    fr = c.freeze()
+    return fr, [fr.slot(nm, "delvto") for nm in names]
+
+
+def digital_block_vto(n_devices: int, lanes: int, seed: int = 7, sigma: float = 0.02):
+    """Per-device threshold shifts of the large transient configuration's
+    lanes: DELVTO ~ N(0, sigma) per MOSFET and lane, [lanes][n_devices]."""
+    return np.random.default_rng(seed).normal(0.0, sigma, size=(lanes, n_devices))

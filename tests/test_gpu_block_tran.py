@@ -118,3 +118,21 @@ def test_rc_ladder_beyond_the_warp_lanes():
     _check_oracle(res_b, res_o)
     assert (res_b[3][:, 0] == lanes.TRAN_DONE).all()
     print(f"rc ladder: {int(res_b[3][0, 1])} accepted steps a lane, {res_b[5]:.1f} ms")
+
+
+def test_digital_block_20k_unknowns():
+    """The large transient configuration's circuit (20,001 unknowns, 2,000
+    BSIM3 MOSFETs in NAND2 cells on an RC mesh, PWL inputs with 50 ps edges)
+    as two block lanes with per-device threshold shifts over its first
+    100 ps: the oracle's step decisions and final solutions."""
+    fr, slots = decks.digital_block()
+    values = decks.digital_block_vto(len(slots), 2)
+    probes = [fr.unknown("v(m0)")]
+    go = lanes.tran_opts(1e-10, 1e-11, 0.0, max_steps=100_000)
+    oo = oracle.tran_opts(1e-10, 1e-11, 0.0, max_steps=100_000)
+    res_b = _tran(fr, slots, values, go, probes, 1000, lanes.PATH_AUTO)
+    res_o = oracle.tran(fr, slots, values, oo, probes, 1000)
+    _check_oracle(res_b, res_o)
+    assert (res_b[3][:, 0] == lanes.TRAN_DONE).all()
+    print(f"digital block: {int(res_b[3][0, 1])} steps, {int(res_b[3][0, 3])} Newton iterations a lane, "
+          f"{res_b[5]:.0f} ms for 2 lanes")
