@@ -615,6 +615,71 @@ def uneven_c3(args, local, flush, lanes_per_topo=512):
     return out
 
 
+C5_LANES = 256
+C5_WINDOW = 1e-10
+
+
+def large_transient_c5(args, local):
+    """The large transient configuration (C5): the 20,001-unknown digital
+    block (500 BSIM3 NAND2 cells, 2,000 MOSFETs, on a planar RC mesh, 16
+    seeded PWL pulse trains with 50 ps edges), 256 lanes with per-device
+    DELVTO ~ N(0, 20 mV), trapezoidal, on the block lanes (a CTA per lane,
+    the working set in the CTA's global slab). Timed over the first
+    `c5_window` seconds of the 5 ns run with the 5 ns run's maximum step
+    (10 ps), FP64 and mixed precision (FP32 refactor and solves, FP64
+    refinement near convergence), each one persistent launch timed with CUDA
+    events on the context's stream after a 2 ps warm-up run. The lanes'
+    working sets (about 11 MB each) far exceed L2. The FP64 lanes' step
+    decisions equal the oracle's (tests/test_gpu_block_tran.py); here the
+    mixed lanes are checked against the FP64 lanes."""
+    import torch
+    from espice_b200 import decks, lanes
+    fr, slots = decks.digital_block()
+    N, n = args.c5_lanes, fr.n
+    vals = decks.digital_block_vto(len(slots), N)
+    go = lanes.tran_opts(args.c5_window, 1e-11, 1e-11, max_steps=100_000)
+    warm = lanes.tran_opts(2e-12, 1e-11, 1e-11, max_steps=100_000)
+    acc, nri = lanes.TS_FIELDS.index("accepted"), lanes.TS_FIELDS.index("nr_iters")
+    res, info = {}, None
+    for prec, name, skip in ((lanes.PREC_FP64, "fp64", 0.0), (lanes.PREC_MIXED, "mixed", REFINE_SKIP)):
+        ctx = lanes.DcLanes(fr, device=local)
+        ctx.set_mode(precision=prec, path=lanes.PATH_BLOCK, refine_skip=skip)
+        ctx.set_lanes(slots, vals)
+        d_x = torch.zeros((N, n), dtype=torch.float64, device="cuda")
+        d_st = torch.zeros((N, len(lanes.TS_FIELDS)), dtype=torch.int32, device="cuda")
+        ctx.tran_device(warm, d_x.data_ptr(), d_st.data_ptr())
+        ms = ctx.tran_device(go, d_x.data_ptr(), d_st.data_ptr())
+        st = d_st.cpu().numpy().astype(np.int64)
+        corr = ctx.tran_refinements()
+        if info is None:
+            bi = ctx.block_info()
+            info = {k: bi[k] for k in ("a_rows", "a_levels", "a_nops", "ntv", "lane_bytes", "in_smem", "ctas_per_sm")}
+        ctx.close()
+        done = int((st[:, 0] == lanes.TRAN_DONE).sum())
+        steps = int(st[:, acc].sum())
+        iters = int(st[:, nri].sum())
+        res[name] = {"device_ms": ms, "lanes_done": done, "accepted_steps_per_lane": steps / N,
+                     "newton_iters_per_lane": iters / N, "lane_steps_per_s": steps / (ms / 1e3),
+                     "window_lanes_per_s": done / (ms / 1e3), "stats": st, "x": d_x.cpu().numpy()}
+        if prec == lanes.PREC_MIXED:
+            res[name]["refinements_per_newton_iter"] = corr / max(iters, 1)
+    dev, within = _dev(res["mixed"]["x"], res["fp64"]["x"])
+    same = int((res["mixed"]["stats"] == res["fp64"]["stats"]).all(axis=1).sum())
+    for r in res.values():
+        del r["stats"], r["x"]
+    return {"workload": "digital_block: 20,001 unknowns (500 BSIM3 NAND2 cells = 2,000 MOSFETs on a planar RC "
+                        "mesh, R 10-10k log-uniform, C 1-100 fF; 16 seeded PWL pulse trains, 50 ps edges), "
+                        f"{N} lanes, per-device DELVTO ~ N(0, 20 mV), trapezoidal",
+            "window_s": args.c5_window, "t_stop_config_s": 5e-9, "t_max_s": 1e-11, "lanes": N, "unknowns": n,
+            "fp64": res["fp64"], "mixed": res["mixed"],
+            "mixed_over_fp64": res["fp64"]["device_ms"] / res["mixed"]["device_ms"],
+            "mixed_vs_fp64": {"max_rel_dev": dev, "within_1e-9_rel_or_1e-12_abs": within,
+                              "lanes_with_equal_step_statistics": same},
+            "block_lanes": info,
+            "note": "a window of the 5 ns configuration (its whole run would hold the GPU for minutes); "
+                    "lane_steps_per_s = accepted steps of all lanes / device time"}
+
+
 def load_peaks():
     peaks = {}
     try:
@@ -948,6 +1013,8 @@ def our_arm(args, rank, world):
         out["dc_sweep_lanes"] = dc_sweep_lanes(args, local, flush)
         out["ring_period_early_stop"] = ring_period_early_stop(args, local, flush)
         out["uneven_c3"] = uneven_c3(args, local, flush)
+        if args.c5_window > 0:
+            out["large_transient_c5"] = large_transient_c5(args, local)
     print(json.dumps(out), flush=True)
 
 
@@ -967,6 +1034,8 @@ def main():
     ap.add_argument("--train", type=int, default=C4_TRAIN)
     ap.add_argument("--no-side", dest="side", action="store_false")
     ap.add_argument("--t-stop", type=float, default=None)
+    ap.add_argument("--c5-window", type=float, default=C5_WINDOW, help="seconds of the C5 run to time (0: skip)")
+    ap.add_argument("--c5-lanes", type=int, default=C5_LANES)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -260,6 +260,7 @@ struct esl_ctx {
   DevBuf d_sweep_state, d_sweep_rows;  // paused sweep lanes' state
   DevBuf d_tran_state, d_tran_save;    // paused transient lanes' state
   esl_stats last_peels{};              // the last call's peel counts (esl_peel_stats)
+  uint64_t last_tran_refinements = 0;  // the last block transient's FP64 corrections (mixed)
   uint32_t n_seq_a = 0, n_seq = 0, seq_warps = 0;  // lane-interleaved op list
   uint32_t n_seq_f = 0, mixed_warps = 0;            // its forward-only tail, the mixed kernel's warps
   LuJitKernels lu_jit;                               // the tape-compiled lane LU of the current tape
@@ -1581,26 +1582,35 @@ namespace {
 
 // One transient launch over every lane, then the host factors of the lanes
 // that paused (serve_pauses) and resume launches until none pauses.
-// The transient on the block lanes (a CTA per lane, FP64): one persistent
-// launch, every lane's run state in the CTA's part of the transient slab.
-// Lanes whose factor leaves the lead tape stop (kTranLeftTape): no host
-// factor on this path.
+// The transient on the block lanes (a CTA per lane, FP64 or mixed
+// precision): one persistent launch, every lane's run state in the CTA's
+// part of the transient slab. Lanes whose factor leaves the lead tape stop
+// (kTranLeftTape): no host factor on this path.
 int32_t run_tran_block(esl_ctx* ctx, LaneDev L, TranDev P, const LaneOpts& lo) {
   cudaStream_t s = ctx->stream;
   const uint32_t N = ctx->n_lanes;
   if (P.meas) return ctx->fail(ESL_NOT_ELIGIBLE, "the block transient lanes stream no measure cards");
+  const bool mixed = ctx->precision == ESL_PREC_MIXED;
   BlockDev D{};
-  if (int32_t rc = block_view(ctx, false, N, D)) return rc;
+  if (int32_t rc = block_view(ctx, mixed, N, D)) return rc;
+  if (mixed) ESL_CUDA(cudaMemsetAsync(D.refine_out, 0, size_t(N) * 4, s));
   ESL_CUDA(ctx->d_tran_slab.ensure(size_t(D.grid) * tran_block_slab(ctx->topo) * 8));
   ESL_CUDA(ctx->d_x_good.ensure(size_t(N) * ctx->topo.n * 8));
   L.x_good = ctx->d_x_good.as<double>();
   ESL_CUDA(cudaMemsetAsync(L.status, 0, size_t(N) * 4, s));
   std::memset(&ctx->last_peels, 0, sizeof(ctx->last_peels));
   ESL_CUDA(cudaEventRecord(ctx->ev0, s));
-  ESL_CUDA(launch_tran_block(D, L, P, lo, topo_has_b3(ctx->topo), ctx->d_tran_slab.as<double>(), s));
+  ESL_CUDA(launch_tran_block(D, L, P, lo, mixed, topo_has_b3(ctx->topo), ctx->d_tran_slab.as<double>(), s));
   ctx->last_peels.launches = 1;
   ESL_CUDA(cudaEventRecord(ctx->ev1, s));
   ESL_CUDA(cudaEventSynchronize(ctx->ev1));
+  ctx->last_tran_refinements = 0;
+  if (mixed) {
+    std::vector<uint32_t> ref(N);
+    ESL_CUDA(cudaMemcpyAsync(ref.data(), D.refine_out, size_t(N) * 4, cudaMemcpyDeviceToHost, s));
+    ESL_CUDA(cudaStreamSynchronize(s));
+    for (uint32_t v : ref) ctx->last_tran_refinements += v;
+  }
   return ESL_OK;
 }
 
@@ -1655,8 +1665,10 @@ int32_t esl_tran_device(esl_ctx* ctx, const esl_tran_opts* opts, double* d_x, ui
   LaneOpts lo;
   if (int32_t rc = tran_view(ctx, opts, P, lo)) return rc;
   if (int32_t rc = ensure_tape_cold(ctx)) return rc;
-  // the block lanes when asked for, or when a warp lane cannot hold the run
-  const bool block = ctx->path == ESL_PATH_BLOCK || !ctx->warp_ok || ctx->tran_lanes_eff == 0;
+  // the block lanes when asked for, for mixed precision (the warp lanes are
+  // FP64), or when a warp lane cannot hold the run
+  const bool block = ctx->path == ESL_PATH_BLOCK || ctx->precision == ESL_PREC_MIXED || !ctx->warp_ok ||
+                     ctx->tran_lanes_eff == 0;
   P.stats = d_stats;
   P.n_probes = max_pts ? n_probes : 0;
   P.max_pts = max_pts;
@@ -2048,6 +2060,12 @@ int32_t esl_peel_counts(const esl_ctx* ctx, uint32_t* lanes, uint32_t* host_solv
   if (lanes) *lanes = ctx->last_peels.peeled;
   if (host_solves) *host_solves = ctx->last_peels.host_solves;
   if (launches) *launches = ctx->last_peels.launches;
+  return ESL_OK;
+}
+
+int32_t esl_tran_refinements(const esl_ctx* ctx, uint64_t* corrections) {
+  if (!ctx || !corrections) return ESL_INVALID_ARGUMENT;
+  *corrections = ctx->last_tran_refinements;
   return ESL_OK;
 }
 

@@ -723,9 +723,11 @@ int group_occupancy_t(size_t smem) {
 // Transient block lanes (tran.zig Sim.begin / Sim.end and the integrator.zig
 // kernels on a CTA per lane): the warp transient lanes' run, step for step,
 // for circuits whose working set leaves a warp's share of shared memory, and
-// for few lanes (a lane's rows spread over the CTA's 256 threads). FP64; no
-// streamed measures; a lane whose factor leaves the lead tape stops with
-// kTranLeftTape (no host factor).
+// for few lanes (a lane's rows spread over the CTA's 256 threads). FP64, or
+// mixed precision: the FP32 refactor and solves with the step refined in
+// FP64 on the FP64 residual (evaluation, assembly, the companion, the gates
+// and the LTE control stay FP64). No streamed measures; a lane whose factor
+// leaves the lead tape stops with kTranLeftTape (no host factor).
 // ---------------------------------------------------------------------------
 
 // The transient's row charges (q of every row that carries charge cells,
@@ -751,8 +753,9 @@ struct BlockCompanion {
   const double* ip;
 };
 
-template <uint32_t kW>
-__device__ void block_companion(const TopoDev& T, const BlockMem<double>& b, const BlockCompanion& c, int tid) {
+template <typename V, uint32_t kW>
+__device__ void block_companion(const TopoDev& T, const BlockMem<V>& b, const BlockCompanion& c, int tid) {
+  constexpr bool kMixed = sizeof(V) == 4;
   const double* st = b.m.st;
   for (uint32_t i = tid; i < T.n; i += kW) {
     const uint32_t e0 = T.q_ptr[i], e1 = T.q_ptr[i + 1];
@@ -763,16 +766,24 @@ __device__ void block_companion(const TopoDev& T, const BlockMem<double>& b, con
     const double base = b.m.rhs[i] + dq;
     const double r = c.trap ? base - c.ag1 * c.ip[i] : base;
     b.m.rhs[i] = r;
-    b.y[T.pinv[i]] = -r;
+    b.y[T.pinv[i]] = V(-r);
   }
+  // the mixed form adds to the FP64 matrix (the refinement's) and rounds the
+  // sum into the FP32 tape value, so both hold G + ag0 C of the FP64 form
   for (uint32_t p = tid; p < T.nnz; p += kW) {
     const uint32_t e0 = T.c_ptr[p], e1 = T.c_ptr[p + 1];
     if (e0 == e1) continue;
     double s = 0.0;
     for (uint32_t e = e0; e < e1; ++e) s = __dadd_rn(s, st[T.c_src[e]]);
     const uint32_t at = T.amap[p], dr = T.slot_row[p];
-    const double v = b.v[at] + c.ag0 * s;
-    b.v[at] = v;
+    double v;
+    if constexpr (kMixed) {
+      v = b.a64[p] + c.ag0 * s;
+      b.a64[p] = v;
+    } else {
+      v = b.v[at] + c.ag0 * s;
+    }
+    b.v[at] = V(v);
     if (dr != kNoDiag) b.m.diag[dr] = v;
   }
 }
@@ -781,10 +792,15 @@ __device__ void block_companion(const TopoDev& T, const BlockMem<double>& b, con
 // the warp lanes' lane_newton): the companion when cp is given, the
 // gmin-stepping stamps at o.gstamp. Returns 0 converged (x holds the
 // published iterate), 1 out of iterations, 2 a factor left the lead tape.
-template <typename OpT, bool kHasB3, uint32_t kW>
-__device__ int block_tran_newton(const BlockDev& D, const BlockMem<double>& b, const double* rec, const LaneOpts& o,
+// The mixed form (V = float) refactors and solves in FP32 and refines the
+// step in FP64 as the DC block lanes do (block_refine, refine_skip), adding
+// the corrections made to `refinements`.
+template <typename V, typename OpT, bool kHasB3, uint32_t kW>
+__device__ int block_tran_newton(const BlockDev& D, const BlockMem<V>& b, const double* rec, const LaneOpts& o,
                                  const SimDev& sim, const BlockCompanion* cp, bool& lim_active, bool init_fix,
-                                 uint32_t& iters, const double* vsrc, uint64_t* red, int tid) {
+                                 uint32_t& iters, const double* vsrc, uint64_t* red, int tid,
+                                 uint32_t& refinements) {
+  constexpr bool kMixed = sizeof(V) == 4;
   const TopoDev& T = D.T;
   const LaneMem& m = b.m;
   const uint32_t n = T.n;
@@ -795,10 +811,10 @@ __device__ int block_tran_newton(const BlockDev& D, const BlockMem<double>& b, c
     eval_all<kHasB3, kW>(T, rec, m, lim_active, sim, tid, false, vsrc);
     if (tid == 0) m.st[T.n_stage + kGCellX0] = m.x[0];
     __syncthreads();
-    block_assemble<double, kW>(D, b, o.gmin, o.gstamp, tid);
+    block_assemble<V, kW>(D, b, o.gmin, o.gstamp, tid);
     __syncthreads();
     if (cp) {
-      block_companion<kW>(T, b, *cp, tid);
+      block_companion<V, kW>(T, b, *cp, tid);
       __syncthreads();
     }
     if (iter == 0) {
@@ -817,13 +833,28 @@ __device__ int block_tran_newton(const BlockDev& D, const BlockMem<double>& b, c
       const double scale = fmin(fmax(from_bits(xm), from_bits(fm) * gd), 1e18);
       limit = !(1e3 * scale > kXPlausible) ? kXPlausible : 1e3 * scale;
     }
-    if (block_refactor<double, OpT, kW>(D, b.v, b.ring, tid)) {
+    if (block_refactor<V, OpT, kW>(D, b.v, b.ring, tid)) {
       iters = iter + 1;
       return 2;
     }
-    block_rows<double, OpT, kW>(static_cast<const OpT*>(D.b_ops), D.b_rows, b.v, b.ring, tid);
-    for (uint32_t j = tid; j < n; j += kW) b.dx[T.qcol[j]] = b.y[j];
+    block_rows<V, OpT, kW>(static_cast<const OpT*>(D.b_ops), D.b_rows, b.v, b.ring, tid);
+    for (uint32_t j = tid; j < n; j += kW) b.dx[T.qcol[j]] = double(b.y[j]);
     __syncthreads();
+    if constexpr (kMixed) {
+      bool refine = true;
+      if (D.refine_skip > 0.0) {
+        uint64_t q = 0;
+        for (uint32_t i = tid; i < n; i += kW) {
+          const double d = b.dx[i], xo = m.x[i], xn = xo + d;
+          const double tol = o.reltol * fmax(fabs(xn), fabs(xo)) + (T.cur_row[i] ? o.abstol : o.vntol);
+          const double s = div_rn(fabs(d), tol);
+          const uint64_t bits = dbits(s == s ? s : CUDART_INF);
+          q = bits > q ? bits : q;
+        }
+        refine = !(from_bits(block_max_bits<kW>(q, red)) > D.refine_skip);
+      }
+      if (refine) refinements += block_refine<OpT, kW>(D, b, red, tid);
+    }
     // finalizeStep: x_old = x, x += dx, delta score (updateAndNorm)
     uint64_t worst = 0;
     for (uint32_t i = tid; i < n; i += kW) {
@@ -881,14 +912,15 @@ __host__ __device__ inline size_t tran_block_slab_doubles(const TopoDev& T) {
 // One lane's whole transient on the CTA (tran_lane's run): the operating
 // point through op.zig's ladder, then the trapezoidal steps with the
 // predictor, LTE control, order promotion and source breakpoints.
-template <typename OpT, bool kHasB3, uint32_t kW>
+template <typename V, typename OpT, bool kHasB3, uint32_t kW>
 __device__ void block_tran_lane(const BlockDev& D, const LaneDev& L, const TranDev& P, const LaneOpts& o,
                                 unsigned char* base, unsigned char* cold, unsigned char* ring, double* tslab,
                                 uint64_t* red, uint32_t lane) {
   const TopoDev& T = D.T;
   const int tid = threadIdx.x;
   const uint32_t n = T.n, nq = T.n_qt;
-  const BlockMem<double> b = block_carve<double>(D, base, cold, ring, sizeof(OpT));
+  const BlockMem<V> b = block_carve<V>(D, base, cold, ring, sizeof(OpT));
+  uint32_t refinements = 0;
   const LaneMem& m = b.m;
   double* cur = tslab;
   double* prev = cur + n;
@@ -903,9 +935,9 @@ __device__ void block_tran_lane(const BlockDev& D, const LaneDev& L, const TranD
   uint32_t stat[kTsN];
   for (int k = 0; k < kTsN; ++k) stat[k] = 0;
   if (tid == 0) {
-    b.v[T.ntv + n] = 0.0;
-    b.v[T.ntv + n + 1] = 1.0;
-    b.v[T.ntv + n + 2] = 0.0;
+    b.v[T.ntv + n] = V(0);
+    b.v[T.ntv + n + 1] = V(1);
+    b.v[T.ntv + n + 2] = V(0);
     m.st[T.n_stage + kGCellZero] = 0.0;
     m.st[T.n_stage + kGCellOne] = 1.0;
   }
@@ -967,8 +999,8 @@ __device__ void block_tran_lane(const BlockDev& D, const LaneDev& L, const TranD
       rs.gmin = run.gmin_dev;
       fill_sources<kW>(T, rec, rs, vsrc, tid);
       uint32_t it = 0;
-      const int r = block_tran_newton<OpT, kHasB3, kW>(D, b, rec, ro, rs, nullptr, lim_active, mv.init_fix, it, vsrc,
-                                                        red, tid);
+      const int r = block_tran_newton<V, OpT, kHasB3, kW>(D, b, rec, ro, rs, nullptr, lim_active, mv.init_fix, it,
+                                                           vsrc, red, tid, refinements);
       if (r == 2) {
         left = true;
         break;
@@ -1043,7 +1075,8 @@ __device__ void block_tran_lane(const BlockDev& D, const LaneDev& L, const TranD
       const BlockCompanion c{ag0, ag1, trap, slot(qh, n, 1), ipr};
       uint32_t iters = 0;
       fill_sources<kW>(T, rec, sim, vsrc, tid);
-      rc = block_tran_newton<OpT, kHasB3, kW>(D, b, rec, nr, sim, &c, lim_active, false, iters, vsrc, red, tid);
+      rc = block_tran_newton<V, OpT, kHasB3, kW>(D, b, rec, nr, sim, &c, lim_active, false, iters, vsrc, red, tid,
+                                                 refinements);
       lim_active = false;
       if (rc == 2) {
         stat[kTsStatus] = kTranLeftTape;
@@ -1162,13 +1195,14 @@ __device__ void block_tran_lane(const BlockDev& D, const LaneDev& L, const TranD
   if (tid == 0) {
     if (P.n_pts) P.n_pts[lane] = n_rec;
     L.status[lane] = kConverged;
+    if (D.refine_out) D.refine_out[lane] = refinements;
   }
 }
 
 // Persistent grid over the lanes, one CTA per lane at a time; the working
 // set placed as the DC block lanes place it (shared memory, split or slab),
 // the run state in the CTA's part of tslab.
-template <typename OpT, bool kHasB3, uint32_t kW>
+template <typename V, typename OpT, bool kHasB3, uint32_t kW>
 __global__ void __launch_bounds__(kW, 2) tran_block_kernel(BlockDev D, LaneDev L, TranDev P, LaneOpts o,
                                                           double* tslab, size_t tslab_stride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1178,15 +1212,15 @@ __global__ void __launch_bounds__(kW, 2) tran_block_kernel(BlockDev D, LaneDev L
   unsigned char* ring = smem_raw + (D.in_smem ? D.lane_bytes : 0u);
   double* ts = tslab + size_t(blockIdx.x) * tslab_stride;
   for (uint32_t lane = blockIdx.x; lane < L.n_lanes; lane += gridDim.x) {
-    block_tran_lane<OpT, kHasB3, kW>(D, L, P, o, base, own, ring, ts, red, lane);
+    block_tran_lane<V, OpT, kHasB3, kW>(D, L, P, o, base, own, ring, ts, red, lane);
     __syncthreads();
   }
 }
 
-template <typename OpT, bool kHasB3>
+template <typename V, typename OpT, bool kHasB3>
 cudaError_t launch_tran_t(const BlockDev& D, const LaneDev& L, const TranDev& P, const LaneOpts& o, double* tslab,
                           size_t tslab_stride, cudaStream_t s) {
-  auto* k = tran_block_kernel<OpT, kHasB3, kBlockThreads>;
+  auto* k = tran_block_kernel<V, OpT, kHasB3, kBlockThreads>;
   const size_t smem = (D.in_smem ? D.lane_bytes : 0) + D.ring_bytes;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
@@ -1216,14 +1250,11 @@ cudaError_t launch_dc_block(const BlockDev& D, const LaneDev& L, const LaneOpts&
 
 size_t tran_block_slab(const TopoDev& T) { return tran_block_slab_doubles(T); }
 
-cudaError_t launch_tran_block(const BlockDev& D, const LaneDev& L, const TranDev& P, const LaneOpts& o, bool has_b3,
-                              double* tslab, cudaStream_t s) {
+cudaError_t launch_tran_block(const BlockDev& D, const LaneDev& L, const TranDev& P, const LaneOpts& o, bool mixed,
+                              bool has_b3, double* tslab, cudaStream_t s) {
   const size_t stride = tran_block_slab_doubles(D.T);
-  if (D.op_bytes == 16)
-    return has_b3 ? launch_tran_t<uint4, true>(D, L, P, o, tslab, stride, s)
-                  : launch_tran_t<uint4, false>(D, L, P, o, tslab, stride, s);
-  return has_b3 ? launch_tran_t<uint2, true>(D, L, P, o, tslab, stride, s)
-                : launch_tran_t<uint2, false>(D, L, P, o, tslab, stride, s);
+  const bool long_ops = D.op_bytes == 16;
+  ESL_BLOCK_DISPATCH(launch_tran_t, D, L, P, o, tslab, stride, s);
 }
 
 int block_occupancy(bool mixed, bool long_ops, bool has_b3, size_t smem) {

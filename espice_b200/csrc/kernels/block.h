@@ -99,13 +99,15 @@ cudaError_t launch_dc_block_group(const BlockDev* d_Ds, const LaneDev* d_Ls, con
 int block_group_occupancy(bool mixed, bool long_ops, bool has_b3, size_t smem);
 
 // Transient block lanes: every lane's operating point and whole transient
-// (the warp lanes' tran_kernel run, FP64, no measure cards) on a CTA per
-// lane; tslab: the run state, tran_block_slab(T) doubles per CTA of the
-// launch (D.grid, or fewer when there are fewer lanes). A lane whose factor
-// leaves the lead tape stops with kTranLeftTape.
+// (the warp lanes' tran_kernel run, no measure cards) on a CTA per lane,
+// FP64 or mixed precision (FP32 refactor and solves, the step refined in
+// FP64 as the DC block lanes refine it; D.refine_out[lane] gets the lane's
+// corrections); tslab: the run state, tran_block_slab(T) doubles per CTA of
+// the launch (D.grid, or fewer when there are fewer lanes). A lane whose
+// factor leaves the lead tape stops with kTranLeftTape.
 size_t tran_block_slab(const TopoDev& T);
-cudaError_t launch_tran_block(const BlockDev& D, const LaneDev& L, const TranDev& P, const LaneOpts& o, bool has_b3,
-                              double* tslab, cudaStream_t s);
+cudaError_t launch_tran_block(const BlockDev& D, const LaneDev& L, const TranDev& P, const LaneOpts& o, bool mixed,
+                              bool has_b3, double* tslab, cudaStream_t s);
 
 // The lead lane's first Jacobian in pattern order (D.slab as scratch).
 cudaError_t launch_block_lead(const BlockDev& D, const LaneDev& L, uint32_t lane, double* out, bool has_b3,

@@ -34,7 +34,7 @@ EXPORTS = ["esl_create", "esl_destroy", "esl_last_error", "esl_dims", "esl_set_l
            "esl_tran_meas_device", "esl_lu_lanes_compiled_device", "esl_lu_compiled_log",
            "esl_lu_compiled_source", "esl_lu_lanes_mixed_compiled_device", "esl_lu_compiled_mixed_source",
            "esl_set_mode", "esl_block_info", "esl_block_profile", "esl_peel_counts", "esl_op_solve",
-           "esl_op_solve_device"]
+           "esl_op_solve_device", "esl_tran_refinements"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 f64p = ctypes.POINTER(ctypes.c_double)
@@ -386,6 +386,13 @@ class DcLanes:
         self._check(self._L.esl_peel_counts(self._ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
                     "esl_peel_counts")
         return a.value, b.value, c.value
+
+    def tran_refinements(self):
+        """esl_tran_refinements: the FP64 corrections of the last mixed
+        block-lane transient, summed over its lanes."""
+        c = ctypes.c_uint64(0)
+        self._check(self._L.esl_tran_refinements(self._ctx, ctypes.byref(c)), "esl_tran_refinements")
+        return c.value
 
     def block_info(self):
         info = BlockInfo()

@@ -284,7 +284,7 @@ enum {
     ESL_TRAN_UNDERFLOW = 1,  /* TimestepTooSmall */
     ESL_TRAN_OP_FAILED = 2,  /* the operating point did not converge */
     ESL_TRAN_MAX_STEPS = 3,
-    ESL_TRAN_LEFT_TAPE = 4   /* unused: a lane that leaves the lead tape is peeled to the host */
+    ESL_TRAN_LEFT_TAPE = 4   /* a block lane whose factor left the lead tape (the warp lanes peel instead) */
 };
 
 /* Monte-Carlo transient lanes (tran.runGpuLanes, tran.zig:1654, driving
@@ -299,7 +299,17 @@ enum {
  * [n_lanes][ESL_TS_N]; with max_pts > 0, probes [n_probes] unknowns
  * recorded at t = 0 and every accepted step into t_out [n_lanes][max_pts],
  * v_out [n_lanes][max_pts][n_probes], rows per lane in n_pts. ms: the
- * kernel's device time (may be NULL). */
+ * kernel's device time (may be NULL).
+ *
+ * Lane shape (esl_set_mode): the warp lanes for FP64 when the run fits a
+ * warp's share of shared memory, else (or with ESL_PATH_BLOCK, or with
+ * ESL_PREC_MIXED) the block lanes, a CTA per lane. The block lanes stream
+ * no measures and do not peel: a lane whose factor leaves the lead tape
+ * stops with ESL_TRAN_LEFT_TAPE. Their mixed form refactors and solves in
+ * FP32 and refines every Newton step in FP64 on the FP64 residual as the DC
+ * block lanes do (refine_tol, refine_max, refine_skip); evaluation,
+ * assembly, the companion, the Newton gates and the LTE control stay FP64
+ * (esl_tran_refinements counts the corrections). */
 int32_t esl_tran(esl_ctx *ctx, const esl_tran_opts *opts, const uint32_t *probes,
                  uint32_t n_probes, uint32_t max_pts, double *t_out, double *v_out,
                  uint32_t *n_pts, uint32_t *stats, double *x_out, float *ms);
@@ -407,6 +417,12 @@ int32_t esl_block_profile(esl_ctx *ctx, uint64_t *cycles);
  * host factor at least once, host factor + solve calls, and kernel launches
  * (the first and every resume). Any pointer may be NULL. */
 int32_t esl_peel_counts(const esl_ctx *ctx, uint32_t *lanes, uint32_t *host_solves, uint32_t *launches);
+
+/* The FP64 refinement corrections of the context's last transient call on
+ * the block lanes in mixed precision, summed over its lanes (0 after an
+ * FP64 or warp-lane transient). No counterpart in the reference, whose
+ * lane solver is FP64 only. */
+int32_t esl_tran_refinements(const esl_ctx *ctx, uint64_t *corrections);
 
 /* Picks the context's lanes per CTA (1, 2, 4 or 8, as shared memory allows)
  * by timing its DC solve from x0 (NULL: cold) on its current lanes; keeps

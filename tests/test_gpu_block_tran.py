@@ -136,3 +136,68 @@ def test_digital_block_20k_unknowns():
     assert (res_b[3][:, 0] == lanes.TRAN_DONE).all()
     print(f"digital block: {int(res_b[3][0, 1])} steps, {int(res_b[3][0, 3])} Newton iterations a lane, "
           f"{res_b[5]:.0f} ms for 2 lanes")
+
+
+def _tran_mixed(fr, slots, values, go, probes, max_pts, refine_skip):
+    ctx = lanes.DcLanes(fr)
+    ctx.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK, refine_skip=refine_skip)
+    ctx.set_lanes(slots, values)
+    res = ctx.tran(go, probes, max_pts)
+    corrections = ctx.tran_refinements()
+    ctx.close()
+    return res, corrections
+
+
+def _mixed_decks():
+    """(name, circuit, slots, values, t_stop, t_step, probes): a linear RC
+    ladder beyond the warp lanes and a nonlinear BSIM3 inverter chain."""
+    c = Circuit()
+    c.V("vin", "n0", "0", pulse=(0.0, 1.0, 1e-10, 5e-11, 5e-11, 1e-9, 4e-9))
+    for k in range(257):
+        c.R(f"r{k}", f"n{k}", f"n{k + 1}", 100.0)
+        c.C(f"c{k}", f"n{k + 1}", "0", 1e-15)
+    ladder = c.freeze()
+    yield ("rc_ladder", ladder, [ladder.slot("r0", "r")], np.linspace(50.0, 400.0, 8).reshape(-1, 1), 2e-9, 2e-11,
+           [ladder.unknown("v(n1)"), ladder.unknown("v(n257)")])
+    fr, slots, values = decks.bsim3_inverters(seed=5, stages=4, lanes=8, c_load=20e-15,
+                                              pulse=[0.0, 1.8, 0.1e-9, 50e-12, 50e-12, 0.4e-9, 1e-9])
+    yield ("bsim3_chain", fr, slots[1:], values[:, 1:], 2e-9, 10e-12, [fr.unknown("v(s0)"), fr.unknown("v(s3)")])
+
+
+@pytest.mark.parametrize("case", list(range(2)))
+def test_mixed_block_transient_against_oracle(case):
+    """Mixed-precision block transient lanes (FP32 refactor and solves, every
+    Newton step refined in FP64 on the FP64 residual to 1e-12 of it;
+    evaluation, the companion, the gates and the LTE control in FP64): the
+    oracle's (FP64) step decisions on every lane, and waveforms and final
+    solutions within 1e-9 relative or 1e-12 absolute."""
+    name, fr, slots, values, t_stop, t_step, probes = list(_mixed_decks())[case]
+    go = lanes.tran_opts(t_stop, t_step, 0.0, max_steps=100_000)
+    oo = oracle.tran_opts(t_stop, t_step, 0.0, max_steps=100_000)
+    res_m, corrections = _tran_mixed(fr, slots, values, go, probes, 20_000, 0.0)
+    res_o = oracle.tran(fr, slots, values, oo, probes, 20_000)
+    assert (res_m[3][:, 0] == lanes.TRAN_DONE).all()
+    _check_oracle(res_m, res_o)
+    nr = int(res_m[3][:, lanes.TS_FIELDS.index("nr_iters")].sum())
+    assert corrections > 0
+    print(f"{name}: {fr.n} unknowns, {int(res_m[3][0, 1])} steps a lane, "
+          f"{corrections / nr:.2f} FP64 corrections a Newton iteration")
+
+
+def test_mixed_block_transient_refining_near_convergence():
+    """The mixed block transient with refine_skip (steps farther than 1e3
+    tolerances from convergence taken unrefined): every lane finishes, the
+    accepted step counts stay the oracle's and the final solutions are
+    within 1e-9 relative or 1e-12 absolute of it (an unrefined step only
+    moves an iterate the next iteration corrects)."""
+    name, fr, slots, values, t_stop, t_step, probes = list(_mixed_decks())[1]
+    go = lanes.tran_opts(t_stop, t_step, 0.0, max_steps=100_000)
+    oo = oracle.tran_opts(t_stop, t_step, 0.0, max_steps=100_000)
+    (tg, vg, ng, sg, xg, _), corrections = _tran_mixed(fr, slots, values, go, probes, 20_000, 1e3)
+    to, vo, no, so, xo = oracle.tran(fr, slots, values, oo, probes, 20_000)
+    assert (sg[:, 0] == lanes.TRAN_DONE).all()
+    acc = lanes.TS_FIELDS.index("accepted")
+    assert np.array_equal(sg[:, acc], so[:, acc])
+    assert _close(xg, xo).all(), float(np.max(np.abs(xg - xo)))
+    nr = int(sg[:, lanes.TS_FIELDS.index("nr_iters")].sum())
+    print(f"{name}: {corrections / nr:.2f} FP64 corrections a Newton iteration with refine_skip 1e3")
