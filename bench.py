@@ -1036,6 +1036,8 @@ def main():
     ap.add_argument("--t-stop", type=float, default=None)
     ap.add_argument("--c5-window", type=float, default=C5_WINDOW, help="seconds of the C5 run to time (0: skip)")
     ap.add_argument("--c5-lanes", type=int, default=C5_LANES)
+    # the C5 block alone (a small case for a profiler capture of its kernel)
+    ap.add_argument("--only-c5", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -1048,7 +1050,11 @@ def main():
         backend = "nccl" if args.impl == "ours" else "gloo"
         torch.distributed.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     try:
-        if args.impl == "reference":
+        if args.only_c5:
+            import torch
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+            print(json.dumps(large_transient_c5(args, int(os.environ.get("LOCAL_RANK", "0")))), flush=True)
+        elif args.impl == "reference":
             reference_arm(args, rank, world)
         else:
             our_arm(args, rank, world)

@@ -885,16 +885,42 @@ void build_block_gather(const esl_ctx* ctx, uint32_t W, std::vector<uint32_t>& t
   }
 }
 
+void block_layout(const TopoDev& T, uint32_t nv, bool mixed, bool split, BlockDev& D);
+uint32_t block_ring_bytes(uint32_t op_bytes, uint32_t row_k);
+constexpr size_t kBlockSmemRoom = size_t(227) * 1024 - 256;
+
+// Ops a thread a program row: kSlabRowOps when no placement of the working
+// set (whole or its hot part, FP64 or mixed) fits a CTA's shared memory
+// beside the op ring, so that the lanes run from the slab; 1 otherwise.
+uint32_t block_row_k(const TopoDev& T, uint32_t op_bytes) {
+  BlockDev D{};
+  for (int mixed = 0; mixed < 2; ++mixed)
+    for (int split = 0; split < 2; ++split) {
+      block_layout(T, T.nv, mixed != 0, split != 0, D);
+      if (D.lane_bytes + block_ring_bytes(op_bytes, 1) <= kBlockSmemRoom) return 1;
+    }
+  return kSlabRowOps;
+}
+
+// The block programs at rows of k ops a thread, uploaded in the context's
+// op format.
+int32_t set_block_programs(esl_ctx* ctx, uint32_t k) {
+  cudaStream_t s = ctx->stream;
+  const bool short_ops = ctx->block_op_bytes == 8;
+  ctx->bprog = compile_block(ctx->prog, k * kBlockThreads);
+  ctx->bprog.row_k = k;
+  ESL_CUDA(upload(ctx->d_ba, block_words(ctx->bprog.a_ops, short_ops), s));
+  ESL_CUDA(upload(ctx->d_bb, block_words(ctx->bprog.b_ops, short_ops), s));
+  ESL_CUDA(upload(ctx->d_bf, block_words(ctx->bprog.f_ops, short_ops), s));
+  return ESL_OK;
+}
+
 // The block lanes' programs and assembly streams of the current tape.
 int32_t ensure_block(esl_ctx* ctx) {
   if (ctx->have_block) return ESL_OK;
   cudaStream_t s = ctx->stream;
-  ctx->bprog = compile_block(ctx->prog, kBlockThreads);
-  const bool short_ops = ctx->prog.nv < 65536;
-  ctx->block_op_bytes = short_ops ? 8 : 16;
-  ESL_CUDA(upload(ctx->d_ba, block_words(ctx->bprog.a_ops, short_ops), s));
-  ESL_CUDA(upload(ctx->d_bb, block_words(ctx->bprog.b_ops, short_ops), s));
-  ESL_CUDA(upload(ctx->d_bf, block_words(ctx->bprog.f_ops, short_ops), s));
+  ctx->block_op_bytes = ctx->prog.nv < 65536 ? 8 : 16;
+  if (int32_t rc = set_block_programs(ctx, block_row_k(ctx->topo, ctx->block_op_bytes))) return rc;
   std::vector<uint32_t> terms, cells;
   build_block_gather(ctx, kBlockThreads, terms, cells, ctx->block_g_len, ctx->block_g_ncells);
   ESL_CUDA(upload(ctx->d_bg_terms, terms, s));
@@ -903,9 +929,12 @@ int32_t ensure_block(esl_ctx* ctx) {
   return ESL_OK;
 }
 
-// The op ring a block-lane CTA streams its programs through: kDepth + 1
-// slots of one op word per thread (block.cu OpFormat).
-uint32_t block_ring_bytes(uint32_t op_bytes) { return 5u * kBlockThreads * op_bytes; }
+// The op ring a block-lane CTA streams its programs through (block.cu
+// block_rows_k): kDepth + 1 slots of row_k op words per thread, 4 rows
+// ahead for rows of one op a thread, 2 for rows of kSlabRowOps.
+uint32_t block_ring_bytes(uint32_t op_bytes, uint32_t row_k) {
+  return (row_k == 1 ? 5u : 3u) * row_k * kBlockThreads * op_bytes;
+}
 
 // A block lane's working set (block.cu carves the same): the hot part x,
 // rhs, diag, dx (FP64, n each), limited images, the FP64 matrix (mixed
@@ -935,9 +964,8 @@ void block_layout(const TopoDev& T, uint32_t nv, bool mixed, bool split, BlockDe
   D.cold_bytes = uint32_t(split ? at : 0);
 }
 
-// Shared memory a block lane may take (a CTA's 227 KB, less the static
-// reduction words).
-constexpr size_t kBlockSmemRoom = size_t(227) * 1024 - 256;
+// Shared memory a block lane may take (kBlockSmemRoom: a CTA's 227 KB, less
+// the static reduction words).
 
 // The launch view of the block lanes for n_lanes lanes: programs, layout,
 // where the working set lives, the persistent grid and its slab.
@@ -953,7 +981,8 @@ int32_t block_view(esl_ctx* ctx, bool mixed, uint32_t n_lanes, BlockDev& D) {
   D.b_rows = ctx->bprog.b_rows;
   D.f_rows = ctx->bprog.f_rows;
   D.op_bytes = ctx->block_op_bytes;
-  D.ring_bytes = block_ring_bytes(D.op_bytes);
+  D.row_k = ctx->bprog.row_k;
+  D.ring_bytes = block_ring_bytes(D.op_bytes, D.row_k);
   D.g_terms = ctx->d_bg_terms.as<uint32_t>();
   D.g_cells = ctx->d_bg_cells.as<uint4>();
   D.g_len = ctx->block_g_len;
@@ -1861,6 +1890,14 @@ int32_t group_block(esl_ctx* const* ctxs, uint32_t n_ctx, const esl_newton_opts*
   size_t smem = 0, stride = 16;
   for (uint32_t c = 0; c < n_ctx; ++c) {
     esl_ctx* x = ctxs[c];
+    // one op ring for the whole launch: rows of one op a thread for every
+    // topology (a slab topology's wider rows would size every CTA's ring
+    // for them); the context keeps these programs after the group
+    if (int32_t rc = ensure_block(x)) return rc;
+    if (x->bprog.row_k != 1) {
+      if (int32_t rc = set_block_programs(x, 1)) return rc;
+      ESL_CUDA(cudaStreamSynchronize(x->stream));
+    }
     if (int32_t rc = block_view(x, mixed, x->n_lanes, Ds[c])) return rc;
     if (Ds[c].refine_out) ESL_CUDA(cudaMemsetAsync(Ds[c].refine_out, 0, size_t(x->n_lanes) * 4, x->stream));
     ESL_CUDA(cudaStreamSynchronize(x->stream));
@@ -1882,7 +1919,8 @@ int32_t group_block(esl_ctx* const* ctxs, uint32_t n_ctx, const esl_newton_opts*
         x->block_op_bytes = 16;
         if (int32_t rc = block_view(x, mixed, x->n_lanes, Ds[c])) return rc;
       }
-  const uint32_t ring = block_ring_bytes(long_ops ? 16 : 8);
+  uint32_t ring = 0;
+  for (uint32_t c = 0; c < n_ctx; ++c) ring = std::max(ring, block_ring_bytes(long_ops ? 16 : 8, Ds[c].row_k));
   std::vector<BlockDev> Dg = Ds;
   for (uint32_t c = 0; c < n_ctx; ++c) {
     // each topology keeps its own placement (block_view's), the whole

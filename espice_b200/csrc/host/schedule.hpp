@@ -51,7 +51,8 @@ struct Programs {
 // rows), padding as no-ops, plus program F, the forward substitution alone
 // (the mixed form's refinement solves on finished factors).
 struct BlockPrograms {
-  uint32_t width = 0;
+  uint32_t width = 0;  // ops a row: row_k * the CTA's threads
+  uint32_t row_k = 1;  // ops a thread a row
   std::vector<Op4> a_ops, b_ops, f_ops;
   uint32_t a_rows = 0, b_rows = 0, f_rows = 0, a_levels = 0;
 };

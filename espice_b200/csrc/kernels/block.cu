@@ -119,6 +119,38 @@ __device__ __forceinline__ bool run_op(const uint4& op, V* v) {
   return false;
 }
 
+// K independent ops of one row: every operand loaded first, then the
+// results computed and stored in op order (run_op's arithmetic and checks).
+template <typename V, uint32_t K>
+__device__ __forceinline__ bool run_ops(const uint4 (&op)[K], V* v) {
+  V a[K], b[K], d[K];
+#pragma unroll
+  for (uint32_t j = 0; j < K; ++j) {
+    const uint32_t kind = op[j].x >> 28;
+    if (kind != kOpNop) {
+      a[j] = v[op[j].y];
+      b[j] = v[op[j].z];
+      d[j] = v[op[j].x & 0x0fffffffu];
+    }
+  }
+  bool bad = false;
+#pragma unroll
+  for (uint32_t j = 0; j < K; ++j) {
+    const uint32_t kind = op[j].x >> 28;
+    if (kind == kOpNop) continue;
+    V* pd = v + (op[j].x & 0x0fffffffu);
+    if (kind == kOpDivGrowth || kind == kOpDivScaled || kind == kOpDivY) {
+      const V q = op_div(b[j], a[j]);
+      *pd = q;
+      if (kind == kOpDivGrowth) bad |= !(fabs(a[j]) >= growth(a[j]) * fabs(b[j]));
+      if (kind == kOpDivScaled) bad |= !(fabs(q) < inf_of(q));
+    } else if (kind == kOpFlop || b[j] != V(0)) {
+      *pd = op_msub(d[j], a[j], b[j]);
+    }
+  }
+  return bad;
+}
+
 // Op words: 8 bytes {dst | kind << 28, a | b << 16} when the value space
 // has 16-bit indices, 16 bytes {dst | kind << 28, a, b, 0} otherwise. A
 // thread's ring holds kDepth + 1 op words (10 or 20 KB a CTA): kDepth rows
@@ -158,32 +190,71 @@ __device__ __forceinline__ uint4 ld_ring(uint32_t a, uint4*) {
   return r;
 }
 
-// Runs a program over v: row r's op for this thread is ops[r * kW + tid];
-// a CTA barrier after each row. Each thread keeps its next kDepth ops in
-// flight through its ring (slot s at ring + s * kW * sizeof(OpT), one commit
-// group per row), so a row waits only for its own op word, copied kDepth rows
-// earlier. Returns this thread's pivot-test failures.
-template <typename V, typename OpT, uint32_t kW>
-__device__ bool block_rows(const OpT* __restrict__ ops, uint32_t rows, V* v, uint32_t ring, int tid) {
-  constexpr uint32_t D = OpFormat<OpT>::kDepth, kSlot = kW * sizeof(OpT);
+// Runs a program over v: row r holds K * kW ops, this thread's are
+// ops[(r * K + j) * kW + tid] for j < K; a CTA barrier after each row. The
+// ops of a row are independent (no op reads or writes a value another op of
+// the row writes), so a thread loads the operands of all K before it stores
+// any: K loads in flight per thread, the rows' latency paid once per K ops.
+// Each thread keeps its next kDepth rows of op words in flight through its
+// ring (slot s at ring + s * K * kW * sizeof(OpT), op j of the slot
+// j * kW * sizeof(OpT) further, one commit group per row), so a row waits
+// only for its own op words, copied kDepth rows earlier. K = 1 (rows of kW
+// ops, 4 rows ahead) for working sets in shared memory; K = kSlabRowOps (2
+// rows ahead) for working sets in the CTA's global slab, whose operand
+// loads are L2 and HBM round trips. Returns this thread's pivot-test
+// failures.
+template <typename V, typename OpT, uint32_t kW, uint32_t K>
+__device__ bool block_rows_k(const OpT* __restrict__ ops, uint32_t rows, V* v, uint32_t ring, int tid) {
+  constexpr uint32_t D = K == 1 ? OpFormat<OpT>::kDepth : 2u, kSlot = K * kW * sizeof(OpT);
+  constexpr uint32_t kStep = kW * sizeof(OpT);
   for (uint32_t d = 0; d < D; ++d) {
-    if (d < rows) ring_copy(ring + d * kSlot, ops + size_t(d) * kW + tid, sizeof(OpT));
+    if (d < rows)
+#pragma unroll
+      for (uint32_t j = 0; j < K; ++j)
+        ring_copy(ring + d * kSlot + j * kStep, ops + (size_t(d) * K + j) * kW + tid, sizeof(OpT));
     ring_commit();
   }
   bool bad = false;
   uint32_t slot = 0, fill = D;  // the slot of row r, of row r + D
   for (uint32_t r = 0; r < rows; ++r) {
     ring_wait<D - 1>();  // row r's group has landed
-    const uint4 op = OpFormat<OpT>::decode(ld_ring(ring + slot * kSlot, static_cast<OpT*>(nullptr)));
-    if (r + D < rows) ring_copy(ring + fill * kSlot, ops + size_t(r + D) * kW + tid, sizeof(OpT));
-    ring_commit();
+    if constexpr (K == 1) {
+      const uint4 op = OpFormat<OpT>::decode(ld_ring(ring + slot * kSlot, static_cast<OpT*>(nullptr)));
+      if (r + D < rows) ring_copy(ring + fill * kSlot, ops + size_t(r + D) * kW + tid, sizeof(OpT));
+      ring_commit();
+      bad |= run_op(op, v);
+    } else {
+      uint4 op[K];
+#pragma unroll
+      for (uint32_t j = 0; j < K; ++j)
+        op[j] = OpFormat<OpT>::decode(ld_ring(ring + slot * kSlot + j * kStep, static_cast<OpT*>(nullptr)));
+      if (r + D < rows)
+#pragma unroll
+        for (uint32_t j = 0; j < K; ++j)
+          ring_copy(ring + fill * kSlot + j * kStep, ops + (size_t(r + D) * K + j) * kW + tid, sizeof(OpT));
+      ring_commit();
+      bad |= run_ops<V, K>(op, v);
+    }
     slot = slot == D ? 0 : slot + 1;
     fill = fill == D ? 0 : fill + 1;
-    bad |= run_op(op, v);
     __syncthreads();
   }
   ring_wait<0>();
   return bad;
+}
+
+// The wide rows out of line: their K operand sets would otherwise raise the
+// register pressure of every kernel that inlines the one-op rows.
+template <typename V, typename OpT, uint32_t kW>
+__device__ __noinline__ bool block_rows_wide(const OpT* __restrict__ ops, uint32_t rows, V* v, uint32_t ring,
+                                             int tid) {
+  return block_rows_k<V, OpT, kW, kSlabRowOps>(ops, rows, v, ring, tid);
+}
+
+template <typename V, typename OpT, uint32_t kW>
+__device__ bool block_rows(const OpT* __restrict__ ops, uint32_t rows, V* v, uint32_t ring, int tid, uint32_t k) {
+  if (k == kSlabRowOps) return block_rows_wide<V, OpT, kW>(ops, rows, v, ring, tid);
+  return block_rows_k<V, OpT, kW, 1>(ops, rows, v, ring, tid);
 }
 
 // The lane's views into its working set.
@@ -314,7 +385,7 @@ __device__ void block_assemble(const BlockDev& D, const BlockMem<V>& b, double g
 template <typename V, typename OpT, uint32_t kW>
 __device__ bool block_refactor(const BlockDev& D, V* v, uint32_t ring, int tid) {
   const TopoDev& T = D.T;
-  bool bad = block_rows<V, OpT, kW>(static_cast<const OpT*>(D.a_ops), D.a_rows, v, ring, tid);
+  bool bad = block_rows<V, OpT, kW>(static_cast<const OpT*>(D.a_ops), D.a_rows, v, ring, tid, D.row_k);
   const uint32_t l0 = T.nu + T.n;
   for (uint32_t s = tid; s < T.nu; s += kW)
     if (!(fabs(v[s]) < inf_of(v[s]))) bad = true;
@@ -350,8 +421,8 @@ __device__ uint32_t block_refine(const BlockDev& D, const BlockMem<float>& b, ui
     rmax = block_max_abs<kW>(rmax, red);
     bmax = block_max_abs<kW>(bmax, red);
     if (!(rmax > D.refine_tol * bmax) || it >= D.refine_max) break;
-    block_rows<float, OpT, kW>(static_cast<const OpT*>(D.f_ops), D.f_rows, b.v, b.ring, tid);
-    block_rows<float, OpT, kW>(static_cast<const OpT*>(D.b_ops), D.b_rows, b.v, b.ring, tid);
+    block_rows<float, OpT, kW>(static_cast<const OpT*>(D.f_ops), D.f_rows, b.v, b.ring, tid, D.row_k);
+    block_rows<float, OpT, kW>(static_cast<const OpT*>(D.b_ops), D.b_rows, b.v, b.ring, tid, D.row_k);
     for (uint32_t j = tid; j < T.n; j += kW) {
       const uint32_t i = T.qcol[j];
       b.dx[i] = __dadd_rn(b.dx[i], double(b.y[j]));
@@ -474,7 +545,7 @@ __device__ void block_lane(const BlockDev& D, const LaneDev& L, const LaneOpts& 
         }
         return;
       }
-      block_rows<V, OpT, kW>(static_cast<const OpT*>(D.b_ops), D.b_rows, b.v, b.ring, tid);
+      block_rows<V, OpT, kW>(static_cast<const OpT*>(D.b_ops), D.b_rows, b.v, b.ring, tid, D.row_k);
       for (uint32_t j = tid; j < n; j += kW) b.dx[T.qcol[j]] = double(b.y[j]);
       __syncthreads();
       phase_mark(D.prof, kBlockPhaseSolve, t0);
@@ -837,7 +908,7 @@ __device__ int block_tran_newton(const BlockDev& D, const BlockMem<V>& b, const 
       iters = iter + 1;
       return 2;
     }
-    block_rows<V, OpT, kW>(static_cast<const OpT*>(D.b_ops), D.b_rows, b.v, b.ring, tid);
+    block_rows<V, OpT, kW>(static_cast<const OpT*>(D.b_ops), D.b_rows, b.v, b.ring, tid, D.row_k);
     for (uint32_t j = tid; j < n; j += kW) b.dx[T.qcol[j]] = double(b.y[j]);
     __syncthreads();
     if constexpr (kMixed) {

@@ -13,6 +13,9 @@ namespace esl {
 
 // Threads of a block lane's CTA (its program rows are this wide).
 constexpr uint32_t kBlockThreads = 256;
+// Ops per thread in a program row of a working set that lives in the CTA's
+// global slab (rows of kSlabRowOps * kBlockThreads ops); 1 in shared memory.
+constexpr uint32_t kSlabRowOps = 4;
 
 // The block lanes' assembly streams (see block_assemble): a term word is a
 // staging index, with kGTermEnd on a cell's last term. Three cells past the
@@ -29,13 +32,14 @@ constexpr uint32_t kGCellRow = 0x80000000u;
 struct BlockDev {
   TopoDev T;  // the topology's tables (pattern, gathers, tape maps, batches)
   // Programs A (refactor + forward solve), B (back solve) and F (forward
-  // solve alone), rows of kBlockThreads ops, op_bytes each: 8 {dst | kind <<
-  // 28, a | b << 16} (value space below 65,536) or 16 {dst | kind << 28, a,
-  // b, 0}; ring_bytes: the per-CTA ring the ops stream through.
+  // solve alone), rows of row_k * kBlockThreads ops (row_k 1 or
+  // kSlabRowOps), op_bytes each: 8 {dst | kind << 28, a | b << 16} (value
+  // space below 65,536) or 16 {dst | kind << 28, a, b, 0}; ring_bytes: the
+  // per-CTA ring the ops stream through.
   const void* a_ops;
   const void* b_ops;
   const void* f_ops;
-  uint32_t a_rows, b_rows, f_rows, op_bytes, ring_bytes;
+  uint32_t a_rows, b_rows, f_rows, op_bytes, ring_bytes, row_k;
   // The assembly: term stream [g_len][kBlockThreads], cell stream
   // [g_ncells][kBlockThreads] (uint4).
   const uint32_t* g_terms;
