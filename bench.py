@@ -883,8 +883,11 @@ def our_arm(args, rank, world):
     fb.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK, refine_skip=REFINE_SKIP)
 
     # e2e through the public API with host buffers: the points' parameters
-    # in, every point's solution out
+    # in (the lanes' 16 live parameter values from pinned memory, expanded
+    # to the 248 device fields on the device by esl_set_lanes_cols, and the
+    # network's FP32 inputs), every point's solution out to pinned memory
     p_pin = torch.empty((N, p_test.shape[1]), dtype=torch.float32).pin_memory()
+    lp_pin = torch.empty((N, p_test.shape[1]), dtype=torch.float64).pin_memory()
     x_host = torch.empty((N, n), dtype=torch.float64).pin_memory()
     d_p_e = torch.empty((N, p_test.shape[1]), dtype=torch.float32, device="cuda")
     e2e_t, e2e_conv, e2e_fb, h2d, d2h = 0.0, 0, 0, 0, 0
@@ -892,18 +895,20 @@ def our_arm(args, rank, world):
         flush.zero_()
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        vals_h = expand(p_test)
-        mixed.set_lanes(slots, vals_h)
+        lp = lp_pin.numpy()
+        lp[:] = expand.lane_params(p_test)
+        mixed.set_lanes(slots, lp, cols=expand.cols)
         p_pin.copy_(torch.from_numpy(p_test))
         d_p_e.copy_(p_pin)
-        xl, it, conv, nfb = learned.solve(mixed, fb, ws, slots, vals_h, x_nom, k=8, opts=opts, d_values=d_p_e)
+        xl, it, conv, nfb = learned.solve(mixed, fb, ws, slots, lp, x_nom, k=8, opts=opts, d_values=d_p_e,
+                                          cols=expand.cols)
         x_host.copy_(xl)
         t2 = time.perf_counter()
         if i >= 1:
             e2e_t += t2 - t1
             e2e_conv += int(conv.sum())
             e2e_fb += nfb
-            h2d += vals_h.nbytes + p_pin.numel() * 4 + nfb * (vals_h.shape[1] + n) * 8
+            h2d += lp.nbytes + p_pin.numel() * 4 + nfb * (lp.shape[1] + n) * 8
             d2h += N * n * 8 + 2 * N * 4 + nfb * n * 8
 
     # the mixed lanes' phase cycles (one untimed, profiled pass)

@@ -1264,11 +1264,17 @@ int32_t esl_dims(const esl_ctx* ctx, uint32_t* n, uint32_t* nnz) {
 
 int32_t esl_set_lanes(esl_ctx* ctx, const esl_slot* slots, uint32_t n_slots, const double* values,
                       uint32_t n_lanes) {
-  if (!ctx || n_lanes == 0 || (n_slots && (!slots || !values))) return ESL_INVALID_ARGUMENT;
+  return esl_set_lanes_cols(ctx, slots, n_slots, nullptr, values, n_slots, n_lanes);
+}
+
+int32_t esl_set_lanes_cols(esl_ctx* ctx, const esl_slot* slots, uint32_t n_slots, const uint32_t* cols,
+                           const double* values, uint32_t n_cols, uint32_t n_lanes) {
+  if (!ctx || n_lanes == 0 || (n_slots && (!slots || !values || n_cols == 0))) return ESL_INVALID_ARGUMENT;
   for (uint32_t k = 0; k < n_slots; ++k) {
     if (slots[k].batch >= ctx->bats.size()) return ESL_INVALID_ARGUMENT;
     const HostBatch& B = ctx->bats[slots[k].batch];
     if (slots[k].inst >= B.count || slots[k].param >= B.np) return ESL_INVALID_ARGUMENT;
+    if ((cols ? cols[k] : k) >= n_cols) return ESL_INVALID_ARGUMENT;
   }
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
@@ -1295,7 +1301,7 @@ int32_t esl_set_lanes(esl_ctx* ctx, const esl_slot* slots, uint32_t n_slots, con
       it.prm_at = ctx->prm_off[b] + inst * B.np;
       it.slot0 = uint32_t(dslots.size());
       for (; i < keyed.size() && keyed[i].first == ((uint64_t(b) << 32) | inst); ++i)
-        dslots.push_back({slots[keyed[i].second].param, keyed[i].second});
+        dslots.push_back({slots[keyed[i].second].param, cols ? cols[keyed[i].second] : keyed[i].second});
       it.slot1 = uint32_t(dslots.size());
       items.push_back(it);
     }
@@ -1304,12 +1310,12 @@ int32_t esl_set_lanes(esl_ctx* ctx, const esl_slot* slots, uint32_t n_slots, con
   if (!items.empty()) {
     ESL_CUDA(upload(ctx->d_derive_items, items, s));
     ESL_CUDA(upload(ctx->d_derive_slots, dslots, s));
-    ESL_CUDA(ctx->d_values.ensure(size_t(n_lanes) * n_slots * 8));
-    ESL_CUDA(cudaMemcpyAsync(ctx->d_values.p, values, size_t(n_lanes) * n_slots * 8, cudaMemcpyHostToDevice, s));
+    ESL_CUDA(ctx->d_values.ensure(size_t(n_lanes) * n_cols * 8));
+    ESL_CUDA(cudaMemcpyAsync(ctx->d_values.p, values, size_t(n_lanes) * n_cols * 8, cudaMemcpyHostToDevice, s));
   }
   ESL_CUDA(launch_derive_lanes(ctx->d_rec_nominal.as<double>(), uint32_t(R), ctx->d_derive_items.as<DeriveItem>(),
                                uint32_t(items.size()), ctx->d_derive_slots.as<DeriveSlot>(),
-                               ctx->d_params.as<double>(), ctx->d_values.as<double>(), n_slots, n_lanes,
+                               ctx->d_params.as<double>(), ctx->d_values.as<double>(), n_cols, n_lanes,
                                ctx->d_rec.as<double>(), s));
   ctx->rec_lane0.resize(R);
   ESL_CUDA(cudaMemcpyAsync(ctx->rec_lane0.data(), ctx->d_rec.p, R * 8, cudaMemcpyDeviceToHost, s));

@@ -229,7 +229,17 @@ def analog_block(seed: int = 1, rows: int = 20, cols: int = 21, n_ota: int = 20)
         out[:, 8 + n_dev:] = params[:, 9 + group]
         return out
 
+    def lane_params(params):
+        """The points' 16 parameters as the lanes' live parameter values
+        (esl_set_lanes_cols): the temperature in kelvin, the rest as given;
+        slot s takes column expand.cols[s]."""
+        out = np.array(params, np.float64, ndmin=2, copy=True)
+        out[:, 8] += 273.15
+        return out
+
     expand.slots = list(vsl) + list(isl) + list(tsl) + list(dsl)
+    expand.cols = np.concatenate([np.arange(8), np.full(n_dev, 8), 9 + np.asarray(group)]).astype(np.uint32)
+    expand.lane_params = lane_params
     expand.n_devices = n_dev
     return fr, expand
 

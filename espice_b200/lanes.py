@@ -34,7 +34,7 @@ EXPORTS = ["esl_create", "esl_destroy", "esl_last_error", "esl_dims", "esl_set_l
            "esl_tran_meas_device", "esl_lu_lanes_compiled_device", "esl_lu_compiled_log",
            "esl_lu_compiled_source", "esl_lu_lanes_mixed_compiled_device", "esl_lu_compiled_mixed_source",
            "esl_set_mode", "esl_block_info", "esl_block_profile", "esl_peel_counts", "esl_op_solve",
-           "esl_op_solve_device", "esl_tran_refinements"]
+           "esl_op_solve_device", "esl_tran_refinements", "esl_set_lanes_cols"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 f64p = ctypes.POINTER(ctypes.c_double)
@@ -313,13 +313,26 @@ class DcLanes:
         except Exception:
             pass
 
-    def set_lanes(self, slots, values):
-        """values [lanes][len(slots)]: each lane's swept parameter values."""
-        values = np.ascontiguousarray(values, np.float64).reshape(-1, max(1, len(slots)))
+    def set_lanes(self, slots, values, cols=None):
+        """values [lanes][len(slots)]: each lane's swept parameter values; or,
+        with cols (one column per slot), values [lanes][n_cols]: each lane's
+        live parameter values, slot s taking column cols[s]
+        (esl_set_lanes_cols). A C-contiguous float64 array (pinned memory
+        included) is passed without a copy."""
         arr = (Slot * max(1, len(slots)))(*slots)
-        self._check(self._L.esl_set_lanes(self._ctx, arr, ctypes.c_uint32(len(slots)),
-                                          _p(values, f64p), ctypes.c_uint32(values.shape[0])),
-                    "esl_set_lanes")
+        if cols is None:
+            values = np.ascontiguousarray(values, np.float64).reshape(-1, max(1, len(slots)))
+            self._check(self._L.esl_set_lanes(self._ctx, arr, ctypes.c_uint32(len(slots)),
+                                              _p(values, f64p), ctypes.c_uint32(values.shape[0])),
+                        "esl_set_lanes")
+        else:
+            values = np.ascontiguousarray(values, np.float64)
+            values = values.reshape(values.shape[0], -1)
+            c = np.ascontiguousarray(cols, np.uint32)
+            self._check(self._L.esl_set_lanes_cols(self._ctx, arr, ctypes.c_uint32(len(slots)), _p(c, u32p),
+                                                   _p(values, f64p), ctypes.c_uint32(values.shape[1]),
+                                                   ctypes.c_uint32(values.shape[0])),
+                        "esl_set_lanes_cols")
         self.n_lanes = values.shape[0]
 
     def solve(self, x0=None, opts=None):

@@ -64,7 +64,7 @@ class LearnedWarmStart:
         return out.double()
 
 
-def solve(ctx, fallback, ws, slots, values, x_nominal, k=8, opts=None, d_values=None, stats_out=None):
+def solve(ctx, fallback, ws, slots, values, x_nominal, k=8, opts=None, d_values=None, stats_out=None, cols=None):
     """Solves every lane of `ctx` (lanes already set to `values`) from the
     learned guess with at most `k` Newton iterations, then the lanes that did
     not converge again from `x_nominal` on `fallback` (a DcLanes of the same
@@ -74,7 +74,9 @@ def solve(ctx, fallback, ws, slots, values, x_nominal, k=8, opts=None, d_values=
     fallback lanes). The returned x is the learned start's work buffer for
     this batch size: valid until its next solve of the same size. With
     stats_out a list, the solves' statistics (esl_stats dicts) are appended
-    to it."""
+    to it. With cols, `values` are the lanes' live parameter values
+    (DcLanes.set_lanes with cols) and the fallback lanes take them the same
+    way."""
     import torch
     opts = opts or lanes.newton_opts()
     N = values.shape[0]
@@ -93,7 +95,7 @@ def solve(ctx, fallback, ws, slots, values, x_nominal, k=8, opts=None, d_values=
     it = host[1].astype(np.int64)
     failed = np.flatnonzero(st != lanes.LANE_CONVERGED)
     if len(failed):
-        fallback.set_lanes(slots, values[failed])
+        fallback.set_lanes(slots, values[failed], cols=cols)
         xf, itf, stf, sf = fallback.solve(x0=np.broadcast_to(x_nominal, (len(failed), len(x_nominal))), opts=opts)
         if stats_out is not None:
             stats_out.append(sf)

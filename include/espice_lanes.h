@@ -185,6 +185,17 @@ int32_t esl_dims(const esl_ctx *ctx, uint32_t *n, uint32_t *nnz);
 int32_t esl_set_lanes(esl_ctx *ctx, const esl_slot *slots, uint32_t n_slots,
                       const double *values, uint32_t n_lanes);
 
+/* esl_set_lanes with the values of a lane's live parameters: values is
+ * [n_lanes][n_cols] row-major and slot s takes column cols[s] (cols[s] <
+ * n_cols), so one parameter can set many device fields, as a live .param
+ * (include/espice.h:99,310-312, espice_append_points' [count]
+ * [live_param_count] rows) sets every instance that names it. The host
+ * uploads n_lanes * n_cols values; the device expands them while it derives
+ * the records. INVALID_ARGUMENT for a column out of range. */
+int32_t esl_set_lanes_cols(esl_ctx *ctx, const esl_slot *slots, uint32_t n_slots,
+                           const uint32_t *cols, const double *values, uint32_t n_cols,
+                           uint32_t n_lanes);
+
 /* DC Newton for every lane, each bitwise its own converger.run on its own
  * direct solver (sweep/lanes.zig solveBatch, :186-233). Host buffers:
  * x0 [n_lanes][n] start points (NULL: cold, op.zig coldStart), x_out

@@ -65,3 +65,15 @@ def test_points_config_checked_before_the_device():
         with pytest.raises(points.PointsError) as e:
             points.Points(fr, slots, points.OP, [("x1", points.RESULT_UNKNOWN, 1)])
         assert e.value.code == points.PTS_FAILED
+
+
+def test_analog_block_live_parameter_columns():
+    """The analog block's 16 live parameters (temperature in kelvin) taken
+    through its slot-to-column map are its 248 expanded lane values."""
+    import numpy as np
+
+    from espice_b200 import decks
+    fr, expand = decks.analog_block()
+    p, _ = decks.analog_block_params(seed=9, points=64)
+    assert len(expand.cols) == len(expand.slots)
+    assert np.array_equal(expand.lane_params(p)[:, expand.cols], expand(p))

@@ -196,3 +196,26 @@ def test_mesh_gates_20k_unknowns_slab_lanes():
     assert np.array_equal(xb[:2].view(np.uint64), xo.view(np.uint64))
     print(f"20k lanes: {stats['kernel_ms']:.1f} ms for 16 lanes, {itb.mean():.2f} iterations, "
           f"{info['a_rows']} rows in program A over {info['a_levels']} levels")
+
+
+def test_live_parameter_lanes_equal_expanded_lanes():
+    """esl_set_lanes_cols: the analog block's points given as their 16 live
+    parameters with the slot-to-column map solve bitwise as the same points
+    given as their 248 expanded slot values, with the same iteration counts,
+    and both equal the oracle's."""
+    fr, expand = decks.analog_block()
+    params, nominal = decks.analog_block_params(seed=6, points=24)
+    out = []
+    for cols in (None, expand.cols):
+        ctx = lanes.DcLanes(fr)
+        ctx.set_mode(path=lanes.PATH_BLOCK)
+        ctx.set_lanes(expand.slots, expand(params) if cols is None else expand.lane_params(params), cols=cols)
+        out.append(ctx.solve(x0=None))
+        ctx.close()
+    (xa, ita, sta, _), (xb, itb, stb, _) = out
+    assert np.array_equal(xa.view(np.uint64), xb.view(np.uint64))
+    assert np.array_equal(ita, itb) and np.array_equal(sta, stb)
+    xo, ito, cvo = oracle.dc_points(fr, expand.slots, expand(params), warm=None)
+    assert np.array_equal(stb == lanes.LANE_CONVERGED, cvo.astype(bool))
+    assert np.array_equal(itb, ito)
+    assert np.array_equal(xb.view(np.uint64), xo.view(np.uint64))
