@@ -1018,7 +1018,9 @@ def our_arm(args, rank, world):
         out["dc_sweep_lanes"] = dc_sweep_lanes(args, local, flush)
         out["ring_period_early_stop"] = ring_period_early_stop(args, local, flush)
         out["uneven_c3"] = uneven_c3(args, local, flush)
-        if args.c5_window > 0:
+        # one GPU's measurement: under torchrun the other ranks wait at the
+        # closing barrier meanwhile, so it runs only at N = 1
+        if args.c5_window > 0 and world == 1:
             out["large_transient_c5"] = large_transient_c5(args, local)
     print(json.dumps(out), flush=True)
 
