@@ -457,11 +457,37 @@ def dc_grid_diodes(args, local, flush):
         if i >= args.warmup:
             e2e_t.append(t2 - t1)
             e2e_conv += int((sth == lanes.LANE_CONVERGED).sum())
+    # the warp lanes' device-buffer result of the timed steps (from 0 V)
+    d_x.zero_()
+    ctx.solve_device(d_x.data_ptr(), d_it.data_ptr(), d_st.data_ptr(), cold=False, opts=opts)
+    x_fp64 = d_x.cpu().numpy()
+    it_fp64 = d_it.cpu().numpy()
     ctx.close()
+    # the same points in mixed precision (the block lanes: FP32 refactor and
+    # solves, every Newton step refined in FP64 to 1e-12 of the residual)
+    mx = lanes.DcLanes(fr, device=local)
+    mx.set_mode(precision=lanes.PREC_MIXED, path=lanes.PATH_BLOCK)
+    mx.set_lanes(slots, values)
+    mms, mconv = [], 0
+    for i in range(args.warmup + args.steps):
+        d_x.zero_()
+        flush.zero_()
+        torch.cuda.synchronize()
+        s = mx.solve_device(d_x.data_ptr(), d_it.data_ptr(), d_st.data_ptr(), cold=False, opts=opts)
+        if i >= args.warmup:
+            mms.append(s["kernel_ms"])
+            mconv += s["converged"]
+    dev, within = _dev(d_x.cpu().numpy(), x_fp64)
+    same_it = int((d_it.cpu().numpy() == it_fp64).sum())
+    mx.close()
     return {"workload": "grid_diodes: 8x8 R grid (100..10k log-uniform) + 16 diodes (IS=1e-14, N=1, "
                         "RS=10), source swept 0..5 V in 256 independent points from 0 V",
             "value": conv / (sum(ms) / 1e3), "unit": UNIT, "ms_per_step": float(np.mean(ms)),
-            "e2e": conv and e2e_conv / sum(e2e_t)}
+            "e2e": conv and e2e_conv / sum(e2e_t),
+            "mixed_block_lanes": {"value": mconv / (sum(mms) / 1e3), "ms_per_step": float(np.mean(mms)),
+                                  "over_fp64_warp_lanes": (mconv / sum(mms)) / (conv / sum(ms)),
+                                  "max_rel_dev_vs_fp64": dev, "within_1e-9_rel_or_1e-12_abs": within,
+                                  "iterations_equal_fp64": same_it}}
 
 
 def dc_sweep_lanes(args, local, flush):
@@ -764,6 +790,7 @@ def ring_transient(args, rank, world, local, flush):
            "newton_iters_per_point": nr_iters / max(1, ring_steps * N)}
     out["lu_roofline"] = lu_lanes_roofline(fr, ctx, hbm_peak, peak_src)
     out["lu_roofline_warp_per_lane"] = lu_replay_roofline(fr, ctx, hbm_peak, peak_src)
+    out["mixed_block_lanes_2ns"] = ring_mixed_window(fr, slots, values, local, 2e-9)
     if args.cpu_baseline:
         threads = os.cpu_count() or 1
         keep = {}
@@ -773,6 +800,38 @@ def ring_transient(args, rank, world, local, flush):
         out["parity"] = parity_block(keep, sth, xh)
     ctx.close()
     return out
+
+
+def ring_mixed_window(fr, slots, values, local, t_stop):
+    """The ring's lanes in mixed precision (the block lanes: FP32 refactor
+    and solves, every Newton step refined in FP64 to 1e-12 of the residual;
+    the warp lanes are FP64 only) over the first t_stop of the run, against
+    the FP64 warp lanes over the same window: device times of one launch
+    each (CUDA events on the context's stream), the lanes whose step
+    statistics are equal, and the end states' deviation."""
+    import torch
+    from espice_b200 import lanes
+    go, _ = tran_opts_pair(t_stop)
+    N, n = values.shape[0], fr.n
+    res = {}
+    for name, prec, path in (("fp64_warp", lanes.PREC_FP64, lanes.PATH_WARP),
+                             ("mixed_block", lanes.PREC_MIXED, lanes.PATH_BLOCK)):
+        ctx = lanes.DcLanes(fr, device=local)
+        ctx.set_mode(precision=prec, path=path)
+        ctx.set_lanes(slots, values)
+        d_x = torch.zeros((N, n), dtype=torch.float64, device="cuda")
+        d_st = torch.zeros((N, len(lanes.TS_FIELDS)), dtype=torch.int32, device="cuda")
+        ctx.tran_device(tran_opts_pair(1e-11)[0], d_x.data_ptr(), d_st.data_ptr())
+        ms = ctx.tran_device(go, d_x.data_ptr(), d_st.data_ptr())
+        res[name] = (ms, d_st.cpu().numpy(), d_x.cpu().numpy(), ctx.tran_refinements())
+        ctx.close()
+    (mf, sf, xf, _), (mm, sm, xm, corr) = res["fp64_warp"], res["mixed_block"]
+    dev, within = _dev(xm, xf)
+    nr = int(sm[:, lanes.TS_FIELDS.index("nr_iters")].sum())
+    return {"window_s": t_stop, "lanes": N, "fp64_warp_ms": mf, "mixed_block_ms": mm,
+            "mixed_over_fp64": mf / mm, "lanes_with_equal_step_statistics": int((sm == sf).all(axis=1).sum()),
+            "max_rel_dev_vs_fp64": dev, "within_1e-9_rel_or_1e-12_abs": within,
+            "refinements_per_newton_iter": corr / max(nr, 1)}
 
 
 def our_arm(args, rank, world):
