@@ -433,6 +433,30 @@ __device__ uint32_t block_refine(const BlockDev& D, const BlockMem<float>& b, ui
   return made;
 }
 
+// The mixed form's refinement of a Newton step (dx in unknown order, x the
+// iterate it moves): every step, or with refine_skip > 0 only a step whose
+// FP32 solution scores within refine_skip tolerances of the Newton delta
+// test (a step farther out is taken as an inexact Newton step: its FP32
+// error, about 1e-7 of the step, is far below what the next iterate still
+// corrects). Returns the corrections made.
+template <typename OpT, uint32_t kW>
+__device__ uint32_t block_refine_step(const BlockDev& D, const BlockMem<float>& b, const LaneOpts& o, uint64_t* red,
+                                      int tid) {
+  const TopoDev& T = D.T;
+  if (D.refine_skip > 0.0) {
+    uint64_t q = 0;
+    for (uint32_t i = tid; i < T.n; i += kW) {
+      const double d = b.dx[i], xo = b.m.x[i], xn = xo + d;
+      const double tol = o.reltol * fmax(fabs(xn), fabs(xo)) + (T.cur_row[i] ? o.abstol : o.vntol);
+      const double s = div_rn(fabs(d), tol);
+      const uint64_t bits = dbits(s == s ? s : CUDART_INF);
+      q = bits > q ? bits : q;
+    }
+    if (from_bits(block_max_bits<kW>(q, red)) > D.refine_skip) return 0;
+  }
+  return block_refine<OpT, kW>(D, b, red, tid);
+}
+
 // Phase profile: thread 0 adds the cycles since `t` to prof[phase] and
 // restarts the clock (nothing when profiling is off).
 __device__ __forceinline__ void phase_mark(unsigned long long* prof, uint32_t phase, long long& t) {
@@ -550,22 +574,7 @@ __device__ void block_lane(const BlockDev& D, const LaneDev& L, const LaneOpts& 
       __syncthreads();
       phase_mark(D.prof, kBlockPhaseSolve, t0);
       if constexpr (kMixed) {
-        bool refine = true;
-        if (D.refine_skip > 0.0) {
-          // an inexact Newton step far from convergence keeps its FP32 error
-          // (about 1e-7 of the step, far below what the next iterate
-          // corrects); the steps nearer convergence are refined
-          uint64_t q = 0;
-          for (uint32_t i = tid; i < n; i += kW) {
-            const double d = b.dx[i], xo = m.x[i], xn = xo + d;
-            const double tol = o.reltol * fmax(fabs(xn), fabs(xo)) + (T.cur_row[i] ? o.abstol : o.vntol);
-            const double s = div_rn(fabs(d), tol);
-            const uint64_t bits = dbits(s == s ? s : CUDART_INF);
-            q = bits > q ? bits : q;
-          }
-          refine = !(from_bits(block_max_bits<kW>(q, red)) > D.refine_skip);
-        }
-        if (refine) refinements += block_refine<OpT, kW>(D, b, red, tid);
+        refinements += block_refine_step<OpT, kW>(D, b, o, red, tid);
         phase_mark(D.prof, kBlockPhaseRefine, t0);
       }
     }
@@ -911,21 +920,7 @@ __device__ int block_tran_newton(const BlockDev& D, const BlockMem<V>& b, const 
     block_rows<V, OpT, kW>(static_cast<const OpT*>(D.b_ops), D.b_rows, b.v, b.ring, tid, D.row_k);
     for (uint32_t j = tid; j < n; j += kW) b.dx[T.qcol[j]] = double(b.y[j]);
     __syncthreads();
-    if constexpr (kMixed) {
-      bool refine = true;
-      if (D.refine_skip > 0.0) {
-        uint64_t q = 0;
-        for (uint32_t i = tid; i < n; i += kW) {
-          const double d = b.dx[i], xo = m.x[i], xn = xo + d;
-          const double tol = o.reltol * fmax(fabs(xn), fabs(xo)) + (T.cur_row[i] ? o.abstol : o.vntol);
-          const double s = div_rn(fabs(d), tol);
-          const uint64_t bits = dbits(s == s ? s : CUDART_INF);
-          q = bits > q ? bits : q;
-        }
-        refine = !(from_bits(block_max_bits<kW>(q, red)) > D.refine_skip);
-      }
-      if (refine) refinements += block_refine<OpT, kW>(D, b, red, tid);
-    }
+    if constexpr (kMixed) refinements += block_refine_step<OpT, kW>(D, b, o, red, tid);
     // finalizeStep: x_old = x, x += dx, delta score (updateAndNorm)
     uint64_t worst = 0;
     for (uint32_t i = tid; i < n; i += kW) {
